@@ -1,0 +1,312 @@
+"""Host-side mirror of the Geneva matching path over the native C ABI.
+
+The reference exposes its GPU path as C++ functions and a CLI:
+
+    loadDataBase(mygraph, metadata)            src/loadDataBase.cpp:309
+    genMatchOrder(query, ...)                  src/genMatchOrder.cpp:672
+    genMatchOrderSingleV(query, ...)           src/genMatchOrderSingleV.cpp:678
+    gpumine <mygraph> <metadata> <query>       src/gpumine.cpp:866
+    gpumineSV <mygraph> <metadata> <query>     src/gpumine_singleV.cpp:722
+
+This module offers the same operations with the same argument meaning on top
+of ``libgeneva.so`` (include/geneva.h), loaded with ctypes.  The CUDA kernels
+are the only compute path: if the library is missing, every call raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from dataclasses import dataclass
+from pathlib import Path
+from typing import List, Optional, Sequence
+
+import numpy as np
+
+__all__ = [
+    "GenevaError", "Database", "probe_graph", "Plan", "Result", "MODE_DV", "MODE_SV", "library", "library_path",
+    "loadDataBase", "genMatchOrder", "genMatchOrderSingleV", "match", "gpumine", "gpumineSV",
+]
+
+MODE_DV = 0
+MODE_SV = 1
+
+_PKG = Path(__file__).resolve().parent
+_LIB = None
+
+
+class GenevaError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__(f"[{status}] {message}")
+        self.status = status
+
+
+def library_path() -> Path:
+    return _PKG / "lib" / "libgeneva.so"
+
+
+class _DbInfo(ctypes.Structure):
+    _fields_ = [("max_vertex_id", ctypes.c_uint32), ("num_vertex_labels", ctypes.c_uint32),
+                ("num_partitions", ctypes.c_uint32), ("reserved", ctypes.c_uint32),
+                ("num_adjacency", ctypes.c_uint64), ("device_bytes", ctypes.c_uint64)]
+
+
+class _MatchOpts(ctypes.Structure):
+    _fields_ = [("stream", ctypes.c_void_p), ("budget_bytes", ctypes.c_uint64),
+                ("count_only", ctypes.c_int), ("reserved", ctypes.c_int)]
+
+
+def _declare(lib):
+    P = ctypes.POINTER
+    vp, u32, u64, i32, sz, cp = (ctypes.c_void_p, ctypes.c_uint32, ctypes.c_uint64, ctypes.c_int,
+                                 ctypes.c_size_t, ctypes.c_char_p)
+    sig = {
+        "gva_last_error": (cp, []),
+        "gva_status_string": (cp, [i32]),
+        "gva_version": (cp, []),
+        "gva_db_load": (i32, [cp, cp, i32, P(vp)]),
+        "gva_db_from_edges": (i32, [vp, u32, vp, vp, vp, u64, i32, P(vp)]),
+        "gva_db_get_info": (i32, [vp, P(_DbInfo)]),
+        "gva_db_warnings": (cp, [vp]),
+        "gva_graph_probe": (i32, [cp, cp, P(_DbInfo), ctypes.c_char_p, sz]),
+        "gva_db_free": (None, [vp]),
+        "gva_plan_from_file": (i32, [cp, i32, P(vp)]),
+        "gva_plan_from_text": (i32, [cp, i32, P(vp)]),
+        "gva_plan_describe": (sz, [vp, ctypes.c_char_p, sz]),
+        "gva_plan_num_phases": (i32, [vp]),
+        "gva_plan_num_vertices": (i32, [vp]),
+        "gva_plan_column_vertices": (i32, [vp, P(u32), i32]),
+        "gva_plan_free": (None, [vp]),
+        "gva_match": (i32, [vp, vp, P(_MatchOpts), P(vp)]),
+        "gva_result_num_rows": (u64, [vp]),
+        "gva_result_num_columns": (i32, [vp]),
+        "gva_result_phase_rows": (i32, [vp, P(u64), i32]),
+        "gva_result_device_rows": (vp, [vp]),
+        "gva_result_copy_rows": (i32, [vp, vp, u64, u64]),
+        "gva_result_write_text": (i32, [vp, cp]),
+        "gva_result_gpu_ms": (ctypes.c_double, [vp]),
+        "gva_result_free": (None, [vp]),
+        "gva_plan_num_steps": (i32, [vp, vp]),
+        "gva_plan_step_width_in": (i32, [vp, vp, i32]),
+        "gva_plan_step_width_out": (i32, [vp, vp, i32]),
+        "gva_step_scratch_bytes": (sz, [u64]),
+        "gva_step_run": (i32, [vp, vp, i32, vp, u64, vp, u64, P(u64), vp, sz, vp]),
+    }
+    for name, (res, args) in sig.items():
+        f = getattr(lib, name)
+        f.restype = res
+        f.argtypes = args
+    return lib
+
+
+def library():
+    """The loaded native library (built by geneva_b200.build)."""
+    global _LIB
+    if _LIB is None:
+        path = library_path()
+        if not path.exists():
+            raise GenevaError(6, f"native library missing: {path} (run python -m geneva_b200.build)")
+        _LIB = _declare(ctypes.CDLL(str(path)))
+    return _LIB
+
+
+def _check(status: int):
+    if status != 0:
+        lib = library()
+        raise GenevaError(status, lib.gva_last_error().decode())
+
+
+class Database:
+    """Device-resident database (gva_db)."""
+
+    def __init__(self, handle):
+        self._h = ctypes.c_void_p(handle)
+
+    @classmethod
+    def load(cls, mygraph: str, metadata: str, device: int = 0) -> "Database":
+        h = ctypes.c_void_p()
+        _check(library().gva_db_load(str(mygraph).encode(), str(metadata).encode(), device, ctypes.byref(h)))
+        return cls(h.value)
+
+    @classmethod
+    def from_edges(cls, vertex_labels, src, dst, edge_labels, device: int = 0) -> "Database":
+        vl = np.ascontiguousarray(vertex_labels, dtype=np.uint32)
+        s = np.ascontiguousarray(src, dtype=np.uint32)
+        d = np.ascontiguousarray(dst, dtype=np.uint32)
+        el = np.ascontiguousarray(edge_labels, dtype=np.uint32)
+        h = ctypes.c_void_p()
+        _check(library().gva_db_from_edges(vl.ctypes.data, len(vl) - 1, s.ctypes.data, d.ctypes.data,
+                                           el.ctypes.data, len(s), device, ctypes.byref(h)))
+        return cls(h.value)
+
+    def info(self) -> dict:
+        i = _DbInfo()
+        _check(library().gva_db_get_info(self._h, ctypes.byref(i)))
+        return {f: getattr(i, f) for f, _ in _DbInfo._fields_ if f != "reserved"}
+
+    @property
+    def warnings(self) -> str:
+        return library().gva_db_warnings(self._h).decode()
+
+    def close(self):
+        if self._h:
+            library().gva_db_free(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def probe_graph(mygraph: str, metadata: str) -> dict:
+    """Host-only parse of a .mygraph/.metadata pair (gva_graph_probe)."""
+    i = _DbInfo()
+    buf = ctypes.create_string_buffer(4096)
+    _check(library().gva_graph_probe(str(mygraph).encode(), str(metadata).encode(), ctypes.byref(i), buf, 4096))
+    d = {f: getattr(i, f) for f, _ in _DbInfo._fields_ if f != "reserved"}
+    d["warnings"] = buf.value.decode()
+    return d
+
+
+class Plan:
+    """Match order + restrictions (gva_plan)."""
+
+    def __init__(self, handle):
+        self._h = ctypes.c_void_p(handle)
+
+    @classmethod
+    def from_text(cls, text: str, mode: int = MODE_DV) -> "Plan":
+        h = ctypes.c_void_p()
+        _check(library().gva_plan_from_text(text.encode(), mode, ctypes.byref(h)))
+        return cls(h.value)
+
+    @classmethod
+    def from_file(cls, path: str, mode: int = MODE_DV) -> "Plan":
+        h = ctypes.c_void_p()
+        _check(library().gva_plan_from_file(str(path).encode(), mode, ctypes.byref(h)))
+        return cls(h.value)
+
+    def describe(self) -> str:
+        lib = library()
+        n = lib.gva_plan_describe(self._h, None, 0)
+        buf = ctypes.create_string_buffer(n + 1)
+        lib.gva_plan_describe(self._h, buf, n + 1)
+        return buf.value.decode()
+
+    @property
+    def columns(self) -> List[int]:
+        arr = (ctypes.c_uint32 * 32)()
+        n = library().gva_plan_column_vertices(self._h, arr, 32)
+        return list(arr[:n])
+
+    @property
+    def num_phases(self) -> int:
+        return library().gva_plan_num_phases(self._h)
+
+    def close(self):
+        if self._h:
+            library().gva_plan_free(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Result:
+    """Final frontier on the device plus per-phase row counts (gva_result)."""
+
+    def __init__(self, handle):
+        self._h = ctypes.c_void_p(handle)
+
+    @property
+    def num_rows(self) -> int:
+        return int(library().gva_result_num_rows(self._h))
+
+    @property
+    def num_columns(self) -> int:
+        return int(library().gva_result_num_columns(self._h))
+
+    @property
+    def phase_rows(self) -> List[int]:
+        arr = (ctypes.c_uint64 * 64)()
+        n = library().gva_result_phase_rows(self._h, arr, 64)
+        return [int(x) for x in arr[:n]]
+
+    @property
+    def gpu_ms(self) -> float:
+        return float(library().gva_result_gpu_ms(self._h))
+
+    @property
+    def device_ptr(self) -> Optional[int]:
+        return library().gva_result_device_rows(self._h)
+
+    def rows(self, first: int = 0, count: Optional[int] = None, out: Optional[np.ndarray] = None) -> np.ndarray:
+        n = self.num_rows - first if count is None else count
+        w = self.num_columns
+        if out is None:
+            out = np.empty((n, w), dtype=np.uint32)
+        if n:
+            _check(library().gva_result_copy_rows(self._h, out.ctypes.data, first, n))
+        return out
+
+    def write_text(self, path: str):
+        _check(library().gva_result_write_text(self._h, str(path).encode()))
+
+    def close(self):
+        if self._h:
+            library().gva_result_free(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def match(db: Database, plan: Plan, stream: Optional[int] = None, budget_bytes: int = 0,
+          count_only: bool = False) -> Result:
+    """Runs every phase of `plan` on `db` (gva_match)."""
+    o = _MatchOpts(stream or None, budget_bytes, 1 if count_only else 0, 0)
+    h = ctypes.c_void_p()
+    _check(library().gva_match(db._h, plan._h, ctypes.byref(o), ctypes.byref(h)))
+    return Result(h.value)
+
+
+# ---- reference-named entry points -------------------------------------------
+
+def loadDataBase(mygraph: str, metadata: str, device: int = 0) -> Database:
+    """src/loadDataBase.cpp:309 — here the database lands in HBM directly."""
+    return Database.load(mygraph, metadata, device)
+
+
+def genMatchOrder(query: str) -> Plan:
+    """src/genMatchOrder.cpp:672 — `query` is a .query path or its text."""
+    return Plan.from_file(query, MODE_DV) if os.path.exists(str(query)) else Plan.from_text(query, MODE_DV)
+
+
+def genMatchOrderSingleV(query: str) -> Plan:
+    """src/genMatchOrderSingleV.cpp:678."""
+    return Plan.from_file(query, MODE_SV) if os.path.exists(str(query)) else Plan.from_text(query, MODE_SV)
+
+
+def gpumine(mygraph: str, metadata: str, query: str, out: str = "partialResultsGPU.txt",
+            mode: int = MODE_DV) -> Result:
+    """The gpumine driver (src/gpumine.cpp:866-1072) as a function: loads,
+    plans, matches and writes the match-ordered rows to `out`."""
+    db = loadDataBase(mygraph, metadata)
+    plan = genMatchOrder(query) if mode == MODE_DV else genMatchOrderSingleV(query)
+    res = match(db, plan)
+    if out:
+        res.write_text(out)
+    res._db, res._plan = db, plan  # keep alive with the result
+    return res
+
+
+def gpumineSV(mygraph: str, metadata: str, query: str, out: str = "partialResultsGPU.txt") -> Result:
+    """The gpumineSV driver (src/gpumine_singleV.cpp:722-928)."""
+    return gpumine(mygraph, metadata, query, out, MODE_SV)

@@ -1,0 +1,308 @@
+// extern "C" boundary (include/geneva.h).  Handles own their memory; every
+// entry point returns a status and records a message for gva_last_error().
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <fstream>
+#include <sstream>
+
+#include "../../include/geneva.h"
+#include "gva_engine.cuh"
+#include "gva_internal.h"
+
+namespace gva {
+const char* last_error_cstr();
+}
+
+using namespace gva;
+
+struct gva_db {
+    DevDB* dev = nullptr;
+    std::string warnings;
+};
+struct gva_plan {
+    Plan plan;
+    // steps are lowered per database (labels differ); cache the last lowering
+    const gva_db* lowered_for = nullptr;
+    std::vector<Step> steps;
+};
+struct gva_result {
+    MatchResult r;
+};
+
+namespace {
+
+int steps_for(const gva_plan* p, const gva_db* db, std::vector<Step>& out) {
+    return lower_plan(p->plan, db->dev->meta, out);
+}
+
+int read_file(const char* path, std::string& out) {
+    std::ifstream f(path, std::ios::binary);
+    if (!f.is_open()) return fail(GVA_ERR_IO, std::string("cannot open ") + path);
+    std::ostringstream ss;
+    ss << f.rdbuf();
+    out = ss.str();
+    return GVA_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* gva_last_error(void) { return last_error_cstr(); }
+
+const char* gva_status_string(int s) {
+    switch (s) {
+        case GVA_OK: return "ok";
+        case GVA_ERR_IO: return "i/o error";
+        case GVA_ERR_FORMAT: return "format error";
+        case GVA_ERR_CUDA: return "cuda error";
+        case GVA_ERR_NOMEM: return "out of memory";
+        case GVA_ERR_ARG: return "bad argument";
+        case GVA_ERR_UNSUPPORTED: return "unsupported";
+        default: return "unknown status";
+    }
+}
+
+const char* gva_version(void) { return "geneva_b200 0.1 (sm_100a)"; }
+
+int gva_db_load(const char* mygraph_path, const char* metadata_path, int device, gva_db** out) {
+    if (!out || !mygraph_path || !metadata_path) return fail(GVA_ERR_ARG, "null argument");
+    *out = nullptr;
+    HostGraph g;
+    std::string warn;
+    int st = load_mygraph(mygraph_path, metadata_path, g, &warn);
+    if (st) return st;
+    DevDB* dev = nullptr;
+    st = upload_graph(g, device, dev);
+    if (st) return st;
+    gva_db* h = new gva_db();
+    h->dev = dev;
+    h->warnings = warn;
+    *out = h;
+    return GVA_OK;
+}
+
+int gva_db_from_edges(const uint32_t* vertex_labels, uint32_t max_vertex_id, const uint32_t* src, const uint32_t* dst,
+                      const uint32_t* edge_labels, uint64_t num_edges, int device, gva_db** out) {
+    if (!out) return fail(GVA_ERR_ARG, "null argument");
+    *out = nullptr;
+    HostGraph g;
+    int st = graph_from_edges(vertex_labels, max_vertex_id, src, dst, edge_labels, num_edges, g);
+    if (st) return st;
+    DevDB* dev = nullptr;
+    st = upload_graph(g, device, dev);
+    if (st) return st;
+    gva_db* h = new gva_db();
+    h->dev = dev;
+    *out = h;
+    return GVA_OK;
+}
+
+int gva_db_get_info(const gva_db* db, gva_db_info* out) {
+    if (!db || !out) return fail(GVA_ERR_ARG, "null argument");
+    memset(out, 0, sizeof *out);
+    out->max_vertex_id = db->dev->max_id;
+    out->num_vertex_labels = db->dev->L;
+    out->num_partitions = (uint32_t)db->dev->parts.size();
+    out->num_adjacency = db->dev->n_adj;
+    out->device_bytes = db->dev->arena_bytes;
+    return GVA_OK;
+}
+
+int gva_graph_probe(const char* mygraph_path, const char* metadata_path, gva_db_info* out, char* warn, size_t cap) {
+    if (!mygraph_path || !metadata_path || !out) return fail(GVA_ERR_ARG, "null argument");
+    HostGraph g;
+    std::string w;
+    int st = load_mygraph(mygraph_path, metadata_path, g, &w);
+    if (st) return st;
+    memset(out, 0, sizeof *out);
+    out->max_vertex_id = g.max_id;
+    out->num_vertex_labels = g.num_labels();
+    out->num_partitions = (uint32_t)g.parts.size();
+    uint64_t bytes = 0;
+    for (auto& p : g.parts) {
+        out->num_adjacency += p.adj.size();
+        bytes += ((p.off.size() * 4 + 255) / 256 + (p.adj.size() * 4 + 4 + 255) / 256) * 256;
+    }
+    out->device_bytes = bytes + ((uint64_t)g.max_id * 4 + 4 + 255) / 256 * 256;
+    if (warn && cap) {
+        size_t n = std::min(cap - 1, w.size());
+        memcpy(warn, w.data(), n);
+        warn[n] = 0;
+    }
+    return GVA_OK;
+}
+
+const char* gva_db_warnings(const gva_db* db) { return db ? db->warnings.c_str() : ""; }
+
+void gva_db_free(gva_db* db) {
+    if (!db) return;
+    free_devdb(db->dev);
+    delete db;
+}
+
+int gva_plan_from_text(const char* query_text, int mode, gva_plan** out) {
+    if (!out || !query_text) return fail(GVA_ERR_ARG, "null argument");
+    *out = nullptr;
+    gva_plan* p = new gva_plan();
+    int st = plan_from_text(query_text, mode, p->plan);
+    if (st) {
+        delete p;
+        return st;
+    }
+    *out = p;
+    return GVA_OK;
+}
+
+int gva_plan_from_file(const char* query_path, int mode, gva_plan** out) {
+    if (!out || !query_path) return fail(GVA_ERR_ARG, "null argument");
+    std::string text;
+    int st = read_file(query_path, text);
+    if (st) return st;
+    return gva_plan_from_text(text.c_str(), mode, out);
+}
+
+size_t gva_plan_describe(const gva_plan* plan, char* buf, size_t cap) {
+    if (!plan) return 0;
+    std::string s = plan->plan.describe();
+    if (buf && cap) {
+        size_t n = s.size() < cap - 1 ? s.size() : cap - 1;
+        memcpy(buf, s.data(), n);
+        buf[n] = 0;
+    }
+    return s.size();
+}
+
+int gva_plan_num_phases(const gva_plan* plan) { return plan ? (int)plan->plan.phases.size() : -1; }
+int gva_plan_num_vertices(const gva_plan* plan) { return plan ? (int)plan->plan.vnum : -1; }
+
+int gva_plan_column_vertices(const gva_plan* plan, uint32_t* out, int cap) {
+    if (!plan) return -1;
+    const auto& c = plan->plan.columns;
+    for (int i = 0; i < (int)c.size() && i < cap; ++i) out[i] = c[i];
+    return (int)c.size();
+}
+
+void gva_plan_free(gva_plan* plan) { delete plan; }
+
+int gva_match(gva_db* db, const gva_plan* plan, const gva_match_opts* opts, gva_result** out) {
+    if (!db || !plan || !out) return fail(GVA_ERR_ARG, "null argument");
+    *out = nullptr;
+    std::vector<Step> steps;
+    int st = steps_for(plan, db, steps);
+    if (st) return st;
+    gva_match_opts o{};
+    if (opts) o = *opts;
+    gva_result* r = new gva_result();
+    st = run_match(*db->dev, plan->plan, steps, (cudaStream_t)o.stream, o.budget_bytes, o.count_only != 0, r->r);
+    if (st) {
+        delete r;
+        return st;
+    }
+    *out = r;
+    return GVA_OK;
+}
+
+uint64_t gva_result_num_rows(const gva_result* res) { return res ? res->r.rows : 0; }
+int gva_result_num_columns(const gva_result* res) { return res ? (int)res->r.width : -1; }
+
+int gva_result_phase_rows(const gva_result* res, uint64_t* out, int cap) {
+    if (!res) return -1;
+    const auto& v = res->r.phase_rows;
+    for (int i = 0; i < (int)v.size() && i < cap; ++i) out[i] = v[i];
+    return (int)v.size();
+}
+
+const uint32_t* gva_result_device_rows(const gva_result* res) { return res ? res->r.rows_dev : nullptr; }
+
+int gva_result_copy_rows(const gva_result* res, uint32_t* host_dst, uint64_t first_row, uint64_t num_rows) {
+    if (!res || (!host_dst && num_rows)) return fail(GVA_ERR_ARG, "null argument");
+    if (first_row + num_rows > res->r.rows) return fail(GVA_ERR_ARG, "row range out of bounds");
+    if (num_rows == 0) return GVA_OK;
+    if (!res->r.rows_dev) return fail(GVA_ERR_ARG, "result holds counts only");
+    cudaSetDevice(res->r.device);
+    const size_t w = res->r.width;
+    cudaError_t e = cudaMemcpyAsync(host_dst, res->r.rows_dev + first_row * w, num_rows * w * 4,
+                                    cudaMemcpyDeviceToHost, res->r.stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(res->r.stream);
+    if (e != cudaSuccess) return fail(GVA_ERR_CUDA, cudaGetErrorString(e));
+    return GVA_OK;
+}
+
+int gva_result_write_text(const gva_result* res, const char* path) {
+    if (!res || !path) return fail(GVA_ERR_ARG, "null argument");
+    FILE* f = fopen(path, "w");
+    if (!f) return fail(GVA_ERR_IO, std::string("cannot write ") + path);
+    const uint64_t chunk = 1 << 20;
+    const uint32_t w = res->r.width;
+    std::vector<uint32_t> buf;
+    std::string line;
+    for (uint64_t r0 = 0; r0 < res->r.rows; r0 += chunk) {
+        const uint64_t n = std::min<uint64_t>(chunk, res->r.rows - r0);
+        buf.resize(n * w);
+        int st = gva_result_copy_rows(res, buf.data(), r0, n);
+        if (st) {
+            fclose(f);
+            return st;
+        }
+        for (uint64_t i = 0; i < n; ++i) {
+            line.clear();
+            for (uint32_t c = 0; c < w; ++c) {
+                if (c) line.push_back(' ');
+                line += std::to_string(buf[i * w + c]);
+            }
+            line.push_back('\n');
+            fwrite(line.data(), 1, line.size(), f);
+        }
+    }
+    fclose(f);
+    return GVA_OK;
+}
+
+double gva_result_gpu_ms(const gva_result* res) { return res ? res->r.gpu_ms : 0.0; }
+
+void gva_result_free(gva_result* res) {
+    if (!res) return;
+    MatchResult* m = new MatchResult(std::move(res->r));
+    free_result(m);
+    delete res;
+}
+
+int gva_plan_num_steps(const gva_plan* plan, const gva_db* db) {
+    if (!plan || !db) return -1;
+    std::vector<Step> s;
+    if (steps_for(plan, db, s)) return -1;
+    return (int)s.size();
+}
+
+int gva_plan_step_width_in(const gva_plan* plan, const gva_db* db, int step) {
+    std::vector<Step> s;
+    if (!plan || !db || steps_for(plan, db, s) || step < 0 || step >= (int)s.size()) return -1;
+    return (int)s[step].width_in;
+}
+
+int gva_plan_step_width_out(const gva_plan* plan, const gva_db* db, int step) {
+    std::vector<Step> s;
+    if (!plan || !db || steps_for(plan, db, s) || step < 0 || step >= (int)s.size()) return -1;
+    const Step& t = s[step];
+    return t.kind == STEP_SEED ? 1 : (t.kind == STEP_EXT ? (int)t.width_in + 1 : (int)t.width_in);
+}
+
+size_t gva_step_scratch_bytes(uint64_t in_rows) { return step_scratch_bytes(in_rows); }
+
+int gva_step_run(gva_db* db, const gva_plan* plan, int step, const uint32_t* in_dev, uint64_t in_rows,
+                 uint32_t* out_dev, uint64_t out_capacity_rows, uint64_t* out_rows, void* scratch_dev,
+                 size_t scratch_bytes, void* stream) {
+    if (!db || !plan) return fail(GVA_ERR_ARG, "null argument");
+    std::vector<Step> s;
+    int st = steps_for(plan, db, s);
+    if (st) return st;
+    if (step < 0 || step >= (int)s.size()) return fail(GVA_ERR_ARG, "step index out of range");
+    return run_step(*db->dev, s[step], in_dev, in_rows, out_dev, out_capacity_rows, out_rows, scratch_dev,
+                    scratch_bytes, (cudaStream_t)stream);
+}
+
+}  // extern "C"

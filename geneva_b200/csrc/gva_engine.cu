@@ -1,0 +1,684 @@
+// CUDA engine for sm_100a: device database, phase kernels, phase executor.
+//
+// Frontiers are row-major uint32 tables (one column per matched query
+// vertex).  Every extension or reduction runs as
+//   count  (thread per row)            -> per-256-row block totals
+//   scan   (one block)                 -> exclusive block offsets + total
+//   write  (block per 256 rows)        -> rows staged in shared memory,
+//                                         outputs balanced across the block,
+//                                         flushed with coalesced stores
+// so the output size is known before it is written (no device-side overflow
+// protocol, unlike src/miningPattern.cu:3325-3343) and output order is
+// deterministic (input-row order, candidates ascending).
+//
+// Label segments come from a dense (vertex, label) offset table, one load per
+// lookup, replacing the warp bisection with vLabel gathers of the reference
+// (FIND_LABEL_LIMIT, include/common.h:18-66).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <string>
+
+#include "../../include/geneva.h"
+#include "gva_engine.cuh"
+
+namespace gva {
+
+namespace {
+
+constexpr int kRowsPerBlock = 256;  // rows handled by one count/write block
+constexpr int kThreads = 256;
+constexpr int kScanThreads = 1024;
+
+#define GVA_CUDA(call)                                                                                  \
+    do {                                                                                                \
+        cudaError_t e_ = (call);                                                                        \
+        if (e_ != cudaSuccess)                                                                          \
+            return fail(GVA_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_));              \
+    } while (0)
+
+inline size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+// ---------------------------------------------------------------- params ----
+struct ExtArgs {
+    const uint32_t* in;
+    uint64_t nrows;
+    uint32_t* out;
+    const uint32_t* off;
+    const uint32_t* adj;
+    uint32_t k;        // input width
+    uint32_t L;        // dense labels
+    uint32_t lab;      // dense candidate label
+    int32_t src_col;
+    int32_t bound_col;
+    uint32_t bound_incl;
+    uint32_t n_eq;
+    uint8_t eq_cols[kMaxCols];
+};
+
+struct RedArgs {
+    const uint32_t* in;
+    uint64_t nrows;
+    uint32_t* out;
+    const uint32_t* off;
+    const uint32_t* adj;
+    uint32_t k;
+    uint32_t L;
+    uint32_t n_pairs;
+    uint8_t rs[16];
+    uint8_t re[16];
+    uint32_t rl[16];
+};
+
+__device__ __forceinline__ uint64_t umin64(uint64_t a, uint64_t b) { return a < b ? a : b; }
+
+// first index in [lo, hi) with a[i] >= x (hi if none)
+__device__ __forceinline__ uint32_t lower_bound_u32(const uint32_t* __restrict__ a, uint32_t lo, uint32_t hi,
+                                                    uint64_t x) {
+    while (lo < hi) {
+        const uint32_t mid = lo + ((hi - lo) >> 1);
+        if ((uint64_t)__ldg(a + mid) < x)
+            lo = mid + 1;
+        else
+            hi = mid;
+    }
+    return lo;
+}
+
+// Candidate range of one row: the (source, label) segment cut below the
+// restriction bound.
+__device__ __forceinline__ void ext_range(const ExtArgs& p, const uint32_t* row, uint32_t& lo, uint32_t& hi) {
+    const uint32_t s = row[p.src_col];
+    const uint64_t t = (uint64_t)s * p.L + p.lab;
+    lo = __ldg(p.off + t);
+    hi = __ldg(p.off + t + 1);
+    if (p.bound_col >= 0 && lo < hi) {
+        const uint64_t b = (uint64_t)row[p.bound_col] + p.bound_incl;
+        hi = lower_bound_u32(p.adj, lo, hi, b);
+    }
+}
+
+// Position of w in adj[lo, hi), or 0xffffffff.
+__device__ __forceinline__ uint32_t find_in(const uint32_t* __restrict__ adj, uint32_t lo, uint32_t hi, uint32_t w) {
+    if (lo >= hi) return 0xffffffffu;
+    if (w < __ldg(adj + lo) || w > __ldg(adj + hi - 1)) return 0xffffffffu;
+    const uint32_t pos = lower_bound_u32(adj, lo, hi, w);
+    return (pos < hi && __ldg(adj + pos) == w) ? pos : 0xffffffffu;
+}
+
+// Number of candidates of one row (segment minus already-matched vertices).
+__device__ __forceinline__ uint32_t ext_count_row(const ExtArgs& p, const uint32_t* row) {
+    uint32_t lo, hi;
+    ext_range(p, row, lo, hi);
+    if (lo >= hi) return 0;
+    uint32_t n = hi - lo;
+    for (uint32_t j = 0; j < p.n_eq; ++j) {
+        const uint32_t w = row[p.eq_cols[j]];
+        bool dup = false;  // the same vertex in two columns collides once
+        for (uint32_t i = 0; i < j; ++i) dup |= (row[p.eq_cols[i]] == w);
+        if (!dup && find_in(p.adj, lo, hi, w) != 0xffffffffu) --n;
+    }
+    return n;
+}
+
+__device__ __forceinline__ bool red_keep_row(const RedArgs& p, const uint32_t* row) {
+    for (uint32_t j = 0; j < p.n_pairs; ++j) {
+        const uint32_t s = row[p.rs[j]];
+        const uint32_t e = row[p.re[j]];
+        const uint64_t t = (uint64_t)s * p.L + p.rl[j];
+        const uint32_t lo = __ldg(p.off + t), hi = __ldg(p.off + t + 1);
+        if (find_in(p.adj, lo, hi, e) == 0xffffffffu) return false;
+    }
+    return true;
+}
+
+// ------------------------------------------------------------ block sums ----
+template <typename T>
+__device__ __forceinline__ T warp_sum(T v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    return v;
+}
+
+__device__ __forceinline__ void store_block_sum(uint64_t v, uint64_t* block_sums) {
+    __shared__ uint64_t ws[kThreads / 32];
+    v = warp_sum(v);
+    if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = v;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        uint64_t x = threadIdx.x < kThreads / 32 ? ws[threadIdx.x] : 0;
+        x = warp_sum(x);
+        if (threadIdx.x == 0) block_sums[blockIdx.x] = x;
+    }
+}
+
+// Exclusive scan of 256 per-thread values in shared memory (uint64).
+__device__ __forceinline__ uint64_t block_exclusive_scan(uint64_t v, uint64_t* total) {
+    __shared__ uint64_t ws[kThreads / 32];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    uint64_t x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint64_t y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) ws[wid] = x;
+    __syncthreads();
+    if (wid == 0) {
+        uint64_t w = lane < kThreads / 32 ? ws[lane] : 0;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint64_t y = __shfl_up_sync(0xffffffffu, w, o);
+            if (lane >= o) w += y;
+        }
+        if (lane < kThreads / 32) ws[lane] = w;
+    }
+    __syncthreads();
+    const uint64_t before = (wid > 0 ? ws[wid - 1] : 0) + x - v;
+    *total = ws[kThreads / 32 - 1];
+    __syncthreads();
+    return before;
+}
+
+// ---------------------------------------------------------------- kernels ---
+__global__ void __launch_bounds__(kThreads) ext_count_kernel(ExtArgs p, uint64_t* __restrict__ block_sums) {
+    const uint64_t r = (uint64_t)blockIdx.x * kRowsPerBlock + threadIdx.x;
+    uint64_t c = 0;
+    if (r < p.nrows) c = ext_count_row(p, p.in + r * p.k);
+    store_block_sum(c, block_sums);
+}
+
+__global__ void __launch_bounds__(kThreads) red_count_kernel(RedArgs p, uint64_t* __restrict__ block_sums) {
+    const uint64_t r = (uint64_t)blockIdx.x * kRowsPerBlock + threadIdx.x;
+    uint64_t c = 0;
+    if (r < p.nrows) c = red_keep_row(p, p.in + r * p.k) ? 1 : 0;
+    store_block_sum(c, block_sums);
+}
+
+// In-place exclusive scan of n block totals; sums[n] receives the total.
+__global__ void __launch_bounds__(kScanThreads) scan_block_sums_kernel(uint64_t* __restrict__ sums, uint64_t n) {
+    __shared__ uint64_t ws[kScanThreads / 32];
+    __shared__ uint64_t carry_s;
+    if (threadIdx.x == 0) carry_s = 0;
+    __syncthreads();
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    for (uint64_t base = 0; base < n; base += kScanThreads) {
+        const uint64_t i = base + threadIdx.x;
+        const uint64_t v = i < n ? sums[i] : 0;
+        uint64_t x = v;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint64_t y = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o) x += y;
+        }
+        if (lane == 31) ws[wid] = x;
+        __syncthreads();
+        if (wid == 0) {
+            uint64_t w = ws[lane];
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint64_t y = __shfl_up_sync(0xffffffffu, w, o);
+                if (lane >= o) w += y;
+            }
+            ws[lane] = w;
+        }
+        __syncthreads();
+        const uint64_t carry = carry_s;
+        if (i < n) sums[i] = carry + (wid > 0 ? ws[wid - 1] : 0) + x - v;
+        __syncthreads();
+        if (threadIdx.x == 0) carry_s = carry + ws[kScanThreads / 32 - 1];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) sums[n] = carry_s;
+}
+
+// Block b expands rows [256b, 256b + 256): every thread produces one output
+// row per tile, so a block's work is balanced however the candidates are
+// spread over its rows.
+__global__ void __launch_bounds__(kThreads) ext_write_kernel(ExtArgs p, const uint64_t* __restrict__ block_off) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    uint64_t* offs_s = reinterpret_cast<uint64_t*>(smem_raw);           // 257
+    uint32_t* rows_s = reinterpret_cast<uint32_t*>(offs_s + kRowsPerBlock + 1);  // 256 * k
+    uint32_t* lo_s = rows_s + kRowsPerBlock * p.k;                        // 256
+    uint32_t* ncol_s = lo_s + kRowsPerBlock;                              // 256
+    uint32_t* coll_s = ncol_s + kRowsPerBlock;                            // 256 * n_eq
+    uint32_t* out_s = coll_s + kRowsPerBlock * p.n_eq;                    // 256 * (k + 1)
+
+    const uint64_t row0 = (uint64_t)blockIdx.x * kRowsPerBlock;
+    const uint32_t nr = (uint32_t)umin64((uint64_t)kRowsPerBlock, p.nrows - row0);
+    const uint32_t k = p.k, k1 = p.k + 1;
+
+    // coalesced load of this block's rows
+    const uint32_t* gin = p.in + row0 * k;
+    for (uint32_t w = threadIdx.x; w < nr * k; w += kThreads) rows_s[w] = gin[w];
+    __syncthreads();
+
+    uint64_t cnt = 0;
+    if (threadIdx.x < nr) {
+        const uint32_t* row = rows_s + threadIdx.x * k;
+        uint32_t lo, hi;
+        ext_range(p, row, lo, hi);
+        uint32_t nc = 0;
+        uint32_t* mine = coll_s + threadIdx.x * p.n_eq;
+        if (lo < hi) {
+            for (uint32_t j = 0; j < p.n_eq; ++j) {
+                const uint32_t pos = find_in(p.adj, lo, hi, row[p.eq_cols[j]]);
+                if (pos == 0xffffffffu) continue;
+                bool dup = false;
+                for (uint32_t i = 0; i < nc; ++i) dup |= (mine[i] == pos);
+                if (dup) continue;
+                uint32_t i = nc++;  // insertion sort, ascending
+                while (i > 0 && mine[i - 1] > pos) {
+                    mine[i] = mine[i - 1];
+                    --i;
+                }
+                mine[i] = pos;
+            }
+            cnt = hi - lo - nc;
+        }
+        lo_s[threadIdx.x] = lo;
+        ncol_s[threadIdx.x] = nc;
+    }
+    uint64_t total;
+    const uint64_t before = block_exclusive_scan(cnt, &total);
+    offs_s[threadIdx.x] = before;
+    if (threadIdx.x == 0) offs_s[nr] = total;
+    __syncthreads();
+
+    const uint64_t out0 = block_off[blockIdx.x];
+    for (uint64_t base = 0; base < total; base += kThreads) {
+        const uint64_t o = base + threadIdx.x;
+        if (o < total) {
+            // largest r with offs_s[r] <= o; rows with no candidate are skipped
+            int a = 0, b = (int)nr - 1;
+            while (a < b) {
+                const int m = (a + b + 1) >> 1;
+                if (offs_s[m] <= o)
+                    a = m;
+                else
+                    b = m - 1;
+            }
+            uint32_t j = lo_s[a] + (uint32_t)(o - offs_s[a]);
+            const uint32_t* mine = coll_s + a * p.n_eq;
+            for (uint32_t c = 0; c < ncol_s[a]; ++c) j += (mine[c] <= j) ? 1u : 0u;
+            uint32_t* dst = out_s + threadIdx.x * k1;
+            const uint32_t* src = rows_s + a * k;
+            for (uint32_t c = 0; c < k; ++c) dst[c] = src[c];
+            dst[k] = __ldg(p.adj + j);
+        }
+        __syncthreads();
+        const uint32_t n_tile = (uint32_t)umin64((uint64_t)kThreads, total - base);
+        uint32_t* gout = p.out + (out0 + base) * k1;
+        for (uint32_t w = threadIdx.x; w < n_tile * k1; w += kThreads) gout[w] = out_s[w];
+        __syncthreads();
+    }
+}
+
+__global__ void __launch_bounds__(kThreads) red_write_kernel(RedArgs p, const uint64_t* __restrict__ block_off) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    uint32_t* rows_s = reinterpret_cast<uint32_t*>(smem_raw);  // 256 * k (compacted in a second buffer)
+    uint32_t* out_s = rows_s + kRowsPerBlock * p.k;
+    const uint64_t row0 = (uint64_t)blockIdx.x * kRowsPerBlock;
+    const uint32_t nr = (uint32_t)umin64((uint64_t)kRowsPerBlock, p.nrows - row0);
+    const uint32_t k = p.k;
+    const uint32_t* gin = p.in + row0 * k;
+    for (uint32_t w = threadIdx.x; w < nr * k; w += kThreads) rows_s[w] = gin[w];
+    __syncthreads();
+    bool keep = false;
+    if (threadIdx.x < nr) keep = red_keep_row(p, rows_s + threadIdx.x * k);
+    uint64_t total;
+    const uint64_t before = block_exclusive_scan(keep ? 1 : 0, &total);
+    if (keep)
+        for (uint32_t c = 0; c < k; ++c) out_s[before * k + c] = rows_s[threadIdx.x * k + c];
+    __syncthreads();
+    uint32_t* gout = p.out + block_off[blockIdx.x] * k;
+    for (uint32_t w = threadIdx.x; w < (uint32_t)total * k; w += kThreads) gout[w] = out_s[w];
+}
+
+size_t ext_smem_bytes(uint32_t k, uint32_t n_eq) {
+    return sizeof(uint64_t) * (kRowsPerBlock + 1) +
+           sizeof(uint32_t) * ((size_t)kRowsPerBlock * k + 2 * kRowsPerBlock + (size_t)kRowsPerBlock * n_eq +
+                               (size_t)kRowsPerBlock * (k + 1));
+}
+size_t red_smem_bytes(uint32_t k) { return sizeof(uint32_t) * 2 * (size_t)kRowsPerBlock * k; }
+
+int set_smem_limits() {
+    static bool done[64] = {};
+    int dev = 0;
+    GVA_CUDA(cudaGetDevice(&dev));
+    if (dev < 64 && done[dev]) return GVA_OK;
+    GVA_CUDA(cudaFuncSetAttribute(ext_write_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)ext_smem_bytes(kMaxCols - 1, kMaxCols)));
+    GVA_CUDA(cudaFuncSetAttribute(red_write_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)red_smem_bytes(kMaxCols)));
+    if (dev < 64) done[dev] = true;
+    return GVA_OK;
+}
+
+void fill_ext(ExtArgs& a, const DevDB& db, const Step& st, const uint32_t* in, uint64_t nrows, uint32_t* out) {
+    memset(&a, 0, sizeof a);
+    const DevPart& P = db.parts[st.part - 1];
+    a.in = in;
+    a.nrows = nrows;
+    a.out = out;
+    a.off = P.off;
+    a.adj = P.adj;
+    a.k = st.width_in;
+    a.L = db.L;
+    a.lab = st.label;
+    a.src_col = st.src_col;
+    a.bound_col = st.bound_col;
+    a.bound_incl = st.bound_inclusive;
+    a.n_eq = st.n_eq;
+    for (uint32_t i = 0; i < st.n_eq; ++i) a.eq_cols[i] = st.eq_cols[i];
+}
+
+void fill_red(RedArgs& a, const DevDB& db, const Step& st, const uint32_t* in, uint64_t nrows, uint32_t* out) {
+    memset(&a, 0, sizeof a);
+    const DevPart& P = db.parts[st.part - 1];
+    a.in = in;
+    a.nrows = nrows;
+    a.out = out;
+    a.off = P.off;
+    a.adj = P.adj;
+    a.k = st.width_in;
+    a.L = db.L;
+    a.n_pairs = st.n_pairs;
+    for (uint32_t i = 0; i < st.n_pairs; ++i) {
+        a.rs[i] = st.rs_col[i];
+        a.re[i] = st.re_col[i];
+        a.rl[i] = st.re_label[i];
+    }
+}
+
+// count + scan; leaves exclusive block offsets in sums[0..nb) and the total in sums[nb]
+int launch_count(const DevDB& db, const Step& st, const uint32_t* in, uint64_t nrows, uint64_t* sums,
+                 cudaStream_t s) {
+    const uint64_t nb = (nrows + kRowsPerBlock - 1) / kRowsPerBlock;
+    if (nb > 0x7fffffffull) return fail(GVA_ERR_UNSUPPORTED, "frontier too large for one launch");
+    if (st.kind == STEP_EXT) {
+        ExtArgs a;
+        fill_ext(a, db, st, in, nrows, nullptr);
+        ext_count_kernel<<<(unsigned)nb, kThreads, 0, s>>>(a, sums);
+    } else {
+        RedArgs a;
+        fill_red(a, db, st, in, nrows, nullptr);
+        red_count_kernel<<<(unsigned)nb, kThreads, 0, s>>>(a, sums);
+    }
+    GVA_CUDA(cudaGetLastError());
+    scan_block_sums_kernel<<<1, kScanThreads, 0, s>>>(sums, nb);
+    GVA_CUDA(cudaGetLastError());
+    return GVA_OK;
+}
+
+int launch_write(const DevDB& db, const Step& st, const uint32_t* in, uint64_t nrows, uint32_t* out,
+                 const uint64_t* sums, cudaStream_t s) {
+    const uint64_t nb = (nrows + kRowsPerBlock - 1) / kRowsPerBlock;
+    int rc = set_smem_limits();
+    if (rc) return rc;
+    if (st.kind == STEP_EXT) {
+        ExtArgs a;
+        fill_ext(a, db, st, in, nrows, out);
+        ext_write_kernel<<<(unsigned)nb, kThreads, ext_smem_bytes(a.k, a.n_eq), s>>>(a, sums);
+    } else {
+        RedArgs a;
+        fill_red(a, db, st, in, nrows, out);
+        red_write_kernel<<<(unsigned)nb, kThreads, red_smem_bytes(a.k), s>>>(a, sums);
+    }
+    GVA_CUDA(cudaGetLastError());
+    return GVA_OK;
+}
+
+int ensure_pool(int device) {
+    static bool done[64] = {};
+    if (device < 64 && done[device]) return GVA_OK;
+    cudaMemPool_t pool;
+    GVA_CUDA(cudaDeviceGetDefaultMemPool(&pool, device));
+    uint64_t keep = UINT64_MAX;  // keep freed frontier memory cached for the next phase / query
+    GVA_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
+    if (device < 64) done[device] = true;
+    return GVA_OK;
+}
+
+}  // namespace
+
+// ------------------------------------------------------------- database ----
+int upload_graph(HostGraph& g, int device, DevDB*& out) {
+    out = nullptr;
+    int ndev = 0;
+    GVA_CUDA(cudaGetDeviceCount(&ndev));
+    if (device < 0 || device >= ndev) return fail(GVA_ERR_ARG, "device index out of range");
+    GVA_CUDA(cudaSetDevice(device));
+    const uint32_t L = g.num_labels();
+    // vertices grouped by dense label: the seed frontiers of init phases
+    std::vector<uint32_t> seed_off(L + 1, 0), seed_verts;
+    for (uint32_t v = 1; v <= g.max_id; ++v)
+        if (g.dlabel[v] != kNone) seed_off[g.dlabel[v] + 1]++;
+    for (uint32_t l = 0; l < L; ++l) seed_off[l + 1] += seed_off[l];
+    seed_verts.resize(seed_off[L]);
+    {
+        std::vector<uint32_t> fill(seed_off.begin(), seed_off.end() - 1);
+        for (uint32_t v = 1; v <= g.max_id; ++v)
+            if (g.dlabel[v] != kNone) seed_verts[fill[g.dlabel[v]]++] = v;
+    }
+    size_t bytes = align256(seed_verts.size() * 4 + 4);
+    for (auto& p : g.parts) bytes += align256(p.off.size() * 4) + align256(p.adj.size() * 4 + 4);
+    void* arena = nullptr;
+    cudaError_t e = cudaMalloc(&arena, bytes);
+    if (e != cudaSuccess) return fail(GVA_ERR_NOMEM, std::string("database allocation failed: ") + cudaGetErrorString(e));
+    DevDB* db = new DevDB();
+    db->device = device;
+    db->max_id = g.max_id;
+    db->L = L;
+    db->labels = g.labels;
+    db->seed_off = seed_off;
+    db->arena = arena;
+    db->arena_bytes = bytes;
+    char* cur = (char*)arena;
+    auto put = [&](const std::vector<uint32_t>& v) -> const uint32_t* {
+        const uint32_t* at = (const uint32_t*)cur;
+        if (!v.empty()) cudaMemcpy(cur, v.data(), v.size() * 4, cudaMemcpyHostToDevice);
+        cur += align256(v.size() * 4 + 4);
+        return at;
+    };
+    db->seed_verts = put(seed_verts);
+    db->parts.resize(g.parts.size());
+    for (size_t i = 0; i < g.parts.size(); ++i) {
+        HostPartition& hp = g.parts[i];
+        if (hp.off.empty()) continue;
+        const uint32_t* off = (const uint32_t*)cur;
+        cudaMemcpy(cur, hp.off.data(), hp.off.size() * 4, cudaMemcpyHostToDevice);
+        cur += align256(hp.off.size() * 4);
+        db->parts[i].off = off;
+        db->parts[i].adj = put(hp.adj);
+        db->parts[i].n_adj = hp.adj.size();
+        db->n_adj += hp.adj.size();
+    }
+    e = cudaDeviceSynchronize();
+    if (e != cudaSuccess) {
+        cudaFree(arena);
+        delete db;
+        return fail(GVA_ERR_CUDA, std::string("database upload failed: ") + cudaGetErrorString(e));
+    }
+    // keep label tables and partition presence for planning; drop host adjacency
+    db->meta.max_id = g.max_id;
+    db->meta.labels = g.labels;
+    db->meta.parts.resize(g.parts.size());
+    for (size_t i = 0; i < g.parts.size(); ++i)
+        if (!g.parts[i].off.empty()) db->meta.parts[i].off.assign(1, 0);
+    out = db;
+    return GVA_OK;
+}
+
+void free_devdb(DevDB* db) {
+    if (!db) return;
+    if (db->arena) {
+        cudaSetDevice(db->device);
+        cudaFree(db->arena);
+    }
+    delete db;
+}
+
+size_t step_scratch_bytes(uint64_t in_rows) {
+    const uint64_t nb = (in_rows + kRowsPerBlock - 1) / kRowsPerBlock;
+    return align256((nb + 1) * sizeof(uint64_t));
+}
+
+// ---------------------------------------------------------- one step (L4) --
+int run_step(DevDB& db, const Step& st, const uint32_t* in, uint64_t in_rows, uint32_t* out, uint64_t out_cap,
+             uint64_t* out_rows, void* scratch, size_t scratch_bytes, cudaStream_t s) {
+    if (!out_rows) return fail(GVA_ERR_ARG, "out_rows is null");
+    *out_rows = 0;
+    GVA_CUDA(cudaSetDevice(db.device));
+    if (st.always_empty) return GVA_OK;
+    if (st.kind == STEP_SEED) {
+        const uint64_t n = db.seed_off[st.label + 1] - db.seed_off[st.label];
+        *out_rows = n;
+        if (n > out_cap) return fail(GVA_ERR_NOMEM, "output capacity too small");
+        if (n) GVA_CUDA(cudaMemcpyAsync(out, db.seed_verts + db.seed_off[st.label], n * 4, cudaMemcpyDeviceToDevice, s));
+        return GVA_OK;
+    }
+    if (in_rows == 0) return GVA_OK;
+    if (!in || !scratch) return fail(GVA_ERR_ARG, "null device buffer");
+    if (scratch_bytes < step_scratch_bytes(in_rows)) return fail(GVA_ERR_ARG, "scratch too small");
+    uint64_t* sums = (uint64_t*)scratch;
+    int rc = launch_count(db, st, in, in_rows, sums, s);
+    if (rc) return rc;
+    const uint64_t nb = (in_rows + kRowsPerBlock - 1) / kRowsPerBlock;
+    uint64_t total = 0;
+    GVA_CUDA(cudaMemcpyAsync(&total, sums + nb, 8, cudaMemcpyDeviceToHost, s));
+    GVA_CUDA(cudaStreamSynchronize(s));
+    *out_rows = total;
+    if (total > out_cap) return fail(GVA_ERR_NOMEM, "output capacity too small");
+    if (total == 0) return GVA_OK;
+    if (!out) return fail(GVA_ERR_ARG, "null output buffer");
+    return launch_write(db, st, in, in_rows, out, sums, s);
+}
+
+// ------------------------------------------------------- whole query (L3) --
+int run_match(DevDB& db, const Plan& plan, const std::vector<Step>& steps, cudaStream_t s, uint64_t budget,
+              bool count_only, MatchResult& res) {
+    GVA_CUDA(cudaSetDevice(db.device));
+    int rc = ensure_pool(db.device);
+    if (rc) return rc;
+    res = MatchResult();
+    res.device = db.device;
+    res.stream = s;
+    res.columns = plan.columns;
+    res.phase_rows.assign(plan.phases.size(), 0);
+    if (budget == 0) {
+        size_t fr = 0, tot = 0;
+        GVA_CUDA(cudaMemGetInfo(&fr, &tot));
+        budget = (uint64_t)fr / 4 * 3;
+    }
+    cudaEvent_t ev0, ev1;
+    GVA_CUDA(cudaEventCreate(&ev0));
+    GVA_CUDA(cudaEventCreate(&ev1));
+    GVA_CUDA(cudaEventRecord(ev0, s));
+
+    const uint32_t* cur = nullptr;
+    uint32_t* owned = nullptr;  // frontier we must free
+    uint64_t rows = 0;
+    uint32_t width = 0;
+    uint64_t* sums = nullptr;
+    size_t sums_bytes = 0;
+    uint64_t* total_h = nullptr;
+    cudaError_t ce = cudaMallocHost(&total_h, sizeof(uint64_t));
+    if (ce != cudaSuccess) return fail(GVA_ERR_NOMEM, "pinned host allocation failed");
+    int status = GVA_OK;
+    bool counted_only = false;
+
+    for (size_t i = 0; i < steps.size(); ++i) {
+        const Step& st = steps[i];
+        const bool last = (i + 1 == steps.size());
+        const uint32_t out_w = st.kind == STEP_SEED ? 1 : (st.kind == STEP_EXT ? width + 1 : width);
+        if (st.always_empty) {
+            rows = 0;
+        } else if (st.kind == STEP_SEED) {
+            cur = db.seed_verts + db.seed_off[st.label];
+            rows = db.seed_off[st.label + 1] - db.seed_off[st.label];
+        } else if (rows > 0) {
+            const size_t need = step_scratch_bytes(rows);
+            if (need > sums_bytes) {
+                if (sums) cudaFreeAsync(sums, s);
+                ce = cudaMallocAsync((void**)&sums, need, s);
+                if (ce != cudaSuccess) { status = fail(GVA_ERR_NOMEM, "scratch allocation failed"); sums = nullptr; break; }
+                sums_bytes = need;
+            }
+            status = launch_count(db, st, cur, rows, sums, s);
+            if (status) break;
+            const uint64_t nb = (rows + kRowsPerBlock - 1) / kRowsPerBlock;
+            ce = cudaMemcpyAsync(total_h, sums + nb, 8, cudaMemcpyDeviceToHost, s);
+            if (ce == cudaSuccess) ce = cudaStreamSynchronize(s);
+            if (ce != cudaSuccess) { status = fail(GVA_ERR_CUDA, cudaGetErrorString(ce)); break; }
+            const uint64_t total = *total_h;
+            if (last && count_only) {
+                rows = total;
+                counted_only = true;
+            } else if (total == 0) {
+                rows = 0;
+            } else {
+                const uint64_t bytes = total * out_w * 4ull;
+                if (bytes > budget) {
+                    status = fail(GVA_ERR_NOMEM, "frontier of " + std::to_string(total) + " rows exceeds the memory budget");
+                    break;
+                }
+                uint32_t* out = nullptr;
+                ce = cudaMallocAsync((void**)&out, bytes, s);
+                if (ce != cudaSuccess) { status = fail(GVA_ERR_NOMEM, "frontier allocation failed"); break; }
+                status = launch_write(db, st, cur, rows, out, sums, s);
+                if (status) { cudaFreeAsync(out, s); break; }
+                if (owned) cudaFreeAsync(owned, s);
+                owned = out;
+                cur = out;
+                rows = total;
+            }
+        }
+        width = out_w;
+        if (st.phase_end >= 0) res.phase_rows[st.phase_end] = rows;
+        if (rows == 0) break;
+    }
+    if (sums) cudaFreeAsync(sums, s);
+    cudaFreeHost(total_h);
+    if (status) {
+        if (owned) cudaFreeAsync(owned, s);
+        cudaEventDestroy(ev0);
+        cudaEventDestroy(ev1);
+        return status;
+    }
+    GVA_CUDA(cudaEventRecord(ev1, s));
+    GVA_CUDA(cudaEventSynchronize(ev1));
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, ev0, ev1);
+    cudaEventDestroy(ev0);
+    cudaEventDestroy(ev1);
+    res.gpu_ms = ms;
+    // the final width is the number of columns of the plan
+    res.width = (uint32_t)plan.columns.size();
+    res.rows = rows;
+    if (rows == 0 || counted_only) {
+        if (owned) cudaFreeAsync(owned, s);
+        res.rows_dev = nullptr;
+    } else if (owned) {
+        res.rows_dev = owned;
+    } else {
+        // the final frontier is still the seed list (cannot happen: a plan ends with an extension or reduction)
+        res.rows_dev = nullptr;
+    }
+    GVA_CUDA(cudaStreamSynchronize(s));
+    return GVA_OK;
+}
+
+void free_result(MatchResult* r) {
+    if (!r) return;
+    if (r->rows_dev) {
+        cudaSetDevice(r->device);
+        cudaFreeAsync(r->rows_dev, r->stream);
+        cudaStreamSynchronize(r->stream);
+    }
+    delete r;
+}
+
+}  // namespace gva

@@ -1,0 +1,325 @@
+// Host side of the database: .mygraph/.metadata parsing, edge-list builder,
+// and the lowering of a plan to engine steps.
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <fstream>
+#include <map>
+#include <sstream>
+
+#include "../../include/geneva.h"
+#include "gva_internal.h"
+
+namespace gva {
+
+static thread_local std::string g_err = "no error";
+
+void set_error(int status, const std::string& msg) {
+    (void)status;
+    g_err = msg;
+}
+int fail(int status, const std::string& msg) {
+    set_error(status, msg);
+    return status;
+}
+const char* last_error_cstr() { return g_err.c_str(); }
+
+uint32_t HostGraph::dense_label(uint32_t orig) const {
+    auto it = std::lower_bound(labels.begin(), labels.end(), orig);
+    if (it == labels.end() || *it != orig) return kNone;
+    return (uint32_t)(it - labels.begin());
+}
+
+namespace {
+
+// Per-partition adjacency in (vertex, label, id) order -> dense offset table.
+// lists[v] holds the already-sorted neighbours of v; their dense labels are
+// non-decreasing.
+int build_partition(HostGraph& g, uint32_t edge_label, const std::vector<std::vector<uint32_t>>& lists) {
+    const uint64_t L = g.num_labels();
+    const uint64_t entries = (uint64_t)(g.max_id + 1) * L + 1;
+    if (entries >= 0xffffffffull) return fail(GVA_ERR_UNSUPPORTED, "vertex count x label count exceeds 2^32");
+    HostPartition p;
+    p.edge_label = edge_label;
+    uint64_t total = 0;
+    for (auto& l : lists) total += l.size();
+    if (total >= 0xffffffffull) return fail(GVA_ERR_UNSUPPORTED, "partition has 2^32 or more adjacency entries");
+    p.off.resize(entries);
+    p.adj.reserve(total);
+    for (uint32_t v = 0; v <= g.max_id; ++v) {
+        const std::vector<uint32_t>* lst = v < lists.size() ? &lists[v] : nullptr;
+        size_t j = 0;
+        for (uint32_t l = 0; l < L; ++l) {
+            p.off[(uint64_t)v * L + l] = (uint32_t)p.adj.size();
+            if (!lst) continue;
+            while (j < lst->size() && g.dlabel[(*lst)[j]] == l) p.adj.push_back((*lst)[j++]);
+        }
+        if (lst && j != lst->size()) return fail(GVA_ERR_FORMAT, "neighbour list is not grouped by vertex label");
+    }
+    p.off[entries - 1] = (uint32_t)p.adj.size();
+    if (g.parts.size() < edge_label) g.parts.resize(edge_label);
+    g.parts[edge_label - 1] = std::move(p);
+    return GVA_OK;
+}
+
+void finish_labels(HostGraph& g) {
+    std::vector<uint32_t> ls;
+    for (uint32_t v = 1; v <= g.max_id; ++v)
+        if (g.vlabel[v] != kNone) ls.push_back(g.vlabel[v]);
+    std::sort(ls.begin(), ls.end());
+    ls.erase(std::unique(ls.begin(), ls.end()), ls.end());
+    g.labels = ls;
+    g.dlabel.assign(g.max_id + 1, kNone);
+    for (uint32_t v = 1; v <= g.max_id; ++v) g.dlabel[v] = g.dense_label(g.vlabel[v]);
+}
+
+// Number of index vertices genDatabase prepends to a label group of raw
+// length n (tools/genDatabase.cpp:415-436, decoded as src/loadDataBase.cpp:71-98).
+uint32_t index_prefix(uint32_t n) {
+    if (n <= 128) return 0;
+    if (n <= 32 * 128 + 32) return (n + 128) / 129;
+    return 32;
+}
+
+}  // namespace
+
+int load_mygraph(const std::string& mygraph, const std::string& metadata, HostGraph& g, std::string* warnings) {
+    // ---- .metadata: "newid label oldid" (src/loadDataBase.cpp:320-340) ----
+    std::ifstream mf(metadata);
+    if (!mf.is_open()) return fail(GVA_ERR_IO, "cannot open metadata file " + metadata);
+    std::vector<std::pair<uint32_t, uint32_t>> vl;
+    uint32_t nid, lab, oid, maxid = 0;
+    while (mf >> nid >> lab >> oid) {
+        vl.push_back({nid, lab});
+        maxid = std::max(maxid, nid);
+    }
+    if (vl.empty()) return fail(GVA_ERR_FORMAT, "metadata file has no vertices");
+    g = HostGraph();
+    g.max_id = maxid;
+    g.vlabel.assign(maxid + 1, kNone);
+    for (auto& p : vl)
+        if (p.first != 0 && g.vlabel[p.first] == kNone) g.vlabel[p.first] = p.second;  // first wins
+    finish_labels(g);
+
+    // ---- .mygraph: uint32 P, then P partitions (tools/genDatabase.cpp:856-869) ----
+    std::ifstream gf(mygraph, std::ios::binary);
+    if (!gf.is_open()) return fail(GVA_ERR_IO, "cannot open graph file " + mygraph);
+    uint32_t P = 0;
+    if (!gf.read((char*)&P, 4)) return fail(GVA_ERR_FORMAT, "graph file is empty");
+    std::vector<uint32_t> part;
+    for (uint32_t key = 1; key <= P; ++key) {
+        uint32_t tot = 0;
+        if (!gf.read((char*)&tot, 4)) {
+            // The shipped Enron.mygraph declares 4 partitions and holds 3.
+            if (warnings) *warnings += "graph header declares " + std::to_string(P) + " partitions, file holds " +
+                                       std::to_string(key - 1) + "\n";
+            break;
+        }
+        if (tot < 5) return fail(GVA_ERR_FORMAT, "partition shorter than its header");
+        part.assign(tot, 0);
+        part[0] = tot;
+        if (!gf.read((char*)&part[1], (std::streamsize)(tot - 1) * 4)) return fail(GVA_ERR_FORMAT, "truncated partition");
+        // header: [1] source slots, [2] intervals, [3]/[4] hash/neighbour offsets from word 5
+        const uint64_t nslot = part[1], nint = part[2];
+        const uint64_t slots_at = 5 + 2 * nint + 2, nbr_at = 5 + (uint64_t)part[4];
+        if (part[3] != part[4]) return fail(GVA_ERR_UNSUPPORTED, "hash-indexed partitions are not supported");
+        if (slots_at + nslot + 1 > tot || nbr_at > tot || 5 + 2 * nint + 1 > tot)
+            return fail(GVA_ERR_FORMAT, "partition offsets out of range");
+        const uint64_t nnbr = tot - nbr_at;
+        const uint32_t* start = &part[5];
+        const uint32_t* cum = &part[5 + nint + 1];
+        const uint32_t* soff = &part[slots_at];
+        const uint32_t* nbr = &part[nbr_at];
+        if (soff[nslot] > nnbr) return fail(GVA_ERR_FORMAT, "neighbour offsets beyond partition");
+        if (soff[nslot] < nnbr && warnings)
+            *warnings += "partition " + std::to_string(key) +
+                         " holds neighbours of sources beyond its 256 intervals (dropped, as the reference)\n";
+        std::vector<std::vector<uint32_t>> lists(maxid + 1);
+        uint32_t prev = 0;
+        for (uint64_t i = 0; i < nint; ++i) {
+            if (cum[i] < prev || cum[i] > nslot) return fail(GVA_ERR_FORMAT, "interval lengths not cumulative");
+            for (uint32_t s = prev; s < cum[i]; ++s) {
+                const uint64_t v = (uint64_t)start[i] + (s - prev);
+                if (v == 0 || v > maxid) return fail(GVA_ERR_FORMAT, "source vertex id outside metadata");
+                uint32_t b = soff[s], e = soff[s + 1];
+                if (b > e || e > nnbr) return fail(GVA_ERR_FORMAT, "bad neighbour range");
+                std::vector<uint32_t>& out = lists[v];
+                // split into vertex-label groups, dropping each group's index prefix
+                uint32_t j = b;
+                while (j < e) {
+                    const uint32_t u0 = nbr[j];
+                    if (u0 == 0 || u0 > maxid || g.vlabel[u0] == kNone)
+                        return fail(GVA_ERR_FORMAT, "neighbour id outside metadata");
+                    uint32_t k = j;
+                    while (k < e && nbr[k] != 0 && nbr[k] <= maxid && g.vlabel[nbr[k]] == g.vlabel[u0]) ++k;
+                    const uint32_t skip = index_prefix(k - j);
+                    for (uint32_t t = j + skip; t < k; ++t) {
+                        if (!out.empty() && g.dlabel[out.back()] == g.dlabel[nbr[t]] && out.back() >= nbr[t])
+                            return fail(GVA_ERR_FORMAT, "neighbour group not strictly ascending");
+                        out.push_back(nbr[t]);
+                    }
+                    j = k;
+                }
+            }
+            prev = cum[i];
+        }
+        int st = build_partition(g, key, lists);
+        if (st) return st;
+    }
+    if (g.parts.empty()) return fail(GVA_ERR_FORMAT, "graph file holds no partition");
+    return GVA_OK;
+}
+
+int graph_from_edges(const uint32_t* vlabels, uint32_t max_id, const uint32_t* src, const uint32_t* dst,
+                     const uint32_t* elabel, uint64_t ne, HostGraph& g) {
+    if (!vlabels || (ne && (!src || !dst || !elabel))) return fail(GVA_ERR_ARG, "null array");
+    if (max_id == 0) return fail(GVA_ERR_ARG, "max_vertex_id must be >= 1");
+    g = HostGraph();
+    g.max_id = max_id;
+    g.vlabel.assign(vlabels, vlabels + max_id + 1);
+    g.vlabel[0] = kNone;
+    finish_labels(g);
+    uint32_t P = 0;
+    for (uint64_t i = 0; i < ne; ++i) {
+        if (elabel[i] == 0) return fail(GVA_ERR_ARG, "edge labels must be >= 1");
+        if (src[i] == 0 || dst[i] == 0 || src[i] > max_id || dst[i] > max_id)
+            return fail(GVA_ERR_ARG, "edge endpoint outside 1..max_vertex_id");
+        P = std::max(P, elabel[i]);
+    }
+    // bucket by label, then by source: (src, dst) both directions
+    std::vector<uint64_t> cnt((uint64_t)P * (max_id + 1) + 1, 0);
+    for (uint64_t i = 0; i < ne; ++i) {
+        cnt[(uint64_t)(elabel[i] - 1) * (max_id + 1) + src[i]]++;
+        cnt[(uint64_t)(elabel[i] - 1) * (max_id + 1) + dst[i]]++;
+    }
+    for (uint32_t p = 1; p <= P; ++p) {
+        std::vector<std::vector<uint32_t>> lists(max_id + 1);
+        for (uint32_t v = 0; v <= max_id; ++v) lists[v].reserve(cnt[(uint64_t)(p - 1) * (max_id + 1) + v]);
+        for (uint64_t i = 0; i < ne; ++i) {
+            if (elabel[i] != p) continue;
+            lists[src[i]].push_back(dst[i]);
+            lists[dst[i]].push_back(src[i]);
+        }
+        for (auto& l : lists) {
+            std::sort(l.begin(), l.end(), [&](uint32_t a, uint32_t b) {
+                if (g.dlabel[a] != g.dlabel[b]) return g.dlabel[a] < g.dlabel[b];
+                return a < b;
+            });
+            l.erase(std::unique(l.begin(), l.end()), l.end());
+            for (uint32_t u : l)
+                if (g.dlabel[u] == kNone) return fail(GVA_ERR_ARG, "edge endpoint without a vertex label");
+        }
+        int st = build_partition(g, p, lists);
+        if (st) return st;
+    }
+    if (g.parts.empty()) g.parts.resize(1);
+    return GVA_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Plan -> steps.  Column c of a row holds plan.columns[c].
+//   init, one pair (s,e)      : seed(label s) + ext(s->e, e < s iff restricted to s)
+//                               (cpumine genInit 2V, src/cpumine.cpp:60-119: no injectivity test)
+//   init, two pairs (s,e1,e2) : seed + ext(s->e1, e1 <= s) + ext(s->e2, e2 < e1 or e2 <= s,
+//                               e2 != e1) (src/cpumine.cpp:120-194)
+//   E, one pair               : ext(s->e, injective against same-label columns, e < row[restrict])
+//   E, two pairs              : two such exts; the second also avoids the first
+//                               (src/cpumine.cpp:298-435)
+//   R                         : reduce over all pairs (src/cpumine.cpp:486-584); more than
+//                               16 pairs empties the frontier as the reference does (:499-502)
+int lower_plan(const Plan& plan, const HostGraph& g, std::vector<Step>& steps) {
+    steps.clear();
+    const uint32_t P = (uint32_t)g.parts.size();
+    std::vector<int> col(plan.vnum, -1);
+    int width = 0;
+    auto part_of = [&](uint32_t el) -> uint32_t { return (el >= 1 && el <= P && !g.parts[el - 1].off.empty()) ? el : 0; };
+    auto ext = [&](uint32_t el, uint32_t s, uint32_t e, int bound_col, bool incl, const std::vector<int>& eq) {
+        Step st;
+        st.kind = STEP_EXT;
+        st.width_in = (uint32_t)width;
+        st.part = part_of(el);
+        st.label = g.dense_label(plan.qlabel[e]);
+        st.src_col = col[s];
+        st.bound_col = bound_col;
+        st.bound_inclusive = incl ? 1 : 0;
+        st.n_eq = (uint32_t)eq.size();
+        for (size_t i = 0; i < eq.size(); ++i) st.eq_cols[i] = (uint8_t)eq[i];
+        st.always_empty = (st.part == 0 || st.label == kNone) ? 1 : 0;
+        steps.push_back(st);
+        col[e] = width++;
+    };
+    auto same_label_cols = [&](uint32_t e) {
+        std::vector<int> eq;
+        for (uint32_t v = 0; v < plan.vnum; ++v)
+            if (col[v] >= 0 && plan.qlabel[v] == plan.qlabel[e]) eq.push_back(col[v]);
+        std::sort(eq.begin(), eq.end());
+        return eq;
+    };
+    for (size_t pi = 0; pi < plan.phases.size(); ++pi) {
+        const Phase& ph = plan.phases[pi];
+        const size_t np = ph.pairs.size() / 2;
+        if (pi == 0) {
+            if (ph.type != 'E' || np < 1 || np > 2) return fail(GVA_ERR_FORMAT, "first phase must extend 1 or 2 vertices");
+            const uint32_t s = ph.pairs[0];
+            Step seed;
+            seed.kind = STEP_SEED;
+            seed.width_in = 0;
+            seed.part = part_of(ph.edge_label);
+            seed.label = g.dense_label(plan.qlabel[s]);
+            seed.always_empty = (seed.part == 0 || seed.label == kNone) ? 1 : 0;
+            steps.push_back(seed);
+            col[s] = width++;
+            if (np == 1 || plan.mode == GVA_MODE_SV) {
+                const uint32_t e = ph.pairs[1];
+                ext(ph.edge_label, s, e, plan.restricts[e] == s ? 0 : -1, false, {});
+            } else {
+                const uint32_t e1 = ph.pairs[1], e2 = ph.pairs[3];
+                ext(ph.edge_label, s, e1, plan.restricts[e1] != kNone ? 0 : -1, true, {});
+                std::vector<int> eq;
+                if (plan.qlabel[e2] == plan.qlabel[e1]) eq.push_back(col[e1]);
+                if (plan.restricts[e2] == e1)
+                    ext(ph.edge_label, s, e2, col[e1], false, eq);
+                else
+                    ext(ph.edge_label, s, e2, plan.restricts[e2] != kNone ? 0 : -1, true, eq);
+            }
+            steps.back().phase_end = 0;
+            continue;
+        }
+        if (ph.type == 'E') {
+            for (size_t i = 0; i < np; ++i) {
+                const uint32_t s = ph.pairs[2 * i], e = ph.pairs[2 * i + 1];
+                if (col[s] < 0) return fail(GVA_ERR_FORMAT, "extension from an unmatched vertex");
+                int bc = -1;
+                if (plan.restricts[e] != kNone) {
+                    bc = col[plan.restricts[e]];
+                    if (bc < 0) return fail(GVA_ERR_FORMAT, "restriction names an unmatched vertex");
+                }
+                ext(ph.edge_label, s, e, bc, false, same_label_cols(e));
+            }
+        } else {
+            Step st;
+            st.kind = STEP_REDUCE;
+            st.width_in = (uint32_t)width;
+            st.part = part_of(ph.edge_label);
+            if (np > GVA_MAX_REDUCE_PAIRS) {
+                st.always_empty = 1;
+            } else {
+                st.n_pairs = (uint32_t)np;
+                for (size_t i = 0; i < np; ++i) {
+                    const uint32_t a = ph.pairs[2 * i], b = ph.pairs[2 * i + 1];
+                    if (col[a] < 0 || col[b] < 0) return fail(GVA_ERR_FORMAT, "reduction over an unmatched vertex");
+                    st.rs_col[i] = (uint8_t)col[a];
+                    st.re_col[i] = (uint8_t)col[b];
+                    st.re_label[i] = g.dense_label(plan.qlabel[b]);
+                    if (st.re_label[i] == kNone) st.always_empty = 1;
+                }
+                if (st.part == 0) st.always_empty = 1;
+            }
+            steps.push_back(st);
+        }
+        steps.back().phase_end = (int)pi;
+    }
+    return GVA_OK;
+}
+
+}  // namespace gva

@@ -1,0 +1,93 @@
+// Internal types shared by the host library and the CUDA engine.
+#pragma once
+
+#include <cstdint>
+#include <map>
+#include <string>
+#include <vector>
+
+namespace gva {
+
+constexpr uint32_t kNone = 0xffffffffu;
+constexpr int kMaxCols = 32;
+
+// ---------------------------------------------------------------- errors ----
+void set_error(int status, const std::string& msg);  // thread-local message
+int fail(int status, const std::string& msg);         // set_error + return status
+
+// ----------------------------------------------------------------- graph ----
+// Host copy of one database: per edge label a CSR whose per-vertex lists are
+// sorted by (dense vertex label, vertex id), plus a dense (vertex, label) ->
+// offset table.  seg(v, l) = adj[off[v*L + l] .. off[v*L + l + 1]).
+struct HostPartition {
+    uint32_t edge_label = 0;       // 1..P
+    std::vector<uint32_t> off;     // (max_id + 1) * L + 1 entries
+    std::vector<uint32_t> adj;     // neighbour ids
+};
+
+struct HostGraph {
+    uint32_t max_id = 0;                 // vertex ids are 1..max_id
+    std::vector<uint32_t> vlabel;        // original label per id (max_id + 1)
+    std::vector<uint32_t> labels;        // sorted distinct original labels
+    std::vector<uint32_t> dlabel;        // dense label per id (max_id + 1)
+    std::vector<HostPartition> parts;    // parts[p - 1] is edge label p
+    uint32_t num_labels() const { return (uint32_t)labels.size(); }
+    // dense index of an original label, kNone when absent from the data
+    uint32_t dense_label(uint32_t orig) const;
+};
+
+// Parses .metadata + .mygraph (src/loadDataBase.cpp:309-365 layout).
+int load_mygraph(const std::string& mygraph, const std::string& metadata, HostGraph& g,
+                 std::string* warnings);
+// Builds from an edge list (tools/genDatabase.cpp:600-667 semantics, no renumbering).
+int graph_from_edges(const uint32_t* vlabels, uint32_t max_id, const uint32_t* src, const uint32_t* dst,
+                     const uint32_t* elabel, uint64_t ne, HostGraph& g);
+
+// ----------------------------------------------------------------- plan -----
+struct Phase {
+    char type = 'E';                  // 'E' extension, 'R' reduction
+    uint32_t edge_label = 0;
+    std::vector<uint32_t> pairs;      // (svid, evid) pairs, flattened
+};
+
+struct Plan {
+    int mode = 0;                                  // GVA_MODE_DV / GVA_MODE_SV
+    uint32_t vnum = 0;
+    std::vector<uint32_t> qlabel;                  // query vertex -> label
+    std::vector<Phase> phases;
+    std::vector<uint32_t> restricts;               // vnum + 1 entries (kNone = none)
+    std::map<uint64_t, uint32_t> repeat_flag;      // (edge label << 32 | vlabel) -> flag
+    std::map<uint32_t, std::vector<uint32_t>> record_stat;  // edge label -> vlabels
+    std::vector<uint32_t> columns;                 // query vertex of each output column
+    std::string describe() const;
+};
+
+int plan_from_text(const std::string& text, int mode, Plan& out);
+
+// ---------------------------------------------------------------- steps -----
+// A plan lowered to engine steps.  Every reference phase becomes one or more
+// steps; the row set after the last step of a phase equals the reference's
+// rows after that phase.
+enum StepKind : uint32_t { STEP_SEED = 0, STEP_EXT = 1, STEP_REDUCE = 2 };
+
+struct Step {
+    StepKind kind = STEP_EXT;
+    uint32_t width_in = 0;         // columns read
+    uint32_t part = 0;             // edge label partition (1-based), 0 = absent
+    uint32_t label = kNone;        // dense candidate label (SEED: source label)
+    int32_t src_col = -1;          // EXT: column of the source vertex
+    int32_t bound_col = -1;        // EXT: candidate < row[bound_col] (or <=)
+    uint32_t bound_inclusive = 0;
+    uint32_t n_eq = 0;             // EXT: injectivity columns
+    uint8_t eq_cols[kMaxCols] = {};
+    // REDUCE: pairs of (svid column, evid column, dense label of evid)
+    uint32_t n_pairs = 0;
+    uint8_t rs_col[16] = {}, re_col[16] = {};
+    uint32_t re_label[16] = {};
+    uint32_t always_empty = 0;     // reference limit reached (>16 pairs) or label absent
+    int phase_end = -1;            // reference phase index completed by this step, else -1
+};
+
+int lower_plan(const Plan& plan, const HostGraph& g, std::vector<Step>& steps);
+
+}  // namespace gva

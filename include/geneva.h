@@ -1,0 +1,155 @@
+/*
+ * geneva.h — C ABI of the B200-native Geneva subgraph-matching path.
+ *
+ * The reference drives its GPU path from C++ with no stable boundary: a CLI
+ * (`gpumine`, `gpumineSV`), a loader returning std::map<uint, uint*>, a planner
+ * filling std::vector<Phase>, and void kernel launchers that read their row
+ * counts back through a device word.  This header replaces that surface with
+ * plain pointers, sizes and int status codes.  Every entry point names the
+ * reference interface it replaces (paths relative to the reference project).
+ *
+ * Conventions
+ *   - Data vertex ids are 1-based uint32 (0 is never a vertex), query vertex
+ *     ids are 0-based, as in the reference (src/gpumine.cpp:1-3).
+ *   - A frontier ("partial embedding" table) is row-major uint32 with one
+ *     column per matched query vertex, columns in match order — the order the
+ *     reference prints them (src/gpumine.cpp:184-199).
+ *   - Row counts are uint64 (the reference uses uint32, src/gpumine.cpp:904).
+ *   - Functions return GVA_OK (0) or a positive GVA_ERR_* code; the message of
+ *     the last failure on the calling thread is gva_last_error().  Nothing in
+ *     the library calls exit() (the reference does, src/loadDataBase.cpp:311-319).
+ *   - `stream` arguments are cudaStream_t passed as void* (NULL = the legacy
+ *     default stream).  Device pointers are CUDA device addresses.
+ */
+#ifndef GENEVA_H
+#define GENEVA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define GVA_OK 0
+#define GVA_ERR_IO 1          /* file missing or unreadable                 */
+#define GVA_ERR_FORMAT 2      /* malformed .mygraph/.metadata/.query/.g     */
+#define GVA_ERR_CUDA 3        /* a CUDA runtime call failed                  */
+#define GVA_ERR_NOMEM 4       /* device or host allocation failed / budget  */
+#define GVA_ERR_ARG 5         /* bad argument (null, out of range, size)    */
+#define GVA_ERR_UNSUPPORTED 6 /* outside the reference's limits (see docs)  */
+
+#define GVA_MODE_DV 0 /* genMatchOrder        (src/genMatchOrder.cpp:672)       */
+#define GVA_MODE_SV 1 /* genMatchOrderSingleV (src/genMatchOrderSingleV.cpp:678) */
+
+#define GVA_MAX_QUERY_VERTICES 32 /* bitmask planner limit, src/gpumine.cpp:123-124 */
+#define GVA_MAX_REDUCE_PAIRS 16   /* src/reduction.cu auxArray, src/gpumine.cpp:759-762 */
+
+typedef struct gva_db gva_db;         /* device-resident database            */
+typedef struct gva_plan gva_plan;     /* match order + restrictions          */
+typedef struct gva_result gva_result; /* final frontier + per-phase counts   */
+
+typedef struct gva_db_info {
+    uint32_t max_vertex_id;   /* vLabel[0] in the reference                  */
+    uint32_t num_vertex_labels;
+    uint32_t num_partitions;  /* edge labels 1..num_partitions               */
+    uint32_t reserved;
+    uint64_t num_adjacency;   /* directed adjacency entries, all partitions  */
+    uint64_t device_bytes;    /* HBM held by the database                    */
+} gva_db_info;
+
+typedef struct gva_match_opts {
+    void* stream;          /* cudaStream_t; NULL = legacy default stream             */
+    uint64_t budget_bytes; /* frontier memory cap (0 = 3/4 of free HBM at call time)  */
+    int count_only;        /* 1: the last phase only counts (no final rows kept)      */
+    int reserved;
+} gva_match_opts;
+
+/* ---- status -------------------------------------------------------------- */
+const char* gva_last_error(void);
+const char* gva_status_string(int status);
+const char* gva_version(void);
+
+/* ---- L1: database ---------------------------------------------------------
+ * Replaces loadDataBase(mygraph, metadata) (src/loadDataBase.cpp:309-365,
+ * include/loadDataBase.h:1) plus the per-phase partition upload of
+ * src/gpumine.cpp:885-911,999-1006.  All edge-label partitions are uploaded
+ * once, as label-sorted CSR with a (vertex, label) -> segment offset table, so
+ * kernels never search labels.  Index vertices (tools/genDatabase.cpp:415-436)
+ * are stripped.  Partitions are keyed 1..P in file order, as the reference. */
+int gva_db_load(const char* mygraph_path, const char* metadata_path, int device, gva_db** out);
+
+/* Builds the same database from an in-memory labelled edge list with the
+ * semantics of tools/genDatabase.cpp:600-667 (undirected, duplicate edges
+ * dropped) but without renumbering: vertex v keeps id v.  vertex_labels has
+ * max_vertex_id + 1 entries (entry 0 ignored); edge labels are 1..P. */
+int gva_db_from_edges(const uint32_t* vertex_labels, uint32_t max_vertex_id, const uint32_t* src,
+                      const uint32_t* dst, const uint32_t* edge_labels, uint64_t num_edges, int device,
+                      gva_db** out);
+int gva_db_get_info(const gva_db* db, gva_db_info* out);
+/* Host-only parse of .mygraph + .metadata (no device needed): fills the
+ * counts of gva_db_info (device_bytes = bytes an upload would take) and
+ * copies loader notes into warn (may be NULL). */
+int gva_graph_probe(const char* mygraph_path, const char* metadata_path, gva_db_info* out, char* warn, size_t cap);
+/* Loader notes (e.g. a header that declares more partitions than the file
+ * holds, or neighbours dropped past 256 intervals); "" when none. */
+const char* gva_db_warnings(const gva_db* db);
+void gva_db_free(gva_db* db);
+
+/* ---- L2: planner ----------------------------------------------------------
+ * Replaces genMatchOrder / genMatchOrderSingleV (src/genMatchOrderCPU.cpp:670-983,
+ * src/genMatchOrderSingleV.cpp:678-1003): same phases, pair orientation,
+ * restrictions and repeat flags for the same query text.  Host-only. */
+int gva_plan_from_file(const char* query_path, int mode, gva_plan** out);
+int gva_plan_from_text(const char* query_text, int mode, gva_plan** out);
+/* Canonical text: "vnum", "phase", "restrict", "repeat", "stat" lines.
+ * Returns the needed length (excluding NUL); writes at most cap bytes. */
+size_t gva_plan_describe(const gva_plan* plan, char* buf, size_t cap);
+int gva_plan_num_phases(const gva_plan* plan);
+int gva_plan_num_vertices(const gva_plan* plan);
+/* query vertex id of each output column (match order, src/gpumine.cpp:158) */
+int gva_plan_column_vertices(const gva_plan* plan, uint32_t* out, int cap);
+void gva_plan_free(gva_plan* plan);
+
+/* ---- L3: one query end to end -----------------------------------------------
+ * Replaces the phase loop of gpumine / gpumineSV main (src/gpumine.cpp:932-1061):
+ * init, every E and R phase, frontier growth handled by chunking against
+ * budget_bytes instead of host spill.  The result stays on the device. */
+int gva_match(gva_db* db, const gva_plan* plan, const gva_match_opts* opts, gva_result** out);
+uint64_t gva_result_num_rows(const gva_result* res);
+int gva_result_num_columns(const gva_result* res);
+/* rows after each reference phase (index 0 = init) */
+int gva_result_phase_rows(const gva_result* res, uint64_t* out, int cap);
+/* device pointer to the row-major final rows (NULL when count_only) */
+const uint32_t* gva_result_device_rows(const gva_result* res);
+int gva_result_copy_rows(const gva_result* res, uint32_t* host_dst, uint64_t first_row, uint64_t num_rows);
+/* partialResultsGPU.txt format (src/gpumine.cpp:184-199) */
+int gva_result_write_text(const gva_result* res, const char* path);
+/* GPU time of the phase loop, from CUDA events on opts->stream */
+double gva_result_gpu_ms(const gva_result* res);
+void gva_result_free(gva_result* res);
+
+/* ---- L4: one phase step on caller-owned device buffers ----------------------
+ * Replaces the kernel launchers of include/miningPattern.h:1-30
+ * (initEmb_*, extEmb_1V_NoHash, extEmb_2V_*) and include/reduction.h:1-3
+ * (reductionPhase).  A plan is lowered to steps (gva_plan_num_steps); a step
+ * is an init seed, a one-vertex extension or a back-edge reduction.  The
+ * step reads `in_rows` rows of width gva_plan_step_width_in() and writes at
+ * most `out_capacity_rows` rows of width gva_plan_step_width_out().
+ * Scratch: gva_step_scratch_bytes(in_rows) bytes of device memory, 256-byte
+ * aligned.  *out_rows receives the produced row count; when it exceeds
+ * out_capacity_rows nothing is written and GVA_ERR_NOMEM is returned (the
+ * count is still valid, so the caller can grow and retry).  For a seed step
+ * in_rows/in_dev are ignored. Synchronises the stream once (count read-back). */
+int gva_plan_num_steps(const gva_plan* plan, const gva_db* db);
+int gva_plan_step_width_in(const gva_plan* plan, const gva_db* db, int step);
+int gva_plan_step_width_out(const gva_plan* plan, const gva_db* db, int step);
+size_t gva_step_scratch_bytes(uint64_t in_rows);
+int gva_step_run(gva_db* db, const gva_plan* plan, int step, const uint32_t* in_dev, uint64_t in_rows,
+                 uint32_t* out_dev, uint64_t out_capacity_rows, uint64_t* out_rows, void* scratch_dev,
+                 size_t scratch_bytes, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* GENEVA_H */

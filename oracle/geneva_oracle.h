@@ -1,0 +1,46 @@
+/*
+ * Test infrastructure only — the CPU oracle of the matching path.  Only
+ * tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg may load it;
+ * the product never links it.
+ *
+ * A plain restatement of the reference CPU matcher `cpumine`
+ * (src/cpumine.cpp:54-584) and of its planner (src/genMatchOrderCPU.cpp:69-983),
+ * held in memory instead of temp files, over the adjacency the reference GPU
+ * driver sees (.mygraph lists without genDatabase's index vertices).  Pinned
+ * against the reference itself: tests/golden holds rows/plans produced by the
+ * reference binaries compiled from source (oracle/Makefile `ref`).
+ */
+#ifndef GENEVA_ORACLE_H
+#define GENEVA_ORACLE_H
+#include <stddef.h>
+#include <stdint.h>
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct oracle_graph oracle_graph;
+
+/* .mygraph + .metadata (src/loadDataBase.cpp:309-365) */
+int oracle_graph_load(const char* mygraph, const char* metadata, oracle_graph** out);
+/* edge list, ids kept (tools/genDatabase.cpp:600-667 without renumbering) */
+int oracle_graph_from_edges(const uint32_t* vlabels, uint32_t max_id, const uint32_t* src, const uint32_t* dst,
+                            const uint32_t* elabel, uint64_t ne, oracle_graph** out);
+void oracle_graph_free(oracle_graph* g);
+
+/* Canonical plan text (same lines as gva_plan_describe). Returns length. */
+size_t oracle_plan(const char* query_text, char* buf, size_t cap);
+
+/* Runs every phase.  *rows is malloc'd (free with oracle_free), row-major,
+ * *width columns in match order.  phase_rows receives up to cap counts.
+ * Returns 0 on success. */
+int oracle_match(const oracle_graph* g, const char* query_text, uint32_t** rows, uint64_t* nrows, int* width,
+                 uint64_t* phase_rows, int cap, int* nphases);
+/* Counts only (no rows kept after the last phase). */
+int oracle_count(const oracle_graph* g, const char* query_text, uint64_t* nrows);
+void oracle_free(void* p);
+const char* oracle_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

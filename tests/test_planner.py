@@ -1,0 +1,71 @@
+"""Product planner (gva_plan_*, host-only) against the reference planner's
+plans (src/genMatchOrderCPU.cpp) and the oracle's restatement."""
+import random
+
+import pytest
+
+import geneva_b200 as gv
+from querygen import random_query
+
+
+def test_planner_matches_reference_plans(native, golden_plans):
+    bad = []
+    for g in golden_plans:
+        p = gv.Plan.from_text(g["q"], gv.MODE_DV)
+        if p.describe() != g["plan"]:
+            bad.append(g["q"])
+    assert not bad, f"{len(bad)} of {len(golden_plans)} plans differ; first:\n{bad[0]}"
+
+
+def test_planner_matches_oracle_on_fresh_queries(native, oracle):
+    rng = random.Random(99)
+    for _ in range(400):
+        q = random_query(rng)
+        assert gv.Plan.from_text(q).describe() == oracle.plan(q), q
+
+
+def _phases(desc):
+    out = []
+    for line in desc.splitlines():
+        t = line.split()
+        if t[0] == "phase":
+            out.append((t[2], int(t[3]), [int(x) for x in t[5:]]))
+    return out
+
+
+def test_single_vertex_mode_splits_phases(native, golden_plans):
+    for g in golden_plans[:300]:
+        dv = _phases(gv.Plan.from_text(g["q"], gv.MODE_DV).describe())
+        sv = _phases(gv.Plan.from_text(g["q"], gv.MODE_SV).describe())
+        split = []
+        for typ, el, pairs in dv:
+            for i in range(0, len(pairs), 2):
+                split.append((typ, el, pairs[i:i + 2]))
+        assert sv == split
+        assert gv.Plan.from_text(g["q"], gv.MODE_SV).columns == gv.Plan.from_text(g["q"]).columns
+
+
+def test_columns_follow_match_order(native):
+    p = gv.genMatchOrder("v 0 2\nv 1 1\nv 2 3\nv 3 1\ne 0 1 3\ne 0 2 1\ne 1 3 2\ne 1 2 2\n")
+    assert p.columns == [0, 1, 2, 3]
+    assert p.num_phases == 4
+
+
+@pytest.mark.parametrize("text,status", [
+    ("", gv.MODE_DV),
+    ("v 0 1\n", 2),
+    ("v 0 1\nv 1 1\nv 2 1\ne 0 1 1\n", 6),            # disconnected
+    ("v 0 1\nv 1 1\ne 0 0 1\ne 0 1 1\n", 6),          # self-loop
+    ("v 0 1\nv 2 1\ne 0 2 1\n", 2),                   # ids not 0..n-1
+    ("".join(f"v {i} 1\n" for i in range(33)) + "".join(f"e {i} {i+1} 1\n" for i in range(32)), 6),
+])
+def test_planner_errors(native, text, status):
+    with pytest.raises(gv.GenevaError) as ei:
+        gv.Plan.from_text(text)
+    assert ei.value.status in (2, 6)
+
+
+def test_bad_mode_rejected(native):
+    with pytest.raises(gv.GenevaError) as ei:
+        gv.Plan.from_text("v 0 1\nv 1 1\ne 0 1 1\n", 7)
+    assert ei.value.status == 5
