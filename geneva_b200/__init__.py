@@ -23,7 +23,7 @@ from typing import List, Optional, Sequence
 import numpy as np
 
 __all__ = [
-    "GenevaError", "Database", "probe_graph", "Plan", "Result", "MODE_DV", "MODE_SV", "library", "library_path",
+    "GenevaError", "Database", "probe_graph", "batch_count", "kernel_launches", "Plan", "Result", "MODE_DV", "MODE_SV", "library", "library_path",
     "loadDataBase", "genMatchOrder", "genMatchOrderSingleV", "match", "gpumine", "gpumineSV",
 ]
 
@@ -52,7 +52,22 @@ class _DbInfo(ctypes.Structure):
 
 class _MatchOpts(ctypes.Structure):
     _fields_ = [("stream", ctypes.c_void_p), ("budget_bytes", ctypes.c_uint64),
-                ("count_only", ctypes.c_int), ("reserved", ctypes.c_int)]
+                ("count_only", ctypes.c_int), ("profile", ctypes.c_int)]
+
+
+class _KernelStat(ctypes.Structure):
+    _fields_ = [("name", ctypes.c_char * 24), ("launches", ctypes.c_uint64), ("ms", ctypes.c_double),
+                ("bytes", ctypes.c_double)]
+
+
+class _BatchOpts(ctypes.Structure):
+    _fields_ = [("stream", ctypes.c_void_p), ("budget_bytes", ctypes.c_uint64), ("profile", ctypes.c_int),
+                ("reserved", ctypes.c_int)]
+
+
+class _BatchStats(ctypes.Structure):
+    _fields_ = [("gpu_ms", ctypes.c_double), ("rounds", ctypes.c_uint64), ("splits", ctypes.c_uint64),
+                ("launches", ctypes.c_uint64), ("kernels", _KernelStat * 5)]
 
 
 def _declare(lib):
@@ -63,6 +78,8 @@ def _declare(lib):
         "gva_last_error": (cp, []),
         "gva_status_string": (cp, [i32]),
         "gva_version": (cp, []),
+        "gva_kernel_launches": (u64, []),
+        "gva_result_kernel_stats": (i32, [vp, P(_KernelStat), i32]),
         "gva_db_load": (i32, [cp, cp, i32, P(vp)]),
         "gva_db_from_edges": (i32, [vp, u32, vp, vp, vp, u64, i32, P(vp)]),
         "gva_db_get_info": (i32, [vp, P(_DbInfo)]),
@@ -90,6 +107,8 @@ def _declare(lib):
         "gva_plan_step_width_out": (i32, [vp, vp, i32]),
         "gva_step_scratch_bytes": (sz, [u64]),
         "gva_step_run": (i32, [vp, vp, i32, vp, u64, vp, u64, P(u64), vp, sz, vp]),
+        "gva_db_set_graphs": (i32, [vp, vp, u32]),
+        "gva_batch_count": (i32, [vp, vp, i32, P(_BatchOpts), vp, vp, vp, P(_BatchStats)]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)
@@ -120,6 +139,7 @@ class Database:
 
     def __init__(self, handle):
         self._h = ctypes.c_void_p(handle)
+        self.num_graphs = 0
 
     @classmethod
     def load(cls, mygraph: str, metadata: str, device: int = 0) -> "Database":
@@ -146,6 +166,12 @@ class Database:
     @property
     def warnings(self) -> str:
         return library().gva_db_warnings(self._h).decode()
+
+    def set_graphs(self, first) -> None:
+        """Declare graph g as vertex ids [first[g], first[g+1]) (gva_db_set_graphs)."""
+        f = np.ascontiguousarray(first, dtype=np.uint64)
+        _check(library().gva_db_set_graphs(self._h, f.ctypes.data, len(f) - 1))
+        self.num_graphs = len(f) - 1
 
     def close(self):
         if self._h:
@@ -240,6 +266,13 @@ class Result:
     def gpu_ms(self) -> float:
         return float(library().gva_result_gpu_ms(self._h))
 
+    def kernel_stats(self) -> dict:
+        """Per-kernel {launches, ms, bytes} of a profiled match."""
+        arr = (_KernelStat * 16)()
+        n = library().gva_result_kernel_stats(self._h, arr, 16)
+        return {arr[i].name.decode(): dict(launches=int(arr[i].launches), ms=float(arr[i].ms),
+                                            bytes=float(arr[i].bytes)) for i in range(n)}
+
     @property
     def device_ptr(self) -> Optional[int]:
         return library().gva_result_device_rows(self._h)
@@ -268,13 +301,45 @@ class Result:
             pass
 
 
+def kernel_launches() -> int:
+    """Kernels launched by the native library in this process."""
+    return int(library().gva_kernel_launches())
+
+
 def match(db: Database, plan: Plan, stream: Optional[int] = None, budget_bytes: int = 0,
-          count_only: bool = False) -> Result:
+          count_only: bool = False, profile: bool = False) -> Result:
     """Runs every phase of `plan` on `db` (gva_match)."""
-    o = _MatchOpts(stream or None, budget_bytes, 1 if count_only else 0, 0)
+    o = _MatchOpts(stream or None, budget_bytes, 1 if count_only else 0, 1 if profile else 0)
     h = ctypes.c_void_p()
     _check(library().gva_match(db._h, plan._h, ctypes.byref(o), ctypes.byref(h)))
     return Result(h.value)
+
+
+def batch_count(db: Database, plans: Sequence[Plan], stream: Optional[int] = None, budget_bytes: int = 0,
+                graph_counts: bool = False, support: bool = False, profile: bool = False):
+    """Counts embeddings of many plans in shared rounds (gva_batch_count).
+
+    Returns (counts[n] uint64, per_graph, stats) where per_graph is the
+    [n, num_graphs] uint64 count matrix when graph_counts, else the [n]
+    uint32 supporting-graph counts when support, else None."""
+    n = len(plans)
+    arr = (ctypes.c_void_p * max(n, 1))(*[p._h.value for p in plans])
+    counts = np.zeros(n, dtype=np.uint64)
+    gc = np.zeros((n, db.num_graphs), dtype=np.uint64) if graph_counts else None
+    sup = np.zeros(n, dtype=np.uint32) if support else None
+    o = _BatchOpts(stream or None, budget_bytes, 1 if profile else 0, 0)
+    st = _BatchStats()
+    _check(library().gva_batch_count(db._h, arr, n, ctypes.byref(o), counts.ctypes.data,
+                                     gc.ctypes.data if gc is not None else None,
+                                     sup.ctypes.data if sup is not None else None, ctypes.byref(st)))
+    stats = {"gpu_ms": st.gpu_ms, "rounds": int(st.rounds), "splits": int(st.splits), "launches": int(st.launches),
+             "kernels": {st.kernels[i].name.decode(): dict(launches=int(st.kernels[i].launches),
+                                                           ms=float(st.kernels[i].ms), bytes=float(st.kernels[i].bytes))
+                         for i in range(5)}}
+    per_graph = gc if graph_counts else sup
+    if graph_counts and support:
+        per_graph = (gc, sup)
+    return counts, per_graph, stats
 
 
 # ---- reference-named entry points -------------------------------------------

@@ -1,0 +1,648 @@
+// Batched engine: many query patterns advance together.
+//
+// A task is (query, slice of that query's frontier, next step).  One round
+// advances every active task by one step:
+//   count   one launch over the 256-row blocks of all tasks (per-task step
+//           parameters from a descriptor array); final steps in count mode
+//           also add their rows into per-(query, graph) counters and graph
+//           bitmaps here and never write rows
+//   scan    exclusive scan of all block totals
+//   totals  per-task output rows
+//   write   persistent kernel: blocks pull 256-row items from an atomic work
+//           queue (load balance across SMs however uneven the tasks are) and
+//           expand / compact them into the round's output buffer
+// A task whose output does not fit the memory budget is split in half (its
+// input rows) and retried next round, so any frontier is processed in
+// budget-sized pieces, deepest tasks first.  This replaces the reference's
+// kernel-abort/host-spill protocol (src/gpumine.cpp:406-467,
+// src/miningPattern.cu:3325-3343) and its one-query-per-process driver.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <atomic>
+#include <cstring>
+#include <memory>
+#include <numeric>
+#include <string>
+#include <vector>
+
+#include "../../include/geneva.h"
+#include "gva_engine.cuh"
+#include "gva_kernels.cuh"
+
+namespace gva {
+
+namespace {
+
+#define GVA_CUDA_B(call)                                                                                \
+    do {                                                                                                \
+        cudaError_t e_ = (call);                                                                        \
+        if (e_ != cudaSuccess)                                                                          \
+            return fail(GVA_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_));              \
+    } while (0)
+
+enum TaskMode : uint32_t { MODE_WRITE = 0, MODE_COUNT = 1, MODE_COUNT_GRAPHS = 2 };
+
+struct TaskDesc {
+    uint32_t kind;     // STEP_EXT / STEP_REDUCE
+    uint32_t mode;     // TaskMode
+    uint32_t query;    // index into the batch
+    uint32_t pad;
+    uint64_t block0;   // first global block of this task
+    union {
+        ExtArgs e;
+        RedArgs r;
+    };
+};
+
+struct BatchCtx {
+    uint64_t* graph_counts;   // [nq * G] or null
+    uint32_t* graph_bits;     // [nq * words] or null
+    const uint32_t* vgraph;   // vertex -> graph
+    uint32_t G;
+    uint32_t words;           // bitmap words per query
+};
+
+__device__ __forceinline__ int find_task(const uint64_t* __restrict__ block0, int ntasks, uint64_t b) {
+    int lo = 0, hi = ntasks - 1;  // largest t with block0[t] <= b
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (__ldg(block0 + mid) <= b)
+            lo = mid;
+        else
+            hi = mid - 1;
+    }
+    return lo;
+}
+
+__device__ __forceinline__ void load_desc(TaskDesc& dst, const TaskDesc* src) {
+    const uint32_t* s = reinterpret_cast<const uint32_t*>(src);
+    uint32_t* d = reinterpret_cast<uint32_t*>(&dst);
+    for (int i = threadIdx.x; i < (int)(sizeof(TaskDesc) / 4); i += blockDim.x) d[i] = s[i];
+}
+
+// Per-(query, graph) accounting of a final-step row: lanes of a warp whose
+// rows lie in the same graph (rows arrive grouped by their first vertex)
+// combine their counts before one 64-bit atomic.
+__device__ __forceinline__ void add_graph_count(const BatchCtx& c, uint32_t query, uint32_t first_vertex, uint32_t cnt,
+                                                bool valid) {
+    uint32_t g = 0xffffffffu;
+    if (valid && cnt > 0) g = __ldg(c.vgraph + first_vertex);
+    const bool take = g < c.G;  // vertices outside every declared graph are not counted
+    const uint32_t active = __ballot_sync(0xffffffffu, take);
+    if (!take) return;
+    const uint32_t peers = __match_any_sync(active, g);
+    const uint32_t sum = __reduce_add_sync(peers, cnt);
+    if ((threadIdx.x & 31) == (uint32_t)(__ffs(peers) - 1)) {
+        if (c.graph_counts) atomicAdd((unsigned long long*)(c.graph_counts + (uint64_t)query * c.G + g), (unsigned long long)sum);
+        if (c.graph_bits) atomicOr(c.graph_bits + (uint64_t)query * c.words + (g >> 5), 1u << (g & 31));
+    }
+}
+
+__global__ void __launch_bounds__(kThreads)
+batch_count_kernel(const TaskDesc* __restrict__ tasks, const uint64_t* __restrict__ block0, int ntasks,
+                   uint64_t* __restrict__ block_sums, BatchCtx ctx) {
+    __shared__ TaskDesc d;
+    const uint64_t b = blockIdx.x;
+    const int t = find_task(block0, ntasks, b);
+    load_desc(d, tasks + t);
+    __syncthreads();
+    const uint64_t r = (b - d.block0) * kRowsPerBlock + threadIdx.x;
+    uint32_t c = 0;
+    uint32_t first = 0;
+    bool valid = false;
+    if (d.kind == STEP_EXT) {
+        valid = r < d.e.nrows;
+        if (valid) {
+            const uint32_t* row = d.e.in + r * d.e.k;
+            c = ext_count_row(d.e, row);
+            first = row[0];
+        }
+    } else {
+        valid = r < d.r.nrows;
+        if (valid) {
+            const uint32_t* row = d.r.in + r * d.r.k;
+            c = red_keep_row(d.r, row) ? 1u : 0u;
+            first = row[0];
+        }
+    }
+    if (d.mode == MODE_COUNT_GRAPHS) add_graph_count(ctx, d.query, first, c, valid);
+    store_block_sum(c, block_sums);
+}
+
+__global__ void task_totals_kernel(const uint64_t* __restrict__ block0, int ntasks, const uint64_t* __restrict__ sums,
+                                   uint64_t* __restrict__ totals) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < ntasks) totals[t] = sums[block0[t + 1]] - sums[block0[t]];
+}
+
+// Persistent: each CTA repeatedly takes the next 256-row item.
+__global__ void __launch_bounds__(kThreads)
+batch_write_kernel(const TaskDesc* __restrict__ tasks, const uint64_t* __restrict__ block0, int ntasks, uint64_t nblocks,
+                   const uint64_t* __restrict__ sums, uint32_t* __restrict__ const* __restrict__ task_out,
+                   unsigned long long* __restrict__ queue) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ TaskDesc d;
+    __shared__ unsigned long long item_s;
+    __shared__ uint64_t base_s;
+    for (;;) {
+        if (threadIdx.x == 0) item_s = atomicAdd(queue, 1ull);
+        __syncthreads();
+        const uint64_t b = item_s;
+        if (b >= nblocks) return;
+        const int t = find_task(block0, ntasks, b);
+        uint32_t* out = task_out[t];
+        if (out == nullptr) {  // task deferred or counted only: nothing to write
+            __syncthreads();
+            continue;
+        }
+        load_desc(d, tasks + t);
+        if (threadIdx.x == 0) base_s = sums[b] - sums[block0[t]];  // task-local output row of this item
+        __syncthreads();
+        const uint64_t row0 = (b - d.block0) * kRowsPerBlock;
+        const uint64_t out0 = base_s;
+        if (d.kind == STEP_EXT) {
+            const ExtArgs& p = d.e;
+            const uint32_t k = p.k, k1 = p.k + 1;
+            uint64_t* offs_s = reinterpret_cast<uint64_t*>(smem_raw);
+            uint32_t* rows_s = reinterpret_cast<uint32_t*>(offs_s + kRowsPerBlock + 1);
+            uint32_t* lo_s = rows_s + kRowsPerBlock * k;
+            uint32_t* ncol_s = lo_s + kRowsPerBlock;
+            uint32_t* coll_s = ncol_s + kRowsPerBlock;
+            uint32_t* out_s = coll_s + kRowsPerBlock * p.n_eq;
+            const uint32_t nr = (uint32_t)umin64((uint64_t)kRowsPerBlock, p.nrows - row0);
+            const uint32_t* gin = p.in + row0 * k;
+            for (uint32_t w = threadIdx.x; w < nr * k; w += kThreads) rows_s[w] = gin[w];
+            __syncthreads();
+            uint64_t cnt = 0;
+            if (threadIdx.x < nr) {
+                const uint32_t* row = rows_s + threadIdx.x * k;
+                uint32_t lo, hi;
+                ext_range(p, row, lo, hi);
+                uint32_t nc = 0;
+                uint32_t* mine = coll_s + threadIdx.x * p.n_eq;
+                if (lo < hi) {
+                    for (uint32_t j = 0; j < p.n_eq; ++j) {
+                        const uint32_t pos = find_in(p.adj, lo, hi, row[p.eq_cols[j]]);
+                        if (pos == 0xffffffffu) continue;
+                        bool dup = false;
+                        for (uint32_t i = 0; i < nc; ++i) dup |= (mine[i] == pos);
+                        if (dup) continue;
+                        uint32_t i = nc++;
+                        while (i > 0 && mine[i - 1] > pos) {
+                            mine[i] = mine[i - 1];
+                            --i;
+                        }
+                        mine[i] = pos;
+                    }
+                    cnt = hi - lo - nc;
+                }
+                lo_s[threadIdx.x] = lo;
+                ncol_s[threadIdx.x] = nc;
+            }
+            uint64_t total;
+            const uint64_t before = block_exclusive_scan(cnt, &total);
+            offs_s[threadIdx.x] = before;
+            if (threadIdx.x == 0) offs_s[nr] = total;
+            __syncthreads();
+            for (uint64_t base = 0; base < total; base += kThreads) {
+                const uint64_t o = base + threadIdx.x;
+                if (o < total) {
+                    int a = 0, z = (int)nr - 1;
+                    while (a < z) {
+                        const int m = (a + z + 1) >> 1;
+                        if (offs_s[m] <= o)
+                            a = m;
+                        else
+                            z = m - 1;
+                    }
+                    uint32_t j = lo_s[a] + (uint32_t)(o - offs_s[a]);
+                    const uint32_t* mine = coll_s + a * p.n_eq;
+                    for (uint32_t c = 0; c < ncol_s[a]; ++c) j += (mine[c] <= j) ? 1u : 0u;
+                    uint32_t* dst = out_s + threadIdx.x * k1;
+                    const uint32_t* src = rows_s + a * k;
+                    for (uint32_t c = 0; c < k; ++c) dst[c] = src[c];
+                    dst[k] = __ldg(p.adj + j);
+                }
+                __syncthreads();
+                const uint32_t n_tile = (uint32_t)umin64((uint64_t)kThreads, total - base);
+                uint32_t* gout = out + (out0 + base) * k1;
+                for (uint32_t w = threadIdx.x; w < n_tile * k1; w += kThreads) gout[w] = out_s[w];
+                __syncthreads();
+            }
+        } else {
+            const RedArgs& p = d.r;
+            const uint32_t k = p.k;
+            uint32_t* rows_s = reinterpret_cast<uint32_t*>(smem_raw);
+            uint32_t* out_s = rows_s + kRowsPerBlock * k;
+            const uint32_t nr = (uint32_t)umin64((uint64_t)kRowsPerBlock, p.nrows - row0);
+            const uint32_t* gin = p.in + row0 * k;
+            for (uint32_t w = threadIdx.x; w < nr * k; w += kThreads) rows_s[w] = gin[w];
+            __syncthreads();
+            bool keep = false;
+            if (threadIdx.x < nr) keep = red_keep_row(p, rows_s + threadIdx.x * k);
+            uint64_t total;
+            const uint64_t before = block_exclusive_scan(keep ? 1 : 0, &total);
+            if (keep)
+                for (uint32_t c = 0; c < k; ++c) out_s[before * k + c] = rows_s[threadIdx.x * k + c];
+            __syncthreads();
+            uint32_t* gout = out + out0 * k;
+            for (uint32_t w = threadIdx.x; w < (uint32_t)total * k; w += kThreads) gout[w] = out_s[w];
+            __syncthreads();
+        }
+    }
+}
+
+size_t batch_smem_bytes() {
+    // the larger of the extension layout at k = 31, n_eq = 32 and the reduction layout at k = 32
+    const size_t ext = sizeof(uint64_t) * (kRowsPerBlock + 1) +
+                       sizeof(uint32_t) * ((size_t)kRowsPerBlock * 31 + 2 * kRowsPerBlock + (size_t)kRowsPerBlock * 32 +
+                                           (size_t)kRowsPerBlock * 32);
+    const size_t red = sizeof(uint32_t) * 2 * (size_t)kRowsPerBlock * 32;
+    return std::max(ext, red);
+}
+
+size_t batch_smem_bytes_for(uint32_t kmax, uint32_t eqmax) {
+    const size_t ext = sizeof(uint64_t) * (kRowsPerBlock + 1) +
+                       sizeof(uint32_t) * ((size_t)kRowsPerBlock * kmax + 2 * kRowsPerBlock +
+                                           (size_t)kRowsPerBlock * eqmax + (size_t)kRowsPerBlock * (kmax + 1));
+    const size_t red = sizeof(uint32_t) * 2 * (size_t)kRowsPerBlock * (kmax + 1);
+    return std::max(ext, red);
+}
+
+std::atomic<uint64_t> g_batch_launches{0};
+
+// Device buffer shared by every task whose frontier slice lives in it.
+struct DevBuf {
+    void* p = nullptr;
+    cudaStream_t s = nullptr;
+    ~DevBuf() {
+        if (p) cudaFreeAsync(p, s);
+    }
+};
+
+struct Task {
+    int q;                       // query index
+    int step;                    // next step to run
+    const uint32_t* in;          // frontier slice
+    uint64_t rows;
+    std::shared_ptr<DevBuf> owner;
+};
+
+}  // namespace
+
+uint64_t batch_kernel_launches() { return g_batch_launches.load(); }
+
+struct BatchRun {
+    DevDB& db;
+    const std::vector<std::vector<Step>>& steps;
+    cudaStream_t s;
+    uint64_t budget;
+    BatchCtx ctx{};
+    Profiler* prof;
+    BatchStats* stats;
+};
+
+int run_batch(DevDB& db, const std::vector<std::vector<Step>>& steps, cudaStream_t s, uint64_t budget,
+              const uint32_t* vgraph, uint32_t G, uint64_t* counts, uint64_t* graph_counts_host,
+              uint32_t* support_host, bool profile, BatchStats* stats) {
+    GVA_CUDA_B(cudaSetDevice(db.device));
+    const int nq = (int)steps.size();
+    if (nq == 0) return GVA_OK;
+    if ((graph_counts_host || support_host) && (!vgraph || G == 0))
+        return fail(GVA_ERR_ARG, "per-graph results need the database's graph ids (gva_db_set_graphs)");
+    if (budget == 0) {
+        size_t fr = 0, tot = 0;
+        GVA_CUDA_B(cudaMemGetInfo(&fr, &tot));
+        budget = (uint64_t)fr / 4 * 3;
+    }
+    Profiler profiler;
+    Profiler* prof = profile ? &profiler : nullptr;
+    cudaEvent_t ev0, ev1;
+    GVA_CUDA_B(cudaEventCreate(&ev0));
+    GVA_CUDA_B(cudaEventCreate(&ev1));
+    GVA_CUDA_B(cudaEventRecord(ev0, s));
+
+    // per-graph accumulators
+    BatchCtx ctx{};
+    ctx.vgraph = vgraph;
+    ctx.G = G;
+    ctx.words = (G + 31) / 32;
+    const bool per_graph = graph_counts_host || support_host;
+    void* acc = nullptr;
+    size_t acc_bytes = 0;
+    if (per_graph) {
+        acc_bytes = (graph_counts_host ? (size_t)nq * G * 8 : 0) + (size_t)nq * ctx.words * 4;
+        if (cudaMallocAsync(&acc, acc_bytes, s) != cudaSuccess) return fail(GVA_ERR_NOMEM, "per-graph counters");
+        GVA_CUDA_B(cudaMemsetAsync(acc, 0, acc_bytes, s));
+        char* a = (char*)acc;
+        if (graph_counts_host) {
+            ctx.graph_counts = (uint64_t*)a;
+            a += (size_t)nq * G * 8;
+        }
+        ctx.graph_bits = (uint32_t*)a;
+    }
+    for (int q = 0; q < nq; ++q) counts[q] = 0;
+
+    // seed tasks
+    std::vector<Task> active;
+    for (int q = 0; q < nq; ++q) {
+        const std::vector<Step>& st = steps[q];
+        if (st.empty() || st[0].kind != STEP_SEED) return fail(GVA_ERR_ARG, "plan must start with a seed step");
+        if (st[0].always_empty) continue;
+        const uint64_t n = db.seed_off[st[0].label + 1] - db.seed_off[st[0].label];
+        if (n) active.push_back({q, 1, db.seed_verts + db.seed_off[st[0].label], n, nullptr});
+    }
+
+    int status = GVA_OK;
+    std::vector<TaskDesc> descs;
+    std::vector<uint64_t> block0;
+    std::vector<uint64_t> totals;
+    std::vector<uint32_t*> outs;
+    TaskDesc* d_desc = nullptr;
+    size_t desc_cap = 0;
+    uint64_t* d_block0 = nullptr;
+    size_t block0_cap = 0;
+    uint64_t* d_sums = nullptr;
+    size_t sums_cap = 0;
+    uint64_t* d_totals = nullptr;
+    size_t totals_cap = 0;
+    uint32_t** d_outs = nullptr;
+    size_t outs_cap = 0;
+    unsigned long long* d_queue = nullptr;
+    uint64_t* h_pinned = nullptr;
+    size_t pinned_cap = 0;
+    GVA_CUDA_B(cudaMallocAsync((void**)&d_queue, 8, s));
+    static bool smem_set[64] = {};
+    int dev = db.device;
+    if (dev < 64 && !smem_set[dev]) {
+        GVA_CUDA_B(cudaFuncSetAttribute(batch_write_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)batch_smem_bytes()));
+        smem_set[dev] = true;
+    }
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+
+    auto grow = [&](void** p, size_t& cap, size_t need) -> bool {
+        if (need <= cap) return true;
+        if (*p) cudaFreeAsync(*p, s);
+        size_t c = std::max(need, cap * 2);
+        if (cudaMallocAsync(p, c, s) != cudaSuccess) {
+            *p = nullptr;
+            cap = 0;
+            return false;
+        }
+        cap = c;
+        return true;
+    };
+
+    uint64_t rounds = 0, splits = 0, launches = 0;
+    while (!active.empty() && status == GVA_OK) {
+        // steps that cannot match (label or partition absent) end their task
+        active.erase(std::remove_if(active.begin(), active.end(),
+                                    [&](const Task& t) { return steps[t.q][t.step].always_empty != 0; }),
+                     active.end());
+        if (active.empty()) break;
+        ++rounds;
+        const int nt = (int)active.size();
+        descs.assign(nt, TaskDesc{});
+        block0.assign(nt + 1, 0);
+        uint32_t kmax = 1, eqmax = 0;
+        for (int t = 0; t < nt; ++t) {
+            const Task& tk = active[t];
+            const Step& st = steps[tk.q][tk.step];
+            const bool last = tk.step + 1 == (int)steps[tk.q].size();
+            TaskDesc& d = descs[t];
+            memset(&d, 0, sizeof d);
+            d.kind = st.kind;
+            d.query = (uint32_t)tk.q;
+            d.mode = last ? (per_graph ? MODE_COUNT_GRAPHS : MODE_COUNT) : MODE_WRITE;
+            d.block0 = block0[t];
+            const DevPart& P = db.parts[st.part - 1];
+            if (st.kind == STEP_EXT) {
+                ExtArgs& a = d.e;
+                a.in = tk.in;
+                a.nrows = tk.rows;
+                a.off = P.off;
+                a.adj = P.adj;
+                a.k = st.width_in;
+                a.L = db.L;
+                a.lab = st.label;
+                a.src_col = st.src_col;
+                a.bound_col = st.bound_col;
+                a.bound_incl = st.bound_inclusive;
+                a.n_eq = st.n_eq;
+                for (uint32_t i = 0; i < st.n_eq; ++i) a.eq_cols[i] = st.eq_cols[i];
+                eqmax = std::max(eqmax, st.n_eq);
+            } else {
+                RedArgs& a = d.r;
+                a.in = tk.in;
+                a.nrows = tk.rows;
+                a.off = P.off;
+                a.adj = P.adj;
+                a.k = st.width_in;
+                a.L = db.L;
+                a.n_pairs = st.n_pairs;
+                for (uint32_t i = 0; i < st.n_pairs; ++i) {
+                    a.rs[i] = st.rs_col[i];
+                    a.re[i] = st.re_col[i];
+                    a.rl[i] = st.re_label[i];
+                }
+            }
+            kmax = std::max(kmax, st.width_in);
+            block0[t + 1] = block0[t] + (tk.rows + kRowsPerBlock - 1) / kRowsPerBlock;
+        }
+        const uint64_t nb = block0[nt];
+        if (nb > 0x7fffffffull) {
+            status = fail(GVA_ERR_UNSUPPORTED, "round too large for one launch");
+            break;
+        }
+        if (!grow((void**)&d_desc, desc_cap, nt * sizeof(TaskDesc)) ||
+            !grow((void**)&d_block0, block0_cap, (nt + 1) * sizeof(uint64_t)) ||
+            !grow((void**)&d_sums, sums_cap, (nb + 1) * sizeof(uint64_t)) ||
+            !grow((void**)&d_totals, totals_cap, nt * sizeof(uint64_t)) ||
+            !grow((void**)&d_outs, outs_cap, nt * sizeof(uint32_t*))) {
+            status = fail(GVA_ERR_NOMEM, "batch bookkeeping allocation failed");
+            break;
+        }
+        if (pinned_cap < (size_t)nt) {
+            if (h_pinned) cudaFreeHost(h_pinned);
+            pinned_cap = std::max<size_t>(nt, pinned_cap * 2);
+            if (cudaMallocHost(&h_pinned, pinned_cap * 8) != cudaSuccess) {
+                status = fail(GVA_ERR_NOMEM, "pinned host allocation failed");
+                h_pinned = nullptr;
+                break;
+            }
+        }
+        GVA_CUDA_B(cudaMemcpyAsync(d_desc, descs.data(), nt * sizeof(TaskDesc), cudaMemcpyHostToDevice, s));
+        GVA_CUDA_B(cudaMemcpyAsync(d_block0, block0.data(), (nt + 1) * sizeof(uint64_t), cudaMemcpyHostToDevice, s));
+
+        cudaEvent_t ev = nullptr;
+        double cbytes = 0;
+        for (int t = 0; t < nt; ++t) {
+            const Step& st = steps[active[t].q][active[t].step];
+            cbytes += (4.0 * st.width_in + 8.0 * (st.kind == STEP_EXT ? 1 : st.n_pairs)) * (double)active[t].rows;
+        }
+        if (prof) prof->begin(K_EXT_COUNT, cbytes, s, ev);
+        batch_count_kernel<<<(unsigned)nb, kThreads, 0, s>>>(d_desc, d_block0, nt, d_sums, ctx);
+        if (prof) prof->end(ev, K_EXT_COUNT, cbytes, s);
+        if (prof) prof->begin(K_SCAN, 16.0 * nb, s, ev);
+        scan_block_sums_kernel<<<1, kScanThreads, 0, s>>>(d_sums, nb);
+        if (prof) prof->end(ev, K_SCAN, 16.0 * nb, s);
+        task_totals_kernel<<<(nt + 255) / 256, 256, 0, s>>>(d_block0, nt, d_sums, d_totals);
+        launches += 3;
+        GVA_CUDA_B(cudaGetLastError());
+        GVA_CUDA_B(cudaMemcpyAsync(h_pinned, d_totals, nt * sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
+        GVA_CUDA_B(cudaStreamSynchronize(s));
+        totals.assign(h_pinned, h_pinned + nt);
+
+        // choose which tasks write this round: deepest first, within the budget
+        std::vector<int> order;
+        outs.assign(nt, nullptr);
+        std::vector<Task> next;
+        for (int t = 0; t < nt; ++t) {
+            const Task& tk = active[t];
+            const bool last = tk.step + 1 == (int)steps[tk.q].size();
+            if (last) {
+                counts[tk.q] += totals[t];
+            } else if (totals[t] > 0) {
+                order.push_back(t);
+            }
+        }
+        std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return active[a].step > active[b].step; });
+        uint64_t used = 0;
+        std::vector<uint64_t> off_words(nt, 0);
+        std::vector<int> chosen;
+        for (int t : order) {
+            const Step& st = steps[active[t].q][active[t].step];
+            const uint32_t w = st.kind == STEP_EXT ? st.width_in + 1 : st.width_in;
+            const uint64_t bytes = totals[t] * w * 4ull;
+            if (used + bytes <= budget) {
+                off_words[t] = used / 4;
+                used += (bytes + 15) & ~15ull;
+                chosen.push_back(t);
+            } else if (bytes > budget) {
+                // split the task's input rows and retry both halves next round
+                Task a = active[t], b = active[t];
+                const uint64_t half = a.rows / 2;
+                if (half == 0) {
+                    status = fail(GVA_ERR_NOMEM, "a single frontier row expands beyond the memory budget");
+                    break;
+                }
+                const uint32_t win = st.width_in;
+                a.rows = half;
+                b.in = a.in + half * win;
+                b.rows = active[t].rows - half;
+                next.push_back(a);
+                next.push_back(b);
+                ++splits;
+            } else {
+                next.push_back(active[t]);  // fits alone: waits for the next round
+            }
+        }
+        if (status) break;
+        std::shared_ptr<DevBuf> buf;
+        if (used > 0) {
+            buf = std::make_shared<DevBuf>();
+            buf->s = s;
+            if (cudaMallocAsync(&buf->p, used, s) != cudaSuccess) {
+                buf->p = nullptr;
+                status = fail(GVA_ERR_NOMEM, "frontier allocation failed");
+                break;
+            }
+            double wbytes = 0;
+            for (int t : chosen) {
+                outs[t] = (uint32_t*)buf->p + off_words[t];
+                const Step& st = steps[active[t].q][active[t].step];
+                const double k = st.width_in;
+                wbytes += (4.0 * k + 8.0) * (double)active[t].rows +
+                          (st.kind == STEP_EXT ? (4.0 + 4.0 * (k + 1)) : 4.0 * k) * (double)totals[t];
+            }
+            GVA_CUDA_B(cudaMemcpyAsync(d_outs, outs.data(), nt * sizeof(uint32_t*), cudaMemcpyHostToDevice, s));
+            GVA_CUDA_B(cudaMemsetAsync(d_queue, 0, 8, s));
+            const size_t smem = batch_smem_bytes_for(kmax, std::max(eqmax, 1u));
+            int per_sm = 1;
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_write_kernel, kThreads, smem);
+            const uint64_t grid = std::min<uint64_t>(nb, (uint64_t)std::max(per_sm, 1) * sms);
+            if (prof) prof->begin(K_EXT_WRITE, wbytes, s, ev);
+            batch_write_kernel<<<(unsigned)grid, kThreads, smem, s>>>(d_desc, d_block0, nt, nb, d_sums, d_outs,
+                                                                      d_queue);
+            if (prof) prof->end(ev, K_EXT_WRITE, wbytes, s);
+            launches += 1;
+            GVA_CUDA_B(cudaGetLastError());
+        }
+        for (int t : chosen) {
+            Task nt2 = active[t];
+            nt2.in = outs[t];
+            nt2.rows = totals[t];
+            nt2.step += 1;
+            nt2.owner = buf;
+            next.push_back(nt2);
+        }
+        active.swap(next);
+        if (prof) {
+            GVA_CUDA_B(cudaStreamSynchronize(s));
+            prof->resolve();
+        }
+    }
+    g_batch_launches += launches;
+    active.clear();  // releases frontier buffers (stream-ordered)
+
+    if (status == GVA_OK && per_graph) {
+        if (graph_counts_host)
+            GVA_CUDA_B(cudaMemcpyAsync(graph_counts_host, ctx.graph_counts, (size_t)nq * G * 8, cudaMemcpyDeviceToHost, s));
+        if (support_host) {
+            std::vector<uint32_t> bits((size_t)nq * ctx.words);
+            GVA_CUDA_B(cudaMemcpyAsync(bits.data(), ctx.graph_bits, bits.size() * 4, cudaMemcpyDeviceToHost, s));
+            GVA_CUDA_B(cudaStreamSynchronize(s));
+            for (int q = 0; q < nq; ++q) {
+                uint32_t c = 0;
+                for (uint32_t w = 0; w < ctx.words; ++w) c += (uint32_t)__builtin_popcount(bits[(size_t)q * ctx.words + w]);
+                support_host[q] = c;
+            }
+        }
+    }
+    if (acc) cudaFreeAsync(acc, s);
+    for (void* p : {(void*)d_desc, (void*)d_block0, (void*)d_sums, (void*)d_totals, (void*)d_outs, (void*)d_queue})
+        if (p) cudaFreeAsync(p, s);
+    if (h_pinned) {
+        cudaStreamSynchronize(s);
+        cudaFreeHost(h_pinned);
+    }
+    cudaEventRecord(ev1, s);
+    cudaEventSynchronize(ev1);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, ev0, ev1);
+    cudaEventDestroy(ev0);
+    cudaEventDestroy(ev1);
+    if (stats) {
+        stats->gpu_ms = ms;
+        stats->rounds = rounds;
+        stats->splits = splits;
+        stats->launches = launches;
+        if (prof) {
+            prof->resolve();
+            for (int i = 0; i < K_NUM; ++i) stats->kstat[i] = prof->stat[i];
+        }
+    }
+    return status;
+}
+
+int set_graph_ids(DevDB& db, const uint64_t* first, uint32_t num_graphs) {
+    if (!first || num_graphs == 0) return fail(GVA_ERR_ARG, "graph boundaries missing");
+    std::vector<uint32_t> vg(db.max_id + 1, 0xffffffffu);
+    for (uint32_t g = 0; g < num_graphs; ++g) {
+        if (first[g] > first[g + 1] || first[g + 1] > (uint64_t)db.max_id + 1)
+            return fail(GVA_ERR_ARG, "graph boundaries must be ascending within 1..max_vertex_id+1");
+        for (uint64_t v = first[g]; v < first[g + 1]; ++v) vg[v] = g;
+    }
+    GVA_CUDA_B(cudaSetDevice(db.device));
+    if (db.vgraph) cudaFree(db.vgraph);
+    db.vgraph = nullptr;
+    GVA_CUDA_B(cudaMalloc(&db.vgraph, vg.size() * 4));
+    GVA_CUDA_B(cudaMemcpy(db.vgraph, vg.data(), vg.size() * 4, cudaMemcpyHostToDevice));
+    db.num_graphs = num_graphs;
+    return GVA_OK;
+}
+
+}  // namespace gva

@@ -68,6 +68,20 @@ const char* gva_status_string(int s) {
 
 const char* gva_version(void) { return "geneva_b200 0.1 (sm_100a)"; }
 
+uint64_t gva_kernel_launches(void) { return kernel_launches(); }
+
+int gva_result_kernel_stats(const gva_result* res, gva_kernel_stat* out, int cap) {
+    if (!res) return -1;
+    for (int i = 0; i < K_NUM && i < cap; ++i) {
+        memset(&out[i], 0, sizeof out[i]);
+        strncpy(out[i].name, kKernelNames[i], sizeof out[i].name - 1);
+        out[i].launches = res->r.kstat[i].launches;
+        out[i].ms = res->r.kstat[i].ms;
+        out[i].bytes = res->r.kstat[i].bytes;
+    }
+    return K_NUM;
+}
+
 int gva_db_load(const char* mygraph_path, const char* metadata_path, int device, gva_db** out) {
     if (!out || !mygraph_path || !metadata_path) return fail(GVA_ERR_ARG, "null argument");
     *out = nullptr;
@@ -197,7 +211,8 @@ int gva_match(gva_db* db, const gva_plan* plan, const gva_match_opts* opts, gva_
     gva_match_opts o{};
     if (opts) o = *opts;
     gva_result* r = new gva_result();
-    st = run_match(*db->dev, plan->plan, steps, (cudaStream_t)o.stream, o.budget_bytes, o.count_only != 0, r->r);
+    st = run_match(*db->dev, plan->plan, steps, (cudaStream_t)o.stream, o.budget_bytes, o.count_only != 0,
+                   o.profile != 0, r->r);
     if (st) {
         delete r;
         return st;
@@ -269,6 +284,41 @@ void gva_result_free(gva_result* res) {
     MatchResult* m = new MatchResult(std::move(res->r));
     free_result(m);
     delete res;
+}
+
+int gva_db_set_graphs(gva_db* db, const uint64_t* first, uint32_t num_graphs) {
+    if (!db) return fail(GVA_ERR_ARG, "null argument");
+    return set_graph_ids(*db->dev, first, num_graphs);
+}
+
+int gva_batch_count(gva_db* db, const gva_plan* const* plans, int nplans, const gva_batch_opts* opts,
+                    uint64_t* counts, uint64_t* graph_counts, uint32_t* graph_support, gva_batch_stats* stats) {
+    if (!db || (nplans > 0 && (!plans || !counts))) return fail(GVA_ERR_ARG, "null argument");
+    gva_batch_opts o{};
+    if (opts) o = *opts;
+    std::vector<std::vector<Step>> steps(nplans);
+    for (int i = 0; i < nplans; ++i) {
+        if (!plans[i]) return fail(GVA_ERR_ARG, "null plan");
+        int st = steps_for(plans[i], db, steps[i]);
+        if (st) return st;
+    }
+    BatchStats bs;
+    int st = run_batch(*db->dev, steps, (cudaStream_t)o.stream, o.budget_bytes, db->dev->vgraph, db->dev->num_graphs,
+                       counts, graph_counts, graph_support, o.profile != 0, &bs);
+    if (stats) {
+        memset(stats, 0, sizeof *stats);
+        stats->gpu_ms = bs.gpu_ms;
+        stats->rounds = bs.rounds;
+        stats->splits = bs.splits;
+        stats->launches = bs.launches;
+        for (int i = 0; i < K_NUM && i < 5; ++i) {
+            strncpy(stats->kernels[i].name, kKernelNames[i], sizeof stats->kernels[i].name - 1);
+            stats->kernels[i].launches = bs.kstat[i].launches;
+            stats->kernels[i].ms = bs.kstat[i].ms;
+            stats->kernels[i].bytes = bs.kstat[i].bytes;
+        }
+    }
+    return st;
 }
 
 int gva_plan_num_steps(const gva_plan* plan, const gva_db* db) {

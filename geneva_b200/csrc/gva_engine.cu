@@ -17,20 +17,18 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cstdio>
 #include <cstring>
 #include <string>
 
 #include "../../include/geneva.h"
 #include "gva_engine.cuh"
+#include "gva_kernels.cuh"
 
 namespace gva {
 
 namespace {
-
-constexpr int kRowsPerBlock = 256;  // rows handled by one count/write block
-constexpr int kThreads = 256;
-constexpr int kScanThreads = 1024;
 
 #define GVA_CUDA(call)                                                                                  \
     do {                                                                                                \
@@ -40,147 +38,6 @@ constexpr int kScanThreads = 1024;
     } while (0)
 
 inline size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
-
-// ---------------------------------------------------------------- params ----
-struct ExtArgs {
-    const uint32_t* in;
-    uint64_t nrows;
-    uint32_t* out;
-    const uint32_t* off;
-    const uint32_t* adj;
-    uint32_t k;        // input width
-    uint32_t L;        // dense labels
-    uint32_t lab;      // dense candidate label
-    int32_t src_col;
-    int32_t bound_col;
-    uint32_t bound_incl;
-    uint32_t n_eq;
-    uint8_t eq_cols[kMaxCols];
-};
-
-struct RedArgs {
-    const uint32_t* in;
-    uint64_t nrows;
-    uint32_t* out;
-    const uint32_t* off;
-    const uint32_t* adj;
-    uint32_t k;
-    uint32_t L;
-    uint32_t n_pairs;
-    uint8_t rs[16];
-    uint8_t re[16];
-    uint32_t rl[16];
-};
-
-__device__ __forceinline__ uint64_t umin64(uint64_t a, uint64_t b) { return a < b ? a : b; }
-
-// first index in [lo, hi) with a[i] >= x (hi if none)
-__device__ __forceinline__ uint32_t lower_bound_u32(const uint32_t* __restrict__ a, uint32_t lo, uint32_t hi,
-                                                    uint64_t x) {
-    while (lo < hi) {
-        const uint32_t mid = lo + ((hi - lo) >> 1);
-        if ((uint64_t)__ldg(a + mid) < x)
-            lo = mid + 1;
-        else
-            hi = mid;
-    }
-    return lo;
-}
-
-// Candidate range of one row: the (source, label) segment cut below the
-// restriction bound.
-__device__ __forceinline__ void ext_range(const ExtArgs& p, const uint32_t* row, uint32_t& lo, uint32_t& hi) {
-    const uint32_t s = row[p.src_col];
-    const uint64_t t = (uint64_t)s * p.L + p.lab;
-    lo = __ldg(p.off + t);
-    hi = __ldg(p.off + t + 1);
-    if (p.bound_col >= 0 && lo < hi) {
-        const uint64_t b = (uint64_t)row[p.bound_col] + p.bound_incl;
-        hi = lower_bound_u32(p.adj, lo, hi, b);
-    }
-}
-
-// Position of w in adj[lo, hi), or 0xffffffff.
-__device__ __forceinline__ uint32_t find_in(const uint32_t* __restrict__ adj, uint32_t lo, uint32_t hi, uint32_t w) {
-    if (lo >= hi) return 0xffffffffu;
-    if (w < __ldg(adj + lo) || w > __ldg(adj + hi - 1)) return 0xffffffffu;
-    const uint32_t pos = lower_bound_u32(adj, lo, hi, w);
-    return (pos < hi && __ldg(adj + pos) == w) ? pos : 0xffffffffu;
-}
-
-// Number of candidates of one row (segment minus already-matched vertices).
-__device__ __forceinline__ uint32_t ext_count_row(const ExtArgs& p, const uint32_t* row) {
-    uint32_t lo, hi;
-    ext_range(p, row, lo, hi);
-    if (lo >= hi) return 0;
-    uint32_t n = hi - lo;
-    for (uint32_t j = 0; j < p.n_eq; ++j) {
-        const uint32_t w = row[p.eq_cols[j]];
-        bool dup = false;  // the same vertex in two columns collides once
-        for (uint32_t i = 0; i < j; ++i) dup |= (row[p.eq_cols[i]] == w);
-        if (!dup && find_in(p.adj, lo, hi, w) != 0xffffffffu) --n;
-    }
-    return n;
-}
-
-__device__ __forceinline__ bool red_keep_row(const RedArgs& p, const uint32_t* row) {
-    for (uint32_t j = 0; j < p.n_pairs; ++j) {
-        const uint32_t s = row[p.rs[j]];
-        const uint32_t e = row[p.re[j]];
-        const uint64_t t = (uint64_t)s * p.L + p.rl[j];
-        const uint32_t lo = __ldg(p.off + t), hi = __ldg(p.off + t + 1);
-        if (find_in(p.adj, lo, hi, e) == 0xffffffffu) return false;
-    }
-    return true;
-}
-
-// ------------------------------------------------------------ block sums ----
-template <typename T>
-__device__ __forceinline__ T warp_sum(T v) {
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-    return v;
-}
-
-__device__ __forceinline__ void store_block_sum(uint64_t v, uint64_t* block_sums) {
-    __shared__ uint64_t ws[kThreads / 32];
-    v = warp_sum(v);
-    if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = v;
-    __syncthreads();
-    if (threadIdx.x < 32) {
-        uint64_t x = threadIdx.x < kThreads / 32 ? ws[threadIdx.x] : 0;
-        x = warp_sum(x);
-        if (threadIdx.x == 0) block_sums[blockIdx.x] = x;
-    }
-}
-
-// Exclusive scan of 256 per-thread values in shared memory (uint64).
-__device__ __forceinline__ uint64_t block_exclusive_scan(uint64_t v, uint64_t* total) {
-    __shared__ uint64_t ws[kThreads / 32];
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    uint64_t x = v;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        const uint64_t y = __shfl_up_sync(0xffffffffu, x, o);
-        if (lane >= o) x += y;
-    }
-    if (lane == 31) ws[wid] = x;
-    __syncthreads();
-    if (wid == 0) {
-        uint64_t w = lane < kThreads / 32 ? ws[lane] : 0;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const uint64_t y = __shfl_up_sync(0xffffffffu, w, o);
-            if (lane >= o) w += y;
-        }
-        if (lane < kThreads / 32) ws[lane] = w;
-    }
-    __syncthreads();
-    const uint64_t before = (wid > 0 ? ws[wid - 1] : 0) + x - v;
-    *total = ws[kThreads / 32 - 1];
-    __syncthreads();
-    return before;
-}
 
 // ---------------------------------------------------------------- kernels ---
 __global__ void __launch_bounds__(kThreads) ext_count_kernel(ExtArgs p, uint64_t* __restrict__ block_sums) {
@@ -195,43 +52,6 @@ __global__ void __launch_bounds__(kThreads) red_count_kernel(RedArgs p, uint64_t
     uint64_t c = 0;
     if (r < p.nrows) c = red_keep_row(p, p.in + r * p.k) ? 1 : 0;
     store_block_sum(c, block_sums);
-}
-
-// In-place exclusive scan of n block totals; sums[n] receives the total.
-__global__ void __launch_bounds__(kScanThreads) scan_block_sums_kernel(uint64_t* __restrict__ sums, uint64_t n) {
-    __shared__ uint64_t ws[kScanThreads / 32];
-    __shared__ uint64_t carry_s;
-    if (threadIdx.x == 0) carry_s = 0;
-    __syncthreads();
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    for (uint64_t base = 0; base < n; base += kScanThreads) {
-        const uint64_t i = base + threadIdx.x;
-        const uint64_t v = i < n ? sums[i] : 0;
-        uint64_t x = v;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const uint64_t y = __shfl_up_sync(0xffffffffu, x, o);
-            if (lane >= o) x += y;
-        }
-        if (lane == 31) ws[wid] = x;
-        __syncthreads();
-        if (wid == 0) {
-            uint64_t w = ws[lane];
-#pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-                const uint64_t y = __shfl_up_sync(0xffffffffu, w, o);
-                if (lane >= o) w += y;
-            }
-            ws[lane] = w;
-        }
-        __syncthreads();
-        const uint64_t carry = carry_s;
-        if (i < n) sums[i] = carry + (wid > 0 ? ws[wid - 1] : 0) + x - v;
-        __syncthreads();
-        if (threadIdx.x == 0) carry_s = carry + ws[kScanThreads / 32 - 1];
-        __syncthreads();
-    }
-    if (threadIdx.x == 0) sums[n] = carry_s;
 }
 
 // Block b expands rows [256b, 256b + 256): every thread produces one output
@@ -344,6 +164,8 @@ size_t ext_smem_bytes(uint32_t k, uint32_t n_eq) {
 }
 size_t red_smem_bytes(uint32_t k) { return sizeof(uint32_t) * 2 * (size_t)kRowsPerBlock * k; }
 
+std::atomic<uint64_t> g_launches{0};
+
 int set_smem_limits() {
     static bool done[64] = {};
     int dev = 0;
@@ -395,39 +217,60 @@ void fill_red(RedArgs& a, const DevDB& db, const Step& st, const uint32_t* in, u
 
 // count + scan; leaves exclusive block offsets in sums[0..nb) and the total in sums[nb]
 int launch_count(const DevDB& db, const Step& st, const uint32_t* in, uint64_t nrows, uint64_t* sums,
-                 cudaStream_t s) {
+                 cudaStream_t s, Profiler* prof) {
     const uint64_t nb = (nrows + kRowsPerBlock - 1) / kRowsPerBlock;
     if (nb > 0x7fffffffull) return fail(GVA_ERR_UNSUPPORTED, "frontier too large for one launch");
+    const double k = st.width_in;
+    cudaEvent_t ev = nullptr;
     if (st.kind == STEP_EXT) {
         ExtArgs a;
         fill_ext(a, db, st, in, nrows, nullptr);
+        const double bytes = (4.0 * k + 8.0) * (double)nrows;
+        if (prof) prof->begin(K_EXT_COUNT, bytes, s, ev);
         ext_count_kernel<<<(unsigned)nb, kThreads, 0, s>>>(a, sums);
+        if (prof) prof->end(ev, K_EXT_COUNT, bytes, s);
     } else {
         RedArgs a;
         fill_red(a, db, st, in, nrows, nullptr);
+        const double bytes = (4.0 * k + 8.0 * st.n_pairs) * (double)nrows;
+        if (prof) prof->begin(K_RED_COUNT, bytes, s, ev);
         red_count_kernel<<<(unsigned)nb, kThreads, 0, s>>>(a, sums);
+        if (prof) prof->end(ev, K_RED_COUNT, bytes, s);
     }
     GVA_CUDA(cudaGetLastError());
+    const double sbytes = 16.0 * (double)nb;
+    if (prof) prof->begin(K_SCAN, sbytes, s, ev);
     scan_block_sums_kernel<<<1, kScanThreads, 0, s>>>(sums, nb);
+    if (prof) prof->end(ev, K_SCAN, sbytes, s);
     GVA_CUDA(cudaGetLastError());
+    g_launches += 2;
     return GVA_OK;
 }
 
 int launch_write(const DevDB& db, const Step& st, const uint32_t* in, uint64_t nrows, uint32_t* out,
-                 const uint64_t* sums, cudaStream_t s) {
+                 const uint64_t* sums, uint64_t nout, cudaStream_t s, Profiler* prof) {
     const uint64_t nb = (nrows + kRowsPerBlock - 1) / kRowsPerBlock;
     int rc = set_smem_limits();
     if (rc) return rc;
+    const double k = st.width_in;
+    cudaEvent_t ev = nullptr;
     if (st.kind == STEP_EXT) {
         ExtArgs a;
         fill_ext(a, db, st, in, nrows, out);
+        const double bytes = (4.0 * k + 8.0) * (double)nrows + (4.0 + 4.0 * (k + 1)) * (double)nout;
+        if (prof) prof->begin(K_EXT_WRITE, bytes, s, ev);
         ext_write_kernel<<<(unsigned)nb, kThreads, ext_smem_bytes(a.k, a.n_eq), s>>>(a, sums);
+        if (prof) prof->end(ev, K_EXT_WRITE, bytes, s);
     } else {
         RedArgs a;
         fill_red(a, db, st, in, nrows, out);
+        const double bytes = (4.0 * k + 8.0 * st.n_pairs) * (double)nrows + 4.0 * k * (double)nout;
+        if (prof) prof->begin(K_RED_WRITE, bytes, s, ev);
         red_write_kernel<<<(unsigned)nb, kThreads, red_smem_bytes(a.k), s>>>(a, sums);
+        if (prof) prof->end(ev, K_RED_WRITE, bytes, s);
     }
     GVA_CUDA(cudaGetLastError());
+    g_launches += 1;
     return GVA_OK;
 }
 
@@ -443,6 +286,38 @@ int ensure_pool(int device) {
 }
 
 }  // namespace
+
+const char* const kKernelNames[K_NUM] = {"ext_count", "ext_write", "red_count", "red_write", "scan_block_sums"};
+
+uint64_t kernel_launches() { return g_launches.load() + batch_kernel_launches(); }
+
+void Profiler::begin(int kind, double bytes, cudaStream_t s, cudaEvent_t& a) {
+    (void)kind;
+    (void)bytes;
+    cudaEventCreate(&a);
+    cudaEventRecord(a, s);
+}
+
+void Profiler::end(cudaEvent_t a, int kind, double bytes, cudaStream_t s) {
+    cudaEvent_t b;
+    cudaEventCreate(&b);
+    cudaEventRecord(b, s);
+    pending.push_back({kind, a, b, bytes});
+}
+
+void Profiler::resolve() {
+    for (auto& p : pending) {
+        float ms = 0.f;
+        cudaEventSynchronize(p.b);
+        cudaEventElapsedTime(&ms, p.a, p.b);
+        stat[p.kind].launches += 1;
+        stat[p.kind].ms += ms;
+        stat[p.kind].bytes += p.bytes;
+        cudaEventDestroy(p.a);
+        cudaEventDestroy(p.b);
+    }
+    pending.clear();
+}
 
 // ------------------------------------------------------------- database ----
 int upload_graph(HostGraph& g, int device, DevDB*& out) {
@@ -514,10 +389,9 @@ int upload_graph(HostGraph& g, int device, DevDB*& out) {
 
 void free_devdb(DevDB* db) {
     if (!db) return;
-    if (db->arena) {
-        cudaSetDevice(db->device);
-        cudaFree(db->arena);
-    }
+    if (db->arena || db->vgraph) cudaSetDevice(db->device);
+    if (db->arena) cudaFree(db->arena);
+    if (db->vgraph) cudaFree(db->vgraph);
     delete db;
 }
 
@@ -544,7 +418,7 @@ int run_step(DevDB& db, const Step& st, const uint32_t* in, uint64_t in_rows, ui
     if (!in || !scratch) return fail(GVA_ERR_ARG, "null device buffer");
     if (scratch_bytes < step_scratch_bytes(in_rows)) return fail(GVA_ERR_ARG, "scratch too small");
     uint64_t* sums = (uint64_t*)scratch;
-    int rc = launch_count(db, st, in, in_rows, sums, s);
+    int rc = launch_count(db, st, in, in_rows, sums, s, nullptr);
     if (rc) return rc;
     const uint64_t nb = (in_rows + kRowsPerBlock - 1) / kRowsPerBlock;
     uint64_t total = 0;
@@ -554,12 +428,14 @@ int run_step(DevDB& db, const Step& st, const uint32_t* in, uint64_t in_rows, ui
     if (total > out_cap) return fail(GVA_ERR_NOMEM, "output capacity too small");
     if (total == 0) return GVA_OK;
     if (!out) return fail(GVA_ERR_ARG, "null output buffer");
-    return launch_write(db, st, in, in_rows, out, sums, s);
+    return launch_write(db, st, in, in_rows, out, sums, total, s, nullptr);
 }
 
 // ------------------------------------------------------- whole query (L3) --
 int run_match(DevDB& db, const Plan& plan, const std::vector<Step>& steps, cudaStream_t s, uint64_t budget,
-              bool count_only, MatchResult& res) {
+              bool count_only, bool profile, MatchResult& res) {
+    Profiler profiler;
+    Profiler* prof = profile ? &profiler : nullptr;
     GVA_CUDA(cudaSetDevice(db.device));
     int rc = ensure_pool(db.device);
     if (rc) return rc;
@@ -607,7 +483,7 @@ int run_match(DevDB& db, const Plan& plan, const std::vector<Step>& steps, cudaS
                 if (ce != cudaSuccess) { status = fail(GVA_ERR_NOMEM, "scratch allocation failed"); sums = nullptr; break; }
                 sums_bytes = need;
             }
-            status = launch_count(db, st, cur, rows, sums, s);
+            status = launch_count(db, st, cur, rows, sums, s, prof);
             if (status) break;
             const uint64_t nb = (rows + kRowsPerBlock - 1) / kRowsPerBlock;
             ce = cudaMemcpyAsync(total_h, sums + nb, 8, cudaMemcpyDeviceToHost, s);
@@ -628,7 +504,7 @@ int run_match(DevDB& db, const Plan& plan, const std::vector<Step>& steps, cudaS
                 uint32_t* out = nullptr;
                 ce = cudaMallocAsync((void**)&out, bytes, s);
                 if (ce != cudaSuccess) { status = fail(GVA_ERR_NOMEM, "frontier allocation failed"); break; }
-                status = launch_write(db, st, cur, rows, out, sums, s);
+                status = launch_write(db, st, cur, rows, out, sums, total, s, prof);
                 if (status) { cudaFreeAsync(out, s); break; }
                 if (owned) cudaFreeAsync(owned, s);
                 owned = out;
@@ -644,6 +520,7 @@ int run_match(DevDB& db, const Plan& plan, const std::vector<Step>& steps, cudaS
     cudaFreeHost(total_h);
     if (status) {
         if (owned) cudaFreeAsync(owned, s);
+        if (prof) prof->resolve();
         cudaEventDestroy(ev0);
         cudaEventDestroy(ev1);
         return status;
@@ -655,6 +532,10 @@ int run_match(DevDB& db, const Plan& plan, const std::vector<Step>& steps, cudaS
     cudaEventDestroy(ev0);
     cudaEventDestroy(ev1);
     res.gpu_ms = ms;
+    if (prof) {
+        prof->resolve();
+        for (int i = 0; i < K_NUM; ++i) res.kstat[i] = prof->stat[i];
+    }
     // the final width is the number of columns of the plan
     res.width = (uint32_t)plan.columns.size();
     res.rows = rows;

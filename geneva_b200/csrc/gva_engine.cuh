@@ -31,10 +31,34 @@ struct DevDB {
     size_t arena_bytes = 0;
     uint64_t n_adj = 0;
     HostGraph meta;                       // labels/partition presence for lowering (no adjacency)
+    uint32_t* vgraph = nullptr;           // optional vertex -> graph id map (graph databases)
+    uint32_t num_graphs = 0;
 };
 
 int upload_graph(HostGraph& g, int device, DevDB*& out);
 void free_devdb(DevDB* db);
+
+enum KernelKind { K_EXT_COUNT = 0, K_EXT_WRITE, K_RED_COUNT, K_RED_WRITE, K_SCAN, K_NUM };
+extern const char* const kKernelNames[K_NUM];
+
+struct KernelStat {
+    uint64_t launches = 0;
+    double ms = 0.0;
+    double bytes = 0.0;
+};
+
+// Optional per-launch CUDA-event timing.
+struct Profiler {
+    bool on = false;
+    struct Pending { int kind; cudaEvent_t a, b; double bytes; };
+    std::vector<Pending> pending;
+    KernelStat stat[K_NUM];
+    void begin(int kind, double bytes, cudaStream_t s, cudaEvent_t& a);
+    void end(cudaEvent_t a, int kind, double bytes, cudaStream_t s);
+    void resolve();  // after a stream sync
+};
+
+uint64_t kernel_launches();
 
 struct MatchResult {
     int device = 0;
@@ -45,11 +69,26 @@ struct MatchResult {
     std::vector<uint64_t> phase_rows;
     double gpu_ms = 0.0;
     std::vector<uint32_t> columns;
+    KernelStat kstat[K_NUM];
 };
 
 int run_match(DevDB& db, const Plan& plan, const std::vector<Step>& steps, cudaStream_t stream, uint64_t budget,
-              bool count_only, MatchResult& res);
+              bool count_only, bool profile, MatchResult& res);
 void free_result(MatchResult* r);
+
+struct BatchStats {
+    double gpu_ms = 0.0;
+    uint64_t rounds = 0, splits = 0, launches = 0;
+    KernelStat kstat[K_NUM];
+};
+
+// Counts the embeddings of many plans in shared rounds.  counts[q] always;
+// graph_counts [nq * G] and support [nq] when given (need db.vgraph).
+int run_batch(DevDB& db, const std::vector<std::vector<Step>>& steps, cudaStream_t s, uint64_t budget,
+              const uint32_t* vgraph, uint32_t G, uint64_t* counts, uint64_t* graph_counts_host,
+              uint32_t* support_host, bool profile, BatchStats* stats);
+uint64_t batch_kernel_launches();
+int set_graph_ids(DevDB& db, const uint64_t* first, uint32_t num_graphs);
 
 size_t step_scratch_bytes(uint64_t in_rows);
 int run_step(DevDB& db, const Step& st, const uint32_t* in, uint64_t in_rows, uint32_t* out, uint64_t out_cap,

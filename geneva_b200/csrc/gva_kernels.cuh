@@ -1,0 +1,198 @@
+// Device-side building blocks shared by the per-query and the batched
+// engines: kernel argument blocks, segment lookup, membership test, block
+// scans.  Included by gva_engine.cu and gva_batch.cu (internal linkage).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "gva_internal.h"
+
+namespace gva {
+namespace {
+
+constexpr int kRowsPerBlock = 256;  // rows handled by one count/write block
+constexpr int kThreads = 256;
+constexpr int kScanThreads = 1024;
+
+// ---------------------------------------------------------------- params ----
+struct ExtArgs {
+    const uint32_t* in;
+    uint64_t nrows;
+    uint32_t* out;
+    const uint32_t* off;
+    const uint32_t* adj;
+    uint32_t k;        // input width
+    uint32_t L;        // dense labels
+    uint32_t lab;      // dense candidate label
+    int32_t src_col;
+    int32_t bound_col;
+    uint32_t bound_incl;
+    uint32_t n_eq;
+    uint8_t eq_cols[kMaxCols];
+};
+
+struct RedArgs {
+    const uint32_t* in;
+    uint64_t nrows;
+    uint32_t* out;
+    const uint32_t* off;
+    const uint32_t* adj;
+    uint32_t k;
+    uint32_t L;
+    uint32_t n_pairs;
+    uint8_t rs[16];
+    uint8_t re[16];
+    uint32_t rl[16];
+};
+
+__device__ __forceinline__ uint64_t umin64(uint64_t a, uint64_t b) { return a < b ? a : b; }
+
+// first index in [lo, hi) with a[i] >= x (hi if none)
+__device__ __forceinline__ uint32_t lower_bound_u32(const uint32_t* __restrict__ a, uint32_t lo, uint32_t hi,
+                                                    uint64_t x) {
+    while (lo < hi) {
+        const uint32_t mid = lo + ((hi - lo) >> 1);
+        if ((uint64_t)__ldg(a + mid) < x)
+            lo = mid + 1;
+        else
+            hi = mid;
+    }
+    return lo;
+}
+
+// Candidate range of one row: the (source, label) segment cut below the
+// restriction bound.
+__device__ __forceinline__ void ext_range(const ExtArgs& p, const uint32_t* row, uint32_t& lo, uint32_t& hi) {
+    const uint32_t s = row[p.src_col];
+    const uint64_t t = (uint64_t)s * p.L + p.lab;
+    lo = __ldg(p.off + t);
+    hi = __ldg(p.off + t + 1);
+    if (p.bound_col >= 0 && lo < hi) {
+        const uint64_t b = (uint64_t)row[p.bound_col] + p.bound_incl;
+        hi = lower_bound_u32(p.adj, lo, hi, b);
+    }
+}
+
+// Position of w in adj[lo, hi), or 0xffffffff.
+__device__ __forceinline__ uint32_t find_in(const uint32_t* __restrict__ adj, uint32_t lo, uint32_t hi, uint32_t w) {
+    if (lo >= hi) return 0xffffffffu;
+    if (w < __ldg(adj + lo) || w > __ldg(adj + hi - 1)) return 0xffffffffu;
+    const uint32_t pos = lower_bound_u32(adj, lo, hi, w);
+    return (pos < hi && __ldg(adj + pos) == w) ? pos : 0xffffffffu;
+}
+
+// Number of candidates of one row (segment minus already-matched vertices).
+__device__ __forceinline__ uint32_t ext_count_row(const ExtArgs& p, const uint32_t* row) {
+    uint32_t lo, hi;
+    ext_range(p, row, lo, hi);
+    if (lo >= hi) return 0;
+    uint32_t n = hi - lo;
+    for (uint32_t j = 0; j < p.n_eq; ++j) {
+        const uint32_t w = row[p.eq_cols[j]];
+        bool dup = false;  // the same vertex in two columns collides once
+        for (uint32_t i = 0; i < j; ++i) dup |= (row[p.eq_cols[i]] == w);
+        if (!dup && find_in(p.adj, lo, hi, w) != 0xffffffffu) --n;
+    }
+    return n;
+}
+
+__device__ __forceinline__ bool red_keep_row(const RedArgs& p, const uint32_t* row) {
+    for (uint32_t j = 0; j < p.n_pairs; ++j) {
+        const uint32_t s = row[p.rs[j]];
+        const uint32_t e = row[p.re[j]];
+        const uint64_t t = (uint64_t)s * p.L + p.rl[j];
+        const uint32_t lo = __ldg(p.off + t), hi = __ldg(p.off + t + 1);
+        if (find_in(p.adj, lo, hi, e) == 0xffffffffu) return false;
+    }
+    return true;
+}
+
+// ------------------------------------------------------------ block sums ----
+template <typename T>
+__device__ __forceinline__ T warp_sum(T v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    return v;
+}
+
+__device__ __forceinline__ void store_block_sum(uint64_t v, uint64_t* block_sums) {
+    __shared__ uint64_t ws[kThreads / 32];
+    v = warp_sum(v);
+    if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = v;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        uint64_t x = threadIdx.x < kThreads / 32 ? ws[threadIdx.x] : 0;
+        x = warp_sum(x);
+        if (threadIdx.x == 0) block_sums[blockIdx.x] = x;
+    }
+}
+
+// Exclusive scan of 256 per-thread values in shared memory (uint64).
+__device__ __forceinline__ uint64_t block_exclusive_scan(uint64_t v, uint64_t* total) {
+    __shared__ uint64_t ws[kThreads / 32];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    uint64_t x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint64_t y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) ws[wid] = x;
+    __syncthreads();
+    if (wid == 0) {
+        uint64_t w = lane < kThreads / 32 ? ws[lane] : 0;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint64_t y = __shfl_up_sync(0xffffffffu, w, o);
+            if (lane >= o) w += y;
+        }
+        if (lane < kThreads / 32) ws[lane] = w;
+    }
+    __syncthreads();
+    const uint64_t before = (wid > 0 ? ws[wid - 1] : 0) + x - v;
+    *total = ws[kThreads / 32 - 1];
+    __syncthreads();
+    return before;
+}
+
+// In-place exclusive scan of n block totals; sums[n] receives the total.
+__global__ void __launch_bounds__(kScanThreads) scan_block_sums_kernel(uint64_t* __restrict__ sums, uint64_t n) {
+    __shared__ uint64_t ws[kScanThreads / 32];
+    __shared__ uint64_t carry_s;
+    if (threadIdx.x == 0) carry_s = 0;
+    __syncthreads();
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    for (uint64_t base = 0; base < n; base += kScanThreads) {
+        const uint64_t i = base + threadIdx.x;
+        const uint64_t v = i < n ? sums[i] : 0;
+        uint64_t x = v;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint64_t y = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o) x += y;
+        }
+        if (lane == 31) ws[wid] = x;
+        __syncthreads();
+        if (wid == 0) {
+            uint64_t w = ws[lane];
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint64_t y = __shfl_up_sync(0xffffffffu, w, o);
+                if (lane >= o) w += y;
+            }
+            ws[lane] = w;
+        }
+        __syncthreads();
+        const uint64_t carry = carry_s;
+        if (i < n) sums[i] = carry + (wid > 0 ? ws[wid - 1] : 0) + x - v;
+        __syncthreads();
+        if (threadIdx.x == 0) carry_s = carry + ws[kScanThreads / 32 - 1];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) sums[n] = carry_s;
+}
+
+}  // namespace
+}  // namespace gva

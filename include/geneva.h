@@ -62,13 +62,26 @@ typedef struct gva_match_opts {
     void* stream;          /* cudaStream_t; NULL = legacy default stream             */
     uint64_t budget_bytes; /* frontier memory cap (0 = 3/4 of free HBM at call time)  */
     int count_only;        /* 1: the last phase only counts (no final rows kept)      */
-    int reserved;
+    int profile;           /* 1: time every kernel with CUDA events (gva_result_kernel_stats) */
 } gva_match_opts;
+
+/* Per-kernel totals of one profiled gva_match: launches, summed CUDA-event
+ * milliseconds, and algorithmic bytes (the minimum traffic the kernel's
+ * arithmetic needs: rows read and written, one 8-byte segment lookup per
+ * row and pair, one 4-byte neighbour read per produced row). */
+typedef struct gva_kernel_stat {
+    char name[24];
+    uint64_t launches;
+    double ms;
+    double bytes;
+} gva_kernel_stat;
 
 /* ---- status -------------------------------------------------------------- */
 const char* gva_last_error(void);
 const char* gva_status_string(int status);
 const char* gva_version(void);
+/* Kernels this library has launched in this process (all devices). */
+uint64_t gva_kernel_launches(void);
 
 /* ---- L1: database ---------------------------------------------------------
  * Replaces loadDataBase(mygraph, metadata) (src/loadDataBase.cpp:309-365,
@@ -127,7 +140,40 @@ int gva_result_copy_rows(const gva_result* res, uint32_t* host_dst, uint64_t fir
 int gva_result_write_text(const gva_result* res, const char* path);
 /* GPU time of the phase loop, from CUDA events on opts->stream */
 double gva_result_gpu_ms(const gva_result* res);
+/* Filled when opts->profile was set; returns the number of kernel kinds. */
+int gva_result_kernel_stats(const gva_result* res, gva_kernel_stat* out, int cap);
 void gva_result_free(gva_result* res);
+
+/* ---- batched form ----------------------------------------------------------
+ * Many plans in shared rounds: each round advances every (plan, frontier
+ * slice) task by one step with one count, scan, totals and one persistent
+ * write launch fed by a device work queue; a task whose output exceeds
+ * budget_bytes is split.  Replaces running the gpumine driver once per query
+ * (src/gpumine.cpp:866-1072).  Results are counts: the final step of every
+ * plan only counts. */
+typedef struct gva_batch_opts {
+    void* stream;          /* cudaStream_t; NULL = legacy default stream            */
+    uint64_t budget_bytes; /* frontier memory cap (0 = 3/4 of free HBM)            */
+    int profile;           /* 1: per-kernel CUDA-event timing in stats->kernels     */
+    int reserved;
+} gva_batch_opts;
+
+typedef struct gva_batch_stats {
+    double gpu_ms;
+    uint64_t rounds, splits, launches;
+    gva_kernel_stat kernels[5];
+} gva_batch_stats;
+
+/* Declares the database a union of graphs: graph g owns vertex ids
+ * [first[g], first[g+1]) (num_graphs + 1 entries).  Needed for per-graph
+ * counts and supports. */
+int gva_db_set_graphs(gva_db* db, const uint64_t* first, uint32_t num_graphs);
+
+/* counts[nplans]: embeddings per plan.  graph_counts[nplans * num_graphs]
+ * (optional): embeddings per (plan, graph).  graph_support[nplans]
+ * (optional): graphs holding at least one embedding. */
+int gva_batch_count(gva_db* db, const gva_plan* const* plans, int nplans, const gva_batch_opts* opts,
+                    uint64_t* counts, uint64_t* graph_counts, uint32_t* graph_support, gva_batch_stats* stats);
 
 /* ---- L4: one phase step on caller-owned device buffers ----------------------
  * Replaces the kernel launchers of include/miningPattern.h:1-30

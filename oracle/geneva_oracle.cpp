@@ -611,9 +611,15 @@ struct Planner {
 };
 
 // ---------------------------------------------------------------- matcher --
+struct CapExceeded {};
+
 struct Matcher {
     const oracle_graph& g;
     Planner& P;
+    uint64_t cap_words = 0;  // 0 = unlimited; else abort when a frontier grows past it
+    void check(const std::vector<uint>& out) const {
+        if (cap_words && out.size() > cap_words) throw CapExceeded();
+    }
     std::map<uint, uint> pos;               // posOfVisitedV
     std::map<uint, std::vector<uint>> eq;   // equalPos
     std::vector<uint> cur;                  // current frontier, row-major
@@ -677,6 +683,7 @@ struct Matcher {
                         if (r12 && x < y) continue;
                         out.push_back(v); out.push_back(x); out.push_back(y);
                     }
+                check(out);
             }
             width = 3;
         }
@@ -709,6 +716,7 @@ struct Matcher {
                     out.insert(out.end(), row, row + pre);
                     out.push_back(u);
                 }
+                check(out);
             }
             width = pre + 1;
         } else {
@@ -744,6 +752,7 @@ struct Matcher {
                         out.push_back(x);
                         out.push_back(y);
                     }
+                    check(out);
                 }
             }
             width = pre + 2;
@@ -844,10 +853,20 @@ int oracle_match(const oracle_graph* g, const char* text, uint32_t** rows, uint6
 }
 
 int oracle_count(const oracle_graph* g, const char* text, uint64_t* nrows) {
+    return oracle_count_capped(g, text, 0, nrows);
+}
+
+int oracle_count_capped(const oracle_graph* g, const char* text, uint64_t cap_rows, uint64_t* nrows) {
     Planner p;
     if (!p.plan(text)) return fail("planner failed");
     Matcher m(*g, p);
-    m.run();
+    m.cap_words = cap_rows * 32;
+    try {
+        m.run();
+    } catch (const CapExceeded&) {
+        *nrows = 0;
+        return 2;
+    }
     *nrows = m.width ? m.cur.size() / m.width : 0;
     return 0;
 }

@@ -37,6 +37,8 @@ int oracle_match(const oracle_graph* g, const char* query_text, uint32_t** rows,
                  uint64_t* phase_rows, int cap, int* nphases);
 /* Counts only (no rows kept after the last phase). */
 int oracle_count(const oracle_graph* g, const char* query_text, uint64_t* nrows);
+/* Same, giving up (returns 2) once any frontier holds about cap_rows rows. */
+int oracle_count_capped(const oracle_graph* g, const char* query_text, uint64_t cap_rows, uint64_t* nrows);
 void oracle_free(void* p);
 const char* oracle_last_error(void);
 

@@ -46,6 +46,7 @@ class Oracle:
         lib.oracle_match.argtypes = [vp, ctypes.c_char_p, P(P(u32)), P(u64), P(ctypes.c_int), P(u64),
                                      ctypes.c_int, P(ctypes.c_int)]
         lib.oracle_count.argtypes = [vp, ctypes.c_char_p, P(u64)]
+        lib.oracle_count_capped.argtypes = [vp, ctypes.c_char_p, u64, P(u64)]
         lib.oracle_free.argtypes = [vp]
         lib.oracle_last_error.restype = ctypes.c_char_p
         self.lib = lib
@@ -90,8 +91,12 @@ class Oracle:
         self.lib.oracle_free(ctypes.cast(rows_p, ctypes.c_void_p))
         return arr, [int(x) for x in ph[:nph.value]]
 
-    def count(self, g, query_text: str) -> int:
+    def count(self, g, query_text: str, cap_rows: int = 0):
+        """Embedding count, or None when a frontier passes about cap_rows rows."""
         n = ctypes.c_uint64()
-        if self.lib.oracle_count(g, query_text.encode(), ctypes.byref(n)):
+        st = self.lib.oracle_count_capped(g, query_text.encode(), cap_rows, ctypes.byref(n))
+        if st == 2:
+            return None
+        if st:
             raise RuntimeError(self.lib.oracle_last_error().decode())
         return int(n.value)

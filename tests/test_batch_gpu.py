@@ -1,0 +1,81 @@
+"""Batched engine (gva_batch_count) against the plain path and the oracle."""
+import random
+
+import numpy as np
+import pytest
+
+import geneva_b200 as gv
+from geneva_b200 import workloads
+from querygen import random_query
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def small_db(native, oracle):
+    db = workloads.graph_database(300, 10, 30, 3.0, 4, None, 2, seed=77, name="small")
+    gdb = gv.Database.from_edges(db.vlabels, db.src, db.dst, db.elabels)
+    gdb.set_graphs(db.first)
+    og = oracle.from_edges(db.vlabels, db.src, db.dst, db.elabels)
+    yield db, gdb, og
+    oracle.free(og)
+    gdb.close()
+
+
+def _patterns(db, n, seed):
+    pats = workloads.sample_patterns(db, n, 3, 6, seed=seed)
+    rng = random.Random(seed)
+    pats += [random_query(rng) for _ in range(n // 4)]
+    return pats
+
+
+def test_batch_counts_match_plain_and_oracle(small_db, oracle):
+    db, gdb, og = small_db
+    pats = [p for p in _patterns(db, 80, 5) if oracle.count(og, p, cap_rows=1_000_000) is not None]
+    plans = [gv.Plan.from_text(p) for p in pats]
+    counts, _, stats = gv.batch_count(gdb, plans)
+    assert stats["rounds"] >= 2
+    for p, plan, c in zip(pats, plans, counts):
+        assert int(c) == oracle.count(og, p), p
+        assert int(c) == gv.match(gdb, plan, count_only=True).num_rows, p
+    # single-vertex plans give the same counts
+    sv = [gv.Plan.from_text(p, gv.MODE_SV) for p in pats]
+    counts_sv, _, _ = gv.batch_count(gdb, sv)
+    assert np.array_equal(counts, counts_sv)
+
+
+def test_per_graph_counts_and_support(small_db, oracle):
+    db, gdb, og = small_db
+    pats = [p for p in _patterns(db, 40, 9) if oracle.count(og, p, cap_rows=500_000) is not None]
+    plans = [gv.Plan.from_text(p) for p in pats]
+    counts, (gc, sup), _ = gv.batch_count(gdb, plans, graph_counts=True, support=True)
+    G = len(db.first) - 1
+    assert gc.shape == (len(pats), G)
+    for i, p in enumerate(pats):
+        rows, _ = oracle.match(og, p)
+        g = db.graph_of(rows[:, 0].astype(np.int64)) if rows.size else np.zeros(0, dtype=np.int64)
+        want = np.bincount(g, minlength=G).astype(np.uint64)
+        assert np.array_equal(gc[i], want), p
+        assert int(sup[i]) == int((want > 0).sum()), p
+        assert int(counts[i]) == int(want.sum())
+
+
+def test_small_budget_splits_tasks(small_db, oracle):
+    db, gdb, og = small_db
+    pats = [p for p in _patterns(db, 30, 13) if oracle.count(og, p, cap_rows=500_000) is not None]
+    plans = [gv.Plan.from_text(p) for p in pats]
+    full, _, s_full = gv.batch_count(gdb, plans)
+    tiny, _, s_tiny = gv.batch_count(gdb, plans, budget_bytes=64 << 10)
+    assert np.array_equal(full, tiny)
+    assert s_tiny["splits"] > 0 and s_tiny["rounds"] > s_full["rounds"]
+
+
+def test_enron_batch(native, enron_dir):
+    db = gv.loadDataBase(enron_dir / "Enron.mygraph", enron_dir / "Enron.metadata")
+    q = (enron_dir / "Enron_4_6_0.query").read_text()
+    plans = [gv.Plan.from_text(q), gv.Plan.from_text(q, gv.MODE_SV), gv.Plan.from_text("v 0 1\nv 1 9\ne 0 1 1\n")]
+    counts, _, _ = gv.batch_count(db, plans)
+    assert counts.tolist() == [157502, 157502, 0]
+    with pytest.raises(gv.GenevaError):
+        gv.batch_count(db, plans, support=True)  # no graph ids declared
+    db.close()
