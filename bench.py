@@ -342,7 +342,7 @@ def main():
                          "frac": achieved / peak, "peak_source": peak_kind, "traffic": traffic,
                          "launches": s["launches"], "kernel_ms": s["ms"]},
             "kernels": kstats,
-            "batch": {k: pstats[k] for k in ("rounds", "splits", "launches")},
+            "batch": {k: pstats[k] for k in ("rounds", "splits", "launches", "trie_nodes")},
             "e2e": {"value": e2e_value, "unit": "embeddings/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h,
                     "note": "pattern text planned on the host each step; counts and supports copied to host"},

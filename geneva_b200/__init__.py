@@ -67,7 +67,7 @@ class _BatchOpts(ctypes.Structure):
 
 class _BatchStats(ctypes.Structure):
     _fields_ = [("gpu_ms", ctypes.c_double), ("rounds", ctypes.c_uint64), ("splits", ctypes.c_uint64),
-                ("launches", ctypes.c_uint64), ("kernels", _KernelStat * 5)]
+                ("launches", ctypes.c_uint64), ("trie_nodes", ctypes.c_uint64), ("kernels", _KernelStat * 5)]
 
 
 def _declare(lib):
@@ -333,6 +333,7 @@ def batch_count(db: Database, plans: Sequence[Plan], stream: Optional[int] = Non
                                      gc.ctypes.data if gc is not None else None,
                                      sup.ctypes.data if sup is not None else None, ctypes.byref(st)))
     stats = {"gpu_ms": st.gpu_ms, "rounds": int(st.rounds), "splits": int(st.splits), "launches": int(st.launches),
+             "trie_nodes": int(st.trie_nodes),
              "kernels": {st.kernels[i].name.decode(): dict(launches=int(st.kernels[i].launches),
                                                            ms=float(st.kernels[i].ms), bytes=float(st.kernels[i].bytes))
                          for i in range(5)}}

@@ -22,6 +22,7 @@
 #include <atomic>
 #include <cstring>
 #include <memory>
+#include <map>
 #include <numeric>
 #include <string>
 #include <vector>
@@ -41,7 +42,9 @@ namespace {
             return fail(GVA_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_));              \
     } while (0)
 
-enum TaskMode : uint32_t { MODE_WRITE = 0, MODE_COUNT = 1, MODE_COUNT_GRAPHS = 2 };
+// WRITE: output feeds child steps; COUNT: a plan ends here; *_GRAPHS: it also
+// needs per-graph accounting (slot `query`).
+enum TaskMode : uint32_t { MODE_WRITE = 0, MODE_COUNT = 1, MODE_COUNT_GRAPHS = 2, MODE_WRITE_AND_GRAPHS = 3 };
 
 struct TaskDesc {
     uint32_t kind;     // STEP_EXT / STEP_REDUCE
@@ -126,7 +129,7 @@ batch_count_kernel(const TaskDesc* __restrict__ tasks, const uint64_t* __restric
             first = row[0];
         }
     }
-    if (d.mode == MODE_COUNT_GRAPHS) add_graph_count(ctx, d.query, first, c, valid);
+    if (d.mode == MODE_COUNT_GRAPHS || d.mode == MODE_WRITE_AND_GRAPHS) add_graph_count(ctx, d.query, first, c, valid);
     store_block_sum(c, block_sums);
 }
 
@@ -281,33 +284,73 @@ struct DevBuf {
     }
 };
 
+// A node of the step trie: the plans of a batch that agree on their first
+// steps share those steps' frontiers.
+struct Node {
+    Step step;
+    int depth = 0;
+    std::vector<int> children;
+    std::vector<int> terminal;  // plans whose last step is this node
+};
+
 struct Task {
-    int q;                       // query index
-    int step;                    // next step to run
+    int node;
     const uint32_t* in;          // frontier slice
     uint64_t rows;
     std::shared_ptr<DevBuf> owner;
+};
+
+// Bytes that determine a step's output from its input (everything but phase_end).
+std::string step_key(const Step& st) {
+    std::string k;
+    auto put = [&](const void* p, size_t n) { k.append((const char*)p, n); };
+    put(&st.kind, sizeof st.kind);
+    put(&st.width_in, 4);
+    put(&st.part, 4);
+    put(&st.label, 4);
+    put(&st.always_empty, 4);
+    if (st.kind == STEP_EXT) {
+        put(&st.src_col, 4);
+        put(&st.bound_col, 4);
+        put(&st.bound_inclusive, 4);
+        put(&st.n_eq, 4);
+        put(st.eq_cols, st.n_eq);
+    } else if (st.kind == STEP_REDUCE) {
+        put(&st.n_pairs, 4);
+        put(st.rs_col, st.n_pairs);
+        put(st.re_col, st.n_pairs);
+        put(st.re_label, 4 * st.n_pairs);
+    }
+    return k;
+}
+
+// Pinned host staging reused across rounds and calls (per thread and device).
+struct Staging {
+    char* p = nullptr;
+    size_t cap = 0;
+    char* get(size_t need) {
+        if (need > cap) {
+            if (p) cudaFreeHost(p);
+            cap = std::max(need, cap * 2);
+            if (cudaMallocHost((void**)&p, cap) != cudaSuccess) {
+                p = nullptr;
+                cap = 0;
+            }
+        }
+        return p;
+    }
 };
 
 }  // namespace
 
 uint64_t batch_kernel_launches() { return g_batch_launches.load(); }
 
-struct BatchRun {
-    DevDB& db;
-    const std::vector<std::vector<Step>>& steps;
-    cudaStream_t s;
-    uint64_t budget;
-    BatchCtx ctx{};
-    Profiler* prof;
-    BatchStats* stats;
-};
-
 int run_batch(DevDB& db, const std::vector<std::vector<Step>>& steps, cudaStream_t s, uint64_t budget,
               const uint32_t* vgraph, uint32_t G, uint64_t* counts, uint64_t* graph_counts_host,
               uint32_t* support_host, bool profile, BatchStats* stats) {
     GVA_CUDA_B(cudaSetDevice(db.device));
     const int nq = (int)steps.size();
+    for (int q = 0; q < nq; ++q) counts[q] = 0;
     if (nq == 0) return GVA_OK;
     if ((graph_counts_host || support_host) && (!vgraph || G == 0))
         return fail(GVA_ERR_ARG, "per-graph results need the database's graph ids (gva_db_set_graphs)");
@@ -318,21 +361,53 @@ int run_batch(DevDB& db, const std::vector<std::vector<Step>>& steps, cudaStream
     }
     Profiler profiler;
     Profiler* prof = profile ? &profiler : nullptr;
-    cudaEvent_t ev0, ev1;
-    GVA_CUDA_B(cudaEventCreate(&ev0));
-    GVA_CUDA_B(cudaEventCreate(&ev1));
+    static thread_local cudaEvent_t tev[64][2];
+    const int dev = db.device;
+    if (dev < 0 || dev >= 64) return fail(GVA_ERR_ARG, "device index out of range");
+    if (!tev[dev][0]) {
+        GVA_CUDA_B(cudaEventCreate(&tev[dev][0]));
+        GVA_CUDA_B(cudaEventCreate(&tev[dev][1]));
+    }
+    cudaEvent_t ev0 = tev[dev][0], ev1 = tev[dev][1];
     GVA_CUDA_B(cudaEventRecord(ev0, s));
 
-    // per-graph accumulators
+    // ---- step trie: plans sharing a prefix of steps share its frontiers
+    std::vector<Node> nodes;
+    std::map<std::string, int> roots;
+    std::vector<std::map<std::string, int>> kids;
+    for (int q = 0; q < nq; ++q) {
+        const std::vector<Step>& st = steps[q];
+        if (st.size() < 2 || st[0].kind != STEP_SEED) return fail(GVA_ERR_ARG, "plan must start with a seed step");
+        int cur = -1;
+        for (size_t i = 0; i < st.size(); ++i) {
+            const std::string key = step_key(st[i]);
+            std::map<std::string, int>& m = cur < 0 ? roots : kids[cur];
+            auto it = m.find(key);
+            int id;
+            if (it == m.end()) {
+                id = (int)nodes.size();
+                nodes.push_back(Node{st[i], (int)i, {}, {}});
+                kids.emplace_back();
+                m[key] = id;
+                if (cur >= 0) nodes[cur].children.push_back(id);
+            } else {
+                id = it->second;
+            }
+            cur = id;
+        }
+        nodes[cur].terminal.push_back(q);
+    }
+
+    // per-graph accumulators: one slot per plan; plans that end on the same
+    // node are filled from its first plan at the end
     BatchCtx ctx{};
     ctx.vgraph = vgraph;
     ctx.G = G;
     ctx.words = (G + 31) / 32;
     const bool per_graph = graph_counts_host || support_host;
     void* acc = nullptr;
-    size_t acc_bytes = 0;
     if (per_graph) {
-        acc_bytes = (graph_counts_host ? (size_t)nq * G * 8 : 0) + (size_t)nq * ctx.words * 4;
+        const size_t acc_bytes = (graph_counts_host ? (size_t)nq * G * 8 : 0) + (size_t)nq * ctx.words * 4;
         if (cudaMallocAsync(&acc, acc_bytes, s) != cudaSuccess) return fail(GVA_ERR_NOMEM, "per-graph counters");
         GVA_CUDA_B(cudaMemsetAsync(acc, 0, acc_bytes, s));
         char* a = (char*)acc;
@@ -342,40 +417,27 @@ int run_batch(DevDB& db, const std::vector<std::vector<Step>>& steps, cudaStream
         }
         ctx.graph_bits = (uint32_t*)a;
     }
-    for (int q = 0; q < nq; ++q) counts[q] = 0;
 
-    // seed tasks
     std::vector<Task> active;
-    for (int q = 0; q < nq; ++q) {
-        const std::vector<Step>& st = steps[q];
-        if (st.empty() || st[0].kind != STEP_SEED) return fail(GVA_ERR_ARG, "plan must start with a seed step");
-        if (st[0].always_empty) continue;
-        const uint64_t n = db.seed_off[st[0].label + 1] - db.seed_off[st[0].label];
-        if (n) active.push_back({q, 1, db.seed_verts + db.seed_off[st[0].label], n, nullptr});
+    for (auto& kv : roots) {
+        const Node& seed = nodes[kv.second];
+        if (seed.step.always_empty) continue;
+        const uint64_t n = db.seed_off[seed.step.label + 1] - db.seed_off[seed.step.label];
+        if (!n) continue;
+        for (int c : seed.children) active.push_back({c, db.seed_verts + db.seed_off[seed.step.label], n, nullptr});
     }
 
     int status = GVA_OK;
-    std::vector<TaskDesc> descs;
-    std::vector<uint64_t> block0;
-    std::vector<uint64_t> totals;
-    std::vector<uint32_t*> outs;
+    static thread_local Staging staging[64];
+    Staging& stg = staging[dev];
     TaskDesc* d_desc = nullptr;
     size_t desc_cap = 0;
-    uint64_t* d_block0 = nullptr;
-    size_t block0_cap = 0;
     uint64_t* d_sums = nullptr;
     size_t sums_cap = 0;
-    uint64_t* d_totals = nullptr;
-    size_t totals_cap = 0;
-    uint32_t** d_outs = nullptr;
-    size_t outs_cap = 0;
-    unsigned long long* d_queue = nullptr;
-    uint64_t* h_pinned = nullptr;
-    size_t pinned_cap = 0;
-    GVA_CUDA_B(cudaMallocAsync((void**)&d_queue, 8, s));
+    uint64_t* d_small = nullptr;  // block0[nt + 1] | totals[nt] | outs[nt] | queue
+    size_t small_cap = 0;
     static bool smem_set[64] = {};
-    int dev = db.device;
-    if (dev < 64 && !smem_set[dev]) {
+    if (!smem_set[dev]) {
         GVA_CUDA_B(cudaFuncSetAttribute(batch_write_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                         (int)batch_smem_bytes()));
         smem_set[dev] = true;
@@ -397,26 +459,43 @@ int run_batch(DevDB& db, const std::vector<std::vector<Step>>& steps, cudaStream
     };
 
     uint64_t rounds = 0, splits = 0, launches = 0;
+    std::vector<uint64_t> block0, totals;
     while (!active.empty() && status == GVA_OK) {
         // steps that cannot match (label or partition absent) end their task
         active.erase(std::remove_if(active.begin(), active.end(),
-                                    [&](const Task& t) { return steps[t.q][t.step].always_empty != 0; }),
+                                    [&](const Task& t) { return nodes[t.node].step.always_empty != 0; }),
                      active.end());
         if (active.empty()) break;
         ++rounds;
         const int nt = (int)active.size();
-        descs.assign(nt, TaskDesc{});
+        // pinned staging: descs | block0 | totals | outs
+        const size_t desc_bytes = (size_t)nt * sizeof(TaskDesc);
+        const size_t small_words = (size_t)(nt + 1) + nt + nt + 1;
+        char* h = stg.get(desc_bytes + small_words * 8);
+        if (!h) {
+            status = fail(GVA_ERR_NOMEM, "pinned staging allocation failed");
+            break;
+        }
+        TaskDesc* descs = (TaskDesc*)h;
+        uint64_t* h_block0 = (uint64_t*)(h + desc_bytes);
+        uint64_t* h_totals = h_block0 + (nt + 1);
+        uint32_t** h_outs = (uint32_t**)(h_totals + nt);
         block0.assign(nt + 1, 0);
         uint32_t kmax = 1, eqmax = 0;
+        double cbytes = 0;
         for (int t = 0; t < nt; ++t) {
             const Task& tk = active[t];
-            const Step& st = steps[tk.q][tk.step];
-            const bool last = tk.step + 1 == (int)steps[tk.q].size();
+            const Node& nd = nodes[tk.node];
+            const Step& st = nd.step;
             TaskDesc& d = descs[t];
             memset(&d, 0, sizeof d);
             d.kind = st.kind;
-            d.query = (uint32_t)tk.q;
-            d.mode = last ? (per_graph ? MODE_COUNT_GRAPHS : MODE_COUNT) : MODE_WRITE;
+            d.mode = MODE_WRITE;
+            if (nd.children.empty()) d.mode = MODE_COUNT;
+            if (per_graph && !nd.terminal.empty()) {
+                d.mode = nd.children.empty() ? MODE_COUNT_GRAPHS : MODE_WRITE_AND_GRAPHS;
+                d.query = (uint32_t)nd.terminal[0];
+            }
             d.block0 = block0[t];
             const DevPart& P = db.parts[st.part - 1];
             if (st.kind == STEP_EXT) {
@@ -451,38 +530,27 @@ int run_batch(DevDB& db, const std::vector<std::vector<Step>>& steps, cudaStream
             }
             kmax = std::max(kmax, st.width_in);
             block0[t + 1] = block0[t] + (tk.rows + kRowsPerBlock - 1) / kRowsPerBlock;
+            cbytes += (4.0 * st.width_in + 8.0 * (st.kind == STEP_EXT ? 1 : st.n_pairs)) * (double)tk.rows;
         }
         const uint64_t nb = block0[nt];
         if (nb > 0x7fffffffull) {
             status = fail(GVA_ERR_UNSUPPORTED, "round too large for one launch");
             break;
         }
-        if (!grow((void**)&d_desc, desc_cap, nt * sizeof(TaskDesc)) ||
-            !grow((void**)&d_block0, block0_cap, (nt + 1) * sizeof(uint64_t)) ||
-            !grow((void**)&d_sums, sums_cap, (nb + 1) * sizeof(uint64_t)) ||
-            !grow((void**)&d_totals, totals_cap, nt * sizeof(uint64_t)) ||
-            !grow((void**)&d_outs, outs_cap, nt * sizeof(uint32_t*))) {
+        std::copy(block0.begin(), block0.end(), h_block0);
+        if (!grow((void**)&d_desc, desc_cap, desc_bytes) || !grow((void**)&d_sums, sums_cap, (nb + 1) * 8) ||
+            !grow((void**)&d_small, small_cap, small_words * 8)) {
             status = fail(GVA_ERR_NOMEM, "batch bookkeeping allocation failed");
             break;
         }
-        if (pinned_cap < (size_t)nt) {
-            if (h_pinned) cudaFreeHost(h_pinned);
-            pinned_cap = std::max<size_t>(nt, pinned_cap * 2);
-            if (cudaMallocHost(&h_pinned, pinned_cap * 8) != cudaSuccess) {
-                status = fail(GVA_ERR_NOMEM, "pinned host allocation failed");
-                h_pinned = nullptr;
-                break;
-            }
-        }
-        GVA_CUDA_B(cudaMemcpyAsync(d_desc, descs.data(), nt * sizeof(TaskDesc), cudaMemcpyHostToDevice, s));
-        GVA_CUDA_B(cudaMemcpyAsync(d_block0, block0.data(), (nt + 1) * sizeof(uint64_t), cudaMemcpyHostToDevice, s));
+        uint64_t* d_block0 = d_small;
+        uint64_t* d_totals = d_block0 + (nt + 1);
+        uint32_t** d_outs = (uint32_t**)(d_totals + nt);
+        unsigned long long* d_queue = (unsigned long long*)(d_totals + 2 * nt);
+        GVA_CUDA_B(cudaMemcpyAsync(d_desc, descs, desc_bytes, cudaMemcpyHostToDevice, s));
+        GVA_CUDA_B(cudaMemcpyAsync(d_block0, h_block0, (nt + 1) * 8, cudaMemcpyHostToDevice, s));
 
         cudaEvent_t ev = nullptr;
-        double cbytes = 0;
-        for (int t = 0; t < nt; ++t) {
-            const Step& st = steps[active[t].q][active[t].step];
-            cbytes += (4.0 * st.width_in + 8.0 * (st.kind == STEP_EXT ? 1 : st.n_pairs)) * (double)active[t].rows;
-        }
         if (prof) prof->begin(K_EXT_COUNT, cbytes, s, ev);
         batch_count_kernel<<<(unsigned)nb, kThreads, 0, s>>>(d_desc, d_block0, nt, d_sums, ctx);
         if (prof) prof->end(ev, K_EXT_COUNT, cbytes, s);
@@ -492,29 +560,25 @@ int run_batch(DevDB& db, const std::vector<std::vector<Step>>& steps, cudaStream
         task_totals_kernel<<<(nt + 255) / 256, 256, 0, s>>>(d_block0, nt, d_sums, d_totals);
         launches += 3;
         GVA_CUDA_B(cudaGetLastError());
-        GVA_CUDA_B(cudaMemcpyAsync(h_pinned, d_totals, nt * sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
+        GVA_CUDA_B(cudaMemcpyAsync(h_totals, d_totals, nt * 8, cudaMemcpyDeviceToHost, s));
         GVA_CUDA_B(cudaStreamSynchronize(s));
-        totals.assign(h_pinned, h_pinned + nt);
+        totals.assign(h_totals, h_totals + nt);
 
         // choose which tasks write this round: deepest first, within the budget
         std::vector<int> order;
-        outs.assign(nt, nullptr);
         std::vector<Task> next;
         for (int t = 0; t < nt; ++t) {
-            const Task& tk = active[t];
-            const bool last = tk.step + 1 == (int)steps[tk.q].size();
-            if (last) {
-                counts[tk.q] += totals[t];
-            } else if (totals[t] > 0) {
-                order.push_back(t);
-            }
+            const Node& nd = nodes[active[t].node];
+            for (int q : nd.terminal) counts[q] += totals[t];
+            if (!nd.children.empty() && totals[t] > 0) order.push_back(t);
         }
-        std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return active[a].step > active[b].step; });
+        std::stable_sort(order.begin(), order.end(),
+                         [&](int a, int b) { return nodes[active[a].node].depth > nodes[active[b].node].depth; });
         uint64_t used = 0;
         std::vector<uint64_t> off_words(nt, 0);
         std::vector<int> chosen;
         for (int t : order) {
-            const Step& st = steps[active[t].q][active[t].step];
+            const Step& st = nodes[active[t].node].step;
             const uint32_t w = st.kind == STEP_EXT ? st.width_in + 1 : st.width_in;
             const uint64_t bytes = totals[t] * w * 4ull;
             if (used + bytes <= budget) {
@@ -522,16 +586,15 @@ int run_batch(DevDB& db, const std::vector<std::vector<Step>>& steps, cudaStream
                 used += (bytes + 15) & ~15ull;
                 chosen.push_back(t);
             } else if (bytes > budget) {
-                // split the task's input rows and retry both halves next round
+                // split the task's input rows; both halves retry next round
                 Task a = active[t], b = active[t];
                 const uint64_t half = a.rows / 2;
                 if (half == 0) {
                     status = fail(GVA_ERR_NOMEM, "a single frontier row expands beyond the memory budget");
                     break;
                 }
-                const uint32_t win = st.width_in;
                 a.rows = half;
-                b.in = a.in + half * win;
+                b.in = a.in + half * st.width_in;
                 b.rows = active[t].rows - half;
                 next.push_back(a);
                 next.push_back(b);
@@ -551,14 +614,15 @@ int run_batch(DevDB& db, const std::vector<std::vector<Step>>& steps, cudaStream
                 break;
             }
             double wbytes = 0;
+            for (int t = 0; t < nt; ++t) h_outs[t] = nullptr;
             for (int t : chosen) {
-                outs[t] = (uint32_t*)buf->p + off_words[t];
-                const Step& st = steps[active[t].q][active[t].step];
+                h_outs[t] = (uint32_t*)buf->p + off_words[t];
+                const Step& st = nodes[active[t].node].step;
                 const double k = st.width_in;
                 wbytes += (4.0 * k + 8.0) * (double)active[t].rows +
                           (st.kind == STEP_EXT ? (4.0 + 4.0 * (k + 1)) : 4.0 * k) * (double)totals[t];
             }
-            GVA_CUDA_B(cudaMemcpyAsync(d_outs, outs.data(), nt * sizeof(uint32_t*), cudaMemcpyHostToDevice, s));
+            GVA_CUDA_B(cudaMemcpyAsync(d_outs, h_outs, nt * sizeof(uint32_t*), cudaMemcpyHostToDevice, s));
             GVA_CUDA_B(cudaMemsetAsync(d_queue, 0, 8, s));
             const size_t smem = batch_smem_bytes_for(kmax, std::max(eqmax, 1u));
             int per_sm = 1;
@@ -571,14 +635,8 @@ int run_batch(DevDB& db, const std::vector<std::vector<Step>>& steps, cudaStream
             launches += 1;
             GVA_CUDA_B(cudaGetLastError());
         }
-        for (int t : chosen) {
-            Task nt2 = active[t];
-            nt2.in = outs[t];
-            nt2.rows = totals[t];
-            nt2.step += 1;
-            nt2.owner = buf;
-            next.push_back(nt2);
-        }
+        for (int t : chosen)
+            for (int c : nodes[active[t].node].children) next.push_back({c, h_outs[t], totals[t], buf});
         active.swap(next);
         if (prof) {
             GVA_CUDA_B(cudaStreamSynchronize(s));
@@ -589,12 +647,22 @@ int run_batch(DevDB& db, const std::vector<std::vector<Step>>& steps, cudaStream
     active.clear();  // releases frontier buffers (stream-ordered)
 
     if (status == GVA_OK && per_graph) {
+        std::vector<uint32_t> bits((size_t)nq * ctx.words);
+        GVA_CUDA_B(cudaMemcpyAsync(bits.data(), ctx.graph_bits, bits.size() * 4, cudaMemcpyDeviceToHost, s));
         if (graph_counts_host)
             GVA_CUDA_B(cudaMemcpyAsync(graph_counts_host, ctx.graph_counts, (size_t)nq * G * 8, cudaMemcpyDeviceToHost, s));
+        GVA_CUDA_B(cudaStreamSynchronize(s));
+        for (const Node& nd : nodes) {  // identical plans share the first one's results
+            for (size_t i = 1; i < nd.terminal.size(); ++i) {
+                const int q0 = nd.terminal[0], q = nd.terminal[i];
+                std::copy(bits.begin() + (size_t)q0 * ctx.words, bits.begin() + (size_t)(q0 + 1) * ctx.words,
+                          bits.begin() + (size_t)q * ctx.words);
+                if (graph_counts_host)
+                    std::copy(graph_counts_host + (size_t)q0 * G, graph_counts_host + (size_t)(q0 + 1) * G,
+                              graph_counts_host + (size_t)q * G);
+            }
+        }
         if (support_host) {
-            std::vector<uint32_t> bits((size_t)nq * ctx.words);
-            GVA_CUDA_B(cudaMemcpyAsync(bits.data(), ctx.graph_bits, bits.size() * 4, cudaMemcpyDeviceToHost, s));
-            GVA_CUDA_B(cudaStreamSynchronize(s));
             for (int q = 0; q < nq; ++q) {
                 uint32_t c = 0;
                 for (uint32_t w = 0; w < ctx.words; ++w) c += (uint32_t)__builtin_popcount(bits[(size_t)q * ctx.words + w]);
@@ -603,23 +671,18 @@ int run_batch(DevDB& db, const std::vector<std::vector<Step>>& steps, cudaStream
         }
     }
     if (acc) cudaFreeAsync(acc, s);
-    for (void* p : {(void*)d_desc, (void*)d_block0, (void*)d_sums, (void*)d_totals, (void*)d_outs, (void*)d_queue})
+    for (void* p : {(void*)d_desc, (void*)d_sums, (void*)d_small})
         if (p) cudaFreeAsync(p, s);
-    if (h_pinned) {
-        cudaStreamSynchronize(s);
-        cudaFreeHost(h_pinned);
-    }
     cudaEventRecord(ev1, s);
     cudaEventSynchronize(ev1);
     float ms = 0.f;
     cudaEventElapsedTime(&ms, ev0, ev1);
-    cudaEventDestroy(ev0);
-    cudaEventDestroy(ev1);
     if (stats) {
         stats->gpu_ms = ms;
         stats->rounds = rounds;
         stats->splits = splits;
         stats->launches = launches;
+        stats->nodes = nodes.size();
         if (prof) {
             prof->resolve();
             for (int i = 0; i < K_NUM; ++i) stats->kstat[i] = prof->stat[i];

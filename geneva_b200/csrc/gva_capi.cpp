@@ -311,6 +311,7 @@ int gva_batch_count(gva_db* db, const gva_plan* const* plans, int nplans, const 
         stats->rounds = bs.rounds;
         stats->splits = bs.splits;
         stats->launches = bs.launches;
+        stats->trie_nodes = bs.nodes;
         for (int i = 0; i < K_NUM && i < 5; ++i) {
             strncpy(stats->kernels[i].name, kKernelNames[i], sizeof stats->kernels[i].name - 1);
             stats->kernels[i].launches = bs.kstat[i].launches;

@@ -274,6 +274,27 @@ int launch_write(const DevDB& db, const Step& st, const uint32_t* in, uint64_t n
     return GVA_OK;
 }
 
+// Per-thread, per-device host staging reused by every query: a pinned word
+// for count read-backs and two timing events (creating these per call costs
+// more than a small query's kernels).
+struct HostStage {
+    uint64_t* pinned = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+};
+
+int host_stage(int device, HostStage*& out) {
+    static thread_local HostStage stages[64];
+    if (device < 0 || device >= 64) return fail(GVA_ERR_ARG, "device index out of range");
+    HostStage& h = stages[device];
+    if (!h.pinned) {
+        GVA_CUDA(cudaMallocHost(&h.pinned, 64));
+        GVA_CUDA(cudaEventCreate(&h.ev0));
+        GVA_CUDA(cudaEventCreate(&h.ev1));
+    }
+    out = &h;
+    return GVA_OK;
+}
+
 int ensure_pool(int device) {
     static bool done[64] = {};
     if (device < 64 && done[device]) return GVA_OK;
@@ -449,9 +470,10 @@ int run_match(DevDB& db, const Plan& plan, const std::vector<Step>& steps, cudaS
         GVA_CUDA(cudaMemGetInfo(&fr, &tot));
         budget = (uint64_t)fr / 4 * 3;
     }
-    cudaEvent_t ev0, ev1;
-    GVA_CUDA(cudaEventCreate(&ev0));
-    GVA_CUDA(cudaEventCreate(&ev1));
+    HostStage* hs = nullptr;
+    rc = host_stage(db.device, hs);
+    if (rc) return rc;
+    cudaEvent_t ev0 = hs->ev0, ev1 = hs->ev1;
     GVA_CUDA(cudaEventRecord(ev0, s));
 
     const uint32_t* cur = nullptr;
@@ -460,9 +482,8 @@ int run_match(DevDB& db, const Plan& plan, const std::vector<Step>& steps, cudaS
     uint32_t width = 0;
     uint64_t* sums = nullptr;
     size_t sums_bytes = 0;
-    uint64_t* total_h = nullptr;
-    cudaError_t ce = cudaMallocHost(&total_h, sizeof(uint64_t));
-    if (ce != cudaSuccess) return fail(GVA_ERR_NOMEM, "pinned host allocation failed");
+    uint64_t* total_h = hs->pinned;
+    cudaError_t ce = cudaSuccess;
     int status = GVA_OK;
     bool counted_only = false;
 
@@ -517,20 +538,15 @@ int run_match(DevDB& db, const Plan& plan, const std::vector<Step>& steps, cudaS
         if (rows == 0) break;
     }
     if (sums) cudaFreeAsync(sums, s);
-    cudaFreeHost(total_h);
     if (status) {
         if (owned) cudaFreeAsync(owned, s);
         if (prof) prof->resolve();
-        cudaEventDestroy(ev0);
-        cudaEventDestroy(ev1);
         return status;
     }
     GVA_CUDA(cudaEventRecord(ev1, s));
     GVA_CUDA(cudaEventSynchronize(ev1));
     float ms = 0.f;
     cudaEventElapsedTime(&ms, ev0, ev1);
-    cudaEventDestroy(ev0);
-    cudaEventDestroy(ev1);
     res.gpu_ms = ms;
     if (prof) {
         prof->resolve();

@@ -78,7 +78,7 @@ void free_result(MatchResult* r);
 
 struct BatchStats {
     double gpu_ms = 0.0;
-    uint64_t rounds = 0, splits = 0, launches = 0;
+    uint64_t rounds = 0, splits = 0, launches = 0, nodes = 0;
     KernelStat kstat[K_NUM];
 };
 

@@ -161,6 +161,7 @@ typedef struct gva_batch_opts {
 typedef struct gva_batch_stats {
     double gpu_ms;
     uint64_t rounds, splits, launches;
+    uint64_t trie_nodes; /* distinct step prefixes: plans sharing a prefix share its frontier */
     gva_kernel_stat kernels[5];
 } gva_batch_stats;
 

@@ -65,9 +65,23 @@ def test_small_budget_splits_tasks(small_db, oracle):
     pats = [p for p in _patterns(db, 30, 13) if oracle.count(og, p, cap_rows=500_000) is not None]
     plans = [gv.Plan.from_text(p) for p in pats]
     full, _, s_full = gv.batch_count(gdb, plans)
-    tiny, _, s_tiny = gv.batch_count(gdb, plans, budget_bytes=64 << 10)
+    tiny, _, s_tiny = gv.batch_count(gdb, plans, budget_bytes=2048)
     assert np.array_equal(full, tiny)
     assert s_tiny["splits"] > 0 and s_tiny["rounds"] > s_full["rounds"]
+
+
+def test_shared_prefixes_and_duplicates(small_db, oracle):
+    db, gdb, og = small_db
+    pats = [p for p in _patterns(db, 20, 21) if oracle.count(og, p, cap_rows=500_000) is not None]
+    plans = [gv.Plan.from_text(p) for p in pats] * 3  # every plan three times
+    counts, (gc, sup), stats = gv.batch_count(gdb, plans, graph_counts=True, support=True)
+    n = len(pats)
+    for i in range(n):
+        assert counts[i] == counts[i + n] == counts[i + 2 * n] == oracle.count(og, pats[i])
+        assert np.array_equal(gc[i], gc[i + 2 * n]) and sup[i] == sup[i + n]
+    single, _, s1 = gv.batch_count(gdb, plans[:n])
+    assert stats["trie_nodes"] == s1["trie_nodes"]  # duplicates add no work
+    assert np.array_equal(single, counts[:n])
 
 
 def test_enron_batch(native, enron_dir):
