@@ -381,14 +381,14 @@ int run_batch(DevDB& db, const std::vector<std::vector<Step>>& steps, cudaStream
         int cur = -1;
         for (size_t i = 0; i < st.size(); ++i) {
             const std::string key = step_key(st[i]);
-            std::map<std::string, int>& m = cur < 0 ? roots : kids[cur];
-            auto it = m.find(key);
+            auto& m0 = cur < 0 ? roots : kids[cur];
+            auto it = m0.find(key);
             int id;
-            if (it == m.end()) {
+            if (it == m0.end()) {
                 id = (int)nodes.size();
                 nodes.push_back(Node{st[i], (int)i, {}, {}});
-                kids.emplace_back();
-                m[key] = id;
+                kids.emplace_back();  // may reallocate: look the parent's map up again
+                (cur < 0 ? roots : kids[cur])[key] = id;
                 if (cur >= 0) nodes[cur].children.push_back(id);
             } else {
                 id = it->second;
