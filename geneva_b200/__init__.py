@@ -23,7 +23,7 @@ from typing import List, Optional, Sequence
 import numpy as np
 
 __all__ = [
-    "GenevaError", "Database", "probe_graph", "batch_count", "kernel_launches", "Plan", "Result", "MODE_DV", "MODE_SV", "library", "library_path",
+    "GenevaError", "Database", "probe_graph", "batch_count", "kernel_launches", "mine", "MinedPattern", "Plan", "Result", "MODE_DV", "MODE_SV", "library", "library_path",
     "loadDataBase", "genMatchOrder", "genMatchOrderSingleV", "match", "gpumine", "gpumineSV",
 ]
 
@@ -58,6 +58,17 @@ class _MatchOpts(ctypes.Structure):
 class _KernelStat(ctypes.Structure):
     _fields_ = [("name", ctypes.c_char * 24), ("launches", ctypes.c_uint64), ("ms", ctypes.c_double),
                 ("bytes", ctypes.c_double)]
+
+
+class _MineOpts(ctypes.Structure):
+    _fields_ = [("stream", ctypes.c_void_p), ("budget_bytes", ctypes.c_uint64), ("max_edges", ctypes.c_uint32),
+                ("min_support", ctypes.c_uint32), ("batch_limit", ctypes.c_uint32), ("reserved", ctypes.c_uint32)]
+
+
+class _MineStats(ctypes.Structure):
+    _fields_ = [("candidates", ctypes.c_uint64), ("frequent", ctypes.c_uint64), ("embeddings", ctypes.c_uint64),
+                ("levels", ctypes.c_uint64), ("pruned", ctypes.c_uint64), ("gpu_ms", ctypes.c_double),
+                ("host_ms", ctypes.c_double)]
 
 
 class _BatchOpts(ctypes.Structure):
@@ -108,6 +119,12 @@ def _declare(lib):
         "gva_step_scratch_bytes": (sz, [u64]),
         "gva_step_run": (i32, [vp, vp, i32, vp, u64, vp, u64, P(u64), vp, sz, vp]),
         "gva_db_set_graphs": (i32, [vp, vp, u32]),
+        "gva_mine": (i32, [vp, P(_MineOpts), P(vp)]),
+        "gva_mine_num_patterns": (i32, [vp]),
+        "gva_mine_get": (i32, [vp, i32, P(u32), P(u32), P(u64)]),
+        "gva_mine_pattern_text": (sz, [vp, i32, ctypes.c_char_p, sz]),
+        "gva_mine_get_stats": (i32, [vp, P(_MineStats)]),
+        "gva_mine_free": (None, [vp]),
         "gva_batch_count": (i32, [vp, vp, i32, P(_BatchOpts), vp, vp, vp, P(_BatchStats)]),
     }
     for name, (res, args) in sig.items():
@@ -341,6 +358,39 @@ def batch_count(db: Database, plans: Sequence[Plan], stream: Optional[int] = Non
     if graph_counts and support:
         per_graph = (gc, sup)
     return counts, per_graph, stats
+
+
+@dataclass
+class MinedPattern:
+    text: str
+    edges: int
+    support: int
+    embeddings: int
+
+
+def mine(db: Database, max_edges: int, min_support: int, stream: Optional[int] = None, budget_bytes: int = 0,
+         batch_limit: int = 0):
+    """Frequent connected patterns of a graph database (gva_mine).
+    Returns (patterns, stats)."""
+    lib = library()
+    o = _MineOpts(stream or None, budget_bytes, max_edges, min_support, batch_limit, 0)
+    h = ctypes.c_void_p()
+    _check(lib.gva_mine(db._h, ctypes.byref(o), ctypes.byref(h)))
+    try:
+        pats = []
+        e, s_, m = ctypes.c_uint32(), ctypes.c_uint32(), ctypes.c_uint64()
+        for i in range(lib.gva_mine_num_patterns(h)):
+            _check(lib.gva_mine_get(h, i, ctypes.byref(e), ctypes.byref(s_), ctypes.byref(m)))
+            n = lib.gva_mine_pattern_text(h, i, None, 0)
+            buf = ctypes.create_string_buffer(n + 1)
+            lib.gva_mine_pattern_text(h, i, buf, n + 1)
+            pats.append(MinedPattern(buf.value.decode(), e.value, s_.value, m.value))
+        st = _MineStats()
+        _check(lib.gva_mine_get_stats(h, ctypes.byref(st)))
+        stats = {f: getattr(st, f) for f, _ in _MineStats._fields_}
+    finally:
+        lib.gva_mine_free(h)
+    return pats, stats
 
 
 # ---- reference-named entry points -------------------------------------------

@@ -31,6 +31,10 @@ struct gva_plan {
 struct gva_result {
     MatchResult r;
 };
+struct gva_mine_result {
+    std::vector<MinedPattern> pats;
+    MineStats stats;
+};
 
 namespace {
 
@@ -321,6 +325,56 @@ int gva_batch_count(gva_db* db, const gva_plan* const* plans, int nplans, const 
     }
     return st;
 }
+
+int gva_mine(gva_db* db, const gva_mine_opts* opts, gva_mine_result** out) {
+    if (!db || !opts || !out) return fail(GVA_ERR_ARG, "null argument");
+    *out = nullptr;
+    gva_mine_result* r = new gva_mine_result();
+    int st = run_mine(*db->dev, (cudaStream_t)opts->stream, opts->budget_bytes, opts->max_edges, opts->min_support,
+                      opts->batch_limit, r->pats, r->stats);
+    if (st) {
+        delete r;
+        return st;
+    }
+    *out = r;
+    return GVA_OK;
+}
+
+int gva_mine_num_patterns(const gva_mine_result* res) { return res ? (int)res->pats.size() : -1; }
+
+int gva_mine_get(const gva_mine_result* res, int index, uint32_t* edges, uint32_t* support, uint64_t* embeddings) {
+    if (!res || index < 0 || index >= (int)res->pats.size()) return fail(GVA_ERR_ARG, "pattern index out of range");
+    const MinedPattern& p = res->pats[index];
+    if (edges) *edges = p.edges;
+    if (support) *support = p.support;
+    if (embeddings) *embeddings = p.embeddings;
+    return GVA_OK;
+}
+
+size_t gva_mine_pattern_text(const gva_mine_result* res, int index, char* buf, size_t cap) {
+    if (!res || index < 0 || index >= (int)res->pats.size()) return 0;
+    const std::string& s = res->pats[index].text;
+    if (buf && cap) {
+        size_t n = std::min(cap - 1, s.size());
+        memcpy(buf, s.data(), n);
+        buf[n] = 0;
+    }
+    return s.size();
+}
+
+int gva_mine_get_stats(const gva_mine_result* res, gva_mine_stats* out) {
+    if (!res || !out) return fail(GVA_ERR_ARG, "null argument");
+    out->candidates = res->stats.candidates;
+    out->frequent = res->stats.frequent;
+    out->embeddings = res->stats.embeddings;
+    out->levels = res->stats.levels;
+    out->pruned = res->stats.pruned;
+    out->gpu_ms = res->stats.gpu_ms;
+    out->host_ms = res->stats.host_ms;
+    return GVA_OK;
+}
+
+void gva_mine_free(gva_mine_result* res) { delete res; }
 
 int gva_plan_num_steps(const gva_plan* plan, const gva_db* db) {
     if (!plan || !db) return -1;

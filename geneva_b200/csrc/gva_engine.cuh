@@ -90,6 +90,22 @@ int run_batch(DevDB& db, const std::vector<std::vector<Step>>& steps, cudaStream
 uint64_t batch_kernel_launches();
 int set_graph_ids(DevDB& db, const uint64_t* first, uint32_t num_graphs);
 
+struct MinedPattern {
+    std::string text;  // query text, vertices in canonical order
+    uint32_t edges;
+    uint32_t support;
+    uint64_t embeddings;
+};
+
+struct MineStats {
+    uint64_t candidates = 0, frequent = 0, embeddings = 0, levels = 0, pruned = 0;
+    double gpu_ms = 0.0, host_ms = 0.0;
+};
+
+// Frequent connected patterns with up to max_edges edges (support = graphs).
+int run_mine(DevDB& db, cudaStream_t s, uint64_t budget, uint32_t max_edges, uint32_t min_support,
+             uint32_t batch_limit, std::vector<MinedPattern>& out, MineStats& st);
+
 size_t step_scratch_bytes(uint64_t in_rows);
 int run_step(DevDB& db, const Step& st, const uint32_t* in, uint64_t in_rows, uint32_t* out, uint64_t out_cap,
              uint64_t* out_rows, void* scratch, size_t scratch_bytes, cudaStream_t stream);

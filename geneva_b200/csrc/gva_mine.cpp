@@ -1,0 +1,321 @@
+// Frequent-pattern mining over a graph database (transaction setting: the
+// support of a pattern is the number of graphs holding at least one
+// embedding), built on the batched matcher.
+//
+// The reference matches one given pattern per process (src/gpumine.cpp:866);
+// it has no pattern generation.  Here patterns grow level by level:
+//   level 1   every (vertex label, edge label, vertex label) edge pattern
+//   level k+1 each frequent k-edge pattern plus one edge, either between two
+//             of its vertices (backward) or to a new vertex (forward), using
+//             only frequent edge types; duplicates removed by a canonical
+//             code; a candidate is kept only if every connected k-edge
+//             sub-pattern is frequent (anti-monotone support)
+// and each level's candidates are matched in one gva_batch_count-style run
+// (shared step prefixes, per-graph bitmaps) whose supports decide the next
+// level.  Each candidate is matched with the planner's own plan for its
+// query text, so embedding counts are the reference's row counts.
+#include <algorithm>
+#include <array>
+#include <chrono>
+#include <cstring>
+#include <functional>
+#include <map>
+#include <set>
+#include <sstream>
+#include <string>
+#include <unordered_set>
+#include <vector>
+
+#include "../../include/geneva.h"
+#include "gva_engine.cuh"
+#include "gva_internal.h"
+
+namespace gva {
+
+namespace {
+
+struct Pattern {
+    uint32_t n = 0;
+    uint32_t vl[GVA_MAX_QUERY_VERTICES];
+    std::vector<std::array<uint32_t, 3>> edges;  // (u, v, edge label), u < v
+    uint32_t el(uint32_t a, uint32_t b) const {
+        for (auto& e : edges)
+            if ((e[0] == a && e[1] == b) || (e[0] == b && e[1] == a)) return e[2];
+        return 0;
+    }
+};
+
+using Code = std::vector<uint32_t>;
+
+struct CodeHash {
+    size_t operator()(const Code& c) const {
+        size_t h = 1469598103934665603ull;
+        for (uint32_t x : c) h = (h ^ x) * 1099511628211ull;
+        return h;
+    }
+};
+
+// Canonical code: the lexicographically smallest (n, labels, upper-triangle
+// edge labels) over vertex orders that sort vertices by an invariant
+// (label, degree, sorted (edge label, neighbour label) list); only orders
+// within equal-invariant cells are tried.
+Code canonical(const Pattern& p, std::vector<uint32_t>* order_out = nullptr) {
+    const uint32_t n = p.n;
+    std::vector<uint32_t> adj(n * n, 0);
+    for (auto& e : p.edges) adj[e[0] * n + e[1]] = adj[e[1] * n + e[0]] = e[2];
+    std::vector<std::vector<uint32_t>> inv(n);
+    for (uint32_t v = 0; v < n; ++v) {
+        std::vector<uint32_t> nb;
+        for (uint32_t u = 0; u < n; ++u)
+            if (adj[v * n + u]) nb.push_back((adj[v * n + u] << 16) | p.vl[u]);
+        std::sort(nb.begin(), nb.end());
+        inv[v] = {p.vl[v], (uint32_t)nb.size()};
+        inv[v].insert(inv[v].end(), nb.begin(), nb.end());
+    }
+    std::vector<uint32_t> ord(n);
+    for (uint32_t i = 0; i < n; ++i) ord[i] = i;
+    std::sort(ord.begin(), ord.end(), [&](uint32_t a, uint32_t b) { return inv[a] < inv[b]; });
+    std::vector<std::pair<uint32_t, uint32_t>> cells;  // [begin, end)
+    for (uint32_t i = 0; i < n;) {
+        uint32_t j = i + 1;
+        while (j < n && inv[ord[j]] == inv[ord[i]]) ++j;
+        cells.push_back({i, j});
+        i = j;
+    }
+    Code best;
+    std::vector<uint32_t> best_ord;
+    Code cur(1 + n + n * (n - 1) / 2);
+    auto evaluate = [&]() {
+        cur[0] = n;
+        for (uint32_t i = 0; i < n; ++i) cur[1 + i] = p.vl[ord[i]];
+        size_t k = 1 + n;
+        for (uint32_t i = 0; i < n; ++i)
+            for (uint32_t j = i + 1; j < n; ++j) cur[k++] = adj[ord[i] * n + ord[j]];
+        if (best.empty() || cur < best) {
+            best = cur;
+            best_ord = ord;
+        }
+    };
+    // iterate the product of within-cell permutations
+    std::function<void(size_t)> rec = [&](size_t c) {
+        if (c == cells.size()) {
+            evaluate();
+            return;
+        }
+        auto b = ord.begin() + cells[c].first, e = ord.begin() + cells[c].second;
+        std::sort(b, e);
+        do {
+            rec(c + 1);
+        } while (std::next_permutation(b, e));
+    };
+    rec(0);
+    if (order_out) *order_out = best_ord;
+    return best;
+}
+
+Pattern relabel(const Pattern& p, const std::vector<uint32_t>& ord) {
+    Pattern q;
+    q.n = p.n;
+    std::vector<uint32_t> pos(p.n);
+    for (uint32_t i = 0; i < p.n; ++i) {
+        pos[ord[i]] = i;
+        q.vl[i] = p.vl[ord[i]];
+    }
+    for (auto& e : p.edges) {
+        uint32_t a = pos[e[0]], b = pos[e[1]];
+        q.edges.push_back({std::min(a, b), std::max(a, b), e[2]});
+    }
+    std::sort(q.edges.begin(), q.edges.end());
+    return q;
+}
+
+std::string query_text(const Pattern& p) {
+    std::ostringstream o;
+    for (uint32_t i = 0; i < p.n; ++i) o << "v " << i << " " << p.vl[i] << "\n";
+    for (auto& e : p.edges) o << "e " << e[0] << " " << e[1] << " " << e[2] << "\n";
+    return o.str();
+}
+
+bool connected_without(const Pattern& p, size_t skip, uint32_t& isolated) {
+    // connectivity of the edge set minus edge `skip`; reports a vertex left
+    // without edges (pendant removal), or kNone
+    std::vector<uint32_t> deg(p.n, 0);
+    for (size_t i = 0; i < p.edges.size(); ++i)
+        if (i != skip) deg[p.edges[i][0]]++, deg[p.edges[i][1]]++;
+    isolated = kNone;
+    uint32_t iso_count = 0;
+    for (uint32_t v = 0; v < p.n; ++v)
+        if (deg[v] == 0) isolated = v, ++iso_count;
+    if (iso_count > 1) return false;
+    uint32_t start = kNone;
+    for (uint32_t v = 0; v < p.n; ++v)
+        if (deg[v]) { start = v; break; }
+    if (start == kNone) return false;
+    std::vector<char> seen(p.n, 0);
+    std::vector<uint32_t> st{start};
+    seen[start] = 1;
+    while (!st.empty()) {
+        uint32_t v = st.back();
+        st.pop_back();
+        for (size_t i = 0; i < p.edges.size(); ++i) {
+            if (i == skip) continue;
+            uint32_t a = p.edges[i][0], b = p.edges[i][1];
+            uint32_t o = a == v ? b : (b == v ? a : kNone);
+            if (o != kNone && !seen[o]) seen[o] = 1, st.push_back(o);
+        }
+    }
+    for (uint32_t v = 0; v < p.n; ++v)
+        if (deg[v] && !seen[v]) return false;
+    return true;
+}
+
+Pattern remove_edge(const Pattern& p, size_t skip, uint32_t isolated) {
+    Pattern q;
+    std::vector<uint32_t> map(p.n, kNone);
+    for (uint32_t v = 0; v < p.n; ++v)
+        if (v != isolated) map[v] = q.n, q.vl[q.n++] = p.vl[v];
+    for (size_t i = 0; i < p.edges.size(); ++i)
+        if (i != skip) {
+            uint32_t a = map[p.edges[i][0]], b = map[p.edges[i][1]];
+            q.edges.push_back({std::min(a, b), std::max(a, b), p.edges[i][2]});
+        }
+    return q;
+}
+
+}  // namespace
+
+int run_mine(DevDB& db, cudaStream_t s, uint64_t budget, uint32_t max_edges, uint32_t min_support,
+             uint32_t batch_limit, std::vector<MinedPattern>& out, MineStats& st) {
+    out.clear();
+    st = MineStats();
+    if (!db.vgraph || db.num_graphs == 0) return fail(GVA_ERR_ARG, "mining needs graph ids (gva_db_set_graphs)");
+    if (max_edges == 0 || max_edges + 1 > GVA_MAX_QUERY_VERTICES) return fail(GVA_ERR_ARG, "max_edges out of range");
+    if (batch_limit == 0) batch_limit = 8192;
+    const uint32_t P = (uint32_t)db.parts.size();
+    const std::vector<uint32_t>& labels = db.labels;
+    auto t_host0 = std::chrono::steady_clock::now();
+    double gpu_ms = 0.0;
+
+    // evaluate a candidate list: supports + embeddings, in bounded batches
+    auto evaluate = [&](const std::vector<Pattern>& cands, std::vector<uint32_t>& sup, std::vector<uint64_t>& emb) -> int {
+        sup.assign(cands.size(), 0);
+        emb.assign(cands.size(), 0);
+        for (size_t b0 = 0; b0 < cands.size(); b0 += batch_limit) {
+            const size_t b1 = std::min(cands.size(), b0 + batch_limit);
+            std::vector<std::vector<Step>> steps(b1 - b0);
+            for (size_t i = b0; i < b1; ++i) {
+                Plan plan;
+                int rc = plan_from_text(query_text(cands[i]), GVA_MODE_DV, plan);
+                if (rc) return rc;
+                rc = lower_plan(plan, db.meta, steps[i - b0]);
+                if (rc) return rc;
+            }
+            BatchStats bs;
+            int rc = run_batch(db, steps, s, budget, db.vgraph, db.num_graphs, emb.data() + b0, nullptr,
+                               sup.data() + b0, false, &bs);
+            if (rc) return rc;
+            gpu_ms += bs.gpu_ms;
+        }
+        st.candidates += cands.size();
+        for (uint64_t e : emb) st.embeddings += e;
+        return GVA_OK;
+    };
+
+    // ---- level 1: every edge type
+    std::vector<Pattern> cands;
+    for (uint32_t a = 0; a < labels.size(); ++a)
+        for (uint32_t b = a; b < labels.size(); ++b)
+            for (uint32_t el = 1; el <= P; ++el) {
+                if (!db.parts[el - 1].off) continue;
+                Pattern p;
+                p.n = 2;
+                p.vl[0] = labels[a];
+                p.vl[1] = labels[b];
+                p.edges.push_back({0, 1, el});
+                cands.push_back(p);
+            }
+    std::vector<uint32_t> sup;
+    std::vector<uint64_t> emb;
+    int rc = evaluate(cands, sup, emb);
+    if (rc) return rc;
+    std::set<std::array<uint32_t, 3>> freq_edge;  // (min label, edge label, max label)
+    std::vector<Pattern> level;
+    std::unordered_set<Code, CodeHash> level_codes;
+    for (size_t i = 0; i < cands.size(); ++i) {
+        if (sup[i] < min_support) continue;
+        const Pattern& p = cands[i];
+        freq_edge.insert({std::min(p.vl[0], p.vl[1]), p.edges[0][2], std::max(p.vl[0], p.vl[1])});
+        std::vector<uint32_t> ord;
+        Code c = canonical(p, &ord);
+        Pattern q = relabel(p, ord);
+        level.push_back(q);
+        level_codes.insert(c);
+        out.push_back({query_text(q), 1, sup[i], emb[i]});
+    }
+    st.levels = 1;
+
+    // ---- levels 2..max_edges
+    for (uint32_t k = 1; k < max_edges && !level.empty(); ++k) {
+        std::unordered_set<Code, CodeHash> seen;
+        std::vector<Pattern> next;
+        auto freq = [&](uint32_t a, uint32_t el, uint32_t b) {
+            return freq_edge.count({std::min(a, b), el, std::max(a, b)}) != 0;
+        };
+        auto consider = [&](const Pattern& c) {
+            std::vector<uint32_t> ord;
+            Code code = canonical(c, &ord);
+            if (!seen.insert(code).second) return;
+            // every connected k-edge sub-pattern must be frequent
+            for (size_t e = 0; e < c.edges.size(); ++e) {
+                uint32_t iso;
+                if (!connected_without(c, e, iso)) continue;
+                if (!level_codes.count(canonical(remove_edge(c, e, iso)))) {
+                    st.pruned++;
+                    return;
+                }
+            }
+            next.push_back(relabel(c, ord));
+        };
+        for (const Pattern& p : level) {
+            for (uint32_t u = 0; u < p.n; ++u) {
+                for (uint32_t v = u + 1; v < p.n; ++v) {  // backward edges
+                    if (p.el(u, v)) continue;
+                    for (uint32_t el = 1; el <= P; ++el) {
+                        if (!freq(p.vl[u], el, p.vl[v])) continue;
+                        Pattern c = p;
+                        c.edges.push_back({u, v, el});
+                        consider(c);
+                    }
+                }
+                if (p.n + 1 > max_edges + 1 || p.n + 1 > GVA_MAX_QUERY_VERTICES) continue;
+                for (uint32_t el = 1; el <= P; ++el) {  // forward edges
+                    for (uint32_t l : labels) {
+                        if (!freq(p.vl[u], el, l)) continue;
+                        Pattern c = p;
+                        c.vl[c.n] = l;
+                        c.edges.push_back({u, c.n, el});
+                        c.n += 1;
+                        consider(c);
+                    }
+                }
+            }
+        }
+        rc = evaluate(next, sup, emb);
+        if (rc) return rc;
+        level.clear();
+        level_codes.clear();
+        for (size_t i = 0; i < next.size(); ++i) {
+            if (sup[i] < min_support) continue;
+            level.push_back(next[i]);
+            level_codes.insert(canonical(next[i]));
+            out.push_back({query_text(next[i]), k + 1, sup[i], emb[i]});
+        }
+        st.levels = k + 1;
+    }
+    st.frequent = out.size();
+    st.gpu_ms = gpu_ms;
+    st.host_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_host0).count();
+    return GVA_OK;
+}
+
+}  // namespace gva

@@ -176,6 +176,43 @@ int gva_db_set_graphs(gva_db* db, const uint64_t* first, uint32_t num_graphs);
 int gva_batch_count(gva_db* db, const gva_plan* const* plans, int nplans, const gva_batch_opts* opts,
                     uint64_t* counts, uint64_t* graph_counts, uint32_t* graph_support, gva_batch_stats* stats);
 
+/* ---- mining layer (graph databases) ------------------------------------------
+ * Frequent connected patterns of up to max_edges edges whose support (graphs
+ * holding at least one embedding) is at least min_support.  Level-wise growth
+ * with canonical dedupe and anti-monotone pruning; every level's candidates
+ * are matched in one batched run.  The reference has no pattern generation
+ * (it matches one given .query per process); each candidate here is matched
+ * with the reference planner's plan, so its embedding count is the row count
+ * gpumine would emit for that pattern. */
+typedef struct gva_mine_opts {
+    void* stream;
+    uint64_t budget_bytes;
+    uint32_t max_edges;
+    uint32_t min_support;
+    uint32_t batch_limit;  /* candidates per batched run (0 = 8192) */
+    uint32_t reserved;
+} gva_mine_opts;
+
+typedef struct gva_mine_stats {
+    uint64_t candidates; /* patterns whose support was decided */
+    uint64_t frequent;
+    uint64_t embeddings; /* embeddings enumerated over all candidates */
+    uint64_t levels;
+    uint64_t pruned;     /* candidates dropped by an infrequent sub-pattern */
+    double gpu_ms;
+    double host_ms;
+} gva_mine_stats;
+
+typedef struct gva_mine_result gva_mine_result;
+
+int gva_mine(gva_db* db, const gva_mine_opts* opts, gva_mine_result** out);
+int gva_mine_num_patterns(const gva_mine_result* res);
+int gva_mine_get(const gva_mine_result* res, int index, uint32_t* edges, uint32_t* support, uint64_t* embeddings);
+/* query text of pattern `index` (.query format); returns length */
+size_t gva_mine_pattern_text(const gva_mine_result* res, int index, char* buf, size_t cap);
+int gva_mine_get_stats(const gva_mine_result* res, gva_mine_stats* out);
+void gva_mine_free(gva_mine_result* res);
+
 /* ---- L4: one phase step on caller-owned device buffers ----------------------
  * Replaces the kernel launchers of include/miningPattern.h:1-30
  * (initEmb_*, extEmb_1V_NoHash, extEmb_2V_*) and include/reduction.h:1-3
