@@ -410,4 +410,15 @@ int gva_step_run(gva_db* db, const gva_plan* plan, int step, const uint32_t* in_
                     scratch_bytes, (cudaStream_t)stream);
 }
 
+int gva_step_run_static(gva_db* db, const gva_plan* plan, int step, const uint32_t* in_dev, uint64_t in_rows,
+                        uint32_t* out_dev, uint64_t out_capacity_rows, uint64_t* out_rows, void* stream) {
+    if (!db || !plan) return fail(GVA_ERR_ARG, "null argument");
+    std::vector<Step> s;
+    int st = steps_for(plan, db, s);
+    if (st) return st;
+    if (step < 0 || step >= (int)s.size()) return fail(GVA_ERR_ARG, "step index out of range");
+    return run_step_static(*db->dev, s[step], in_dev, in_rows, out_dev, out_capacity_rows, out_rows,
+                           (cudaStream_t)stream);
+}
+
 }  // extern "C"

@@ -107,6 +107,9 @@ int run_mine(DevDB& db, cudaStream_t s, uint64_t budget, uint32_t max_edges, uin
              uint32_t batch_limit, std::vector<MinedPattern>& out, MineStats& st);
 
 size_t step_scratch_bytes(uint64_t in_rows);
+// run_step with the library's fixed device scratch array (no allocation).
+int run_step_static(DevDB& db, const Step& st, const uint32_t* in, uint64_t in_rows, uint32_t* out,
+                    uint64_t out_cap, uint64_t* out_rows, cudaStream_t stream);
 int run_step(DevDB& db, const Step& st, const uint32_t* in, uint64_t in_rows, uint32_t* out, uint64_t out_cap,
              uint64_t* out_rows, void* scratch, size_t scratch_bytes, cudaStream_t stream);
 
