@@ -1,22 +1,27 @@
 #!/usr/bin/env python
-"""Benchmark of the matching path on the 20,000-graph database.
+"""Benchmark of the pattern-mining path on the 20,000-graph database.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl geneva|reference]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl geneva|reference] [--workload mine|match]
 
-Workload: the 20,000-graph database (|V|~U[20,60], average degree 4,
-16 vertex labels Zipf(1.2), 3 edge labels; seeded, synthetic) resident in HBM,
-and a batch of seeded query patterns of 3-7 vertices sampled from it.  One
-step matches every pattern of the batch and enumerates every embedding
-(gpumine semantics: rows materialised in HBM).  Metric: embeddings/s, the
-final rows of all patterns over the step time.
+Workload (default, "mine"): the 20,000-graph database (|V|~U[20,60], average
+degree 4, 16 vertex labels Zipf(1.2), 3 edge labels; seeded, synthetic)
+resident in HBM; one step mines every connected pattern of up to 6 edges with
+support >= 2% (400 graphs).  Every candidate of every level is matched on the
+GPU (all embeddings enumerated, per-graph support bitmaps).  Metric:
+embeddings/s = embeddings enumerated over all candidates / step time;
+patterns/s (candidates whose support was decided / step time) rides along.
+
+"match": the same database and a batch of seeded 3-7 vertex patterns sampled
+from it, counted per pattern with supporting graphs.
 
 N > 1 (torchrun, one process per GPU): every rank holds the database and
-matches its own batch (weak scaling, no collective on the data path); the
+works on its own share (weak scaling, no collective on the data path); the
 step time is the max over ranks.
 
---impl reference times the reference CPU matcher (oracle/_ref/cpumine,
-built from the reference sources) on the same database and patterns, one
-process per pattern over all host cores.
+--impl reference times the reference CPU matcher (oracle/_ref/cpumine, built
+from the reference sources) on the same database and patterns, one process
+per pattern over the host cores (the reference has no miner: each pattern is
+a separate cpumine run, support from its rows' graph ids).
 """
 from __future__ import annotations
 
@@ -37,6 +42,9 @@ sys.path.insert(0, str(ROOT))
 
 import numpy as np  # noqa: E402
 
+MINE_WORKLOAD = ("config-2 mining: 20000 graphs per rank, |V|~U[20,60], avg degree 4, 16 vertex labels Zipf(1.2), "
+                 "3 edge labels; all connected patterns of up to {me} edges with support >= {ms:g} of the graphs; "
+                 "every candidate matched, all embeddings enumerated")
 WORKLOAD = ("config-2 database: 20000 graphs, |V|~U[20,60], avg degree 4, 16 vertex labels Zipf(1.2), "
             "3 edge labels; batch of seeded 3-7 vertex patterns sampled from it; every embedding enumerated "
             "and counted per pattern, with its supporting graphs")
@@ -48,7 +56,11 @@ def parse_args():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="geneva", choices=["geneva", "reference"])
-    ap.add_argument("--queries", type=int, default=256, help="patterns per rank per step")
+    ap.add_argument("--workload", default="mine", choices=["mine", "match"])
+    ap.add_argument("--queries", type=int, default=256, help="match workload: patterns per rank per step")
+    ap.add_argument("--max-edges", type=int, default=6)
+    ap.add_argument("--min-support", type=float, default=0.02, help="fraction of graphs")
+    ap.add_argument("--sample", type=int, default=256, help="patterns in the plain-path and CPU samples")
     ap.add_argument("--seed", type=int, default=2)
     return ap.parse_args()
 
@@ -141,9 +153,11 @@ def cpu_baseline_port(db, queries, budget_s=15.0):
                       f"{rows} embeddings in {dt:.2f} s"}
 
 
-def reference_arm(args, db, queries):
+def reference_arm(args, db, queries, workload):
     """oracle/_ref/cpumine (the reference CPU matcher built from source) on the
-    same database (converted by oracle/_ref/genDatabase) and patterns."""
+    same database (converted by oracle/_ref/genDatabase) and patterns, one
+    process per pattern, a wave of processes per step over the host cores;
+    each pattern's support comes from its rows' graph ids."""
     ref = ROOT / "oracle" / "_ref"
     if not (ref / "cpumine").exists() or not (ref / "genDatabase").exists():
         return {"impl": "reference", "unavailable": "oracle/_ref binaries not built (reference sources absent at build)"}
@@ -151,11 +165,17 @@ def reference_arm(args, db, queries):
     (work / "datasets").mkdir()
     (work / "run").mkdir()
     (work / "datasets" / "config2.g").write_text(db.to_g_text())
+    t_conv = time.perf_counter()
     subprocess.run([str(ref / "genDatabase"), "config2"], cwd=work / "run", check=True,
                    stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
+    t_conv = time.perf_counter() - t_conv
     ds = work / "datasets"
     reorder = work / "run" / "config2.reorder"
+    meta = np.loadtxt(ds / "config2.metadata", dtype=np.int64)  # new id, label, old id (0-based .g id)
+    new_to_old = np.zeros(int(meta[:, 0].max()) + 1, dtype=np.int64)
+    new_to_old[meta[:, 0]] = meta[:, 2]
     cores = os.cpu_count() or 1
+    wave = max(1, min(cores, len(queries), 8))
 
     def one(i_q):
         i, q = i_q
@@ -165,35 +185,207 @@ def reference_arm(args, db, queries):
         subprocess.run([str(ref / "cpumine"), str(reorder), "q.query", str(ds / "config2.mygraph"),
                         str(ds / "config2.metadata")], cwd=d, stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL,
                        check=True)
-        with open(d / "partialResultsCPU.txt") as f:
-            return sum(1 for _ in f)
+        rows = [l.split() for l in open(d / "partialResultsCPU.txt") if l.strip()]
+        if not rows:
+            return 0, 0
+        r = np.unique(np.array(rows, dtype=np.int64), axis=0)  # cpumine repeats rows via index vertices
+        support = len(np.unique(db.graph_of(new_to_old[r[:, 0]] + 1)))
+        return r.shape[0], support
 
-    # bound each step to about a minute of host time: calibrate on the warm-up
-    sample = queries[: min(len(queries), cores * 4)]
+    steps_done = [0]
+
     def step():
+        k = steps_done[0]
+        steps_done[0] += 1
+        batch = [(k * wave + j, queries[(k * wave + j) % len(queries)]) for j in range(wave)]
         t0 = time.perf_counter()
-        with ThreadPoolExecutor(max_workers=cores) as ex:
-            rows = sum(ex.map(one, list(enumerate(sample))))
-        return rows, time.perf_counter() - t0
+        with ThreadPoolExecutor(max_workers=wave) as ex:
+            res = list(ex.map(one, batch))
+        return sum(r for r, _ in res), len(res), time.perf_counter() - t0
+
     for _ in range(args.warmup):
         step()
-    tot_rows, tot_t = 0, 0.0
+    tot_rows, tot_pats, tot_t = 0, 0, 0.0
     for _ in range(args.steps):
-        r, t = step()
+        r, n, t = step()
         tot_rows += r
+        tot_pats += n
         tot_t += t
     value = tot_rows / tot_t
     return {
         "metric": "embeddings/s", "value": value, "unit": "embeddings/s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * tot_t / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
-        "impl": "reference",
-        "config": {"workload": WORKLOAD, "patterns_per_step": len(sample), "seed": args.seed},
-        "cpu_baseline": {"value": value, "unit": "embeddings/s", "cores": cores, "kind": "reference",
-                         "sample": f"{len(sample)} of the {len(queries)} patterns per step, one cpumine "
-                                   f"process per pattern"},
+        "impl": "reference", "patterns_per_s": tot_pats / tot_t,
+        "config": {"workload": workload, "seed": args.seed, "patterns_per_step": wave,
+                   "database_conversion_s": t_conv},
+        "cpu_baseline": {"value": value, "unit": "embeddings/s", "cores": wave, "kind": "reference",
+                         "sample": f"{wave} seeded 2-7 vertex patterns per step sampled from the database, one "
+                                   f"cpumine process each (it reloads the database per pattern)"},
         "e2e": {"value": value, "unit": "embeddings/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
+
+
+# --------------------------------------------------------------- mining arm ----
+def mine_bench(args, rank, world, local, dist, torch, gv, workloads, shard):
+    """One step = one complete mining run on this rank's 20,000-graph shard."""
+    G = 20000
+    full = workloads.graph_database(G * world, 20, 60, 4.0, 16, 1.2, 3, seed=args.seed, name="config2")
+    db = shard.shard_database(full, rank, world) if world > 1 else full
+    minsup = int(np.ceil(args.min_support * G * world))
+    gdb = gv.Database.from_edges(db.vlabels, db.src, db.dst, db.elabels, device=local)
+    gdb.set_graphs(db.first)
+    reduce = shard.SupportReducer() if world > 1 else None
+    stream = torch.cuda.Stream()
+    sp = stream.cuda_stream
+    flush = torch.empty(512 << 20, dtype=torch.uint8, device="cuda")
+
+    def one(profile=False):
+        return gv.mine(gdb, args.max_edges, minsup, stream=sp, profile=profile, reduce=reduce)
+
+    for _ in range(max(args.warmup, 3)):
+        one()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    clocks = ClockSampler(local)
+    clocks.start()
+    launches0 = gv.kernel_launches()
+    ms, emb_local, cands, frequent = [], 0, 0, 0
+    stats = None
+    for _ in range(args.steps):
+        with torch.cuda.stream(stream):
+            flush.zero_()
+        stream.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        pats, stats = one()
+        e1.record(stream)
+        e1.synchronize()
+        ms.append(e0.elapsed_time(e1))
+        emb_local += stats["embeddings"]
+        cands += stats["candidates"]
+        frequent = len(pats)
+    launches = gv.kernel_launches() - launches0
+    clk = clocks.stop()
+
+    def red(x, op):
+        if not dist:
+            return x
+        t = torch.tensor([float(x)], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=op)
+        return float(t.item())
+
+    t_sum = red(sum(ms), dist.ReduceOp.MAX if dist else None)
+    emb_all = red(emb_local, dist.ReduceOp.SUM if dist else None)
+    value = emb_all / (t_sum / 1000.0)
+    patterns_per_s = cands / (t_sum / 1000.0)  # candidates are identical on every rank
+
+    # ---- batched vs plain per-pattern GPU path on a seeded sample of patterns
+    sample = workloads.sample_patterns(db, args.sample, 2, 7, seed=1000 + rank)
+    plans = [gv.Plan.from_text(q) for q in sample]
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    counts, sup_b, _ = gv.batch_count(gdb, plans, stream=sp, support=True)
+    torch.cuda.synchronize()
+    t_batch = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    plain_rows, sup_p = 0, []
+    for p in plans:
+        r = gv.match(gdb, p, stream=sp)
+        rows = r.rows()
+        plain_rows += rows.shape[0]
+        sup_p.append(len(np.unique(db.graph_of(rows[:, 0].astype(np.int64)))) if rows.size else 0)
+        r.close()
+    t_plain = time.perf_counter() - t0
+    assert plain_rows == int(counts.sum()) and list(sup_b) == sup_p, "batched and plain paths disagree"
+
+    # ---- profiled mining run for the roofline of the dominant kernel
+    with torch.cuda.stream(stream):
+        flush.zero_()
+    stream.synchronize()
+    _, pstats = one(profile=True)
+    kstats = {k: v for k, v in pstats["kernels"].items() if v["launches"]}
+
+    # ---- end to end: host edge arrays -> database upload -> mining -> patterns on the host
+    e2e_steps = max(1, min(args.steps, 3))
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    e2e_emb, h2d, d2h = 0, 0, 0
+    for _ in range(e2e_steps):
+        g2 = gv.Database.from_edges(db.vlabels, db.src, db.dst, db.elabels, device=local)
+        g2.set_graphs(db.first)
+        h2d += g2.info()["device_bytes"] + 4 * (db.num_vertices + 1)
+        pats2, st2 = gv.mine(g2, args.max_edges, minsup, stream=sp, reduce=reduce)
+        e2e_emb += st2["embeddings"]
+        d2h += sum(len(p.text) + 16 for p in pats2)
+        g2.close()
+    torch.cuda.synchronize()
+    e2e_t = red(time.perf_counter() - t0, dist.ReduceOp.MAX if dist else None)
+    e2e_value = red(e2e_emb, dist.ReduceOp.SUM if dist else None) / e2e_t
+
+    peak, peak_kind = measured_peak_gbs()
+    name, s = max(kstats.items(), key=lambda kv: kv[1]["ms"]) if kstats else ("none", {"launches": 0, "ms": 0, "bytes": 0})
+    per_launch_ms = s["ms"] / max(s["launches"], 1)
+    achieved = (s["bytes"] / max(s["launches"], 1)) / (per_launch_ms / 1000.0) / 1e9 if per_launch_ms else 0.0
+    out = {
+        "metric": "embeddings/s", "value": value, "unit": "embeddings/s", "n_gpus": world,
+        "steps": args.steps, "warmup": max(args.warmup, 3), "ms_per_step": t_sum / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
+        "data": "synthetic (seeded generator of the configuration's shapes)",
+        "patterns_per_s": patterns_per_s,
+        "config": {"workload": MINE_WORKLOAD.format(me=args.max_edges, ms=args.min_support), "graphs_per_rank": G,
+                   "min_support_graphs": minsup, "max_edges": args.max_edges, "seed": args.seed,
+                   "candidates_per_step": cands // max(args.steps, 1), "frequent_patterns": frequent,
+                   "l2": "flushed between steps (512 MiB write)",
+                   "parallelism": f"graph database sharded over {world} rank(s); per-level support all-reduce"},
+        "mining": {k: stats[k] for k in ("levels", "candidates", "frequent", "pruned", "gpu_ms", "host_ms", "gen_ms",
+                                         "plan_ms")},
+        "plain": {"sample": f"{len(sample)} seeded 2-7 vertex patterns sampled from the database",
+                  "batched_embeddings_per_s": int(counts.sum()) / t_batch,
+                  "plain_embeddings_per_s": plain_rows / t_plain,
+                  "batched_over_plain": t_plain / t_batch,
+                  "path": "plain = one gva_match per pattern, rows to host, support from their graph ids"},
+        "roofline": {"bound": "hbm", "kernel": name, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "peak_source": peak_kind, "traffic": ncu_traffic(name),
+                     "launches": s["launches"], "kernel_ms": s["ms"]},
+        "kernels": kstats,
+        "e2e": {"value": e2e_value, "unit": "embeddings/s", "h2d_bytes_per_step": h2d // e2e_steps,
+                "d2h_bytes_per_step": d2h // e2e_steps,
+                "note": "database uploaded from host arrays, mined, patterns with supports returned to the host"},
+        "gpu_launches": launches,
+        "clocks": clk,
+    }
+    if rank == 0 and world == 1:
+        out["cpu_baseline"] = cpu_baseline_mine(db, sample)
+    gdb.close()
+    return out
+
+
+def cpu_baseline_mine(db, sample, budget_s=15.0):
+    """The oracle (single-threaded restatement of cpumine) on a bounded sample:
+    every pattern matched, support from its rows' graph ids."""
+    sys.path.insert(0, str(ROOT / "tests"))
+    from oracle_lib import Oracle
+    o = Oracle.get()
+    g = o.from_edges(db.vlabels, db.src, db.dst, db.elabels)
+    t0 = time.perf_counter()
+    rows = done = 0
+    for q in sample:
+        r, _ = o.match(g, q)
+        rows += r.shape[0]
+        if r.size:
+            np.unique(db.graph_of(r[:, 0].astype(np.int64)))
+        done += 1
+        if time.perf_counter() - t0 > budget_s:
+            break
+    dt = time.perf_counter() - t0
+    o.free(g)
+    return {"value": rows / dt, "unit": "embeddings/s", "cores": 1, "kind": "port",
+            "patterns_per_s": done / dt,
+            "sample": f"{done} of the {len(sample)} sampled patterns, oracle restatement of cpumine + graph-id "
+                      f"support, {rows} embeddings in {dt:.2f} s"}
 
 
 # ------------------------------------------------------------------ GPU arm ----
@@ -208,8 +400,13 @@ def main():
         if rank != 0:
             return 0
         db = workloads.config2(seed=args.seed)
-        queries = workloads.sample_patterns(db, args.queries, 3, 7, seed=1000)
-        print(json.dumps(reference_arm(args, db, queries)), flush=True)
+        if args.workload == "mine":
+            queries = workloads.sample_patterns(db, args.sample, 2, 7, seed=1000)
+            wl = MINE_WORKLOAD.format(me=args.max_edges, ms=args.min_support)
+        else:
+            queries = workloads.sample_patterns(db, args.queries, 3, 7, seed=1000)
+            wl = WORKLOAD
+        print(json.dumps(reference_arm(args, db, queries, wl)), flush=True)
         return 0
 
     import torch
@@ -221,6 +418,15 @@ def main():
         import datetime
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    if args.workload == "mine":
+        from geneva_b200 import shard
+        out = mine_bench(args, rank, world, local, dist, torch, gv, workloads, shard)
+        if dist:
+            dist.barrier()
+            dist.destroy_process_group()
+        if rank == 0:
+            print(json.dumps(out), flush=True)
+        return 0
     db = workloads.config2(seed=args.seed)
     queries = workloads.sample_patterns(db, args.queries, 3, 7, seed=1000 + rank)
     gdb = gv.Database.from_edges(db.vlabels, db.src, db.dst, db.elabels, device=local)

@@ -60,15 +60,20 @@ class _KernelStat(ctypes.Structure):
                 ("bytes", ctypes.c_double)]
 
 
+REDUCE_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.POINTER(ctypes.c_uint32), ctypes.POINTER(ctypes.c_uint64),
+                             ctypes.c_uint64, ctypes.c_void_p)
+
+
 class _MineOpts(ctypes.Structure):
     _fields_ = [("stream", ctypes.c_void_p), ("budget_bytes", ctypes.c_uint64), ("max_edges", ctypes.c_uint32),
-                ("min_support", ctypes.c_uint32), ("batch_limit", ctypes.c_uint32), ("reserved", ctypes.c_uint32)]
+                ("min_support", ctypes.c_uint32), ("batch_limit", ctypes.c_uint32), ("profile", ctypes.c_uint32),
+                ("reduce", REDUCE_FN), ("reduce_user", ctypes.c_void_p)]
 
 
 class _MineStats(ctypes.Structure):
     _fields_ = [("candidates", ctypes.c_uint64), ("frequent", ctypes.c_uint64), ("embeddings", ctypes.c_uint64),
                 ("levels", ctypes.c_uint64), ("pruned", ctypes.c_uint64), ("gpu_ms", ctypes.c_double),
-                ("host_ms", ctypes.c_double)]
+                ("host_ms", ctypes.c_double), ("gen_ms", ctypes.c_double), ("plan_ms", ctypes.c_double)]
 
 
 class _BatchOpts(ctypes.Structure):
@@ -125,6 +130,7 @@ def _declare(lib):
         "gva_mine_pattern_text": (sz, [vp, i32, ctypes.c_char_p, sz]),
         "gva_mine_get_stats": (i32, [vp, P(_MineStats)]),
         "gva_mine_free": (None, [vp]),
+        "gva_mine_kernel_stats": (i32, [vp, P(_KernelStat), i32]),
         "gva_batch_count": (i32, [vp, vp, i32, P(_BatchOpts), vp, vp, vp, P(_BatchStats)]),
     }
     for name, (res, args) in sig.items():
@@ -369,11 +375,26 @@ class MinedPattern:
 
 
 def mine(db: Database, max_edges: int, min_support: int, stream: Optional[int] = None, budget_bytes: int = 0,
-         batch_limit: int = 0):
+         batch_limit: int = 0, profile: bool = False, reduce=None):
     """Frequent connected patterns of a graph database (gva_mine).
-    Returns (patterns, stats)."""
+
+    `reduce(supports, embeddings)` (numpy uint32 / uint64 arrays, updated in
+    place) combines each level's counts across processes holding disjoint
+    graph shards.  Returns (patterns, stats); stats["kernels"] is filled
+    when profiling."""
     lib = library()
-    o = _MineOpts(stream or None, budget_bytes, max_edges, min_support, batch_limit, 0)
+    cb = REDUCE_FN(0)
+    if reduce is not None:
+        def _cb(sp, ep, n, user):
+            try:
+                sup = np.ctypeslib.as_array(sp, shape=(n,))
+                emb = np.ctypeslib.as_array(ep, shape=(n,))
+                reduce(sup, emb)
+                return 0
+            except Exception:
+                return 1
+        cb = REDUCE_FN(_cb)
+    o = _MineOpts(stream or None, budget_bytes, max_edges, min_support, batch_limit, 1 if profile else 0, cb, None)
     h = ctypes.c_void_p()
     _check(lib.gva_mine(db._h, ctypes.byref(o), ctypes.byref(h)))
     try:
@@ -388,6 +409,10 @@ def mine(db: Database, max_edges: int, min_support: int, stream: Optional[int] =
         st = _MineStats()
         _check(lib.gva_mine_get_stats(h, ctypes.byref(st)))
         stats = {f: getattr(st, f) for f, _ in _MineStats._fields_}
+        ks = (_KernelStat * 8)()
+        n = lib.gva_mine_kernel_stats(h, ks, 8)
+        stats["kernels"] = {ks[i].name.decode(): dict(launches=int(ks[i].launches), ms=float(ks[i].ms),
+                                                       bytes=float(ks[i].bytes)) for i in range(n)}
     finally:
         lib.gva_mine_free(h)
     return pats, stats

@@ -164,7 +164,38 @@ batch_write_kernel(const TaskDesc* __restrict__ tasks, const uint64_t* __restric
         __syncthreads();
         const uint64_t row0 = (b - d.block0) * kRowsPerBlock;
         const uint64_t out0 = base_s;
-        if (d.kind == STEP_EXT) {
+        if (d.kind == STEP_EXT && d.e.n_chk) {
+            // fused back-edge checks: each thread walks its row's generator
+            // segment twice (count, then write) and stores survivors directly
+            const ExtArgs& p = d.e;
+            const uint32_t k = p.k, k1 = p.k + 1;
+            uint32_t* rows_s = reinterpret_cast<uint32_t*>(smem_raw);
+            const uint32_t nr = (uint32_t)umin64((uint64_t)kRowsPerBlock, p.nrows - row0);
+            const uint32_t* gin = p.in + row0 * k;
+            for (uint32_t w = threadIdx.x; w < nr * k; w += kThreads) rows_s[w] = gin[w];
+            __syncthreads();
+            const uint32_t* row = rows_s + threadIdx.x * k;
+            const uint32_t* gadj = nullptr;
+            uint32_t lo = 0, hi = 0, cnt = 0;
+            int which = -1;
+            if (threadIdx.x < nr) {
+                ext_generator(p, row, gadj, lo, hi, which);
+                for (uint32_t j = lo; j < hi; ++j) cnt += ext_accept(p, row, __ldg(gadj + j), which) ? 1u : 0u;
+            }
+            uint64_t total;
+            const uint64_t before = block_exclusive_scan(cnt, &total);
+            if (cnt) {
+                uint32_t* dst = out + (out0 + before) * k1;
+                for (uint32_t j = lo; j < hi; ++j) {
+                    const uint32_t c = __ldg(gadj + j);
+                    if (!ext_accept(p, row, c, which)) continue;
+                    for (uint32_t q = 0; q < k; ++q) dst[q] = row[q];
+                    dst[k] = c;
+                    dst += k1;
+                }
+            }
+            __syncthreads();
+        } else if (d.kind == STEP_EXT) {
             const ExtArgs& p = d.e;
             const uint32_t k = p.k, k1 = p.k + 1;
             uint64_t* offs_s = reinterpret_cast<uint64_t*>(smem_raw);
@@ -315,6 +346,11 @@ std::string step_key(const Step& st) {
         put(&st.bound_inclusive, 4);
         put(&st.n_eq, 4);
         put(st.eq_cols, st.n_eq);
+        put(&st.n_chk, 4);
+        put(st.chk_col, st.n_chk);
+        put(st.chk_dir, st.n_chk);
+        put(st.chk_part, 4 * st.n_chk);
+        put(st.chk_lab, 4 * st.n_chk);
     } else if (st.kind == STEP_REDUCE) {
         put(&st.n_pairs, 4);
         put(st.rs_col, st.n_pairs);
@@ -513,6 +549,14 @@ int run_batch(DevDB& db, const std::vector<std::vector<Step>>& steps, cudaStream
                 a.n_eq = st.n_eq;
                 for (uint32_t i = 0; i < st.n_eq; ++i) a.eq_cols[i] = st.eq_cols[i];
                 eqmax = std::max(eqmax, st.n_eq);
+                a.n_chk = st.n_chk;
+                for (uint32_t i = 0; i < st.n_chk; ++i) {
+                    a.chk_col[i] = st.chk_col[i];
+                    a.chk_dir[i] = st.chk_dir[i];
+                    a.chk_lab[i] = st.chk_lab[i];
+                    a.chk_off[i] = db.parts[st.chk_part[i] - 1].off;
+                    a.chk_adj[i] = db.parts[st.chk_part[i] - 1].adj;
+                }
             } else {
                 RedArgs& a = d.r;
                 a.in = tk.in;

@@ -303,7 +303,7 @@ int gva_batch_count(gva_db* db, const gva_plan* const* plans, int nplans, const 
     std::vector<std::vector<Step>> steps(nplans);
     for (int i = 0; i < nplans; ++i) {
         if (!plans[i]) return fail(GVA_ERR_ARG, "null plan");
-        int st = steps_for(plans[i], db, steps[i]);
+        int st = lower_plan(plans[i]->plan, db->dev->meta, steps[i], true);
         if (st) return st;
     }
     BatchStats bs;
@@ -331,7 +331,7 @@ int gva_mine(gva_db* db, const gva_mine_opts* opts, gva_mine_result** out) {
     *out = nullptr;
     gva_mine_result* r = new gva_mine_result();
     int st = run_mine(*db->dev, (cudaStream_t)opts->stream, opts->budget_bytes, opts->max_edges, opts->min_support,
-                      opts->batch_limit, r->pats, r->stats);
+                      opts->batch_limit, opts->profile != 0, opts->reduce, opts->reduce_user, r->pats, r->stats);
     if (st) {
         delete r;
         return st;
@@ -371,7 +371,21 @@ int gva_mine_get_stats(const gva_mine_result* res, gva_mine_stats* out) {
     out->pruned = res->stats.pruned;
     out->gpu_ms = res->stats.gpu_ms;
     out->host_ms = res->stats.host_ms;
+    out->gen_ms = res->stats.gen_ms;
+    out->plan_ms = res->stats.plan_ms;
     return GVA_OK;
+}
+
+int gva_mine_kernel_stats(const gva_mine_result* res, gva_kernel_stat* out, int cap) {
+    if (!res) return -1;
+    for (int i = 0; i < K_NUM && i < cap; ++i) {
+        memset(&out[i], 0, sizeof out[i]);
+        strncpy(out[i].name, kKernelNames[i], sizeof out[i].name - 1);
+        out[i].launches = res->stats.kstat[i].launches;
+        out[i].ms = res->stats.kstat[i].ms;
+        out[i].bytes = res->stats.kstat[i].bytes;
+    }
+    return K_NUM;
 }
 
 void gva_mine_free(gva_mine_result* res) { delete res; }

@@ -99,12 +99,15 @@ struct MinedPattern {
 
 struct MineStats {
     uint64_t candidates = 0, frequent = 0, embeddings = 0, levels = 0, pruned = 0;
-    double gpu_ms = 0.0, host_ms = 0.0;
+    double gpu_ms = 0.0, host_ms = 0.0, gen_ms = 0.0, plan_ms = 0.0;
+    KernelStat kstat[K_NUM];
 };
 
 // Frequent connected patterns with up to max_edges edges (support = graphs).
+typedef int (*ReduceFn)(uint32_t* supports, uint64_t* embeddings, uint64_t n, void* user);
 int run_mine(DevDB& db, cudaStream_t s, uint64_t budget, uint32_t max_edges, uint32_t min_support,
-             uint32_t batch_limit, std::vector<MinedPattern>& out, MineStats& st);
+             uint32_t batch_limit, bool profile, ReduceFn reduce, void* reduce_user, std::vector<MinedPattern>& out,
+             MineStats& st);
 
 size_t step_scratch_bytes(uint64_t in_rows);
 // run_step with the library's fixed device scratch array (no allocation).

@@ -227,8 +227,9 @@ int graph_from_edges(const uint32_t* vlabels, uint32_t max_id, const uint32_t* s
 //                               (src/cpumine.cpp:298-435)
 //   R                         : reduce over all pairs (src/cpumine.cpp:486-584); more than
 //                               16 pairs empties the frontier as the reference does (:499-502)
-int lower_plan(const Plan& plan, const HostGraph& g, std::vector<Step>& steps) {
+int lower_plan(const Plan& plan, const HostGraph& g, std::vector<Step>& steps, bool fuse_reductions) {
     steps.clear();
+    int newest = -1;  // query vertex added by the last extension step
     const uint32_t P = (uint32_t)g.parts.size();
     std::vector<int> col(plan.vnum, -1);
     int width = 0;
@@ -247,6 +248,7 @@ int lower_plan(const Plan& plan, const HostGraph& g, std::vector<Step>& steps) {
         st.always_empty = (st.part == 0 || st.label == kNone) ? 1 : 0;
         steps.push_back(st);
         col[e] = width++;
+        newest = (int)e;
     };
     auto same_label_cols = [&](uint32_t e) {
         std::vector<int> eq;
@@ -297,6 +299,31 @@ int lower_plan(const Plan& plan, const HostGraph& g, std::vector<Step>& steps) {
                 ext(ph.edge_label, s, e, bc, false, same_label_cols(e));
             }
         } else {
+            // fold into the previous extension when every pair touches its new vertex
+            if (fuse_reductions && !steps.empty() && steps.back().kind == STEP_EXT && newest >= 0 &&
+                !steps.back().always_empty && np <= 8 - steps.back().n_chk && np <= GVA_MAX_REDUCE_PAIRS) {
+                bool ok = true;
+                for (size_t i = 0; i < np && ok; ++i)
+                    ok = (int)ph.pairs[2 * i] == newest || (int)ph.pairs[2 * i + 1] == newest;
+                if (ok) {
+                    Step& st = steps.back();
+                    const uint32_t part = part_of(ph.edge_label);
+                    if (part == 0) st.always_empty = 1;
+                    for (size_t i = 0; i < np; ++i) {
+                        const uint32_t a = ph.pairs[2 * i], b = ph.pairs[2 * i + 1];
+                        const bool new_is_b = (int)b == newest;  // pair checks b in adj(a) with label(b)
+                        const uint32_t other = new_is_b ? a : b;
+                        st.chk_col[st.n_chk] = (uint8_t)col[other];
+                        st.chk_dir[st.n_chk] = new_is_b ? 0 : 1;
+                        st.chk_part[st.n_chk] = part;
+                        st.chk_lab[st.n_chk] = g.dense_label(plan.qlabel[b]);
+                        if (st.chk_lab[st.n_chk] == kNone) st.always_empty = 1;
+                        st.n_chk++;
+                    }
+                    st.phase_end = (int)pi;
+                    continue;
+                }
+            }
             Step st;
             st.kind = STEP_REDUCE;
             st.width_in = (uint32_t)width;

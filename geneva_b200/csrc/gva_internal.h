@@ -86,8 +86,18 @@ struct Step {
     uint32_t re_label[16] = {};
     uint32_t always_empty = 0;     // reference limit reached (>16 pairs) or label absent
     int phase_end = -1;            // reference phase index completed by this step, else -1
+    // EXT with fused back edges (lowered with fuse_reductions): the candidate
+    // must also be adjacent to row[chk_col[i]] in partition chk_part[i];
+    // dir 0 looks the candidate up in the partner's segment, dir 1 the
+    // partner in the candidate's (the reference's pair orientation)
+    uint32_t n_chk = 0;
+    uint8_t chk_col[8] = {}, chk_dir[8] = {};
+    uint32_t chk_part[8] = {}, chk_lab[8] = {};
 };
 
-int lower_plan(const Plan& plan, const HostGraph& g, std::vector<Step>& steps);
+// fuse_reductions: fold each reduction that only checks edges of the vertex
+// just added into that extension (same final rows, fewer steps; per-phase
+// counts of the folded phases are then not observable).
+int lower_plan(const Plan& plan, const HostGraph& g, std::vector<Step>& steps, bool fuse_reductions = false);
 
 }  // namespace gva

@@ -15,6 +15,7 @@ namespace {
 constexpr int kRowsPerBlock = 256;  // rows handled by one count/write block
 constexpr int kThreads = 256;
 constexpr int kScanThreads = 1024;
+constexpr int kMaxChecks = 8;  // fused back-edge checks per extension
 
 // ---------------------------------------------------------------- params ----
 struct ExtArgs {
@@ -31,6 +32,15 @@ struct ExtArgs {
     uint32_t bound_incl;
     uint32_t n_eq;
     uint8_t eq_cols[kMaxCols];
+    // fused back edges (batched engine): a candidate c is kept only if, for
+    // every check i, c lies in seg_i(row[chk_col[i]], lab) (dir 0) or
+    // row[chk_col[i]] lies in seg_i(c, chk_lab[i]) (dir 1)
+    uint32_t n_chk;
+    uint8_t chk_col[kMaxChecks];
+    uint8_t chk_dir[kMaxChecks];
+    uint32_t chk_lab[kMaxChecks];
+    const uint32_t* chk_off[kMaxChecks];
+    const uint32_t* chk_adj[kMaxChecks];
 };
 
 struct RedArgs {
@@ -83,8 +93,62 @@ __device__ __forceinline__ uint32_t find_in(const uint32_t* __restrict__ adj, ui
     return (pos < hi && __ldg(adj + pos) == w) ? pos : 0xffffffffu;
 }
 
+// Candidate source of a row with fused checks: the shortest of the source
+// segment and the dir-0 check segments, each cut below the restriction
+// bound.  which = -1 (source) or the check index.
+__device__ __forceinline__ void ext_generator(const ExtArgs& p, const uint32_t* row, const uint32_t*& gadj,
+                                              uint32_t& lo, uint32_t& hi, int& which) {
+    ext_range(p, row, lo, hi);
+    gadj = p.adj;
+    which = -1;
+    for (uint32_t i = 0; i < p.n_chk && lo < hi; ++i) {
+        if (p.chk_dir[i]) continue;
+        const uint64_t t = (uint64_t)row[p.chk_col[i]] * p.L + p.lab;
+        uint32_t l2 = __ldg(p.chk_off[i] + t), h2 = __ldg(p.chk_off[i] + t + 1);
+        if (p.bound_col >= 0 && l2 < h2)
+            h2 = lower_bound_u32(p.chk_adj[i], l2, h2, (uint64_t)row[p.bound_col] + p.bound_incl);
+        if (h2 - l2 < hi - lo) {
+            lo = l2;
+            hi = h2;
+            gadj = p.chk_adj[i];
+            which = (int)i;
+        }
+    }
+}
+
+__device__ __forceinline__ bool seg_has(const uint32_t* __restrict__ off, const uint32_t* __restrict__ adj, uint32_t L,
+                                        uint32_t v, uint32_t lab, uint32_t w) {
+    const uint64_t t = (uint64_t)v * L + lab;
+    return find_in(adj, __ldg(off + t), __ldg(off + t + 1), w) != 0xffffffffu;
+}
+
+// Whether generated candidate c survives injectivity, the source edge (when
+// the generator is a check segment) and every other check.
+__device__ __forceinline__ bool ext_accept(const ExtArgs& p, const uint32_t* row, uint32_t c, int which) {
+    for (uint32_t j = 0; j < p.n_eq; ++j)
+        if (row[p.eq_cols[j]] == c) return false;
+    if (which >= 0 && !seg_has(p.off, p.adj, p.L, row[p.src_col], p.lab, c)) return false;
+    for (uint32_t i = 0; i < p.n_chk; ++i) {
+        if ((int)i == which) continue;
+        const uint32_t w = row[p.chk_col[i]];
+        const bool ok = p.chk_dir[i] ? seg_has(p.chk_off[i], p.chk_adj[i], p.L, c, p.chk_lab[i], w)
+                                     : seg_has(p.chk_off[i], p.chk_adj[i], p.L, w, p.lab, c);
+        if (!ok) return false;
+    }
+    return true;
+}
+
 // Number of candidates of one row (segment minus already-matched vertices).
 __device__ __forceinline__ uint32_t ext_count_row(const ExtArgs& p, const uint32_t* row) {
+    if (p.n_chk) {
+        const uint32_t* gadj;
+        uint32_t lo, hi;
+        int which;
+        ext_generator(p, row, gadj, lo, hi, which);
+        uint32_t n = 0;
+        for (uint32_t j = lo; j < hi; ++j) n += ext_accept(p, row, __ldg(gadj + j), which) ? 1u : 0u;
+        return n;
+    }
     uint32_t lo, hi;
     ext_range(p, row, lo, hi);
     if (lo >= hi) return 0;

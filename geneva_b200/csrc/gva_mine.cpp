@@ -19,6 +19,7 @@
 #include <chrono>
 #include <cstring>
 #include <functional>
+#include <thread>
 #include <map>
 #include <set>
 #include <sstream>
@@ -79,6 +80,7 @@ Code canonical(const Pattern& p, std::vector<uint32_t>* order_out = nullptr) {
     for (uint32_t i = 0; i < n;) {
         uint32_t j = i + 1;
         while (j < n && inv[ord[j]] == inv[ord[i]]) ++j;
+        std::sort(ord.begin() + i, ord.begin() + j);
         cells.push_back({i, j});
         i = j;
     }
@@ -96,19 +98,15 @@ Code canonical(const Pattern& p, std::vector<uint32_t>* order_out = nullptr) {
             best_ord = ord;
         }
     };
-    // iterate the product of within-cell permutations
-    std::function<void(size_t)> rec = [&](size_t c) {
-        if (c == cells.size()) {
-            evaluate();
-            return;
-        }
-        auto b = ord.begin() + cells[c].first, e = ord.begin() + cells[c].second;
-        std::sort(b, e);
-        do {
-            rec(c + 1);
-        } while (std::next_permutation(b, e));
-    };
-    rec(0);
+    // odometer over the product of within-cell permutations (each cell
+    // starts sorted; next_permutation wraps back to sorted and carries)
+    for (;;) {
+        evaluate();
+        int c = (int)cells.size() - 1;
+        for (; c >= 0; --c)
+            if (std::next_permutation(ord.begin() + cells[c].first, ord.begin() + cells[c].second)) break;
+        if (c < 0) break;
+    }
     if (order_out) *order_out = best_ord;
     return best;
 }
@@ -185,7 +183,8 @@ Pattern remove_edge(const Pattern& p, size_t skip, uint32_t isolated) {
 }  // namespace
 
 int run_mine(DevDB& db, cudaStream_t s, uint64_t budget, uint32_t max_edges, uint32_t min_support,
-             uint32_t batch_limit, std::vector<MinedPattern>& out, MineStats& st) {
+             uint32_t batch_limit, bool profile, ReduceFn reduce, void* reduce_user, std::vector<MinedPattern>& out,
+             MineStats& st) {
     out.clear();
     st = MineStats();
     if (!db.vgraph || db.num_graphs == 0) return fail(GVA_ERR_ARG, "mining needs graph ids (gva_db_set_graphs)");
@@ -195,6 +194,7 @@ int run_mine(DevDB& db, cudaStream_t s, uint64_t budget, uint32_t max_edges, uin
     const std::vector<uint32_t>& labels = db.labels;
     auto t_host0 = std::chrono::steady_clock::now();
     double gpu_ms = 0.0;
+    const unsigned nthreads = std::max(1u, std::min(64u, std::thread::hardware_concurrency()));
 
     // evaluate a candidate list: supports + embeddings, in bounded batches
     auto evaluate = [&](const std::vector<Pattern>& cands, std::vector<uint32_t>& sup, std::vector<uint64_t>& emb) -> int {
@@ -203,21 +203,40 @@ int run_mine(DevDB& db, cudaStream_t s, uint64_t budget, uint32_t max_edges, uin
         for (size_t b0 = 0; b0 < cands.size(); b0 += batch_limit) {
             const size_t b1 = std::min(cands.size(), b0 + batch_limit);
             std::vector<std::vector<Step>> steps(b1 - b0);
-            for (size_t i = b0; i < b1; ++i) {
-                Plan plan;
-                int rc = plan_from_text(query_text(cands[i]), GVA_MODE_DV, plan);
-                if (rc) return rc;
-                rc = lower_plan(plan, db.meta, steps[i - b0]);
-                if (rc) return rc;
-            }
+            auto t0 = std::chrono::steady_clock::now();
+            std::vector<int> rcs(nthreads, GVA_OK);
+            std::vector<std::thread> pool;
+            for (unsigned t = 0; t < nthreads; ++t)
+                pool.emplace_back([&, t]() {
+                    for (size_t i = b0 + t; i < b1; i += nthreads) {
+                        Plan plan;
+                        int r = plan_from_text(query_text(cands[i]), GVA_MODE_DV, plan);
+                        if (!r) r = lower_plan(plan, db.meta, steps[i - b0], true);
+                        if (r) {
+                            rcs[t] = r;
+                            return;
+                        }
+                    }
+                });
+            for (auto& th : pool) th.join();
+            for (int r : rcs)
+                if (r) return r;
+            st.plan_ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
             BatchStats bs;
             int rc = run_batch(db, steps, s, budget, db.vgraph, db.num_graphs, emb.data() + b0, nullptr,
-                               sup.data() + b0, false, &bs);
+                               sup.data() + b0, profile, &bs);
             if (rc) return rc;
             gpu_ms += bs.gpu_ms;
+            for (int kk = 0; kk < K_NUM; ++kk) {
+                st.kstat[kk].launches += bs.kstat[kk].launches;
+                st.kstat[kk].ms += bs.kstat[kk].ms;
+                st.kstat[kk].bytes += bs.kstat[kk].bytes;
+            }
         }
         st.candidates += cands.size();
-        for (uint64_t e : emb) st.embeddings += e;
+        for (uint64_t e : emb) st.embeddings += e;  // this process's share
+        if (reduce && !cands.empty() && reduce(sup.data(), emb.data(), cands.size(), reduce_user))
+            return fail(GVA_ERR_ARG, "support reduction across processes failed");
         return GVA_OK;
     };
 
@@ -256,50 +275,70 @@ int run_mine(DevDB& db, cudaStream_t s, uint64_t budget, uint32_t max_edges, uin
 
     // ---- levels 2..max_edges
     for (uint32_t k = 1; k < max_edges && !level.empty(); ++k) {
-        std::unordered_set<Code, CodeHash> seen;
-        std::vector<Pattern> next;
+        auto t_gen = std::chrono::steady_clock::now();
         auto freq = [&](uint32_t a, uint32_t el, uint32_t b) {
             return freq_edge.count({std::min(a, b), el, std::max(a, b)}) != 0;
         };
-        auto consider = [&](const Pattern& c) {
-            std::vector<uint32_t> ord;
-            Code code = canonical(c, &ord);
-            if (!seen.insert(code).second) return;
-            // every connected k-edge sub-pattern must be frequent
-            for (size_t e = 0; e < c.edges.size(); ++e) {
-                uint32_t iso;
-                if (!connected_without(c, e, iso)) continue;
-                if (!level_codes.count(canonical(remove_edge(c, e, iso)))) {
-                    st.pruned++;
-                    return;
-                }
-            }
-            next.push_back(relabel(c, ord));
-        };
-        for (const Pattern& p : level) {
-            for (uint32_t u = 0; u < p.n; ++u) {
-                for (uint32_t v = u + 1; v < p.n; ++v) {  // backward edges
-                    if (p.el(u, v)) continue;
-                    for (uint32_t el = 1; el <= P; ++el) {
-                        if (!freq(p.vl[u], el, p.vl[v])) continue;
-                        Pattern c = p;
-                        c.edges.push_back({u, v, el});
-                        consider(c);
+        // each thread extends every nthreads-th pattern; candidates are merged
+        // by canonical code and sorted so the level is deterministic
+        std::vector<std::vector<std::pair<Code, Pattern>>> found(nthreads);
+        std::vector<uint64_t> pruned(nthreads, 0);
+        std::vector<std::thread> pool;
+        for (unsigned t = 0; t < nthreads; ++t)
+            pool.emplace_back([&, t]() {
+                std::unordered_set<Code, CodeHash> seen;
+                auto consider = [&](const Pattern& c) {
+                    std::vector<uint32_t> ord;
+                    Code code = canonical(c, &ord);
+                    if (!seen.insert(code).second) return;
+                    // every connected k-edge sub-pattern must be frequent
+                    for (size_t e = 0; e < c.edges.size(); ++e) {
+                        uint32_t iso;
+                        if (!connected_without(c, e, iso)) continue;
+                        if (!level_codes.count(canonical(remove_edge(c, e, iso)))) {
+                            pruned[t]++;
+                            return;
+                        }
+                    }
+                    found[t].push_back({std::move(code), relabel(c, ord)});
+                };
+                for (size_t i = t; i < level.size(); i += nthreads) {
+                    const Pattern& p = level[i];
+                    for (uint32_t u = 0; u < p.n; ++u) {
+                        for (uint32_t v = u + 1; v < p.n; ++v) {  // backward edges
+                            if (p.el(u, v)) continue;
+                            for (uint32_t el = 1; el <= P; ++el) {
+                                if (!freq(p.vl[u], el, p.vl[v])) continue;
+                                Pattern c = p;
+                                c.edges.push_back({u, v, el});
+                                consider(c);
+                            }
+                        }
+                        if (p.n + 1 > max_edges + 1 || p.n + 1 > GVA_MAX_QUERY_VERTICES) continue;
+                        for (uint32_t el = 1; el <= P; ++el) {  // forward edges
+                            for (uint32_t l : labels) {
+                                if (!freq(p.vl[u], el, l)) continue;
+                                Pattern c = p;
+                                c.vl[c.n] = l;
+                                c.edges.push_back({u, c.n, el});
+                                c.n += 1;
+                                consider(c);
+                            }
+                        }
                     }
                 }
-                if (p.n + 1 > max_edges + 1 || p.n + 1 > GVA_MAX_QUERY_VERTICES) continue;
-                for (uint32_t el = 1; el <= P; ++el) {  // forward edges
-                    for (uint32_t l : labels) {
-                        if (!freq(p.vl[u], el, l)) continue;
-                        Pattern c = p;
-                        c.vl[c.n] = l;
-                        c.edges.push_back({u, c.n, el});
-                        c.n += 1;
-                        consider(c);
-                    }
-                }
-            }
+            });
+        for (auto& th : pool) th.join();
+        std::vector<std::pair<Code, Pattern>> all;
+        for (unsigned t = 0; t < nthreads; ++t) {
+            st.pruned += pruned[t];
+            for (auto& x : found[t]) all.push_back(std::move(x));
         }
+        std::sort(all.begin(), all.end(), [](const auto& a, const auto& b) { return a.first < b.first; });
+        std::vector<Pattern> next;
+        for (size_t i = 0; i < all.size(); ++i)
+            if (i == 0 || all[i].first != all[i - 1].first) next.push_back(std::move(all[i].second));
+        st.gen_ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_gen).count();
         rc = evaluate(next, sup, emb);
         if (rc) return rc;
         level.clear();

@@ -184,13 +184,20 @@ int gva_batch_count(gva_db* db, const gva_plan* const* plans, int nplans, const 
  * (it matches one given .query per process); each candidate here is matched
  * with the reference planner's plan, so its embedding count is the row count
  * gpumine would emit for that pattern. */
+/* Combines one level's per-candidate supports and embedding counts across
+ * processes that hold disjoint shards of the graph database (e.g. an
+ * all-reduce sum); arrays are updated in place; return 0 on success. */
+typedef int (*gva_reduce_fn)(uint32_t* supports, uint64_t* embeddings, uint64_t n, void* user);
+
 typedef struct gva_mine_opts {
     void* stream;
     uint64_t budget_bytes;
     uint32_t max_edges;
     uint32_t min_support;
     uint32_t batch_limit;  /* candidates per batched run (0 = 8192) */
-    uint32_t reserved;
+    uint32_t profile;      /* 1: per-kernel CUDA-event timing (gva_mine_kernel_stats) */
+    gva_reduce_fn reduce;  /* NULL on one process */
+    void* reduce_user;
 } gva_mine_opts;
 
 typedef struct gva_mine_stats {
@@ -199,8 +206,10 @@ typedef struct gva_mine_stats {
     uint64_t embeddings; /* embeddings enumerated over all candidates */
     uint64_t levels;
     uint64_t pruned;     /* candidates dropped by an infrequent sub-pattern */
-    double gpu_ms;
-    double host_ms;
+    double gpu_ms;       /* batched matching (CUDA events) */
+    double host_ms;      /* whole call, wall clock */
+    double gen_ms;       /* candidate generation, dedupe and pruning (host threads) */
+    double plan_ms;      /* planning and lowering of every candidate (host threads) */
 } gva_mine_stats;
 
 typedef struct gva_mine_result gva_mine_result;
@@ -211,6 +220,8 @@ int gva_mine_get(const gva_mine_result* res, int index, uint32_t* edges, uint32_
 /* query text of pattern `index` (.query format); returns length */
 size_t gva_mine_pattern_text(const gva_mine_result* res, int index, char* buf, size_t cap);
 int gva_mine_get_stats(const gva_mine_result* res, gva_mine_stats* out);
+/* per-kernel totals when opts->profile was set; returns the number of kinds */
+int gva_mine_kernel_stats(const gva_mine_result* res, gva_kernel_stat* out, int cap);
 void gva_mine_free(gva_mine_result* res);
 
 /* ---- L4: one phase step on caller-owned device buffers ----------------------
