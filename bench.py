@@ -56,7 +56,9 @@ def parse_args():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="geneva", choices=["geneva", "reference"])
-    ap.add_argument("--workload", default="mine", choices=["mine", "match"])
+    ap.add_argument("--workload", default="mine", choices=["mine", "match", "serve"])
+    ap.add_argument("--rates", default="10,100,500,2000", help="serve workload: arrival rates (req/s)")
+    ap.add_argument("--duration", type=float, default=2.0, help="serve workload: seconds of arrivals per rate")
     ap.add_argument("--queries", type=int, default=256, help="match workload: patterns per rank per step")
     ap.add_argument("--max-edges", type=int, default=6)
     ap.add_argument("--min-support", type=float, default=0.02, help="fraction of graphs")
@@ -224,6 +226,60 @@ def reference_arm(args, db, queries, workload):
                                    f"cpumine process each (it reloads the database per pattern)"},
         "e2e": {"value": value, "unit": "embeddings/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
+
+
+# -------------------------------------------------------------- serving arm ----
+def serve_bench(args, local, torch, gv, workloads):
+    """Poisson arrivals at each rate: 80% matching requests (3-10 vertex
+    patterns sampled from the database), 20% mining requests (max edges 3-5,
+    min support 1-5% of the graphs), all against the resident config-2
+    database; continuous batching with a 150 GB admission budget."""
+    import random
+    from geneva_b200.serve import Server, percentile
+    db = workloads.config2(seed=args.seed)
+    gdb = gv.Database.from_edges(db.vlabels, db.src, db.dst, db.elabels, device=local)
+    gdb.set_graphs(db.first)
+    G = len(db.first) - 1
+    pool = workloads.sample_patterns(db, 512, 3, 10, seed=4242)
+    s_match, s_mine = torch.cuda.Stream(), torch.cuda.Stream()
+    points = []
+    for rate in [float(x) for x in args.rates.split(",")]:
+        srv = Server(gdb, budget_bytes=150 << 30, match_stream=s_match.cuda_stream, mine_stream=s_mine.cuda_stream)
+        rng = random.Random(int(rate))
+        reqs = []
+        t_end = time.perf_counter() + args.duration
+        nxt = time.perf_counter()
+        while nxt < t_end:
+            while time.perf_counter() < nxt:
+                pass
+            if rng.random() < 0.8:
+                reqs.append(srv.submit_match(pool[rng.randrange(len(pool))]))
+            else:
+                reqs.append(srv.submit_mine(rng.randint(3, 5), int(G * rng.uniform(0.01, 0.05))))
+            nxt += rng.expovariate(rate)
+        deadline = time.perf_counter() + 60.0
+        for r in reqs:
+            try:
+                r.future.result(timeout=max(0.0, deadline - time.perf_counter()))
+            except Exception:
+                pass
+        t_stop = time.perf_counter()
+        done = [r for r in reqs if r.future.done() and not r.future.exception()]
+        emb = sum(r.result[0] for r in done if r.kind == "match") + \
+              sum(r.result[1]["embeddings"] for r in done if r.kind == "mine")
+        lm = [r.latency for r in done if r.kind == "match"]
+        ln = [r.latency for r in done if r.kind == "mine"]
+        t0 = min(r.arrival for r in reqs) if reqs else t_stop
+        points.append({"rate": rate, "requests": len(reqs), "completed": len(done),
+                       "match_p50_ms": 1e3 * percentile(lm, 50) if lm else None,
+                       "match_p99_ms": 1e3 * percentile(lm, 99) if lm else None,
+                       "mine_p50_ms": 1e3 * percentile(ln, 50) if ln else None,
+                       "mine_p99_ms": 1e3 * percentile(ln, 99) if ln else None,
+                       "embeddings_per_s": emb / (t_stop - t0), "rounds": srv.rounds})
+        srv.close()
+    gdb.close()
+    return {"metric": "p99 query latency", "unit": "ms", "workload": "serving sweep on the config-2 database "
+            "(mining requests use graph support on the same database)", "points": points}
 
 
 # --------------------------------------------------------------- mining arm ----
@@ -418,6 +474,10 @@ def main():
         import datetime
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    if args.workload == "serve":
+        out = serve_bench(args, local, torch, gv, workloads)
+        print(json.dumps(out), flush=True)
+        return 0
     if args.workload == "mine":
         from geneva_b200 import shard
         out = mine_bench(args, rank, world, local, dist, torch, gv, workloads, shard)

@@ -306,31 +306,6 @@ size_t batch_smem_bytes_for(uint32_t kmax, uint32_t eqmax) {
 
 std::atomic<uint64_t> g_batch_launches{0};
 
-// Device buffer shared by every task whose frontier slice lives in it.
-struct DevBuf {
-    void* p = nullptr;
-    cudaStream_t s = nullptr;
-    ~DevBuf() {
-        if (p) cudaFreeAsync(p, s);
-    }
-};
-
-// A node of the step trie: the plans of a batch that agree on their first
-// steps share those steps' frontiers.
-struct Node {
-    Step step;
-    int depth = 0;
-    std::vector<int> children;
-    std::vector<int> terminal;  // plans whose last step is this node
-};
-
-struct Task {
-    int node;
-    const uint32_t* in;          // frontier slice
-    uint64_t rows;
-    std::shared_ptr<DevBuf> owner;
-};
-
 // Bytes that determine a step's output from its input (everything but phase_end).
 std::string step_key(const Step& st) {
     std::string k;
@@ -360,127 +335,240 @@ std::string step_key(const Step& st) {
     return k;
 }
 
-// Pinned host staging reused across rounds and calls (per thread and device).
-struct Staging {
-    char* p = nullptr;
-    size_t cap = 0;
-    char* get(size_t need) {
-        if (need > cap) {
-            if (p) cudaFreeHost(p);
-            cap = std::max(need, cap * 2);
-            if (cudaMallocHost((void**)&p, cap) != cudaSuccess) {
-                p = nullptr;
-                cap = 0;
-            }
-        }
-        return p;
-    }
-};
-
 }  // namespace
 
 uint64_t batch_kernel_launches() { return g_batch_launches.load(); }
 
-int run_batch(DevDB& db, const std::vector<std::vector<Step>>& steps, cudaStream_t s, uint64_t budget,
-              const uint32_t* vgraph, uint32_t G, uint64_t* counts, uint64_t* graph_counts_host,
-              uint32_t* support_host, bool profile, BatchStats* stats) {
+char* Staging::get(size_t need) {
+    if (need > cap) {
+        if (p) cudaFreeHost(p);
+        cap = std::max(need, cap * 2);
+        if (cudaMallocHost((void**)&p, cap) != cudaSuccess) {
+            p = nullptr;
+            cap = 0;
+        }
+    }
+    return p;
+}
+Staging::~Staging() {
+    if (p) cudaFreeHost(p);
+}
+
+// ---------------------------------------------------------------------------
+// BatchSession: the persistent form of the batched engine.  Plans are
+// submitted in waves (plans of one wave share their common step prefixes);
+// every round() advances all active tasks by one step; a plan completes when
+// no task on its path is left.  run_batch() is one wave run to completion;
+// the serving loop submits new waves between rounds.
+BatchSession::BatchSession(DevDB& db_, cudaStream_t s_, uint64_t budget_, uint32_t slots_, bool graph_counts_,
+                           bool profile_)
+    : db(db_), s(s_), budget(budget_), nslots(slots_), want_graph_counts(graph_counts_), profile(profile_) {}
+
+BatchSession::~BatchSession() {
+    cudaSetDevice(db.device);
+    active.clear();
+    for (void* p : {(void*)d_desc, (void*)d_sums, (void*)d_small, acc})
+        if (p) cudaFreeAsync(p, s);
+    cudaStreamSynchronize(s);
+}
+
+int BatchSession::init() {
     GVA_CUDA_B(cudaSetDevice(db.device));
-    const int nq = (int)steps.size();
-    for (int q = 0; q < nq; ++q) counts[q] = 0;
-    if (nq == 0) return GVA_OK;
-    if ((graph_counts_host || support_host) && (!vgraph || G == 0))
-        return fail(GVA_ERR_ARG, "per-graph results need the database's graph ids (gva_db_set_graphs)");
     if (budget == 0) {
         size_t fr = 0, tot = 0;
         GVA_CUDA_B(cudaMemGetInfo(&fr, &tot));
         budget = (uint64_t)fr / 4 * 3;
     }
-    Profiler profiler;
-    Profiler* prof = profile ? &profiler : nullptr;
-    static thread_local cudaEvent_t tev[64][2];
-    const int dev = db.device;
-    if (dev < 0 || dev >= 64) return fail(GVA_ERR_ARG, "device index out of range");
-    if (!tev[dev][0]) {
-        GVA_CUDA_B(cudaEventCreate(&tev[dev][0]));
-        GVA_CUDA_B(cudaEventCreate(&tev[dev][1]));
-    }
-    cudaEvent_t ev0 = tev[dev][0], ev1 = tev[dev][1];
-    GVA_CUDA_B(cudaEventRecord(ev0, s));
-
-    // ---- step trie: plans sharing a prefix of steps share its frontiers
-    std::vector<Node> nodes;
-    std::map<std::string, int> roots;
-    std::vector<std::map<std::string, int>> kids;
-    for (int q = 0; q < nq; ++q) {
-        const std::vector<Step>& st = steps[q];
-        if (st.size() < 2 || st[0].kind != STEP_SEED) return fail(GVA_ERR_ARG, "plan must start with a seed step");
-        int cur = -1;
-        for (size_t i = 0; i < st.size(); ++i) {
-            const std::string key = step_key(st[i]);
-            auto& m0 = cur < 0 ? roots : kids[cur];
-            auto it = m0.find(key);
-            int id;
-            if (it == m0.end()) {
-                id = (int)nodes.size();
-                nodes.push_back(Node{st[i], (int)i, {}, {}});
-                kids.emplace_back();  // may reallocate: look the parent's map up again
-                (cur < 0 ? roots : kids[cur])[key] = id;
-                if (cur >= 0) nodes[cur].children.push_back(id);
-            } else {
-                id = it->second;
-            }
-            cur = id;
-        }
-        nodes[cur].terminal.push_back(q);
-    }
-
-    // per-graph accumulators: one slot per plan; plans that end on the same
-    // node are filled from its first plan at the end
-    BatchCtx ctx{};
-    ctx.vgraph = vgraph;
-    ctx.G = G;
-    ctx.words = (G + 31) / 32;
-    const bool per_graph = graph_counts_host || support_host;
-    void* acc = nullptr;
+    per_graph = nslots > 0;
     if (per_graph) {
-        const size_t acc_bytes = (graph_counts_host ? (size_t)nq * G * 8 : 0) + (size_t)nq * ctx.words * 4;
-        if (cudaMallocAsync(&acc, acc_bytes, s) != cudaSuccess) return fail(GVA_ERR_NOMEM, "per-graph counters");
-        GVA_CUDA_B(cudaMemsetAsync(acc, 0, acc_bytes, s));
-        char* a = (char*)acc;
-        if (graph_counts_host) {
-            ctx.graph_counts = (uint64_t*)a;
-            a += (size_t)nq * G * 8;
-        }
-        ctx.graph_bits = (uint32_t*)a;
+        if (!db.vgraph || db.num_graphs == 0)
+            return fail(GVA_ERR_ARG, "per-graph results need the database's graph ids (gva_db_set_graphs)");
+        ctx_words = (db.num_graphs + 31) / 32;
+        const size_t bytes = (want_graph_counts ? (size_t)nslots * db.num_graphs * 8 : 0) + (size_t)nslots * ctx_words * 4;
+        if (cudaMallocAsync(&acc, bytes, s) != cudaSuccess) return fail(GVA_ERR_NOMEM, "per-graph counters");
+        GVA_CUDA_B(cudaMemsetAsync(acc, 0, bytes, s));
+        for (uint32_t i = nslots; i > 0; --i) free_slots.push_back((int)i - 1);
     }
-
-    std::vector<Task> active;
-    for (auto& kv : roots) {
-        const Node& seed = nodes[kv.second];
-        if (seed.step.always_empty) continue;
-        const uint64_t n = db.seed_off[seed.step.label + 1] - db.seed_off[seed.step.label];
-        if (!n) continue;
-        for (int c : seed.children) active.push_back({c, db.seed_verts + db.seed_off[seed.step.label], n, nullptr});
-    }
-
-    int status = GVA_OK;
-    static thread_local Staging staging[64];
-    Staging& stg = staging[dev];
-    TaskDesc* d_desc = nullptr;
-    size_t desc_cap = 0;
-    uint64_t* d_sums = nullptr;
-    size_t sums_cap = 0;
-    uint64_t* d_small = nullptr;  // block0[nt + 1] | totals[nt] | outs[nt] | queue
-    size_t small_cap = 0;
+    int dev = db.device;
     static bool smem_set[64] = {};
+    if (dev < 0 || dev >= 64) return fail(GVA_ERR_ARG, "device index out of range");
     if (!smem_set[dev]) {
         GVA_CUDA_B(cudaFuncSetAttribute(batch_write_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                         (int)batch_smem_bytes()));
         smem_set[dev] = true;
     }
-    int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    return GVA_OK;
+}
 
+uint64_t* BatchSession::graph_counts_dev() const { return want_graph_counts ? (uint64_t*)acc : nullptr; }
+uint32_t* BatchSession::graph_bits_dev() const {
+    return per_graph ? (uint32_t*)((char*)acc + (want_graph_counts ? (size_t)nslots * db.num_graphs * 8 : 0)) : nullptr;
+}
+
+void BatchSession::add_task(int node, const uint32_t* in, uint64_t rows, std::shared_ptr<void> owner) {
+    for (int q : nodes[node].below) plans[q].live++;
+    active.push_back({node, in, rows, std::move(owner)});
+}
+
+void BatchSession::end_task(int node) {
+    for (int q : nodes[node].below) {
+        if (--plans[q].live == 0 && !plans[q].done) {
+            plans[q].done = true;
+            completed.push_back(q);
+        }
+    }
+}
+
+int BatchSession::submit(const std::vector<std::vector<Step>>& steps, const std::vector<uint64_t>& tags,
+                         std::vector<int>* ids) {
+    std::map<std::string, int> roots;
+    std::map<int, std::map<std::string, int>> kids;
+    const int first_plan = (int)plans.size();
+    for (size_t qi = 0; qi < steps.size(); ++qi) {
+        const std::vector<Step>& st = steps[qi];
+        if (st.size() < 2 || st[0].kind != STEP_SEED) return fail(GVA_ERR_ARG, "plan must start with a seed step");
+        PlanRec pr;
+        pr.tag = qi < tags.size() ? tags[qi] : qi;
+        if (per_graph) {
+            if (free_slots.empty()) return fail(GVA_ERR_NOMEM, "no free per-graph result slot");
+            pr.slot = free_slots.back();
+            free_slots.pop_back();
+        }
+        const int q = (int)plans.size();
+        plans.push_back(pr);
+        if (ids) ids->push_back(q);
+        int cur = -1;
+        for (size_t i = 0; i < st.size(); ++i) {
+            const std::string key = step_key(st[i]);
+            auto& m = cur < 0 ? roots : kids[cur];
+            auto it = m.find(key);
+            int id;
+            if (it == m.end()) {
+                id = (int)nodes.size();
+                nodes.push_back(BNode{st[i], (int)i, {}, {}, {}});
+                m[key] = id;
+                if (cur >= 0) nodes[cur].children.push_back(id);
+            } else {
+                id = it->second;
+            }
+            nodes[id].below.push_back(q);
+            cur = id;
+        }
+        nodes[cur].terminal.push_back(q);
+        plans[q].terminal = cur;
+    }
+    // seeds: the children of every seed node start from its vertex list
+    for (auto& kv : roots) {
+        const BNode& seed = nodes[kv.second];
+        uint64_t n = 0;
+        if (!seed.step.always_empty) n = db.seed_off[seed.step.label + 1] - db.seed_off[seed.step.label];
+        if (n == 0) {
+            for (int q : seed.below) {
+                plans[q].done = true;
+                completed.push_back(q);
+            }
+            continue;
+        }
+        for (int c : seed.children) add_task(c, db.seed_verts + db.seed_off[seed.step.label], n, nullptr);
+    }
+    (void)first_plan;
+    return GVA_OK;
+}
+
+int BatchSession::round() {
+    GVA_CUDA_B(cudaSetDevice(db.device));
+    // steps that cannot match (label or partition absent) end their task
+    for (size_t i = 0; i < active.size();) {
+        if (nodes[active[i].node].step.always_empty) {
+            const int nd = active[i].node;
+            active.erase(active.begin() + i);
+            end_task(nd);
+        } else {
+            ++i;
+        }
+    }
+    if (active.empty()) return GVA_OK;
+    ++rounds;
+    Profiler prof;
+    Profiler* pf = profile ? &prof : nullptr;
+    BatchCtx ctx{};
+    ctx.vgraph = db.vgraph;
+    ctx.G = db.num_graphs;
+    ctx.words = ctx_words;
+    ctx.graph_counts = graph_counts_dev();
+    ctx.graph_bits = graph_bits_dev();
+    const int nt = (int)active.size();
+    const size_t desc_bytes = (size_t)nt * sizeof(TaskDesc);
+    const size_t small_words = (size_t)(nt + 1) + nt + nt + 1;
+    char* h = staging.get(desc_bytes + small_words * 8);
+    if (!h) return fail(GVA_ERR_NOMEM, "pinned staging allocation failed");
+    TaskDesc* descs = (TaskDesc*)h;
+    uint64_t* h_block0 = (uint64_t*)(h + desc_bytes);
+    uint64_t* h_totals = h_block0 + (nt + 1);
+    uint32_t** h_outs = (uint32_t**)(h_totals + nt);
+    std::vector<uint64_t> block0(nt + 1, 0);
+    uint32_t kmax = 1, eqmax = 0;
+    double cbytes = 0;
+    for (int t = 0; t < nt; ++t) {
+        const BTask& tk = active[t];
+        const BNode& nd = nodes[tk.node];
+        const Step& st = nd.step;
+        TaskDesc& d = descs[t];
+        memset(&d, 0, sizeof d);
+        d.kind = st.kind;
+        d.mode = nd.children.empty() ? MODE_COUNT : MODE_WRITE;
+        if (per_graph && !nd.terminal.empty()) {
+            d.mode = nd.children.empty() ? MODE_COUNT_GRAPHS : MODE_WRITE_AND_GRAPHS;
+            d.query = (uint32_t)plans[nd.terminal[0]].slot;
+        }
+        d.block0 = block0[t];
+        const DevPart& P = db.parts[st.part - 1];
+        if (st.kind == STEP_EXT) {
+            ExtArgs& a = d.e;
+            a.in = tk.in;
+            a.nrows = tk.rows;
+            a.off = P.off;
+            a.adj = P.adj;
+            a.k = st.width_in;
+            a.L = db.L;
+            a.lab = st.label;
+            a.src_col = st.src_col;
+            a.bound_col = st.bound_col;
+            a.bound_incl = st.bound_inclusive;
+            a.n_eq = st.n_eq;
+            for (uint32_t i = 0; i < st.n_eq; ++i) a.eq_cols[i] = st.eq_cols[i];
+            eqmax = std::max(eqmax, st.n_eq);
+            a.n_chk = st.n_chk;
+            for (uint32_t i = 0; i < st.n_chk; ++i) {
+                a.chk_col[i] = st.chk_col[i];
+                a.chk_dir[i] = st.chk_dir[i];
+                a.chk_lab[i] = st.chk_lab[i];
+                a.chk_off[i] = db.parts[st.chk_part[i] - 1].off;
+                a.chk_adj[i] = db.parts[st.chk_part[i] - 1].adj;
+            }
+        } else {
+            RedArgs& a = d.r;
+            a.in = tk.in;
+            a.nrows = tk.rows;
+            a.off = P.off;
+            a.adj = P.adj;
+            a.k = st.width_in;
+            a.L = db.L;
+            a.n_pairs = st.n_pairs;
+            for (uint32_t i = 0; i < st.n_pairs; ++i) {
+                a.rs[i] = st.rs_col[i];
+                a.re[i] = st.re_col[i];
+                a.rl[i] = st.re_label[i];
+            }
+        }
+        kmax = std::max(kmax, st.width_in);
+        block0[t + 1] = block0[t] + (tk.rows + kRowsPerBlock - 1) / kRowsPerBlock;
+        cbytes += (4.0 * st.width_in + 8.0 * (st.kind == STEP_EXT ? 1 : st.n_pairs)) * (double)tk.rows;
+    }
+    const uint64_t nb = block0[nt];
+    if (nb > 0x7fffffffull) return fail(GVA_ERR_UNSUPPORTED, "round too large for one launch");
+    std::copy(block0.begin(), block0.end(), h_block0);
     auto grow = [&](void** p, size_t& cap, size_t need) -> bool {
         if (need <= cap) return true;
         if (*p) cudaFreeAsync(*p, s);
@@ -493,246 +581,248 @@ int run_batch(DevDB& db, const std::vector<std::vector<Step>>& steps, cudaStream
         cap = c;
         return true;
     };
+    if (!grow(&d_desc, desc_cap, desc_bytes) || !grow((void**)&d_sums, sums_cap, (nb + 1) * 8) ||
+        !grow((void**)&d_small, small_cap, small_words * 8))
+        return fail(GVA_ERR_NOMEM, "batch bookkeeping allocation failed");
+    uint64_t* d_block0 = d_small;
+    uint64_t* d_totals = d_block0 + (nt + 1);
+    uint32_t** d_outs = (uint32_t**)(d_totals + nt);
+    unsigned long long* d_queue = (unsigned long long*)(d_totals + 2 * nt);
+    GVA_CUDA_B(cudaMemcpyAsync(d_desc, descs, desc_bytes, cudaMemcpyHostToDevice, s));
+    GVA_CUDA_B(cudaMemcpyAsync(d_block0, h_block0, (nt + 1) * 8, cudaMemcpyHostToDevice, s));
 
-    uint64_t rounds = 0, splits = 0, launches = 0;
-    std::vector<uint64_t> block0, totals;
-    while (!active.empty() && status == GVA_OK) {
-        // steps that cannot match (label or partition absent) end their task
-        active.erase(std::remove_if(active.begin(), active.end(),
-                                    [&](const Task& t) { return nodes[t.node].step.always_empty != 0; }),
-                     active.end());
-        if (active.empty()) break;
-        ++rounds;
-        const int nt = (int)active.size();
-        // pinned staging: descs | block0 | totals | outs
-        const size_t desc_bytes = (size_t)nt * sizeof(TaskDesc);
-        const size_t small_words = (size_t)(nt + 1) + nt + nt + 1;
-        char* h = stg.get(desc_bytes + small_words * 8);
-        if (!h) {
-            status = fail(GVA_ERR_NOMEM, "pinned staging allocation failed");
-            break;
-        }
-        TaskDesc* descs = (TaskDesc*)h;
-        uint64_t* h_block0 = (uint64_t*)(h + desc_bytes);
-        uint64_t* h_totals = h_block0 + (nt + 1);
-        uint32_t** h_outs = (uint32_t**)(h_totals + nt);
-        block0.assign(nt + 1, 0);
-        uint32_t kmax = 1, eqmax = 0;
-        double cbytes = 0;
-        for (int t = 0; t < nt; ++t) {
-            const Task& tk = active[t];
-            const Node& nd = nodes[tk.node];
-            const Step& st = nd.step;
-            TaskDesc& d = descs[t];
-            memset(&d, 0, sizeof d);
-            d.kind = st.kind;
-            d.mode = MODE_WRITE;
-            if (nd.children.empty()) d.mode = MODE_COUNT;
-            if (per_graph && !nd.terminal.empty()) {
-                d.mode = nd.children.empty() ? MODE_COUNT_GRAPHS : MODE_WRITE_AND_GRAPHS;
-                d.query = (uint32_t)nd.terminal[0];
-            }
-            d.block0 = block0[t];
-            const DevPart& P = db.parts[st.part - 1];
-            if (st.kind == STEP_EXT) {
-                ExtArgs& a = d.e;
-                a.in = tk.in;
-                a.nrows = tk.rows;
-                a.off = P.off;
-                a.adj = P.adj;
-                a.k = st.width_in;
-                a.L = db.L;
-                a.lab = st.label;
-                a.src_col = st.src_col;
-                a.bound_col = st.bound_col;
-                a.bound_incl = st.bound_inclusive;
-                a.n_eq = st.n_eq;
-                for (uint32_t i = 0; i < st.n_eq; ++i) a.eq_cols[i] = st.eq_cols[i];
-                eqmax = std::max(eqmax, st.n_eq);
-                a.n_chk = st.n_chk;
-                for (uint32_t i = 0; i < st.n_chk; ++i) {
-                    a.chk_col[i] = st.chk_col[i];
-                    a.chk_dir[i] = st.chk_dir[i];
-                    a.chk_lab[i] = st.chk_lab[i];
-                    a.chk_off[i] = db.parts[st.chk_part[i] - 1].off;
-                    a.chk_adj[i] = db.parts[st.chk_part[i] - 1].adj;
-                }
-            } else {
-                RedArgs& a = d.r;
-                a.in = tk.in;
-                a.nrows = tk.rows;
-                a.off = P.off;
-                a.adj = P.adj;
-                a.k = st.width_in;
-                a.L = db.L;
-                a.n_pairs = st.n_pairs;
-                for (uint32_t i = 0; i < st.n_pairs; ++i) {
-                    a.rs[i] = st.rs_col[i];
-                    a.re[i] = st.re_col[i];
-                    a.rl[i] = st.re_label[i];
-                }
-            }
-            kmax = std::max(kmax, st.width_in);
-            block0[t + 1] = block0[t] + (tk.rows + kRowsPerBlock - 1) / kRowsPerBlock;
-            cbytes += (4.0 * st.width_in + 8.0 * (st.kind == STEP_EXT ? 1 : st.n_pairs)) * (double)tk.rows;
-        }
-        const uint64_t nb = block0[nt];
-        if (nb > 0x7fffffffull) {
-            status = fail(GVA_ERR_UNSUPPORTED, "round too large for one launch");
-            break;
-        }
-        std::copy(block0.begin(), block0.end(), h_block0);
-        if (!grow((void**)&d_desc, desc_cap, desc_bytes) || !grow((void**)&d_sums, sums_cap, (nb + 1) * 8) ||
-            !grow((void**)&d_small, small_cap, small_words * 8)) {
-            status = fail(GVA_ERR_NOMEM, "batch bookkeeping allocation failed");
-            break;
-        }
-        uint64_t* d_block0 = d_small;
-        uint64_t* d_totals = d_block0 + (nt + 1);
-        uint32_t** d_outs = (uint32_t**)(d_totals + nt);
-        unsigned long long* d_queue = (unsigned long long*)(d_totals + 2 * nt);
-        GVA_CUDA_B(cudaMemcpyAsync(d_desc, descs, desc_bytes, cudaMemcpyHostToDevice, s));
-        GVA_CUDA_B(cudaMemcpyAsync(d_block0, h_block0, (nt + 1) * 8, cudaMemcpyHostToDevice, s));
+    cudaEvent_t ev = nullptr;
+    if (pf) pf->begin(K_EXT_COUNT, cbytes, s, ev);
+    batch_count_kernel<<<(unsigned)nb, kThreads, 0, s>>>((const TaskDesc*)d_desc, d_block0, nt, d_sums, ctx);
+    if (pf) pf->end(ev, K_EXT_COUNT, cbytes, s);
+    if (pf) pf->begin(K_SCAN, 16.0 * nb, s, ev);
+    scan_block_sums_kernel<<<1, kScanThreads, 0, s>>>(d_sums, nb);
+    if (pf) pf->end(ev, K_SCAN, 16.0 * nb, s);
+    task_totals_kernel<<<(nt + 255) / 256, 256, 0, s>>>(d_block0, nt, d_sums, d_totals);
+    launches += 3;
+    g_batch_launches += 3;
+    GVA_CUDA_B(cudaGetLastError());
+    GVA_CUDA_B(cudaMemcpyAsync(h_totals, d_totals, nt * 8, cudaMemcpyDeviceToHost, s));
+    GVA_CUDA_B(cudaStreamSynchronize(s));
+    std::vector<uint64_t> totals(h_totals, h_totals + nt);
 
-        cudaEvent_t ev = nullptr;
-        if (prof) prof->begin(K_EXT_COUNT, cbytes, s, ev);
-        batch_count_kernel<<<(unsigned)nb, kThreads, 0, s>>>(d_desc, d_block0, nt, d_sums, ctx);
-        if (prof) prof->end(ev, K_EXT_COUNT, cbytes, s);
-        if (prof) prof->begin(K_SCAN, 16.0 * nb, s, ev);
-        scan_block_sums_kernel<<<1, kScanThreads, 0, s>>>(d_sums, nb);
-        if (prof) prof->end(ev, K_SCAN, 16.0 * nb, s);
-        task_totals_kernel<<<(nt + 255) / 256, 256, 0, s>>>(d_block0, nt, d_sums, d_totals);
-        launches += 3;
-        GVA_CUDA_B(cudaGetLastError());
-        GVA_CUDA_B(cudaMemcpyAsync(h_totals, d_totals, nt * 8, cudaMemcpyDeviceToHost, s));
-        GVA_CUDA_B(cudaStreamSynchronize(s));
-        totals.assign(h_totals, h_totals + nt);
-
-        // choose which tasks write this round: deepest first, within the budget
-        std::vector<int> order;
-        std::vector<Task> next;
-        for (int t = 0; t < nt; ++t) {
-            const Node& nd = nodes[active[t].node];
-            for (int q : nd.terminal) counts[q] += totals[t];
-            if (!nd.children.empty() && totals[t] > 0) order.push_back(t);
-        }
-        std::stable_sort(order.begin(), order.end(),
-                         [&](int a, int b) { return nodes[active[a].node].depth > nodes[active[b].node].depth; });
-        uint64_t used = 0;
-        std::vector<uint64_t> off_words(nt, 0);
-        std::vector<int> chosen;
-        for (int t : order) {
-            const Step& st = nodes[active[t].node].step;
-            const uint32_t w = st.kind == STEP_EXT ? st.width_in + 1 : st.width_in;
-            const uint64_t bytes = totals[t] * w * 4ull;
-            if (used + bytes <= budget) {
-                off_words[t] = used / 4;
-                used += (bytes + 15) & ~15ull;
-                chosen.push_back(t);
-            } else if (bytes > budget) {
-                // split the task's input rows; both halves retry next round
-                Task a = active[t], b = active[t];
-                const uint64_t half = a.rows / 2;
-                if (half == 0) {
-                    status = fail(GVA_ERR_NOMEM, "a single frontier row expands beyond the memory budget");
-                    break;
-                }
-                a.rows = half;
-                b.in = a.in + half * st.width_in;
-                b.rows = active[t].rows - half;
-                next.push_back(a);
-                next.push_back(b);
-                ++splits;
-            } else {
-                next.push_back(active[t]);  // fits alone: waits for the next round
-            }
-        }
-        if (status) break;
-        std::shared_ptr<DevBuf> buf;
-        if (used > 0) {
-            buf = std::make_shared<DevBuf>();
-            buf->s = s;
-            if (cudaMallocAsync(&buf->p, used, s) != cudaSuccess) {
-                buf->p = nullptr;
-                status = fail(GVA_ERR_NOMEM, "frontier allocation failed");
+    // choose which tasks write this round: deepest first, within the budget
+    std::vector<int> order;
+    std::vector<BTask> next;
+    std::vector<char> finished(nt, 0);
+    for (int t = 0; t < nt; ++t) {
+        const BNode& nd = nodes[active[t].node];
+        for (int q : nd.terminal) plans[q].count += totals[t];
+        if (!nd.children.empty() && totals[t] > 0)
+            order.push_back(t);
+        else
+            finished[t] = 1;
+    }
+    std::stable_sort(order.begin(), order.end(),
+                     [&](int a, int b) { return nodes[active[a].node].depth > nodes[active[b].node].depth; });
+    uint64_t used = 0;
+    std::vector<uint64_t> off_words(nt, 0);
+    std::vector<int> chosen;
+    int status = GVA_OK;
+    for (int t : order) {
+        const Step& st = nodes[active[t].node].step;
+        const uint32_t w = st.kind == STEP_EXT ? st.width_in + 1 : st.width_in;
+        const uint64_t bytes = totals[t] * w * 4ull;
+        if (used + bytes <= budget) {
+            off_words[t] = used / 4;
+            used += (bytes + 15) & ~15ull;
+            chosen.push_back(t);
+        } else if (bytes > budget) {
+            // split the task's input rows; both halves retry next round
+            BTask a = active[t], b = active[t];
+            const uint64_t half = a.rows / 2;
+            if (half == 0) {
+                status = fail(GVA_ERR_NOMEM, "a single frontier row expands beyond the memory budget");
                 break;
             }
-            double wbytes = 0;
-            for (int t = 0; t < nt; ++t) h_outs[t] = nullptr;
-            for (int t : chosen) {
-                h_outs[t] = (uint32_t*)buf->p + off_words[t];
-                const Step& st = nodes[active[t].node].step;
-                const double k = st.width_in;
-                wbytes += (4.0 * k + 8.0) * (double)active[t].rows +
-                          (st.kind == STEP_EXT ? (4.0 + 4.0 * (k + 1)) : 4.0 * k) * (double)totals[t];
-            }
-            GVA_CUDA_B(cudaMemcpyAsync(d_outs, h_outs, nt * sizeof(uint32_t*), cudaMemcpyHostToDevice, s));
-            GVA_CUDA_B(cudaMemsetAsync(d_queue, 0, 8, s));
-            const size_t smem = batch_smem_bytes_for(kmax, std::max(eqmax, 1u));
-            int per_sm = 1;
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_write_kernel, kThreads, smem);
-            const uint64_t grid = std::min<uint64_t>(nb, (uint64_t)std::max(per_sm, 1) * sms);
-            if (prof) prof->begin(K_EXT_WRITE, wbytes, s, ev);
-            batch_write_kernel<<<(unsigned)grid, kThreads, smem, s>>>(d_desc, d_block0, nt, nb, d_sums, d_outs,
-                                                                      d_queue);
-            if (prof) prof->end(ev, K_EXT_WRITE, wbytes, s);
-            launches += 1;
-            GVA_CUDA_B(cudaGetLastError());
-        }
-        for (int t : chosen)
-            for (int c : nodes[active[t].node].children) next.push_back({c, h_outs[t], totals[t], buf});
-        active.swap(next);
-        if (prof) {
-            GVA_CUDA_B(cudaStreamSynchronize(s));
-            prof->resolve();
+            a.rows = half;
+            b.in = a.in + half * st.width_in;
+            b.rows = active[t].rows - half;
+            for (int q : nodes[a.node].below) plans[q].live++;  // one task became two
+            next.push_back(a);
+            next.push_back(b);
+            ++splits;
+        } else {
+            next.push_back(active[t]);  // fits alone: waits for the next round
         }
     }
-    g_batch_launches += launches;
-    active.clear();  // releases frontier buffers (stream-ordered)
-
-    if (status == GVA_OK && per_graph) {
-        std::vector<uint32_t> bits((size_t)nq * ctx.words);
-        GVA_CUDA_B(cudaMemcpyAsync(bits.data(), ctx.graph_bits, bits.size() * 4, cudaMemcpyDeviceToHost, s));
-        if (graph_counts_host)
-            GVA_CUDA_B(cudaMemcpyAsync(graph_counts_host, ctx.graph_counts, (size_t)nq * G * 8, cudaMemcpyDeviceToHost, s));
+    if (status) return status;
+    std::shared_ptr<void> buf;
+    if (used > 0) {
+        void* p = nullptr;
+        if (cudaMallocAsync(&p, used, s) != cudaSuccess) return fail(GVA_ERR_NOMEM, "frontier allocation failed");
+        cudaStream_t ss = s;
+        buf = std::shared_ptr<void>(p, [ss](void* q) { cudaFreeAsync(q, ss); });
+        double wbytes = 0;
+        for (int t = 0; t < nt; ++t) h_outs[t] = nullptr;
+        for (int t : chosen) {
+            h_outs[t] = (uint32_t*)p + off_words[t];
+            const Step& st = nodes[active[t].node].step;
+            const double k = st.width_in;
+            wbytes += (4.0 * k + 8.0) * (double)active[t].rows +
+                      (st.kind == STEP_EXT ? (4.0 + 4.0 * (k + 1)) : 4.0 * k) * (double)totals[t];
+        }
+        GVA_CUDA_B(cudaMemcpyAsync(d_outs, h_outs, nt * sizeof(uint32_t*), cudaMemcpyHostToDevice, s));
+        GVA_CUDA_B(cudaMemsetAsync(d_queue, 0, 8, s));
+        const size_t smem = batch_smem_bytes_for(kmax, std::max(eqmax, 1u));
+        int per_sm = 1;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_write_kernel, kThreads, smem);
+        const uint64_t grid = std::min<uint64_t>(nb, (uint64_t)std::max(per_sm, 1) * sms);
+        if (pf) pf->begin(K_EXT_WRITE, wbytes, s, ev);
+        batch_write_kernel<<<(unsigned)grid, kThreads, smem, s>>>((const TaskDesc*)d_desc, d_block0, nt, nb, d_sums, d_outs,
+                                                                  d_queue);
+        if (pf) pf->end(ev, K_EXT_WRITE, wbytes, s);
+        launches += 1;
+        g_batch_launches += 1;
+        GVA_CUDA_B(cudaGetLastError());
+    }
+    std::vector<int> ended;
+    for (int t = 0; t < nt; ++t)
+        if (finished[t]) ended.push_back(active[t].node);
+    for (int t : chosen) {
+        for (int c : nodes[active[t].node].children) {
+            for (int q : nodes[c].below) plans[q].live++;
+            next.push_back({c, h_outs[t], totals[t], buf});
+        }
+        ended.push_back(active[t].node);
+    }
+    active.swap(next);
+    for (int nd : ended) end_task(nd);
+    if (pf) {
         GVA_CUDA_B(cudaStreamSynchronize(s));
-        for (const Node& nd : nodes) {  // identical plans share the first one's results
-            for (size_t i = 1; i < nd.terminal.size(); ++i) {
-                const int q0 = nd.terminal[0], q = nd.terminal[i];
-                std::copy(bits.begin() + (size_t)q0 * ctx.words, bits.begin() + (size_t)(q0 + 1) * ctx.words,
-                          bits.begin() + (size_t)q * ctx.words);
+        pf->resolve();
+        for (int i = 0; i < K_NUM; ++i) {
+            kstat[i].launches += pf->stat[i].launches;
+            kstat[i].ms += pf->stat[i].ms;
+            kstat[i].bytes += pf->stat[i].bytes;
+        }
+    }
+    return GVA_OK;
+}
+
+std::vector<int> BatchSession::take_completed() {
+    std::vector<int> out;
+    out.swap(completed);
+    return out;
+}
+
+int BatchSession::read_support(int q, uint32_t* support, uint64_t* graph_counts_host) {
+    // plans ending on the same node share the first one's slot
+    const int q0 = nodes[plans[q].terminal].terminal[0];
+    const int slot = plans[q0].slot;
+    if (support) {
+        std::vector<uint32_t> bits(ctx_words);
+        GVA_CUDA_B(cudaMemcpyAsync(bits.data(), graph_bits_dev() + (size_t)slot * ctx_words, ctx_words * 4,
+                                   cudaMemcpyDeviceToHost, s));
+        GVA_CUDA_B(cudaStreamSynchronize(s));
+        uint32_t c = 0;
+        for (uint32_t w : bits) c += (uint32_t)__builtin_popcount(w);
+        *support = c;
+    }
+    if (graph_counts_host && want_graph_counts) {
+        GVA_CUDA_B(cudaMemcpyAsync(graph_counts_host, graph_counts_dev() + (size_t)slot * db.num_graphs,
+                                   (size_t)db.num_graphs * 8, cudaMemcpyDeviceToHost, s));
+        GVA_CUDA_B(cudaStreamSynchronize(s));
+    }
+    return GVA_OK;
+}
+
+void BatchSession::release(int q) {
+    // a slot is recycled once every plan sharing it is released
+    PlanRec& p = plans[q];
+    if (p.released) return;
+    p.released = true;
+    if (p.slot < 0) return;
+    const std::vector<int>& peers = nodes[p.terminal].terminal;
+    for (int o : peers)
+        if (!plans[o].released) return;
+    for (int o : peers) {
+        const int sl = plans[o].slot;
+        if (sl < 0) continue;
+        if (want_graph_counts)
+            cudaMemsetAsync(graph_counts_dev() + (size_t)sl * db.num_graphs, 0, (size_t)db.num_graphs * 8, s);
+        cudaMemsetAsync(graph_bits_dev() + (size_t)sl * ctx_words, 0, (size_t)ctx_words * 4, s);
+        free_slots.push_back(sl);
+        plans[o].slot = -1;
+    }
+}
+
+int run_batch(DevDB& db, const std::vector<std::vector<Step>>& steps, cudaStream_t s, uint64_t budget,
+              const uint32_t* vgraph, uint32_t G, uint64_t* counts, uint64_t* graph_counts_host,
+              uint32_t* support_host, bool profile, BatchStats* stats) {
+    (void)vgraph;
+    (void)G;
+    GVA_CUDA_B(cudaSetDevice(db.device));
+    const int nq = (int)steps.size();
+    for (int q = 0; q < nq; ++q) counts[q] = 0;
+    if (nq == 0) return GVA_OK;
+    const bool per_graph = graph_counts_host || support_host;
+    static thread_local cudaEvent_t tev[64][2];
+    const int dev = db.device;
+    if (dev < 0 || dev >= 64) return fail(GVA_ERR_ARG, "device index out of range");
+    if (!tev[dev][0]) {
+        GVA_CUDA_B(cudaEventCreate(&tev[dev][0]));
+        GVA_CUDA_B(cudaEventCreate(&tev[dev][1]));
+    }
+    GVA_CUDA_B(cudaEventRecord(tev[dev][0], s));
+    int rc;
+    {
+        BatchSession ses(db, s, budget, per_graph ? (uint32_t)nq : 0, graph_counts_host != nullptr, profile);
+        rc = ses.init();
+        std::vector<int> ids;
+        if (!rc) rc = ses.submit(steps, {}, &ids);
+        while (!rc && !ses.idle()) rc = ses.round();
+        if (!rc) {
+            for (int q = 0; q < nq; ++q) counts[q] = ses.plan(ids[q]).count;
+            if (per_graph) {
+                // bulk read of every slot, then identical plans copy their first one's results
+                const uint32_t words = ses.words();
+                std::vector<uint32_t> bits((size_t)nq * words);
+                cudaMemcpyAsync(bits.data(), ses.graph_bits_dev(), bits.size() * 4, cudaMemcpyDeviceToHost, s);
                 if (graph_counts_host)
-                    std::copy(graph_counts_host + (size_t)q0 * G, graph_counts_host + (size_t)(q0 + 1) * G,
-                              graph_counts_host + (size_t)q * G);
+                    cudaMemcpyAsync(graph_counts_host, ses.graph_counts_dev(), (size_t)nq * db.num_graphs * 8,
+                                    cudaMemcpyDeviceToHost, s);
+                rc = cudaStreamSynchronize(s) == cudaSuccess ? GVA_OK : fail(GVA_ERR_CUDA, "result read-back failed");
+                for (int q = 0; q < nq && !rc; ++q) {
+                    const int q0 = ses.first_peer(ids[q]);
+                    const int sl = ses.plan(q0).slot, own = ses.plan(ids[q]).slot;
+                    if (sl != own) {
+                        std::copy(bits.begin() + (size_t)sl * words, bits.begin() + (size_t)(sl + 1) * words,
+                                  bits.begin() + (size_t)own * words);
+                        if (graph_counts_host)
+                            std::copy(graph_counts_host + (size_t)sl * db.num_graphs,
+                                      graph_counts_host + (size_t)(sl + 1) * db.num_graphs,
+                                      graph_counts_host + (size_t)own * db.num_graphs);
+                    }
+                }
+                if (support_host && !rc)
+                    for (int q = 0; q < nq; ++q) {
+                        const int own = ses.plan(ids[q]).slot;
+                        uint32_t c = 0;
+                        for (uint32_t w = 0; w < words; ++w) c += (uint32_t)__builtin_popcount(bits[(size_t)own * words + w]);
+                        support_host[q] = c;
+                    }
             }
         }
-        if (support_host) {
-            for (int q = 0; q < nq; ++q) {
-                uint32_t c = 0;
-                for (uint32_t w = 0; w < ctx.words; ++w) c += (uint32_t)__builtin_popcount(bits[(size_t)q * ctx.words + w]);
-                support_host[q] = c;
-            }
+        if (stats) {
+            stats->rounds = ses.rounds;
+            stats->splits = ses.splits;
+            stats->launches = ses.launches;
+            stats->nodes = ses.num_nodes();
+            for (int i = 0; i < K_NUM; ++i) stats->kstat[i] = ses.kstat[i];
         }
     }
-    if (acc) cudaFreeAsync(acc, s);
-    for (void* p : {(void*)d_desc, (void*)d_sums, (void*)d_small})
-        if (p) cudaFreeAsync(p, s);
-    cudaEventRecord(ev1, s);
-    cudaEventSynchronize(ev1);
+    cudaEventRecord(tev[dev][1], s);
+    cudaEventSynchronize(tev[dev][1]);
     float ms = 0.f;
-    cudaEventElapsedTime(&ms, ev0, ev1);
-    if (stats) {
-        stats->gpu_ms = ms;
-        stats->rounds = rounds;
-        stats->splits = splits;
-        stats->launches = launches;
-        stats->nodes = nodes.size();
-        if (prof) {
-            prof->resolve();
-            for (int i = 0; i < K_NUM; ++i) stats->kstat[i] = prof->stat[i];
-        }
-    }
-    return status;
+    cudaEventElapsedTime(&ms, tev[dev][0], tev[dev][1]);
+    if (stats) stats->gpu_ms = ms;
+    return rc;
 }
 
 int set_graph_ids(DevDB& db, const uint64_t* first, uint32_t num_graphs) {

@@ -31,6 +31,11 @@ struct gva_plan {
 struct gva_result {
     MatchResult r;
 };
+struct gva_session {
+    BatchSession* ses = nullptr;
+    gva_db* db = nullptr;
+    std::vector<int> ready;  // completed plans not yet polled
+};
 struct gva_mine_result {
     std::vector<MinedPattern> pats;
     MineStats stats;
@@ -389,6 +394,67 @@ int gva_mine_kernel_stats(const gva_mine_result* res, gva_kernel_stat* out, int 
 }
 
 void gva_mine_free(gva_mine_result* res) { delete res; }
+
+int gva_session_create(gva_db* db, void* stream, uint64_t budget_bytes, uint32_t support_slots, gva_session** out) {
+    if (!db || !out) return fail(GVA_ERR_ARG, "null argument");
+    *out = nullptr;
+    gva_session* h = new gva_session();
+    h->db = db;
+    h->ses = new BatchSession(*db->dev, (cudaStream_t)stream, budget_bytes, support_slots, false, false);
+    int st = h->ses->init();
+    if (st) {
+        delete h->ses;
+        delete h;
+        return st;
+    }
+    *out = h;
+    return GVA_OK;
+}
+
+int gva_session_submit(gva_session* s, const gva_plan* const* plans, const uint64_t* tags, int n) {
+    if (!s || (n > 0 && !plans)) return fail(GVA_ERR_ARG, "null argument");
+    std::vector<std::vector<Step>> steps(n);
+    std::vector<uint64_t> tg(n);
+    for (int i = 0; i < n; ++i) {
+        if (!plans[i]) return fail(GVA_ERR_ARG, "null plan");
+        int st = lower_plan(plans[i]->plan, s->db->dev->meta, steps[i], true);
+        if (st) return st;
+        tg[i] = tags ? tags[i] : (uint64_t)i;
+    }
+    return s->ses->submit(steps, tg, nullptr);
+}
+
+int gva_session_round(gva_session* s, int* active_tasks) {
+    if (!s) return fail(GVA_ERR_ARG, "null argument");
+    int st = s->ses->round();
+    for (int q : s->ses->take_completed()) s->ready.push_back(q);
+    if (active_tasks) *active_tasks = (int)s->ses->num_active();
+    return st;
+}
+
+int gva_session_poll(gva_session* s, uint64_t* tags, uint64_t* counts, uint32_t* supports, int cap) {
+    if (!s) return -1;
+    int n = 0;
+    while (n < cap && !s->ready.empty()) {
+        const int q = s->ready.front();
+        const auto& p = s->ses->plan(q);
+        if (tags) tags[n] = p.tag;
+        if (counts) counts[n] = p.count;
+        uint32_t sup = 0;
+        if (supports && s->ses->words() > 0 && s->ses->read_support(q, &sup, nullptr)) return -1;
+        if (supports) supports[n] = sup;
+        s->ses->release(q);
+        s->ready.erase(s->ready.begin());
+        ++n;
+    }
+    return n;
+}
+
+void gva_session_free(gva_session* s) {
+    if (!s) return;
+    delete s->ses;
+    delete s;
+}
 
 int gva_plan_num_steps(const gva_plan* plan, const gva_db* db) {
     if (!plan || !db) return -1;

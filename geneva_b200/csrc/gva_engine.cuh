@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <memory>
 #include <string>
 #include <vector>
 
@@ -88,6 +89,90 @@ int run_batch(DevDB& db, const std::vector<std::vector<Step>>& steps, cudaStream
               const uint32_t* vgraph, uint32_t G, uint64_t* counts, uint64_t* graph_counts_host,
               uint32_t* support_host, bool profile, BatchStats* stats);
 uint64_t batch_kernel_launches();
+
+// Pinned host staging, grown on demand.
+struct Staging {
+    char* p = nullptr;
+    size_t cap = 0;
+    char* get(size_t need);
+    ~Staging();
+};
+
+// Persistent batched engine (gva_batch.cu).  Plans are submitted in waves;
+// round() advances every active task one step; completed plans are reported
+// by take_completed().  Per-graph results need slots > 0 (one per live plan).
+class BatchSession {
+public:
+    struct BNode {
+        Step step;
+        int depth = 0;
+        std::vector<int> children;
+        std::vector<int> terminal;  // plans whose last step is this node
+        std::vector<int> below;     // plans whose path passes through this node
+    };
+    struct BTask {
+        int node;
+        const uint32_t* in;  // frontier slice
+        uint64_t rows;
+        std::shared_ptr<void> owner;
+    };
+    struct PlanRec {
+        uint64_t tag = 0;
+        int slot = -1;
+        int terminal = -1;
+        uint64_t count = 0;
+        int live = 0;
+        bool done = false;
+        bool released = false;
+    };
+
+    BatchSession(DevDB& db, cudaStream_t s, uint64_t budget, uint32_t slots, bool graph_counts, bool profile);
+    ~BatchSession();
+    int init();
+    int submit(const std::vector<std::vector<Step>>& steps, const std::vector<uint64_t>& tags, std::vector<int>* ids);
+    int round();
+    bool idle() const { return active.empty(); }
+    std::vector<int> take_completed();
+    const PlanRec& plan(int q) const { return plans[q]; }
+    int first_peer(int q) const { return nodes[plans[q].terminal].terminal[0]; }
+    int read_support(int q, uint32_t* support, uint64_t* graph_counts_host);
+    void release(int q);
+    size_t num_nodes() const { return nodes.size(); }
+    size_t num_active() const { return active.size(); }
+    uint32_t words() const { return ctx_words; }
+    uint64_t* graph_counts_dev() const;
+    uint32_t* graph_bits_dev() const;
+
+    uint64_t rounds = 0, splits = 0, launches = 0;
+    KernelStat kstat[K_NUM];
+
+private:
+    void add_task(int node, const uint32_t* in, uint64_t rows, std::shared_ptr<void> owner);
+    void end_task(int node);
+
+    DevDB& db;
+    cudaStream_t s;
+    uint64_t budget;
+    uint32_t nslots;
+    bool want_graph_counts;
+    bool profile;
+    bool per_graph = false;
+    uint32_t ctx_words = 0;
+    int sms = 148;
+    void* acc = nullptr;
+    std::vector<int> free_slots;
+    std::vector<BNode> nodes;
+    std::vector<PlanRec> plans;
+    std::vector<BTask> active;
+    std::vector<int> completed;
+    Staging staging;
+    void* d_desc = nullptr;  // task descriptors (layout private to gva_batch.cu)
+    size_t desc_cap = 0;
+    uint64_t* d_sums = nullptr;
+    size_t sums_cap = 0;
+    uint64_t* d_small = nullptr;
+    size_t small_cap = 0;
+};
 int set_graph_ids(DevDB& db, const uint64_t* first, uint32_t num_graphs);
 
 struct MinedPattern {

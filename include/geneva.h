@@ -176,6 +176,25 @@ int gva_db_set_graphs(gva_db* db, const uint64_t* first, uint32_t num_graphs);
 int gva_batch_count(gva_db* db, const gva_plan* const* plans, int nplans, const gva_batch_opts* opts,
                     uint64_t* counts, uint64_t* graph_counts, uint32_t* graph_support, gva_batch_stats* stats);
 
+/* ---- serving: a persistent batch -------------------------------------------
+ * The batched engine kept open: plans may be submitted at any time and join
+ * the running work at the next round (continuous batching); each round
+ * advances every active task one step; finished plans are polled.  Replaces
+ * nothing in the reference (it serves one query per process). */
+typedef struct gva_session gva_session;
+
+/* support_slots > 0 enables per-plan supporting-graph counts (needs
+ * gva_db_set_graphs); it bounds the number of plans in flight. */
+int gva_session_create(gva_db* db, void* stream, uint64_t budget_bytes, uint32_t support_slots, gva_session** out);
+/* tags are returned by gva_session_poll with the plan's results. */
+int gva_session_submit(gva_session* s, const gva_plan* const* plans, const uint64_t* tags, int n);
+/* One round; *active_tasks receives the tasks left (0 = idle). */
+int gva_session_round(gva_session* s, int* active_tasks);
+/* Up to cap finished plans: tag, embedding count, supporting graphs (0 when
+ * support_slots == 0).  Returns how many were written. */
+int gva_session_poll(gva_session* s, uint64_t* tags, uint64_t* counts, uint32_t* supports, int cap);
+void gva_session_free(gva_session* s);
+
 /* ---- mining layer (graph databases) ------------------------------------------
  * Frequent connected patterns of up to max_edges edges whose support (graphs
  * holding at least one embedding) is at least min_support.  Level-wise growth
