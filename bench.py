@@ -396,8 +396,8 @@ def mine_bench(args, rank, world, local, dist, torch, gv, workloads, shard):
                    "candidates_per_step": cands // max(args.steps, 1), "frequent_patterns": frequent,
                    "l2": "flushed between steps (512 MiB write)",
                    "parallelism": f"graph database sharded over {world} rank(s); per-level support all-reduce"},
-        "mining": {k: stats[k] for k in ("levels", "candidates", "frequent", "pruned", "gpu_ms", "host_ms", "gen_ms",
-                                         "plan_ms")},
+        "mining": dict({k: stats[k] for k in ("levels", "candidates", "frequent", "pruned", "gpu_ms", "host_ms",
+                                              "gen_ms", "plan_ms", "eval_ms", "merge_ms")}, host_cpus=os.cpu_count()),
         "plain": {"sample": f"{len(sample)} seeded 2-7 vertex patterns sampled from the database",
                   "batched_embeddings_per_s": int(counts.sum()) / t_batch,
                   "plain_embeddings_per_s": plain_rows / t_plain,

@@ -23,6 +23,7 @@
 #include <cstring>
 #include <memory>
 #include <map>
+#include <unordered_map>
 #include <numeric>
 #include <string>
 #include <vector>
@@ -78,10 +79,35 @@ __device__ __forceinline__ int find_task(const uint64_t* __restrict__ block0, in
     return lo;
 }
 
+// Per-round task reference: the step parameters live in a per-node
+// descriptor uploaded once per submitted wave; a round uploads only these.
+struct TaskRef {
+    uint32_t node;
+    uint32_t pad;
+    uint64_t block0;
+    const uint32_t* in;
+    uint64_t nrows;
+};
+
 __device__ __forceinline__ void load_desc(TaskDesc& dst, const TaskDesc* src) {
     const uint32_t* s = reinterpret_cast<const uint32_t*>(src);
     uint32_t* d = reinterpret_cast<uint32_t*>(&dst);
     for (int i = threadIdx.x; i < (int)(sizeof(TaskDesc) / 4); i += blockDim.x) d[i] = s[i];
+}
+
+// Descriptor of task t: its node's parameters patched with the task's frontier
+// slice (ExtArgs and RedArgs both start with `in`, `nrows`).
+__device__ __forceinline__ void load_task(TaskDesc& d, const TaskDesc* __restrict__ nodes,
+                                          const TaskRef* __restrict__ refs, int t) {
+    const TaskRef r = refs[t];
+    load_desc(d, nodes + r.node);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        d.block0 = r.block0;
+        d.e.in = r.in;
+        d.e.nrows = r.nrows;
+    }
+    __syncthreads();
 }
 
 // Per-(query, graph) accounting of a final-step row: lanes of a warp whose
@@ -103,13 +129,12 @@ __device__ __forceinline__ void add_graph_count(const BatchCtx& c, uint32_t quer
 }
 
 __global__ void __launch_bounds__(kThreads)
-batch_count_kernel(const TaskDesc* __restrict__ tasks, const uint64_t* __restrict__ block0, int ntasks,
-                   uint64_t* __restrict__ block_sums, BatchCtx ctx) {
+batch_count_kernel(const TaskDesc* __restrict__ nodes, const TaskRef* __restrict__ refs,
+                   const uint64_t* __restrict__ block0, int ntasks, uint64_t* __restrict__ block_sums, BatchCtx ctx) {
     __shared__ TaskDesc d;
     const uint64_t b = blockIdx.x;
     const int t = find_task(block0, ntasks, b);
-    load_desc(d, tasks + t);
-    __syncthreads();
+    load_task(d, nodes, refs, t);
     const uint64_t r = (b - d.block0) * kRowsPerBlock + threadIdx.x;
     uint32_t c = 0;
     uint32_t first = 0;
@@ -141,7 +166,8 @@ __global__ void task_totals_kernel(const uint64_t* __restrict__ block0, int ntas
 
 // Persistent: each CTA repeatedly takes the next 256-row item.
 __global__ void __launch_bounds__(kThreads)
-batch_write_kernel(const TaskDesc* __restrict__ tasks, const uint64_t* __restrict__ block0, int ntasks, uint64_t nblocks,
+batch_write_kernel(const TaskDesc* __restrict__ nodes, const TaskRef* __restrict__ refs,
+                   const uint64_t* __restrict__ block0, int ntasks, uint64_t nblocks,
                    const uint64_t* __restrict__ sums, uint32_t* __restrict__ const* __restrict__ task_out,
                    unsigned long long* __restrict__ queue) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -159,9 +185,8 @@ batch_write_kernel(const TaskDesc* __restrict__ tasks, const uint64_t* __restric
             __syncthreads();
             continue;
         }
-        load_desc(d, tasks + t);
         if (threadIdx.x == 0) base_s = sums[b] - sums[block0[t]];  // task-local output row of this item
-        __syncthreads();
+        load_task(d, nodes, refs, t);
         const uint64_t row0 = (b - d.block0) * kRowsPerBlock;
         const uint64_t out0 = base_s;
         if (d.kind == STEP_EXT && d.e.n_chk) {
@@ -306,35 +331,6 @@ size_t batch_smem_bytes_for(uint32_t kmax, uint32_t eqmax) {
 
 std::atomic<uint64_t> g_batch_launches{0};
 
-// Bytes that determine a step's output from its input (everything but phase_end).
-std::string step_key(const Step& st) {
-    std::string k;
-    auto put = [&](const void* p, size_t n) { k.append((const char*)p, n); };
-    put(&st.kind, sizeof st.kind);
-    put(&st.width_in, 4);
-    put(&st.part, 4);
-    put(&st.label, 4);
-    put(&st.always_empty, 4);
-    if (st.kind == STEP_EXT) {
-        put(&st.src_col, 4);
-        put(&st.bound_col, 4);
-        put(&st.bound_inclusive, 4);
-        put(&st.n_eq, 4);
-        put(st.eq_cols, st.n_eq);
-        put(&st.n_chk, 4);
-        put(st.chk_col, st.n_chk);
-        put(st.chk_dir, st.n_chk);
-        put(st.chk_part, 4 * st.n_chk);
-        put(st.chk_lab, 4 * st.n_chk);
-    } else if (st.kind == STEP_REDUCE) {
-        put(&st.n_pairs, 4);
-        put(st.rs_col, st.n_pairs);
-        put(st.re_col, st.n_pairs);
-        put(st.re_label, 4 * st.n_pairs);
-    }
-    return k;
-}
-
 }  // namespace
 
 uint64_t batch_kernel_launches() { return g_batch_launches.load(); }
@@ -367,7 +363,7 @@ BatchSession::BatchSession(DevDB& db_, cudaStream_t s_, uint64_t budget_, uint32
 BatchSession::~BatchSession() {
     cudaSetDevice(db.device);
     active.clear();
-    for (void* p : {(void*)d_desc, (void*)d_sums, (void*)d_small, acc})
+    for (void* p : {(void*)d_desc, (void*)d_sums, (void*)d_small, acc, d_nodes})
         if (p) cudaFreeAsync(p, s);
     cudaStreamSynchronize(s);
 }
@@ -420,11 +416,94 @@ void BatchSession::end_task(int node) {
     }
 }
 
+// Serialised step parameters (everything that decides a step's output from
+// its input) into buf; returns the length.
+size_t step_key_bytes(const Step& st, uint8_t* buf) {
+    size_t n = 0;
+    auto put = [&](const void* p, size_t k) {
+        memcpy(buf + n, p, k);
+        n += k;
+    };
+    put(&st.kind, sizeof st.kind);
+    put(&st.width_in, 4);
+    put(&st.part, 4);
+    put(&st.label, 4);
+    put(&st.always_empty, 4);
+    if (st.kind == STEP_EXT) {
+        put(&st.src_col, 4);
+        put(&st.bound_col, 4);
+        put(&st.bound_inclusive, 4);
+        put(&st.n_eq, 4);
+        put(st.eq_cols, st.n_eq);
+        put(&st.n_chk, 4);
+        put(st.chk_col, st.n_chk);
+        put(st.chk_dir, st.n_chk);
+        put(st.chk_part, 4 * st.n_chk);
+        put(st.chk_lab, 4 * st.n_chk);
+    } else if (st.kind == STEP_REDUCE) {
+        put(&st.n_pairs, 4);
+        put(st.rs_col, st.n_pairs);
+        put(st.re_col, st.n_pairs);
+        put(st.re_label, 4 * st.n_pairs);
+    }
+    return n;
+}
+
+void BatchSession::fill_node_desc(int id) {
+    const BNode& nd = nodes[id];
+    TaskDesc& d = *reinterpret_cast<TaskDesc*>(&node_desc[(size_t)id * sizeof(TaskDesc)]);
+    memset(&d, 0, sizeof d);
+    const Step& st = nd.step;
+    d.kind = st.kind;
+    d.mode = nd.children.empty() ? MODE_COUNT : MODE_WRITE;
+    if (per_graph && !nd.terminal.empty()) {
+        d.mode = nd.children.empty() ? MODE_COUNT_GRAPHS : MODE_WRITE_AND_GRAPHS;
+        d.query = (uint32_t)plans[nd.terminal[0]].slot;
+    }
+    if (st.kind == STEP_SEED || st.always_empty || st.part == 0) return;
+    const DevPart& P = db.parts[st.part - 1];
+    if (st.kind == STEP_EXT) {
+        ExtArgs& a = d.e;
+        a.off = P.off;
+        a.adj = P.adj;
+        a.k = st.width_in;
+        a.L = db.L;
+        a.lab = st.label;
+        a.src_col = st.src_col;
+        a.bound_col = st.bound_col;
+        a.bound_incl = st.bound_inclusive;
+        a.n_eq = st.n_eq;
+        for (uint32_t i = 0; i < st.n_eq; ++i) a.eq_cols[i] = st.eq_cols[i];
+        a.n_chk = st.n_chk;
+        for (uint32_t i = 0; i < st.n_chk; ++i) {
+            a.chk_col[i] = st.chk_col[i];
+            a.chk_dir[i] = st.chk_dir[i];
+            a.chk_lab[i] = st.chk_lab[i];
+            a.chk_off[i] = db.parts[st.chk_part[i] - 1].off;
+            a.chk_adj[i] = db.parts[st.chk_part[i] - 1].adj;
+        }
+    } else {
+        RedArgs& a = d.r;
+        a.off = P.off;
+        a.adj = P.adj;
+        a.k = st.width_in;
+        a.L = db.L;
+        a.n_pairs = st.n_pairs;
+        for (uint32_t i = 0; i < st.n_pairs; ++i) {
+            a.rs[i] = st.rs_col[i];
+            a.re[i] = st.re_col[i];
+            a.rl[i] = st.re_label[i];
+        }
+    }
+}
+
 int BatchSession::submit(const std::vector<std::vector<Step>>& steps, const std::vector<uint64_t>& tags,
                          std::vector<int>* ids) {
-    std::map<std::string, int> roots;
-    std::map<int, std::map<std::string, int>> kids;
-    const int first_plan = (int)plans.size();
+    // trie of this wave: (parent, step bytes) -> node, looked up by a 64-bit
+    // hash and confirmed by comparing the bytes
+    std::unordered_multimap<uint64_t, int> index;
+    const int first_node = (int)nodes.size();
+    uint8_t kb[512], kb2[512];
     for (size_t qi = 0; qi < steps.size(); ++qi) {
         const std::vector<Step>& st = steps[qi];
         if (st.size() < 2 || st[0].kind != STEP_SEED) return fail(GVA_ERR_ARG, "plan must start with a seed step");
@@ -440,17 +519,25 @@ int BatchSession::submit(const std::vector<std::vector<Step>>& steps, const std:
         if (ids) ids->push_back(q);
         int cur = -1;
         for (size_t i = 0; i < st.size(); ++i) {
-            const std::string key = step_key(st[i]);
-            auto& m = cur < 0 ? roots : kids[cur];
-            auto it = m.find(key);
-            int id;
-            if (it == m.end()) {
+            const size_t n = step_key_bytes(st[i], kb);
+            uint64_t h = 1469598103934665603ull ^ (uint64_t)(int64_t)cur;
+            for (size_t j = 0; j < n; ++j) h = (h ^ kb[j]) * 1099511628211ull;
+            int id = -1;
+            auto range = index.equal_range(h);
+            for (auto it = range.first; it != range.second && id < 0; ++it) {
+                const BNode& cand = nodes[it->second];
+                if (cand.parent != cur) continue;
+                if (step_key_bytes(cand.step, kb2) == n && memcmp(kb, kb2, n) == 0) id = it->second;
+            }
+            if (id < 0) {
                 id = (int)nodes.size();
-                nodes.push_back(BNode{st[i], (int)i, {}, {}, {}});
-                m[key] = id;
+                BNode nd;
+                nd.step = st[i];
+                nd.depth = (int)i;
+                nd.parent = cur;
+                nodes.push_back(std::move(nd));
+                index.emplace(h, id);
                 if (cur >= 0) nodes[cur].children.push_back(id);
-            } else {
-                id = it->second;
             }
             nodes[id].below.push_back(q);
             cur = id;
@@ -458,9 +545,32 @@ int BatchSession::submit(const std::vector<std::vector<Step>>& steps, const std:
         nodes[cur].terminal.push_back(q);
         plans[q].terminal = cur;
     }
+    // step parameters of the new nodes, uploaded once
+    node_desc.resize(nodes.size() * sizeof(TaskDesc));
+    for (int id = first_node; id < (int)nodes.size(); ++id) fill_node_desc(id);
+    const size_t need = nodes.size() * sizeof(TaskDesc);
+    if (need > node_cap) {
+        void* p = nullptr;
+        const size_t cap = std::max(need, node_cap * 2);
+        if (cudaMallocAsync(&p, cap, s) != cudaSuccess) return fail(GVA_ERR_NOMEM, "node descriptor allocation failed");
+        if (d_nodes && first_node > 0)
+            GVA_CUDA_B(cudaMemcpyAsync(p, d_nodes, (size_t)first_node * sizeof(TaskDesc), cudaMemcpyDeviceToDevice, s));
+        if (d_nodes) cudaFreeAsync(d_nodes, s);
+        d_nodes = p;
+        node_cap = cap;
+    }
+    const size_t off = (size_t)first_node * sizeof(TaskDesc);
+    if (need > off) {
+        char* h = staging_nodes.get(need - off);
+        if (!h) return fail(GVA_ERR_NOMEM, "pinned staging allocation failed");
+        memcpy(h, node_desc.data() + off, need - off);
+        GVA_CUDA_B(cudaMemcpyAsync((char*)d_nodes + off, h, need - off, cudaMemcpyHostToDevice, s));
+        GVA_CUDA_B(cudaStreamSynchronize(s));  // staging is reused by the next submit
+    }
     // seeds: the children of every seed node start from its vertex list
-    for (auto& kv : roots) {
-        const BNode& seed = nodes[kv.second];
+    for (int id = first_node; id < (int)nodes.size(); ++id) {
+        const BNode& seed = nodes[id];
+        if (seed.parent != -1) continue;
         uint64_t n = 0;
         if (!seed.step.always_empty) n = db.seed_off[seed.step.label + 1] - db.seed_off[seed.step.label];
         if (n == 0) {
@@ -472,7 +582,6 @@ int BatchSession::submit(const std::vector<std::vector<Step>>& steps, const std:
         }
         for (int c : seed.children) add_task(c, db.seed_verts + db.seed_off[seed.step.label], n, nullptr);
     }
-    (void)first_plan;
     return GVA_OK;
 }
 
@@ -499,11 +608,11 @@ int BatchSession::round() {
     ctx.graph_counts = graph_counts_dev();
     ctx.graph_bits = graph_bits_dev();
     const int nt = (int)active.size();
-    const size_t desc_bytes = (size_t)nt * sizeof(TaskDesc);
+    const size_t desc_bytes = (size_t)nt * sizeof(TaskRef);
     const size_t small_words = (size_t)(nt + 1) + nt + nt + 1;
     char* h = staging.get(desc_bytes + small_words * 8);
     if (!h) return fail(GVA_ERR_NOMEM, "pinned staging allocation failed");
-    TaskDesc* descs = (TaskDesc*)h;
+    TaskRef* refs = (TaskRef*)h;
     uint64_t* h_block0 = (uint64_t*)(h + desc_bytes);
     uint64_t* h_totals = h_block0 + (nt + 1);
     uint32_t** h_outs = (uint32_t**)(h_totals + nt);
@@ -512,57 +621,10 @@ int BatchSession::round() {
     double cbytes = 0;
     for (int t = 0; t < nt; ++t) {
         const BTask& tk = active[t];
-        const BNode& nd = nodes[tk.node];
-        const Step& st = nd.step;
-        TaskDesc& d = descs[t];
-        memset(&d, 0, sizeof d);
-        d.kind = st.kind;
-        d.mode = nd.children.empty() ? MODE_COUNT : MODE_WRITE;
-        if (per_graph && !nd.terminal.empty()) {
-            d.mode = nd.children.empty() ? MODE_COUNT_GRAPHS : MODE_WRITE_AND_GRAPHS;
-            d.query = (uint32_t)plans[nd.terminal[0]].slot;
-        }
-        d.block0 = block0[t];
-        const DevPart& P = db.parts[st.part - 1];
-        if (st.kind == STEP_EXT) {
-            ExtArgs& a = d.e;
-            a.in = tk.in;
-            a.nrows = tk.rows;
-            a.off = P.off;
-            a.adj = P.adj;
-            a.k = st.width_in;
-            a.L = db.L;
-            a.lab = st.label;
-            a.src_col = st.src_col;
-            a.bound_col = st.bound_col;
-            a.bound_incl = st.bound_inclusive;
-            a.n_eq = st.n_eq;
-            for (uint32_t i = 0; i < st.n_eq; ++i) a.eq_cols[i] = st.eq_cols[i];
-            eqmax = std::max(eqmax, st.n_eq);
-            a.n_chk = st.n_chk;
-            for (uint32_t i = 0; i < st.n_chk; ++i) {
-                a.chk_col[i] = st.chk_col[i];
-                a.chk_dir[i] = st.chk_dir[i];
-                a.chk_lab[i] = st.chk_lab[i];
-                a.chk_off[i] = db.parts[st.chk_part[i] - 1].off;
-                a.chk_adj[i] = db.parts[st.chk_part[i] - 1].adj;
-            }
-        } else {
-            RedArgs& a = d.r;
-            a.in = tk.in;
-            a.nrows = tk.rows;
-            a.off = P.off;
-            a.adj = P.adj;
-            a.k = st.width_in;
-            a.L = db.L;
-            a.n_pairs = st.n_pairs;
-            for (uint32_t i = 0; i < st.n_pairs; ++i) {
-                a.rs[i] = st.rs_col[i];
-                a.re[i] = st.re_col[i];
-                a.rl[i] = st.re_label[i];
-            }
-        }
+        const Step& st = nodes[tk.node].step;
+        refs[t] = TaskRef{(uint32_t)tk.node, 0u, block0[t], tk.in, tk.rows};
         kmax = std::max(kmax, st.width_in);
+        if (st.kind == STEP_EXT) eqmax = std::max(eqmax, st.n_eq);
         block0[t + 1] = block0[t] + (tk.rows + kRowsPerBlock - 1) / kRowsPerBlock;
         cbytes += (4.0 * st.width_in + 8.0 * (st.kind == STEP_EXT ? 1 : st.n_pairs)) * (double)tk.rows;
     }
@@ -588,12 +650,13 @@ int BatchSession::round() {
     uint64_t* d_totals = d_block0 + (nt + 1);
     uint32_t** d_outs = (uint32_t**)(d_totals + nt);
     unsigned long long* d_queue = (unsigned long long*)(d_totals + 2 * nt);
-    GVA_CUDA_B(cudaMemcpyAsync(d_desc, descs, desc_bytes, cudaMemcpyHostToDevice, s));
+    GVA_CUDA_B(cudaMemcpyAsync(d_desc, refs, desc_bytes, cudaMemcpyHostToDevice, s));
     GVA_CUDA_B(cudaMemcpyAsync(d_block0, h_block0, (nt + 1) * 8, cudaMemcpyHostToDevice, s));
 
     cudaEvent_t ev = nullptr;
     if (pf) pf->begin(K_EXT_COUNT, cbytes, s, ev);
-    batch_count_kernel<<<(unsigned)nb, kThreads, 0, s>>>((const TaskDesc*)d_desc, d_block0, nt, d_sums, ctx);
+    batch_count_kernel<<<(unsigned)nb, kThreads, 0, s>>>((const TaskDesc*)d_nodes, (const TaskRef*)d_desc, d_block0,
+                                                         nt, d_sums, ctx);
     if (pf) pf->end(ev, K_EXT_COUNT, cbytes, s);
     if (pf) pf->begin(K_SCAN, 16.0 * nb, s, ev);
     scan_block_sums_kernel<<<1, kScanThreads, 0, s>>>(d_sums, nb);
@@ -674,8 +737,8 @@ int BatchSession::round() {
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_write_kernel, kThreads, smem);
         const uint64_t grid = std::min<uint64_t>(nb, (uint64_t)std::max(per_sm, 1) * sms);
         if (pf) pf->begin(K_EXT_WRITE, wbytes, s, ev);
-        batch_write_kernel<<<(unsigned)grid, kThreads, smem, s>>>((const TaskDesc*)d_desc, d_block0, nt, nb, d_sums, d_outs,
-                                                                  d_queue);
+        batch_write_kernel<<<(unsigned)grid, kThreads, smem, s>>>((const TaskDesc*)d_nodes, (const TaskRef*)d_desc, d_block0,
+                                                                  nt, nb, d_sums, d_outs, d_queue);
         if (pf) pf->end(ev, K_EXT_WRITE, wbytes, s);
         launches += 1;
         g_batch_launches += 1;

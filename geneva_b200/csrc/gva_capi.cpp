@@ -378,6 +378,8 @@ int gva_mine_get_stats(const gva_mine_result* res, gva_mine_stats* out) {
     out->host_ms = res->stats.host_ms;
     out->gen_ms = res->stats.gen_ms;
     out->plan_ms = res->stats.plan_ms;
+    out->eval_ms = res->stats.eval_ms;
+    out->merge_ms = res->stats.merge_ms;
     return GVA_OK;
 }
 

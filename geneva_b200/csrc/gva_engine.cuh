@@ -106,6 +106,7 @@ public:
     struct BNode {
         Step step;
         int depth = 0;
+        int parent = -1;
         std::vector<int> children;
         std::vector<int> terminal;  // plans whose last step is this node
         std::vector<int> below;     // plans whose path passes through this node
@@ -148,6 +149,7 @@ public:
 
 private:
     void add_task(int node, const uint32_t* in, uint64_t rows, std::shared_ptr<void> owner);
+    void fill_node_desc(int id);
     void end_task(int node);
 
     DevDB& db;
@@ -165,8 +167,11 @@ private:
     std::vector<PlanRec> plans;
     std::vector<BTask> active;
     std::vector<int> completed;
-    Staging staging;
-    void* d_desc = nullptr;  // task descriptors (layout private to gva_batch.cu)
+    Staging staging, staging_nodes;
+    std::vector<char> node_desc;  // host copy of the per-node step descriptors
+    void* d_nodes = nullptr;      // device copy (layout private to gva_batch.cu)
+    size_t node_cap = 0;
+    void* d_desc = nullptr;  // per-round task references
     size_t desc_cap = 0;
     uint64_t* d_sums = nullptr;
     size_t sums_cap = 0;
@@ -184,7 +189,7 @@ struct MinedPattern {
 
 struct MineStats {
     uint64_t candidates = 0, frequent = 0, embeddings = 0, levels = 0, pruned = 0;
-    double gpu_ms = 0.0, host_ms = 0.0, gen_ms = 0.0, plan_ms = 0.0;
+    double gpu_ms = 0.0, host_ms = 0.0, gen_ms = 0.0, plan_ms = 0.0, eval_ms = 0.0, merge_ms = 0.0;
     KernelStat kstat[K_NUM];
 };
 

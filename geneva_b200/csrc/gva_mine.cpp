@@ -57,57 +57,68 @@ struct CodeHash {
 };
 
 // Canonical code: the lexicographically smallest (n, labels, upper-triangle
-// edge labels) over vertex orders that sort vertices by an invariant
-// (label, degree, sorted (edge label, neighbour label) list); only orders
-// within equal-invariant cells are tried.
+// edge labels) over vertex orders that sort vertices by an isomorphism-
+// invariant key (label, degree, hash of the sorted (edge label, neighbour
+// label) list); only orders within equal-key cells are tried.  Equal keys of
+// non-equivalent vertices only enlarge a cell, which costs time, not
+// correctness.  Work arrays live on the stack (patterns have <= 32 vertices).
 Code canonical(const Pattern& p, std::vector<uint32_t>* order_out = nullptr) {
     const uint32_t n = p.n;
-    std::vector<uint32_t> adj(n * n, 0);
-    for (auto& e : p.edges) adj[e[0] * n + e[1]] = adj[e[1] * n + e[0]] = e[2];
-    std::vector<std::vector<uint32_t>> inv(n);
+    uint32_t adj[GVA_MAX_QUERY_VERTICES][GVA_MAX_QUERY_VERTICES];
+    for (uint32_t i = 0; i < n; ++i)
+        for (uint32_t j = 0; j < n; ++j) adj[i][j] = 0;
+    for (auto& e : p.edges) adj[e[0]][e[1]] = adj[e[1]][e[0]] = e[2];
+    uint64_t key[GVA_MAX_QUERY_VERTICES];
     for (uint32_t v = 0; v < n; ++v) {
-        std::vector<uint32_t> nb;
+        uint64_t nb[GVA_MAX_QUERY_VERTICES];
+        uint32_t d = 0;
         for (uint32_t u = 0; u < n; ++u)
-            if (adj[v * n + u]) nb.push_back((adj[v * n + u] << 16) | p.vl[u]);
-        std::sort(nb.begin(), nb.end());
-        inv[v] = {p.vl[v], (uint32_t)nb.size()};
-        inv[v].insert(inv[v].end(), nb.begin(), nb.end());
+            if (adj[v][u]) nb[d++] = ((uint64_t)adj[v][u] << 32) | p.vl[u];
+        std::sort(nb, nb + d);
+        uint64_t h = 1469598103934665603ull;
+        for (uint32_t i = 0; i < d; ++i) h = (h ^ nb[i]) * 1099511628211ull;
+        key[v] = ((uint64_t)(p.vl[v] & 0xffffu) << 48) | ((uint64_t)d << 40) | (h & 0xffffffffffull);
     }
-    std::vector<uint32_t> ord(n);
+    uint32_t ord[GVA_MAX_QUERY_VERTICES];
     for (uint32_t i = 0; i < n; ++i) ord[i] = i;
-    std::sort(ord.begin(), ord.end(), [&](uint32_t a, uint32_t b) { return inv[a] < inv[b]; });
-    std::vector<std::pair<uint32_t, uint32_t>> cells;  // [begin, end)
+    std::sort(ord, ord + n, [&](uint32_t a, uint32_t b) { return key[a] != key[b] ? key[a] < key[b] : a < b; });
+    uint32_t cb[GVA_MAX_QUERY_VERTICES], ce[GVA_MAX_QUERY_VERTICES], nc = 0;  // cells [cb, ce)
     for (uint32_t i = 0; i < n;) {
         uint32_t j = i + 1;
-        while (j < n && inv[ord[j]] == inv[ord[i]]) ++j;
-        std::sort(ord.begin() + i, ord.begin() + j);
-        cells.push_back({i, j});
+        while (j < n && key[ord[j]] == key[ord[i]]) ++j;
+        cb[nc] = i;
+        ce[nc++] = j;
         i = j;
     }
-    Code best;
-    std::vector<uint32_t> best_ord;
-    Code cur(1 + n + n * (n - 1) / 2);
-    auto evaluate = [&]() {
-        cur[0] = n;
-        for (uint32_t i = 0; i < n; ++i) cur[1 + i] = p.vl[ord[i]];
-        size_t k = 1 + n;
-        for (uint32_t i = 0; i < n; ++i)
-            for (uint32_t j = i + 1; j < n; ++j) cur[k++] = adj[ord[i] * n + ord[j]];
-        if (best.empty() || cur < best) {
-            best = cur;
-            best_ord = ord;
-        }
-    };
-    // odometer over the product of within-cell permutations (each cell
-    // starts sorted; next_permutation wraps back to sorted and carries)
+    const size_t len = 1 + n + (size_t)n * (n - 1) / 2;
+    Code best(len), cur(len);
+    uint32_t best_ord[GVA_MAX_QUERY_VERTICES];
+    bool have = false;
     for (;;) {
-        evaluate();
-        int c = (int)cells.size() - 1;
+        // build the code, giving up as soon as it exceeds the best one
+        cur[0] = n;
+        int cmp = have ? 0 : -1;
+        size_t k = 1;
+        for (uint32_t i = 0; i < n && cmp <= 0; ++i, ++k) {
+            cur[k] = p.vl[ord[i]];
+            if (cmp == 0 && cur[k] != best[k]) cmp = cur[k] < best[k] ? -1 : 1;
+        }
+        for (uint32_t i = 0; i < n && cmp <= 0; ++i)
+            for (uint32_t j = i + 1; j < n && cmp <= 0; ++j, ++k) {
+                cur[k] = adj[ord[i]][ord[j]];
+                if (cmp == 0 && cur[k] != best[k]) cmp = cur[k] < best[k] ? -1 : 1;
+            }
+        if (cmp < 0) {
+            best.swap(cur);
+            for (uint32_t i = 0; i < n; ++i) best_ord[i] = ord[i];
+            have = true;
+        }
+        int c = (int)nc - 1;
         for (; c >= 0; --c)
-            if (std::next_permutation(ord.begin() + cells[c].first, ord.begin() + cells[c].second)) break;
+            if (std::next_permutation(ord + cb[c], ord + ce[c])) break;
         if (c < 0) break;
     }
-    if (order_out) *order_out = best_ord;
+    if (order_out) order_out->assign(best_ord, best_ord + n);
     return best;
 }
 
@@ -334,13 +345,17 @@ int run_mine(DevDB& db, cudaStream_t s, uint64_t budget, uint32_t max_edges, uin
             st.pruned += pruned[t];
             for (auto& x : found[t]) all.push_back(std::move(x));
         }
+        auto t_merge = std::chrono::steady_clock::now();
         std::sort(all.begin(), all.end(), [](const auto& a, const auto& b) { return a.first < b.first; });
         std::vector<Pattern> next;
         for (size_t i = 0; i < all.size(); ++i)
             if (i == 0 || all[i].first != all[i - 1].first) next.push_back(std::move(all[i].second));
         st.gen_ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_gen).count();
+        st.merge_ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_merge).count();
+        auto t_eval = std::chrono::steady_clock::now();
         rc = evaluate(next, sup, emb);
         if (rc) return rc;
+        st.eval_ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_eval).count();
         level.clear();
         level_codes.clear();
         for (size_t i = 0; i < next.size(); ++i) {

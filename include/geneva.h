@@ -229,6 +229,8 @@ typedef struct gva_mine_stats {
     double host_ms;      /* whole call, wall clock */
     double gen_ms;       /* candidate generation, dedupe and pruning (host threads) */
     double plan_ms;      /* planning and lowering of every candidate (host threads) */
+    double eval_ms;      /* matching of every candidate, host bookkeeping included */
+    double merge_ms;     /* merging and ordering the candidates of each level */
 } gva_mine_stats;
 
 typedef struct gva_mine_result gva_mine_result;
