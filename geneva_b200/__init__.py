@@ -23,7 +23,7 @@ from typing import List, Optional, Sequence
 import numpy as np
 
 __all__ = [
-    "GenevaError", "Database", "probe_graph", "batch_count", "kernel_launches", "mine", "MinedPattern", "Plan", "Result", "MODE_DV", "MODE_SV", "library", "library_path",
+    "GenevaError", "Database", "probe_graph", "convert_g", "batch_count", "kernel_launches", "mine", "MinedPattern", "Plan", "Result", "MODE_DV", "MODE_SV", "library", "library_path",
     "loadDataBase", "genMatchOrder", "genMatchOrderSingleV", "match", "gpumine", "gpumineSV",
 ]
 
@@ -125,6 +125,7 @@ def _declare(lib):
         "gva_step_scratch_bytes": (sz, [u64]),
         "gva_step_run": (i32, [vp, vp, i32, vp, u64, vp, u64, P(u64), vp, sz, vp]),
         "gva_db_set_graphs": (i32, [vp, vp, u32]),
+        "gva_convert_g": (i32, [cp, cp, cp, cp]),
         "gva_mine": (i32, [vp, P(_MineOpts), P(vp)]),
         "gva_mine_num_patterns": (i32, [vp]),
         "gva_mine_get": (i32, [vp, i32, P(u32), P(u32), P(u64)]),
@@ -207,6 +208,13 @@ class Database:
             self.close()
         except Exception:
             pass
+
+
+def convert_g(g_path: str, out_prefix: str) -> None:
+    """.g -> <out_prefix>.mygraph/.metadata/.reorder, as tools/genDatabase.cpp writes them."""
+    p = str(out_prefix)
+    _check(library().gva_convert_g(str(g_path).encode(), (p + ".mygraph").encode(), (p + ".metadata").encode(),
+                                   (p + ".reorder").encode()))
 
 
 def probe_graph(mygraph: str, metadata: str) -> dict:

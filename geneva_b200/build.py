@@ -26,7 +26,7 @@ NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompil
 CXX_FLAGS = ["-O2", "-std=c++17", "-fPIC", "-Wall", "-Wno-sign-compare", f"-I{ROOT / 'include'}"]
 
 CU_SOURCES = ["gva_engine.cu", "gva_batch.cu", "gva_static.cu"]
-CPP_SOURCES = ["gva_plan.cpp", "gva_graph.cpp", "gva_capi.cpp", "gva_mine.cpp"]
+CPP_SOURCES = ["gva_plan.cpp", "gva_graph.cpp", "gva_capi.cpp", "gva_mine.cpp", "gva_convert.cpp"]
 
 
 def nvcc() -> str:
@@ -83,6 +83,10 @@ def build(verbose: bool = False) -> Path:
     if _newer(so, objs):
         _run([nvcc(), *ARCH, "-shared", "-o", str(so), *map(str, objs), "-Xlinker", "-soname=libgeneva.so",
               "-lstdc++"])
+    conv = LIB / "gvaconvert"
+    if _newer(conv, [so, CSRC / "gva_convert_main.cpp", ROOT / "include" / "geneva.h"]):
+        _run([cxx, *CXX_FLAGS, str(CSRC / "gva_convert_main.cpp"), "-o", str(conv), f"-L{LIB}", "-lgeneva",
+              "-Wl,-rpath,$ORIGIN", "-lstdc++"])
     for name, mode in (("gpumine", 0), ("gpumineSV", 1)):
         exe = LIB / name
         if _newer(exe, [so, CSRC / "gva_cli.cpp", ROOT / "include" / "geneva.h"]):

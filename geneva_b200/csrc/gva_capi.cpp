@@ -167,6 +167,11 @@ void gva_db_free(gva_db* db) {
     delete db;
 }
 
+int gva_convert_g(const char* g_path, const char* mygraph_path, const char* metadata_path, const char* reorder_path) {
+    if (!g_path || !mygraph_path || !metadata_path || !reorder_path) return fail(GVA_ERR_ARG, "null argument");
+    return convert_g(g_path, mygraph_path, metadata_path, reorder_path);
+}
+
 int gva_plan_from_text(const char* query_text, int mode, gva_plan** out) {
     if (!out || !query_text) return fail(GVA_ERR_ARG, "null argument");
     *out = nullptr;

@@ -43,6 +43,10 @@ int load_mygraph(const std::string& mygraph, const std::string& metadata, HostGr
 int graph_from_edges(const uint32_t* vlabels, uint32_t max_id, const uint32_t* src, const uint32_t* dst,
                      const uint32_t* elabel, uint64_t ne, HostGraph& g);
 
+// .g -> .mygraph/.metadata/.reorder exactly as tools/genDatabase.cpp writes them.
+int convert_g(const std::string& g_path, const std::string& mygraph, const std::string& metadata,
+              const std::string& reorder);
+
 // ----------------------------------------------------------------- plan -----
 struct Phase {
     char type = 'E';                  // 'E' extension, 'R' reduction

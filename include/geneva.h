@@ -109,6 +109,12 @@ int gva_graph_probe(const char* mygraph_path, const char* metadata_path, gva_db_
 const char* gva_db_warnings(const gva_db* db);
 void gva_db_free(gva_db* db);
 
+/* Converts a .g file (`v id label`, then `e src dst label` lines) into the
+ * reference's database files, byte-identical to tools/genDatabase.cpp
+ * (vertex renumbering :259-413, index vertices :415-436, partition layout
+ * :451-580, .reorder text :826-846, .metadata :873-879).  Host-only. */
+int gva_convert_g(const char* g_path, const char* mygraph_path, const char* metadata_path, const char* reorder_path);
+
 /* ---- L2: planner ----------------------------------------------------------
  * Replaces genMatchOrder / genMatchOrderSingleV (src/genMatchOrderCPU.cpp:670-983,
  * src/genMatchOrderSingleV.cpp:678-1003): same phases, pair orientation,
