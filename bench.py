@@ -241,7 +241,7 @@ def serve_bench(args, local, torch, gv, workloads):
     gdb.set_graphs(db.first)
     G = len(db.first) - 1
     pool = workloads.sample_patterns(db, 512, 3, 10, seed=4242)
-    s_match, s_mine = torch.cuda.Stream(), torch.cuda.Stream()
+    s_match, s_mine = torch.cuda.Stream(priority=-1), torch.cuda.Stream()  # matching ahead of mining
     points = []
     for rate in [float(x) for x in args.rates.split(",")]:
         srv = Server(gdb, budget_bytes=150 << 30, match_stream=s_match.cuda_stream, mine_stream=s_mine.cuda_stream)
@@ -397,7 +397,8 @@ def mine_bench(args, rank, world, local, dist, torch, gv, workloads, shard):
                    "l2": "flushed between steps (512 MiB write)",
                    "parallelism": f"graph database sharded over {world} rank(s); per-level support all-reduce"},
         "mining": dict({k: stats[k] for k in ("levels", "candidates", "frequent", "pruned", "gpu_ms", "host_ms",
-                                              "gen_ms", "plan_ms", "eval_ms", "merge_ms")}, host_cpus=os.cpu_count()),
+                                              "gen_ms", "plan_ms", "eval_ms", "merge_ms", "submit_ms",
+                                              "round_host_ms", "wait_ms")}, host_cpus=os.cpu_count()),
         "plain": {"sample": f"{len(sample)} seeded 2-7 vertex patterns sampled from the database",
                   "batched_embeddings_per_s": int(counts.sum()) / t_batch,
                   "plain_embeddings_per_s": plain_rows / t_plain,

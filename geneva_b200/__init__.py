@@ -74,7 +74,8 @@ class _MineStats(ctypes.Structure):
     _fields_ = [("candidates", ctypes.c_uint64), ("frequent", ctypes.c_uint64), ("embeddings", ctypes.c_uint64),
                 ("levels", ctypes.c_uint64), ("pruned", ctypes.c_uint64), ("gpu_ms", ctypes.c_double),
                 ("host_ms", ctypes.c_double), ("gen_ms", ctypes.c_double), ("plan_ms", ctypes.c_double),
-                ("eval_ms", ctypes.c_double), ("merge_ms", ctypes.c_double)]
+                ("eval_ms", ctypes.c_double), ("merge_ms", ctypes.c_double), ("submit_ms", ctypes.c_double),
+                ("round_host_ms", ctypes.c_double), ("wait_ms", ctypes.c_double)]
 
 
 class _BatchOpts(ctypes.Structure):

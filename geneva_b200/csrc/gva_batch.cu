@@ -20,6 +20,7 @@
 
 #include <algorithm>
 #include <atomic>
+#include <chrono>
 #include <cstring>
 #include <memory>
 #include <map>
@@ -363,6 +364,7 @@ BatchSession::BatchSession(DevDB& db_, cudaStream_t s_, uint64_t budget_, uint32
 BatchSession::~BatchSession() {
     cudaSetDevice(db.device);
     active.clear();
+    if (staged) cudaEventDestroy(staged);
     for (void* p : {(void*)d_desc, (void*)d_sums, (void*)d_small, acc, d_nodes})
         if (p) cudaFreeAsync(p, s);
     cudaStreamSynchronize(s);
@@ -402,18 +404,28 @@ uint32_t* BatchSession::graph_bits_dev() const {
     return per_graph ? (uint32_t*)((char*)acc + (want_graph_counts ? (size_t)nslots * db.num_graphs * 8 : 0)) : nullptr;
 }
 
+// Plan completion: a node closes when its parent is closed and no task is
+// left at it (tasks only move down the trie, so none can arrive later);
+// closing a node completes the plans that end there and tries its children.
 void BatchSession::add_task(int node, const uint32_t* in, uint64_t rows, std::shared_ptr<void> owner) {
-    for (int q : nodes[node].below) plans[q].live++;
+    nodes[node].at++;
     active.push_back({node, in, rows, std::move(owner)});
 }
 
-void BatchSession::end_task(int node) {
-    for (int q : nodes[node].below) {
-        if (--plans[q].live == 0 && !plans[q].done) {
-            plans[q].done = true;
-            completed.push_back(q);
-        }
+void BatchSession::try_close(int n) {
+    BNode& nd = nodes[n];
+    if (nd.closed || nd.at != 0 || (nd.parent >= 0 && !nodes[nd.parent].closed)) return;
+    nd.closed = true;
+    for (int q = nd.first_term; q >= 0; q = plans[q].next_term) {
+        plans[q].done = true;
+        completed.push_back(q);
     }
+    for (int c = nd.first_child; c >= 0; c = nodes[c].next_sibling) try_close(c);
+}
+
+void BatchSession::finish_task(int node) {
+    nodes[node].at--;
+    try_close(node);
 }
 
 // Serialised step parameters (everything that decides a step's output from
@@ -449,16 +461,16 @@ size_t step_key_bytes(const Step& st, uint8_t* buf) {
     return n;
 }
 
-void BatchSession::fill_node_desc(int id) {
+void BatchSession::fill_node_desc(int id, void* out) const {
     const BNode& nd = nodes[id];
-    TaskDesc& d = *reinterpret_cast<TaskDesc*>(&node_desc[(size_t)id * sizeof(TaskDesc)]);
+    TaskDesc& d = *reinterpret_cast<TaskDesc*>(out);
     memset(&d, 0, sizeof d);
     const Step& st = nd.step;
     d.kind = st.kind;
-    d.mode = nd.children.empty() ? MODE_COUNT : MODE_WRITE;
-    if (per_graph && !nd.terminal.empty()) {
-        d.mode = nd.children.empty() ? MODE_COUNT_GRAPHS : MODE_WRITE_AND_GRAPHS;
-        d.query = (uint32_t)plans[nd.terminal[0]].slot;
+    d.mode = nd.first_child < 0 ? MODE_COUNT : MODE_WRITE;
+    if (per_graph && nd.first_term >= 0) {
+        d.mode = nd.first_child < 0 ? MODE_COUNT_GRAPHS : MODE_WRITE_AND_GRAPHS;
+        d.query = (uint32_t)plans[nd.first_term].slot;
     }
     if (st.kind == STEP_SEED || st.always_empty || st.part == 0) return;
     const DevPart& P = db.parts[st.part - 1];
@@ -499,9 +511,16 @@ void BatchSession::fill_node_desc(int id) {
 
 int BatchSession::submit(const std::vector<std::vector<Step>>& steps, const std::vector<uint64_t>& tags,
                          std::vector<int>* ids) {
+    const auto t_start = std::chrono::steady_clock::now();
+    struct Timer {
+        std::chrono::steady_clock::time_point t0;
+        double& acc;
+        ~Timer() { acc += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count(); }
+    } timer{t_start, submit_ms};
     // trie of this wave: (parent, step bytes) -> node, looked up by a 64-bit
     // hash and confirmed by comparing the bytes
     std::unordered_multimap<uint64_t, int> index;
+    index.reserve(steps.size() * 4);
     const int first_node = (int)nodes.size();
     uint8_t kb[512], kb2[512];
     for (size_t qi = 0; qi < steps.size(); ++qi) {
@@ -520,8 +539,13 @@ int BatchSession::submit(const std::vector<std::vector<Step>>& steps, const std:
         int cur = -1;
         for (size_t i = 0; i < st.size(); ++i) {
             const size_t n = step_key_bytes(st[i], kb);
-            uint64_t h = 1469598103934665603ull ^ (uint64_t)(int64_t)cur;
-            for (size_t j = 0; j < n; ++j) h = (h ^ kb[j]) * 1099511628211ull;
+            uint64_t h = 1469598103934665603ull ^ ((uint64_t)(int64_t)cur * 0x9e3779b97f4a7c15ull);
+            for (size_t j = 0; j + 8 <= n; j += 8) {
+                uint64_t w;
+                memcpy(&w, kb + j, 8);
+                h = (h ^ w) * 1099511628211ull;
+            }
+            for (size_t j = n & ~(size_t)7; j < n; ++j) h = (h ^ kb[j]) * 1099511628211ull;
             int id = -1;
             auto range = index.equal_range(h);
             for (auto it = range.first; it != range.second && id < 0; ++it) {
@@ -535,70 +559,70 @@ int BatchSession::submit(const std::vector<std::vector<Step>>& steps, const std:
                 nd.step = st[i];
                 nd.depth = (int)i;
                 nd.parent = cur;
-                nodes.push_back(std::move(nd));
+                if (cur >= 0) {
+                    nd.next_sibling = nodes[cur].first_child;
+                    nodes.push_back(nd);
+                    nodes[cur].first_child = id;
+                } else {
+                    nodes.push_back(nd);
+                }
                 index.emplace(h, id);
-                if (cur >= 0) nodes[cur].children.push_back(id);
             }
-            nodes[id].below.push_back(q);
             cur = id;
         }
-        nodes[cur].terminal.push_back(q);
         plans[q].terminal = cur;
-    }
-    // step parameters of the new nodes, uploaded once
-    node_desc.resize(nodes.size() * sizeof(TaskDesc));
-    for (int id = first_node; id < (int)nodes.size(); ++id) fill_node_desc(id);
-    const size_t need = nodes.size() * sizeof(TaskDesc);
-    if (need > node_cap) {
-        void* p = nullptr;
-        const size_t cap = std::max(need, node_cap * 2);
-        if (cudaMallocAsync(&p, cap, s) != cudaSuccess) return fail(GVA_ERR_NOMEM, "node descriptor allocation failed");
-        if (d_nodes && first_node > 0)
-            GVA_CUDA_B(cudaMemcpyAsync(p, d_nodes, (size_t)first_node * sizeof(TaskDesc), cudaMemcpyDeviceToDevice, s));
-        if (d_nodes) cudaFreeAsync(d_nodes, s);
-        d_nodes = p;
-        node_cap = cap;
-    }
-    const size_t off = (size_t)first_node * sizeof(TaskDesc);
-    if (need > off) {
-        char* h = staging_nodes.get(need - off);
-        if (!h) return fail(GVA_ERR_NOMEM, "pinned staging allocation failed");
-        memcpy(h, node_desc.data() + off, need - off);
-        GVA_CUDA_B(cudaMemcpyAsync((char*)d_nodes + off, h, need - off, cudaMemcpyHostToDevice, s));
-        GVA_CUDA_B(cudaStreamSynchronize(s));  // staging is reused by the next submit
+        plans[q].next_term = nodes[cur].first_term;
+        nodes[cur].first_term = q;
     }
     // seeds: the children of every seed node start from its vertex list
     for (int id = first_node; id < (int)nodes.size(); ++id) {
-        const BNode& seed = nodes[id];
-        if (seed.parent != -1) continue;
+        if (nodes[id].parent != -1) continue;
+        const Step& sd = nodes[id].step;
         uint64_t n = 0;
-        if (!seed.step.always_empty) n = db.seed_off[seed.step.label + 1] - db.seed_off[seed.step.label];
-        if (n == 0) {
-            for (int q : seed.below) {
-                plans[q].done = true;
-                completed.push_back(q);
-            }
-            continue;
-        }
-        for (int c : seed.children) add_task(c, db.seed_verts + db.seed_off[seed.step.label], n, nullptr);
+        if (!sd.always_empty) n = db.seed_off[sd.label + 1] - db.seed_off[sd.label];
+        if (n)
+            for (int c = nodes[id].first_child; c >= 0; c = nodes[c].next_sibling)
+                add_task(c, db.seed_verts + db.seed_off[sd.label], n, nullptr);
+        try_close(id);
     }
     return GVA_OK;
 }
 
 int BatchSession::round() {
+    const auto t_start = std::chrono::steady_clock::now();
+    double wait_before = wait_ms;
+    struct Timer {
+        std::chrono::steady_clock::time_point t0;
+        double& acc;
+        double& wait;
+        double wait0;
+        ~Timer() {
+            acc += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count() -
+                   (wait - wait0);
+        }
+    } timer{t_start, round_host_ms, wait_ms, wait_before};
     GVA_CUDA_B(cudaSetDevice(db.device));
     // steps that cannot match (label or partition absent) end their task
-    for (size_t i = 0; i < active.size();) {
-        if (nodes[active[i].node].step.always_empty) {
-            const int nd = active[i].node;
-            active.erase(active.begin() + i);
-            end_task(nd);
-        } else {
-            ++i;
+    {
+        size_t w = 0;
+        std::vector<int> gone;
+        for (size_t i = 0; i < active.size(); ++i) {
+            if (nodes[active[i].node].step.always_empty)
+                gone.push_back(active[i].node);
+            else
+                active[w++] = std::move(active[i]);
         }
+        active.resize(w);
+        for (int nd : gone) finish_task(nd);
     }
     if (active.empty()) return GVA_OK;
     ++rounds;
+    // the previous round's host-to-device copies read the staging area
+    if (staged) {
+        GVA_CUDA_B(cudaEventSynchronize(staged));
+    } else {
+        GVA_CUDA_B(cudaEventCreateWithFlags(&staged, cudaEventDisableTiming));
+    }
     Profiler prof;
     Profiler* pf = profile ? &prof : nullptr;
     BatchCtx ctx{};
@@ -608,29 +632,38 @@ int BatchSession::round() {
     ctx.graph_counts = graph_counts_dev();
     ctx.graph_bits = graph_bits_dev();
     const int nt = (int)active.size();
-    const size_t desc_bytes = (size_t)nt * sizeof(TaskRef);
+    // staging: refs[nt] | new node descriptors (<= nt) | block0[nt+1] | totals[nt] | outs[nt] + queue
+    const size_t ref_bytes = (size_t)nt * sizeof(TaskRef);
+    const size_t desc_max = (size_t)nt * sizeof(TaskDesc);
     const size_t small_words = (size_t)(nt + 1) + nt + nt + 1;
-    char* h = staging.get(desc_bytes + small_words * 8);
+    char* h = staging.get(ref_bytes + desc_max + small_words * 8);
     if (!h) return fail(GVA_ERR_NOMEM, "pinned staging allocation failed");
     TaskRef* refs = (TaskRef*)h;
-    uint64_t* h_block0 = (uint64_t*)(h + desc_bytes);
+    char* new_desc = h + ref_bytes;
+    uint64_t* h_block0 = (uint64_t*)(h + ref_bytes + desc_max);
     uint64_t* h_totals = h_block0 + (nt + 1);
     uint32_t** h_outs = (uint32_t**)(h_totals + nt);
-    std::vector<uint64_t> block0(nt + 1, 0);
+    const int dev_first = dev_count;
     uint32_t kmax = 1, eqmax = 0;
     double cbytes = 0;
+    uint64_t nb = 0;
+    h_block0[0] = 0;
     for (int t = 0; t < nt; ++t) {
         const BTask& tk = active[t];
-        const Step& st = nodes[tk.node].step;
-        refs[t] = TaskRef{(uint32_t)tk.node, 0u, block0[t], tk.in, tk.rows};
+        BNode& nd = nodes[tk.node];
+        if (nd.dev < 0) {  // first task of this node: ship its parameters
+            nd.dev = dev_count++;
+            fill_node_desc(tk.node, new_desc + (size_t)(nd.dev - dev_first) * sizeof(TaskDesc));
+        }
+        const Step& st = nd.step;
+        refs[t] = TaskRef{(uint32_t)nd.dev, 0u, nb, tk.in, tk.rows};
         kmax = std::max(kmax, st.width_in);
         if (st.kind == STEP_EXT) eqmax = std::max(eqmax, st.n_eq);
-        block0[t + 1] = block0[t] + (tk.rows + kRowsPerBlock - 1) / kRowsPerBlock;
+        nb += (tk.rows + kRowsPerBlock - 1) / kRowsPerBlock;
+        h_block0[t + 1] = nb;
         cbytes += (4.0 * st.width_in + 8.0 * (st.kind == STEP_EXT ? 1 : st.n_pairs)) * (double)tk.rows;
     }
-    const uint64_t nb = block0[nt];
     if (nb > 0x7fffffffull) return fail(GVA_ERR_UNSUPPORTED, "round too large for one launch");
-    std::copy(block0.begin(), block0.end(), h_block0);
     auto grow = [&](void** p, size_t& cap, size_t need) -> bool {
         if (need <= cap) return true;
         if (*p) cudaFreeAsync(*p, s);
@@ -643,14 +676,28 @@ int BatchSession::round() {
         cap = c;
         return true;
     };
-    if (!grow(&d_desc, desc_cap, desc_bytes) || !grow((void**)&d_sums, sums_cap, (nb + 1) * 8) ||
+    const size_t dev_need = (size_t)dev_count * sizeof(TaskDesc);
+    if (dev_need > node_cap) {  // keep the descriptors already shipped
+        void* p = nullptr;
+        const size_t cap = std::max(dev_need, node_cap * 2);
+        if (cudaMallocAsync(&p, cap, s) != cudaSuccess) return fail(GVA_ERR_NOMEM, "node descriptor allocation failed");
+        if (d_nodes && dev_first > 0)
+            GVA_CUDA_B(cudaMemcpyAsync(p, d_nodes, (size_t)dev_first * sizeof(TaskDesc), cudaMemcpyDeviceToDevice, s));
+        if (d_nodes) cudaFreeAsync(d_nodes, s);
+        d_nodes = p;
+        node_cap = cap;
+    }
+    if (!grow(&d_desc, desc_cap, ref_bytes) || !grow((void**)&d_sums, sums_cap, (nb + 1) * 8) ||
         !grow((void**)&d_small, small_cap, small_words * 8))
         return fail(GVA_ERR_NOMEM, "batch bookkeeping allocation failed");
     uint64_t* d_block0 = d_small;
     uint64_t* d_totals = d_block0 + (nt + 1);
     uint32_t** d_outs = (uint32_t**)(d_totals + nt);
     unsigned long long* d_queue = (unsigned long long*)(d_totals + 2 * nt);
-    GVA_CUDA_B(cudaMemcpyAsync(d_desc, refs, desc_bytes, cudaMemcpyHostToDevice, s));
+    if (dev_count > dev_first)
+        GVA_CUDA_B(cudaMemcpyAsync((char*)d_nodes + (size_t)dev_first * sizeof(TaskDesc), new_desc,
+                                   (size_t)(dev_count - dev_first) * sizeof(TaskDesc), cudaMemcpyHostToDevice, s));
+    GVA_CUDA_B(cudaMemcpyAsync(d_desc, refs, ref_bytes, cudaMemcpyHostToDevice, s));
     GVA_CUDA_B(cudaMemcpyAsync(d_block0, h_block0, (nt + 1) * 8, cudaMemcpyHostToDevice, s));
 
     cudaEvent_t ev = nullptr;
@@ -666,37 +713,48 @@ int BatchSession::round() {
     g_batch_launches += 3;
     GVA_CUDA_B(cudaGetLastError());
     GVA_CUDA_B(cudaMemcpyAsync(h_totals, d_totals, nt * 8, cudaMemcpyDeviceToHost, s));
-    GVA_CUDA_B(cudaStreamSynchronize(s));
-    std::vector<uint64_t> totals(h_totals, h_totals + nt);
+    {
+        const auto w0 = std::chrono::steady_clock::now();
+        cudaError_t e = cudaStreamSynchronize(s);
+        wait_ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - w0).count();
+        if (e != cudaSuccess) return fail(GVA_ERR_CUDA, cudaGetErrorString(e));
+    }
 
-    // choose which tasks write this round: deepest first, within the budget
-    std::vector<int> order;
-    std::vector<BTask> next;
-    std::vector<char> finished(nt, 0);
+    // which tasks write this round: all when the outputs fit the budget,
+    // else deepest first; a task larger than the budget is split
+    uint64_t want = 0;
     for (int t = 0; t < nt; ++t) {
         const BNode& nd = nodes[active[t].node];
-        for (int q : nd.terminal) plans[q].count += totals[t];
-        if (!nd.children.empty() && totals[t] > 0)
-            order.push_back(t);
-        else
-            finished[t] = 1;
+        if (nd.first_child < 0 || h_totals[t] == 0) continue;
+        const Step& st = nd.step;
+        want += ((h_totals[t] * (st.kind == STEP_EXT ? st.width_in + 1 : st.width_in) * 4ull) + 15) & ~15ull;
     }
-    std::stable_sort(order.begin(), order.end(),
-                     [&](int a, int b) { return nodes[active[a].node].depth > nodes[active[b].node].depth; });
+    std::vector<int>& order = scratch_order;
+    order.clear();
+    for (int t = 0; t < nt; ++t) {
+        const BNode& nd = nodes[active[t].node];
+        for (int q = nd.first_term; q >= 0; q = plans[q].next_term) plans[q].count += h_totals[t];
+        if (nd.first_child >= 0 && h_totals[t] > 0) order.push_back(t);
+    }
+    if (want > budget)
+        std::stable_sort(order.begin(), order.end(),
+                         [&](int a, int b) { return nodes[active[a].node].depth > nodes[active[b].node].depth; });
+    std::vector<BTask> next;
+    std::vector<char>& chosen_flag = scratch_flag;
+    chosen_flag.assign(nt, 0);
     uint64_t used = 0;
-    std::vector<uint64_t> off_words(nt, 0);
-    std::vector<int> chosen;
+    std::vector<uint64_t>& off_words = scratch_off;
+    off_words.assign(nt, 0);
     int status = GVA_OK;
     for (int t : order) {
         const Step& st = nodes[active[t].node].step;
         const uint32_t w = st.kind == STEP_EXT ? st.width_in + 1 : st.width_in;
-        const uint64_t bytes = totals[t] * w * 4ull;
+        const uint64_t bytes = h_totals[t] * w * 4ull;
         if (used + bytes <= budget) {
             off_words[t] = used / 4;
             used += (bytes + 15) & ~15ull;
-            chosen.push_back(t);
+            chosen_flag[t] = 1;
         } else if (bytes > budget) {
-            // split the task's input rows; both halves retry next round
             BTask a = active[t], b = active[t];
             const uint64_t half = a.rows / 2;
             if (half == 0) {
@@ -706,12 +764,14 @@ int BatchSession::round() {
             a.rows = half;
             b.in = a.in + half * st.width_in;
             b.rows = active[t].rows - half;
-            for (int q : nodes[a.node].below) plans[q].live++;  // one task became two
+            nodes[a.node].at++;  // one task became two
             next.push_back(a);
             next.push_back(b);
+            chosen_flag[t] = 2;
             ++splits;
         } else {
             next.push_back(active[t]);  // fits alone: waits for the next round
+            chosen_flag[t] = 2;
         }
     }
     if (status) return status;
@@ -722,13 +782,13 @@ int BatchSession::round() {
         cudaStream_t ss = s;
         buf = std::shared_ptr<void>(p, [ss](void* q) { cudaFreeAsync(q, ss); });
         double wbytes = 0;
-        for (int t = 0; t < nt; ++t) h_outs[t] = nullptr;
-        for (int t : chosen) {
-            h_outs[t] = (uint32_t*)p + off_words[t];
+        for (int t = 0; t < nt; ++t) {
+            h_outs[t] = chosen_flag[t] == 1 ? (uint32_t*)p + off_words[t] : nullptr;
+            if (chosen_flag[t] != 1) continue;
             const Step& st = nodes[active[t].node].step;
             const double k = st.width_in;
             wbytes += (4.0 * k + 8.0) * (double)active[t].rows +
-                      (st.kind == STEP_EXT ? (4.0 + 4.0 * (k + 1)) : 4.0 * k) * (double)totals[t];
+                      (st.kind == STEP_EXT ? (4.0 + 4.0 * (k + 1)) : 4.0 * k) * (double)h_totals[t];
         }
         GVA_CUDA_B(cudaMemcpyAsync(d_outs, h_outs, nt * sizeof(uint32_t*), cudaMemcpyHostToDevice, s));
         GVA_CUDA_B(cudaMemsetAsync(d_queue, 0, 8, s));
@@ -737,25 +797,26 @@ int BatchSession::round() {
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_write_kernel, kThreads, smem);
         const uint64_t grid = std::min<uint64_t>(nb, (uint64_t)std::max(per_sm, 1) * sms);
         if (pf) pf->begin(K_EXT_WRITE, wbytes, s, ev);
-        batch_write_kernel<<<(unsigned)grid, kThreads, smem, s>>>((const TaskDesc*)d_nodes, (const TaskRef*)d_desc, d_block0,
-                                                                  nt, nb, d_sums, d_outs, d_queue);
+        batch_write_kernel<<<(unsigned)grid, kThreads, smem, s>>>((const TaskDesc*)d_nodes, (const TaskRef*)d_desc,
+                                                                  d_block0, nt, nb, d_sums, d_outs, d_queue);
         if (pf) pf->end(ev, K_EXT_WRITE, wbytes, s);
         launches += 1;
         g_batch_launches += 1;
         GVA_CUDA_B(cudaGetLastError());
     }
+    GVA_CUDA_B(cudaEventRecord(staged, s));
     std::vector<int> ended;
-    for (int t = 0; t < nt; ++t)
-        if (finished[t]) ended.push_back(active[t].node);
-    for (int t : chosen) {
-        for (int c : nodes[active[t].node].children) {
-            for (int q : nodes[c].below) plans[q].live++;
-            next.push_back({c, h_outs[t], totals[t], buf});
-        }
+    for (int t = 0; t < nt; ++t) {
+        if (chosen_flag[t] == 2) continue;  // still active (deferred or split)
+        if (chosen_flag[t] == 1)
+            for (int c = nodes[active[t].node].first_child; c >= 0; c = nodes[c].next_sibling) {
+                nodes[c].at++;
+                next.push_back({c, h_outs[t], h_totals[t], buf});
+            }
         ended.push_back(active[t].node);
     }
     active.swap(next);
-    for (int nd : ended) end_task(nd);
+    for (int nd : ended) finish_task(nd);
     if (pf) {
         GVA_CUDA_B(cudaStreamSynchronize(s));
         pf->resolve();
@@ -775,9 +836,8 @@ std::vector<int> BatchSession::take_completed() {
 }
 
 int BatchSession::read_support(int q, uint32_t* support, uint64_t* graph_counts_host) {
-    // plans ending on the same node share the first one's slot
-    const int q0 = nodes[plans[q].terminal].terminal[0];
-    const int slot = plans[q0].slot;
+    // plans ending on the same node share the slot of the node's first plan
+    const int slot = plans[first_peer(q)].slot;
     if (support) {
         std::vector<uint32_t> bits(ctx_words);
         GVA_CUDA_B(cudaMemcpyAsync(bits.data(), graph_bits_dev() + (size_t)slot * ctx_words, ctx_words * 4,
@@ -801,10 +861,10 @@ void BatchSession::release(int q) {
     if (p.released) return;
     p.released = true;
     if (p.slot < 0) return;
-    const std::vector<int>& peers = nodes[p.terminal].terminal;
-    for (int o : peers)
+    const int t = p.terminal;
+    for (int o = nodes[t].first_term; o >= 0; o = plans[o].next_term)
         if (!plans[o].released) return;
-    for (int o : peers) {
+    for (int o = nodes[t].first_term; o >= 0; o = plans[o].next_term) {
         const int sl = plans[o].slot;
         if (sl < 0) continue;
         if (want_graph_counts)
@@ -812,6 +872,23 @@ void BatchSession::release(int q) {
         cudaMemsetAsync(graph_bits_dev() + (size_t)sl * ctx_words, 0, (size_t)ctx_words * 4, s);
         free_slots.push_back(sl);
         plans[o].slot = -1;
+    }
+}
+
+__global__ void slot_popcount_kernel(const uint32_t* __restrict__ bits, uint32_t words, uint32_t nslots,
+                                     uint32_t* __restrict__ out) {
+    const uint32_t slot = blockIdx.x;
+    if (slot >= nslots) return;
+    uint32_t c = 0;
+    for (uint32_t w = threadIdx.x; w < words; w += blockDim.x) c += __popc(bits[(uint64_t)slot * words + w]);
+    c = warp_sum(c);
+    __shared__ uint32_t ws[8];
+    if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = c;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t t = 0;
+        for (int i = 0; i < (int)(blockDim.x >> 5); ++i) t += ws[i];
+        out[slot] = t;
     }
 }
 
@@ -843,36 +920,35 @@ int run_batch(DevDB& db, const std::vector<std::vector<Step>>& steps, cudaStream
         if (!rc) {
             for (int q = 0; q < nq; ++q) counts[q] = ses.plan(ids[q]).count;
             if (per_graph) {
-                // bulk read of every slot, then identical plans copy their first one's results
-                const uint32_t words = ses.words();
-                std::vector<uint32_t> bits((size_t)nq * words);
-                cudaMemcpyAsync(bits.data(), ses.graph_bits_dev(), bits.size() * 4, cudaMemcpyDeviceToHost, s);
-                if (graph_counts_host)
+                // supports counted on the device; identical plans read their first one's slot
+                uint32_t* d_pop = nullptr;
+                if (cudaMallocAsync((void**)&d_pop, (size_t)nq * 4, s) != cudaSuccess)
+                    rc = fail(GVA_ERR_NOMEM, "support counters");
+                std::vector<uint32_t> pop(nq, 0);
+                if (!rc) {
+                    slot_popcount_kernel<<<nq, 256, 0, s>>>(ses.graph_bits_dev(), ses.words(), (uint32_t)nq, d_pop);
+                    cudaMemcpyAsync(pop.data(), d_pop, (size_t)nq * 4, cudaMemcpyDeviceToHost, s);
+                    cudaFreeAsync(d_pop, s);
+                }
+                if (!rc && graph_counts_host)
                     cudaMemcpyAsync(graph_counts_host, ses.graph_counts_dev(), (size_t)nq * db.num_graphs * 8,
                                     cudaMemcpyDeviceToHost, s);
-                rc = cudaStreamSynchronize(s) == cudaSuccess ? GVA_OK : fail(GVA_ERR_CUDA, "result read-back failed");
+                if (!rc)
+                    rc = cudaStreamSynchronize(s) == cudaSuccess ? GVA_OK : fail(GVA_ERR_CUDA, "result read-back failed");
                 for (int q = 0; q < nq && !rc; ++q) {
-                    const int q0 = ses.first_peer(ids[q]);
-                    const int sl = ses.plan(q0).slot, own = ses.plan(ids[q]).slot;
-                    if (sl != own) {
-                        std::copy(bits.begin() + (size_t)sl * words, bits.begin() + (size_t)(sl + 1) * words,
-                                  bits.begin() + (size_t)own * words);
-                        if (graph_counts_host)
-                            std::copy(graph_counts_host + (size_t)sl * db.num_graphs,
-                                      graph_counts_host + (size_t)(sl + 1) * db.num_graphs,
-                                      graph_counts_host + (size_t)own * db.num_graphs);
-                    }
+                    const int sl = ses.plan(ses.first_peer(ids[q])).slot, own = ses.plan(ids[q]).slot;
+                    if (support_host) support_host[q] = pop[sl];
+                    if (graph_counts_host && sl != own)
+                        std::copy(graph_counts_host + (size_t)sl * db.num_graphs,
+                                  graph_counts_host + (size_t)(sl + 1) * db.num_graphs,
+                                  graph_counts_host + (size_t)own * db.num_graphs);
                 }
-                if (support_host && !rc)
-                    for (int q = 0; q < nq; ++q) {
-                        const int own = ses.plan(ids[q]).slot;
-                        uint32_t c = 0;
-                        for (uint32_t w = 0; w < words; ++w) c += (uint32_t)__builtin_popcount(bits[(size_t)own * words + w]);
-                        support_host[q] = c;
-                    }
             }
         }
         if (stats) {
+            stats->submit_ms = ses.submit_ms;
+            stats->round_host_ms = ses.round_host_ms;
+            stats->wait_ms = ses.wait_ms;
             stats->rounds = ses.rounds;
             stats->splits = ses.splits;
             stats->launches = ses.launches;

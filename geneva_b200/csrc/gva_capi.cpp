@@ -385,6 +385,9 @@ int gva_mine_get_stats(const gva_mine_result* res, gva_mine_stats* out) {
     out->plan_ms = res->stats.plan_ms;
     out->eval_ms = res->stats.eval_ms;
     out->merge_ms = res->stats.merge_ms;
+    out->submit_ms = res->stats.submit_ms;
+    out->round_host_ms = res->stats.round_host_ms;
+    out->wait_ms = res->stats.wait_ms;
     return GVA_OK;
 }
 

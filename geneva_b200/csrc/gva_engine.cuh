@@ -79,6 +79,7 @@ void free_result(MatchResult* r);
 
 struct BatchStats {
     double gpu_ms = 0.0;
+    double submit_ms = 0.0, round_host_ms = 0.0, wait_ms = 0.0;
     uint64_t rounds = 0, splits = 0, launches = 0, nodes = 0;
     KernelStat kstat[K_NUM];
 };
@@ -107,9 +108,11 @@ public:
         Step step;
         int depth = 0;
         int parent = -1;
-        std::vector<int> children;
-        std::vector<int> terminal;  // plans whose last step is this node
-        std::vector<int> below;     // plans whose path passes through this node
+        int first_child = -1, next_sibling = -1;  // children as a linked list
+        int first_term = -1;                       // plans ending here, linked through PlanRec::next_term
+        int at = 0;                                // active tasks at this node
+        int dev = -1;                              // index of its descriptor on the device
+        bool closed = false;
     };
     struct BTask {
         int node;
@@ -121,8 +124,8 @@ public:
         uint64_t tag = 0;
         int slot = -1;
         int terminal = -1;
+        int next_term = -1;
         uint64_t count = 0;
-        int live = 0;
         bool done = false;
         bool released = false;
     };
@@ -135,7 +138,9 @@ public:
     bool idle() const { return active.empty(); }
     std::vector<int> take_completed();
     const PlanRec& plan(int q) const { return plans[q]; }
-    int first_peer(int q) const { return nodes[plans[q].terminal].terminal[0]; }
+    // the plan whose slot holds q's per-graph results: the head of the list of
+    // plans ending on q's node (the node descriptor names that slot)
+    int first_peer(int q) const { return nodes[plans[q].terminal].first_term; }
     int read_support(int q, uint32_t* support, uint64_t* graph_counts_host);
     void release(int q);
     size_t num_nodes() const { return nodes.size(); }
@@ -145,12 +150,14 @@ public:
     uint32_t* graph_bits_dev() const;
 
     uint64_t rounds = 0, splits = 0, launches = 0;
+    double submit_ms = 0, round_host_ms = 0, wait_ms = 0;  // host time split
     KernelStat kstat[K_NUM];
 
 private:
     void add_task(int node, const uint32_t* in, uint64_t rows, std::shared_ptr<void> owner);
-    void fill_node_desc(int id);
-    void end_task(int node);
+    void fill_node_desc(int id, void* out) const;
+    void finish_task(int node);
+    void try_close(int node);
 
     DevDB& db;
     cudaStream_t s;
@@ -167,10 +174,14 @@ private:
     std::vector<PlanRec> plans;
     std::vector<BTask> active;
     std::vector<int> completed;
-    Staging staging, staging_nodes;
-    std::vector<char> node_desc;  // host copy of the per-node step descriptors
-    void* d_nodes = nullptr;      // device copy (layout private to gva_batch.cu)
+    Staging staging;
+    cudaEvent_t staged = nullptr;  // marks the last copies out of `staging`
+    void* d_nodes = nullptr;       // per-node step descriptors (layout private to gva_batch.cu)
     size_t node_cap = 0;
+    int dev_count = 0;
+    std::vector<int> scratch_order;
+    std::vector<char> scratch_flag;
+    std::vector<uint64_t> scratch_off;
     void* d_desc = nullptr;  // per-round task references
     size_t desc_cap = 0;
     uint64_t* d_sums = nullptr;
@@ -190,6 +201,7 @@ struct MinedPattern {
 struct MineStats {
     uint64_t candidates = 0, frequent = 0, embeddings = 0, levels = 0, pruned = 0;
     double gpu_ms = 0.0, host_ms = 0.0, gen_ms = 0.0, plan_ms = 0.0, eval_ms = 0.0, merge_ms = 0.0;
+    double submit_ms = 0.0, round_host_ms = 0.0, wait_ms = 0.0;
     KernelStat kstat[K_NUM];
 };
 

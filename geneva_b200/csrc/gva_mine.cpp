@@ -238,6 +238,9 @@ int run_mine(DevDB& db, cudaStream_t s, uint64_t budget, uint32_t max_edges, uin
                                sup.data() + b0, profile, &bs);
             if (rc) return rc;
             gpu_ms += bs.gpu_ms;
+            st.submit_ms += bs.submit_ms;
+            st.round_host_ms += bs.round_host_ms;
+            st.wait_ms += bs.wait_ms;
             for (int kk = 0; kk < K_NUM; ++kk) {
                 st.kstat[kk].launches += bs.kstat[kk].launches;
                 st.kstat[kk].ms += bs.kstat[kk].ms;
@@ -340,18 +343,39 @@ int run_mine(DevDB& db, cudaStream_t s, uint64_t budget, uint32_t max_edges, uin
                 }
             });
         for (auto& th : pool) th.join();
-        std::vector<std::pair<Code, Pattern>> all;
-        for (unsigned t = 0; t < nthreads; ++t) {
-            st.pruned += pruned[t];
-            for (auto& x : found[t]) all.push_back(std::move(x));
-        }
+        // merge: bucket candidates by code hash, dedupe and sort each bucket on
+        // its own thread, concatenate the buckets in order (deterministic)
         auto t_merge = std::chrono::steady_clock::now();
-        std::sort(all.begin(), all.end(), [](const auto& a, const auto& b) { return a.first < b.first; });
+        for (unsigned t = 0; t < nthreads; ++t) st.pruned += pruned[t];
+        std::vector<std::vector<Pattern>> buckets(nthreads);
+        {
+            CodeHash hasher;
+            std::vector<std::vector<size_t>> hs(nthreads);
+            std::vector<std::thread> hp;
+            for (unsigned t = 0; t < nthreads; ++t)
+                hp.emplace_back([&, t]() {
+                    hs[t].reserve(found[t].size());
+                    for (auto& x : found[t]) hs[t].push_back(hasher(x.first) % nthreads);
+                });
+            for (auto& th : hp) th.join();
+            std::vector<std::thread> bp;
+            for (unsigned b = 0; b < nthreads; ++b)
+                bp.emplace_back([&, b]() {
+                    std::vector<std::pair<Code, Pattern>*> mine;
+                    for (unsigned t = 0; t < nthreads; ++t)
+                        for (size_t i = 0; i < found[t].size(); ++i)
+                            if (hs[t][i] == b) mine.push_back(&found[t][i]);
+                    std::sort(mine.begin(), mine.end(), [](const auto* a, const auto* c) { return a->first < c->first; });
+                    for (size_t i = 0; i < mine.size(); ++i)
+                        if (i == 0 || mine[i]->first != mine[i - 1]->first) buckets[b].push_back(std::move(mine[i]->second));
+                });
+            for (auto& th : bp) th.join();
+        }
         std::vector<Pattern> next;
-        for (size_t i = 0; i < all.size(); ++i)
-            if (i == 0 || all[i].first != all[i - 1].first) next.push_back(std::move(all[i].second));
-        st.gen_ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_gen).count();
+        for (auto& bk : buckets)
+            for (auto& pt : bk) next.push_back(std::move(pt));
         st.merge_ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_merge).count();
+        st.gen_ms += std::chrono::duration<double, std::milli>(t_merge - t_gen).count();
         auto t_eval = std::chrono::steady_clock::now();
         rc = evaluate(next, sup, emb);
         if (rc) return rc;

@@ -237,6 +237,9 @@ typedef struct gva_mine_stats {
     double plan_ms;      /* planning and lowering of every candidate (host threads) */
     double eval_ms;      /* matching of every candidate, host bookkeeping included */
     double merge_ms;     /* merging and ordering the candidates of each level */
+    double submit_ms;    /* within eval: building the step trie and descriptors */
+    double round_host_ms;/* within eval: per-round host bookkeeping */
+    double wait_ms;      /* within eval: host waiting for the GPU */
 } gva_mine_stats;
 
 typedef struct gva_mine_result gva_mine_result;
