@@ -122,15 +122,20 @@ def measured_peak_gbs():
     return 6650.0, "fallback"
 
 
-def ncu_traffic(kernel: str):
-    """Per-launch DRAM bytes of `kernel` from the committed ncu summary, if any."""
+def ncu_traffic(kernel: str, stat: dict):
+    """DRAM bytes per launch of `kernel`: the committed ncu capture's bytes per
+    frontier row (profiles/ncu_traffic.json) times this run's mean rows per
+    launch, or None without a capture."""
     p = ROOT / "profiles" / "ncu_traffic.json"
-    if not p.exists():
+    if not p.exists() or not stat.get("launches"):
         return None
     try:
-        return json.loads(p.read_text()).get(kernel)
+        cap = json.loads(p.read_text()).get(kernel)
     except Exception:
         return None
+    if not cap:
+        return None
+    return cap["dram_bytes"] / cap["rows"] * (stat.get("rows", 0.0) / stat["launches"])
 
 
 # ------------------------------------------------------------ CPU baseline ----
@@ -405,7 +410,7 @@ def mine_bench(args, rank, world, local, dist, torch, gv, workloads, shard):
                   "batched_over_plain": t_plain / t_batch,
                   "path": "plain = one gva_match per pattern, rows to host, support from their graph ids"},
         "roofline": {"bound": "hbm", "kernel": name, "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "peak_source": peak_kind, "traffic": ncu_traffic(name),
+                     "frac": achieved / peak, "peak_source": peak_kind, "traffic": ncu_traffic(name, s),
                      "launches": s["launches"], "kernel_ms": s["ms"]},
         "kernels": kstats,
         "e2e": {"value": e2e_value, "unit": "embeddings/s", "h2d_bytes_per_step": h2d // e2e_steps,
@@ -588,7 +593,7 @@ def main():
     name, s = max(kstats.items(), key=lambda kv: kv[1]["ms"]) if kstats else ("none", {"launches": 0, "ms": 0, "bytes": 0})
     per_launch_ms = s["ms"] / max(s["launches"], 1)
     achieved = (s["bytes"] / max(s["launches"], 1)) / (per_launch_ms / 1000.0) / 1e9 if per_launch_ms else 0.0
-    traffic = ncu_traffic(name)
+    traffic = ncu_traffic(name, s)
 
     out = None
     if rank == 0:

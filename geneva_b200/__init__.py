@@ -57,7 +57,7 @@ class _MatchOpts(ctypes.Structure):
 
 class _KernelStat(ctypes.Structure):
     _fields_ = [("name", ctypes.c_char * 24), ("launches", ctypes.c_uint64), ("ms", ctypes.c_double),
-                ("bytes", ctypes.c_double)]
+                ("bytes", ctypes.c_double), ("rows", ctypes.c_double)]
 
 
 REDUCE_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.POINTER(ctypes.c_uint32), ctypes.POINTER(ctypes.c_uint64),
@@ -304,7 +304,7 @@ class Result:
         arr = (_KernelStat * 16)()
         n = library().gva_result_kernel_stats(self._h, arr, 16)
         return {arr[i].name.decode(): dict(launches=int(arr[i].launches), ms=float(arr[i].ms),
-                                            bytes=float(arr[i].bytes)) for i in range(n)}
+                                            bytes=float(arr[i].bytes), rows=float(arr[i].rows)) for i in range(n)}
 
     @property
     def device_ptr(self) -> Optional[int]:
@@ -368,7 +368,8 @@ def batch_count(db: Database, plans: Sequence[Plan], stream: Optional[int] = Non
     stats = {"gpu_ms": st.gpu_ms, "rounds": int(st.rounds), "splits": int(st.splits), "launches": int(st.launches),
              "trie_nodes": int(st.trie_nodes),
              "kernels": {st.kernels[i].name.decode(): dict(launches=int(st.kernels[i].launches),
-                                                           ms=float(st.kernels[i].ms), bytes=float(st.kernels[i].bytes))
+                                                           ms=float(st.kernels[i].ms), bytes=float(st.kernels[i].bytes),
+                                                           rows=float(st.kernels[i].rows))
                          for i in range(5)}}
     per_graph = gc if graph_counts else sup
     if graph_counts and support:
@@ -422,7 +423,8 @@ def mine(db: Database, max_edges: int, min_support: int, stream: Optional[int] =
         ks = (_KernelStat * 8)()
         n = lib.gva_mine_kernel_stats(h, ks, 8)
         stats["kernels"] = {ks[i].name.decode(): dict(launches=int(ks[i].launches), ms=float(ks[i].ms),
-                                                       bytes=float(ks[i].bytes)) for i in range(n)}
+                                                       bytes=float(ks[i].bytes), rows=float(ks[i].rows))
+                            for i in range(n)}
     finally:
         lib.gva_mine_free(h)
     return pats, stats

@@ -645,7 +645,7 @@ int BatchSession::round() {
     uint32_t** h_outs = (uint32_t**)(h_totals + nt);
     const int dev_first = dev_count;
     uint32_t kmax = 1, eqmax = 0;
-    double cbytes = 0;
+    double cbytes = 0, crows = 0;
     uint64_t nb = 0;
     h_block0[0] = 0;
     for (int t = 0; t < nt; ++t) {
@@ -662,6 +662,7 @@ int BatchSession::round() {
         nb += (tk.rows + kRowsPerBlock - 1) / kRowsPerBlock;
         h_block0[t + 1] = nb;
         cbytes += (4.0 * st.width_in + 8.0 * (st.kind == STEP_EXT ? 1 : st.n_pairs)) * (double)tk.rows;
+        crows += (double)tk.rows;
     }
     if (nb > 0x7fffffffull) return fail(GVA_ERR_UNSUPPORTED, "round too large for one launch");
     auto grow = [&](void** p, size_t& cap, size_t need) -> bool {
@@ -704,10 +705,10 @@ int BatchSession::round() {
     if (pf) pf->begin(K_EXT_COUNT, cbytes, s, ev);
     batch_count_kernel<<<(unsigned)nb, kThreads, 0, s>>>((const TaskDesc*)d_nodes, (const TaskRef*)d_desc, d_block0,
                                                          nt, d_sums, ctx);
-    if (pf) pf->end(ev, K_EXT_COUNT, cbytes, s);
+    if (pf) pf->end(ev, K_EXT_COUNT, cbytes, s, crows);
     if (pf) pf->begin(K_SCAN, 16.0 * nb, s, ev);
     scan_block_sums_kernel<<<1, kScanThreads, 0, s>>>(d_sums, nb);
-    if (pf) pf->end(ev, K_SCAN, 16.0 * nb, s);
+    if (pf) pf->end(ev, K_SCAN, 16.0 * nb, s, (double)nb);
     task_totals_kernel<<<(nt + 255) / 256, 256, 0, s>>>(d_block0, nt, d_sums, d_totals);
     launches += 3;
     g_batch_launches += 3;
@@ -781,10 +782,11 @@ int BatchSession::round() {
         if (cudaMallocAsync(&p, used, s) != cudaSuccess) return fail(GVA_ERR_NOMEM, "frontier allocation failed");
         cudaStream_t ss = s;
         buf = std::shared_ptr<void>(p, [ss](void* q) { cudaFreeAsync(q, ss); });
-        double wbytes = 0;
+        double wbytes = 0, wrows = 0;
         for (int t = 0; t < nt; ++t) {
             h_outs[t] = chosen_flag[t] == 1 ? (uint32_t*)p + off_words[t] : nullptr;
             if (chosen_flag[t] != 1) continue;
+            wrows += (double)active[t].rows;
             const Step& st = nodes[active[t].node].step;
             const double k = st.width_in;
             wbytes += (4.0 * k + 8.0) * (double)active[t].rows +
@@ -799,7 +801,7 @@ int BatchSession::round() {
         if (pf) pf->begin(K_EXT_WRITE, wbytes, s, ev);
         batch_write_kernel<<<(unsigned)grid, kThreads, smem, s>>>((const TaskDesc*)d_nodes, (const TaskRef*)d_desc,
                                                                   d_block0, nt, nb, d_sums, d_outs, d_queue);
-        if (pf) pf->end(ev, K_EXT_WRITE, wbytes, s);
+        if (pf) pf->end(ev, K_EXT_WRITE, wbytes, s, wrows);
         launches += 1;
         g_batch_launches += 1;
         GVA_CUDA_B(cudaGetLastError());
@@ -824,6 +826,7 @@ int BatchSession::round() {
             kstat[i].launches += pf->stat[i].launches;
             kstat[i].ms += pf->stat[i].ms;
             kstat[i].bytes += pf->stat[i].bytes;
+            kstat[i].rows += pf->stat[i].rows;
         }
     }
     return GVA_OK;

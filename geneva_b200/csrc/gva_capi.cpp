@@ -87,6 +87,7 @@ int gva_result_kernel_stats(const gva_result* res, gva_kernel_stat* out, int cap
         out[i].launches = res->r.kstat[i].launches;
         out[i].ms = res->r.kstat[i].ms;
         out[i].bytes = res->r.kstat[i].bytes;
+        out[i].rows = res->r.kstat[i].rows;
     }
     return K_NUM;
 }
@@ -331,6 +332,7 @@ int gva_batch_count(gva_db* db, const gva_plan* const* plans, int nplans, const 
             stats->kernels[i].launches = bs.kstat[i].launches;
             stats->kernels[i].ms = bs.kstat[i].ms;
             stats->kernels[i].bytes = bs.kstat[i].bytes;
+            stats->kernels[i].rows = bs.kstat[i].rows;
         }
     }
     return st;
@@ -399,6 +401,7 @@ int gva_mine_kernel_stats(const gva_mine_result* res, gva_kernel_stat* out, int 
         out[i].launches = res->stats.kstat[i].launches;
         out[i].ms = res->stats.kstat[i].ms;
         out[i].bytes = res->stats.kstat[i].bytes;
+        out[i].rows = res->stats.kstat[i].rows;
     }
     return K_NUM;
 }

@@ -228,20 +228,20 @@ int launch_count(const DevDB& db, const Step& st, const uint32_t* in, uint64_t n
         const double bytes = (4.0 * k + 8.0) * (double)nrows;
         if (prof) prof->begin(K_EXT_COUNT, bytes, s, ev);
         ext_count_kernel<<<(unsigned)nb, kThreads, 0, s>>>(a, sums);
-        if (prof) prof->end(ev, K_EXT_COUNT, bytes, s);
+        if (prof) prof->end(ev, K_EXT_COUNT, bytes, s, (double)nrows);
     } else {
         RedArgs a;
         fill_red(a, db, st, in, nrows, nullptr);
         const double bytes = (4.0 * k + 8.0 * st.n_pairs) * (double)nrows;
         if (prof) prof->begin(K_RED_COUNT, bytes, s, ev);
         red_count_kernel<<<(unsigned)nb, kThreads, 0, s>>>(a, sums);
-        if (prof) prof->end(ev, K_RED_COUNT, bytes, s);
+        if (prof) prof->end(ev, K_RED_COUNT, bytes, s, (double)nrows);
     }
     GVA_CUDA(cudaGetLastError());
     const double sbytes = 16.0 * (double)nb;
     if (prof) prof->begin(K_SCAN, sbytes, s, ev);
     scan_block_sums_kernel<<<1, kScanThreads, 0, s>>>(sums, nb);
-    if (prof) prof->end(ev, K_SCAN, sbytes, s);
+    if (prof) prof->end(ev, K_SCAN, sbytes, s, (double)nb);
     GVA_CUDA(cudaGetLastError());
     g_launches += 2;
     return GVA_OK;
@@ -260,14 +260,14 @@ int launch_write(const DevDB& db, const Step& st, const uint32_t* in, uint64_t n
         const double bytes = (4.0 * k + 8.0) * (double)nrows + (4.0 + 4.0 * (k + 1)) * (double)nout;
         if (prof) prof->begin(K_EXT_WRITE, bytes, s, ev);
         ext_write_kernel<<<(unsigned)nb, kThreads, ext_smem_bytes(a.k, a.n_eq), s>>>(a, sums);
-        if (prof) prof->end(ev, K_EXT_WRITE, bytes, s);
+        if (prof) prof->end(ev, K_EXT_WRITE, bytes, s, (double)nrows);
     } else {
         RedArgs a;
         fill_red(a, db, st, in, nrows, out);
         const double bytes = (4.0 * k + 8.0 * st.n_pairs) * (double)nrows + 4.0 * k * (double)nout;
         if (prof) prof->begin(K_RED_WRITE, bytes, s, ev);
         red_write_kernel<<<(unsigned)nb, kThreads, red_smem_bytes(a.k), s>>>(a, sums);
-        if (prof) prof->end(ev, K_RED_WRITE, bytes, s);
+        if (prof) prof->end(ev, K_RED_WRITE, bytes, s, (double)nrows);
     }
     GVA_CUDA(cudaGetLastError());
     g_launches += 1;
@@ -319,11 +319,11 @@ void Profiler::begin(int kind, double bytes, cudaStream_t s, cudaEvent_t& a) {
     cudaEventRecord(a, s);
 }
 
-void Profiler::end(cudaEvent_t a, int kind, double bytes, cudaStream_t s) {
+void Profiler::end(cudaEvent_t a, int kind, double bytes, cudaStream_t s, double rows) {
     cudaEvent_t b;
     cudaEventCreate(&b);
     cudaEventRecord(b, s);
-    pending.push_back({kind, a, b, bytes});
+    pending.push_back({kind, a, b, bytes, rows});
 }
 
 void Profiler::resolve() {
@@ -334,6 +334,7 @@ void Profiler::resolve() {
         stat[p.kind].launches += 1;
         stat[p.kind].ms += ms;
         stat[p.kind].bytes += p.bytes;
+        stat[p.kind].rows += p.rows;
         cudaEventDestroy(p.a);
         cudaEventDestroy(p.b);
     }

@@ -46,16 +46,17 @@ struct KernelStat {
     uint64_t launches = 0;
     double ms = 0.0;
     double bytes = 0.0;
+    double rows = 0.0;  // frontier rows read (scan: blocks)
 };
 
 // Optional per-launch CUDA-event timing.
 struct Profiler {
     bool on = false;
-    struct Pending { int kind; cudaEvent_t a, b; double bytes; };
+    struct Pending { int kind; cudaEvent_t a, b; double bytes, rows; };
     std::vector<Pending> pending;
     KernelStat stat[K_NUM];
     void begin(int kind, double bytes, cudaStream_t s, cudaEvent_t& a);
-    void end(cudaEvent_t a, int kind, double bytes, cudaStream_t s);
+    void end(cudaEvent_t a, int kind, double bytes, cudaStream_t s, double rows = 0.0);
     void resolve();  // after a stream sync
 };
 

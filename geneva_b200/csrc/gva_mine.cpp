@@ -245,6 +245,7 @@ int run_mine(DevDB& db, cudaStream_t s, uint64_t budget, uint32_t max_edges, uin
                 st.kstat[kk].launches += bs.kstat[kk].launches;
                 st.kstat[kk].ms += bs.kstat[kk].ms;
                 st.kstat[kk].bytes += bs.kstat[kk].bytes;
+                st.kstat[kk].rows += bs.kstat[kk].rows;
             }
         }
         st.candidates += cands.size();

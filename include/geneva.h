@@ -74,6 +74,7 @@ typedef struct gva_kernel_stat {
     uint64_t launches;
     double ms;
     double bytes;
+    double rows; /* frontier rows read (scan kernel: 256-row blocks) */
 } gva_kernel_stat;
 
 /* ---- status -------------------------------------------------------------- */
