@@ -793,6 +793,7 @@ int BatchSession::round() {
                       (st.kind == STEP_EXT ? (4.0 + 4.0 * (k + 1)) : 4.0 * k) * (double)h_totals[t];
         }
         GVA_CUDA_B(cudaMemcpyAsync(d_outs, h_outs, nt * sizeof(uint32_t*), cudaMemcpyHostToDevice, s));
+        GVA_CUDA_B(cudaEventRecord(staged, s));  // the last read of the staging area this round
         GVA_CUDA_B(cudaMemsetAsync(d_queue, 0, 8, s));
         const size_t smem = batch_smem_bytes_for(kmax, std::max(eqmax, 1u));
         int per_sm = 1;
@@ -805,8 +806,9 @@ int BatchSession::round() {
         launches += 1;
         g_batch_launches += 1;
         GVA_CUDA_B(cudaGetLastError());
+    } else {
+        GVA_CUDA_B(cudaEventRecord(staged, s));
     }
-    GVA_CUDA_B(cudaEventRecord(staged, s));
     std::vector<int> ended;
     for (int t = 0; t < nt; ++t) {
         if (chosen_flag[t] == 2) continue;  // still active (deferred or split)

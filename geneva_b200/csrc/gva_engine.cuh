@@ -87,6 +87,11 @@ struct BatchStats {
 
 // Counts the embeddings of many plans in shared rounds.  counts[q] always;
 // graph_counts [nq * G] and support [nq] when given (need db.vgraph).
+// Serialised parameters of a step (everything that decides its output from
+// its input); two steps are the same trie node when these bytes and their
+// parents agree.  buf must hold 512 bytes.
+size_t step_key_bytes(const Step& st, uint8_t* buf);
+
 int run_batch(DevDB& db, const std::vector<std::vector<Step>>& steps, cudaStream_t s, uint64_t budget,
               const uint32_t* vgraph, uint32_t G, uint64_t* counts, uint64_t* graph_counts_host,
               uint32_t* support_host, bool profile, BatchStats* stats);

@@ -14,6 +14,7 @@ constexpr int kMaxCols = 32;
 // ---------------------------------------------------------------- errors ----
 void set_error(int status, const std::string& msg);  // thread-local message
 int fail(int status, const std::string& msg);         // set_error + return status
+const char* last_error_cstr();                        // this thread's last message
 
 // ----------------------------------------------------------------- graph ----
 // Host copy of one database: per edge label a CSR whose per-vertex lists are

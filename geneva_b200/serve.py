@@ -81,6 +81,7 @@ class Server:
         self._next_tag = 1
         self._stop = threading.Event()
         self.rounds = 0
+        self.round_s: List[float] = []  # wall time of each round (host + device)
         self.completed: List[Request] = []
         self._lock = threading.Lock()
         self._loop = threading.Thread(target=self._run, daemon=True)
@@ -180,7 +181,9 @@ class Server:
         while True:
             self._admit()
             if self._inflight:
+                t0 = time.perf_counter()
                 st = self.lib.gva_session_round(self._ses, ctypes.byref(active))
+                self.round_s.append(time.perf_counter() - t0)
                 if st:
                     err = GenevaError(st, self.lib.gva_last_error().decode())
                     for r in self._inflight.values():

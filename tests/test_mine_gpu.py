@@ -48,3 +48,15 @@ def test_mining_small_batches_give_same_result(native):
     key = lambda ps: sorted((p.text, p.support, p.embeddings) for p in ps)
     assert key(a) == key(b)
     gdb.close()
+
+
+def test_mining_with_more_than_256_labels(native):
+    # canonical codes switch to 2-byte values past 256 vertex labels
+    db = workloads.graph_database(200, 6, 12, 2.8, 1000, 1.0, 2, seed=77, name="manylabels")
+    assert len(np.unique(db.vlabels)) > 256
+    gdb = gv.Database.from_edges(db.vlabels, db.src, db.dst, db.elabels)
+    gdb.set_graphs(db.first)
+    pats, _ = gv.mine(gdb, 3, 3)
+    got = {pattern_from_text(p.text): p.support for p in pats}
+    assert got == brute_mine(db, 3, 3) and len(got) > 0
+    gdb.close()
