@@ -11,8 +11,11 @@ GPU (all embeddings enumerated, per-graph support bitmaps).  Metric:
 embeddings/s = embeddings enumerated over all candidates / step time;
 patterns/s (candidates whose support was decided / step time) rides along.
 
-"match": the same database and a batch of seeded 3-7 vertex patterns sampled
-from it, counted per pattern with supporting graphs.
+"match": 4,096 query patterns of 3-8 vertices, connected induced subgraphs
+sampled from the 1,000-graph database (|V|~U[10,30], average degree 3, 4
+uniform vertex labels, unlabeled edges, seed 1), all counted in one batched
+run against that database: int64 embedding counts per (query, graph) and the
+support of every query; the plain path runs one gva_match per query.
 
 N > 1 (torchrun, one process per GPU): every rank holds the database and
 works on its own share (weak scaling, no collective on the data path); the
@@ -45,9 +48,10 @@ import numpy as np  # noqa: E402
 MINE_WORKLOAD = ("config-2 mining: 20000 graphs per rank, |V|~U[20,60], avg degree 4, 16 vertex labels Zipf(1.2), "
                  "3 edge labels; all connected patterns of up to {me} edges with support >= {ms:g} of the graphs; "
                  "every candidate matched, all embeddings enumerated")
-WORKLOAD = ("config-2 database: 20000 graphs, |V|~U[20,60], avg degree 4, 16 vertex labels Zipf(1.2), "
-            "3 edge labels; batch of seeded 3-7 vertex patterns sampled from it; every embedding enumerated "
-            "and counted per pattern, with its supporting graphs")
+WORKLOAD = ("config-3 batched matching: 4096 query patterns of 3-8 vertices, each a connected induced subgraph "
+            "sampled from a config-1 graph, matched (non-induced) against the config-1 database (1000 graphs, "
+            "|V|~U[10,30], avg degree 3, 4 uniform vertex labels, unlabeled edges, seed 1); int64 embedding counts "
+            "per (query, graph) and the support of every query")
 
 
 def parse_args():
@@ -59,7 +63,7 @@ def parse_args():
     ap.add_argument("--workload", default="mine", choices=["mine", "match", "serve"])
     ap.add_argument("--rates", default="10,100,500,2000", help="serve workload: arrival rates (req/s)")
     ap.add_argument("--duration", type=float, default=2.0, help="serve workload: seconds of arrivals per rate")
-    ap.add_argument("--queries", type=int, default=256, help="match workload: patterns per rank per step")
+    ap.add_argument("--queries", type=int, default=4096, help="match workload: patterns per rank per step")
     ap.add_argument("--max-edges", type=int, default=6)
     ap.add_argument("--min-support", type=float, default=0.02, help="fraction of graphs")
     ap.add_argument("--sample", type=int, default=256, help="patterns in the plain-path and CPU samples")
@@ -171,14 +175,14 @@ def reference_arm(args, db, queries, workload):
     work = Path(tempfile.mkdtemp(prefix="geneva_ref_"))
     (work / "datasets").mkdir()
     (work / "run").mkdir()
-    (work / "datasets" / "config2.g").write_text(db.to_g_text())
+    (work / "datasets" / f"{db.name}.g").write_text(db.to_g_text())
     t_conv = time.perf_counter()
-    subprocess.run([str(ref / "genDatabase"), "config2"], cwd=work / "run", check=True,
+    subprocess.run([str(ref / "genDatabase"), db.name], cwd=work / "run", check=True,
                    stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
     t_conv = time.perf_counter() - t_conv
     ds = work / "datasets"
-    reorder = work / "run" / "config2.reorder"
-    meta = np.loadtxt(ds / "config2.metadata", dtype=np.int64)  # new id, label, old id (0-based .g id)
+    reorder = work / "run" / f"{db.name}.reorder"
+    meta = np.loadtxt(ds / f"{db.name}.metadata", dtype=np.int64)  # new id, label, old id (0-based .g id)
     new_to_old = np.zeros(int(meta[:, 0].max()) + 1, dtype=np.int64)
     new_to_old[meta[:, 0]] = meta[:, 2]
     cores = os.cpu_count() or 1
@@ -189,8 +193,8 @@ def reference_arm(args, db, queries, workload):
         d = work / f"q{i}"
         d.mkdir(exist_ok=True)
         (d / "q.query").write_text(q)
-        subprocess.run([str(ref / "cpumine"), str(reorder), "q.query", str(ds / "config2.mygraph"),
-                        str(ds / "config2.metadata")], cwd=d, stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL,
+        subprocess.run([str(ref / "cpumine"), str(reorder), "q.query", str(ds / f"{db.name}.mygraph"),
+                        str(ds / f"{db.name}.metadata")], cwd=d, stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL,
                        check=True)
         rows = [l.split() for l in open(d / "partialResultsCPU.txt") if l.strip()]
         if not rows:
@@ -227,7 +231,7 @@ def reference_arm(args, db, queries, workload):
         "config": {"workload": workload, "seed": args.seed, "patterns_per_step": wave,
                    "database_conversion_s": t_conv},
         "cpu_baseline": {"value": value, "unit": "embeddings/s", "cores": wave, "kind": "reference",
-                         "sample": f"{wave} seeded 2-7 vertex patterns per step sampled from the database, one "
+                         "sample": f"{wave} seeded patterns per step sampled from the {db.name} database, one "
                                    f"cpumine process each (it reloads the database per pattern)"},
         "e2e": {"value": value, "unit": "embeddings/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -354,21 +358,47 @@ def mine_bench(args, rank, world, local, dist, torch, gv, workloads, shard):
     # ---- batched vs plain per-pattern GPU path on a seeded sample of patterns
     sample = workloads.sample_patterns(db, args.sample, 2, 7, seed=1000 + rank)
     plans = [gv.Plan.from_text(q) for q in sample]
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    counts, sup_b, _ = gv.batch_count(gdb, plans, stream=sp, support=True)
-    torch.cuda.synchronize()
-    t_batch = time.perf_counter() - t0
-    t0 = time.perf_counter()
-    plain_rows, sup_p = 0, []
-    for p in plans:
-        r = gv.match(gdb, p, stream=sp)
-        rows = r.rows()
-        plain_rows += rows.shape[0]
-        sup_p.append(len(np.unique(db.graph_of(rows[:, 0].astype(np.int64)))) if rows.size else 0)
-        r.close()
-    t_plain = time.perf_counter() - t0
-    assert plain_rows == int(counts.sum()) and list(sup_b) == sup_p, "batched and plain paths disagree"
+
+    def batched_sample():
+        counts, sup, _ = gv.batch_count(gdb, plans, stream=sp, support=True)
+        return counts, list(sup)
+
+    def plain_sample():
+        rows_n, sup = 0, []
+        for p in plans:
+            r = gv.match(gdb, p, stream=sp)
+            rows = r.rows()
+            rows_n += rows.shape[0]
+            sup.append(len(np.unique(db.graph_of(rows[:, 0].astype(np.int64)))) if rows.size else 0)
+            r.close()
+        return rows_n, sup
+
+    def plain_count_sample():
+        n = 0
+        for p in plans:
+            r = gv.match(gdb, p, stream=sp, count_only=True)
+            n += r.num_rows
+            r.close()
+        return n
+
+    def wall(fn, reps=3):
+        # both paths warmed first: the first calls grow the stream-ordered
+        # pool, set kernel attributes and pin host staging
+        fn()
+        fn()
+        ts, out = [], None
+        for _ in range(reps):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            out = fn()
+            torch.cuda.synchronize()
+            ts.append(time.perf_counter() - t0)
+        return statistics.mean(ts), out
+
+    t_batch, (counts, sup_b) = wall(batched_sample)
+    t_plain, (plain_rows, sup_p) = wall(plain_sample)
+    t_plain_c, plain_count_rows = wall(plain_count_sample)
+    assert plain_rows == int(counts.sum()) == plain_count_rows and sup_b == sup_p, "batched and plain paths disagree"
 
     # ---- profiled mining run for the roofline of the dominant kernel
     with torch.cuda.stream(stream):
@@ -418,7 +448,11 @@ def mine_bench(args, rank, world, local, dist, torch, gv, workloads, shard):
                   "batched_embeddings_per_s": int(counts.sum()) / t_batch,
                   "plain_embeddings_per_s": plain_rows / t_plain,
                   "batched_over_plain": t_plain / t_batch,
-                  "path": "plain = one gva_match per pattern, rows to host, support from their graph ids"},
+                  "plain_count_only_embeddings_per_s": plain_count_rows / t_plain_c,
+                  "batched_over_plain_count_only": t_plain_c / t_batch,
+                  "timing": "wall clock, mean of 3 calls after 2 warm-up calls per path",
+                  "path": "batched = one gva_batch_count with supports; plain = one gva_match per pattern, rows "
+                          "to host, support from their graph ids (count_only: embeddings only)"},
         "roofline": {"bound": "hbm", "kernel": name, "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_source": peak_kind, "traffic": ncu_traffic(name, s),
                      "launches": s["launches"], "kernel_ms": s["ms"]},
@@ -471,12 +505,13 @@ def main():
     if args.impl == "reference":
         if rank != 0:
             return 0
-        db = workloads.config2(seed=args.seed)
         if args.workload == "mine":
+            db = workloads.config2(seed=args.seed)
             queries = workloads.sample_patterns(db, args.sample, 2, 7, seed=1000)
             wl = MINE_WORKLOAD.format(me=args.max_edges, ms=args.min_support)
         else:
-            queries = workloads.sample_patterns(db, args.queries, 3, 7, seed=1000)
+            db = workloads.config1(seed=1)
+            queries = workloads.config3_queries(db, args.queries, seed=1000)
             wl = WORKLOAD
         print(json.dumps(reference_arm(args, db, queries, wl)), flush=True)
         return 0
@@ -503,8 +538,8 @@ def main():
         if rank == 0:
             print(json.dumps(out), flush=True)
         return 0
-    db = workloads.config2(seed=args.seed)
-    queries = workloads.sample_patterns(db, args.queries, 3, 7, seed=1000 + rank)
+    db = workloads.config1(seed=1)
+    queries = workloads.config3_queries(db, args.queries, seed=1000 + rank)
     gdb = gv.Database.from_edges(db.vlabels, db.src, db.dst, db.elabels, device=local)
     gdb.set_graphs(db.first)
     plans = [gv.Plan.from_text(q) for q in queries]
@@ -513,7 +548,9 @@ def main():
     flush = torch.empty(512 << 20, dtype=torch.uint8, device="cuda")
 
     def batched_step(profile=False):
-        counts, support, stats = gv.batch_count(gdb, plans, stream=sp, support=True, profile=profile)
+        # int64 counts per (query, graph) and supports, copied to host memory
+        counts, (per_graph, support), stats = gv.batch_count(gdb, plans, stream=sp, graph_counts=True, support=True,
+                                                             profile=profile)
         return int(counts.sum()), stats
 
     def plain_step():
@@ -587,13 +624,13 @@ def main():
     # host), per-pattern embedding counts and supports out to host memory
     e2e_steps = max(1, args.steps)
     h2d = sum(len(q.encode()) for q in queries)
-    d2h = len(queries) * (8 + 4)
+    d2h = len(queries) * (8 + 4 + 8 * gdb.num_graphs)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     e2e_rows = 0
     for _ in range(e2e_steps):
         ps = [gv.Plan.from_text(q) for q in queries]
-        counts, support, _ = gv.batch_count(gdb, ps, stream=sp, support=True)
+        counts, _, _ = gv.batch_count(gdb, ps, stream=sp, graph_counts=True, support=True)
         e2e_rows += int(counts.sum())
         for p in ps:
             p.close()
@@ -614,9 +651,10 @@ def main():
             "steps": args.steps, "warmup": max(args.warmup, 3), "ms_per_step": t_sum / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
             "data": "synthetic (seeded generator of the configuration's shapes)",
-            "config": {"workload": WORKLOAD, "patterns_per_rank_per_step": len(queries), "seed": args.seed,
+            "config": {"workload": WORKLOAD, "patterns_per_rank_per_step": len(queries), "database_seed": 1,
+                       "query_seed": 1000,
                        "path": "batched: all patterns of a step advance together (gva_batch_count)",
-                       "outputs": "embeddings and supporting-graph count per pattern",
+                       "outputs": "int64 embedding counts per (query, graph) and supporting graphs per query",
                        "l2": "flushed between steps (512 MiB write)",
                        "parallelism": f"replicated database, patterns sharded over {world} rank(s)"},
             "plain": {"value": plain_value, "unit": "embeddings/s", "ms_per_step": sum(plain_ms) / args.steps,
@@ -629,7 +667,8 @@ def main():
             "batch": {k: pstats[k] for k in ("rounds", "splits", "launches", "trie_nodes")},
             "e2e": {"value": e2e_value, "unit": "embeddings/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h,
-                    "note": "pattern text planned on the host each step; counts and supports copied to host"},
+                    "note": "pattern text planned on the host each step; per-(query, graph) counts and supports "
+                            "copied to host"},
             "gpu_launches": launches,
             "clocks": clk,
         }

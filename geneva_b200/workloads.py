@@ -176,3 +176,10 @@ def sample_patterns(db: GraphDB, count: int, vmin: int, vmax: int, seed: int, p_
         lines += [f"e {a} {b} {l}" for (a, b), l in sorted(es.items())]
         out.append("\n".join(lines) + "\n")
     return out
+
+
+def config3_queries(db: GraphDB, count: int = 4096, seed: int = 1000) -> List[str]:
+    """4,096 query patterns of 3-8 vertices, each a connected induced subgraph
+    (every database edge among the chosen vertices kept) of a random graph of
+    `db`, so every query has at least one embedding."""
+    return sample_patterns(db, count, 3, 8, seed=seed, p_extra=1.0)
