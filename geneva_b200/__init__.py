@@ -23,7 +23,7 @@ from typing import List, Optional, Sequence
 import numpy as np
 
 __all__ = [
-    "GenevaError", "Database", "probe_graph", "convert_g", "batch_count", "kernel_launches", "mine", "MinedPattern", "Plan", "Result", "MODE_DV", "MODE_SV", "library", "library_path",
+    "GenevaError", "Database", "probe_graph", "convert_g", "batch_count", "kernel_launches", "mine", "mni_support", "MinedPattern", "Plan", "Result", "MODE_DV", "MODE_SV", "library", "library_path",
     "loadDataBase", "genMatchOrder", "genMatchOrderSingleV", "match", "gpumine", "gpumineSV",
 ]
 
@@ -64,10 +64,15 @@ REDUCE_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.POINTER(ctypes.c_uint32), ctyp
                              ctypes.c_uint64, ctypes.c_void_p)
 
 
+SUPPORT_GRAPHS = 0
+SUPPORT_MNI = 1
+
+
 class _MineOpts(ctypes.Structure):
     _fields_ = [("stream", ctypes.c_void_p), ("budget_bytes", ctypes.c_uint64), ("max_edges", ctypes.c_uint32),
                 ("min_support", ctypes.c_uint32), ("batch_limit", ctypes.c_uint32), ("profile", ctypes.c_uint32),
-                ("reduce", REDUCE_FN), ("reduce_user", ctypes.c_void_p)]
+                ("reduce", REDUCE_FN), ("reduce_user", ctypes.c_void_p), ("support_mode", ctypes.c_uint32),
+                ("mni_cap", ctypes.c_uint32)]
 
 
 class _MineStats(ctypes.Structure):
@@ -75,7 +80,13 @@ class _MineStats(ctypes.Structure):
                 ("levels", ctypes.c_uint64), ("pruned", ctypes.c_uint64), ("gpu_ms", ctypes.c_double),
                 ("host_ms", ctypes.c_double), ("gen_ms", ctypes.c_double), ("plan_ms", ctypes.c_double),
                 ("eval_ms", ctypes.c_double), ("merge_ms", ctypes.c_double), ("submit_ms", ctypes.c_double),
-                ("round_host_ms", ctypes.c_double), ("wait_ms", ctypes.c_double)]
+                ("round_host_ms", ctypes.c_double), ("wait_ms", ctypes.c_double), ("mni_tasks", ctypes.c_uint64),
+                ("mni_rounds", ctypes.c_uint64)]
+
+
+class _MniOpts(ctypes.Structure):
+    _fields_ = [("stream", ctypes.c_void_p), ("cap", ctypes.c_uint32), ("plain", ctypes.c_int),
+                ("profile", ctypes.c_int), ("reserved", ctypes.c_int)]
 
 
 class _BatchOpts(ctypes.Structure):
@@ -86,6 +97,12 @@ class _BatchOpts(ctypes.Structure):
 class _BatchStats(ctypes.Structure):
     _fields_ = [("gpu_ms", ctypes.c_double), ("rounds", ctypes.c_uint64), ("splits", ctypes.c_uint64),
                 ("launches", ctypes.c_uint64), ("trie_nodes", ctypes.c_uint64), ("kernels", _KernelStat * 5)]
+
+
+class _MniStats(ctypes.Structure):
+    _fields_ = [("gpu_ms", ctypes.c_double), ("rounds", ctypes.c_uint64), ("launches", ctypes.c_uint64),
+                ("tasks", ctypes.c_uint64), ("seeds", ctypes.c_uint64), ("roots", ctypes.c_uint64),
+                ("found", ctypes.c_uint64), ("kernel", _KernelStat)]
 
 
 def _declare(lib):
@@ -135,6 +152,7 @@ def _declare(lib):
         "gva_mine_free": (None, [vp]),
         "gva_mine_kernel_stats": (i32, [vp, P(_KernelStat), i32]),
         "gva_batch_count": (i32, [vp, vp, i32, P(_BatchOpts), vp, vp, vp, P(_BatchStats)]),
+        "gva_mni_support": (i32, [vp, vp, i32, P(_MniOpts), vp, P(_MniStats)]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)
@@ -386,13 +404,17 @@ class MinedPattern:
 
 
 def mine(db: Database, max_edges: int, min_support: int, stream: Optional[int] = None, budget_bytes: int = 0,
-         batch_limit: int = 0, profile: bool = False, reduce=None):
-    """Frequent connected patterns of a graph database (gva_mine).
+         batch_limit: int = 0, profile: bool = False, reduce=None, support: str = "graphs", mni_cap: int = 0):
+    """Frequent connected patterns (gva_mine).
 
+    support="graphs": a pattern's support is the number of database graphs
+    holding an embedding (needs Database.set_graphs).  support="mni": the
+    minimum image-based support on the whole data graph, reported as
+    min(MNI, mni_cap) (mni_cap 0 = min_support, which decides frequency).
     `reduce(supports, embeddings)` (numpy uint32 / uint64 arrays, updated in
     place) combines each level's counts across processes holding disjoint
-    graph shards.  Returns (patterns, stats); stats["kernels"] is filled
-    when profiling."""
+    graph shards (graph support only).  Returns (patterns, stats);
+    stats["kernels"] is filled when profiling."""
     lib = library()
     cb = REDUCE_FN(0)
     if reduce is not None:
@@ -405,7 +427,9 @@ def mine(db: Database, max_edges: int, min_support: int, stream: Optional[int] =
             except Exception:
                 return 1
         cb = REDUCE_FN(_cb)
-    o = _MineOpts(stream or None, budget_bytes, max_edges, min_support, batch_limit, 1 if profile else 0, cb, None)
+    mode = {"graphs": SUPPORT_GRAPHS, "mni": SUPPORT_MNI}[support]
+    o = _MineOpts(stream or None, budget_bytes, max_edges, min_support, batch_limit, 1 if profile else 0, cb, None,
+                  mode, mni_cap)
     h = ctypes.c_void_p()
     _check(lib.gva_mine(db._h, ctypes.byref(o), ctypes.byref(h)))
     try:
@@ -428,6 +452,26 @@ def mine(db: Database, max_edges: int, min_support: int, stream: Optional[int] =
     finally:
         lib.gva_mine_free(h)
     return pats, stats
+
+
+def mni_support(db: Database, patterns: Sequence[str], cap: int = 0, plain: bool = False, stream: Optional[int] = None,
+                profile: bool = False):
+    """Minimum image-based support of each pattern (.query text) on the data
+    graph, as min(MNI, cap) (cap 0 = exact) (gva_mni_support).  plain runs
+    one pattern at a time.  Returns (supports uint32[n], stats)."""
+    n = len(patterns)
+    enc = [p.encode() for p in patterns]
+    arr = (ctypes.c_char_p * max(n, 1))(*enc)
+    sup = np.zeros(n, dtype=np.uint32)
+    o = _MniOpts(stream or None, cap, 1 if plain else 0, 1 if profile else 0, 0)
+    st = _MniStats()
+    _check(library().gva_mni_support(db._h, ctypes.cast(arr, ctypes.c_void_p), n, ctypes.byref(o), sup.ctypes.data,
+                                     ctypes.byref(st)))
+    stats = {f: getattr(st, f) for f, _ in _MniStats._fields_ if f != "kernel"}
+    k = st.kernel
+    stats["kernel"] = dict(name=k.name.decode(), launches=int(k.launches), ms=float(k.ms), bytes=float(k.bytes),
+                           rows=float(k.rows))
+    return sup, stats
 
 
 # ---- reference-named entry points -------------------------------------------

@@ -343,7 +343,8 @@ int gva_mine(gva_db* db, const gva_mine_opts* opts, gva_mine_result** out) {
     *out = nullptr;
     gva_mine_result* r = new gva_mine_result();
     int st = run_mine(*db->dev, (cudaStream_t)opts->stream, opts->budget_bytes, opts->max_edges, opts->min_support,
-                      opts->batch_limit, opts->profile != 0, opts->reduce, opts->reduce_user, r->pats, r->stats);
+                      opts->batch_limit, opts->profile != 0, opts->reduce, opts->reduce_user, opts->support_mode,
+                      opts->mni_cap, r->pats, r->stats);
     if (st) {
         delete r;
         return st;
@@ -390,6 +391,45 @@ int gva_mine_get_stats(const gva_mine_result* res, gva_mine_stats* out) {
     out->submit_ms = res->stats.submit_ms;
     out->round_host_ms = res->stats.round_host_ms;
     out->wait_ms = res->stats.wait_ms;
+    out->mni_tasks = res->stats.mni_tasks;
+    out->mni_rounds = res->stats.mni_rounds;
+    return GVA_OK;
+}
+
+int gva_mni_support(gva_db* db, const char* const* pattern_texts, int n, const gva_mni_opts* opts, uint32_t* support,
+                    gva_mni_stats* stats) {
+    if (!db || n < 0 || (n > 0 && (!pattern_texts || !support))) return fail(GVA_ERR_ARG, "null argument");
+    gva_mni_opts o{};
+    if (opts) o = *opts;
+    std::vector<MniPattern> pats(n);
+    std::vector<char> absent(n, 0);
+    for (int i = 0; i < n; ++i) {
+        if (!pattern_texts[i]) return fail(GVA_ERR_ARG, "null pattern text");
+        bool ab = false;
+        int st = mni_pattern_from_text(*db->dev, pattern_texts[i], pats[i], ab);
+        if (st) return st;
+        absent[i] = ab ? 1 : 0;
+    }
+    std::vector<uint32_t> sup;
+    MniStats ms;
+    int st = run_mni(*db->dev, pats, absent, o.cap, o.plain != 0, o.profile != 0, (cudaStream_t)o.stream, sup, ms);
+    if (st) return st;
+    for (int i = 0; i < n; ++i) support[i] = sup[i];
+    if (stats) {
+        memset(stats, 0, sizeof *stats);
+        stats->gpu_ms = ms.gpu_ms;
+        stats->rounds = ms.rounds;
+        stats->launches = ms.launches;
+        stats->tasks = ms.tasks;
+        stats->seeds = ms.seeds;
+        stats->roots = ms.roots;
+        stats->found = ms.found;
+        strncpy(stats->kernel.name, kKernelNames[K_MNI], sizeof stats->kernel.name - 1);
+        stats->kernel.launches = ms.kstat.launches;
+        stats->kernel.ms = ms.kstat.ms;
+        stats->kernel.bytes = ms.kstat.bytes;
+        stats->kernel.rows = ms.kstat.rows;
+    }
     return GVA_OK;
 }
 

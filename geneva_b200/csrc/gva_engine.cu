@@ -308,9 +308,10 @@ int ensure_pool(int device) {
 
 }  // namespace
 
-const char* const kKernelNames[K_NUM] = {"ext_count", "ext_write", "red_count", "red_write", "scan_block_sums"};
+const char* const kKernelNames[K_NUM] = {"ext_count", "ext_write", "red_count", "red_write", "scan_block_sums",
+                                         "mni_search"};
 
-uint64_t kernel_launches() { return g_launches.load() + batch_kernel_launches(); }
+uint64_t kernel_launches() { return g_launches.load() + batch_kernel_launches() + mni_kernel_launches(); }
 
 void Profiler::begin(int kind, double bytes, cudaStream_t s, cudaEvent_t& a) {
     (void)kind;

@@ -39,7 +39,7 @@ struct DevDB {
 int upload_graph(HostGraph& g, int device, DevDB*& out);
 void free_devdb(DevDB* db);
 
-enum KernelKind { K_EXT_COUNT = 0, K_EXT_WRITE, K_RED_COUNT, K_RED_WRITE, K_SCAN, K_NUM };
+enum KernelKind { K_EXT_COUNT = 0, K_EXT_WRITE, K_RED_COUNT, K_RED_WRITE, K_SCAN, K_MNI, K_NUM };
 extern const char* const kKernelNames[K_NUM];
 
 struct KernelStat {
@@ -206,6 +206,7 @@ struct MinedPattern {
 
 struct MineStats {
     uint64_t candidates = 0, frequent = 0, embeddings = 0, levels = 0, pruned = 0;
+    uint64_t mni_tasks = 0, mni_rounds = 0, mni_found = 0;  // MNI mode
     double gpu_ms = 0.0, host_ms = 0.0, gen_ms = 0.0, plan_ms = 0.0, eval_ms = 0.0, merge_ms = 0.0;
     double submit_ms = 0.0, round_host_ms = 0.0, wait_ms = 0.0;
     KernelStat kstat[K_NUM];
@@ -213,9 +214,36 @@ struct MineStats {
 
 // Frequent connected patterns with up to max_edges edges (support = graphs).
 typedef int (*ReduceFn)(uint32_t* supports, uint64_t* embeddings, uint64_t n, void* user);
+// support_mode GVA_SUPPORT_GRAPHS: graphs holding an embedding (needs graph
+// ids); GVA_SUPPORT_MNI: min(MNI, mni_cap) on the whole data graph (mni_cap 0
+// = min_support, which decides frequency).
 int run_mine(DevDB& db, cudaStream_t s, uint64_t budget, uint32_t max_edges, uint32_t min_support,
-             uint32_t batch_limit, bool profile, ReduceFn reduce, void* reduce_user, std::vector<MinedPattern>& out,
-             MineStats& st);
+             uint32_t batch_limit, bool profile, ReduceFn reduce, void* reduce_user, uint32_t support_mode,
+             uint32_t mni_cap, std::vector<MinedPattern>& out, MineStats& st);
+
+// ---- single-graph MNI support (gva_mni.cu) ----
+constexpr int kMniMaxVertices = 8;
+// A connected pattern: dense vertex labels, el[a][b] = partition (1-based
+// edge label) of edge (a, b), 0 = no edge.
+struct MniPattern {
+    uint32_t n = 0;
+    uint32_t vl[kMniMaxVertices] = {};
+    uint8_t el[kMniMaxVertices][kMniMaxVertices] = {};
+};
+struct MniStats {
+    double gpu_ms = 0.0, host_ms = 0.0, wait_ms = 0.0;
+    uint64_t rounds = 0, launches = 0, tasks = 0;
+    uint64_t seeds = 0, roots = 0, opens = 0, scanned = 0, checks = 0, found = 0;  // filled when profiling
+    KernelStat kstat;
+};
+// Parses a .query-format pattern; `absent` is set when a label or edge label
+// does not occur in the database (support 0).
+int mni_pattern_from_text(const DevDB& db, const std::string& text, MniPattern& p, bool& absent);
+// support[q] = min(MNI of pats[q], cap) (cap 0 = exact); absent[q] != 0 gives 0.
+// plain: one pattern's rounds at a time instead of all patterns together.
+int run_mni(DevDB& db, const std::vector<MniPattern>& pats, const std::vector<char>& absent, uint32_t cap, bool plain,
+            bool profile, cudaStream_t s, std::vector<uint32_t>& support, MniStats& st);
+uint64_t mni_kernel_launches();
 
 size_t step_scratch_bytes(uint64_t in_rows);
 // run_step with the library's fixed device scratch array (no allocation).

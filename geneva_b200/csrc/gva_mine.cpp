@@ -301,13 +301,22 @@ constexpr uint32_t kBuckets = 256;  // candidate partitions by code hash (fixed:
 }  // namespace
 
 int run_mine(DevDB& db, cudaStream_t s, uint64_t budget, uint32_t max_edges, uint32_t min_support,
-             uint32_t batch_limit, bool profile, ReduceFn reduce, void* reduce_user, std::vector<MinedPattern>& out,
-             MineStats& st) {
+             uint32_t batch_limit, bool profile, ReduceFn reduce, void* reduce_user, uint32_t support_mode,
+             uint32_t mni_cap, std::vector<MinedPattern>& out, MineStats& st) {
     out.clear();
     st = MineStats();
-    if (!db.vgraph || db.num_graphs == 0) return fail(GVA_ERR_ARG, "mining needs graph ids (gva_db_set_graphs)");
-    if (max_edges == 0 || max_edges + 1 > GVA_MAX_QUERY_VERTICES) return fail(GVA_ERR_ARG, "max_edges out of range");
-    if (batch_limit == 0) batch_limit = 8192;
+    const bool mni = support_mode == GVA_SUPPORT_MNI;
+    if (support_mode != GVA_SUPPORT_GRAPHS && !mni) return fail(GVA_ERR_ARG, "unknown support mode");
+    if (mni) {
+        if (reduce) return fail(GVA_ERR_UNSUPPORTED, "MNI supports of graph shards do not add up; mine one graph per process");
+        if (max_edges == 0 || max_edges + 1 > (uint32_t)kMniMaxVertices)
+            return fail(GVA_ERR_ARG, "MNI mining handles max_edges 1..7");
+        if (mni_cap == 0) mni_cap = min_support;
+    } else {
+        if (!db.vgraph || db.num_graphs == 0) return fail(GVA_ERR_ARG, "mining needs graph ids (gva_db_set_graphs)");
+        if (max_edges == 0 || max_edges + 1 > GVA_MAX_QUERY_VERTICES) return fail(GVA_ERR_ARG, "max_edges out of range");
+    }
+    if (batch_limit == 0) batch_limit = mni ? 65536 : 8192;
     const uint32_t P = (uint32_t)db.parts.size();
     const std::vector<uint32_t>& labels = db.labels;
     auto t_host0 = std::chrono::steady_clock::now();
@@ -350,8 +359,47 @@ int run_mine(DevDB& db, cudaStream_t s, uint64_t budget, uint32_t max_edges, uin
     // planned first and ordered by their step sequences, so that candidates
     // sharing plan prefixes land in the same batch (one trie: a shared prefix
     // is matched once); then they run in bounded batches.
+    // MNI: image-set supports of every candidate on the one data graph, in
+    // batches of batch_limit patterns (no embedding counts)
+    auto evaluate_mni = [&](const std::vector<Pattern>& cands, std::vector<uint32_t>& sup,
+                            std::vector<uint64_t>& emb) -> int {
+        const size_t n = cands.size();
+        sup.assign(n, 0);
+        emb.assign(n, 0);
+        std::vector<MniPattern> mp;
+        std::vector<uint32_t> bsup;
+        for (size_t b0 = 0; b0 < n; b0 += batch_limit) {
+            const size_t b1 = std::min(n, b0 + (size_t)batch_limit);
+            mp.assign(b1 - b0, MniPattern());
+            for (size_t i = b0; i < b1; ++i) {
+                const Pattern& c = cands[i];
+                MniPattern& m = mp[i - b0];
+                m.n = c.n;
+                for (uint32_t v = 0; v < c.n; ++v) m.vl[v] = c.vl[v];
+                for (uint32_t e = 0; e < c.ne; ++e)
+                    m.el[c.edges[e].u][c.edges[e].v] = m.el[c.edges[e].v][c.edges[e].u] = (uint8_t)c.edges[e].el;
+            }
+            MniStats ms;
+            int rc = run_mni(db, mp, {}, mni_cap, false, profile, s, bsup, ms);
+            if (rc) return rc;
+            for (size_t i = b0; i < b1; ++i) sup[i] = bsup[i - b0];
+            gpu_ms += ms.gpu_ms;
+            st.wait_ms += ms.wait_ms;
+            st.mni_tasks += ms.tasks;
+            st.mni_rounds += ms.rounds;
+            st.mni_found += ms.found;
+            st.kstat[K_MNI].launches += ms.kstat.launches;
+            st.kstat[K_MNI].ms += ms.kstat.ms;
+            st.kstat[K_MNI].bytes += ms.kstat.bytes;
+            st.kstat[K_MNI].rows += ms.kstat.rows;
+        }
+        st.candidates += n;
+        return GVA_OK;
+    };
+
     auto evaluate = [&](const std::vector<Pattern>& cands, std::vector<uint32_t>& sup, std::vector<uint64_t>& emb) -> int {
         const size_t n = cands.size();
+        if (mni) return evaluate_mni(cands, sup, emb);
         sup.assign(n, 0);
         emb.assign(n, 0);
         if (n == 0) return GVA_OK;

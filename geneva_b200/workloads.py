@@ -183,3 +183,69 @@ def config3_queries(db: GraphDB, count: int = 4096, seed: int = 1000) -> List[st
     (every database edge among the chosen vertices kept) of a random graph of
     `db`, so every query has at least one embedding."""
     return sample_patterns(db, count, 3, 8, seed=seed, p_extra=1.0)
+
+
+def _sorted_unique(x: np.ndarray) -> np.ndarray:
+    x = np.sort(x, kind="quicksort")
+    if len(x) == 0:
+        return x
+    keep = np.empty(len(x), dtype=bool)
+    keep[0] = True
+    np.not_equal(x[1:], x[:-1], out=keep[1:])
+    return x[keep]
+
+
+def rmat_graph(scale: int, num_edges: int, vlabel_k: int, vlabel_zipf: Optional[float], seed: int,
+               a: float = 0.57, b: float = 0.19, c: float = 0.19, name: str = "rmat") -> GraphDB:
+    """One R-MAT graph (Chakrabarti et al.): 2**scale vertices, each edge's
+    endpoints chosen bit by bit from the quadrant probabilities (a, b, c,
+    1-a-b-c); self-loops and duplicate edges dropped and edges redrawn until
+    `num_edges` distinct undirected edges exist.  Vertex labels Zipf over
+    `vlabel_k` labels (uniform when vlabel_zipf is None); one edge label.
+    Returned as a one-graph database (first = [1, V + 1])."""
+    rng = np.random.default_rng(seed)
+    n = 1 << scale
+    ta, tab, tabc = int(a * 65536), int((a + b) * 65536), int((a + b + c) * 65536)
+    keys = np.empty(0, dtype=np.uint64)
+    for _ in range(64):
+        need = num_edges - len(keys)
+        if need <= 0:
+            break
+        m = int(need * 1.2) + 1024
+        src = np.zeros(m, dtype=np.uint32)
+        dst = np.zeros(m, dtype=np.uint32)
+        for _lvl in range(scale):
+            # quadrant q in 0..3 = (src bit, dst bit) from one 16-bit draw
+            r = rng.integers(0, 65536, size=m, dtype=np.uint16)
+            q = (r >= ta).astype(np.uint8)
+            q += r >= tab
+            q += r >= tabc
+            src <<= 1
+            dst <<= 1
+            src |= q >> 1
+            dst |= q & 1
+        ok = src != dst
+        lo = np.minimum(src[ok], dst[ok]).astype(np.uint64)
+        hi = np.maximum(src[ok], dst[ok]).astype(np.uint64)
+        keys = _sorted_unique(np.concatenate([keys, (lo << np.uint64(32)) | hi]))
+    if len(keys) > num_edges:  # drop a seeded random surplus
+        keys = np.sort(keys[rng.permutation(len(keys))[:num_edges]])
+    src = ((keys >> np.uint64(32)) + np.uint64(1)).astype(np.uint32)
+    dst = ((keys & np.uint64(0xffffffff)) + np.uint64(1)).astype(np.uint32)
+    if vlabel_zipf is None:
+        vl = rng.integers(1, vlabel_k + 1, size=n).astype(np.uint32)
+    else:
+        vl = zipf_labels(rng, n, vlabel_k, vlabel_zipf)
+    vlabels = np.zeros(n + 1, dtype=np.uint32)
+    vlabels[1:] = vl
+    el = np.ones(len(src), dtype=np.uint32)
+    first = np.array([1, n + 1], dtype=np.int64)
+    return GraphDB(name, vlabels, src, dst, el, first,
+                   dict(scale=scale, edges=num_edges, a=a, b=b, c=c, vertex_labels=vlabel_k,
+                        vertex_label_zipf=vlabel_zipf, seed=seed))
+
+
+def config4(seed: int = 4, scale: int = 22, num_edges: int = 64 << 20) -> GraphDB:
+    """R-MAT (a=0.57, b=c=0.19) with 2^22 (~4M) vertices and 64M undirected
+    edges after dedup, 32 vertex labels Zipf(1.0), one edge label."""
+    return rmat_graph(scale, num_edges, 32, 1.0, seed, name="config4")

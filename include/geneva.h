@@ -215,15 +215,20 @@ void gva_session_free(gva_session* s);
  * all-reduce sum); arrays are updated in place; return 0 on success. */
 typedef int (*gva_reduce_fn)(uint32_t* supports, uint64_t* embeddings, uint64_t n, void* user);
 
+#define GVA_SUPPORT_GRAPHS 0 /* graphs of the database holding an embedding (gva_db_set_graphs) */
+#define GVA_SUPPORT_MNI 1    /* minimum image-based support on one data graph */
+
 typedef struct gva_mine_opts {
     void* stream;
     uint64_t budget_bytes;
     uint32_t max_edges;
     uint32_t min_support;
-    uint32_t batch_limit;  /* candidates per batched run (0 = 8192) */
+    uint32_t batch_limit;  /* candidates per batched run (0 = 8192; MNI: 65536) */
     uint32_t profile;      /* 1: per-kernel CUDA-event timing (gva_mine_kernel_stats) */
-    gva_reduce_fn reduce;  /* NULL on one process */
+    gva_reduce_fn reduce;  /* NULL on one process (GVA_SUPPORT_GRAPHS only) */
     void* reduce_user;
+    uint32_t support_mode; /* GVA_SUPPORT_GRAPHS or GVA_SUPPORT_MNI */
+    uint32_t mni_cap;      /* MNI: supports are min(MNI, mni_cap); 0 = min_support */
 } gva_mine_opts;
 
 typedef struct gva_mine_stats {
@@ -241,6 +246,8 @@ typedef struct gva_mine_stats {
     double submit_ms;    /* within eval: building the step trie and descriptors */
     double round_host_ms;/* within eval: per-round host bookkeeping */
     double wait_ms;      /* within eval: host waiting for the GPU */
+    uint64_t mni_tasks;  /* MNI: rooted searches set up (one per pattern orbit) */
+    uint64_t mni_rounds; /* MNI: search rounds */
 } gva_mine_stats;
 
 typedef struct gva_mine_result gva_mine_result;
@@ -254,6 +261,36 @@ int gva_mine_get_stats(const gva_mine_result* res, gva_mine_stats* out);
 /* per-kernel totals when opts->profile was set; returns the number of kinds */
 int gva_mine_kernel_stats(const gva_mine_result* res, gva_kernel_stat* out, int cap);
 void gva_mine_free(gva_mine_result* res);
+
+/* ---- single-graph support: MNI ----------------------------------------------
+ * The minimum image-based support of each pattern (for every pattern vertex,
+ * the number of distinct data vertices some embedding maps it to; the
+ * minimum over the pattern's vertices), decided by rooted existence searches
+ * on the device, one per automorphism orbit and data vertex, stopped once an
+ * orbit reaches the cap.  Replaces nothing in the reference (it enumerates
+ * the embeddings of one pattern, src/gpumine.cpp:994-1061, and has no support
+ * notion); embeddings follow its semantics (injective, vertex and edge labels
+ * kept, non-induced).  Patterns are .query text (`v id label`, `e a b
+ * elabel`), connected, up to 8 vertices; a label absent from the database
+ * gives support 0.  plain = 1 runs one pattern at a time (the per-query
+ * path); the default runs all patterns' searches in shared rounds. */
+typedef struct gva_mni_opts {
+    void* stream;
+    uint32_t cap;  /* supports are min(MNI, cap); 0 = exact MNI */
+    int plain;
+    int profile;   /* 1: kernel timing and search counters in stats */
+    int reserved;
+} gva_mni_opts;
+
+typedef struct gva_mni_stats {
+    double gpu_ms;
+    uint64_t rounds, launches, tasks;
+    uint64_t seeds, roots, found; /* profile: vertices tried, roots past the degree filter, embeddings found */
+    gva_kernel_stat kernel;       /* profile: mni_search launches, CUDA-event ms, algorithmic bytes */
+} gva_mni_stats;
+
+int gva_mni_support(gva_db* db, const char* const* pattern_texts, int n, const gva_mni_opts* opts, uint32_t* support,
+                    gva_mni_stats* stats);
 
 /* ---- L4: one phase step on caller-owned device buffers ----------------------
  * Replaces the kernel launchers of include/miningPattern.h:1-30

@@ -10,6 +10,7 @@
 #include "geneva_oracle.h"
 
 #include <algorithm>
+#include <array>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -872,5 +873,181 @@ int oracle_count_capped(const oracle_graph* g, const char* text, uint64_t cap_ro
 }
 
 void oracle_free(void* p) { free(p); }
+
+}  // extern "C"
+
+// ---------------------------------------------------------------- MNI ------
+// Test infrastructure: the CPU statement of minimum image-based support.
+struct oracle_mni_graph {
+    uint n = 0;
+    std::vector<uint> vlabel;                 // original label per id (0..n)
+    std::vector<std::vector<uint>> by_label;  // original label -> vertex ids (ascending)
+    // adjacency per edge label: adj[el][v] = neighbours sorted by (label, id)
+    std::vector<std::vector<std::vector<uint>>> adj;
+};
+
+namespace {
+
+struct MniPat {
+    uint n = 0;
+    uint vl[8];
+    uint el[8][8];
+};
+
+bool parse_mni_pattern(const char* text, MniPat& p) {
+    std::istringstream in(text);
+    std::string t;
+    std::vector<std::pair<uint, uint>> vs;
+    std::vector<std::array<uint, 3>> es;
+    while (in >> t) {
+        if (t == "v") {
+            uint a, b;
+            in >> a >> b;
+            vs.push_back({a, b});
+        } else if (t == "e") {
+            uint a, b, c;
+            in >> a >> b >> c;
+            es.push_back({a, b, c});
+        } else {
+            return false;
+        }
+    }
+    if (vs.empty() || vs.size() > 8) return false;
+    p.n = (uint)vs.size();
+    memset(p.el, 0, sizeof p.el);
+    for (auto& v : vs) {
+        if (v.first >= p.n) return false;
+        p.vl[v.first] = v.second;
+    }
+    for (auto& e : es) {
+        if (e[0] >= p.n || e[1] >= p.n) return false;
+        p.el[e[0]][e[1]] = p.el[e[1]][e[0]] = e[2];
+    }
+    return true;
+}
+
+// all vertex permutations that keep labels and edges; orbit[v] = min image
+void mni_orbits(const MniPat& p, uint* orbit) {
+    uint perm[8];
+    for (uint i = 0; i < p.n; ++i) perm[i] = i, orbit[i] = i;
+    do {
+        bool ok = true;
+        for (uint i = 0; i < p.n && ok; ++i) ok = p.vl[perm[i]] == p.vl[i];
+        for (uint i = 0; i < p.n && ok; ++i)
+            for (uint j = 0; j < p.n && ok; ++j) ok = p.el[perm[i]][perm[j]] == p.el[i][j];
+        if (ok)
+            for (uint i = 0; i < p.n; ++i) orbit[i] = std::min(orbit[i], perm[i]);
+    } while (std::next_permutation(perm, perm + p.n));
+    for (int it = 0; it < 8; ++it)
+        for (uint i = 0; i < p.n; ++i) orbit[i] = orbit[orbit[i]];
+}
+
+struct MniSearch {
+    const oracle_mni_graph& g;
+    const MniPat& p;
+    uint order[8];
+    uint f[8];
+    // neighbours of v (edge label el) with vertex label lab
+    std::pair<const uint*, const uint*> seg(uint v, uint el, uint lab) const {
+        if (el >= g.adj.size() || g.adj[el].empty()) return {nullptr, nullptr};
+        const std::vector<uint>& a = g.adj[el][v];
+        auto lo = std::lower_bound(a.begin(), a.end(), lab, [&](uint w, uint l) { return g.vlabel[w] < l; });
+        auto hi = std::upper_bound(lo, a.end(), lab, [&](uint l, uint w) { return l < g.vlabel[w]; });
+        return {a.data() + (lo - a.begin()), a.data() + (hi - a.begin())};
+    }
+    bool extend(uint k) {
+        if (k == p.n) return true;
+        const uint u = order[k];
+        // candidates: neighbours of the first matched neighbour of u
+        uint j0 = 8;
+        for (uint j = 0; j < k && j0 == 8; ++j)
+            if (p.el[u][order[j]]) j0 = j;
+        auto s = seg(f[j0], p.el[u][order[j0]], p.vl[u]);
+        for (const uint* c = s.first; c != s.second; ++c) {
+            bool ok = true;
+            for (uint j = 0; j < k && ok; ++j) {
+                if (f[j] == *c) ok = false;
+                else if (j != j0 && p.el[u][order[j]]) {
+                    auto t = seg(f[j], p.el[u][order[j]], p.vl[u]);
+                    ok = std::binary_search(t.first, t.second, *c,
+                                            [&](uint a, uint b) { return g.vlabel[a] != g.vlabel[b] ? g.vlabel[a] < g.vlabel[b] : a < b; });
+                }
+            }
+            if (!ok) continue;
+            f[k] = *c;
+            if (extend(k + 1)) return true;
+        }
+        return false;
+    }
+};
+
+}  // namespace
+
+extern "C" {
+
+int oracle_mni_graph_from_edges(const uint32_t* vl, uint32_t maxid, const uint32_t* src, const uint32_t* dst,
+                                const uint32_t* el, uint64_t ne, oracle_mni_graph** out) {
+    oracle_mni_graph* g = new oracle_mni_graph();
+    g->n = maxid;
+    g->vlabel.assign(vl, vl + maxid + 1);
+    uint maxl = 0, P = 0;
+    for (uint v = 1; v <= maxid; ++v) maxl = std::max(maxl, g->vlabel[v]);
+    g->by_label.assign(maxl + 1, {});
+    for (uint v = 1; v <= maxid; ++v) g->by_label[g->vlabel[v]].push_back(v);
+    for (uint64_t i = 0; i < ne; ++i) P = std::max(P, el[i]);
+    g->adj.assign(P + 1, {});
+    for (uint l = 1; l <= P; ++l) g->adj[l].assign(maxid + 1, {});
+    for (uint64_t i = 0; i < ne; ++i) {
+        g->adj[el[i]][src[i]].push_back(dst[i]);
+        g->adj[el[i]][dst[i]].push_back(src[i]);
+    }
+    for (auto& part : g->adj)
+        for (auto& l : part) {
+            std::sort(l.begin(), l.end(), [&](uint a, uint b) {
+                return g->vlabel[a] != g->vlabel[b] ? g->vlabel[a] < g->vlabel[b] : a < b;
+            });
+            l.erase(std::unique(l.begin(), l.end()), l.end());
+        }
+    *out = g;
+    return 0;
+}
+
+void oracle_mni_graph_free(oracle_mni_graph* g) { delete g; }
+
+int oracle_mni(const oracle_mni_graph* g, const char* text, uint32_t cap, uint32_t* support, uint64_t* searches) {
+    MniPat p;
+    if (!parse_mni_pattern(text, p)) return fail("bad pattern text");
+    if (cap == 0) cap = NONE;
+    uint orbit[8];
+    mni_orbits(p, orbit);
+    uint best = cap;
+    uint64_t ns = 0;
+    for (uint r = 0; r < p.n; ++r) {
+        if (orbit[r] != r) continue;
+        MniSearch s{*g, p, {}, {}};
+        // search order: breadth-first from r, pattern vertex ids ascending
+        uint seen = 1u << r, k = 1;
+        s.order[0] = r;
+        for (uint h = 0; h < k; ++h)
+            for (uint w = 0; w < p.n; ++w)
+                if (p.el[s.order[h]][w] && !(seen >> w & 1)) {
+                    seen |= 1u << w;
+                    s.order[k++] = w;
+                }
+        if (k != p.n) return fail("pattern is not connected");
+        uint count = 0;
+        if (p.vl[r] < g->by_label.size())
+            for (uint v : g->by_label[p.vl[r]]) {
+                if (count >= best) break;
+                s.f[0] = v;
+                ++ns;
+                if (s.extend(1)) ++count;
+            }
+        best = std::min(best, count);
+    }
+    *support = best;
+    if (searches) *searches = ns;
+    return 0;
+}
 
 }  // extern "C"

@@ -42,6 +42,21 @@ int oracle_count_capped(const oracle_graph* g, const char* query_text, uint64_t 
 void oracle_free(void* p);
 const char* oracle_last_error(void);
 
+/* MNI support on one data graph (no counterpart in the reference, which has
+ * no support notion): for each automorphism orbit of the pattern, the data
+ * vertices some embedding maps the orbit's representative to, decided one
+ * vertex at a time by a depth-first existence search; support = the smallest
+ * such set, reported as min(MNI, cap) (cap 0 = exact).  Single-threaded,
+ * over its own sorted adjacency (no per-vertex maps), so it scales to the
+ * large single-graph configuration for bounded samples. */
+typedef struct oracle_mni_graph oracle_mni_graph;
+int oracle_mni_graph_from_edges(const uint32_t* vlabels, uint32_t max_id, const uint32_t* src, const uint32_t* dst,
+                                const uint32_t* elabel, uint64_t ne, oracle_mni_graph** out);
+void oracle_mni_graph_free(oracle_mni_graph* g);
+/* *searches receives the number of rooted searches run (may be NULL). */
+int oracle_mni(const oracle_mni_graph* g, const char* pattern_text, uint32_t cap, uint32_t* support,
+               uint64_t* searches);
+
 #ifdef __cplusplus
 }
 #endif

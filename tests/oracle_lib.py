@@ -49,6 +49,9 @@ class Oracle:
         lib.oracle_count_capped.argtypes = [vp, ctypes.c_char_p, u64, P(u64)]
         lib.oracle_free.argtypes = [vp]
         lib.oracle_last_error.restype = ctypes.c_char_p
+        lib.oracle_mni_graph_from_edges.argtypes = [vp, u32, vp, vp, vp, u64, P(vp)]
+        lib.oracle_mni_graph_free.argtypes = [vp]
+        lib.oracle_mni.argtypes = [vp, ctypes.c_char_p, u32, P(u32), P(u64)]
         self.lib = lib
 
     def load(self, mygraph, metadata):
@@ -100,3 +103,25 @@ class Oracle:
         if st:
             raise RuntimeError(self.lib.oracle_last_error().decode())
         return int(n.value)
+
+    # ---- MNI on one data graph (CPU existence search) ----
+    def mni_graph(self, vlabels, src, dst, elabel):
+        vl = np.ascontiguousarray(vlabels, dtype=np.uint32)
+        s = np.ascontiguousarray(src, dtype=np.uint32)
+        d = np.ascontiguousarray(dst, dtype=np.uint32)
+        e = np.ascontiguousarray(elabel, dtype=np.uint32)
+        h = ctypes.c_void_p()
+        self.lib.oracle_mni_graph_from_edges(vl.ctypes.data, len(vl) - 1, s.ctypes.data, d.ctypes.data,
+                                             e.ctypes.data, len(s), ctypes.byref(h))
+        return h
+
+    def mni_graph_free(self, g):
+        self.lib.oracle_mni_graph_free(g)
+
+    def mni(self, g, text: str, cap: int = 0):
+        """-> (min(MNI, cap) (cap 0 = exact), rooted searches run)"""
+        sup = ctypes.c_uint32()
+        ns = ctypes.c_uint64()
+        if self.lib.oracle_mni(g, text.encode(), cap, ctypes.byref(sup), ctypes.byref(ns)):
+            raise RuntimeError(self.lib.oracle_last_error().decode())
+        return int(sup.value), int(ns.value)
