@@ -16,6 +16,7 @@ from __future__ import annotations
 
 import ctypes
 import os
+from collections import abc as _abc
 from dataclasses import dataclass
 from pathlib import Path
 from typing import List, Optional, Sequence
@@ -23,7 +24,7 @@ from typing import List, Optional, Sequence
 import numpy as np
 
 __all__ = [
-    "GenevaError", "Database", "probe_graph", "convert_g", "batch_count", "kernel_launches", "mine", "mni_support", "MinedPattern", "Plan", "Result", "MODE_DV", "MODE_SV", "library", "library_path",
+    "GenevaError", "Database", "probe_graph", "convert_g", "batch_count", "kernel_launches", "mine", "mni_support", "MinedPatterns", "MinedPattern", "Plan", "Result", "MODE_DV", "MODE_SV", "library", "library_path",
     "loadDataBase", "genMatchOrder", "genMatchOrderSingleV", "match", "gpumine", "gpumineSV",
 ]
 
@@ -151,6 +152,7 @@ def _declare(lib):
         "gva_mine_get_stats": (i32, [vp, P(_MineStats)]),
         "gva_mine_free": (None, [vp]),
         "gva_mine_kernel_stats": (i32, [vp, P(_KernelStat), i32]),
+        "gva_mine_export": (sz, [vp, vp, sz, vp, vp, vp, vp]),
         "gva_batch_count": (i32, [vp, vp, i32, P(_BatchOpts), vp, vp, vp, P(_BatchStats)]),
         "gva_mni_support": (i32, [vp, vp, i32, P(_MniOpts), vp, P(_MniStats)]),
     }
@@ -403,6 +405,39 @@ class MinedPattern:
     embeddings: int
 
 
+class MinedPatterns(_abc.Sequence):
+    """The patterns of one gva_mine call, copied out in one gva_mine_export:
+    numpy arrays `edges`, `supports`, `embeddings` and the pattern texts,
+    decoded one at a time on access (runs can yield tens of millions)."""
+
+    def __init__(self, blob: np.ndarray, offsets: np.ndarray, edges: np.ndarray, supports: np.ndarray,
+                 embeddings: np.ndarray):
+        self._blob, self._off = blob, offsets
+        self.edges, self.supports, self.embeddings = edges, supports, embeddings
+
+    def __len__(self) -> int:
+        return len(self.edges)
+
+    @property
+    def text_bytes(self) -> int:
+        """Bytes of all pattern texts (without terminators)."""
+        return len(self._blob) - len(self)
+
+    def text(self, i: int) -> str:
+        a = int(self._off[i])
+        b = int(self._off[i + 1]) - 1 if i + 1 < len(self._off) else len(self._blob) - 1
+        return self._blob[a:b].tobytes().decode()
+
+    def __getitem__(self, i):
+        if isinstance(i, slice):
+            return [self[j] for j in range(*i.indices(len(self)))]
+        if i < 0:
+            i += len(self)
+        if not 0 <= i < len(self):
+            raise IndexError(i)
+        return MinedPattern(self.text(i), int(self.edges[i]), int(self.supports[i]), int(self.embeddings[i]))
+
+
 def mine(db: Database, max_edges: int, min_support: int, stream: Optional[int] = None, budget_bytes: int = 0,
          batch_limit: int = 0, profile: bool = False, reduce=None, support: str = "graphs", mni_cap: int = 0):
     """Frequent connected patterns (gva_mine).
@@ -433,14 +468,16 @@ def mine(db: Database, max_edges: int, min_support: int, stream: Optional[int] =
     h = ctypes.c_void_p()
     _check(lib.gva_mine(db._h, ctypes.byref(o), ctypes.byref(h)))
     try:
-        pats = []
-        e, s_, m = ctypes.c_uint32(), ctypes.c_uint32(), ctypes.c_uint64()
-        for i in range(lib.gva_mine_num_patterns(h)):
-            _check(lib.gva_mine_get(h, i, ctypes.byref(e), ctypes.byref(s_), ctypes.byref(m)))
-            n = lib.gva_mine_pattern_text(h, i, None, 0)
-            buf = ctypes.create_string_buffer(n + 1)
-            lib.gva_mine_pattern_text(h, i, buf, n + 1)
-            pats.append(MinedPattern(buf.value.decode(), e.value, s_.value, m.value))
+        n = lib.gva_mine_num_patterns(h)
+        need = lib.gva_mine_export(h, None, 0, None, None, None, None)
+        blob = np.empty(max(need, 1), dtype=np.uint8)
+        off = np.empty(n, dtype=np.uint64)
+        edges = np.empty(n, dtype=np.uint32)
+        sups = np.empty(n, dtype=np.uint32)
+        embs = np.empty(n, dtype=np.uint64)
+        lib.gva_mine_export(h, blob.ctypes.data, need, off.ctypes.data, edges.ctypes.data, sups.ctypes.data,
+                            embs.ctypes.data)
+        pats = MinedPatterns(blob[:need], off, edges, sups, embs)
         st = _MineStats()
         _check(lib.gva_mine_get_stats(h, ctypes.byref(st)))
         stats = {f: getattr(st, f) for f, _ in _MineStats._fields_}

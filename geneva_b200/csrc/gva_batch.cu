@@ -24,6 +24,7 @@
 #include <cstring>
 #include <memory>
 #include <map>
+#include <mutex>
 #include <unordered_map>
 #include <numeric>
 #include <string>
@@ -67,18 +68,6 @@ struct BatchCtx {
     uint32_t G;
     uint32_t words;           // bitmap words per query
 };
-
-__device__ __forceinline__ int find_task(const uint64_t* __restrict__ block0, int ntasks, uint64_t b) {
-    int lo = 0, hi = ntasks - 1;  // largest t with block0[t] <= b
-    while (lo < hi) {
-        const int mid = (lo + hi + 1) >> 1;
-        if (__ldg(block0 + mid) <= b)
-            lo = mid;
-        else
-            hi = mid - 1;
-    }
-    return lo;
-}
 
 // Per-round task reference: the step parameters live in a per-node
 // descriptor uploaded once per submitted wave; a round uploads only these.
@@ -131,10 +120,10 @@ __device__ __forceinline__ void add_graph_count(const BatchCtx& c, uint32_t quer
 
 __global__ void __launch_bounds__(kThreads)
 batch_count_kernel(const TaskDesc* __restrict__ nodes, const TaskRef* __restrict__ refs,
-                   const uint64_t* __restrict__ block0, int ntasks, uint64_t* __restrict__ block_sums, BatchCtx ctx) {
+                   const uint32_t* __restrict__ blk_task, uint64_t* __restrict__ block_sums, BatchCtx ctx) {
     __shared__ TaskDesc d;
     const uint64_t b = blockIdx.x;
-    const int t = find_task(block0, ntasks, b);
+    const int t = (int)__ldg(blk_task + b);
     load_task(d, nodes, refs, t);
     const uint64_t r = (b - d.block0) * kRowsPerBlock + threadIdx.x;
     uint32_t c = 0;
@@ -168,7 +157,7 @@ __global__ void task_totals_kernel(const uint64_t* __restrict__ block0, int ntas
 // Persistent: each CTA repeatedly takes the next 256-row item.
 __global__ void __launch_bounds__(kThreads)
 batch_write_kernel(const TaskDesc* __restrict__ nodes, const TaskRef* __restrict__ refs,
-                   const uint64_t* __restrict__ block0, int ntasks, uint64_t nblocks,
+                   const uint64_t* __restrict__ block0, const uint32_t* __restrict__ blk_task, uint64_t nblocks,
                    const uint64_t* __restrict__ sums, uint32_t* __restrict__ const* __restrict__ task_out,
                    unsigned long long* __restrict__ queue) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -180,7 +169,7 @@ batch_write_kernel(const TaskDesc* __restrict__ nodes, const TaskRef* __restrict
         __syncthreads();
         const uint64_t b = item_s;
         if (b >= nblocks) return;
-        const int t = find_task(block0, ntasks, b);
+        const int t = (int)__ldg(blk_task + b);
         uint32_t* out = task_out[t];
         if (out == nullptr) {  // task deferred or counted only: nothing to write
             __syncthreads();
@@ -336,20 +325,51 @@ std::atomic<uint64_t> g_batch_launches{0};
 
 uint64_t batch_kernel_launches() { return g_batch_launches.load(); }
 
-char* Staging::get(size_t need) {
-    if (need > cap) {
-        if (p) cudaFreeHost(p);
-        cap = std::max(need, cap * 2);
-        if (cudaMallocHost((void**)&p, cap) != cudaSuccess) {
-            p = nullptr;
-            cap = 0;
+// Pinned host buffers are expensive to create (page locking), and every
+// batched run and MNI call stages through them; released buffers are kept in
+// a process-wide pool and handed to the next Staging that needs one.
+namespace {
+std::mutex g_pin_mu;
+std::vector<std::pair<char*, size_t>> g_pin_free;  // (buffer, capacity)
+
+char* pin_take(size_t need, size_t& cap) {
+    {
+        std::lock_guard<std::mutex> lk(g_pin_mu);
+        size_t best = g_pin_free.size();
+        for (size_t i = 0; i < g_pin_free.size(); ++i)
+            if (g_pin_free[i].second >= need && (best == g_pin_free.size() || g_pin_free[i].second < g_pin_free[best].second))
+                best = i;
+        if (best < g_pin_free.size()) {
+            char* p = g_pin_free[best].first;
+            cap = g_pin_free[best].second;
+            g_pin_free.erase(g_pin_free.begin() + best);
+            return p;
         }
+    }
+    size_t c = (size_t)1 << 20;
+    while (c < need) c <<= 1;
+    char* p = nullptr;
+    if (cudaMallocHost((void**)&p, c) != cudaSuccess) return nullptr;
+    cap = c;
+    return p;
+}
+
+void pin_give(char* p, size_t cap) {
+    if (!p) return;
+    std::lock_guard<std::mutex> lk(g_pin_mu);
+    g_pin_free.push_back({p, cap});
+}
+}  // namespace
+
+char* Staging::get(size_t need) {
+    if (need > cap || !p) {
+        pin_give(p, cap);
+        p = pin_take(std::max(need, cap * 2), cap);
+        if (!p) cap = 0;
     }
     return p;
 }
-Staging::~Staging() {
-    if (p) cudaFreeHost(p);
-}
+Staging::~Staging() { pin_give(p, cap); }
 
 // ---------------------------------------------------------------------------
 // BatchSession: the persistent form of the batched engine.  Plans are
@@ -365,7 +385,7 @@ BatchSession::~BatchSession() {
     cudaSetDevice(db.device);
     active.clear();
     if (staged) cudaEventDestroy(staged);
-    for (void* p : {(void*)d_desc, (void*)d_sums, (void*)d_small, acc, d_nodes})
+    for (void* p : {(void*)d_desc, (void*)d_sums, (void*)d_small, (void*)d_blk, acc, d_nodes})
         if (p) cudaFreeAsync(p, s);
     cudaStreamSynchronize(s);
 }
@@ -465,7 +485,7 @@ void BatchSession::fill_node_desc(int id, void* out) const {
     const BNode& nd = nodes[id];
     TaskDesc& d = *reinterpret_cast<TaskDesc*>(out);
     memset(&d, 0, sizeof d);
-    const Step& st = nd.step;
+    const Step& st = node_steps[id];
     d.kind = st.kind;
     d.mode = nd.first_child < 0 ? MODE_COUNT : MODE_WRITE;
     if (per_graph && nd.first_term >= 0) {
@@ -523,9 +543,12 @@ int BatchSession::submit(const std::vector<std::vector<Step>>& steps, const std:
     index.reserve(steps.size() * 4);
     const int first_node = (int)nodes.size();
     uint8_t kb[512], kb2[512];
+    const std::vector<Step>* prev = nullptr;
+    std::vector<int> prev_path, path;
     for (size_t qi = 0; qi < steps.size(); ++qi) {
         const std::vector<Step>& st = steps[qi];
         if (st.size() < 2 || st[0].kind != STEP_SEED) return fail(GVA_ERR_ARG, "plan must start with a seed step");
+        if (path.size() < st.size()) path.resize(st.size());
         PlanRec pr;
         pr.tag = qi < tags.size() ? tags[qi] : qi;
         if (per_graph) {
@@ -538,6 +561,15 @@ int BatchSession::submit(const std::vector<std::vector<Step>>& steps, const std:
         if (ids) ids->push_back(q);
         int cur = -1;
         for (size_t i = 0; i < st.size(); ++i) {
+            // fast path: plans usually arrive ordered by their step sequences, so
+            // a step equal to the previous plan's step under the same parent is
+            // that plan's node (byte-equal steps have equal keys)
+            if (prev && i < prev_path.size() && i < prev->size() && cur == (i ? prev_path[i - 1] : -1) &&
+                memcmp(&st[i], &(*prev)[i], sizeof(Step)) == 0) {
+                cur = prev_path[i];
+                path[i] = cur;
+                continue;
+            }
             const size_t n = step_key_bytes(st[i], kb);
             uint64_t h = 1469598103934665603ull ^ ((uint64_t)(int64_t)cur * 0x9e3779b97f4a7c15ull);
             for (size_t j = 0; j + 8 <= n; j += 8) {
@@ -551,13 +583,18 @@ int BatchSession::submit(const std::vector<std::vector<Step>>& steps, const std:
             for (auto it = range.first; it != range.second && id < 0; ++it) {
                 const BNode& cand = nodes[it->second];
                 if (cand.parent != cur) continue;
-                if (step_key_bytes(cand.step, kb2) == n && memcmp(kb, kb2, n) == 0) id = it->second;
+                if (step_key_bytes(node_steps[it->second], kb2) == n && memcmp(kb, kb2, n) == 0) id = it->second;
             }
             if (id < 0) {
                 id = (int)nodes.size();
                 BNode nd;
-                nd.step = st[i];
+                nd.kind = st[i].kind;
+                nd.width_in = st[i].width_in;
+                nd.n_eq = st[i].n_eq;
+                nd.n_pairs = st[i].n_pairs;
+                nd.always_empty = st[i].always_empty;
                 nd.depth = (int)i;
+                node_steps.push_back(st[i]);
                 nd.parent = cur;
                 if (cur >= 0) {
                     nd.next_sibling = nodes[cur].first_child;
@@ -569,7 +606,10 @@ int BatchSession::submit(const std::vector<std::vector<Step>>& steps, const std:
                 index.emplace(h, id);
             }
             cur = id;
+            path[i] = cur;
         }
+        prev = &st;
+        prev_path.assign(path.begin(), path.begin() + st.size());
         plans[q].terminal = cur;
         plans[q].next_term = nodes[cur].first_term;
         nodes[cur].first_term = q;
@@ -577,7 +617,7 @@ int BatchSession::submit(const std::vector<std::vector<Step>>& steps, const std:
     // seeds: the children of every seed node start from its vertex list
     for (int id = first_node; id < (int)nodes.size(); ++id) {
         if (nodes[id].parent != -1) continue;
-        const Step& sd = nodes[id].step;
+        const Step& sd = node_steps[id];
         uint64_t n = 0;
         if (!sd.always_empty) n = db.seed_off[sd.label + 1] - db.seed_off[sd.label];
         if (n)
@@ -601,13 +641,19 @@ int BatchSession::round() {
                    (wait - wait0);
         }
     } timer{t_start, round_host_ms, wait_ms, wait_before};
+    auto t_lap = t_start;
+    auto lap = [&](int k) {
+        const auto now = std::chrono::steady_clock::now();
+        phase_ms[k] += std::chrono::duration<double, std::milli>(now - t_lap).count();
+        t_lap = now;
+    };
     GVA_CUDA_B(cudaSetDevice(db.device));
     // steps that cannot match (label or partition absent) end their task
     {
         size_t w = 0;
         std::vector<int> gone;
         for (size_t i = 0; i < active.size(); ++i) {
-            if (nodes[active[i].node].step.always_empty)
+            if (nodes[active[i].node].always_empty)
                 gone.push_back(active[i].node);
             else
                 active[w++] = std::move(active[i]);
@@ -655,7 +701,7 @@ int BatchSession::round() {
             nd.dev = dev_count++;
             fill_node_desc(tk.node, new_desc + (size_t)(nd.dev - dev_first) * sizeof(TaskDesc));
         }
-        const Step& st = nd.step;
+        const BNode& st = nd;
         refs[t] = TaskRef{(uint32_t)nd.dev, 0u, nb, tk.in, tk.rows};
         kmax = std::max(kmax, st.width_in);
         if (st.kind == STEP_EXT) eqmax = std::max(eqmax, st.n_eq);
@@ -665,6 +711,11 @@ int BatchSession::round() {
         crows += (double)tk.rows;
     }
     if (nb > 0x7fffffffull) return fail(GVA_ERR_UNSUPPORTED, "round too large for one launch");
+    // block -> task, so that no block searches block0
+    uint32_t* h_blk = (uint32_t*)staging_blk.get(nb * 4);
+    if (!h_blk) return fail(GVA_ERR_NOMEM, "pinned staging allocation failed");
+    for (int t = 0; t < nt; ++t)
+        for (uint64_t b = h_block0[t]; b < h_block0[t + 1]; ++b) h_blk[b] = (uint32_t)t;
     auto grow = [&](void** p, size_t& cap, size_t need) -> bool {
         if (need <= cap) return true;
         if (*p) cudaFreeAsync(*p, s);
@@ -689,7 +740,7 @@ int BatchSession::round() {
         node_cap = cap;
     }
     if (!grow(&d_desc, desc_cap, ref_bytes) || !grow((void**)&d_sums, sums_cap, (nb + 1) * 8) ||
-        !grow((void**)&d_small, small_cap, small_words * 8))
+        !grow((void**)&d_small, small_cap, small_words * 8) || !grow((void**)&d_blk, blk_cap, nb * 4))
         return fail(GVA_ERR_NOMEM, "batch bookkeeping allocation failed");
     uint64_t* d_block0 = d_small;
     uint64_t* d_totals = d_block0 + (nt + 1);
@@ -700,11 +751,13 @@ int BatchSession::round() {
                                    (size_t)(dev_count - dev_first) * sizeof(TaskDesc), cudaMemcpyHostToDevice, s));
     GVA_CUDA_B(cudaMemcpyAsync(d_desc, refs, ref_bytes, cudaMemcpyHostToDevice, s));
     GVA_CUDA_B(cudaMemcpyAsync(d_block0, h_block0, (nt + 1) * 8, cudaMemcpyHostToDevice, s));
+    GVA_CUDA_B(cudaMemcpyAsync(d_blk, h_blk, nb * 4, cudaMemcpyHostToDevice, s));
 
+    lap(0);
     cudaEvent_t ev = nullptr;
     if (pf) pf->begin(K_EXT_COUNT, cbytes, s, ev);
-    batch_count_kernel<<<(unsigned)nb, kThreads, 0, s>>>((const TaskDesc*)d_nodes, (const TaskRef*)d_desc, d_block0,
-                                                         nt, d_sums, ctx);
+    batch_count_kernel<<<(unsigned)nb, kThreads, 0, s>>>((const TaskDesc*)d_nodes, (const TaskRef*)d_desc, d_blk,
+                                                         d_sums, ctx);
     if (pf) pf->end(ev, K_EXT_COUNT, cbytes, s, crows);
     if (pf) pf->begin(K_SCAN, 16.0 * nb, s, ev);
     scan_block_sums_kernel<<<1, kScanThreads, 0, s>>>(d_sums, nb);
@@ -714,11 +767,13 @@ int BatchSession::round() {
     g_batch_launches += 3;
     GVA_CUDA_B(cudaGetLastError());
     GVA_CUDA_B(cudaMemcpyAsync(h_totals, d_totals, nt * 8, cudaMemcpyDeviceToHost, s));
+    lap(1);
     {
         const auto w0 = std::chrono::steady_clock::now();
         cudaError_t e = cudaStreamSynchronize(s);
         wait_ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - w0).count();
         if (e != cudaSuccess) return fail(GVA_ERR_CUDA, cudaGetErrorString(e));
+        t_lap = std::chrono::steady_clock::now();
     }
 
     // which tasks write this round: all when the outputs fit the budget,
@@ -727,7 +782,7 @@ int BatchSession::round() {
     for (int t = 0; t < nt; ++t) {
         const BNode& nd = nodes[active[t].node];
         if (nd.first_child < 0 || h_totals[t] == 0) continue;
-        const Step& st = nd.step;
+        const BNode& st = nd;
         want += ((h_totals[t] * (st.kind == STEP_EXT ? st.width_in + 1 : st.width_in) * 4ull) + 15) & ~15ull;
     }
     std::vector<int>& order = scratch_order;
@@ -748,7 +803,7 @@ int BatchSession::round() {
     off_words.assign(nt, 0);
     int status = GVA_OK;
     for (int t : order) {
-        const Step& st = nodes[active[t].node].step;
+        const BNode& st = nodes[active[t].node];
         const uint32_t w = st.kind == STEP_EXT ? st.width_in + 1 : st.width_in;
         const uint64_t bytes = h_totals[t] * w * 4ull;
         if (used + bytes <= budget) {
@@ -776,6 +831,7 @@ int BatchSession::round() {
         }
     }
     if (status) return status;
+    lap(2);
     std::shared_ptr<void> buf;
     if (used > 0) {
         void* p = nullptr;
@@ -787,7 +843,7 @@ int BatchSession::round() {
             h_outs[t] = chosen_flag[t] == 1 ? (uint32_t*)p + off_words[t] : nullptr;
             if (chosen_flag[t] != 1) continue;
             wrows += (double)active[t].rows;
-            const Step& st = nodes[active[t].node].step;
+            const BNode& st = nodes[active[t].node];
             const double k = st.width_in;
             wbytes += (4.0 * k + 8.0) * (double)active[t].rows +
                       (st.kind == STEP_EXT ? (4.0 + 4.0 * (k + 1)) : 4.0 * k) * (double)h_totals[t];
@@ -801,7 +857,7 @@ int BatchSession::round() {
         const uint64_t grid = std::min<uint64_t>(nb, (uint64_t)std::max(per_sm, 1) * sms);
         if (pf) pf->begin(K_EXT_WRITE, wbytes, s, ev);
         batch_write_kernel<<<(unsigned)grid, kThreads, smem, s>>>((const TaskDesc*)d_nodes, (const TaskRef*)d_desc,
-                                                                  d_block0, nt, nb, d_sums, d_outs, d_queue);
+                                                                  d_block0, d_blk, nb, d_sums, d_outs, d_queue);
         if (pf) pf->end(ev, K_EXT_WRITE, wbytes, s, wrows);
         launches += 1;
         g_batch_launches += 1;
@@ -809,6 +865,7 @@ int BatchSession::round() {
     } else {
         GVA_CUDA_B(cudaEventRecord(staged, s));
     }
+    lap(3);
     std::vector<int> ended;
     for (int t = 0; t < nt; ++t) {
         if (chosen_flag[t] == 2) continue;  // still active (deferred or split)
@@ -821,6 +878,7 @@ int BatchSession::round() {
     }
     active.swap(next);
     for (int nd : ended) finish_task(nd);
+    lap(4);
     if (pf) {
         GVA_CUDA_B(cudaStreamSynchronize(s));
         pf->resolve();
@@ -916,12 +974,16 @@ int run_batch(DevDB& db, const std::vector<std::vector<Step>>& steps, cudaStream
     }
     GVA_CUDA_B(cudaEventRecord(tev[dev][0], s));
     int rc;
+    const auto t_ses0 = std::chrono::steady_clock::now();
+    double loop_ms = 0.0;
     {
         BatchSession ses(db, s, budget, per_graph ? (uint32_t)nq : 0, graph_counts_host != nullptr, profile);
         rc = ses.init();
         std::vector<int> ids;
         if (!rc) rc = ses.submit(steps, {}, &ids);
+        const auto t_loop0 = std::chrono::steady_clock::now();
         while (!rc && !ses.idle()) rc = ses.round();
+        loop_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_loop0).count();
         if (!rc) {
             for (int q = 0; q < nq; ++q) counts[q] = ses.plan(ids[q]).count;
             if (per_graph) {
@@ -958,6 +1020,7 @@ int run_batch(DevDB& db, const std::vector<std::vector<Step>>& steps, cudaStream
             stats->splits = ses.splits;
             stats->launches = ses.launches;
             stats->nodes = ses.num_nodes();
+            for (int i = 0; i < 5; ++i) stats->phase_ms[i] = ses.phase_ms[i];
             for (int i = 0; i < K_NUM; ++i) stats->kstat[i] = ses.kstat[i];
         }
     }
@@ -965,7 +1028,11 @@ int run_batch(DevDB& db, const std::vector<std::vector<Step>>& steps, cudaStream
     cudaEventSynchronize(tev[dev][1]);
     float ms = 0.f;
     cudaEventElapsedTime(&ms, tev[dev][0], tev[dev][1]);
-    if (stats) stats->gpu_ms = ms;
+    if (stats) {
+        stats->gpu_ms = ms;
+        stats->session_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_ses0).count() -
+                            loop_ms - stats->submit_ms;
+    }
     return rc;
 }
 

@@ -375,6 +375,30 @@ size_t gva_mine_pattern_text(const gva_mine_result* res, int index, char* buf, s
     return s.size();
 }
 
+size_t gva_mine_export(const gva_mine_result* res, char* text_buf, size_t text_cap, uint64_t* offsets,
+                       uint32_t* edges, uint32_t* supports, uint64_t* embeddings) {
+    if (!res) return 0;
+    size_t need = 0;
+    for (const MinedPattern& p : res->pats) need += p.text.size() + 1;
+    const size_t n = res->pats.size();
+    for (size_t i = 0; i < n; ++i) {
+        if (edges) edges[i] = res->pats[i].edges;
+        if (supports) supports[i] = res->pats[i].support;
+        if (embeddings) embeddings[i] = res->pats[i].embeddings;
+    }
+    if (text_buf && offsets && text_cap >= need) {
+        size_t at = 0;
+        for (size_t i = 0; i < n; ++i) {
+            const std::string& t = res->pats[i].text;
+            offsets[i] = at;
+            memcpy(text_buf + at, t.data(), t.size());
+            text_buf[at + t.size()] = 0;
+            at += t.size() + 1;
+        }
+    }
+    return need;
+}
+
 int gva_mine_get_stats(const gva_mine_result* res, gva_mine_stats* out) {
     if (!res || !out) return fail(GVA_ERR_ARG, "null argument");
     out->candidates = res->stats.candidates;

@@ -361,7 +361,20 @@ int upload_graph(HostGraph& g, int device, DevDB*& out) {
         for (uint32_t v = 1; v <= g.max_id; ++v)
             if (g.dlabel[v] != kNone) seed_verts[fill[g.dlabel[v]]++] = v;
     }
-    size_t bytes = align256(seed_verts.size() * 4 + 4);
+    // the same groups ordered by total degree (descending, then id): rooted
+    // existence searches try the vertices most likely to succeed first
+    std::vector<uint32_t> seed_deg(seed_verts);
+    {
+        std::vector<uint32_t> deg(g.max_id + 1, 0);
+        for (auto& p : g.parts)
+            if (!p.off.empty())
+                for (uint32_t v = 0; v <= g.max_id; ++v)
+                    deg[v] += p.off[(uint64_t)(v + 1) * L] - p.off[(uint64_t)v * L];
+        for (uint32_t l = 0; l < L; ++l)
+            std::sort(seed_deg.begin() + seed_off[l], seed_deg.begin() + seed_off[l + 1],
+                      [&](uint32_t a, uint32_t b) { return deg[a] != deg[b] ? deg[a] > deg[b] : a < b; });
+    }
+    size_t bytes = 2 * align256(seed_verts.size() * 4 + 4);
     for (auto& p : g.parts) bytes += align256(p.off.size() * 4) + align256(p.adj.size() * 4 + 4);
     void* arena = nullptr;
     cudaError_t e = cudaMalloc(&arena, bytes);
@@ -382,6 +395,7 @@ int upload_graph(HostGraph& g, int device, DevDB*& out) {
         return at;
     };
     db->seed_verts = put(seed_verts);
+    db->seed_by_degree = put(seed_deg);
     db->parts.resize(g.parts.size());
     for (size_t i = 0; i < g.parts.size(); ++i) {
         HostPartition& hp = g.parts[i];

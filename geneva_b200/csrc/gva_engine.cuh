@@ -19,7 +19,7 @@ struct DevPart {
 };
 
 // One database resident in HBM.  A single allocation holds, 256-byte aligned:
-//   seed_off[L + 1] | seed_verts[...] | per partition: off[...] adj[...]
+//   seed_verts[...] | seed_by_degree[...] | per partition: off[...] adj[...]
 struct DevDB {
     int device = 0;
     uint32_t max_id = 0;
@@ -28,6 +28,7 @@ struct DevDB {
     std::vector<DevPart> parts;           // parts[p - 1] = edge label p (off == nullptr: absent)
     std::vector<uint32_t> seed_off;       // host copy of seed_off
     const uint32_t* seed_verts = nullptr; // vertices grouped by dense label, ascending id
+    const uint32_t* seed_by_degree = nullptr;  // same groups (seed_off), by degree descending
     void* arena = nullptr;
     size_t arena_bytes = 0;
     uint64_t n_adj = 0;
@@ -81,6 +82,8 @@ void free_result(MatchResult* r);
 struct BatchStats {
     double gpu_ms = 0.0;
     double submit_ms = 0.0, round_host_ms = 0.0, wait_ms = 0.0;
+    double phase_ms[5] = {0, 0, 0, 0, 0};
+    double session_ms = 0.0;  // session set-up, support read-back and tear-down
     uint64_t rounds = 0, splits = 0, launches = 0, nodes = 0;
     KernelStat kstat[K_NUM];
 };
@@ -110,8 +113,12 @@ struct Staging {
 // by take_completed().  Per-graph results need slots > 0 (one per live plan).
 class BatchSession {
 public:
+    // Trie node.  The few step fields every round reads are copied here so a
+    // round's passes over its tasks stay in a small array; the full step
+    // lives in node_steps.
     struct BNode {
-        Step step;
+        uint32_t kind = 0, width_in = 0, n_eq = 0, n_pairs = 0;
+        uint32_t always_empty = 0;
         int depth = 0;
         int parent = -1;
         int first_child = -1, next_sibling = -1;  // children as a linked list
@@ -157,6 +164,9 @@ public:
 
     uint64_t rounds = 0, splits = 0, launches = 0;
     double submit_ms = 0, round_host_ms = 0, wait_ms = 0;  // host time split
+    // round_host_ms by part: task scan + uploads, count launches, totals and
+    // budget choice, write launch, next tasks and completion
+    double phase_ms[5] = {0, 0, 0, 0, 0};
     KernelStat kstat[K_NUM];
 
 private:
@@ -177,6 +187,7 @@ private:
     void* acc = nullptr;
     std::vector<int> free_slots;
     std::vector<BNode> nodes;
+    std::vector<Step> node_steps;  // parallel to nodes
     std::vector<PlanRec> plans;
     std::vector<BTask> active;
     std::vector<int> completed;
@@ -194,6 +205,9 @@ private:
     size_t sums_cap = 0;
     uint64_t* d_small = nullptr;
     size_t small_cap = 0;
+    uint32_t* d_blk = nullptr;  // per-round block -> task
+    size_t blk_cap = 0;
+    Staging staging_blk;
 };
 int set_graph_ids(DevDB& db, const uint64_t* first, uint32_t num_graphs);
 
@@ -209,6 +223,8 @@ struct MineStats {
     uint64_t mni_tasks = 0, mni_rounds = 0, mni_found = 0;  // MNI mode
     double gpu_ms = 0.0, host_ms = 0.0, gen_ms = 0.0, plan_ms = 0.0, eval_ms = 0.0, merge_ms = 0.0;
     double submit_ms = 0.0, round_host_ms = 0.0, wait_ms = 0.0;
+    double phase_ms[5] = {0, 0, 0, 0, 0};
+    double session_ms = 0.0;
     KernelStat kstat[K_NUM];
 };
 

@@ -15,6 +15,8 @@
 // level.  Each candidate is matched with the planner's own plan for its
 // query text, so embedding counts are the reference's row counts.
 #include <algorithm>
+#include <cstdio>
+#include <cstdlib>
 #include <array>
 #include <atomic>
 #include <chrono>
@@ -316,7 +318,7 @@ int run_mine(DevDB& db, cudaStream_t s, uint64_t budget, uint32_t max_edges, uin
         if (!db.vgraph || db.num_graphs == 0) return fail(GVA_ERR_ARG, "mining needs graph ids (gva_db_set_graphs)");
         if (max_edges == 0 || max_edges + 1 > GVA_MAX_QUERY_VERTICES) return fail(GVA_ERR_ARG, "max_edges out of range");
     }
-    if (batch_limit == 0) batch_limit = mni ? 65536 : 8192;
+    if (batch_limit == 0) batch_limit = mni ? 65536 : 32768;
     const uint32_t P = (uint32_t)db.parts.size();
     const std::vector<uint32_t>& labels = db.labels;
     auto t_host0 = std::chrono::steady_clock::now();
@@ -454,6 +456,8 @@ int run_mine(DevDB& db, cudaStream_t s, uint64_t budget, uint32_t max_edges, uin
             st.submit_ms += bs.submit_ms;
             st.round_host_ms += bs.round_host_ms;
             st.wait_ms += bs.wait_ms;
+            st.session_ms += bs.session_ms;
+            for (int i = 0; i < 5; ++i) st.phase_ms[i] += bs.phase_ms[i];
             for (int kk = 0; kk < K_NUM; ++kk) {
                 st.kstat[kk].launches += bs.kstat[kk].launches;
                 st.kstat[kk].ms += bs.kstat[kk].ms;
@@ -634,6 +638,13 @@ int run_mine(DevDB& db, cudaStream_t s, uint64_t budget, uint32_t max_edges, uin
     st.frequent = out.size();
     st.gpu_ms = gpu_ms;
     st.host_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_host0).count();
+    if (getenv("GVA_TRACE"))  // host-time split, for tuning
+        fprintf(stderr,
+                "gva_mine: host %.1f ms: gen %.1f merge %.1f plan %.1f eval %.1f (submit %.1f session %.1f rounds %.1f "
+                "[scan %.1f count %.1f choose %.1f write %.1f next %.1f] wait %.1f) gpu %.1f\n",
+                st.host_ms, st.gen_ms, st.merge_ms, st.plan_ms, st.eval_ms, st.submit_ms, st.session_ms,
+                st.round_host_ms, st.phase_ms[0], st.phase_ms[1], st.phase_ms[2], st.phase_ms[3], st.phase_ms[4],
+                st.wait_ms, st.gpu_ms);
     return GVA_OK;
 }
 

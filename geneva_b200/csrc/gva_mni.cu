@@ -25,9 +25,12 @@
 //           of its pattern, so the support returned is min(MNI, cap) exactly
 //
 // Tasks run in rounds: each active task gets the next 2048 << round seeds,
-// cut into 128-seed work items that a persistent kernel hands to warps
-// through an atomic queue (SM-level load balance however skewed the seeds'
-// degrees are); the host retires capped and exhausted tasks between rounds.
+// as work items that a persistent kernel hands to warps through an atomic
+// queue (SM-level load balance however skewed the seeds' degrees are).  With
+// many tasks an item is a task's whole quota, scanned by one warp in seed
+// order and stopped as soon as the count reaches the cap; with few, quotas
+// are cut into items of down to 128 seeds so that every warp has work.  The
+// host retires capped and exhausted tasks between rounds.
 // The batched form puts every task of many patterns in one round; the plain
 // form runs the same rounds one pattern at a time.
 #include <cuda_runtime.h>
@@ -37,6 +40,7 @@
 #include <chrono>
 #include <cstring>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/geneva.h"
@@ -55,7 +59,7 @@ namespace {
     } while (0)
 
 constexpr int kMniWarps = 8;       // warps per block
-constexpr uint32_t kMniItem = 128; // seeds per work item
+constexpr uint32_t kMniItem = 128; // smallest work item (seeds); rounds with few tasks use it
 constexpr uint32_t kMniFirst = 2048;  // seeds per task in the first round (doubles every round)
 
 struct PartPtr {
@@ -68,7 +72,7 @@ struct PartPtr {
 // its edges to earlier levels, and the earlier levels sharing its label.
 struct MniTask {
     uint32_t n;
-    uint32_t seed_begin;  // seeds: seed_verts[seed_begin, seed_begin + seed_count)
+    uint32_t seed_begin;  // seeds: seed_by_degree[seed_begin, seed_begin + seed_count)
     uint32_t seed_count;
     uint32_t n_rootf;
     uint16_t lab[kMniMaxVertices];
@@ -91,16 +95,10 @@ struct MniSlot {  // one active task in one round
 
 enum MniProf { P_SEEDS = 0, P_ROOTS, P_OPENS, P_SCANNED, P_CHECKS, P_FOUND, P_NUM };
 
-__device__ __forceinline__ int find_slot(const uint64_t* __restrict__ item0, int nslots, uint64_t it) {
-    int lo = 0, hi = nslots - 1;  // largest s with item0[s] <= it
-    while (lo < hi) {
-        const int mid = (lo + hi + 1) >> 1;
-        if (__ldg(item0 + mid) <= it)
-            lo = mid;
-        else
-            hi = mid - 1;
-    }
-    return lo;
+// item -> slot, so that no warp searches item0 for its item's slot
+__global__ void mni_expand_kernel(const uint64_t* __restrict__ item0, int nslots, uint32_t* __restrict__ item_slot) {
+    for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < nslots; s += gridDim.x * blockDim.x)
+        for (uint64_t i = item0[s]; i < item0[s + 1]; ++i) item_slot[i] = (uint32_t)s;
 }
 
 __device__ __forceinline__ bool root_ok(const MniTask& T, const PartPtr* __restrict__ parts, uint32_t L, uint32_t v) {
@@ -197,7 +195,8 @@ __device__ bool mni_dfs(const MniTask& T, const PartPtr* __restrict__ parts, uin
 // runs one search per surviving root.
 __global__ void __launch_bounds__(kMniWarps * 32)
 mni_search_kernel(const MniTask* __restrict__ tasks, const MniSlot* __restrict__ slots,
-                  const uint64_t* __restrict__ item0, int nslots, uint64_t nitems, const uint32_t* __restrict__ seeds,
+                  const uint64_t* __restrict__ item0, const uint32_t* __restrict__ item_slot, uint64_t nitems,
+                  const uint32_t* __restrict__ seeds, uint32_t item_len,
                   const PartPtr* __restrict__ parts, uint32_t L, uint32_t* __restrict__ counts,
                   unsigned long long* __restrict__ queue, unsigned long long* __restrict__ prof) {
     __shared__ MniTask tsh[kMniWarps];
@@ -210,7 +209,7 @@ mni_search_kernel(const MniTask* __restrict__ tasks, const MniSlot* __restrict__
         if (lane == 0) it = atomicAdd(queue, 1ull);
         it = __shfl_sync(0xffffffffu, it, 0);
         if (it >= nitems) break;
-        const int s = find_slot(item0, nslots, it);
+        const int s = (int)__ldg(item_slot + it);
         const MniSlot sl = slots[s];
         if ((int)sl.task != cur) {
             __syncwarp();
@@ -220,8 +219,8 @@ mni_search_kernel(const MniTask* __restrict__ tasks, const MniSlot* __restrict__
             __syncwarp();
             cur = (int)sl.task;
         }
-        const uint32_t a = sl.start + (uint32_t)(it - item0[s]) * kMniItem;
-        const uint32_t b = min(a + kMniItem, sl.start + sl.len);
+        const uint32_t a = sl.start + (uint32_t)(it - item0[s]) * item_len;
+        const uint32_t b = min(a + item_len, sl.start + sl.len);
         for (uint32_t c0 = a; c0 < b; c0 += 32) {
             // one lane reads the count so that the whole warp takes the same branch
             uint32_t seen = 0;
@@ -424,25 +423,42 @@ int run_mni(DevDB& db, const std::vector<MniPattern>& pats, const std::vector<ch
     support.assign(np, 0);
     if (np == 0) return GVA_OK;
     if (cap == 0) cap = 0xffffffffu;
-    // tasks: one per automorphism orbit of each pattern whose labels all occur
+    // tasks: one per automorphism orbit of each pattern whose labels all
+    // occur, built on all host threads over contiguous blocks of patterns
     std::vector<MniTask> tasks;
     std::vector<uint32_t> task_pat;
     std::vector<uint32_t> first_task(np + 1, 0);
-    for (size_t q = 0; q < np; ++q) {
-        first_task[q] = (uint32_t)tasks.size();
-        const MniPattern& p = pats[q];
-        if ((!absent.empty() && absent[q]) || p.n == 0) continue;
-        uint32_t orbit[kMniMaxVertices];
-        pattern_orbits(p, orbit);
-        for (uint32_t v = 0; v < p.n; ++v) {
-            if (orbit[v] != v) continue;
-            MniTask T;
-            build_task(db, p, v, T);
-            tasks.push_back(T);
-            task_pat.push_back((uint32_t)q);
-        }
+    {
+        const unsigned nth = (unsigned)std::max<size_t>(1, std::min<size_t>({64, std::thread::hardware_concurrency(),
+                                                                             (np + 255) / 256}));
+        std::vector<std::vector<MniTask>> tl(nth);
+        std::vector<uint32_t> per_pat(np, 0);
+        std::vector<std::thread> pool;
+        for (unsigned t = 0; t < nth; ++t)
+            pool.emplace_back([&, t]() {
+                const size_t q0 = np * t / nth, q1 = np * (t + 1) / nth;
+                tl[t].reserve((q1 - q0) * 3);
+                for (size_t q = q0; q < q1; ++q) {
+                    const MniPattern& p = pats[q];
+                    if ((!absent.empty() && absent[q]) || p.n == 0) continue;
+                    uint32_t orbit[kMniMaxVertices];
+                    pattern_orbits(p, orbit);
+                    for (uint32_t v = 0; v < p.n; ++v) {
+                        if (orbit[v] != v) continue;
+                        tl[t].emplace_back();
+                        build_task(db, p, v, tl[t].back());
+                        per_pat[q]++;
+                    }
+                }
+            });
+        for (auto& th : pool) th.join();
+        for (size_t q = 0; q < np; ++q) first_task[q + 1] = first_task[q] + per_pat[q];
+        tasks.reserve(first_task[np]);
+        for (auto& v : tl) tasks.insert(tasks.end(), v.begin(), v.end());
+        task_pat.resize(tasks.size());
+        for (size_t q = 0; q < np; ++q)
+            for (uint32_t t = first_task[q]; t < first_task[q + 1]; ++t) task_pat[t] = (uint32_t)q;
     }
-    first_task[np] = (uint32_t)tasks.size();
     const size_t nt = tasks.size();
     st.tasks += nt;
     if (nt == 0) return GVA_OK;
@@ -519,23 +535,33 @@ int run_mni(DevDB& db, const std::vector<MniPattern>& pats, const std::vector<ch
             slots.clear();
             item0.assign(1, 0);
             const uint64_t quota = (uint64_t)kMniFirst << std::min(round, 20u);
+            uint64_t total = 0;
             for (uint32_t t : active) {
                 const uint32_t left = tasks[t].seed_count - processed[t];
                 const uint32_t len = (uint32_t)std::min<uint64_t>(left, quota);
                 slots.push_back(MniSlot{t, processed[t], len, std::min(cap, pcap[task_pat[t]])});
-                item0.push_back(item0.back() + (len + kMniItem - 1) / kMniItem);
+                total += len;
             }
+            // items: a whole slot per warp when there are many (its count is
+            // checked every 32 seeds, so a task stops right at its cap), cut
+            // down to 128 seeds when few tasks must fill the GPU
+            const uint64_t want_items = (uint64_t)8 * per_sm * sms * kMniWarps;
+            uint64_t item_len = std::max<uint64_t>(kMniItem, (total / want_items + 31) & ~(uint64_t)31);
+            item_len = std::min<uint64_t>(item_len, 1u << 30);
+            for (const MniSlot& sl : slots) item0.push_back(item0.back() + (sl.len + item_len - 1) / item_len);
             const int ns = (int)slots.size();
             const uint64_t nitems = item0.back();
+            // device: slots | item0 | item -> slot (filled on the device); host stages the first two
             const size_t need = al(ns * sizeof(MniSlot)) + (ns + 1) * 8;
+            const size_t dneed = al(need) + nitems * 4;
             char* h = stage.get(need);
             if (!h) {
                 rc = fail(GVA_ERR_NOMEM, "pinned staging allocation failed");
                 break;
             }
-            if (need > dround_cap) {
+            if (dneed > dround_cap) {
                 if (dround) cudaFreeAsync(dround, s);
-                dround_cap = std::max(need, dround_cap * 2);
+                dround_cap = std::max(dneed, dround_cap * 2);
                 if (cudaMallocAsync(&dround, dround_cap, s) != cudaSuccess) {
                     dround = nullptr;
                     rc = fail(GVA_ERR_NOMEM, "MNI round allocation failed");
@@ -546,6 +572,7 @@ int run_mni(DevDB& db, const std::vector<MniPattern>& pats, const std::vector<ch
             memcpy(h + al(ns * sizeof(MniSlot)), item0.data(), (ns + 1) * 8);
             MniSlot* d_slots = (MniSlot*)dround;
             uint64_t* d_item0 = (uint64_t*)((char*)dround + al(ns * sizeof(MniSlot)));
+            uint32_t* d_item_slot = (uint32_t*)((char*)dround + al(need));
             if (cudaMemcpyAsync(dround, h, need, cudaMemcpyHostToDevice, s) != cudaSuccess ||
                 cudaMemsetAsync(d_queue, 0, 8, s) != cudaSuccess) {
                 rc = fail(GVA_ERR_CUDA, "MNI round upload failed");
@@ -553,14 +580,17 @@ int run_mni(DevDB& db, const std::vector<MniPattern>& pats, const std::vector<ch
             }
             const uint64_t grid = std::min<uint64_t>((uint64_t)per_sm * sms, (nitems + kMniWarps - 1) / kMniWarps);
             cudaEvent_t ev = nullptr;
-            const double rows = (double)nitems * kMniItem;
+            const double rows = (double)total;
+            mni_expand_kernel<<<(unsigned)std::min<uint64_t>((ns + 255) / 256, 4096), 256, 0, s>>>(d_item0, ns,
+                                                                                                  d_item_slot);
             if (profile) prof.begin(K_MNI, 0.0, s, ev);
             mni_search_kernel<<<(unsigned)std::max<uint64_t>(grid, 1), kMniWarps * 32, 0, s>>>(
-                d_tasks, d_slots, d_item0, ns, nitems, db.seed_verts, d_parts, db.L, d_counts, d_queue,
+                d_tasks, d_slots, d_item0, d_item_slot, nitems, db.seed_by_degree, (uint32_t)item_len, d_parts, db.L,
+                d_counts, d_queue,
                 profile ? d_prof : nullptr);
             if (profile) prof.end(ev, K_MNI, 0.0, s, rows);
-            st.launches++;
-            g_mni_launches++;
+            st.launches += 2;
+            g_mni_launches += 2;
             st.rounds++;
             if (cudaGetLastError() != cudaSuccess ||
                 cudaMemcpyAsync(counts.data(), d_counts, bytes_counts, cudaMemcpyDeviceToHost, s) != cudaSuccess) {

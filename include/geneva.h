@@ -223,7 +223,7 @@ typedef struct gva_mine_opts {
     uint64_t budget_bytes;
     uint32_t max_edges;
     uint32_t min_support;
-    uint32_t batch_limit;  /* candidates per batched run (0 = 8192; MNI: 65536) */
+    uint32_t batch_limit;  /* candidates per batched run (0 = 32768; MNI: 65536) */
     uint32_t profile;      /* 1: per-kernel CUDA-event timing (gva_mine_kernel_stats) */
     gva_reduce_fn reduce;  /* NULL on one process (GVA_SUPPORT_GRAPHS only) */
     void* reduce_user;
@@ -257,6 +257,13 @@ int gva_mine_num_patterns(const gva_mine_result* res);
 int gva_mine_get(const gva_mine_result* res, int index, uint32_t* edges, uint32_t* support, uint64_t* embeddings);
 /* query text of pattern `index` (.query format); returns length */
 size_t gva_mine_pattern_text(const gva_mine_result* res, int index, char* buf, size_t cap);
+/* Every pattern in one call: texts concatenated into text_buf, each ending in
+ * a NUL, pattern i's text starting at offsets[i]; edges, supports and
+ * embeddings (any may be NULL) receive one entry per pattern.  Returns the
+ * text bytes needed (NULs included); text_buf and offsets are written only
+ * when text_cap is at least that. */
+size_t gva_mine_export(const gva_mine_result* res, char* text_buf, size_t text_cap, uint64_t* offsets,
+                       uint32_t* edges, uint32_t* supports, uint64_t* embeddings);
 int gva_mine_get_stats(const gva_mine_result* res, gva_mine_stats* out);
 /* per-kernel totals when opts->profile was set; returns the number of kinds */
 int gva_mine_kernel_stats(const gva_mine_result* res, gva_kernel_stat* out, int cap);
