@@ -63,6 +63,7 @@ def parse_args():
     ap.add_argument("--workload", default="mine", choices=["mine", "match", "serve", "mni"])
     ap.add_argument("--rates", default="10,100,500,2000", help="serve workload: arrival rates (req/s)")
     ap.add_argument("--duration", type=float, default=2.0, help="serve workload: seconds of arrivals per rate")
+    ap.add_argument("--drain", type=float, default=120.0, help="serve workload: seconds to wait for results per rate")
     ap.add_argument("--queries", type=int, default=4096, help="match workload: patterns per rank per step")
     ap.add_argument("--max-edges", type=int, default=6)
     ap.add_argument("--min-support", type=float, default=0.02, help="fraction of graphs")
@@ -242,26 +243,32 @@ def reference_arm(args, db, queries, workload):
 # -------------------------------------------------------------- serving arm ----
 def serve_bench(args, local, torch, gv, workloads):
     """Poisson arrivals at each rate: 80% matching requests (3-10 vertex
-    patterns sampled from the database), 20% mining requests (max edges 3-5,
-    min support 1-5% of the graphs), all against the resident config-2
-    database; continuous batching with a 150 GB admission budget."""
+    patterns sampled from the resident config-2 database), 20% mining
+    requests (max edges 3-5, minimum MNI support 1-5% of the vertices) against
+    the resident config-4 graph; continuous batching with a 150 GB admission
+    budget; matching on a high-priority stream, mining on its own stream."""
     import random
     from geneva_b200.serve import Server, percentile
     db = workloads.config2(seed=args.seed)
     gdb = gv.Database.from_edges(db.vlabels, db.src, db.dst, db.elabels, device=local)
     gdb.set_graphs(db.first)
-    G = len(db.first) - 1
+    g4 = workloads.config4()
+    mdb = gv.Database.from_edges(g4.vlabels, g4.src, g4.dst, g4.elabels, device=local)
+    V4 = g4.num_vertices
+    del g4
     pool = workloads.sample_patterns(db, 512, 3, 10, seed=4242)
     s_match, s_mine = torch.cuda.Stream(priority=-1), torch.cuda.Stream()  # matching ahead of mining
+    mk = lambda: Server(gdb, budget_bytes=150 << 30, match_stream=s_match.cuda_stream,
+                        mine_stream=s_mine.cuda_stream, mine_db=mdb)
     # warm-up: first launches, pool growth and pinned staging happen here, not in the first rate point
-    srv = Server(gdb, budget_bytes=150 << 30, match_stream=s_match.cuda_stream, mine_stream=s_mine.cuda_stream)
-    warm = [srv.submit_match(q) for q in pool[:32]] + [srv.submit_mine(2, int(G * 0.05))]
+    srv = mk()
+    warm = [srv.submit_match(q) for q in pool[:32]] + [srv.submit_mine(3, int(V4 * 0.05))]
     for r in warm:
-        r.future.result(timeout=300)
+        r.future.result(timeout=600)
     srv.close()
     points = []
     for rate in [float(x) for x in args.rates.split(",")]:
-        srv = Server(gdb, budget_bytes=150 << 30, match_stream=s_match.cuda_stream, mine_stream=s_mine.cuda_stream)
+        srv = mk()
         rng = random.Random(int(rate))
         reqs = []
         t_end = time.perf_counter() + args.duration
@@ -272,9 +279,9 @@ def serve_bench(args, local, torch, gv, workloads):
             if rng.random() < 0.8:
                 reqs.append(srv.submit_match(pool[rng.randrange(len(pool))]))
             else:
-                reqs.append(srv.submit_mine(rng.randint(3, 5), int(G * rng.uniform(0.01, 0.05))))
+                reqs.append(srv.submit_mine(rng.randint(3, 5), int(V4 * rng.uniform(0.01, 0.05))))
             nxt += rng.expovariate(rate)
-        deadline = time.perf_counter() + 60.0
+        deadline = time.perf_counter() + args.drain
         for r in reqs:
             try:
                 r.future.result(timeout=max(0.0, deadline - time.perf_counter()))
@@ -282,23 +289,30 @@ def serve_bench(args, local, torch, gv, workloads):
                 pass
         t_stop = time.perf_counter()
         done = [r for r in reqs if r.future.done() and not r.future.exception()]
-        emb = sum(r.result[0] for r in done if r.kind == "match") + \
-              sum(r.result[1]["embeddings"] for r in done if r.kind == "mine")
+        emb = sum(r.result[0] for r in done if r.kind == "match")
+        pats = sum(r.result[1]["candidates"] for r in done if r.kind == "mine")
         lm = [r.latency for r in done if r.kind == "match"]
         ln = [r.latency for r in done if r.kind == "mine"]
         t0 = min(r.arrival for r in reqs) if reqs else t_stop
         points.append({"rate": rate, "requests": len(reqs), "completed": len(done),
+                       "match_requests": sum(r.kind == "match" for r in reqs), "match_completed": len(lm),
+                       "mine_requests": sum(r.kind == "mine" for r in reqs), "mine_completed": len(ln),
                        "match_p50_ms": 1e3 * percentile(lm, 50) if lm else None,
                        "match_p99_ms": 1e3 * percentile(lm, 99) if lm else None,
                        "mine_p50_ms": 1e3 * percentile(ln, 50) if ln else None,
                        "mine_p99_ms": 1e3 * percentile(ln, 99) if ln else None,
-                       "embeddings_per_s": emb / (t_stop - t0), "rounds": srv.rounds,
+                       "embeddings_per_s": emb / (t_stop - t0), "mined_patterns_per_s": pats / (t_stop - t0),
+                       "rounds": srv.rounds,
                        "round_p50_ms": 1e3 * percentile(srv.round_s, 50) if srv.round_s else None,
                        "round_p99_ms": 1e3 * percentile(srv.round_s, 99) if srv.round_s else None})
         srv.close()
     gdb.close()
-    return {"metric": "p99 query latency", "unit": "ms", "workload": "serving sweep on the config-2 database "
-            "(mining requests use graph support on the same database)", "points": points}
+    mdb.close()
+    return {"metric": "p99 query latency", "unit": "ms",
+            "workload": "config-5 serving sweep: Poisson arrivals, 80% matching queries (3-10 vertices) against the "
+                        "config-2 database, 20% MNI mining requests (max edges 3-5, min support 1-5% of |V|) against "
+                        "the config-4 graph; 150 GB admission budget",
+            "duration_s_per_rate": args.duration, "drain_s": args.drain, "points": points}
 
 
 # ------------------------------------------------------------ MNI mining arm ----

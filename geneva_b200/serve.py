@@ -8,7 +8,9 @@ server keeps one database resident and a batched session open (gva_session):
   running work at the next round; every round advances all admitted work one
   step, so a short query does not wait for a long one to finish;
 * mining requests (max edges, min support) run on a worker thread with their
-  own CUDA stream, so their rounds overlap the matching rounds on the device.
+  own CUDA stream, so their rounds overlap the matching rounds on the device;
+  they mine the graph database (graph support) or, when the server is given
+  one data graph for mining, that graph (MNI support).
 
 Latency of a request = completion time - arrival time (host wall clock).
 """
@@ -62,9 +64,14 @@ class Server:
     """One database, one open session, one mining worker."""
 
     def __init__(self, db: Database, budget_bytes: int = 150 << 30, support: bool = True,
-                 slots: int = 4096, match_stream: Optional[int] = None, mine_stream: Optional[int] = None):
+                 slots: int = 4096, match_stream: Optional[int] = None, mine_stream: Optional[int] = None,
+                 mine_db: Optional[Database] = None):
+        """db: the graph database matching requests run against (and mining
+        requests, with graph support, when mine_db is None).  mine_db: one
+        data graph that mining requests run against with MNI support."""
         self.lib = _declare(library())
         self.db = db
+        self.mine_db = mine_db
         self.budget = budget_bytes
         self.support = support and db.num_graphs > 0
         self.mine_stream = mine_stream
@@ -204,7 +211,11 @@ class Server:
                 return
             r.admitted = time.perf_counter()
             try:
-                pats, stats = mine(self.db, r.payload[0], r.payload[1], stream=self.mine_stream)
+                if self.mine_db is not None:
+                    pats, stats = mine(self.mine_db, r.payload[0], r.payload[1], stream=self.mine_stream,
+                                       support="mni")
+                else:
+                    pats, stats = mine(self.db, r.payload[0], r.payload[1], stream=self.mine_stream)
                 r.result = (pats, stats)
                 r.done = time.perf_counter()
                 with self._lock:

@@ -69,3 +69,24 @@ def test_bad_request_fails_alone(served_db):
         bad.future.result(timeout=60)
     assert good.future.result(timeout=60)[0] >= 0
     srv.close()
+
+
+def test_mni_mining_requests_on_a_second_graph(served_db):
+    """Mining requests against a separate single graph (MNI support) give the
+    same patterns in the mix as alone, while matching requests keep flowing."""
+    db, gdb = served_db
+    g4 = workloads.rmat_graph(9, 3000, 4, 1.0, seed=6, name="serve_rmat")
+    mdb = gv.Database.from_edges(g4.vlabels, g4.src, g4.dst, g4.elabels)
+    alone, _ = gv.mine(mdb, 3, 40, support="mni")
+    pats = workloads.sample_patterns(db, 20, 3, 6, seed=13)
+    want = [int(gv.batch_count(gdb, [gv.Plan.from_text(p)])[0][0]) for p in pats]
+    srv = Server(gdb, budget_bytes=1 << 30, mine_db=mdb)
+    m = srv.submit_mine(3, 40)
+    reqs = [srv.submit_match(p) for p in pats]
+    got = [r.future.result(timeout=300)[0] for r in reqs]
+    mined, _ = m.future.result(timeout=300)
+    srv.close()
+    assert got == want
+    key = lambda ps: sorted((p.text, p.support) for p in ps)
+    assert key(mined) == key(alone) and len(mined) > 0
+    mdb.close()
