@@ -190,20 +190,26 @@ batch_write_kernel(const TaskDesc* __restrict__ nodes, const TaskRef* __restrict
             for (uint32_t w = threadIdx.x; w < nr * k; w += kThreads) rows_s[w] = gin[w];
             __syncthreads();
             const uint32_t* row = rows_s + threadIdx.x * k;
-            const uint32_t* gadj = nullptr;
-            uint32_t lo = 0, hi = 0, cnt = 0;
-            int which = -1;
+            GenState g;
+            g.lo = g.hi = 0;
+            uint32_t cnt = 0, acc = 0;  // acc: verdicts of the first 32 candidates
             if (threadIdx.x < nr) {
-                ext_generator(p, row, gadj, lo, hi, which);
-                for (uint32_t j = lo; j < hi; ++j) cnt += ext_accept(p, row, __ldg(gadj + j), which) ? 1u : 0u;
+                ext_generator(p, row, g);
+                for (uint32_t j = g.lo; j < g.hi; ++j) {
+                    const bool ok = ext_accept(p, row, __ldg(g.gadj + j), g);
+                    cnt += ok ? 1u : 0u;
+                    if (ok && j - g.lo < 32) acc |= 1u << (j - g.lo);
+                }
             }
             uint64_t total;
             const uint64_t before = block_exclusive_scan(cnt, &total);
             if (cnt) {
                 uint32_t* dst = out + (out0 + before) * k1;
-                for (uint32_t j = lo; j < hi; ++j) {
-                    const uint32_t c = __ldg(gadj + j);
-                    if (!ext_accept(p, row, c, which)) continue;
+                for (uint32_t j = g.lo; j < g.hi; ++j) {
+                    const bool early = j - g.lo < 32;
+                    if (early && !(acc >> (j - g.lo) & 1)) continue;
+                    const uint32_t c = __ldg(g.gadj + j);
+                    if (!early && !ext_accept(p, row, c, g)) continue;
                     for (uint32_t q = 0; q < k; ++q) dst[q] = row[q];
                     dst[k] = c;
                     dst += k1;

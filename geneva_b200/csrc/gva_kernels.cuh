@@ -95,23 +95,36 @@ __device__ __forceinline__ uint32_t find_in(const uint32_t* __restrict__ adj, ui
 
 // Candidate source of a row with fused checks: the shortest of the source
 // segment and the dir-0 check segments, each cut below the restriction
-// bound.  which = -1 (source) or the check index.
-__device__ __forceinline__ void ext_generator(const ExtArgs& p, const uint32_t* row, const uint32_t*& gadj,
-                                              uint32_t& lo, uint32_t& hi, int& which) {
-    ext_range(p, row, lo, hi);
-    gadj = p.adj;
-    which = -1;
-    for (uint32_t i = 0; i < p.n_chk && lo < hi; ++i) {
+// bound.  The segments stay in the state, so that membership tests of the
+// candidates need no offset loads (a candidate lies below the bound, so the
+// cut segments answer membership as the full ones would).
+struct GenState {
+    const uint32_t* gadj;
+    uint32_t lo, hi;  // generator range
+    int which;        // -1 = source, else the check index
+    uint32_t slo, shi;                          // source segment
+    uint32_t clo[kMaxChecks], chi[kMaxChecks];  // dir-0 check segments
+};
+
+__device__ __forceinline__ void ext_generator(const ExtArgs& p, const uint32_t* row, GenState& g) {
+    ext_range(p, row, g.slo, g.shi);
+    g.lo = g.slo;
+    g.hi = g.shi;
+    g.gadj = p.adj;
+    g.which = -1;
+    for (uint32_t i = 0; i < p.n_chk && g.lo < g.hi; ++i) {
         if (p.chk_dir[i]) continue;
         const uint64_t t = (uint64_t)row[p.chk_col[i]] * p.L + p.lab;
         uint32_t l2 = __ldg(p.chk_off[i] + t), h2 = __ldg(p.chk_off[i] + t + 1);
         if (p.bound_col >= 0 && l2 < h2)
             h2 = lower_bound_u32(p.chk_adj[i], l2, h2, (uint64_t)row[p.bound_col] + p.bound_incl);
-        if (h2 - l2 < hi - lo) {
-            lo = l2;
-            hi = h2;
-            gadj = p.chk_adj[i];
-            which = (int)i;
+        g.clo[i] = l2;
+        g.chi[i] = h2;
+        if (h2 - l2 < g.hi - g.lo) {
+            g.lo = l2;
+            g.hi = h2;
+            g.gadj = p.chk_adj[i];
+            g.which = (int)i;
         }
     }
 }
@@ -124,15 +137,14 @@ __device__ __forceinline__ bool seg_has(const uint32_t* __restrict__ off, const 
 
 // Whether generated candidate c survives injectivity, the source edge (when
 // the generator is a check segment) and every other check.
-__device__ __forceinline__ bool ext_accept(const ExtArgs& p, const uint32_t* row, uint32_t c, int which) {
+__device__ __forceinline__ bool ext_accept(const ExtArgs& p, const uint32_t* row, uint32_t c, const GenState& g) {
     for (uint32_t j = 0; j < p.n_eq; ++j)
         if (row[p.eq_cols[j]] == c) return false;
-    if (which >= 0 && !seg_has(p.off, p.adj, p.L, row[p.src_col], p.lab, c)) return false;
+    if (g.which >= 0 && find_in(p.adj, g.slo, g.shi, c) == 0xffffffffu) return false;
     for (uint32_t i = 0; i < p.n_chk; ++i) {
-        if ((int)i == which) continue;
-        const uint32_t w = row[p.chk_col[i]];
-        const bool ok = p.chk_dir[i] ? seg_has(p.chk_off[i], p.chk_adj[i], p.L, c, p.chk_lab[i], w)
-                                     : seg_has(p.chk_off[i], p.chk_adj[i], p.L, w, p.lab, c);
+        if ((int)i == g.which) continue;
+        const bool ok = p.chk_dir[i] ? seg_has(p.chk_off[i], p.chk_adj[i], p.L, c, p.chk_lab[i], row[p.chk_col[i]])
+                                     : find_in(p.chk_adj[i], g.clo[i], g.chi[i], c) != 0xffffffffu;
         if (!ok) return false;
     }
     return true;
@@ -141,12 +153,10 @@ __device__ __forceinline__ bool ext_accept(const ExtArgs& p, const uint32_t* row
 // Number of candidates of one row (segment minus already-matched vertices).
 __device__ __forceinline__ uint32_t ext_count_row(const ExtArgs& p, const uint32_t* row) {
     if (p.n_chk) {
-        const uint32_t* gadj;
-        uint32_t lo, hi;
-        int which;
-        ext_generator(p, row, gadj, lo, hi, which);
+        GenState g;
+        ext_generator(p, row, g);
         uint32_t n = 0;
-        for (uint32_t j = lo; j < hi; ++j) n += ext_accept(p, row, __ldg(gadj + j), which) ? 1u : 0u;
+        for (uint32_t j = g.lo; j < g.hi; ++j) n += ext_accept(p, row, __ldg(g.gadj + j), g) ? 1u : 0u;
         return n;
     }
     uint32_t lo, hi;
