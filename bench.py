@@ -1,7 +1,7 @@
 #!/usr/bin/env python
 """Benchmark of the pattern-mining path on the 20,000-graph database.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl geneva|reference] [--workload mine|match]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl geneva|reference] [--workload mine|match|mni|serve]
 
 Workload (default, "mine"): the 20,000-graph database (|V|~U[20,60], average
 degree 4, 16 vertex labels Zipf(1.2), 3 edge labels; seeded, synthetic)
@@ -16,6 +16,15 @@ sampled from the 1,000-graph database (|V|~U[10,30], average degree 3, 4
 uniform vertex labels, unlabeled edges, seed 1), all counted in one batched
 run against that database: int64 embedding counts per (query, graph) and the
 support of every query; the plain path runs one gva_match per query.
+
+"mni": one R-MAT graph (a=0.57, b=c=0.19; 2^22 vertices, 64M undirected
+edges after dedup, 32 vertex labels Zipf(1.0)) resident in HBM; one step
+mines every connected pattern of up to 4 edges with MNI support >= 1000.
+Metric: patterns/s (candidates whose support was decided / step time).
+
+"serve": Poisson arrivals at each --rates value: 80% matching requests
+against the 20,000-graph database, 20% MNI mining requests against the
+R-MAT graph; p50/p99 latency per request kind and rate.
 
 N > 1 (torchrun, one process per GPU): every rank holds the database and
 works on its own share (weak scaling, no collective on the data path); the
@@ -189,7 +198,7 @@ def reference_arm(args, db, queries, workload):
     new_to_old = np.zeros(int(meta[:, 0].max()) + 1, dtype=np.int64)
     new_to_old[meta[:, 0]] = meta[:, 2]
     cores = os.cpu_count() or 1
-    wave = max(1, min(cores, len(queries), 8))
+    wave = max(1, min(cores, len(queries), 64))  # one cpumine process per host core
 
     def one(i_q):
         i, q = i_q

@@ -961,16 +961,32 @@ __global__ void slot_popcount_kernel(const uint32_t* __restrict__ bits, uint32_t
     }
 }
 
-int run_batch(DevDB& db, const std::vector<std::vector<Step>>& steps, cudaStream_t s, uint64_t budget,
-              const uint32_t* vgraph, uint32_t G, uint64_t* counts, uint64_t* graph_counts_host,
-              uint32_t* support_host, bool profile, BatchStats* stats) {
-    (void)vgraph;
-    (void)G;
+int prepare_batch(DevDB& db, const std::vector<std::vector<Step>>& steps, cudaStream_t s, uint64_t budget,
+                  bool per_graph, bool graph_counts, bool profile, PreparedBatch& out) {
+    const auto t0 = std::chrono::steady_clock::now();
     GVA_CUDA_B(cudaSetDevice(db.device));
-    const int nq = (int)steps.size();
+    out.nq = (int)steps.size();
+    out.per_graph = per_graph;
+    out.graph_counts = graph_counts;
+    out.ids.clear();
+    if (out.nq == 0) return GVA_OK;
+    out.ses.reset(new BatchSession(db, s, budget, per_graph ? (uint32_t)out.nq : 0, graph_counts, profile));
+    int rc = out.ses->init();
+    if (!rc) rc = out.ses->submit(steps, {}, &out.ids);
+    out.prep_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    return rc;
+}
+
+int finish_batch(DevDB& db, PreparedBatch& pb, uint64_t* counts, uint64_t* graph_counts_host, uint32_t* support_host,
+                 BatchStats* stats) {
+    const int nq = pb.nq;
     for (int q = 0; q < nq; ++q) counts[q] = 0;
     if (nq == 0) return GVA_OK;
-    const bool per_graph = graph_counts_host || support_host;
+    GVA_CUDA_B(cudaSetDevice(db.device));
+    BatchSession& ses = *pb.ses;
+    cudaStream_t s = ses.stream();
+    if ((graph_counts_host && !pb.graph_counts) || (support_host && !pb.per_graph))
+        return fail(GVA_ERR_ARG, "per-graph results were not prepared for this batch");
     static thread_local cudaEvent_t tev[64][2];
     const int dev = db.device;
     if (dev < 0 || dev >= 64) return fail(GVA_ERR_ARG, "device index out of range");
@@ -978,68 +994,76 @@ int run_batch(DevDB& db, const std::vector<std::vector<Step>>& steps, cudaStream
         GVA_CUDA_B(cudaEventCreate(&tev[dev][0]));
         GVA_CUDA_B(cudaEventCreate(&tev[dev][1]));
     }
+    const auto t_fin0 = std::chrono::steady_clock::now();
     GVA_CUDA_B(cudaEventRecord(tev[dev][0], s));
-    int rc;
-    const auto t_ses0 = std::chrono::steady_clock::now();
-    double loop_ms = 0.0;
-    {
-        BatchSession ses(db, s, budget, per_graph ? (uint32_t)nq : 0, graph_counts_host != nullptr, profile);
-        rc = ses.init();
-        std::vector<int> ids;
-        if (!rc) rc = ses.submit(steps, {}, &ids);
-        const auto t_loop0 = std::chrono::steady_clock::now();
-        while (!rc && !ses.idle()) rc = ses.round();
-        loop_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_loop0).count();
-        if (!rc) {
-            for (int q = 0; q < nq; ++q) counts[q] = ses.plan(ids[q]).count;
-            if (per_graph) {
-                // supports counted on the device; identical plans read their first one's slot
-                uint32_t* d_pop = nullptr;
-                if (cudaMallocAsync((void**)&d_pop, (size_t)nq * 4, s) != cudaSuccess)
-                    rc = fail(GVA_ERR_NOMEM, "support counters");
-                std::vector<uint32_t> pop(nq, 0);
-                if (!rc) {
-                    slot_popcount_kernel<<<nq, 256, 0, s>>>(ses.graph_bits_dev(), ses.words(), (uint32_t)nq, d_pop);
-                    cudaMemcpyAsync(pop.data(), d_pop, (size_t)nq * 4, cudaMemcpyDeviceToHost, s);
-                    cudaFreeAsync(d_pop, s);
-                }
-                if (!rc && graph_counts_host)
-                    cudaMemcpyAsync(graph_counts_host, ses.graph_counts_dev(), (size_t)nq * db.num_graphs * 8,
-                                    cudaMemcpyDeviceToHost, s);
-                if (!rc)
-                    rc = cudaStreamSynchronize(s) == cudaSuccess ? GVA_OK : fail(GVA_ERR_CUDA, "result read-back failed");
-                for (int q = 0; q < nq && !rc; ++q) {
-                    const int sl = ses.plan(ses.first_peer(ids[q])).slot, own = ses.plan(ids[q]).slot;
-                    if (support_host) support_host[q] = pop[sl];
-                    if (graph_counts_host && sl != own)
-                        std::copy(graph_counts_host + (size_t)sl * db.num_graphs,
-                                  graph_counts_host + (size_t)(sl + 1) * db.num_graphs,
-                                  graph_counts_host + (size_t)own * db.num_graphs);
-                }
+    int rc = GVA_OK;
+    const auto t_loop0 = std::chrono::steady_clock::now();
+    while (!rc && !ses.idle()) rc = ses.round();
+    const double loop_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_loop0).count();
+    const std::vector<int>& ids = pb.ids;
+    if (!rc) {
+        for (int q = 0; q < nq; ++q) counts[q] = ses.plan(ids[q]).count;
+        if (support_host || graph_counts_host) {
+            // supports counted on the device; identical plans read their first one's slot
+            uint32_t* d_pop = nullptr;
+            if (cudaMallocAsync((void**)&d_pop, (size_t)nq * 4, s) != cudaSuccess)
+                rc = fail(GVA_ERR_NOMEM, "support counters");
+            std::vector<uint32_t> pop(nq, 0);
+            if (!rc) {
+                slot_popcount_kernel<<<nq, 256, 0, s>>>(ses.graph_bits_dev(), ses.words(), (uint32_t)nq, d_pop);
+                cudaMemcpyAsync(pop.data(), d_pop, (size_t)nq * 4, cudaMemcpyDeviceToHost, s);
+                cudaFreeAsync(d_pop, s);
+            }
+            if (!rc && graph_counts_host)
+                cudaMemcpyAsync(graph_counts_host, ses.graph_counts_dev(), (size_t)nq * db.num_graphs * 8,
+                                cudaMemcpyDeviceToHost, s);
+            if (!rc)
+                rc = cudaStreamSynchronize(s) == cudaSuccess ? GVA_OK : fail(GVA_ERR_CUDA, "result read-back failed");
+            for (int q = 0; q < nq && !rc; ++q) {
+                const int sl = ses.plan(ses.first_peer(ids[q])).slot, own = ses.plan(ids[q]).slot;
+                if (support_host) support_host[q] = pop[sl];
+                if (graph_counts_host && sl != own)
+                    std::copy(graph_counts_host + (size_t)sl * db.num_graphs,
+                              graph_counts_host + (size_t)(sl + 1) * db.num_graphs,
+                              graph_counts_host + (size_t)own * db.num_graphs);
             }
         }
-        if (stats) {
-            stats->submit_ms = ses.submit_ms;
-            stats->round_host_ms = ses.round_host_ms;
-            stats->wait_ms = ses.wait_ms;
-            stats->rounds = ses.rounds;
-            stats->splits = ses.splits;
-            stats->launches = ses.launches;
-            stats->nodes = ses.num_nodes();
-            for (int i = 0; i < 5; ++i) stats->phase_ms[i] = ses.phase_ms[i];
-            for (int i = 0; i < K_NUM; ++i) stats->kstat[i] = ses.kstat[i];
-        }
+    }
+    if (stats) {
+        stats->submit_ms = ses.submit_ms;
+        stats->round_host_ms = ses.round_host_ms;
+        stats->wait_ms = ses.wait_ms;
+        stats->rounds = ses.rounds;
+        stats->splits = ses.splits;
+        stats->launches = ses.launches;
+        stats->nodes = ses.num_nodes();
+        for (int i = 0; i < 5; ++i) stats->phase_ms[i] = ses.phase_ms[i];
+        for (int i = 0; i < K_NUM; ++i) stats->kstat[i] = ses.kstat[i];
     }
     cudaEventRecord(tev[dev][1], s);
+    pb.ses.reset();  // frees the session's device memory (stream-ordered) and syncs its stream
     cudaEventSynchronize(tev[dev][1]);
     float ms = 0.f;
     cudaEventElapsedTime(&ms, tev[dev][0], tev[dev][1]);
     if (stats) {
         stats->gpu_ms = ms;
-        stats->session_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_ses0).count() -
-                            loop_ms - stats->submit_ms;
+        const double fin_ms =
+            std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_fin0).count();
+        stats->session_ms = (pb.prep_ms - stats->submit_ms) + (fin_ms - loop_ms);
     }
     return rc;
+}
+
+int run_batch(DevDB& db, const std::vector<std::vector<Step>>& steps, cudaStream_t s, uint64_t budget,
+              const uint32_t* vgraph, uint32_t G, uint64_t* counts, uint64_t* graph_counts_host,
+              uint32_t* support_host, bool profile, BatchStats* stats) {
+    (void)vgraph;
+    (void)G;
+    PreparedBatch pb;
+    int rc = prepare_batch(db, steps, s, budget, graph_counts_host || support_host, graph_counts_host != nullptr,
+                           profile, pb);
+    if (rc) return rc;
+    return finish_batch(db, pb, counts, graph_counts_host, support_host, stats);
 }
 
 int set_graph_ids(DevDB& db, const uint64_t* first, uint32_t num_graphs) {

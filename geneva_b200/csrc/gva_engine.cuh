@@ -157,6 +157,7 @@ public:
     int read_support(int q, uint32_t* support, uint64_t* graph_counts_host);
     void release(int q);
     size_t num_nodes() const { return nodes.size(); }
+    cudaStream_t stream() const { return s; }
     size_t num_active() const { return active.size(); }
     uint32_t words() const { return ctx_words; }
     uint64_t* graph_counts_dev() const;
@@ -209,6 +210,20 @@ private:
     size_t blk_cap = 0;
     Staging staging_blk;
 };
+// run_batch in two halves, so that a caller can build the next batch's
+// session (device set-up and step trie, host work) while the previous one's
+// rounds run: prepare_batch may run on another thread than finish_batch.
+struct PreparedBatch {
+    std::unique_ptr<BatchSession> ses;
+    std::vector<int> ids;
+    int nq = 0;
+    bool per_graph = false, graph_counts = false;
+    double prep_ms = 0.0;
+};
+int prepare_batch(DevDB& db, const std::vector<std::vector<Step>>& steps, cudaStream_t s, uint64_t budget,
+                  bool per_graph, bool graph_counts, bool profile, PreparedBatch& out);
+int finish_batch(DevDB& db, PreparedBatch& pb, uint64_t* counts, uint64_t* graph_counts_host, uint32_t* support_host,
+                 BatchStats* stats);
 int set_graph_ids(DevDB& db, const uint64_t* first, uint32_t num_graphs);
 
 struct MinedPattern {

@@ -22,6 +22,8 @@
 #include <chrono>
 #include <cstring>
 #include <functional>
+#include <future>
+#include <memory>
 #include <thread>
 #include <map>
 #include <set>
@@ -438,15 +440,33 @@ int run_mine(DevDB& db, cudaStream_t s, uint64_t budget, uint32_t max_edges, uin
         st.plan_ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_order).count();
         std::vector<uint32_t> bsup;
         std::vector<uint64_t> bemb;
-        for (size_t b0 = 0; b0 < n; b0 += batch_limit) {
-            const size_t b1 = std::min(n, b0 + batch_limit);
+        // batch b + 1's session (device set-up, step trie) is built on a
+        // helper thread while batch b's rounds run
+        struct Prep {
+            PreparedBatch pb;
+            int rc = GVA_OK;
+            std::string err;
+        };
+        const size_t nbatch = (n + batch_limit - 1) / batch_limit;
+        auto prepare = [&](size_t b) {
+            std::unique_ptr<Prep> p(new Prep());
+            const size_t b0 = b * batch_limit, b1 = std::min(n, b0 + batch_limit);
             std::vector<std::vector<Step>> cur(b1 - b0);
             for (size_t i = b0; i < b1; ++i) cur[i - b0] = std::move(all[order[i]]);
+            p->rc = prepare_batch(db, cur, s, budget, true, false, profile, p->pb);
+            if (p->rc) p->err = last_error_cstr();
+            return p;
+        };
+        std::future<std::unique_ptr<Prep>> next = std::async(std::launch::async, prepare, (size_t)0);
+        for (size_t b = 0; b < nbatch; ++b) {
+            const size_t b0 = b * batch_limit, b1 = std::min(n, b0 + batch_limit);
+            std::unique_ptr<Prep> cur = next.get();
+            if (b + 1 < nbatch) next = std::async(std::launch::async, prepare, b + 1);
+            if (cur->rc) return fail(cur->rc, cur->err);
             bsup.assign(b1 - b0, 0);
             bemb.assign(b1 - b0, 0);
             BatchStats bs;
-            int rc = run_batch(db, cur, s, budget, db.vgraph, db.num_graphs, bemb.data(), nullptr, bsup.data(), profile,
-                               &bs);
+            int rc = finish_batch(db, cur->pb, bemb.data(), nullptr, bsup.data(), &bs);
             if (rc) return rc;
             for (size_t i = b0; i < b1; ++i) {
                 sup[order[i]] = bsup[i - b0];
