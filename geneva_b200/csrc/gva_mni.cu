@@ -15,11 +15,14 @@
 //   task    one automorphism orbit of one pattern (orbits share image sets),
 //           rooted at a representative r; its seeds are the data vertices
 //           carrying r's label
-//   search  for a seed v, a warp runs a depth-first search for one embedding
-//           with f(r) = v: per level the candidates are the shortest segment
-//           among the already matched neighbours, 32 candidates per step (one
-//           per lane), each filtered by injectivity and by binary search in
-//           the other matched neighbours' segments, the first survivor taken
+//   search  a depth-first search for one embedding with f(r) = v: per level
+//           the candidates are the shortest segment among the already matched
+//           neighbours, each filtered by injectivity and by binary search in
+//           the other matched neighbours' segments, the first survivor taken.
+//           Each lane first searches its own seed for up to 64 candidates (32
+//           independent searches per warp keep many loads in flight); seeds
+//           still undecided are searched by the whole warp, 32 candidates per
+//           step, one seed at a time
 //   stop    a task stops once its count reaches the cap (default: the minimum
 //           support, which decides frequency) or the smallest exhausted orbit
 //           of its pattern, so the support returned is min(MNI, cap) exactly
@@ -144,7 +147,7 @@ __device__ bool mni_dfs(const MniTask& T, const PartPtr* __restrict__ parts, uin
         end[lv] = bhi;
         gadj[lv] = ba;
         gsel[lv] = bj;
-        cnt[P_OPENS] += 1;
+        cnt[P_OPENS] += lane == 0 ? 1 : 0;
     };
     int i = 1;
     open(1);
@@ -190,10 +193,87 @@ __device__ bool mni_dfs(const MniTask& T, const PartPtr* __restrict__ parts, uin
     }
 }
 
+// One lane's own depth-first search for an embedding with level 0 at `root`,
+// candidates taken one at a time: 1 = found, 0 = none exists, -1 = gave up
+// after `budget` candidates (the warp-cooperative search then decides).
+// Thirty-two of these run side by side in a warp, one root per lane, so
+// their dependent loads overlap; most roots of frequent patterns succeed or
+// fail within a few candidates.
+__device__ int lane_dfs(const MniTask& T, const PartPtr* __restrict__ parts, uint32_t L, uint32_t root,
+                        uint32_t budget, unsigned long long* cnt) {
+    uint32_t f[kMniMaxVertices];
+    uint32_t pos[kMniMaxVertices], end[kMniMaxVertices], gsel[kMniMaxVertices];
+    const uint32_t* gadj[kMniMaxVertices];
+    const int n = (int)T.n;
+    f[0] = root;
+    if (n <= 1) return 1;
+    auto open = [&](int lv) {
+        uint32_t blo = 0, bhi = 0, bj = 0;
+        const uint32_t* ba = nullptr;
+        bool have = false;
+        uint32_t m = T.nbmask[lv];
+        while (m) {
+            const int j = __ffs(m) - 1;
+            m &= m - 1;
+            const PartPtr P = parts[T.part[lv][j] - 1];
+            const uint64_t t = (uint64_t)f[j] * L + T.lab[lv];
+            const uint32_t lo = __ldg(P.off + t), hi = __ldg(P.off + t + 1);
+            if (!have || hi - lo < bhi - blo) {
+                blo = lo;
+                bhi = hi;
+                bj = (uint32_t)j;
+                ba = P.adj;
+                have = true;
+            }
+        }
+        pos[lv] = blo;
+        end[lv] = bhi;
+        gadj[lv] = ba;
+        gsel[lv] = bj;
+        cnt[P_OPENS] += 1;
+    };
+    int i = 1;
+    open(1);
+    uint32_t steps = 0;
+    for (;;) {
+        if (pos[i] >= end[i]) {
+            if (--i == 0) return 0;
+            continue;
+        }
+        if (++steps > budget) return -1;
+        const uint32_t c = __ldg(gadj[i] + pos[i]);
+        ++pos[i];
+        cnt[P_SCANNED] += 1;
+        bool ok = true;
+        uint32_t e = T.eqmask[i];
+        while (e && ok) {
+            const int j = __ffs(e) - 1;
+            e &= e - 1;
+            ok = c != f[j];
+        }
+        uint32_t m = T.nbmask[i] & ~(1u << gsel[i]);
+        while (m && ok) {
+            const int j = __ffs(m) - 1;
+            m &= m - 1;
+            const PartPtr P = parts[T.part[i][j] - 1];
+            const uint64_t t = (uint64_t)f[j] * L + T.lab[i];
+            ok = find_in(P.adj, __ldg(P.off + t), __ldg(P.off + t + 1), c) != 0xffffffffu;
+            cnt[P_CHECKS] += 1;
+        }
+        if (!ok) continue;
+        f[i] = c;
+        if (i + 1 == n) return 1;
+        ++i;
+        open(i);
+    }
+}
+
+constexpr uint32_t kLaneBudget = 64;  // candidates a lane search may take before the warp search decides
+
 // Persistent: every warp pulls 128-seed items; per 32 seeds it checks the
 // task's count against its cap, filters roots by neighbour-label degrees and
 // runs one search per surviving root.
-__global__ void __launch_bounds__(kMniWarps * 32)
+__global__ void __launch_bounds__(kMniWarps * 32, 6)
 mni_search_kernel(const MniTask* __restrict__ tasks, const MniSlot* __restrict__ slots,
                   const uint64_t* __restrict__ item0, const uint32_t* __restrict__ item_slot, uint64_t nitems,
                   const uint32_t* __restrict__ seeds, uint32_t item_len,
@@ -233,9 +313,13 @@ mni_search_kernel(const MniTask* __restrict__ tasks, const MniSlot* __restrict__
                 ok = root_ok(T, parts, L, v);
                 cnt[P_SEEDS] += 1;
             }
-            uint32_t m = __ballot_sync(0xffffffffu, ok);
-            if (lane == 0) cnt[P_ROOTS] += __popc(m);
-            uint32_t found = 0;
+            if (lane == 0) cnt[P_ROOTS] += __popc(__ballot_sync(0xffffffffu, ok));
+            // every lane searches its own root; roots whose search ran out of
+            // budget are decided by the whole warp, one after another
+            int verdict = 0;
+            if (ok) verdict = lane_dfs(T, parts, L, v, kLaneBudget, cnt);
+            uint32_t found = __popc(__ballot_sync(0xffffffffu, verdict == 1));
+            uint32_t m = __ballot_sync(0xffffffffu, verdict < 0);
             while (m) {
                 const int l = __ffs(m) - 1;
                 m &= m - 1;
@@ -247,10 +331,8 @@ mni_search_kernel(const MniTask* __restrict__ tasks, const MniSlot* __restrict__
         }
     }
     if (prof) {
-        // opens are counted once per lane; every lane counted them
         for (int k = 0; k < P_NUM; ++k) {
             unsigned long long x = cnt[k];
-            if (k == P_OPENS) x = lane == 0 ? x : 0;
             x = warp_sum(x);
             if (lane == 0 && x) atomicAdd(prof + k, x);
         }
