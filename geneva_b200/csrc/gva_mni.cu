@@ -313,7 +313,8 @@ mni_search_kernel(const MniTask* __restrict__ tasks, const MniSlot* __restrict__
                 ok = root_ok(T, parts, L, v);
                 cnt[P_SEEDS] += 1;
             }
-            if (lane == 0) cnt[P_ROOTS] += __popc(__ballot_sync(0xffffffffu, ok));
+            const uint32_t roots = __ballot_sync(0xffffffffu, ok);  // all lanes vote
+            if (lane == 0) cnt[P_ROOTS] += __popc(roots);
             // every lane searches its own root; roots whose search ran out of
             // budget are decided by the whole warp, one after another
             int verdict = 0;
@@ -674,9 +675,10 @@ int run_mni(DevDB& db, const std::vector<MniPattern>& pats, const std::vector<ch
             st.launches += 2;
             g_mni_launches += 2;
             st.rounds++;
-            if (cudaGetLastError() != cudaSuccess ||
-                cudaMemcpyAsync(counts.data(), d_counts, bytes_counts, cudaMemcpyDeviceToHost, s) != cudaSuccess) {
-                rc = fail(GVA_ERR_CUDA, "MNI search launch failed");
+            cudaError_t le = cudaGetLastError();
+            if (le == cudaSuccess) le = cudaMemcpyAsync(counts.data(), d_counts, bytes_counts, cudaMemcpyDeviceToHost, s);
+            if (le != cudaSuccess) {
+                rc = fail(GVA_ERR_CUDA, std::string("MNI search launch failed: ") + cudaGetErrorString(le));
                 break;
             }
             const auto w0 = std::chrono::steady_clock::now();

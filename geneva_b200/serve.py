@@ -109,6 +109,15 @@ class Server:
 
     def close(self):
         self._stop.set()
+        # mining requests not started yet are cancelled (one in progress finishes)
+        while True:
+            try:
+                r = self._mine_q.get_nowait()
+            except queue.Empty:
+                break
+            if r is not None and not r.future.done():
+                r.done = time.perf_counter()
+                r.future.set_exception(GenevaError(5, "server closed before the request started"))
         self._mine_q.put(None)
         self._loop.join()
         self._miner.join()
