@@ -72,7 +72,7 @@ def parse_args():
     ap.add_argument("--workload", default="mine", choices=["mine", "match", "serve", "mni"])
     ap.add_argument("--rates", default="10,100,500,2000", help="serve workload: arrival rates (req/s)")
     ap.add_argument("--duration", type=float, default=2.0, help="serve workload: seconds of arrivals per rate")
-    ap.add_argument("--drain", type=float, default=60.0, help="serve workload: seconds to wait for results per rate")
+    ap.add_argument("--drain", type=float, default=30.0, help="serve workload: seconds to wait for results per rate")
     ap.add_argument("--queries", type=int, default=4096, help="match workload: patterns per rank per step")
     ap.add_argument("--max-edges", type=int, default=6)
     ap.add_argument("--min-support", type=float, default=0.02, help="fraction of graphs")

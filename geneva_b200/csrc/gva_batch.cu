@@ -19,6 +19,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstddef>
 #include <atomic>
 #include <chrono>
 #include <cstring>
@@ -79,23 +80,31 @@ struct TaskRef {
     uint64_t nrows;
 };
 
-__device__ __forceinline__ void load_desc(TaskDesc& dst, const TaskDesc* src) {
-    const uint32_t* s = reinterpret_cast<const uint32_t*>(src);
-    uint32_t* d = reinterpret_cast<uint32_t*>(&dst);
-    for (int i = threadIdx.x; i < (int)(sizeof(TaskDesc) / 4); i += blockDim.x) d[i] = s[i];
-}
-
-// Descriptor of task t: its node's parameters patched with the task's frontier
-// slice (ExtArgs and RedArgs both start with `in`, `nrows`).
+// Descriptor of task t: its node's parameters patched, while they are copied,
+// with the task's frontier slice (ExtArgs and RedArgs both start with `in`,
+// `nrows`), so one barrier makes the copy visible.
 __device__ __forceinline__ void load_task(TaskDesc& d, const TaskDesc* __restrict__ nodes,
                                           const TaskRef* __restrict__ refs, int t) {
+    constexpr int kB0 = (int)(offsetof(TaskDesc, block0) / 4);
+    constexpr int kIn = (int)((offsetof(TaskDesc, e) + offsetof(ExtArgs, in)) / 4);
+    constexpr int kNr = (int)((offsetof(TaskDesc, e) + offsetof(ExtArgs, nrows)) / 4);
+    static_assert(offsetof(ExtArgs, in) == offsetof(RedArgs, in) && offsetof(ExtArgs, nrows) == offsetof(RedArgs, nrows),
+                  "extension and reduction arguments share their frontier fields");
     const TaskRef r = refs[t];
-    load_desc(d, nodes + r.node);
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        d.block0 = r.block0;
-        d.e.in = r.in;
-        d.e.nrows = r.nrows;
+    const uint32_t* s = reinterpret_cast<const uint32_t*>(nodes + r.node);
+    uint32_t* dw = reinterpret_cast<uint32_t*>(&d);
+    const uint64_t in = (uint64_t)r.in;
+    for (int i = threadIdx.x; i < (int)(sizeof(TaskDesc) / 4); i += blockDim.x) {
+        uint32_t v;
+        if (i == kB0 || i == kB0 + 1)
+            v = (uint32_t)(r.block0 >> (32 * (i - kB0)));
+        else if (i == kIn || i == kIn + 1)
+            v = (uint32_t)(in >> (32 * (i - kIn)));
+        else if (i == kNr || i == kNr + 1)
+            v = (uint32_t)(r.nrows >> (32 * (i - kNr)));
+        else
+            v = __ldg(s + i);
+        dw[i] = v;
     }
     __syncthreads();
 }
@@ -978,7 +987,7 @@ int prepare_batch(DevDB& db, const std::vector<std::vector<Step>>& steps, cudaSt
 }
 
 int finish_batch(DevDB& db, PreparedBatch& pb, uint64_t* counts, uint64_t* graph_counts_host, uint32_t* support_host,
-                 BatchStats* stats) {
+                 BatchStats* stats, const volatile int* cancel) {
     const int nq = pb.nq;
     for (int q = 0; q < nq; ++q) counts[q] = 0;
     if (nq == 0) return GVA_OK;
@@ -998,7 +1007,13 @@ int finish_batch(DevDB& db, PreparedBatch& pb, uint64_t* counts, uint64_t* graph
     GVA_CUDA_B(cudaEventRecord(tev[dev][0], s));
     int rc = GVA_OK;
     const auto t_loop0 = std::chrono::steady_clock::now();
-    while (!rc && !ses.idle()) rc = ses.round();
+    while (!rc && !ses.idle()) {
+        if (cancel && *cancel) {
+            rc = fail(GVA_ERR_CANCELLED, "cancelled");
+            break;
+        }
+        rc = ses.round();
+    }
     const double loop_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_loop0).count();
     const std::vector<int>& ids = pb.ids;
     if (!rc) {

@@ -223,7 +223,7 @@ struct PreparedBatch {
 int prepare_batch(DevDB& db, const std::vector<std::vector<Step>>& steps, cudaStream_t s, uint64_t budget,
                   bool per_graph, bool graph_counts, bool profile, PreparedBatch& out);
 int finish_batch(DevDB& db, PreparedBatch& pb, uint64_t* counts, uint64_t* graph_counts_host, uint32_t* support_host,
-                 BatchStats* stats);
+                 BatchStats* stats, const volatile int* cancel = nullptr);
 int set_graph_ids(DevDB& db, const uint64_t* first, uint32_t num_graphs);
 
 struct MinedPattern {
@@ -250,7 +250,7 @@ typedef int (*ReduceFn)(uint32_t* supports, uint64_t* embeddings, uint64_t n, vo
 // = min_support, which decides frequency).
 int run_mine(DevDB& db, cudaStream_t s, uint64_t budget, uint32_t max_edges, uint32_t min_support,
              uint32_t batch_limit, bool profile, ReduceFn reduce, void* reduce_user, uint32_t support_mode,
-             uint32_t mni_cap, std::vector<MinedPattern>& out, MineStats& st);
+             uint32_t mni_cap, std::vector<MinedPattern>& out, MineStats& st, const volatile int* cancel = nullptr);
 
 // ---- single-graph MNI support (gva_mni.cu) ----
 constexpr int kMniMaxVertices = 8;
@@ -275,6 +275,13 @@ int mni_pattern_from_text(const DevDB& db, const std::string& text, MniPattern& 
 int run_mni(DevDB& db, const std::vector<MniPattern>& pats, const std::vector<char>& absent, uint32_t cap, bool plain,
             bool profile, cudaStream_t s, std::vector<uint32_t>& support, MniStats& st);
 uint64_t mni_kernel_launches();
+// run_mni in two halves: the host half (orbits, search orders, task records;
+// no device work, may run on another thread) and the device rounds.
+struct MniPrepared;
+std::shared_ptr<MniPrepared> mni_prepare(const DevDB& db, const std::vector<MniPattern>& pats,
+                                         const std::vector<char>& absent);
+int mni_run_prepared(DevDB& db, const MniPrepared& prep, uint32_t cap, bool plain, bool profile, cudaStream_t s,
+                     std::vector<uint32_t>& support, MniStats& st, const volatile int* cancel = nullptr);
 
 size_t step_scratch_bytes(uint64_t in_rows);
 // run_step with the library's fixed device scratch array (no allocation).

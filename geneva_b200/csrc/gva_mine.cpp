@@ -306,7 +306,7 @@ constexpr uint32_t kBuckets = 256;  // candidate partitions by code hash (fixed:
 
 int run_mine(DevDB& db, cudaStream_t s, uint64_t budget, uint32_t max_edges, uint32_t min_support,
              uint32_t batch_limit, bool profile, ReduceFn reduce, void* reduce_user, uint32_t support_mode,
-             uint32_t mni_cap, std::vector<MinedPattern>& out, MineStats& st) {
+             uint32_t mni_cap, std::vector<MinedPattern>& out, MineStats& st, const volatile int* cancel) {
     out.clear();
     st = MineStats();
     const bool mni = support_mode == GVA_SUPPORT_MNI;
@@ -370,11 +370,13 @@ int run_mine(DevDB& db, cudaStream_t s, uint64_t budget, uint32_t max_edges, uin
         const size_t n = cands.size();
         sup.assign(n, 0);
         emb.assign(n, 0);
-        std::vector<MniPattern> mp;
         std::vector<uint32_t> bsup;
-        for (size_t b0 = 0; b0 < n; b0 += batch_limit) {
-            const size_t b1 = std::min(n, b0 + (size_t)batch_limit);
-            mp.assign(b1 - b0, MniPattern());
+        // batch b + 1's search tasks are built on a helper thread while batch
+        // b's rounds run on the device
+        const size_t nbatch = (n + batch_limit - 1) / batch_limit;
+        auto prepare = [&](size_t b) {
+            const size_t b0 = b * batch_limit, b1 = std::min(n, b0 + (size_t)batch_limit);
+            std::vector<MniPattern> mp(b1 - b0);
             for (size_t i = b0; i < b1; ++i) {
                 const Pattern& c = cands[i];
                 MniPattern& m = mp[i - b0];
@@ -383,8 +385,16 @@ int run_mine(DevDB& db, cudaStream_t s, uint64_t budget, uint32_t max_edges, uin
                 for (uint32_t e = 0; e < c.ne; ++e)
                     m.el[c.edges[e].u][c.edges[e].v] = m.el[c.edges[e].v][c.edges[e].u] = (uint8_t)c.edges[e].el;
             }
+            return mni_prepare(db, mp, {});
+        };
+        std::future<std::shared_ptr<MniPrepared>> next =
+            nbatch ? std::async(std::launch::async, prepare, (size_t)0) : std::future<std::shared_ptr<MniPrepared>>();
+        for (size_t b = 0; b < nbatch; ++b) {
+            const size_t b0 = b * batch_limit, b1 = std::min(n, b0 + (size_t)batch_limit);
+            std::shared_ptr<MniPrepared> cur = next.get();
+            if (b + 1 < nbatch) next = std::async(std::launch::async, prepare, b + 1);
             MniStats ms;
-            int rc = run_mni(db, mp, {}, mni_cap, false, profile, s, bsup, ms);
+            int rc = mni_run_prepared(db, *cur, mni_cap, false, profile, s, bsup, ms, cancel);
             if (rc) return rc;
             for (size_t i = b0; i < b1; ++i) sup[i] = bsup[i - b0];
             gpu_ms += ms.gpu_ms;
@@ -466,7 +476,7 @@ int run_mine(DevDB& db, cudaStream_t s, uint64_t budget, uint32_t max_edges, uin
             bsup.assign(b1 - b0, 0);
             bemb.assign(b1 - b0, 0);
             BatchStats bs;
-            int rc = finish_batch(db, cur->pb, bemb.data(), nullptr, bsup.data(), &bs);
+            int rc = finish_batch(db, cur->pb, bemb.data(), nullptr, bsup.data(), &bs, cancel);
             if (rc) return rc;
             for (size_t i = b0; i < b1; ++i) {
                 sup[order[i]] = bsup[i - b0];
@@ -533,6 +543,7 @@ int run_mine(DevDB& db, cudaStream_t s, uint64_t budget, uint32_t max_edges, uin
 
     // ---- levels 2..max_edges
     for (uint32_t k = 1; k < max_edges && !level.empty(); ++k) {
+        if (cancel && *cancel) return fail(GVA_ERR_CANCELLED, "cancelled");
         auto t_gen = std::chrono::steady_clock::now();
         // (1) each thread extends every nthreads-th pattern by one frequent
         // edge type, keeps the extensions whose canonical code it has not seen

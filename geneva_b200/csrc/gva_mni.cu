@@ -42,6 +42,7 @@
 #include <atomic>
 #include <chrono>
 #include <cstring>
+#include <memory>
 #include <string>
 #include <thread>
 #include <vector>
@@ -498,20 +499,28 @@ int mni_pattern_from_text(const DevDB& db, const std::string& text, MniPattern& 
     return GVA_OK;
 }
 
-int run_mni(DevDB& db, const std::vector<MniPattern>& pats, const std::vector<char>& absent, uint32_t cap, bool plain,
-            bool profile, cudaStream_t s, std::vector<uint32_t>& support, MniStats& st) {
-    const auto t_host0 = std::chrono::steady_clock::now();
-    GVA_CUDA_M(cudaSetDevice(db.device));
+// The host half of an MNI run: the search tasks of a batch of patterns.
+struct MniPrepared {
+    size_t np = 0;
+    std::vector<MniTask> tasks;
+    std::vector<uint32_t> task_pat;    // pattern of each task
+    std::vector<uint32_t> first_task;  // np + 1 offsets
+    double prep_ms = 0.0;
+};
+
+std::shared_ptr<MniPrepared> mni_prepare(const DevDB& db, const std::vector<MniPattern>& pats,
+                                         const std::vector<char>& absent) {
+    const auto t0 = std::chrono::steady_clock::now();
+    auto prep = std::make_shared<MniPrepared>();
     const size_t np = pats.size();
-    support.assign(np, 0);
-    if (np == 0) return GVA_OK;
-    if (cap == 0) cap = 0xffffffffu;
+    prep->np = np;
+    std::vector<MniTask>& tasks = prep->tasks;
+    std::vector<uint32_t>& task_pat = prep->task_pat;
+    std::vector<uint32_t>& first_task = prep->first_task;
+    first_task.assign(np + 1, 0);
     // tasks: one per automorphism orbit of each pattern whose labels all
     // occur, built on all host threads over contiguous blocks of patterns
-    std::vector<MniTask> tasks;
-    std::vector<uint32_t> task_pat;
-    std::vector<uint32_t> first_task(np + 1, 0);
-    {
+    if (np) {
         const unsigned nth = (unsigned)std::max<size_t>(1, std::min<size_t>({64, std::thread::hardware_concurrency(),
                                                                              (np + 255) / 256}));
         std::vector<std::vector<MniTask>> tl(nth);
@@ -542,6 +551,28 @@ int run_mni(DevDB& db, const std::vector<MniPattern>& pats, const std::vector<ch
         for (size_t q = 0; q < np; ++q)
             for (uint32_t t = first_task[q]; t < first_task[q + 1]; ++t) task_pat[t] = (uint32_t)q;
     }
+    prep->prep_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    return prep;
+}
+
+int run_mni(DevDB& db, const std::vector<MniPattern>& pats, const std::vector<char>& absent, uint32_t cap, bool plain,
+            bool profile, cudaStream_t s, std::vector<uint32_t>& support, MniStats& st) {
+    std::shared_ptr<MniPrepared> prep = mni_prepare(db, pats, absent);
+    return mni_run_prepared(db, *prep, cap, plain, profile, s, support, st);
+}
+
+int mni_run_prepared(DevDB& db, const MniPrepared& prep, uint32_t cap, bool plain, bool profile, cudaStream_t s,
+                     std::vector<uint32_t>& support, MniStats& st, const volatile int* cancel) {
+    const auto t_host0 = std::chrono::steady_clock::now();
+    st.host_ms += prep.prep_ms;
+    GVA_CUDA_M(cudaSetDevice(db.device));
+    const size_t np = prep.np;
+    support.assign(np, 0);
+    if (np == 0) return GVA_OK;
+    if (cap == 0) cap = 0xffffffffu;
+    const std::vector<MniTask>& tasks = prep.tasks;
+    const std::vector<uint32_t>& task_pat = prep.task_pat;
+    const std::vector<uint32_t>& first_task = prep.first_task;
     const size_t nt = tasks.size();
     st.tasks += nt;
     if (nt == 0) return GVA_OK;
@@ -609,6 +640,10 @@ int run_mni(DevDB& db, const std::vector<MniPattern>& pats, const std::vector<ch
             }
         }
         for (uint32_t round = 0; !active.empty(); ++round) {
+            if (cancel && *cancel) {
+                rc = fail(GVA_ERR_CANCELLED, "cancelled");
+                break;
+            }
             // retire tasks already at their pattern's cap
             size_t w = 0;
             for (uint32_t t : active)

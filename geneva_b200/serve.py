@@ -87,6 +87,7 @@ class Server:
         self._reserved = 0
         self._next_tag = 1
         self._stop = threading.Event()
+        self._cancel = ctypes.c_int(0)  # set on close: a mining run in progress stops at its next round
         self.rounds = 0
         self.round_s: List[float] = []  # wall time of each round (host + device)
         self.completed: List[Request] = []
@@ -109,7 +110,7 @@ class Server:
 
     def close(self):
         self._stop.set()
-        # mining requests not started yet are cancelled (one in progress finishes)
+        # mining requests not started yet are cancelled; one in progress stops at its next round
         while True:
             try:
                 r = self._mine_q.get_nowait()
@@ -118,6 +119,7 @@ class Server:
             if r is not None and not r.future.done():
                 r.done = time.perf_counter()
                 r.future.set_exception(GenevaError(5, "server closed before the request started"))
+        self._cancel.value = 1
         self._mine_q.put(None)
         self._loop.join()
         self._miner.join()
@@ -222,9 +224,10 @@ class Server:
             try:
                 if self.mine_db is not None:
                     pats, stats = mine(self.mine_db, r.payload[0], r.payload[1], stream=self.mine_stream,
-                                       support="mni")
+                                       support="mni", cancel=self._cancel)
                 else:
-                    pats, stats = mine(self.db, r.payload[0], r.payload[1], stream=self.mine_stream)
+                    pats, stats = mine(self.db, r.payload[0], r.payload[1], stream=self.mine_stream,
+                                       cancel=self._cancel)
                 r.result = (pats, stats)
                 r.done = time.perf_counter()
                 with self._lock:

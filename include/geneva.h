@@ -38,6 +38,7 @@ extern "C" {
 #define GVA_ERR_NOMEM 4       /* device or host allocation failed / budget  */
 #define GVA_ERR_ARG 5         /* bad argument (null, out of range, size)    */
 #define GVA_ERR_UNSUPPORTED 6 /* outside the reference's limits (see docs)  */
+#define GVA_ERR_CANCELLED 7   /* the caller's cancel flag was set            */
 
 #define GVA_MODE_DV 0 /* genMatchOrder        (src/genMatchOrder.cpp:672)       */
 #define GVA_MODE_SV 1 /* genMatchOrderSingleV (src/genMatchOrderSingleV.cpp:678) */
@@ -229,6 +230,8 @@ typedef struct gva_mine_opts {
     void* reduce_user;
     uint32_t support_mode; /* GVA_SUPPORT_GRAPHS or GVA_SUPPORT_MNI */
     uint32_t mni_cap;      /* MNI: supports are min(MNI, mni_cap); 0 = min_support */
+    const volatile int* cancel; /* optional: once *cancel != 0 (set by another thread), the run stops at
+                                   its next batch or round boundary with GVA_ERR_CANCELLED */
 } gva_mine_opts;
 
 typedef struct gva_mine_stats {

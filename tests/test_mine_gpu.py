@@ -60,3 +60,22 @@ def test_mining_with_more_than_256_labels(native):
     got = {pattern_from_text(p.text): p.support for p in pats}
     assert got == brute_mine(db, 3, 3) and len(got) > 0
     gdb.close()
+
+
+def test_mining_cancel_flag(native):
+    """A set cancel flag stops a run at its first batch boundary with status 7."""
+    import ctypes
+    db = workloads.graph_database(100, 6, 14, 3.0, 3, None, 2, seed=5, name="tiny4")
+    gdb = gv.Database.from_edges(db.vlabels, db.src, db.dst, db.elabels)
+    gdb.set_graphs(db.first)
+    flag = ctypes.c_int(1)
+    with pytest.raises(gv.GenevaError) as e:
+        gv.mine(gdb, 3, 5, cancel=flag)
+    assert e.value.status == 7
+    with pytest.raises(gv.GenevaError) as e:
+        gv.mine(gdb, 3, 5, support="mni", cancel=flag)
+    assert e.value.status == 7
+    flag.value = 0
+    pats, _ = gv.mine(gdb, 3, 5, cancel=flag)  # unset: runs to completion
+    assert len(pats) > 0
+    gdb.close()
