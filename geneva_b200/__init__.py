@@ -73,7 +73,8 @@ class _MineOpts(ctypes.Structure):
     _fields_ = [("stream", ctypes.c_void_p), ("budget_bytes", ctypes.c_uint64), ("max_edges", ctypes.c_uint32),
                 ("min_support", ctypes.c_uint32), ("batch_limit", ctypes.c_uint32), ("profile", ctypes.c_uint32),
                 ("reduce", REDUCE_FN), ("reduce_user", ctypes.c_void_p), ("support_mode", ctypes.c_uint32),
-                ("mni_cap", ctypes.c_uint32), ("cancel", ctypes.c_void_p)]
+                ("mni_cap", ctypes.c_uint32), ("cancel", ctypes.c_void_p), ("sm_percent", ctypes.c_uint32),
+                ("host_threads", ctypes.c_uint32)]
 
 
 class _MineStats(ctypes.Structure):
@@ -440,7 +441,7 @@ class MinedPatterns(_abc.Sequence):
 
 def mine(db: Database, max_edges: int, min_support: int, stream: Optional[int] = None, budget_bytes: int = 0,
          batch_limit: int = 0, profile: bool = False, reduce=None, support: str = "graphs", mni_cap: int = 0,
-         cancel: Optional[ctypes.c_int] = None):
+         cancel: Optional[ctypes.c_int] = None, sm_percent: int = 0, host_threads: int = 0):
     """Frequent connected patterns (gva_mine).
 
     support="graphs": a pattern's support is the number of database graphs
@@ -451,8 +452,10 @@ def mine(db: Database, max_edges: int, min_support: int, stream: Optional[int] =
     place) combines each level's counts across processes holding disjoint
     graph shards (graph support only).  `cancel` (a ctypes.c_int another
     thread may set to 1) stops the run at its next batch or round boundary
-    with GenevaError status 7.  Returns (patterns, stats); stats["kernels"]
-    is filled when profiling."""
+    with GenevaError status 7.  sm_percent (MNI) caps the share of the SMs
+    the search kernel fills and host_threads the host threads used (0 = all),
+    so that a server's other work keeps running.  Returns (patterns, stats);
+    stats["kernels"] is filled when profiling."""
     lib = library()
     cb = REDUCE_FN(0)
     if reduce is not None:
@@ -467,7 +470,7 @@ def mine(db: Database, max_edges: int, min_support: int, stream: Optional[int] =
         cb = REDUCE_FN(_cb)
     mode = {"graphs": SUPPORT_GRAPHS, "mni": SUPPORT_MNI}[support]
     o = _MineOpts(stream or None, budget_bytes, max_edges, min_support, batch_limit, 1 if profile else 0, cb, None,
-                  mode, mni_cap, ctypes.addressof(cancel) if cancel is not None else None)
+                  mode, mni_cap, ctypes.addressof(cancel) if cancel is not None else None, sm_percent, host_threads)
     h = ctypes.c_void_p()
     _check(lib.gva_mine(db._h, ctypes.byref(o), ctypes.byref(h)))
     try:

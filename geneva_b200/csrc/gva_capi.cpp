@@ -345,7 +345,7 @@ int gva_mine(gva_db* db, const gva_mine_opts* opts, gva_mine_result** out) {
     gva_mine_result* r = new gva_mine_result();
     int st = run_mine(*db->dev, (cudaStream_t)opts->stream, opts->budget_bytes, opts->max_edges, opts->min_support,
                       opts->batch_limit, opts->profile != 0, opts->reduce, opts->reduce_user, opts->support_mode,
-                      opts->mni_cap, r->pats, r->stats, opts->cancel);
+                      opts->mni_cap, r->pats, r->stats, opts->cancel, opts->sm_percent, opts->host_threads);
     if (st) {
         delete r;
         return st;

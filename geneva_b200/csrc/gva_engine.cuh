@@ -250,7 +250,8 @@ typedef int (*ReduceFn)(uint32_t* supports, uint64_t* embeddings, uint64_t n, vo
 // = min_support, which decides frequency).
 int run_mine(DevDB& db, cudaStream_t s, uint64_t budget, uint32_t max_edges, uint32_t min_support,
              uint32_t batch_limit, bool profile, ReduceFn reduce, void* reduce_user, uint32_t support_mode,
-             uint32_t mni_cap, std::vector<MinedPattern>& out, MineStats& st, const volatile int* cancel = nullptr);
+             uint32_t mni_cap, std::vector<MinedPattern>& out, MineStats& st, const volatile int* cancel = nullptr,
+             uint32_t sm_percent = 0, uint32_t host_threads = 0);
 
 // ---- single-graph MNI support (gva_mni.cu) ----
 constexpr int kMniMaxVertices = 8;
@@ -279,9 +280,11 @@ uint64_t mni_kernel_launches();
 // no device work, may run on another thread) and the device rounds.
 struct MniPrepared;
 std::shared_ptr<MniPrepared> mni_prepare(const DevDB& db, const std::vector<MniPattern>& pats,
-                                         const std::vector<char>& absent);
+                                         const std::vector<char>& absent, unsigned host_threads = 0);
+// sm_percent: the search kernel's persistent grid fills at most this share of the SMs (0 = all)
 int mni_run_prepared(DevDB& db, const MniPrepared& prep, uint32_t cap, bool plain, bool profile, cudaStream_t s,
-                     std::vector<uint32_t>& support, MniStats& st, const volatile int* cancel = nullptr);
+                     std::vector<uint32_t>& support, MniStats& st, const volatile int* cancel = nullptr,
+                     uint32_t sm_percent = 0);
 
 size_t step_scratch_bytes(uint64_t in_rows);
 // run_step with the library's fixed device scratch array (no allocation).

@@ -306,7 +306,8 @@ constexpr uint32_t kBuckets = 256;  // candidate partitions by code hash (fixed:
 
 int run_mine(DevDB& db, cudaStream_t s, uint64_t budget, uint32_t max_edges, uint32_t min_support,
              uint32_t batch_limit, bool profile, ReduceFn reduce, void* reduce_user, uint32_t support_mode,
-             uint32_t mni_cap, std::vector<MinedPattern>& out, MineStats& st, const volatile int* cancel) {
+             uint32_t mni_cap, std::vector<MinedPattern>& out, MineStats& st, const volatile int* cancel,
+             uint32_t sm_percent, uint32_t host_threads) {
     out.clear();
     st = MineStats();
     const bool mni = support_mode == GVA_SUPPORT_MNI;
@@ -325,7 +326,8 @@ int run_mine(DevDB& db, cudaStream_t s, uint64_t budget, uint32_t max_edges, uin
     const std::vector<uint32_t>& labels = db.labels;
     auto t_host0 = std::chrono::steady_clock::now();
     double gpu_ms = 0.0;
-    const unsigned nthreads = std::max(1u, std::min(64u, std::thread::hardware_concurrency()));
+    const unsigned nthreads =
+        std::max(1u, std::min(64u, host_threads ? host_threads : std::thread::hardware_concurrency()));
 
     // plan + lower candidates [b0, b1) on the worker threads; a failure's
     // message (thread-local) is carried back in `msg`
@@ -385,7 +387,7 @@ int run_mine(DevDB& db, cudaStream_t s, uint64_t budget, uint32_t max_edges, uin
                 for (uint32_t e = 0; e < c.ne; ++e)
                     m.el[c.edges[e].u][c.edges[e].v] = m.el[c.edges[e].v][c.edges[e].u] = (uint8_t)c.edges[e].el;
             }
-            return mni_prepare(db, mp, {});
+            return mni_prepare(db, mp, {}, nthreads);
         };
         std::future<std::shared_ptr<MniPrepared>> next =
             nbatch ? std::async(std::launch::async, prepare, (size_t)0) : std::future<std::shared_ptr<MniPrepared>>();
@@ -394,7 +396,7 @@ int run_mine(DevDB& db, cudaStream_t s, uint64_t budget, uint32_t max_edges, uin
             std::shared_ptr<MniPrepared> cur = next.get();
             if (b + 1 < nbatch) next = std::async(std::launch::async, prepare, b + 1);
             MniStats ms;
-            int rc = mni_run_prepared(db, *cur, mni_cap, false, profile, s, bsup, ms, cancel);
+            int rc = mni_run_prepared(db, *cur, mni_cap, false, profile, s, bsup, ms, cancel, sm_percent);
             if (rc) return rc;
             for (size_t i = b0; i < b1; ++i) sup[i] = bsup[i - b0];
             gpu_ms += ms.gpu_ms;

@@ -509,7 +509,7 @@ struct MniPrepared {
 };
 
 std::shared_ptr<MniPrepared> mni_prepare(const DevDB& db, const std::vector<MniPattern>& pats,
-                                         const std::vector<char>& absent) {
+                                         const std::vector<char>& absent, unsigned host_threads) {
     const auto t0 = std::chrono::steady_clock::now();
     auto prep = std::make_shared<MniPrepared>();
     const size_t np = pats.size();
@@ -521,8 +521,8 @@ std::shared_ptr<MniPrepared> mni_prepare(const DevDB& db, const std::vector<MniP
     // tasks: one per automorphism orbit of each pattern whose labels all
     // occur, built on all host threads over contiguous blocks of patterns
     if (np) {
-        const unsigned nth = (unsigned)std::max<size_t>(1, std::min<size_t>({64, std::thread::hardware_concurrency(),
-                                                                             (np + 255) / 256}));
+        const size_t cores = host_threads ? host_threads : std::thread::hardware_concurrency();
+        const unsigned nth = (unsigned)std::max<size_t>(1, std::min<size_t>({64, cores, (np + 255) / 256}));
         std::vector<std::vector<MniTask>> tl(nth);
         std::vector<uint32_t> per_pat(np, 0);
         std::vector<std::thread> pool;
@@ -562,7 +562,7 @@ int run_mni(DevDB& db, const std::vector<MniPattern>& pats, const std::vector<ch
 }
 
 int mni_run_prepared(DevDB& db, const MniPrepared& prep, uint32_t cap, bool plain, bool profile, cudaStream_t s,
-                     std::vector<uint32_t>& support, MniStats& st, const volatile int* cancel) {
+                     std::vector<uint32_t>& support, MniStats& st, const volatile int* cancel, uint32_t sm_percent) {
     const auto t_host0 = std::chrono::steady_clock::now();
     st.host_ms += prep.prep_ms;
     GVA_CUDA_M(cudaSetDevice(db.device));
@@ -696,7 +696,11 @@ int mni_run_prepared(DevDB& db, const MniPrepared& prep, uint32_t cap, bool plai
                 rc = fail(GVA_ERR_CUDA, "MNI round upload failed");
                 break;
             }
-            const uint64_t grid = std::min<uint64_t>((uint64_t)per_sm * sms, (nitems + kMniWarps - 1) / kMniWarps);
+            const uint64_t slots_all = (uint64_t)per_sm * sms;
+            const uint64_t cta_cap = (sm_percent == 0 || sm_percent >= 100)
+                                         ? slots_all
+                                         : std::max<uint64_t>(1, slots_all * sm_percent / 100);
+            const uint64_t grid = std::min<uint64_t>(cta_cap, (nitems + kMniWarps - 1) / kMniWarps);
             cudaEvent_t ev = nullptr;
             const double rows = (double)total;
             mni_expand_kernel<<<(unsigned)std::min<uint64_t>((ns + 255) / 256, 4096), 256, 0, s>>>(d_item0, ns,

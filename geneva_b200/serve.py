@@ -17,6 +17,7 @@ Latency of a request = completion time - arrival time (host wall clock).
 from __future__ import annotations
 
 import ctypes
+import os
 import queue
 import threading
 import time
@@ -65,13 +66,19 @@ class Server:
 
     def __init__(self, db: Database, budget_bytes: int = 150 << 30, support: bool = True,
                  slots: int = 4096, match_stream: Optional[int] = None, mine_stream: Optional[int] = None,
-                 mine_db: Optional[Database] = None):
+                 mine_db: Optional[Database] = None, mine_sm_percent: int = 50,
+                 mine_host_threads: Optional[int] = None):
         """db: the graph database matching requests run against (and mining
         requests, with graph support, when mine_db is None).  mine_db: one
-        data graph that mining requests run against with MNI support."""
+        data graph that mining requests run against with MNI support.
+        Mining runs are long; they get at most mine_sm_percent of the SMs
+        (MNI search kernel) and mine_host_threads host threads (default: half
+        the cores), so that matching rounds keep GPU and host time."""
         self.lib = _declare(library())
         self.db = db
         self.mine_db = mine_db
+        self.mine_sm_percent = mine_sm_percent
+        self.mine_host_threads = mine_host_threads if mine_host_threads is not None else max(1, (os.cpu_count() or 2) // 2)
         self.budget = budget_bytes
         self.support = support and db.num_graphs > 0
         self.mine_stream = mine_stream
@@ -224,10 +231,11 @@ class Server:
             try:
                 if self.mine_db is not None:
                     pats, stats = mine(self.mine_db, r.payload[0], r.payload[1], stream=self.mine_stream,
-                                       support="mni", cancel=self._cancel)
+                                       support="mni", cancel=self._cancel, sm_percent=self.mine_sm_percent,
+                                       host_threads=self.mine_host_threads)
                 else:
                     pats, stats = mine(self.db, r.payload[0], r.payload[1], stream=self.mine_stream,
-                                       cancel=self._cancel)
+                                       cancel=self._cancel, host_threads=self.mine_host_threads)
                 r.result = (pats, stats)
                 r.done = time.perf_counter()
                 with self._lock:

@@ -232,6 +232,9 @@ typedef struct gva_mine_opts {
     uint32_t mni_cap;      /* MNI: supports are min(MNI, mni_cap); 0 = min_support */
     const volatile int* cancel; /* optional: once *cancel != 0 (set by another thread), the run stops at
                                    its next batch or round boundary with GVA_ERR_CANCELLED */
+    uint32_t sm_percent;   /* MNI: the search kernel fills at most this share of the SMs (0 = all),
+                              leaving room for other work on the GPU (a server's matching rounds) */
+    uint32_t host_threads; /* host threads for candidate generation and planning (0 = all cores) */
 } gva_mine_opts;
 
 typedef struct gva_mine_stats {
