@@ -304,6 +304,7 @@ def serve_bench(args, local, torch, gv, workloads):
         emb = sum(r.result[0] for r in done if r.kind == "match")
         pats = sum(r.result[1]["candidates"] for r in done if r.kind == "mine")
         lm = [r.latency for r in done if r.kind == "match"]
+        wait_m = [r.admitted - r.arrival for r in done if r.kind == "match"]  # queued before admission
         ln = [r.latency for r in done if r.kind == "mine"]
         t0 = min(r.arrival for r in reqs) if reqs else t_stop
         points.append({"rate": rate, "requests": len(reqs), "completed": len(done),
@@ -311,6 +312,7 @@ def serve_bench(args, local, torch, gv, workloads):
                        "mine_requests": sum(r.kind == "mine" for r in reqs), "mine_completed": len(ln),
                        "match_p50_ms": 1e3 * percentile(lm, 50) if lm else None,
                        "match_p99_ms": 1e3 * percentile(lm, 99) if lm else None,
+                       "match_admission_wait_p50_ms": 1e3 * percentile(wait_m, 50) if wait_m else None,
                        "mine_p50_ms": 1e3 * percentile(ln, 50) if ln else None,
                        "mine_p99_ms": 1e3 * percentile(ln, 99) if ln else None,
                        "embeddings_per_s": emb / (t_stop - t0), "mined_patterns_per_s": pats / (t_stop - t0),

@@ -917,18 +917,24 @@ int BatchSession::read_support(int q, uint32_t* support, uint64_t* graph_counts_
     // plans ending on the same node share the slot of the node's first plan
     const int slot = plans[first_peer(q)].slot;
     if (support) {
-        std::vector<uint32_t> bits(ctx_words);
-        GVA_CUDA_B(cudaMemcpyAsync(bits.data(), graph_bits_dev() + (size_t)slot * ctx_words, ctx_words * 4,
+        // pinned staging: a pageable read-back would hold this thread inside
+        // the driver until the stream drains
+        uint32_t* bits = (uint32_t*)staging_read.get((size_t)ctx_words * 4);
+        if (!bits) return fail(GVA_ERR_NOMEM, "pinned staging allocation failed");
+        GVA_CUDA_B(cudaMemcpyAsync(bits, graph_bits_dev() + (size_t)slot * ctx_words, ctx_words * 4,
                                    cudaMemcpyDeviceToHost, s));
         GVA_CUDA_B(cudaStreamSynchronize(s));
         uint32_t c = 0;
-        for (uint32_t w : bits) c += (uint32_t)__builtin_popcount(w);
+        for (uint32_t i = 0; i < ctx_words; ++i) c += (uint32_t)__builtin_popcount(bits[i]);
         *support = c;
     }
     if (graph_counts_host && want_graph_counts) {
-        GVA_CUDA_B(cudaMemcpyAsync(graph_counts_host, graph_counts_dev() + (size_t)slot * db.num_graphs,
-                                   (size_t)db.num_graphs * 8, cudaMemcpyDeviceToHost, s));
+        uint64_t* h = (uint64_t*)staging_read.get((size_t)db.num_graphs * 8);
+        if (!h) return fail(GVA_ERR_NOMEM, "pinned staging allocation failed");
+        GVA_CUDA_B(cudaMemcpyAsync(h, graph_counts_dev() + (size_t)slot * db.num_graphs, (size_t)db.num_graphs * 8,
+                                   cudaMemcpyDeviceToHost, s));
         GVA_CUDA_B(cudaStreamSynchronize(s));
+        memcpy(graph_counts_host, h, (size_t)db.num_graphs * 8);
     }
     return GVA_OK;
 }
@@ -1023,10 +1029,15 @@ int finish_batch(DevDB& db, PreparedBatch& pb, uint64_t* counts, uint64_t* graph
             uint32_t* d_pop = nullptr;
             if (cudaMallocAsync((void**)&d_pop, (size_t)nq * 4, s) != cudaSuccess)
                 rc = fail(GVA_ERR_NOMEM, "support counters");
-            std::vector<uint32_t> pop(nq, 0);
+            Staging pop_stage;
+            uint32_t* pop = (uint32_t*)pop_stage.get((size_t)nq * 4);
+            if (!rc && !pop) {
+                cudaFreeAsync(d_pop, s);
+                rc = fail(GVA_ERR_NOMEM, "pinned staging allocation failed");
+            }
             if (!rc) {
                 slot_popcount_kernel<<<nq, 256, 0, s>>>(ses.graph_bits_dev(), ses.words(), (uint32_t)nq, d_pop);
-                cudaMemcpyAsync(pop.data(), d_pop, (size_t)nq * 4, cudaMemcpyDeviceToHost, s);
+                cudaMemcpyAsync(pop, d_pop, (size_t)nq * 4, cudaMemcpyDeviceToHost, s);
                 cudaFreeAsync(d_pop, s);
             }
             if (!rc && graph_counts_host)

@@ -209,6 +209,7 @@ private:
     uint32_t* d_blk = nullptr;  // per-round block -> task
     size_t blk_cap = 0;
     Staging staging_blk;
+    Staging staging_read;  // pinned landing area of per-plan support read-backs
 };
 // run_batch in two halves, so that a caller can build the next batch's
 // session (device set-up and step trie, host work) while the previous one's

@@ -602,8 +602,17 @@ int mni_run_prepared(DevDB& db, const MniPrepared& prep, uint32_t cap, bool plai
     unsigned long long* d_prof = (unsigned long long*)cur;
     cur += al(bytes_prof);
     unsigned long long* d_queue = (unsigned long long*)cur;
-    GVA_CUDA_M(cudaMemcpyAsync(d_tasks, tasks.data(), bytes_tasks, cudaMemcpyHostToDevice, s));
-    GVA_CUDA_M(cudaMemcpyAsync(d_parts, hparts.data(), P * sizeof(PartPtr), cudaMemcpyHostToDevice, s));
+    // every host<->device copy goes through pinned staging: a pageable copy
+    // blocks its thread inside the driver until the stream drains, which
+    // other threads' CUDA calls (a server's matching loop) would wait behind
+    Staging tstage, cstage;
+    char* ht = tstage.get(al(bytes_tasks) + P * sizeof(PartPtr));
+    uint32_t* hcounts = (uint32_t*)cstage.get(bytes_counts);
+    if (!ht || !hcounts) return fail(GVA_ERR_NOMEM, "pinned staging allocation failed");
+    memcpy(ht, tasks.data(), bytes_tasks);
+    memcpy(ht + al(bytes_tasks), hparts.data(), P * sizeof(PartPtr));
+    GVA_CUDA_M(cudaMemcpyAsync(d_tasks, ht, bytes_tasks, cudaMemcpyHostToDevice, s));
+    GVA_CUDA_M(cudaMemcpyAsync(d_parts, ht + al(bytes_tasks), P * sizeof(PartPtr), cudaMemcpyHostToDevice, s));
     GVA_CUDA_M(cudaMemsetAsync(d_counts, 0, bytes_counts, s));
     GVA_CUDA_M(cudaMemsetAsync(d_prof, 0, bytes_prof, s));
 
@@ -715,7 +724,7 @@ int mni_run_prepared(DevDB& db, const MniPrepared& prep, uint32_t cap, bool plai
             g_mni_launches += 2;
             st.rounds++;
             cudaError_t le = cudaGetLastError();
-            if (le == cudaSuccess) le = cudaMemcpyAsync(counts.data(), d_counts, bytes_counts, cudaMemcpyDeviceToHost, s);
+            if (le == cudaSuccess) le = cudaMemcpyAsync(hcounts, d_counts, bytes_counts, cudaMemcpyDeviceToHost, s);
             if (le != cudaSuccess) {
                 rc = fail(GVA_ERR_CUDA, std::string("MNI search launch failed: ") + cudaGetErrorString(le));
                 break;
@@ -727,6 +736,7 @@ int mni_run_prepared(DevDB& db, const MniPrepared& prep, uint32_t cap, bool plai
                 rc = fail(GVA_ERR_CUDA, std::string("MNI search failed: ") + cudaGetErrorString(e));
                 break;
             }
+            memcpy(counts.data(), hcounts, bytes_counts);
             // exhausted tasks fix their pattern's cap; capped ones retire
             w = 0;
             for (const MniSlot& sl : slots) {
