@@ -74,13 +74,22 @@ def parse_args():
     ap.add_argument("--duration", type=float, default=2.0, help="serve workload: seconds of arrivals per rate")
     ap.add_argument("--drain", type=float, default=30.0, help="serve workload: seconds to wait for results per rate")
     ap.add_argument("--queries", type=int, default=4096, help="match workload: patterns per rank per step")
-    ap.add_argument("--max-edges", type=int, default=6)
-    ap.add_argument("--min-support", type=float, default=0.02, help="fraction of graphs")
+    ap.add_argument("--db", default="config2", choices=["config2", "config1"],
+                    help="mine workload: the 20,000-graph database, or the 1,000-graph one (config 1: patterns up "
+                         "to 4 edges, support >= 5%% unless --max-edges / --min-support say otherwise)")
+    ap.add_argument("--max-edges", type=int, default=None)
+    ap.add_argument("--min-support", type=float, default=None, help="fraction of graphs")
     ap.add_argument("--sample", type=int, default=256, help="patterns in the plain-path and CPU samples")
     ap.add_argument("--seed", type=int, default=2)
     ap.add_argument("--mni-max-edges", type=int, default=4, help="mni workload: largest pattern (edges)")
     ap.add_argument("--mni-support", type=int, default=1000, help="mni workload: minimum MNI support")
-    return ap.parse_args()
+    args = ap.parse_args()
+    c1 = args.db == "config1"
+    if args.max_edges is None:
+        args.max_edges = 4 if c1 else 6
+    if args.min_support is None:
+        args.min_support = 0.05 if c1 else 0.02
+    return args
 
 
 # ----------------------------------------------------------------- clocks ----
@@ -458,10 +467,20 @@ def cpu_baseline_mni(db, sample, minsup, budget_s=15.0):
 
 
 # --------------------------------------------------------------- mining arm ----
+MINE1_WORKLOAD = ("config-1 mining: 1000 graphs per rank, |V|~U[10,30], avg degree 3, 4 uniform vertex labels, "
+                  "unlabeled edges, seed 1; all connected patterns of up to {me} edges with support >= {ms:g} of the "
+                  "graphs; every candidate matched, all embeddings enumerated")
+
+
 def mine_bench(args, rank, world, local, dist, torch, gv, workloads, shard):
-    """One step = one complete mining run on this rank's 20,000-graph shard."""
-    G = 20000
-    full = workloads.graph_database(G * world, 20, 60, 4.0, 16, 1.2, 3, seed=args.seed, name="config2")
+    """One step = one complete mining run on this rank's graph shard (20,000
+    graphs of config 2, or 1,000 graphs of config 1)."""
+    if args.db == "config1":
+        G = 1000
+        full = workloads.graph_database(G * world, 10, 30, 3.0, 4, None, 1, seed=1, name="config1")
+    else:
+        G = 20000
+        full = workloads.graph_database(G * world, 20, 60, 4.0, 16, 1.2, 3, seed=args.seed, name="config2")
     db = shard.shard_database(full, rank, world) if world > 1 else full
     minsup = int(np.ceil(args.min_support * G * world))
     gdb = gv.Database.from_edges(db.vlabels, db.src, db.dst, db.elabels, device=local)
@@ -594,8 +613,10 @@ def mine_bench(args, rank, world, local, dist, torch, gv, workloads, shard):
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
         "data": "synthetic (seeded generator of the configuration's shapes)",
         "patterns_per_s": patterns_per_s,
-        "config": {"workload": MINE_WORKLOAD.format(me=args.max_edges, ms=args.min_support), "graphs_per_rank": G,
-                   "min_support_graphs": minsup, "max_edges": args.max_edges, "seed": args.seed,
+        "config": {"workload": (MINE1_WORKLOAD if args.db == "config1" else MINE_WORKLOAD).format(
+                       me=args.max_edges, ms=args.min_support), "graphs_per_rank": G,
+                   "min_support_graphs": minsup, "max_edges": args.max_edges,
+                   "seed": 1 if args.db == "config1" else args.seed,
                    "candidates_per_step": cands // max(args.steps, 1), "frequent_patterns": frequent,
                    "l2": "flushed between steps (512 MiB write)",
                    "parallelism": f"graph database sharded over {world} rank(s); per-level support all-reduce"},
@@ -664,9 +685,10 @@ def main():
         if rank != 0:
             return 0
         if args.workload == "mine":
-            db = workloads.config2(seed=args.seed)
+            c1 = args.db == "config1"
+            db = workloads.config1(seed=1) if c1 else workloads.config2(seed=args.seed)
             queries = workloads.sample_patterns(db, args.sample, 2, 7, seed=1000)
-            wl = MINE_WORKLOAD.format(me=args.max_edges, ms=args.min_support)
+            wl = (MINE1_WORKLOAD if c1 else MINE_WORKLOAD).format(me=args.max_edges, ms=args.min_support)
         else:
             db = workloads.config1(seed=1)
             queries = workloads.config3_queries(db, args.queries, seed=1000)
