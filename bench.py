@@ -249,7 +249,7 @@ def reference_arm(args, db, queries, workload):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * tot_t / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
         "impl": "reference", "patterns_per_s": tot_pats / tot_t,
-        "config": {"workload": workload, "seed": args.seed, "patterns_per_step": wave,
+        "config": {"workload": workload, "seed": db.params.get("seed", args.seed), "patterns_per_step": wave,
                    "database_conversion_s": t_conv},
         "cpu_baseline": {"value": value, "unit": "embeddings/s", "cores": wave, "kind": "reference",
                          "sample": f"{wave} seeded patterns per step sampled from the {db.name} database, one "
