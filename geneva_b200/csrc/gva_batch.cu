@@ -154,7 +154,9 @@ batch_count_kernel(const TaskDesc* __restrict__ nodes, const TaskRef* __restrict
         }
     }
     if (d.mode == MODE_COUNT_GRAPHS || d.mode == MODE_WRITE_AND_GRAPHS) add_graph_count(ctx, d.query, first, c, valid);
-    store_block_sum(c, block_sums);
+    // block total without a barrier: each warp adds its share (sums zeroed before the launch)
+    const uint64_t ws = warp_sum((uint64_t)c);
+    if ((threadIdx.x & 31) == 0 && ws) atomicAdd((unsigned long long*)(block_sums + b), (unsigned long long)ws);
 }
 
 __global__ void task_totals_kernel(const uint64_t* __restrict__ block0, int ntasks, const uint64_t* __restrict__ sums,
@@ -423,12 +425,12 @@ int BatchSession::init() {
         for (uint32_t i = nslots; i > 0; --i) free_slots.push_back((int)i - 1);
     }
     int dev = db.device;
-    static bool smem_set[64] = {};
+    static std::atomic<bool> smem_set[64];  // sessions may start on several threads (server, miner)
     if (dev < 0 || dev >= 64) return fail(GVA_ERR_ARG, "device index out of range");
-    if (!smem_set[dev]) {
+    if (!smem_set[dev].load(std::memory_order_acquire)) {
         GVA_CUDA_B(cudaFuncSetAttribute(batch_write_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                         (int)batch_smem_bytes()));
-        smem_set[dev] = true;
+        smem_set[dev].store(true, std::memory_order_release);
     }
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     return GVA_OK;
@@ -768,6 +770,7 @@ int BatchSession::round() {
     GVA_CUDA_B(cudaMemcpyAsync(d_block0, h_block0, (nt + 1) * 8, cudaMemcpyHostToDevice, s));
     GVA_CUDA_B(cudaMemcpyAsync(d_blk, h_blk, nb * 4, cudaMemcpyHostToDevice, s));
 
+    GVA_CUDA_B(cudaMemsetAsync(d_sums, 0, (nb + 1) * 8, s));
     lap(0);
     cudaEvent_t ev = nullptr;
     if (pf) pf->begin(K_EXT_COUNT, cbytes, s, ev);

@@ -167,15 +167,15 @@ size_t red_smem_bytes(uint32_t k) { return sizeof(uint32_t) * 2 * (size_t)kRowsP
 std::atomic<uint64_t> g_launches{0};
 
 int set_smem_limits() {
-    static bool done[64] = {};
+    static std::atomic<bool> done[64];  // callers may run on several threads
     int dev = 0;
     GVA_CUDA(cudaGetDevice(&dev));
-    if (dev < 64 && done[dev]) return GVA_OK;
+    if (dev < 64 && done[dev].load(std::memory_order_acquire)) return GVA_OK;
     GVA_CUDA(cudaFuncSetAttribute(ext_write_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)ext_smem_bytes(kMaxCols - 1, kMaxCols)));
     GVA_CUDA(cudaFuncSetAttribute(red_write_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)red_smem_bytes(kMaxCols)));
-    if (dev < 64) done[dev] = true;
+    if (dev < 64) done[dev].store(true, std::memory_order_release);
     return GVA_OK;
 }
 
@@ -296,13 +296,13 @@ int host_stage(int device, HostStage*& out) {
 }
 
 int ensure_pool(int device) {
-    static bool done[64] = {};
-    if (device < 64 && done[device]) return GVA_OK;
+    static std::atomic<bool> done[64];
+    if (device < 64 && done[device].load(std::memory_order_acquire)) return GVA_OK;
     cudaMemPool_t pool;
     GVA_CUDA(cudaDeviceGetDefaultMemPool(&pool, device));
     uint64_t keep = UINT64_MAX;  // keep freed frontier memory cached for the next phase / query
     GVA_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
-    if (device < 64) done[device] = true;
+    if (device < 64) done[device].store(true, std::memory_order_release);
     return GVA_OK;
 }
 
