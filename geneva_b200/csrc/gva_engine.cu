@@ -349,6 +349,11 @@ int upload_graph(HostGraph& g, int device, DevDB*& out) {
     GVA_CUDA(cudaGetDeviceCount(&ndev));
     if (device < 0 || device >= ndev) return fail(GVA_ERR_ARG, "device index out of range");
     GVA_CUDA(cudaSetDevice(device));
+    // every engine (per-query, batched, MNI) allocates frontiers and round
+    // buffers from the stream-ordered pool: keep freed memory cached there
+    // instead of returning it to the driver at each synchronisation
+    int prc = ensure_pool(device);
+    if (prc) return prc;
     const uint32_t L = g.num_labels();
     // vertices grouped by dense label: the seed frontiers of init phases
     std::vector<uint32_t> seed_off(L + 1, 0), seed_verts;
