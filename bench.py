@@ -816,7 +816,7 @@ def main():
     t0 = time.perf_counter()
     e2e_rows = 0
     for _ in range(e2e_steps):
-        ps = [gv.Plan.from_text(q) for q in queries]
+        ps = gv.Plan.batch_from_texts(queries)  # planned on the host's cores
         counts, _, _ = gv.batch_count(gdb, ps, stream=sp, graph_counts=True, support=True)
         e2e_rows += int(counts.sum())
         for p in ps:
@@ -854,8 +854,8 @@ def main():
             "batch": {k: pstats[k] for k in ("rounds", "splits", "launches", "trie_nodes")},
             "e2e": {"value": e2e_value, "unit": "embeddings/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h,
-                    "note": "pattern text planned on the host each step; per-(query, graph) counts and supports "
-                            "copied to host"},
+                    "note": "pattern text planned on the host each step (gva_plan_batch); per-(query, graph) counts "
+                            "and supports copied to host"},
             "gpu_launches": launches,
             "clocks": clk,
         }

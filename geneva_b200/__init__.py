@@ -125,6 +125,7 @@ def _declare(lib):
         "gva_db_free": (None, [vp]),
         "gva_plan_from_file": (i32, [cp, i32, P(vp)]),
         "gva_plan_from_text": (i32, [cp, i32, P(vp)]),
+        "gva_plan_batch": (i32, [vp, i32, i32, vp, vp]),
         "gva_plan_describe": (sz, [vp, ctypes.c_char_p, sz]),
         "gva_plan_num_phases": (i32, [vp]),
         "gva_plan_num_vertices": (i32, [vp]),
@@ -260,6 +261,24 @@ class Plan:
         h = ctypes.c_void_p()
         _check(library().gva_plan_from_text(text.encode(), mode, ctypes.byref(h)))
         return cls(h.value)
+
+    @classmethod
+    def batch_from_texts(cls, texts: Sequence[str], mode: int = MODE_DV) -> List["Plan"]:
+        """Plans many queries in one call on the host's cores (gva_plan_batch)."""
+        n = len(texts)
+        enc = (ctypes.c_char_p * max(n, 1))(*[t.encode() for t in texts])
+        out = (ctypes.c_void_p * max(n, 1))()
+        st = (ctypes.c_int * max(n, 1))()
+        rc = library().gva_plan_batch(ctypes.cast(enc, ctypes.c_void_p), n, mode, ctypes.cast(out, ctypes.c_void_p),
+                                      ctypes.cast(st, ctypes.c_void_p))
+        plans = [cls(out[i]) if out[i] else None for i in range(n)]
+        if rc:
+            msg = library().gva_last_error().decode()
+            for p in plans:
+                if p is not None:
+                    p.close()
+            raise GenevaError(rc, msg)
+        return plans
 
     @classmethod
     def from_file(cls, path: str, mode: int = MODE_DV) -> "Plan":

@@ -7,6 +7,9 @@
 #include <cstring>
 #include <fstream>
 #include <sstream>
+#include <string>
+#include <thread>
+#include <vector>
 
 #include "../../include/geneva.h"
 #include "gva_engine.cuh"
@@ -22,6 +25,41 @@ struct gva_db {
     DevDB* dev = nullptr;
     std::string warnings;
 };
+namespace {
+// Runs fn(i) for i in [0, n) on the host's cores (inline below 256 items);
+// returns the first failing status, with that worker's message re-raised on
+// the calling thread.
+template <typename F>
+int parallel_for(int n, F fn) {
+    const unsigned nth = n < 256 ? 1u : std::max(1u, std::min(64u, std::thread::hardware_concurrency()));
+    if (nth == 1) {
+        for (int i = 0; i < n; ++i) {
+            int st = fn(i);
+            if (st) return st;
+        }
+        return GVA_OK;
+    }
+    std::vector<int> rc(nth, GVA_OK);
+    std::vector<std::string> msg(nth);
+    std::vector<std::thread> pool;
+    for (unsigned t = 0; t < nth; ++t)
+        pool.emplace_back([&, t]() {
+            for (int i = (int)t; i < n; i += (int)nth) {
+                int st = fn(i);
+                if (st) {
+                    rc[t] = st;
+                    msg[t] = gva::last_error_cstr();
+                    return;
+                }
+            }
+        });
+    for (auto& th : pool) th.join();
+    for (unsigned t = 0; t < nth; ++t)
+        if (rc[t]) return gva::fail(rc[t], msg[t]);
+    return GVA_OK;
+}
+}  // namespace
+
 struct gva_plan {
     Plan plan;
     // steps are lowered per database (labels differ); cache the last lowering
@@ -174,6 +212,36 @@ int gva_convert_g(const char* g_path, const char* mygraph_path, const char* meta
     return convert_g(g_path, mygraph_path, metadata_path, reorder_path);
 }
 
+int gva_plan_batch(const char* const* query_texts, int n, int mode, gva_plan** out, int* status) {
+    if (n < 0 || (n > 0 && (!query_texts || !out))) return fail(GVA_ERR_ARG, "null argument");
+    for (int i = 0; i < n; ++i) out[i] = nullptr;
+    std::vector<int> st(n, GVA_OK);
+    std::vector<std::string> msg(n);
+    parallel_for(n, [&](int i) {
+        if (!query_texts[i]) {
+            st[i] = GVA_ERR_ARG;
+            msg[i] = "null query text";
+            return GVA_OK;
+        }
+        gva_plan* p = new gva_plan();
+        st[i] = plan_from_text(query_texts[i], mode, p->plan);
+        if (st[i]) {
+            msg[i] = last_error_cstr();
+            delete p;
+        } else {
+            out[i] = p;
+        }
+        return GVA_OK;  // per-query failures are reported in status, not as the call's
+    });
+    int first = -1;
+    for (int i = 0; i < n; ++i) {
+        if (status) status[i] = st[i];
+        if (st[i] && first < 0) first = i;
+    }
+    if (first >= 0) return fail(st[first], "query " + std::to_string(first) + ": " + msg[first]);
+    return GVA_OK;
+}
+
 int gva_plan_from_text(const char* query_text, int mode, gva_plan** out) {
     if (!out || !query_text) return fail(GVA_ERR_ARG, "null argument");
     *out = nullptr;
@@ -313,9 +381,10 @@ int gva_batch_count(gva_db* db, const gva_plan* const* plans, int nplans, const 
     gva_batch_opts o{};
     if (opts) o = *opts;
     std::vector<std::vector<Step>> steps(nplans);
-    for (int i = 0; i < nplans; ++i) {
+    for (int i = 0; i < nplans; ++i)
         if (!plans[i]) return fail(GVA_ERR_ARG, "null plan");
-        int st = lower_plan(plans[i]->plan, db->dev->meta, steps[i], true);
+    {
+        int st = parallel_for(nplans, [&](int i) { return lower_plan(plans[i]->plan, db->dev->meta, steps[i], true); });
         if (st) return st;
     }
     BatchStats bs;

@@ -123,6 +123,12 @@ int gva_convert_g(const char* g_path, const char* mygraph_path, const char* meta
  * restrictions and repeat flags for the same query text.  Host-only. */
 int gva_plan_from_file(const char* query_path, int mode, gva_plan** out);
 int gva_plan_from_text(const char* query_text, int mode, gva_plan** out);
+/* gva_plan_from_text for n queries at once on the host's cores (a batch or a
+ * serving wave planned in one call): out[i] receives query i's plan (NULL on
+ * failure) and status[i] (may be NULL) its status; the call returns the first
+ * failure's status with its message, or GVA_OK.  Same plans as planning the
+ * queries one by one. */
+int gva_plan_batch(const char* const* query_texts, int n, int mode, gva_plan** out, int* status);
 /* Canonical text: "vnum", "phase", "restrict", "repeat", "stat" lines.
  * Returns the needed length (excluding NUL); writes at most cap bytes. */
 size_t gva_plan_describe(const gva_plan* plan, char* buf, size_t cap);

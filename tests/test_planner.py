@@ -69,3 +69,17 @@ def test_bad_mode_rejected(native):
     with pytest.raises(gv.GenevaError) as ei:
         gv.Plan.from_text("v 0 1\nv 1 1\ne 0 1 1\n", 7)
     assert ei.value.status == 5
+
+
+def test_batch_planning_equals_one_by_one(native, golden_plans):
+    """gva_plan_batch (host threads) gives the reference's plans, per query
+    the same as gva_plan_from_text, and reports which query failed."""
+    qs = [g["q"] for g in golden_plans]
+    plans = gv.Plan.batch_from_texts(qs)
+    assert [p.describe() for p in plans] == [g["plan"] for g in golden_plans]
+    sv = gv.Plan.batch_from_texts(qs[:300], gv.MODE_SV)
+    assert [p.describe() for p in sv] == [gv.Plan.from_text(q, gv.MODE_SV).describe() for q in qs[:300]]
+    bad = qs[:400] + ["v 0 1\nv 1 1\nv 2 1\ne 0 1 1\n"] + qs[400:600]  # a disconnected pattern at index 400
+    with pytest.raises(gv.GenevaError) as e:
+        gv.Plan.batch_from_texts(bad)
+    assert "query 400" in str(e.value)
