@@ -14,6 +14,10 @@ independent ways to get a pattern's image sets from that:
   order is one embedding); image sets collected per canonical vertex.
 
 MNI = the smallest image set over the pattern's vertices.
+
+Parity unpinned against the reference: it has no MNI.  The rows-based form
+rests on the oracle's cpumine restatement, which is pinned against the
+reference's own binaries (tests/golden).
 """
 from __future__ import annotations
 
