@@ -85,6 +85,22 @@ uint64_t code_hash(const uint8_t* b, uint32_t len) {
     return h ^ (h >> 29);
 }
 
+// Insertion sort: patterns have at most a few dozen vertices, where it beats
+// std::sort; ties never occur (the comparators are total), so the order is
+// the same.
+template <typename T, typename Less>
+inline void small_sort(T* a, uint32_t n, Less less) {
+    for (uint32_t i = 1; i < n; ++i) {
+        const T x = a[i];
+        uint32_t j = i;
+        while (j > 0 && less(x, a[j - 1])) {
+            a[j] = a[j - 1];
+            --j;
+        }
+        a[j] = x;
+    }
+}
+
 void canonical(const Pattern& p, uint32_t width, CodeBuf& out, uint32_t* order_out = nullptr) {
     const uint32_t n = p.n;
     uint32_t adj[GVA_MAX_QUERY_VERTICES][GVA_MAX_QUERY_VERTICES];
@@ -97,14 +113,14 @@ void canonical(const Pattern& p, uint32_t width, CodeBuf& out, uint32_t* order_o
         uint32_t d = 0;
         for (uint32_t u = 0; u < n; ++u)
             if (adj[v][u]) nb[d++] = ((uint64_t)adj[v][u] << 32) | p.vl[u];
-        std::sort(nb, nb + d);
+        small_sort(nb, d, [](uint64_t a, uint64_t b) { return a < b; });
         uint64_t h = 1469598103934665603ull;
         for (uint32_t i = 0; i < d; ++i) h = (h ^ nb[i]) * 1099511628211ull;
         key[v] = ((uint64_t)(p.vl[v] & 0xffffu) << 48) | ((uint64_t)d << 40) | (h & 0xffffffffffull);
     }
     uint32_t ord[GVA_MAX_QUERY_VERTICES];
     for (uint32_t i = 0; i < n; ++i) ord[i] = i;
-    std::sort(ord, ord + n, [&](uint32_t a, uint32_t b) { return key[a] != key[b] ? key[a] < key[b] : a < b; });
+    small_sort(ord, n, [&](uint32_t a, uint32_t b) { return key[a] != key[b] ? key[a] < key[b] : a < b; });
     uint32_t cb[GVA_MAX_QUERY_VERTICES], ce[GVA_MAX_QUERY_VERTICES], nc = 0;  // cells [cb, ce)
     bool trivial = true;
     for (uint32_t i = 0; i < n;) {

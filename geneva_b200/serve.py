@@ -76,6 +76,7 @@ class Server:
         the cores), so that matching rounds keep GPU and host time."""
         self.lib = _declare(library())
         self.db = db
+        self._max_vertex_id = db.info()["max_vertex_id"]
         self.mine_db = mine_db
         self.mine_sm_percent = mine_sm_percent
         self.mine_host_threads = mine_host_threads if mine_host_threads is not None else max(1, (os.cpu_count() or 2) // 2)
@@ -138,7 +139,7 @@ class Server:
     def _estimate(self, plan: Plan, text: str) -> int:
         """Frontier bytes a request may pin: its widest rows over a seed-sized frontier."""
         k = max(2, text.count("\nv ") + (1 if text.startswith("v ") else 0))
-        return 4 * k * (self.db.info()["max_vertex_id"] // 4 + 1)
+        return 4 * k * (self._max_vertex_id // 4 + 1)
 
     def _admit(self):
         while True:
