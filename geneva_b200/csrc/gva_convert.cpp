@@ -55,13 +55,16 @@ int parse_uints(const std::string& line, uint32_t* out, int want) {
     return n;
 }
 
+// Appends both directions; repeated edges are removed when the lists are
+// sorted after renumbering (the reference skips them on insertion, which
+// gives the same sets: the written lists are sorted either way, and a linear
+// duplicate check per insertion is quadratic in a hub's degree).
 void add_edge(std::vector<Adj>& g, std::map<uint32_t, uint32_t>& vlabel, uint32_t s, uint32_t d, uint32_t el) {
     Adj& part = g[el];
     for (int dir = 0; dir < 2; ++dir) {
         const uint32_t a = dir ? d : s, b = dir ? s : d;
         const uint32_t lb = vlabel[b];  // a vertex without a `v` line has label 0
-        std::vector<uint32_t>& lst = part[a][lb];
-        if (std::find(lst.begin(), lst.end(), b) == lst.end()) lst.push_back(b);
+        part[a][lb].push_back(b);
     }
 }
 
@@ -239,6 +242,7 @@ int convert_g(const std::string& g_path, const std::string& mygraph, const std::
                 std::vector<uint32_t> nv;
                 for (uint32_t u : lv.second) nv.push_back(newid.at(u));
                 std::sort(nv.begin(), nv.end());
+                nv.erase(std::unique(nv.begin(), nv.end()), nv.end());
                 if (nv.size() > 128) add_index_prefix(nv);
                 dst[lv.first] = std::move(nv);
             }

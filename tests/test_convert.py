@@ -64,3 +64,22 @@ def test_converter_cli_and_errors(native, tmp_path):
         gv.convert_g(tmp_path / "empty.g", tmp_path / "empty")
     with pytest.raises(gv.GenevaError):
         gv.convert_g(tmp_path / "missing.g", tmp_path / "missing")
+
+
+def test_converter_repeated_edges_match_reference_binary(native, tmp_path):
+    """Repeated edge lines, in either orientation and around a hub, are
+    dropped as the reference drops them (same bytes out)."""
+    ref = ROOT / "oracle" / "_ref" / "genDatabase"
+    if not ref.exists():
+        pytest.skip("reference converter not built here")
+    spec = SPECS[2]
+    vl, edges = make_graph(spec)
+    dup = list(edges) + [(b, a, l) for (a, b, l) in edges[::7]] + list(edges[::11])
+    (tmp_path / "datasets").mkdir()
+    (tmp_path / "run").mkdir()
+    (tmp_path / "datasets" / "d.g").write_text(write_g(vl, dup))
+    subprocess.run([str(ref), "d"], cwd=tmp_path / "run", check=True, capture_output=True)
+    gv.convert_g(tmp_path / "datasets" / "d.g", tmp_path / "mine")
+    assert filecmp.cmp(tmp_path / "mine.reorder", tmp_path / "run" / "d.reorder", shallow=False)
+    assert filecmp.cmp(tmp_path / "mine.mygraph", tmp_path / "datasets" / "d.mygraph", shallow=False)
+    assert filecmp.cmp(tmp_path / "mine.metadata", tmp_path / "datasets" / "d.metadata", shallow=False)
