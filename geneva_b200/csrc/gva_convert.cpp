@@ -21,6 +21,9 @@
 // the index-vertex prefix (:415-436); partitions are written as in
 // writeHybridDataStructure (:451-580).
 #include <algorithm>
+#include <array>
+#include <thread>
+#include <unordered_map>
 #include <cstdio>
 #include <cstring>
 #include <fstream>
@@ -37,8 +40,6 @@
 namespace gva {
 namespace {
 
-using Adj = std::map<uint32_t, std::map<uint32_t, std::vector<uint32_t>>>;  // svid -> vlabel -> nbrs
-
 // first three unsigned integers of a line (tools/genDatabase.cpp:69-92)
 int parse_uints(const std::string& line, uint32_t* out, int want) {
     int n = 0;
@@ -53,19 +54,6 @@ int parse_uints(const std::string& line, uint32_t* out, int want) {
         }
     }
     return n;
-}
-
-// Appends both directions; repeated edges are removed when the lists are
-// sorted after renumbering (the reference skips them on insertion, which
-// gives the same sets: the written lists are sorted either way, and a linear
-// duplicate check per insertion is quadratic in a hub's degree).
-void add_edge(std::vector<Adj>& g, std::map<uint32_t, uint32_t>& vlabel, uint32_t s, uint32_t d, uint32_t el) {
-    Adj& part = g[el];
-    for (int dir = 0; dir < 2; ++dir) {
-        const uint32_t a = dir ? d : s, b = dir ? s : d;
-        const uint32_t lb = vlabel[b];  // a vertex without a `v` line has label 0
-        part[a][lb].push_back(b);
-    }
 }
 
 // Step 2 of the renumbering for one other partition `cur`.
@@ -85,13 +73,9 @@ void split_by(std::set<uint32_t>& base, const std::set<uint32_t>& cur, std::vect
     for (uint32_t v : common) base.erase(v);
 }
 
-std::map<uint32_t, uint32_t> renumber(const std::vector<Adj>& g) {
+std::map<uint32_t, uint32_t> renumber(const std::vector<std::vector<uint32_t>>& sources) {
     std::vector<std::set<uint32_t>> parts;
-    for (const Adj& p : g) {
-        std::set<uint32_t> s;
-        for (auto& kv : p) s.insert(kv.first);
-        parts.push_back(std::move(s));
-    }
+    for (const std::vector<uint32_t>& src : sources) parts.emplace_back(src.begin(), src.end());
     auto by_size = [](const std::set<uint32_t>& a, const std::set<uint32_t>& b) { return a.size() > b.size(); };
     std::stable_sort(parts.begin(), parts.end(), by_size);
     std::map<uint32_t, uint32_t> newid;  // old -> new
@@ -164,56 +148,90 @@ void add_index_prefix(std::vector<uint32_t>& v) {
     v.insert(v.begin(), idx.begin(), idx.end());
 }
 
-// tools/genDatabase.cpp:451-580 (the hash section is always empty)
-void write_partition(const Adj& part, std::vector<uint32_t>& out) {
-    struct Run { uint32_t s, e; };
-    std::vector<Run> runs;
-    uint64_t nbrs = 0;
-    for (auto it = part.begin(); it != part.end(); ++it) {
-        for (auto& kv : it->second) nbrs += kv.second.size();
-        if (!runs.empty() && it->first == runs.back().e + 1)
-            runs.back().e = it->first;
-        else
-            runs.push_back({it->first, it->first});
+
+// One directed adjacency entry: source, label of the neighbour, neighbour.
+struct Half {
+    uint32_t a, lb, b;
+    bool operator<(const Half& o) const { return a != o.a ? a < o.a : (lb != o.lb ? lb < o.lb : b < o.b); }
+    bool operator==(const Half& o) const { return a == o.a && lb == o.lb && b == o.b; }
+};
+
+// Sorts on the host's cores: chunks sorted in parallel, then merged pairwise.
+void parallel_sort(std::vector<Half>& v) {
+    const size_t n = v.size();
+    const unsigned hw = std::max(1u, std::min(64u, std::thread::hardware_concurrency()));
+    if (n < (1u << 20) || hw == 1) {
+        std::sort(v.begin(), v.end());
+        return;
     }
-    const size_t nint = std::min<size_t>(runs.size(), 256);
-    uint64_t slots = 0;
-    for (size_t i = 0; i < nint; ++i) slots += runs[i].e - runs[i].s + 1;
-    const uint64_t tot = 5 + nint * 2 + 2 + slots + 1 + nbrs;
-    std::vector<uint32_t> w(tot, 0);
-    w[0] = (uint32_t)tot;
-    w[1] = (uint32_t)slots;
-    w[2] = (uint32_t)nint;
-    w[3] = (uint32_t)(nint * 2 + 2 + slots + 1);
-    w[4] = w[3];
-    const uint64_t slot_at = 5 + nint * 2 + 2, nbr_at = slot_at + slots + 1;
-    uint64_t si = slot_at, nb = nbr_at, cum = 0;
-    for (size_t i = 0; i < nint; ++i) {
-        w[5 + i] = runs[i].s;
-        cum += runs[i].e - runs[i].s + 1;
-        w[5 + i + nint + 1] = (uint32_t)cum;
-        for (uint32_t v = runs[i].s; v <= runs[i].e; ++v) {
-            w[si++] = (uint32_t)(nb - nbr_at);
-            for (auto& kv : part.at(v))
-                for (uint32_t u : kv.second) w[nb++] = u;
+    size_t chunks = 1;
+    while (chunks * 2 <= hw) chunks *= 2;
+    std::vector<size_t> cut(chunks + 1);
+    for (size_t c = 0; c <= chunks; ++c) cut[c] = n * c / chunks;
+    std::vector<std::thread> pool;
+    for (size_t c = 0; c < chunks; ++c)
+        pool.emplace_back([&, c]() { std::sort(v.begin() + cut[c], v.begin() + cut[c + 1]); });
+    for (auto& t : pool) t.join();
+    for (size_t width = 1; width < chunks; width *= 2) {
+        pool.clear();
+        for (size_t c = 0; c + width < chunks; c += 2 * width) {
+            const size_t lo = cut[c], mid = cut[c + width], hi = cut[std::min(chunks, c + 2 * width)];
+            pool.emplace_back([&v, lo, mid, hi]() { std::inplace_merge(v.begin() + lo, v.begin() + mid, v.begin() + hi); });
         }
+        for (auto& t : pool) t.join();
     }
-    w[si] = (uint32_t)(nb - nbr_at);
-    out.insert(out.end(), w.begin(), w.end());
+}
+
+// Growing text output with a decimal formatter (the .reorder file is large).
+struct Out {
+    std::string s;
+    void u(uint64_t x) {
+        char b[24];
+        int k = 0;
+        do {
+            b[k++] = (char)('0' + x % 10);
+            x /= 10;
+        } while (x);
+        while (k) s.push_back(b[--k]);
+    }
+    void c(char ch) { s.push_back(ch); }
+};
+
+bool write_file(const std::string& path, const void* data, size_t n) {
+    FILE* f = fopen(path.c_str(), "wb");
+    if (!f) return false;
+    const bool ok = fwrite(data, 1, n, f) == n;
+    return fclose(f) == 0 && ok;
 }
 
 }  // namespace
 
 int convert_g(const std::string& g_path, const std::string& mygraph, const std::string& metadata,
               const std::string& reorder) {
-    std::ifstream in(g_path);
-    if (!in.is_open()) return fail(GVA_ERR_IO, "cannot open " + g_path);
+    std::string text;
+    {
+        FILE* f = fopen(g_path.c_str(), "rb");
+        if (!f) return fail(GVA_ERR_IO, "cannot open " + g_path);
+        char buf[1 << 16];
+        size_t k;
+        while ((k = fread(buf, 1, sizeof buf, f)) > 0) text.append(buf, k);
+        fclose(f);
+    }
     std::map<uint32_t, uint32_t> vlabel;
-    std::string line;
     uint32_t x[3];
+    size_t pos = 0;
+    auto next_line = [&](std::string& line) {
+        if (pos >= text.size()) return false;
+        size_t e = text.find('\n', pos);
+        if (e == std::string::npos) e = text.size();
+        line.assign(text, pos, e - pos);
+        pos = e + 1;
+        return true;
+    };
+    std::string line;
     // vertex section (tools/genDatabase.cpp:769-778): up to the first `e` line
     bool have_edge = false;
-    while (std::getline(in, line)) {
+    while (next_line(line)) {
         if (line.empty() || line[0] == 't') continue;
         if (line[0] == 'v') {
             if (parse_uints(line, x, 2) == 2) vlabel.emplace(x[0], x[1]);
@@ -222,68 +240,181 @@ int convert_g(const std::string& g_path, const std::string& mygraph, const std::
             break;
         }
     }
-    std::vector<Adj> g;
+    std::vector<std::array<uint32_t, 3>> edges;  // (label, src, dst)
+    size_t P = 0;
+    uint32_t max_id = 0;
     while (have_edge) {
         if (!line.empty() && line[0] == 'e') {
             if (parse_uints(line, x, 3) < 3) return fail(GVA_ERR_FORMAT, "malformed edge line: " + line);
-            if (x[2] + 1 > g.size()) g.resize(x[2] + 1);
-            add_edge(g, vlabel, x[0], x[1], x[2]);
+            P = std::max<size_t>(P, (size_t)x[2] + 1);
+            max_id = std::max(max_id, std::max(x[0], x[1]));
+            edges.push_back({x[2], x[0], x[1]});
         }
-        if (!std::getline(in, line)) break;
+        if (!next_line(line)) break;
     }
-    if (g.empty()) return fail(GVA_ERR_FORMAT, "no edges in " + g_path);
-    const std::map<uint32_t, uint32_t> newid = renumber(g);
-    // renumbered partitions: new svid -> label -> sorted new neighbour ids
-    std::vector<Adj> rg(g.size());
-    for (size_t p = 0; p < g.size(); ++p) {
-        for (auto& sv : g[p]) {
-            auto& dst = rg[p][newid.at(sv.first)];
-            for (auto& lv : sv.second) {
-                std::vector<uint32_t> nv;
-                for (uint32_t u : lv.second) nv.push_back(newid.at(u));
-                std::sort(nv.begin(), nv.end());
-                nv.erase(std::unique(nv.begin(), nv.end()), nv.end());
-                if (nv.size() > 128) add_index_prefix(nv);
-                dst[lv.first] = std::move(nv);
+    text.clear();
+    text.shrink_to_fit();
+    if (edges.empty()) return fail(GVA_ERR_FORMAT, "no edges in " + g_path);
+    // neighbour labels: a vertex without a `v` line has label 0
+    const bool dense = max_id < (1u << 28);
+    std::vector<uint32_t> lab_of;
+    if (dense) {
+        lab_of.assign((size_t)max_id + 1, 0);
+        for (auto& kv : vlabel)
+            if (kv.first <= max_id) lab_of[kv.first] = kv.second;
+    }
+    auto label = [&](uint32_t v) -> uint32_t {
+        if (dense) return lab_of[v];
+        auto it = vlabel.find(v);
+        return it == vlabel.end() ? 0u : it->second;
+    };
+    // per edge label both directions, sorted by (source, neighbour label,
+    // neighbour) with repeats removed
+    std::vector<std::vector<Half>> part(P);
+    {
+        std::vector<size_t> cnt(P, 0);
+        for (auto& e : edges) cnt[e[0]] += 2;
+        for (size_t p = 0; p < P; ++p) part[p].reserve(cnt[p]);
+        for (auto& e : edges) {
+            part[e[0]].push_back({e[1], label(e[2]), e[2]});
+            part[e[0]].push_back({e[2], label(e[1]), e[1]});
+        }
+        edges.clear();
+        edges.shrink_to_fit();
+    }
+    std::vector<std::vector<uint32_t>> sources(P);
+    for (size_t p = 0; p < P; ++p) {
+        parallel_sort(part[p]);
+        part[p].erase(std::unique(part[p].begin(), part[p].end()), part[p].end());
+        for (const Half& h : part[p])
+            if (sources[p].empty() || sources[p].back() != h.a) sources[p].push_back(h.a);
+    }
+    const std::map<uint32_t, uint32_t> newid = renumber(sources);
+    std::vector<uint32_t> nid_dense;
+    std::unordered_map<uint32_t, uint32_t> nid_hash;
+    if (dense) {
+        nid_dense.assign((size_t)max_id + 1, 0);
+        for (auto& kv : newid) nid_dense[kv.first] = kv.second;
+    } else {
+        nid_hash.reserve(newid.size() * 2);
+        for (auto& kv : newid) nid_hash.emplace(kv.first, kv.second);
+    }
+    auto nid = [&](uint32_t v) { return dense ? nid_dense[v] : nid_hash.at(v); };
+    // renumbered partitions, sorted by (new source, label, new neighbour)
+    for (size_t p = 0; p < P; ++p) {
+        for (Half& h : part[p]) {
+            h.a = nid(h.a);
+            h.b = nid(h.b);
+        }
+        parallel_sort(part[p]);
+    }
+    // One pass per partition over its (source, label) groups: the written
+    // neighbour list of a group is its sorted ids, with the index-vertex
+    // prefix when longer than 128 (tools/genDatabase.cpp:415-436).
+    Out ro;
+    ro.u(P);
+    ro.c('\n');
+    std::vector<uint32_t> words;
+    words.push_back((uint32_t)(P - 1));  // .mygraph header counts label 0 out (:856-869)
+    std::vector<uint32_t> nv;
+    for (size_t p = 0; p < P; ++p) {
+        const std::vector<Half>& H = part[p];
+        // group boundaries: sources, then (source, label) runs
+        std::vector<size_t> src_at, grp_at;
+        for (size_t i = 0; i < H.size(); ++i) {
+            if (i == 0 || H[i].a != H[i - 1].a) src_at.push_back(i);
+            if (i == 0 || H[i].a != H[i - 1].a || H[i].lb != H[i - 1].lb) grp_at.push_back(i);
+        }
+        src_at.push_back(H.size());
+        grp_at.push_back(H.size());
+        // lists with prefixes, and each source's total written length
+        std::vector<std::vector<uint32_t>> lists(grp_at.size() - 1);
+        for (size_t g = 0; g + 1 < grp_at.size(); ++g) {
+            nv.clear();
+            for (size_t i = grp_at[g]; i < grp_at[g + 1]; ++i) nv.push_back(H[i].b);
+            if (nv.size() > 128) add_index_prefix(nv);
+            lists[g] = nv;
+        }
+        // .reorder (tools/genDatabase.cpp:826-846)
+        ro.u(src_at.size() - 1);
+        ro.c('\n');
+        size_t g = 0;
+        std::vector<uint64_t> src_len(src_at.size() - 1, 0);
+        for (size_t si = 0; si + 1 < src_at.size(); ++si) {
+            size_t ng = 0;
+            for (size_t k = g; k + 1 < grp_at.size() && grp_at[k] < src_at[si + 1]; ++k) ++ng;
+            ro.u(H[src_at[si]].a);
+            ro.c(' ');
+            ro.u(ng);
+            ro.c('\n');
+            for (size_t k = 0; k < ng; ++k, ++g) {
+                ro.u(H[grp_at[g]].lb);
+                ro.c(' ');
+                ro.u(lists[g].size());
+                ro.c('\n');
+                for (uint32_t u : lists[g]) {
+                    ro.u(u);
+                    ro.c(' ');
+                }
+                ro.c('\n');
+                src_len[si] += lists[g].size();
             }
         }
-    }
-    // .reorder (tools/genDatabase.cpp:826-846)
-    {
-        std::ofstream f(reorder);
-        if (!f.is_open()) return fail(GVA_ERR_IO, "cannot write " + reorder);
-        f << rg.size() << "\n";
-        for (const Adj& part : rg) {
-            f << part.size() << "\n";
-            for (auto& sv : part) {
-                f << sv.first << " " << sv.second.size() << "\n";
-                for (auto& lv : sv.second) {
-                    f << lv.first << " " << lv.second.size() << "\n";
-                    for (uint32_t u : lv.second) f << u << " ";
-                    f << "\n";
+        if (H.empty()) continue;
+        // .mygraph partition (tools/genDatabase.cpp:451-580; the hash section is always empty)
+        struct Run { uint32_t s, e; };
+        std::vector<Run> runs;
+        uint64_t nbrs = 0;
+        for (size_t si = 0; si + 1 < src_at.size(); ++si) {
+            const uint32_t v = H[src_at[si]].a;
+            nbrs += src_len[si];
+            if (!runs.empty() && v == runs.back().e + 1)
+                runs.back().e = v;
+            else
+                runs.push_back({v, v});
+        }
+        const size_t nint = std::min<size_t>(runs.size(), 256);
+        uint64_t slots = 0;
+        for (size_t i = 0; i < nint; ++i) slots += runs[i].e - runs[i].s + 1;
+        const uint64_t tot = 5 + nint * 2 + 2 + slots + 1 + nbrs;
+        std::vector<uint32_t> w(tot, 0);
+        w[0] = (uint32_t)tot;
+        w[1] = (uint32_t)slots;
+        w[2] = (uint32_t)nint;
+        w[3] = (uint32_t)(nint * 2 + 2 + slots + 1);
+        w[4] = w[3];
+        const uint64_t slot_at = 5 + nint * 2 + 2, nbr_at = slot_at + slots + 1;
+        uint64_t si_w = slot_at, nb = nbr_at, cum = 0;
+        size_t si = 0, gi = 0;
+        for (size_t i = 0; i < nint; ++i) {
+            w[5 + i] = runs[i].s;
+            cum += runs[i].e - runs[i].s + 1;
+            w[5 + i + nint + 1] = (uint32_t)cum;
+            for (uint32_t v = runs[i].s; v <= runs[i].e; ++v, ++si) {
+                w[si_w++] = (uint32_t)(nb - nbr_at);
+                while (gi + 1 < grp_at.size() && grp_at[gi] < src_at[si + 1]) {
+                    for (uint32_t u : lists[gi]) w[nb++] = u;
+                    ++gi;
                 }
             }
         }
+        w[si_w] = (uint32_t)(nb - nbr_at);
+        words.insert(words.end(), w.begin(), w.end());
     }
-    // .mygraph (tools/genDatabase.cpp:856-869): header counts label 0 out
-    {
-        std::vector<uint32_t> words;
-        words.push_back((uint32_t)(rg.size() - 1));
-        for (const Adj& part : rg)
-            if (!part.empty()) write_partition(part, words);
-        std::ofstream f(mygraph, std::ios::binary);
-        if (!f.is_open()) return fail(GVA_ERR_IO, "cannot write " + mygraph);
-        f.write((const char*)words.data(), (std::streamsize)words.size() * 4);
-    }
+    if (!write_file(reorder, ro.s.data(), ro.s.size())) return fail(GVA_ERR_IO, "cannot write " + reorder);
+    if (!write_file(mygraph, words.data(), words.size() * 4)) return fail(GVA_ERR_IO, "cannot write " + mygraph);
     // .metadata (tools/genDatabase.cpp:873-879): "new label old", by old id
-    {
-        std::ofstream f(metadata);
-        if (!f.is_open()) return fail(GVA_ERR_IO, "cannot write " + metadata);
-        for (auto& kv : newid) {
-            auto it = vlabel.find(kv.first);
-            f << kv.second << " " << (it == vlabel.end() ? 0u : it->second) << " " << kv.first << "\n";
-        }
+    Out md;
+    for (auto& kv : newid) {
+        auto it = vlabel.find(kv.first);
+        md.u(kv.second);
+        md.c(' ');
+        md.u(it == vlabel.end() ? 0u : it->second);
+        md.c(' ');
+        md.u(kv.first);
+        md.c('\n');
     }
+    if (!write_file(metadata, md.s.data(), md.s.size())) return fail(GVA_ERR_IO, "cannot write " + metadata);
     return GVA_OK;
 }
 
