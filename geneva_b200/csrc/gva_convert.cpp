@@ -19,7 +19,10 @@
 //   4. numbered vertices leave every other partition, B is dropped, repeat.
 // Neighbour lists are then renumbered, sorted, and lists longer than 128 get
 // the index-vertex prefix (:415-436); partitions are written as in
-// writeHybridDataStructure (:451-580).
+// writeHybridDataStructure (:451-580).  The adjacency is held as one flat
+// array of (source, neighbour label, neighbour) per edge label, sorted on all
+// host cores (repeated edges removed after sorting), in place of the
+// reference's nested maps; the renumbering keeps ordered sets.
 #include <algorithm>
 #include <array>
 #include <thread>
