@@ -1,6 +1,7 @@
 // Host side of the database: .mygraph/.metadata parsing, edge-list builder,
 // and the lowering of a plan to engine steps.
 #include <algorithm>
+#include <thread>
 #include <cstdio>
 #include <cstring>
 #include <fstream>
@@ -186,31 +187,73 @@ int graph_from_edges(const uint32_t* vlabels, uint32_t max_id, const uint32_t* s
             return fail(GVA_ERR_ARG, "edge endpoint outside 1..max_vertex_id");
         P = std::max(P, elabel[i]);
     }
-    // bucket by label, then by source: (src, dst) both directions
-    std::vector<uint64_t> cnt((uint64_t)P * (max_id + 1) + 1, 0);
-    for (uint64_t i = 0; i < ne; ++i) {
-        cnt[(uint64_t)(elabel[i] - 1) * (max_id + 1) + src[i]]++;
-        cnt[(uint64_t)(elabel[i] - 1) * (max_id + 1) + dst[i]]++;
-    }
+    for (uint64_t i = 0; i < ne; ++i)  // every endpoint is some vertex's neighbour
+        if (g.dlabel[src[i]] == kNone || g.dlabel[dst[i]] == kNone)
+            return fail(GVA_ERR_ARG, "edge endpoint without a vertex label");
+    const uint64_t L = g.num_labels();
+    const uint64_t entries = (uint64_t)(max_id + 1) * L + 1;
+    if (P && entries >= 0xffffffffull) return fail(GVA_ERR_UNSUPPORTED, "vertex count x label count exceeds 2^32");
+    // Per edge label: both directions of every edge bucketed by source
+    // (counting sort), each source's neighbours sorted by (dense label, id)
+    // with repeated edges removed, on the host's cores; then the (vertex,
+    // label) offsets.  Same arrays as sorting all entries at once.
+    const unsigned nth = std::max(1u, std::min(64u, std::thread::hardware_concurrency()));
+    const uint64_t V = (uint64_t)max_id + 1;
+    g.parts.resize(P);
+    std::vector<uint64_t> pos(V + 1), len(V);
     for (uint32_t p = 1; p <= P; ++p) {
-        std::vector<std::vector<uint32_t>> lists(max_id + 1);
-        for (uint32_t v = 0; v <= max_id; ++v) lists[v].reserve(cnt[(uint64_t)(p - 1) * (max_id + 1) + v]);
-        for (uint64_t i = 0; i < ne; ++i) {
-            if (elabel[i] != p) continue;
-            lists[src[i]].push_back(dst[i]);
-            lists[dst[i]].push_back(src[i]);
+        std::fill(pos.begin(), pos.end(), 0);
+        for (uint64_t i = 0; i < ne; ++i)
+            if (elabel[i] == p) pos[src[i] + 1]++, pos[dst[i] + 1]++;
+        for (uint64_t v = 0; v < V; ++v) pos[v + 1] += pos[v];
+        std::vector<uint64_t> keys(pos[V]);  // (dense label << 32) | neighbour
+        {
+            std::vector<uint64_t> cur(pos.begin(), pos.end() - 1);
+            for (uint64_t i = 0; i < ne; ++i) {
+                if (elabel[i] != p) continue;
+                keys[cur[src[i]]++] = ((uint64_t)g.dlabel[dst[i]] << 32) | dst[i];
+                keys[cur[dst[i]]++] = ((uint64_t)g.dlabel[src[i]] << 32) | src[i];
+            }
         }
-        for (auto& l : lists) {
-            std::sort(l.begin(), l.end(), [&](uint32_t a, uint32_t b) {
-                if (g.dlabel[a] != g.dlabel[b]) return g.dlabel[a] < g.dlabel[b];
-                return a < b;
-            });
-            l.erase(std::unique(l.begin(), l.end()), l.end());
-            for (uint32_t u : l)
-                if (g.dlabel[u] == kNone) return fail(GVA_ERR_ARG, "edge endpoint without a vertex label");
+        auto sort_range = [&](uint64_t v0, uint64_t v1) {
+            for (uint64_t v = v0; v < v1; ++v) {
+                uint64_t* a = keys.data() + pos[v];
+                uint64_t* b = keys.data() + pos[v + 1];
+                std::sort(a, b);
+                len[v] = (uint64_t)(std::unique(a, b) - a);
+            }
+        };
+        if (nth == 1 || keys.size() < (1u << 20)) {
+            sort_range(0, V);
+        } else {
+            // vertex ranges of about equal entry counts
+            std::vector<std::thread> pool;
+            uint64_t v0 = 0;
+            for (unsigned t = 0; t < nth; ++t) {
+                const uint64_t target = pos[V] * (t + 1) / nth;
+                uint64_t v1 = t + 1 == nth ? V : (uint64_t)(std::lower_bound(pos.begin(), pos.end(), target) - pos.begin());
+                v1 = std::min(std::max(v1, v0), V);
+                pool.emplace_back(sort_range, v0, v1);
+                v0 = v1;
+            }
+            for (auto& th : pool) th.join();
         }
-        int st = build_partition(g, p, lists);
-        if (st) return st;
+        uint64_t total = 0;
+        for (uint64_t v = 0; v < V; ++v) total += len[v];
+        if (total >= 0xffffffffull) return fail(GVA_ERR_UNSUPPORTED, "partition has 2^32 or more adjacency entries");
+        HostPartition& part = g.parts[p - 1];
+        part.edge_label = p;
+        part.off.assign(entries, 0);  // group (v, l) starts at off[v * L + l]
+        part.adj.resize(total);
+        uint64_t k = 0;
+        for (uint64_t v = 0; v < V; ++v) {
+            const uint64_t* a = keys.data() + pos[v];
+            for (uint64_t j = 0; j < len[v]; ++j) {
+                part.off[v * L + (a[j] >> 32) + 1]++;
+                part.adj[k++] = (uint32_t)a[j];
+            }
+        }
+        for (uint64_t t = 1; t < entries; ++t) part.off[t] += part.off[t - 1];
     }
     if (g.parts.empty()) g.parts.resize(1);
     return GVA_OK;
