@@ -35,290 +35,9 @@
 #include "../../include/geneva.h"
 #include "gva_engine.cuh"
 #include "gva_internal.h"
+#include "gva_grow.h"
 
 namespace gva {
-
-namespace {
-
-constexpr uint32_t kMaxPatEdges = GVA_MAX_QUERY_VERTICES - 1;  // mining keeps max_edges + 1 <= 32 vertices
-constexpr uint32_t kMaxCode = 1 + GVA_MAX_QUERY_VERTICES + GVA_MAX_QUERY_VERTICES * (GVA_MAX_QUERY_VERTICES - 1) / 2;
-
-struct PEdge {
-    uint8_t u, v;  // u < v
-    uint16_t el;   // edge label (partition id)
-    bool operator<(const PEdge& o) const {
-        return u != o.u ? u < o.u : (v != o.v ? v < o.v : el < o.el);
-    }
-};
-
-// A pattern with dense vertex labels (indices into the database's sorted
-// label list) and no heap storage.
-struct Pattern {
-    uint32_t n = 0, ne = 0;
-    uint32_t vl[GVA_MAX_QUERY_VERTICES];
-    PEdge edges[kMaxPatEdges];
-    uint32_t el(uint32_t a, uint32_t b) const {
-        for (uint32_t i = 0; i < ne; ++i)
-            if ((edges[i].u == a && edges[i].v == b) || (edges[i].u == b && edges[i].v == a)) return edges[i].el;
-        return 0;
-    }
-    void add_edge(uint32_t a, uint32_t b, uint32_t l) {
-        edges[ne++] = {(uint8_t)std::min(a, b), (uint8_t)std::max(a, b), (uint16_t)l};
-    }
-};
-
-// Canonical code of a pattern as bytes: the lexicographically smallest
-// (n, vertex labels, upper-triangle edge labels) over vertex orders that sort
-// vertices by an isomorphism-invariant key (label, degree, hash of the sorted
-// (edge label, neighbour label) list); only orders within equal-key cells are
-// tried.  Equal keys of non-equivalent vertices only enlarge a cell, which
-// costs time, not correctness.  Values are written `width` bytes each (1 when
-// labels and edge labels fit a byte).
-struct CodeBuf {
-    uint32_t len = 0;  // bytes
-    uint8_t b[kMaxCode * 4];
-};
-
-uint64_t code_hash(const uint8_t* b, uint32_t len) {
-    uint64_t h = 1469598103934665603ull;
-    for (uint32_t i = 0; i < len; ++i) h = (h ^ b[i]) * 1099511628211ull;
-    return h ^ (h >> 29);
-}
-
-// Insertion sort: patterns have at most a few dozen vertices, where it beats
-// std::sort; ties never occur (the comparators are total), so the order is
-// the same.
-template <typename T, typename Less>
-inline void small_sort(T* a, uint32_t n, Less less) {
-    for (uint32_t i = 1; i < n; ++i) {
-        const T x = a[i];
-        uint32_t j = i;
-        while (j > 0 && less(x, a[j - 1])) {
-            a[j] = a[j - 1];
-            --j;
-        }
-        a[j] = x;
-    }
-}
-
-void canonical(const Pattern& p, uint32_t width, CodeBuf& out, uint32_t* order_out = nullptr) {
-    const uint32_t n = p.n;
-    uint32_t adj[GVA_MAX_QUERY_VERTICES][GVA_MAX_QUERY_VERTICES];
-    for (uint32_t i = 0; i < n; ++i)
-        for (uint32_t j = 0; j < n; ++j) adj[i][j] = 0;
-    for (uint32_t i = 0; i < p.ne; ++i) adj[p.edges[i].u][p.edges[i].v] = adj[p.edges[i].v][p.edges[i].u] = p.edges[i].el;
-    uint64_t key[GVA_MAX_QUERY_VERTICES];
-    for (uint32_t v = 0; v < n; ++v) {
-        uint64_t nb[GVA_MAX_QUERY_VERTICES];
-        uint32_t d = 0;
-        for (uint32_t u = 0; u < n; ++u)
-            if (adj[v][u]) nb[d++] = ((uint64_t)adj[v][u] << 32) | p.vl[u];
-        small_sort(nb, d, [](uint64_t a, uint64_t b) { return a < b; });
-        uint64_t h = 1469598103934665603ull;
-        for (uint32_t i = 0; i < d; ++i) h = (h ^ nb[i]) * 1099511628211ull;
-        key[v] = ((uint64_t)(p.vl[v] & 0xffffu) << 48) | ((uint64_t)d << 40) | (h & 0xffffffffffull);
-    }
-    uint32_t ord[GVA_MAX_QUERY_VERTICES];
-    for (uint32_t i = 0; i < n; ++i) ord[i] = i;
-    small_sort(ord, n, [&](uint32_t a, uint32_t b) { return key[a] != key[b] ? key[a] < key[b] : a < b; });
-    uint32_t cb[GVA_MAX_QUERY_VERTICES], ce[GVA_MAX_QUERY_VERTICES], nc = 0;  // cells [cb, ce)
-    bool trivial = true;
-    for (uint32_t i = 0; i < n;) {
-        uint32_t j = i + 1;
-        while (j < n && key[ord[j]] == key[ord[i]]) ++j;
-        trivial &= (j == i + 1);
-        cb[nc] = i;
-        ce[nc++] = j;
-        i = j;
-    }
-    const uint32_t len = 1 + n + n * (n - 1) / 2;
-    uint32_t best[kMaxCode], cur[kMaxCode];
-    uint32_t best_ord[GVA_MAX_QUERY_VERTICES];
-    bool have = false;
-    for (;;) {
-        // build the code, giving up as soon as it exceeds the best one
-        cur[0] = n;
-        int cmp = have ? 0 : -1;
-        uint32_t k = 1;
-        for (uint32_t i = 0; i < n && cmp <= 0; ++i, ++k) {
-            cur[k] = p.vl[ord[i]];
-            if (cmp == 0 && cur[k] != best[k]) cmp = cur[k] < best[k] ? -1 : 1;
-        }
-        for (uint32_t i = 0; i < n && cmp <= 0; ++i)
-            for (uint32_t j = i + 1; j < n && cmp <= 0; ++j, ++k) {
-                cur[k] = adj[ord[i]][ord[j]];
-                if (cmp == 0 && cur[k] != best[k]) cmp = cur[k] < best[k] ? -1 : 1;
-            }
-        if (cmp < 0) {
-            std::memcpy(best, cur, sizeof(uint32_t) * len);
-            std::memcpy(best_ord, ord, sizeof(uint32_t) * n);
-            have = true;
-        }
-        if (trivial) break;
-        int c = (int)nc - 1;
-        for (; c >= 0; --c)
-            if (std::next_permutation(ord + cb[c], ord + ce[c])) break;
-        if (c < 0) break;
-    }
-    if (order_out) std::memcpy(order_out, best_ord, sizeof(uint32_t) * n);
-    out.len = len * width;
-    if (width == 1) {
-        for (uint32_t i = 0; i < len; ++i) out.b[i] = (uint8_t)best[i];
-    } else {
-        for (uint32_t i = 0; i < len; ++i)
-            for (uint32_t w = 0; w < width; ++w) out.b[i * width + w] = (uint8_t)(best[i] >> (8 * w));
-    }
-}
-
-// Open-addressing set of byte codes; codes are kept in one arena, so
-// inserting and probing allocate nothing per code.
-struct CodeSet {
-    struct Slot {
-        uint64_t hash;
-        uint32_t off, len;  // len 0: empty
-    };
-    std::vector<uint8_t> arena;
-    std::vector<Slot> table;
-    size_t count = 0;
-    CodeSet() : table(1024, Slot{0, 0, 0}) {}
-    const uint8_t* at(uint32_t off) const { return arena.data() + off; }
-    // true when the code was not present; *off_out = its arena offset
-    bool insert(const uint8_t* b, uint32_t len, uint64_t h, uint32_t* off_out = nullptr) {
-        if (2 * (count + 1) > table.size()) grow();
-        const size_t m = table.size() - 1;
-        for (size_t i = h & m;; i = (i + 1) & m) {
-            Slot& s = table[i];
-            if (s.len == 0) {
-                s.hash = h;
-                s.off = (uint32_t)arena.size();
-                s.len = len;
-                arena.insert(arena.end(), b, b + len);
-                ++count;
-                if (off_out) *off_out = s.off;
-                return true;
-            }
-            if (s.hash == h && s.len == len && std::memcmp(arena.data() + s.off, b, len) == 0) {
-                if (off_out) *off_out = s.off;
-                return false;
-            }
-        }
-    }
-    bool contains(const uint8_t* b, uint32_t len, uint64_t h) const {
-        const size_t m = table.size() - 1;
-        for (size_t i = h & m;; i = (i + 1) & m) {
-            const Slot& s = table[i];
-            if (s.len == 0) return false;
-            if (s.hash == h && s.len == len && std::memcmp(arena.data() + s.off, b, len) == 0) return true;
-        }
-    }
-    void grow() {
-        std::vector<Slot> old(table.size() * 2, Slot{0, 0, 0});
-        old.swap(table);
-        const size_t m = table.size() - 1;
-        for (const Slot& s : old) {
-            if (s.len == 0) continue;
-            size_t i = s.hash & m;
-            while (table[i].len) i = (i + 1) & m;
-            table[i] = s;
-        }
-    }
-};
-
-Pattern relabel(const Pattern& p, const uint32_t* ord) {
-    Pattern q;
-    q.n = p.n;
-    uint32_t pos[GVA_MAX_QUERY_VERTICES];
-    for (uint32_t i = 0; i < p.n; ++i) {
-        pos[ord[i]] = i;
-        q.vl[i] = p.vl[ord[i]];
-    }
-    for (uint32_t i = 0; i < p.ne; ++i) q.add_edge(pos[p.edges[i].u], pos[p.edges[i].v], p.edges[i].el);
-    std::sort(q.edges, q.edges + q.ne);
-    return q;
-}
-
-std::string query_text(const Pattern& p, const std::vector<uint32_t>& labels) {
-    std::string o;
-    o.reserve(16 * (p.n + p.ne));
-    for (uint32_t i = 0; i < p.n; ++i)
-        o += "v " + std::to_string(i) + " " + std::to_string(labels[p.vl[i]]) + "\n";
-    for (uint32_t i = 0; i < p.ne; ++i)
-        o += "e " + std::to_string(p.edges[i].u) + " " + std::to_string(p.edges[i].v) + " " +
-             std::to_string(p.edges[i].el) + "\n";
-    return o;
-}
-
-// Connectivity of the edge set minus edge `skip`; reports the vertex left
-// without edges (pendant removal) in `isolated`, or kNone.
-bool connected_without(const Pattern& p, uint32_t skip, uint32_t& isolated) {
-    uint32_t deg[GVA_MAX_QUERY_VERTICES] = {0};
-    for (uint32_t i = 0; i < p.ne; ++i)
-        if (i != skip) deg[p.edges[i].u]++, deg[p.edges[i].v]++;
-    isolated = kNone;
-    uint32_t iso_count = 0, start = kNone;
-    for (uint32_t v = 0; v < p.n; ++v) {
-        if (deg[v] == 0)
-            isolated = v, ++iso_count;
-        else if (start == kNone)
-            start = v;
-    }
-    if (iso_count > 1 || start == kNone) return false;
-    uint32_t seen = 1u << start, frontier = 1u << start;
-    while (frontier) {
-        uint32_t nxt = 0;
-        for (uint32_t i = 0; i < p.ne; ++i) {
-            if (i == skip) continue;
-            const uint32_t a = p.edges[i].u, b = p.edges[i].v;
-            if (frontier >> a & 1) nxt |= 1u << b;
-            if (frontier >> b & 1) nxt |= 1u << a;
-        }
-        frontier = nxt & ~seen;
-        seen |= nxt;
-    }
-    for (uint32_t v = 0; v < p.n; ++v)
-        if (deg[v] && !(seen >> v & 1)) return false;
-    return true;
-}
-
-Pattern remove_edge(const Pattern& p, uint32_t skip, uint32_t isolated) {
-    Pattern q;
-    uint32_t map[GVA_MAX_QUERY_VERTICES];
-    for (uint32_t v = 0; v < p.n; ++v)
-        if (v != isolated) map[v] = q.n, q.vl[q.n++] = p.vl[v];
-    for (uint32_t i = 0; i < p.ne; ++i)
-        if (i != skip) q.add_edge(map[p.edges[i].u], map[p.edges[i].v], p.edges[i].el);
-    return q;
-}
-
-// One generated extension: parent pattern + one edge, with its canonical
-// code (bytes in the generating thread's CodeSet arena).
-struct Ext {
-    uint64_t hash;
-    uint32_t parent;
-    uint32_t code_off;
-    uint16_t code_len;
-    uint8_t thread;
-    uint8_t u, v;  // v == 0xff: forward edge to a new vertex labelled `lab`
-    uint8_t pad;
-    uint16_t el;
-    uint32_t lab;
-};
-
-Pattern apply_ext(const Pattern& p, const Ext& x) {
-    Pattern c = p;
-    if (x.v == 0xff) {
-        c.vl[c.n] = x.lab;
-        c.add_edge(x.u, c.n, x.el);
-        c.n += 1;
-    } else {
-        c.add_edge(x.u, x.v, x.el);
-    }
-    return c;
-}
-
-constexpr uint32_t kBuckets = 256;  // candidate partitions by code hash (fixed: output order is machine-independent)
-
-}  // namespace
 
 int run_mine(DevDB& db, cudaStream_t s, uint64_t budget, uint32_t max_edges, uint32_t min_support,
              uint32_t batch_limit, bool profile, ReduceFn reduce, void* reduce_user, uint32_t support_mode,
@@ -356,9 +75,18 @@ int run_mine(DevDB& db, cudaStream_t s, uint64_t budget, uint32_t max_edges, uin
         std::vector<std::thread> pool;
         for (unsigned t = 0; t < nthreads; ++t)
             pool.emplace_back([&, t]() {
+                uint32_t ql[GVA_MAX_QUERY_VERTICES], sdl[3 * kMaxPatEdges];
                 for (size_t i = b0 + t; i < b1; i += nthreads) {
+                    // the plan of the candidate's query text, built from the pattern
+                    const Pattern& c = cands[i];
+                    for (uint32_t v = 0; v < c.n; ++v) ql[v] = labels[c.vl[v]];
+                    for (uint32_t e = 0; e < c.ne; ++e) {
+                        sdl[3 * e] = c.edges[e].u;
+                        sdl[3 * e + 1] = c.edges[e].v;
+                        sdl[3 * e + 2] = c.edges[e].el;
+                    }
                     Plan plan;
-                    int r = plan_from_text(query_text(cands[i], labels), GVA_MODE_DV, plan);
+                    int r = plan_from_query(c.n, ql, sdl, c.ne, GVA_MODE_DV, plan);
                     if (!r) r = lower_plan(plan, db.meta, steps[i - b0], true);
                     if (r) {
                         rcs[t] = r;
@@ -560,115 +288,17 @@ int run_mine(DevDB& db, cudaStream_t s, uint64_t budget, uint32_t max_edges, uin
     st.levels = 1;
 
     // ---- levels 2..max_edges
+    WedgeTab wedges;
     for (uint32_t k = 1; k < max_edges && !level.empty(); ++k) {
         if (cancel && *cancel) return fail(GVA_ERR_CANCELLED, "cancelled");
-        auto t_gen = std::chrono::steady_clock::now();
-        // (1) each thread extends every nthreads-th pattern by one frequent
-        // edge type, keeps the extensions whose canonical code it has not seen
-        // yet and files them by code hash into kBuckets partitions
-        std::vector<CodeSet> seen(nthreads);
-        std::vector<std::vector<std::vector<Ext>>> exts(nthreads, std::vector<std::vector<Ext>>(kBuckets));
-        std::vector<std::thread> pool;
-        for (unsigned t = 0; t < nthreads; ++t)
-            pool.emplace_back([&, t]() {
-                CodeBuf cb;
-                auto consider = [&](uint32_t parent, const Pattern& c, const Ext& x) {
-                    canonical(c, width, cb);
-                    const uint64_t h = code_hash(cb.b, cb.len);
-                    uint32_t off;
-                    if (!seen[t].insert(cb.b, cb.len, h, &off)) return;
-                    Ext e = x;
-                    e.hash = h;
-                    e.parent = parent;
-                    e.code_off = off;
-                    e.code_len = (uint16_t)cb.len;
-                    e.thread = (uint8_t)t;
-                    exts[t][h % kBuckets].push_back(e);
-                };
-                for (size_t i = t; i < level.size(); i += nthreads) {
-                    const Pattern& p = level[i];
-                    Ext x{};
-                    for (uint32_t u = 0; u < p.n; ++u) {
-                        x.u = (uint8_t)u;
-                        for (uint32_t v = u + 1; v < p.n; ++v) {  // backward edges
-                            if (p.el(u, v)) continue;
-                            x.v = (uint8_t)v;
-                            for (uint32_t el = 1; el <= P; ++el) {
-                                if (!freq(p.vl[u], el, p.vl[v])) continue;
-                                x.el = (uint16_t)el;
-                                consider((uint32_t)i, apply_ext(p, x), x);
-                            }
-                        }
-                        if (p.n + 1 > max_edges + 1 || p.n + 1 > GVA_MAX_QUERY_VERTICES) continue;
-                        x.v = 0xff;
-                        for (uint32_t el = 1; el <= P; ++el) {  // forward edges
-                            x.el = (uint16_t)el;
-                            for (uint32_t l = 0; l < L; ++l) {
-                                if (!freq(p.vl[u], el, l)) continue;
-                                x.lab = l;
-                                consider((uint32_t)i, apply_ext(p, x), x);
-                            }
-                        }
-                    }
-                }
-            });
-        for (auto& th : pool) th.join();
-        // (2) each partition is deduplicated across threads (sorted by code, so
-        // the level's order depends on the codes only), and each distinct
-        // candidate is kept only if every connected k-edge sub-pattern other
-        // than its parent is frequent (anti-monotone support); survivors are
-        // stored in canonical vertex order
-        auto t_merge = std::chrono::steady_clock::now();
-        std::vector<std::vector<Pattern>> buckets(kBuckets);
-        std::vector<uint64_t> pruned(kBuckets, 0);
-        std::atomic<uint32_t> next_bucket{0};
-        pool.clear();
-        for (unsigned t = 0; t < nthreads; ++t)
-            pool.emplace_back([&]() {
-                std::vector<const Ext*> all;
-                CodeBuf sb;
-                for (uint32_t b; (b = next_bucket.fetch_add(1)) < kBuckets;) {
-                    all.clear();
-                    for (unsigned w = 0; w < nthreads; ++w)
-                        for (const Ext& x : exts[w][b]) all.push_back(&x);
-                    auto bytes = [&](const Ext* x) { return seen[x->thread].at(x->code_off); };
-                    auto less = [&](const Ext* a, const Ext* c) {
-                        if (a->hash != c->hash) return a->hash < c->hash;
-                        if (a->code_len != c->code_len) return a->code_len < c->code_len;
-                        return std::memcmp(bytes(a), bytes(c), a->code_len) < 0;
-                    };
-                    std::sort(all.begin(), all.end(), less);
-                    for (size_t i = 0; i < all.size(); ++i) {
-                        if (i > 0 && !less(all[i - 1], all[i])) continue;  // same code as the previous one
-                        const Ext& x = *all[i];
-                        Pattern c = apply_ext(level[x.parent], x);
-                        bool ok = true;
-                        for (uint32_t e = 0; e + 1 < c.ne && ok; ++e) {  // edge c.ne - 1 is the parent's extension
-                            uint32_t iso;
-                            if (!connected_without(c, e, iso)) continue;
-                            canonical(remove_edge(c, e, iso), width, sb);
-                            ok = level_codes.contains(sb.b, sb.len, code_hash(sb.b, sb.len));
-                        }
-                        if (!ok) {
-                            pruned[b]++;
-                            continue;
-                        }
-                        uint32_t ord[GVA_MAX_QUERY_VERTICES];
-                        canonical(c, width, sb, ord);
-                        buckets[b].push_back(relabel(c, ord));
-                    }
-                }
-            });
-        for (auto& th : pool) th.join();
+        GrowStats gt;
         std::vector<Pattern> next;
-        for (uint32_t b = 0; b < kBuckets; ++b) {
-            st.pruned += pruned[b];
-            next.insert(next.end(), buckets[b].begin(), buckets[b].end());
-        }
-        exts.clear();
-        seen.clear();
-        st.merge_ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_merge).count();
-        st.gen_ms += std::chrono::duration<double, std::milli>(t_merge - t_gen).count();
+        if (k == 2 && WedgeTab::fits(L, P)) wedges.build(level, L, P);  // `level` holds the 2-edge patterns
+        grow_level(level, level_codes, freq, L, P, width, max_edges, nthreads, wedges.bits.empty() ? nullptr : &wedges,
+                   next, gt);
+        st.pruned += gt.pruned;
+        st.gen_ms += gt.gen_ms;
+        st.merge_ms += gt.merge_ms;
         auto t_eval = std::chrono::steady_clock::now();
         rc = evaluate(next, sup, emb);
         if (rc) return rc;

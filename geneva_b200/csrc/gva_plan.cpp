@@ -91,7 +91,14 @@ public:
     std::vector<uint32_t> qlabel;
     std::vector<uint32_t> adj;                       // n*n edge label, kNone = no edge
     std::vector<uint32_t> nbr_full;                  // all neighbours (never consumed)
-    std::vector<std::map<uint32_t, LabelGroup>> by_label;
+    // query[v].edgeLabelNeigs as one flat list: vertex v's groups are
+    // groups[group_off[v] .. group_off[v + 1]), ascending edge label
+    struct LabelEntry {
+        uint32_t v, label;
+        LabelGroup g;
+    };
+    std::vector<LabelEntry> groups;
+    std::vector<uint32_t> group_off;
     std::vector<uint32_t> live;                      // neighbours whose edge is not planned yet
     struct QEdge { uint32_t s, e, l; };
     std::vector<QEdge> edges;
@@ -106,7 +113,16 @@ public:
     uint32_t E(uint32_t a, uint32_t b) const { return adj[(size_t)a * n + b]; }
     static uint64_t key(uint32_t el, uint32_t vl) { return ((uint64_t)el << 32) | vl; }
 
+    const LabelGroup& group(uint32_t v, uint32_t label) const {
+        for (uint32_t i = group_off[v]; i < group_off[v + 1]; ++i)
+            if (groups[i].label == label) return groups[i].g;
+        static const LabelGroup none;
+        return none;
+    }
     int parse(const std::string& text);
+    int set_vertices(const std::map<uint32_t, uint32_t>& labels);
+    int set_vertices(uint32_t nv, const uint32_t* labels);  // vertex v labelled labels[v]
+    int set_edges(const uint32_t* sdl, size_t ne);  // (svid, evid, label) triples in query order
     void count_triangle(uint32_t i, TriInfo& t) const;
     void seed_without_triangle(uint32_t& s, uint32_t& e1, uint32_t& e2) const;
     void add_ext(uint32_t s1, uint32_t e1, uint32_t s2, uint32_t e2, int num);
@@ -137,6 +153,22 @@ int Planner::parse(const std::string& text) {
             c.skip_line();
         }
     }
+    int st = set_vertices(labels);
+    if (st) return st;
+    if (!in_edges) return fail(GVA_ERR_FORMAT, "query has no edges");
+    std::vector<uint32_t> sdl;
+    while (c.ok && c.get(ch)) {
+        if (ch != 'e') continue;
+        uint32_t s, d, l;
+        if (!c.read_uint(s) || !c.read_uint(d) || !c.read_uint(l)) break;
+        sdl.push_back(s);
+        sdl.push_back(d);
+        sdl.push_back(l);
+    }
+    return set_edges(sdl.data(), sdl.size() / 3);
+}
+
+int Planner::set_vertices(const std::map<uint32_t, uint32_t>& labels) {
     n = (uint32_t)labels.size();
     if (n == 0) return fail(GVA_ERR_FORMAT, "query has no vertices");
     if (n > GVA_MAX_QUERY_VERTICES) return fail(GVA_ERR_UNSUPPORTED, "query has more than 32 vertices");
@@ -145,23 +177,31 @@ int Planner::parse(const std::string& text) {
         if (kv.first != expect++) return fail(GVA_ERR_FORMAT, "query vertex ids must be 0..n-1");
         qlabel.push_back(kv.second);
     }
+    return GVA_OK;
+}
+
+int Planner::set_vertices(uint32_t nv, const uint32_t* labels) {
+    n = nv;
+    if (n == 0) return fail(GVA_ERR_FORMAT, "query has no vertices");
+    if (n > GVA_MAX_QUERY_VERTICES) return fail(GVA_ERR_UNSUPPORTED, "query has more than 32 vertices");
+    qlabel.assign(labels, labels + n);
+    return GVA_OK;
+}
+
+// Edges in query order; errors at the first offending edge.
+int Planner::set_edges(const uint32_t* sdl, size_t ne) {
     adj.assign((size_t)n * n, kNone);
     nbr_full.assign(n, 0);
-    by_label.assign(n, {});
     live.assign(n, 0);
-    if (!in_edges) return fail(GVA_ERR_FORMAT, "query has no edges");
-    while (c.ok && c.get(ch)) {
-        if (ch != 'e') continue;
-        uint32_t s, d, l;
-        if (!c.read_uint(s) || !c.read_uint(d) || !c.read_uint(l)) break;
+    groups.clear();
+    for (size_t i = 0; i < ne; ++i) {
+        const uint32_t s = sdl[3 * i], d = sdl[3 * i + 1], l = sdl[3 * i + 2];
         if (s >= n || d >= n) return fail(GVA_ERR_FORMAT, "query edge names an undefined vertex");
         if (s == d) return fail(GVA_ERR_UNSUPPORTED, "query self-loop");
         for (int dir = 0; dir < 2; ++dir) {  // addToQueryGraph both ways (:69-85)
             uint32_t a = dir ? d : s, b = dir ? s : d;
             nbr_full[a] |= bit(b);
-            LabelGroup& g = by_label[a][l];
-            g.count += 1;
-            g.mask |= bit(b);
+            groups.push_back({a, l, {1, bit(b)}});
         }
         if (E(s, d) == kNone) {  // first label of a vertex pair wins (:729-737)
             edges.push_back({std::min(s, d), std::max(s, d), l});
@@ -171,6 +211,23 @@ int Planner::parse(const std::string& text) {
         live[s] |= bit(d);
         live[d] |= bit(s);
     }
+    // one group per (vertex, edge label): counts add up, masks join
+    std::sort(groups.begin(), groups.end(), [](const LabelEntry& x, const LabelEntry& y) {
+        return x.v != y.v ? x.v < y.v : x.label < y.label;
+    });
+    size_t k = 0;
+    for (size_t i = 0; i < groups.size(); ++i) {
+        if (k > 0 && groups[k - 1].v == groups[i].v && groups[k - 1].label == groups[i].label) {
+            groups[k - 1].g.count += 1;
+            groups[k - 1].g.mask |= groups[i].g.mask;
+        } else {
+            groups[k++] = groups[i];
+        }
+    }
+    groups.resize(k);
+    group_off.assign(n + 1, 0);
+    for (const LabelEntry& x : groups) group_off[x.v + 1]++;
+    for (uint32_t v = 0; v < n; ++v) group_off[v + 1] += group_off[v];
     if (edges.empty()) return fail(GVA_ERR_FORMAT, "query has no edges");
     // connectivity: the reference loops forever on a disconnected pattern
     uint32_t reach = 1, frontier = 1;
@@ -212,35 +269,73 @@ void Planner::count_triangle(uint32_t i, TriInfo& t) const {
 // src/genMatchOrderCPU.cpp:176-285: a source whose neighbours best share edge
 // and vertex labels, preferring high-degree end vertices.
 void Planner::seed_without_triangle(uint32_t& s_out, uint32_t& e1_out, uint32_t& e2_out) const {
-    std::map<uint64_t, std::vector<uint32_t>> same_el_vl, same_el, same_src;
+    // the reference's three maps (same edge and end label; same edge label;
+    // same source), as (key, members) lists in key order.  Keys are unique
+    // but for same_el_vl keys of edge labels >= 2^20, where the map keeps the
+    // first entry: a stable sort and keeping the first of equal keys does too.
+    struct Entry {
+        uint64_t key;
+        uint32_t at, len;  // members[at .. at + len)
+    };
+    // sized for the worst case: every group's members, at most one entry per
+    // member (repeated edge lines with distinct labels make more groups than
+    // there are edges)
+    size_t cap = 0;
+    for (const LabelEntry& x : groups) cap += (size_t)popc(x.g.mask);
+    thread_local std::vector<uint32_t> members[3];
+    thread_local std::vector<Entry> list[3];
+    for (int i = 0; i < 3; ++i) {
+        if (members[i].size() < cap) members[i].resize(cap);
+        if (list[i].size() < cap + n) list[i].resize(cap + n);
+    }
+    uint32_t used[3] = {0, 0, 0};
+    uint32_t cnt[3] = {0, 0, 0};
+    enum { SAME_EL_VL = 0, SAME_EL = 1, SAME_SRC = 2 };
     for (uint32_t v = 0; v < n; ++v) {
-        for (auto& kv : by_label[v]) {
-            uint64_t k_sv_el = ((uint64_t)kv.first << 20) | v;
-            uint32_t mask = kv.second.mask;
+        const uint32_t src_at = used[SAME_SRC];
+        for (uint32_t gi = group_off[v]; gi < group_off[v + 1]; ++gi) {
+            const uint64_t k_sv_el = ((uint64_t)groups[gi].label << 20) | v;
+            const uint32_t mask = groups[gi].g.mask;
             if (popc(mask) >= 2) {
-                std::map<uint32_t, std::vector<uint32_t>> by_vl;
+                // end vertices by label: ascending label, ascending id within
+                uint32_t ends[32], ne = 0;
                 for (uint32_t u = 0; u < 32; ++u)
-                    if (mask & bit(u)) by_vl[qlabel[u]].push_back(u);
-                for (auto& g : by_vl) {
-                    if (g.second.size() >= 2) {
-                        same_el_vl.emplace(((uint64_t)g.first << 40) | k_sv_el, g.second);
+                    if (mask & bit(u)) ends[ne++] = u;
+                std::stable_sort(ends, ends + ne, [&](uint32_t x, uint32_t y) { return qlabel[x] < qlabel[y]; });
+                const uint32_t el_at = used[SAME_EL];
+                for (uint32_t i = 0; i < ne;) {
+                    uint32_t j = i + 1;
+                    while (j < ne && qlabel[ends[j]] == qlabel[ends[i]]) ++j;
+                    if (j - i >= 2) {
+                        Entry& x = list[SAME_EL_VL][cnt[SAME_EL_VL]++];
+                        x.key = ((uint64_t)qlabel[ends[i]] << 40) | k_sv_el;
+                        x.at = used[SAME_EL_VL];
+                        x.len = j - i;
+                        for (uint32_t t = i; t < j; ++t) members[SAME_EL_VL][used[SAME_EL_VL]++] = ends[t];
                     } else {
-                        auto& dst = same_el[k_sv_el];
-                        dst.insert(dst.end(), g.second.begin(), g.second.end());
+                        members[SAME_EL][used[SAME_EL]++] = ends[i];
                     }
+                    i = j;
                 }
+                if (used[SAME_EL] > el_at) list[SAME_EL][cnt[SAME_EL]++] = {k_sv_el, el_at, used[SAME_EL] - el_at};
             } else {
                 for (uint32_t u = 0; u < 32; ++u)
-                    if (mask & bit(u)) same_src[(uint64_t)v].push_back(u);
+                    if (mask & bit(u)) members[SAME_SRC][used[SAME_SRC]++] = u;
             }
         }
+        if (used[SAME_SRC] > src_at) list[SAME_SRC][cnt[SAME_SRC]++] = {(uint64_t)v, src_at, used[SAME_SRC] - src_at};
     }
-    const bool pairwise = !same_el_vl.empty() || !same_el.empty();
-    const auto& pool = !same_el_vl.empty() ? same_el_vl : (!same_el.empty() ? same_el : same_src);
+    const bool pairwise = cnt[SAME_EL_VL] || cnt[SAME_EL];
+    const int which = cnt[SAME_EL_VL] ? SAME_EL_VL : (cnt[SAME_EL] ? SAME_EL : SAME_SRC);
+    Entry* pool = list[which].data();
+    uint32_t np = cnt[which];
+    std::stable_sort(pool, pool + np, [](const Entry& x, const Entry& y) { return x.key < y.key; });
     uint32_t gs = kNone, g1 = 0, g2 = 0, gv1 = kNone, gv2 = kNone;
-    for (auto& kv : pool) {
+    for (uint32_t pi = 0; pi < np; ++pi) {
+        if (pi > 0 && pool[pi].key == pool[pi - 1].key) continue;  // map::emplace keeps the first
         uint32_t m1 = 0, m2 = 0, v1 = kNone, v2 = kNone;
-        for (uint32_t u : kv.second) {
+        for (uint32_t t = 0; t < pool[pi].len; ++t) {
+            const uint32_t u = members[which][pool[pi].at + t];
             uint32_t deg = (uint32_t)popc(nbr_full[u]);
             if (deg > m1) {
                 m2 = m1; v2 = v1;
@@ -252,11 +347,11 @@ void Planner::seed_without_triangle(uint32_t& s_out, uint32_t& e1_out, uint32_t&
         if (pairwise) {
             if (m1 + m2 > g1 + g2) {
                 g1 = m1; gv1 = v1; g2 = m2; gv2 = v2;
-                gs = (uint32_t)(kv.first & 0xfffffu);
+                gs = (uint32_t)(pool[pi].key & 0xfffffu);
             }
         } else if (m1 > g1) {
             g1 = m1; gv1 = v1;
-            gs = (uint32_t)(kv.first & 0xfffffu);
+            gs = (uint32_t)(pool[pi].key & 0xfffffu);
         }
     }
     s_out = gs;
@@ -323,11 +418,13 @@ void Planner::add_reduce(const std::vector<uint32_t>& pairs) {
 bool Planner::equivalent(uint32_t a, uint32_t b) const {
     if (a == b) return true;
     if (qlabel[a] != qlabel[b]) return false;
-    const auto& ga = by_label[a];
-    const auto& gb = by_label[b];
-    if (ga.size() != gb.size()) return false;
-    for (auto ia = ga.begin(), ib = gb.begin(); ia != ga.end(); ++ia, ++ib)
-        if (ia->first != ib->first || ia->second.count != ib->second.count) return false;
+    const uint32_t na = group_off[a + 1] - group_off[a], nb = group_off[b + 1] - group_off[b];
+    if (na != nb) return false;
+    for (uint32_t i = 0; i < na; ++i) {
+        const LabelEntry& x = groups[group_off[a] + i];
+        const LabelEntry& y = groups[group_off[b] + i];
+        if (x.label != y.label || x.g.count != y.g.count) return false;
+    }
     return true;
 }
 
@@ -481,9 +578,19 @@ int Planner::run(Plan& out) {
     }
 
     // src/genMatchOrderCPU.cpp:823-963: grow one or two vertices at a time
+    // by_el: (edge label, svid, evid) of the edges to unmatched vertices, in
+    // discovery order; stably sorted by label it is the reference's
+    // label -> pairs map walked in key order
+    struct ElPair {
+        uint32_t el, s, u;
+    };
+    std::vector<NeigInfo> infos;
+    std::vector<ElPair> by_el;
+    infos.reserve(64);
+    by_el.reserve(64);
     while (order.size() < n) {
-        std::vector<NeigInfo> infos;
-        std::map<uint32_t, std::vector<uint32_t>> by_el;  // edge label -> (svid, evid) pairs
+        infos.clear();
+        by_el.clear();
         for (uint32_t s : order) {
             const uint32_t nb = live[s];
             for (uint32_t u = 0; u < 32; ++u) {
@@ -494,13 +601,9 @@ int Planner::run(Plan& out) {
                 ni.edgeLabel = E(s, u);
                 ni.commonVNum = (uint32_t)popc(live[u] & visited) - 1u;
                 ni.evLabel = qlabel[u];
-                ni.evNum = (uint32_t)popc(nb & by_label[s].at(ni.edgeLabel).mask);
+                ni.evNum = (uint32_t)popc(nb & group(s, ni.edgeLabel).mask);
                 infos.push_back(ni);
-                if (!(visited & bit(u))) {
-                    auto& v = by_el[ni.edgeLabel];
-                    v.push_back(s);
-                    v.push_back(u);
-                }
+                if (!(visited & bit(u))) by_el.push_back({ni.edgeLabel, s, u});
             }
         }
         if (infos.empty()) return fail(GVA_ERR_UNSUPPORTED, "planner: no edge leaves the matched set");
@@ -537,20 +640,23 @@ int Planner::run(Plan& out) {
         }
         // no back edge: two same-edge-label candidates that are adjacent?
         bool found = false;
-        for (auto& kv : by_el) {
-            const std::vector<uint32_t>& v = kv.second;
-            const size_t cnt = v.size() / 2;
+        std::stable_sort(by_el.begin(), by_el.end(), [](const ElPair& a, const ElPair& b) { return a.el < b.el; });
+        for (size_t g0 = 0; g0 < by_el.size() && !found;) {
+            size_t g1 = g0 + 1;
+            while (g1 < by_el.size() && by_el[g1].el == by_el[g0].el) ++g1;
+            const ElPair* v = by_el.data() + g0;
+            const size_t cnt = g1 - g0;
             for (size_t i = 0; i < cnt && !found; ++i) {
                 for (size_t j = i + 1; j < cnt; ++j) {
-                    if (E(v[2 * i + 1], v[2 * j + 1]) != kNone) {
-                        add_ext(v[2 * i], v[2 * i + 1], v[2 * j], v[2 * j + 1], 2);
-                        add_reduce({v[2 * i + 1], v[2 * j + 1]});
+                    if (E(v[i].u, v[j].u) != kNone) {
+                        add_ext(v[i].s, v[i].u, v[j].s, v[j].u, 2);
+                        add_reduce({v[i].u, v[j].u});
                         found = true;
                         break;
                     }
                 }
             }
-            if (found) break;
+            g0 = g1;
         }
         if (found) continue;
         if (infos[0].evNum > 1) {
@@ -597,16 +703,14 @@ std::string Plan::describe() const {
     return o.str();
 }
 
-int plan_from_text(const std::string& text, int mode, Plan& out) {
-    if (mode != GVA_MODE_DV && mode != GVA_MODE_SV) return fail(GVA_ERR_ARG, "mode must be GVA_MODE_DV or GVA_MODE_SV");
-    Planner p;
-    int st = p.parse(text);
-    if (st) return st;
+namespace {
+
+int finish_plan(Planner& p, int mode, Plan& out) {
     Plan plan;
     plan.mode = mode;
     plan.vnum = p.n;
     plan.qlabel = p.qlabel;
-    st = p.run(plan);
+    int st = p.run(plan);
     if (st) return st;
     // output columns: the first phase's source, then every extended vertex
     plan.columns.push_back(p.phases[0].pairs[0]);
@@ -629,6 +733,25 @@ int plan_from_text(const std::string& text, int mode, Plan& out) {
     }
     out = std::move(plan);
     return GVA_OK;
+}
+
+}  // namespace
+
+int plan_from_text(const std::string& text, int mode, Plan& out) {
+    if (mode != GVA_MODE_DV && mode != GVA_MODE_SV) return fail(GVA_ERR_ARG, "mode must be GVA_MODE_DV or GVA_MODE_SV");
+    Planner p;
+    int st = p.parse(text);
+    if (st) return st;
+    return finish_plan(p, mode, out);
+}
+
+int plan_from_query(uint32_t n, const uint32_t* labels, const uint32_t* sdl, size_t ne, int mode, Plan& out) {
+    if (mode != GVA_MODE_DV && mode != GVA_MODE_SV) return fail(GVA_ERR_ARG, "mode must be GVA_MODE_DV or GVA_MODE_SV");
+    Planner p;
+    int st = p.set_vertices(n, labels);
+    if (!st) st = p.set_edges(sdl, ne);
+    if (st) return st;
+    return finish_plan(p, mode, out);
 }
 
 }  // namespace gva
