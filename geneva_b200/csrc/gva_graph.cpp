@@ -272,12 +272,19 @@ int graph_from_edges(const uint32_t* vlabels, uint32_t max_id, const uint32_t* s
 //                               16 pairs empties the frontier as the reference does (:499-502)
 int lower_plan(const Plan& plan, const HostGraph& g, std::vector<Step>& steps, bool fuse_reductions) {
     steps.clear();
+    steps.reserve(plan.phases.size() + 2);
     int newest = -1;  // query vertex added by the last extension step
     const uint32_t P = (uint32_t)g.parts.size();
-    std::vector<int> col(plan.vnum, -1);
+    if (plan.vnum > (uint32_t)kMaxCols) return fail(GVA_ERR_UNSUPPORTED, "query has more than 32 vertices");
+    int col[kMaxCols];
+    for (uint32_t v = 0; v < plan.vnum; ++v) col[v] = -1;
     int width = 0;
     auto part_of = [&](uint32_t el) -> uint32_t { return (el >= 1 && el <= P && !g.parts[el - 1].off.empty()) ? el : 0; };
-    auto ext = [&](uint32_t el, uint32_t s, uint32_t e, int bound_col, bool incl, const std::vector<int>& eq) {
+    struct EqCols {  // columns of matched vertices with the new vertex's label, ascending
+        uint32_t n = 0;
+        int c[kMaxCols];
+    };
+    auto ext = [&](uint32_t el, uint32_t s, uint32_t e, int bound_col, bool incl, const EqCols& eq) {
         Step st;
         st.kind = STEP_EXT;
         st.width_in = (uint32_t)width;
@@ -286,18 +293,18 @@ int lower_plan(const Plan& plan, const HostGraph& g, std::vector<Step>& steps, b
         st.src_col = col[s];
         st.bound_col = bound_col;
         st.bound_inclusive = incl ? 1 : 0;
-        st.n_eq = (uint32_t)eq.size();
-        for (size_t i = 0; i < eq.size(); ++i) st.eq_cols[i] = (uint8_t)eq[i];
+        st.n_eq = eq.n;
+        for (uint32_t i = 0; i < eq.n; ++i) st.eq_cols[i] = (uint8_t)eq.c[i];
         st.always_empty = (st.part == 0 || st.label == kNone) ? 1 : 0;
         steps.push_back(st);
         col[e] = width++;
         newest = (int)e;
     };
     auto same_label_cols = [&](uint32_t e) {
-        std::vector<int> eq;
+        EqCols eq;
         for (uint32_t v = 0; v < plan.vnum; ++v)
-            if (col[v] >= 0 && plan.qlabel[v] == plan.qlabel[e]) eq.push_back(col[v]);
-        std::sort(eq.begin(), eq.end());
+            if (col[v] >= 0 && plan.qlabel[v] == plan.qlabel[e]) eq.c[eq.n++] = col[v];
+        std::sort(eq.c, eq.c + eq.n);
         return eq;
     };
     for (size_t pi = 0; pi < plan.phases.size(); ++pi) {
@@ -316,12 +323,12 @@ int lower_plan(const Plan& plan, const HostGraph& g, std::vector<Step>& steps, b
             col[s] = width++;
             if (np == 1 || plan.mode == GVA_MODE_SV) {
                 const uint32_t e = ph.pairs[1];
-                ext(ph.edge_label, s, e, plan.restricts[e] == s ? 0 : -1, false, {});
+                ext(ph.edge_label, s, e, plan.restricts[e] == s ? 0 : -1, false, EqCols());
             } else {
                 const uint32_t e1 = ph.pairs[1], e2 = ph.pairs[3];
-                ext(ph.edge_label, s, e1, plan.restricts[e1] != kNone ? 0 : -1, true, {});
-                std::vector<int> eq;
-                if (plan.qlabel[e2] == plan.qlabel[e1]) eq.push_back(col[e1]);
+                ext(ph.edge_label, s, e1, plan.restricts[e1] != kNone ? 0 : -1, true, EqCols());
+                EqCols eq;
+                if (plan.qlabel[e2] == plan.qlabel[e1]) eq.c[eq.n++] = col[e1];
                 if (plan.restricts[e2] == e1)
                     ext(ph.edge_label, s, e2, col[e1], false, eq);
                 else

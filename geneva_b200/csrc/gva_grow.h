@@ -295,6 +295,33 @@ Pattern apply_ext(const Pattern& p, const Ext& x) {
     return c;
 }
 
+// std::sort on `nthreads` threads: sorted chunks merged pairwise.  With a
+// total order (no two elements equivalent) the result is std::sort's.
+template <typename It, typename Less>
+void parallel_sort(It first, It last, Less less, unsigned nthreads) {
+    const size_t n = (size_t)(last - first);
+    if (nthreads <= 1 || n < (1u << 14)) {
+        std::sort(first, last, less);
+        return;
+    }
+    size_t chunks = 1;
+    while (chunks * 2 <= nthreads && chunks < 64) chunks *= 2;
+    std::vector<size_t> cut(chunks + 1);
+    for (size_t c = 0; c <= chunks; ++c) cut[c] = n * c / chunks;
+    std::vector<std::thread> pool;
+    for (size_t c = 0; c < chunks; ++c)
+        pool.emplace_back([&, c]() { std::sort(first + cut[c], first + cut[c + 1], less); });
+    for (auto& t : pool) t.join();
+    for (size_t width = 1; width < chunks; width *= 2) {
+        pool.clear();
+        for (size_t c = 0; c + width < chunks; c += 2 * width) {
+            const size_t lo = cut[c], mid = cut[c + width], hi = cut[std::min(chunks, c + 2 * width)];
+            pool.emplace_back([=]() { std::inplace_merge(first + lo, first + mid, first + hi, less); });
+        }
+        for (auto& t : pool) t.join();
+    }
+}
+
 constexpr uint32_t kBuckets = 256;  // candidate partitions by code hash (fixed: output order is machine-independent)
 
 struct GrowStats {

@@ -186,13 +186,13 @@ int run_mine(DevDB& db, cudaStream_t s, uint64_t budget, uint32_t max_edges, uin
         }
         std::vector<uint32_t> order(n);
         for (size_t i = 0; i < n; ++i) order[i] = (uint32_t)i;
-        std::sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) {
+        parallel_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) {
             const uint64_t* ka = key.data() + (size_t)a * width_k;
             const uint64_t* kb = key.data() + (size_t)b * width_k;
             for (size_t j = 0; j < width_k; ++j)
                 if (ka[j] != kb[j]) return ka[j] < kb[j];
             return a < b;
-        });
+        }, nthreads);
         st.plan_ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_order).count();
         std::vector<uint32_t> bsup;
         std::vector<uint64_t> bemb;

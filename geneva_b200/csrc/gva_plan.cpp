@@ -57,6 +57,38 @@ struct Cursor {
     }
 };
 
+// Stable sort without a heap buffer for the planner's short lists (the
+// order std::stable_sort gives); long lists go to std::stable_sort.
+template <typename T, typename Less>
+void stable_sort_small(T* a, size_t n, Less less) {
+    if (n > 64) {
+        std::stable_sort(a, a + n, less);
+        return;
+    }
+    for (size_t i = 1; i < n; ++i) {
+        T x = a[i];
+        size_t j = i;
+        while (j > 0 && less(x, a[j - 1])) {
+            a[j] = a[j - 1];
+            --j;
+        }
+        a[j] = x;
+    }
+}
+
+// The planner's key -> value maps hold a few keys per query: a vector kept in
+// ascending key order walks like std::map without a node per key.
+template <typename V>
+struct FlatMap {
+    std::vector<std::pair<uint64_t, V>> items;
+    V& operator[](uint64_t k) {
+        auto it = std::lower_bound(items.begin(), items.end(), k,
+                                   [](const std::pair<uint64_t, V>& a, uint64_t b) { return a.first < b; });
+        if (it == items.end() || it->first != k) it = items.insert(it, {k, V()});
+        return it->second;
+    }
+};
+
 struct LabelGroup {  // query[v].edgeLabelNeigs[label] = {count, neighbour mask}
     uint32_t count = 0;
     uint32_t mask = 0;
@@ -106,9 +138,10 @@ public:
     std::vector<uint32_t> order;  // matched query vertices in match order
     uint32_t visited = 0;
     std::vector<Phase> phases;
-    std::map<uint64_t, uint32_t> ext_keys, other_keys;
-    std::map<uint64_t, ReduceKey> red_keys;
-    std::vector<std::vector<uint32_t>> auts;
+    FlatMap<uint32_t> ext_keys, other_keys;
+    FlatMap<ReduceKey> red_keys;
+    std::vector<uint32_t> auts;  // automorphisms, n entries each
+    uint32_t eqmask[32] = {};    // eqmask[a] bit b: equivalent(a, b)
 
     uint32_t E(uint32_t a, uint32_t b) const { return adj[(size_t)a * n + b]; }
     static uint64_t key(uint32_t el, uint32_t vl) { return ((uint64_t)el << 32) | vl; }
@@ -194,6 +227,8 @@ int Planner::set_edges(const uint32_t* sdl, size_t ne) {
     nbr_full.assign(n, 0);
     live.assign(n, 0);
     groups.clear();
+    groups.reserve(2 * ne);
+    edges.reserve(ne);
     for (size_t i = 0; i < ne; ++i) {
         const uint32_t s = sdl[3 * i], d = sdl[3 * i + 1], l = sdl[3 * i + 2];
         if (s >= n || d >= n) return fail(GVA_ERR_FORMAT, "query edge names an undefined vertex");
@@ -212,7 +247,7 @@ int Planner::set_edges(const uint32_t* sdl, size_t ne) {
         live[d] |= bit(s);
     }
     // one group per (vertex, edge label): counts add up, masks join
-    std::sort(groups.begin(), groups.end(), [](const LabelEntry& x, const LabelEntry& y) {
+    stable_sort_small(groups.data(), groups.size(), [](const LabelEntry& x, const LabelEntry& y) {
         return x.v != y.v ? x.v < y.v : x.label < y.label;
     });
     size_t k = 0;
@@ -252,8 +287,8 @@ void Planner::count_triangle(uint32_t i, TriInfo& t) const {
     if (!tri) return;
     int best = -1;
     int best_v = -1;
-    for (uint32_t v = 0; v < 32; ++v) {
-        if (!(tri & bit(v))) continue;
+    for (uint32_t rest = tri; rest; rest &= rest - 1) {
+        const uint32_t v = (uint32_t)__builtin_ctz(rest);
         uint32_t l1 = E(ed.s, v), l2 = E(ed.e, v), l3 = ed.l;
         int score = 10 * ((l1 == l2) + (l1 == l3) + (l2 == l3));
         score += (qlabel[ed.s] == qlabel[ed.e]) + (qlabel[ed.s] == qlabel[v]) + (qlabel[ed.e] == qlabel[v]);
@@ -299,9 +334,8 @@ void Planner::seed_without_triangle(uint32_t& s_out, uint32_t& e1_out, uint32_t&
             if (popc(mask) >= 2) {
                 // end vertices by label: ascending label, ascending id within
                 uint32_t ends[32], ne = 0;
-                for (uint32_t u = 0; u < 32; ++u)
-                    if (mask & bit(u)) ends[ne++] = u;
-                std::stable_sort(ends, ends + ne, [&](uint32_t x, uint32_t y) { return qlabel[x] < qlabel[y]; });
+                for (uint32_t rest = mask; rest; rest &= rest - 1) ends[ne++] = (uint32_t)__builtin_ctz(rest);
+                stable_sort_small(ends, ne, [&](uint32_t x, uint32_t y) { return qlabel[x] < qlabel[y]; });
                 const uint32_t el_at = used[SAME_EL];
                 for (uint32_t i = 0; i < ne;) {
                     uint32_t j = i + 1;
@@ -319,8 +353,8 @@ void Planner::seed_without_triangle(uint32_t& s_out, uint32_t& e1_out, uint32_t&
                 }
                 if (used[SAME_EL] > el_at) list[SAME_EL][cnt[SAME_EL]++] = {k_sv_el, el_at, used[SAME_EL] - el_at};
             } else {
-                for (uint32_t u = 0; u < 32; ++u)
-                    if (mask & bit(u)) members[SAME_SRC][used[SAME_SRC]++] = u;
+                for (uint32_t rest = mask; rest; rest &= rest - 1)
+                    members[SAME_SRC][used[SAME_SRC]++] = (uint32_t)__builtin_ctz(rest);
             }
         }
         if (used[SAME_SRC] > src_at) list[SAME_SRC][cnt[SAME_SRC]++] = {(uint64_t)v, src_at, used[SAME_SRC] - src_at};
@@ -329,7 +363,7 @@ void Planner::seed_without_triangle(uint32_t& s_out, uint32_t& e1_out, uint32_t&
     const int which = cnt[SAME_EL_VL] ? SAME_EL_VL : (cnt[SAME_EL] ? SAME_EL : SAME_SRC);
     Entry* pool = list[which].data();
     uint32_t np = cnt[which];
-    std::stable_sort(pool, pool + np, [](const Entry& x, const Entry& y) { return x.key < y.key; });
+    stable_sort_small(pool, np, [](const Entry& x, const Entry& y) { return x.key < y.key; });
     uint32_t gs = kNone, g1 = 0, g2 = 0, gv1 = kNone, gv2 = kNone;
     for (uint32_t pi = 0; pi < np; ++pi) {
         if (pi > 0 && pool[pi].key == pool[pi - 1].key) continue;  // map::emplace keeps the first
@@ -382,7 +416,7 @@ void Planner::add_ext(uint32_t s1, uint32_t e1, uint32_t s2, uint32_t e2, int nu
         ph.pairs.push_back(e2);
         take(s2, e2);
     }
-    phases.push_back(ph);
+    phases.push_back(std::move(ph));
 }
 
 // src/genMatchOrderCPU.cpp:334-394
@@ -411,7 +445,7 @@ void Planner::add_reduce(const std::vector<uint32_t>& pairs) {
             y.where.push_back({idx, (uint32_t)i});
         }
     }
-    phases.push_back(ph);
+    phases.push_back(std::move(ph));
 }
 
 // src/genMatchOrderCPU.cpp:396-431
@@ -430,7 +464,7 @@ bool Planner::equivalent(uint32_t a, uint32_t b) const {
 
 bool Planner::possible(const std::vector<uint32_t>& cand, uint32_t nid) const {
     uint32_t ori = (uint32_t)cand.size();
-    if (!equivalent(ori, nid)) return false;
+    if (!(eqmask[ori] >> nid & 1)) return false;  // equivalent(ori, nid)
     for (uint32_t i = 0; i < cand.size(); ++i)
         if (E(i, ori) != E(cand[i], nid)) return false;
     return true;
@@ -446,7 +480,7 @@ void Planner::automorphisms(std::vector<uint32_t>& cand, bool identity) {
             if (identity && v == cand.size()) return;
             if (possible(cand, v)) {
                 cand.push_back(v);
-                auts.push_back(cand);
+                auts.insert(auts.end(), cand.begin(), cand.end());
                 cand.pop_back();
             }
             break;
@@ -475,10 +509,9 @@ void Planner::rearrange(Plan& out) {
             std::sort(v.begin(), v.end());
         }
     };
-    while (!red_keys.empty()) {
-        auto it = std::prev(red_keys.end());
-        const uint64_t k = it->first;
-        ReduceKey& rk = it->second;
+    for (size_t ri = red_keys.items.size(); ri-- > 0;) {  // largest key first
+        const uint64_t k = red_keys.items[ri].first;
+        ReduceKey& rk = red_keys.items[ri].second;
         for (size_t i = 0; i < rk.partners.size(); ++i)
             if (rk.count > 0) rk.count -= 1;
         for (auto& w : rk.where) {
@@ -488,10 +521,10 @@ void Planner::rearrange(Plan& out) {
         }
         out.repeat_flag[k] = (rk.count << 16) | rk.count;
         if (rk.count > 1) note_stat(k);
-        red_keys.erase(it);
     }
+    red_keys.items.clear();
     for (auto* m : {&ext_keys, &other_keys}) {
-        for (auto& kv : *m) {
+        for (auto& kv : m->items) {
             auto f = out.repeat_flag.find(kv.first);
             if (f == out.repeat_flag.end()) {
                 out.repeat_flag[kv.first] = (kv.second << 16) | kv.second;
@@ -508,7 +541,8 @@ void Planner::rearrange(Plan& out) {
 // each automorphism that moves v forces aut(v) < v, then only the stabiliser
 // of v is kept.  Per vertex the reference keeps the largest bounding id.
 void Planner::restrictions(Plan& out) const {
-    std::vector<std::vector<uint32_t>> cur = auts;
+    std::vector<uint32_t> cur = auts;  // the stabiliser so far, n entries per automorphism
+    size_t m = n ? cur.size() / n : 0;
     out.restricts.assign(n + 1, kNone);
     uint32_t seen = 0;
     for (const Phase& ph : phases) {
@@ -516,16 +550,18 @@ void Planner::restrictions(Plan& out) const {
         for (uint32_t v : ph.pairs) {
             if (seen & bit(v)) continue;
             seen |= bit(v);
-            std::vector<std::vector<uint32_t>> stab;
-            for (auto& a : cur) {
+            size_t keep = 0;
+            for (size_t i = 0; i < m; ++i) {
+                const uint32_t* a = cur.data() + i * n;
                 if (a[v] == v) {
-                    stab.push_back(a);
+                    if (keep != i) std::copy(a, a + n, cur.begin() + keep * n);
+                    ++keep;
                 } else {
                     uint32_t& r = out.restricts[a[v]];
                     if (r == kNone || r < v) r = v;
                 }
             }
-            cur.swap(stab);
+            m = keep;
         }
     }
 }
@@ -584,17 +620,19 @@ int Planner::run(Plan& out) {
     struct ElPair {
         uint32_t el, s, u;
     };
-    std::vector<NeigInfo> infos;
+    std::vector<NeigInfo> infos, back;
     std::vector<ElPair> by_el;
+    std::vector<uint32_t> red_pairs;
     infos.reserve(64);
     by_el.reserve(64);
+    phases.reserve(2 * n);
     while (order.size() < n) {
         infos.clear();
         by_el.clear();
         for (uint32_t s : order) {
             const uint32_t nb = live[s];
-            for (uint32_t u = 0; u < 32; ++u) {
-                if (!(nb & bit(u))) continue;
+            for (uint32_t rest = nb; rest; rest &= rest - 1) {
+                const uint32_t u = (uint32_t)__builtin_ctz(rest);
                 NeigInfo ni;
                 ni.svid = s;
                 ni.evid = u;
@@ -611,10 +649,10 @@ int Planner::run(Plan& out) {
         if (infos[0].commonVNum > 0) {
             const uint32_t e = infos[0].evid;
             add_ext(infos[0].svid, e, 0, 0, 1);
-            std::vector<NeigInfo> back;
+            back.clear();
             const uint32_t m = live[e] & visited;
-            for (uint32_t u = 0; u < 32; ++u) {
-                if (!(m & bit(u))) continue;
+            for (uint32_t rest = m; rest; rest &= rest - 1) {
+                const uint32_t u = (uint32_t)__builtin_ctz(rest);
                 NeigInfo ni{};
                 ni.svid = e;
                 ni.evid = u;
@@ -626,21 +664,21 @@ int Planner::run(Plan& out) {
                 if (a.edgeLabel != b.edgeLabel) return a.edgeLabel < b.edgeLabel;
                 return a.evLabel < b.evLabel;
             });
-            std::vector<uint32_t> group;
+            red_pairs.clear();
             for (size_t i = 0; i < back.size(); ++i) {
                 if (i > 0 && back[i].edgeLabel != back[i - 1].edgeLabel) {
-                    add_reduce(group);
-                    group.clear();
+                    add_reduce(red_pairs);
+                    red_pairs.clear();
                 }
-                group.push_back(back[i].svid);
-                group.push_back(back[i].evid);
+                red_pairs.push_back(back[i].svid);
+                red_pairs.push_back(back[i].evid);
             }
-            add_reduce(group);
+            add_reduce(red_pairs);
             continue;
         }
         // no back edge: two same-edge-label candidates that are adjacent?
         bool found = false;
-        std::stable_sort(by_el.begin(), by_el.end(), [](const ElPair& a, const ElPair& b) { return a.el < b.el; });
+        stable_sort_small(by_el.data(), by_el.size(), [](const ElPair& a, const ElPair& b) { return a.el < b.el; });
         for (size_t g0 = 0; g0 < by_el.size() && !found;) {
             size_t g1 = g0 + 1;
             while (g1 < by_el.size() && by_el[g1].el == by_el[g0].el) ++g1;
@@ -674,7 +712,13 @@ int Planner::run(Plan& out) {
         if (!paired) add_ext(infos[0].svid, infos[0].evid, 0, 0, 1);
     }
 
+    for (uint32_t a = 0; a < n; ++a) {
+        eqmask[a] = 0;
+        for (uint32_t b = 0; b < n; ++b)
+            if (equivalent(a, b)) eqmask[a] |= bit(b);
+    }
     std::vector<uint32_t> cand;
+    cand.reserve(n);
     automorphisms(cand, true);
     rearrange(out);
     restrictions(out);
