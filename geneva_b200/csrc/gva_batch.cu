@@ -547,7 +547,7 @@ void BatchSession::fill_node_desc(int id, void* out) const {
 }
 
 int BatchSession::submit(const std::vector<std::vector<Step>>& steps, const std::vector<uint64_t>& tags,
-                         std::vector<int>* ids) {
+                         std::vector<int>* ids, bool presorted) {
     const auto t_start = std::chrono::steady_clock::now();
     struct Timer {
         std::chrono::steady_clock::time_point t0;
@@ -555,11 +555,44 @@ int BatchSession::submit(const std::vector<std::vector<Step>>& steps, const std:
         ~Timer() { acc += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count(); }
     } timer{t_start, submit_ms};
     // trie of this wave: (parent, step bytes) -> node, looked up by a 64-bit
-    // hash and confirmed by comparing the bytes
+    // hash and confirmed by comparing the bytes.  A presorted wave (plans in
+    // order of their step keys, so plans that share a prefix are adjacent)
+    // is matched against the previous plan only and keeps no index; a step
+    // that only a non-adjacent plan shares gets a node of its own, which
+    // costs sharing, not correctness.
     std::unordered_multimap<uint64_t, int> index;
-    index.reserve(steps.size() * 4);
+    if (!presorted) index.reserve(steps.size() * 4);
     const int first_node = (int)nodes.size();
     uint8_t kb[512], kb2[512];
+    {  // room for the wave: a plan mostly adds a node or two past its shared prefix
+        size_t total = 0;
+        for (const auto& st : steps) total += st.size();
+        const size_t guess = std::min(total, 2 * steps.size() + 64);
+        nodes.reserve(nodes.size() + guess);
+        node_steps.reserve(node_steps.size() + guess);
+        plans.reserve(plans.size() + steps.size());
+    }
+    // a new node for step `st` at `depth` under `parent` (-1: a root)
+    auto new_node = [&](const Step& st, int parent, int depth) {
+        const int id = (int)nodes.size();
+        BNode nd;
+        nd.kind = st.kind;
+        nd.width_in = st.width_in;
+        nd.n_eq = st.n_eq;
+        nd.n_pairs = st.n_pairs;
+        nd.always_empty = st.always_empty;
+        nd.depth = depth;
+        node_steps.push_back(st);
+        nd.parent = parent;
+        if (parent >= 0) {
+            nd.next_sibling = nodes[parent].first_child;
+            nodes.push_back(nd);
+            nodes[parent].first_child = id;
+        } else {
+            nodes.push_back(nd);
+        }
+        return id;
+    };
     const std::vector<Step>* prev = nullptr;
     std::vector<int> prev_path, path;
     for (size_t qi = 0; qi < steps.size(); ++qi) {
@@ -581,13 +614,21 @@ int BatchSession::submit(const std::vector<std::vector<Step>>& steps, const std:
             // fast path: plans usually arrive ordered by their step sequences, so
             // a step equal to the previous plan's step under the same parent is
             // that plan's node (byte-equal steps have equal keys)
-            if (prev && i < prev_path.size() && i < prev->size() && cur == (i ? prev_path[i - 1] : -1) &&
-                memcmp(&st[i], &(*prev)[i], sizeof(Step)) == 0) {
+            const bool under_prev = prev && i < prev_path.size() && i < prev->size() && cur == (i ? prev_path[i - 1] : -1);
+            if (under_prev && memcmp(&st[i], &(*prev)[i], sizeof(Step)) == 0) {
                 cur = prev_path[i];
                 path[i] = cur;
                 continue;
             }
             const size_t n = step_key_bytes(st[i], kb);
+            if (presorted) {
+                int id = -1;
+                if (under_prev && step_key_bytes((*prev)[i], kb2) == n && memcmp(kb, kb2, n) == 0) id = prev_path[i];
+                if (id < 0) id = new_node(st[i], cur, (int)i);
+                cur = id;
+                path[i] = cur;
+                continue;
+            }
             uint64_t h = 1469598103934665603ull ^ ((uint64_t)(int64_t)cur * 0x9e3779b97f4a7c15ull);
             for (size_t j = 0; j + 8 <= n; j += 8) {
                 uint64_t w;
@@ -603,23 +644,7 @@ int BatchSession::submit(const std::vector<std::vector<Step>>& steps, const std:
                 if (step_key_bytes(node_steps[it->second], kb2) == n && memcmp(kb, kb2, n) == 0) id = it->second;
             }
             if (id < 0) {
-                id = (int)nodes.size();
-                BNode nd;
-                nd.kind = st[i].kind;
-                nd.width_in = st[i].width_in;
-                nd.n_eq = st[i].n_eq;
-                nd.n_pairs = st[i].n_pairs;
-                nd.always_empty = st[i].always_empty;
-                nd.depth = (int)i;
-                node_steps.push_back(st[i]);
-                nd.parent = cur;
-                if (cur >= 0) {
-                    nd.next_sibling = nodes[cur].first_child;
-                    nodes.push_back(nd);
-                    nodes[cur].first_child = id;
-                } else {
-                    nodes.push_back(nd);
-                }
+                id = new_node(st[i], cur, (int)i);
                 index.emplace(h, id);
             }
             cur = id;
@@ -980,7 +1005,7 @@ __global__ void slot_popcount_kernel(const uint32_t* __restrict__ bits, uint32_t
 }
 
 int prepare_batch(DevDB& db, const std::vector<std::vector<Step>>& steps, cudaStream_t s, uint64_t budget,
-                  bool per_graph, bool graph_counts, bool profile, PreparedBatch& out) {
+                  bool per_graph, bool graph_counts, bool profile, PreparedBatch& out, bool presorted) {
     const auto t0 = std::chrono::steady_clock::now();
     GVA_CUDA_B(cudaSetDevice(db.device));
     out.nq = (int)steps.size();
@@ -990,7 +1015,7 @@ int prepare_batch(DevDB& db, const std::vector<std::vector<Step>>& steps, cudaSt
     if (out.nq == 0) return GVA_OK;
     out.ses.reset(new BatchSession(db, s, budget, per_graph ? (uint32_t)out.nq : 0, graph_counts, profile));
     int rc = out.ses->init();
-    if (!rc) rc = out.ses->submit(steps, {}, &out.ids);
+    if (!rc) rc = out.ses->submit(steps, {}, &out.ids, presorted);
     out.prep_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
     return rc;
 }

@@ -146,7 +146,10 @@ public:
     BatchSession(DevDB& db, cudaStream_t s, uint64_t budget, uint32_t slots, bool graph_counts, bool profile);
     ~BatchSession();
     int init();
-    int submit(const std::vector<std::vector<Step>>& steps, const std::vector<uint64_t>& tags, std::vector<int>* ids);
+    // presorted: the plans come in order of their step keys (plans sharing a
+    // prefix are adjacent); the trie is then built without a hash index
+    int submit(const std::vector<std::vector<Step>>& steps, const std::vector<uint64_t>& tags, std::vector<int>* ids,
+               bool presorted = false);
     int round();
     bool idle() const { return active.empty(); }
     std::vector<int> take_completed();
@@ -222,7 +225,7 @@ struct PreparedBatch {
     double prep_ms = 0.0;
 };
 int prepare_batch(DevDB& db, const std::vector<std::vector<Step>>& steps, cudaStream_t s, uint64_t budget,
-                  bool per_graph, bool graph_counts, bool profile, PreparedBatch& out);
+                  bool per_graph, bool graph_counts, bool profile, PreparedBatch& out, bool presorted = false);
 int finish_batch(DevDB& db, PreparedBatch& pb, uint64_t* counts, uint64_t* graph_counts_host, uint32_t* support_host,
                  BatchStats* stats, const volatile int* cancel = nullptr);
 int set_graph_ids(DevDB& db, const uint64_t* first, uint32_t num_graphs);
