@@ -160,6 +160,8 @@ public:
     int read_support(int q, uint32_t* support, uint64_t* graph_counts_host);
     void release(int q);
     size_t num_nodes() const { return nodes.size(); }
+    const BNode& node(int id) const { return nodes[id]; }           // trie introspection (host only)
+    const Step& node_step(int id) const { return node_steps[id]; }
     cudaStream_t stream() const { return s; }
     size_t num_active() const { return active.size(); }
     uint32_t words() const { return ctx_words; }
