@@ -248,7 +248,9 @@ typedef struct gva_mine_stats {
     uint64_t frequent;
     uint64_t embeddings; /* embeddings enumerated over all candidates */
     uint64_t levels;
-    uint64_t pruned;     /* candidates dropped by an infrequent sub-pattern */
+    uint64_t pruned;     /* extensions dropped by an infrequent sub-pattern (most are
+                            dropped before deduplication and count once per parent
+                            that generates them) */
     double gpu_ms;       /* batched matching (CUDA events) */
     double host_ms;      /* whole call, wall clock */
     double gen_ms;       /* candidate generation, dedupe and pruning (host threads) */
