@@ -303,14 +303,37 @@ int run_mine(DevDB& db, cudaStream_t s, uint64_t budget, uint32_t max_edges, uin
         rc = evaluate(next, sup, emb);
         if (rc) return rc;
         st.eval_ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_eval).count();
+        // the frequent ones: codes and query texts on the worker threads,
+        // then filed in candidate order
+        std::vector<uint32_t> fi;
+        for (size_t i = 0; i < next.size(); ++i)
+            if (sup[i] >= min_support) fi.push_back((uint32_t)i);
+        std::vector<std::string> texts(fi.size());
+        std::vector<std::vector<uint8_t>> code_arena(nthreads);
+        std::vector<uint32_t> code_at(fi.size()), code_len(fi.size());
+        std::vector<uint8_t> code_thread(fi.size());
+        std::vector<std::thread> pool;
+        for (unsigned t = 0; t < nthreads; ++t)
+            pool.emplace_back([&, t]() {
+                CodeBuf cb;
+                for (size_t j = t; j < fi.size(); j += nthreads) {
+                    canonical(next[fi[j]], width, cb);
+                    code_at[j] = (uint32_t)code_arena[t].size();
+                    code_len[j] = cb.len;
+                    code_thread[j] = (uint8_t)t;
+                    code_arena[t].insert(code_arena[t].end(), cb.b, cb.b + cb.len);
+                    texts[j] = query_text(next[fi[j]], labels);
+                }
+            });
+        for (auto& th : pool) th.join();
         level.clear();
         level_codes = CodeSet();
-        for (size_t i = 0; i < next.size(); ++i) {
-            if (sup[i] < min_support) continue;
+        for (size_t j = 0; j < fi.size(); ++j) {
+            const uint32_t i = fi[j];
             level.push_back(next[i]);
-            canonical(next[i], width, cbuf);
-            level_codes.insert(cbuf.b, cbuf.len, code_hash(cbuf.b, cbuf.len));
-            out.push_back({query_text(next[i], labels), k + 1, sup[i], emb[i]});
+            const uint8_t* code = code_arena[code_thread[j]].data() + code_at[j];
+            level_codes.insert(code, code_len[j], code_hash(code, code_len[j]));
+            out.push_back({std::move(texts[j]), k + 1, sup[i], emb[i]});
         }
         st.levels = k + 1;
     }
