@@ -232,13 +232,6 @@ int finish_batch(DevDB& db, PreparedBatch& pb, uint64_t* counts, uint64_t* graph
                  BatchStats* stats, const volatile int* cancel = nullptr);
 int set_graph_ids(DevDB& db, const uint64_t* first, uint32_t num_graphs);
 
-struct MinedPattern {
-    std::string text;  // query text, vertices in canonical order
-    uint32_t edges;
-    uint32_t support;
-    uint64_t embeddings;
-};
-
 struct MineStats {
     uint64_t candidates = 0, frequent = 0, embeddings = 0, levels = 0, pruned = 0;
     uint64_t mni_tasks = 0, mni_rounds = 0, mni_found = 0;  // MNI mode

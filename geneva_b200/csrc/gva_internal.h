@@ -108,4 +108,12 @@ struct Step {
 // counts of the folded phases are then not observable).
 int lower_plan(const Plan& plan, const HostGraph& g, std::vector<Step>& steps, bool fuse_reductions = false);
 
+// ---------------------------------------------------------------- mining ---
+struct MinedPattern {
+    std::string text;  // query text, vertices in canonical order
+    uint32_t edges;
+    uint32_t support;
+    uint64_t embeddings;
+};
+
 }  // namespace gva

@@ -248,95 +248,18 @@ int run_mine(DevDB& db, cudaStream_t s, uint64_t budget, uint32_t max_edges, uin
         return GVA_OK;
     };
 
-    // ---- level 1: every edge type
-    const uint32_t L = (uint32_t)labels.size();
-    const uint32_t width = (L <= 256 && P <= 255) ? 1 : (L <= 65536 ? 2 : 4);
-    std::vector<Pattern> cands;
-    for (uint32_t a = 0; a < L; ++a)
-        for (uint32_t b = a; b < L; ++b)
-            for (uint32_t el = 1; el <= P; ++el) {
-                if (!db.parts[el - 1].off) continue;
-                Pattern p;
-                p.n = 2;
-                p.vl[0] = a;
-                p.vl[1] = b;
-                p.add_edge(0, 1, el);
-                cands.push_back(p);
-            }
-    std::vector<uint32_t> sup;
-    std::vector<uint64_t> emb;
-    int rc = evaluate(cands, sup, emb);
+    std::vector<char> has_part(P + 1, 0);
+    for (uint32_t el = 1; el <= P; ++el) has_part[el] = db.parts[el - 1].off != nullptr;
+    LevelStats ls;
+    int rc = mine_levels((uint32_t)labels.size(), P, has_part, labels, max_edges, min_support, nthreads, cancel,
+                         evaluate, out, ls);
+    st.pruned = ls.pruned;
+    st.gen_ms = ls.gen_ms;
+    st.merge_ms = ls.merge_ms;
+    st.eval_ms = ls.eval_ms;
+    st.levels = ls.levels;
+    if (rc == GVA_ERR_CANCELLED) return fail(rc, "cancelled");
     if (rc) return rc;
-    std::vector<char> freq_tab((size_t)L * L * (P + 1), 0);  // frequent edge types (a, b, el), both orientations
-    auto freq = [&](uint32_t a, uint32_t el, uint32_t b) { return freq_tab[((size_t)a * L + b) * (P + 1) + el] != 0; };
-    std::vector<Pattern> level;
-    CodeSet level_codes;
-    CodeBuf cbuf;
-    for (size_t i = 0; i < cands.size(); ++i) {
-        if (sup[i] < min_support) continue;
-        const Pattern& p = cands[i];
-        const uint32_t el = p.edges[0].el;
-        freq_tab[((size_t)p.vl[0] * L + p.vl[1]) * (P + 1) + el] = 1;
-        freq_tab[((size_t)p.vl[1] * L + p.vl[0]) * (P + 1) + el] = 1;
-        uint32_t ord[GVA_MAX_QUERY_VERTICES];
-        canonical(p, width, cbuf, ord);
-        Pattern q = relabel(p, ord);
-        level.push_back(q);
-        level_codes.insert(cbuf.b, cbuf.len, code_hash(cbuf.b, cbuf.len));
-        out.push_back({query_text(q, labels), 1, sup[i], emb[i]});
-    }
-    st.levels = 1;
-
-    // ---- levels 2..max_edges
-    WedgeTab wedges;
-    for (uint32_t k = 1; k < max_edges && !level.empty(); ++k) {
-        if (cancel && *cancel) return fail(GVA_ERR_CANCELLED, "cancelled");
-        GrowStats gt;
-        std::vector<Pattern> next;
-        if (k == 2 && WedgeTab::fits(L, P)) wedges.build(level, L, P);  // `level` holds the 2-edge patterns
-        grow_level(level, level_codes, freq, L, P, width, max_edges, nthreads, wedges.bits.empty() ? nullptr : &wedges,
-                   next, gt);
-        st.pruned += gt.pruned;
-        st.gen_ms += gt.gen_ms;
-        st.merge_ms += gt.merge_ms;
-        auto t_eval = std::chrono::steady_clock::now();
-        rc = evaluate(next, sup, emb);
-        if (rc) return rc;
-        st.eval_ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_eval).count();
-        // the frequent ones: codes and query texts on the worker threads,
-        // then filed in candidate order
-        std::vector<uint32_t> fi;
-        for (size_t i = 0; i < next.size(); ++i)
-            if (sup[i] >= min_support) fi.push_back((uint32_t)i);
-        std::vector<std::string> texts(fi.size());
-        std::vector<std::vector<uint8_t>> code_arena(nthreads);
-        std::vector<uint32_t> code_at(fi.size()), code_len(fi.size());
-        std::vector<uint8_t> code_thread(fi.size());
-        std::vector<std::thread> pool;
-        for (unsigned t = 0; t < nthreads; ++t)
-            pool.emplace_back([&, t]() {
-                CodeBuf cb;
-                for (size_t j = t; j < fi.size(); j += nthreads) {
-                    canonical(next[fi[j]], width, cb);
-                    code_at[j] = (uint32_t)code_arena[t].size();
-                    code_len[j] = cb.len;
-                    code_thread[j] = (uint8_t)t;
-                    code_arena[t].insert(code_arena[t].end(), cb.b, cb.b + cb.len);
-                    texts[j] = query_text(next[fi[j]], labels);
-                }
-            });
-        for (auto& th : pool) th.join();
-        level.clear();
-        level_codes = CodeSet();
-        for (size_t j = 0; j < fi.size(); ++j) {
-            const uint32_t i = fi[j];
-            level.push_back(next[i]);
-            const uint8_t* code = code_arena[code_thread[j]].data() + code_at[j];
-            level_codes.insert(code, code_len[j], code_hash(code, code_len[j]));
-            out.push_back({std::move(texts[j]), k + 1, sup[i], emb[i]});
-        }
-        st.levels = k + 1;
-    }
     st.frequent = out.size();
     st.gpu_ms = gpu_ms;
     st.host_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_host0).count();

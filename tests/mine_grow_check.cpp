@@ -9,7 +9,12 @@
 // frequent edge type; kept when every connected sub-pattern with one edge
 // less is frequent.  Patterns are compared by a canonical code taken as the
 // minimum over ALL vertex orders.  grow_level must return exactly that set,
-// each pattern once, in its own canonical vertex order.
+// each pattern once, in its own canonical vertex order.  Then the miner's
+// whole host level loop (mine_levels: level 1, frequent edge types, wedge
+// table, growth, filing of frequent patterns as query texts) runs with the
+// same supports as its evaluator and must evaluate exactly the brute-force
+// candidates of every level and return exactly its frequent patterns, with
+// their supports, over the original labels.
 //
 // usage: mine_grow_check L P max_edges seed threshold threads
 #include <cstdio>
@@ -101,6 +106,9 @@ int main(int argc, char** argv) {
         for (int c = (int)p.ne - (int)p.n + 1; c > 0; --c) v *= 0.7;
         return v;
     };
+    // supports as the miner sees them: integers, frequent when >= minsup
+    auto isup = [&](const Pattern& p) { return (uint32_t)(support(p) * 1e6); };
+    const uint32_t minsup = (uint32_t)(thr * 1e6);
     const uint32_t width = (L <= 256 && P <= 255) ? 1 : (L <= 65536 ? 2 : 4);
     std::vector<char> freq_tab((size_t)L * L * (P + 1), 0);
     auto freq = [&](uint32_t a, uint32_t el, uint32_t b) { return freq_tab[((size_t)a * L + b) * (P + 1) + el] != 0; };
@@ -114,7 +122,7 @@ int main(int argc, char** argv) {
                 Pattern p;
                 p.n = 2, p.vl[0] = a, p.vl[1] = b;
                 p.add_edge(0, 1, el);
-                if (support(p) < thr) continue;
+                if (isup(p) < minsup) continue;
                 freq_tab[((size_t)a * L + b) * (P + 1) + el] = freq_tab[((size_t)b * L + a) * (P + 1) + el] = 1;
                 uint32_t ord[GVA_MAX_QUERY_VERTICES];
                 canonical(p, width, cb, ord);
@@ -123,6 +131,7 @@ int main(int argc, char** argv) {
                 level_brute.insert(brute_code(p));
             }
     size_t total = 0;
+    std::vector<std::set<Code>> brute_cands(1), brute_freq{level_brute};  // per level (index = edges - 1)
     WedgeTab wedges;
     for (uint32_t k = 1; k < max_edges && !level.empty(); ++k) {
         // brute force
@@ -180,6 +189,7 @@ int main(int argc, char** argv) {
                     return 1;
                 }
         }
+        brute_cands.push_back(want);
         if (got != want) {
             size_t miss = 0, extra = 0;
             for (auto& c : want) miss += !got.count(c);
@@ -194,15 +204,92 @@ int main(int argc, char** argv) {
         level_codes = CodeSet();
         level_brute.clear();
         for (const Pattern& c : next) {
-            if (support(c) < thr) continue;
+            if (isup(c) < minsup) continue;
             level.push_back(c);
             canonical(c, width, cb);
             level_codes.insert(cb.b, cb.len, code_hash(cb.b, cb.len));
             level_brute.insert(brute_code(c));
         }
+        brute_freq.push_back(level_brute);
         printf("level %u: %zu candidates (%llu pruned), %zu frequent\n", k + 1, next.size(),
                (unsigned long long)gt.pruned, level.size());
     }
-    printf("ok %zu candidates\n", total);
+
+    // the miner's whole host level loop (mine_levels) with the same supports:
+    // every level's evaluated candidates and the frequent patterns it returns
+    // (query texts over original labels) against the brute force
+    std::vector<uint32_t> labels(L);
+    for (uint32_t l = 0; l < L; ++l) labels[l] = 100 + 3 * l;
+    std::vector<char> has_part(P + 1, 1);
+    std::vector<std::set<Code>> evaluated;
+    auto evaluate = [&](const std::vector<Pattern>& cands, std::vector<uint32_t>& sup, std::vector<uint64_t>& emb) {
+        std::set<Code> s;
+        sup.assign(cands.size(), 0);
+        emb.assign(cands.size(), 0);
+        for (size_t i = 0; i < cands.size(); ++i) {
+            s.insert(brute_code(cands[i]));
+            sup[i] = isup(cands[i]);
+            emb[i] = cands[i].ne * 1000ull + cands[i].n;
+        }
+        evaluated.push_back(s);
+        return 0;
+    };
+    std::vector<MinedPattern> out;
+    LevelStats ls;
+    if (mine_levels(L, P, has_part, labels, max_edges, minsup, nthreads, nullptr, evaluate, out, ls)) {
+        printf("mine_levels failed\n");
+        return 1;
+    }
+    if (evaluated.empty() || evaluated[0].size() != (size_t)L * (L + 1) / 2 * P) {
+        printf("level 1: wrong edge types evaluated\n");
+        return 1;
+    }
+    if (evaluated.size() != brute_freq.size() && !(evaluated.size() == brute_freq.size() - 1 && brute_freq.back().empty())) {
+        printf("mine_levels evaluated %zu levels, brute force %zu\n", evaluated.size(), brute_freq.size());
+        return 1;
+    }
+    for (size_t lv = 1; lv < evaluated.size(); ++lv)
+        if (evaluated[lv] != brute_cands[lv]) {
+            printf("mine_levels level %zu: evaluated candidates differ from the brute force\n", lv + 1);
+            return 1;
+        }
+    std::vector<std::set<Code>> mined(brute_freq.size());
+    for (const MinedPattern& m : out) {
+        Pattern p;
+        const char* c = m.text.c_str();
+        while (*c) {
+            unsigned a, b, l;
+            int used = 0;
+            if (sscanf(c, "v %u %u\n%n", &a, &l, &used) == 2 && used) {
+                if ((l - 100) % 3 || (l - 100) / 3 >= L || a != p.n) {
+                    printf("bad vertex line in %s\n", m.text.c_str());
+                    return 1;
+                }
+                p.vl[p.n++] = (l - 100) / 3;
+            } else if (sscanf(c, "e %u %u %u\n%n", &a, &b, &l, &used) == 3 && used) {
+                p.add_edge(a, b, l);
+            } else {
+                printf("unparsable pattern text %s\n", m.text.c_str());
+                return 1;
+            }
+            c += used;
+        }
+        if (m.edges != p.ne || m.edges == 0 || m.edges > mined.size() || m.support != isup(p) ||
+            m.embeddings != p.ne * 1000ull + p.n || !connected(p)) {
+            printf("mined pattern with wrong edges/support/embeddings: %s\n", m.text.c_str());
+            return 1;
+        }
+        if (!mined[m.edges - 1].insert(brute_code(p)).second) {
+            printf("pattern mined twice: %s\n", m.text.c_str());
+            return 1;
+        }
+    }
+    for (size_t lv = 0; lv < mined.size(); ++lv)
+        if (mined[lv] != brute_freq[lv]) {
+            printf("mine_levels level %zu: %zu frequent patterns, brute force %zu\n", lv + 1, mined[lv].size(),
+                   brute_freq[lv].size());
+            return 1;
+        }
+    printf("ok %zu candidates, %zu frequent\n", total, out.size());
     return 0;
 }

@@ -7,6 +7,10 @@ vertex orders, every extension checked against every one-edge-less connected
 sub-pattern).  This pins the pruning shortcuts in the miner (wedge table,
 order-free invariants, first sub-pattern check before the code) to the plain
 definition of a candidate: they may only drop what the definition drops.
+The same driver then runs the miner's whole host level loop (mine_levels,
+which the GPU miner calls with the device evaluator) with the stand-in as
+evaluator and checks every level's evaluated candidates and the returned
+frequent patterns (texts, supports) against the brute force.
 """
 import shutil
 import subprocess
