@@ -71,6 +71,9 @@ int plan_from_text(const std::string& text, int mode, Plan& out);
 // The same plan for the query "v i labels[i]" (i < n) followed by the edges
 // "e sdl[3j] sdl[3j+1] sdl[3j+2]" (j < ne), without the text.
 int plan_from_query(uint32_t n, const uint32_t* labels, const uint32_t* sdl, size_t ne, int mode, Plan& out);
+// A plan computed by dplan (gva_dplan.h; status DPLAN_OK) as a Plan.
+struct DPlan;
+int plan_from_dplan(const DPlan& d, const uint32_t* labels, Plan& out);
 
 // ---------------------------------------------------------------- steps -----
 // A plan lowered to engine steps.  Every reference phase becomes one or more

@@ -35,6 +35,7 @@
 #include "../../include/geneva.h"
 #include "gva_engine.cuh"
 #include "gva_internal.h"
+#include "gva_dplan.h"
 #include "gva_grow.h"
 
 namespace gva {
@@ -75,18 +76,25 @@ int run_mine(DevDB& db, cudaStream_t s, uint64_t budget, uint32_t max_edges, uin
         std::vector<std::thread> pool;
         for (unsigned t = 0; t < nthreads; ++t)
             pool.emplace_back([&, t]() {
-                uint32_t ql[GVA_MAX_QUERY_VERTICES], sdl[3 * kMaxPatEdges];
+                uint32_t sdl[3 * kMaxPatEdges];
+                std::unique_ptr<DPlanQuery> dq(new DPlanQuery());
+                std::unique_ptr<DPlan> dp(new DPlan());
                 for (size_t i = b0 + t; i < b1; i += nthreads) {
-                    // the plan of the candidate's query text, built from the pattern
+                    // the plan of the candidate's query text, built from the
+                    // pattern by the heap-free planner, else by the host planner
                     const Pattern& c = cands[i];
-                    for (uint32_t v = 0; v < c.n; ++v) ql[v] = labels[c.vl[v]];
+                    dq->n = c.n;
+                    dq->lines = c.ne;
+                    for (uint32_t v = 0; v < c.n; ++v) dq->label[v] = labels[c.vl[v]];
                     for (uint32_t e = 0; e < c.ne; ++e) {
-                        sdl[3 * e] = c.edges[e].u;
-                        sdl[3 * e + 1] = c.edges[e].v;
-                        sdl[3 * e + 2] = c.edges[e].el;
+                        dq->s[e] = sdl[3 * e] = c.edges[e].u;
+                        dq->d[e] = sdl[3 * e + 1] = c.edges[e].v;
+                        dq->l[e] = sdl[3 * e + 2] = c.edges[e].el;
                     }
+                    dplan(*dq, *dp);
                     Plan plan;
-                    int r = plan_from_query(c.n, ql, sdl, c.ne, GVA_MODE_DV, plan);
+                    int r = dp->status == DPLAN_OK ? plan_from_dplan(*dp, dq->label, plan)
+                                                   : plan_from_query(c.n, dq->label, sdl, c.ne, GVA_MODE_DV, plan);
                     if (!r) r = lower_plan(plan, db.meta, steps[i - b0], true);
                     if (r) {
                         rcs[t] = r;

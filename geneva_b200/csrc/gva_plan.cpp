@@ -16,6 +16,7 @@
 #include <sstream>
 
 #include "../../include/geneva.h"
+#include "gva_dplan.h"
 #include "gva_internal.h"
 
 namespace gva {
@@ -787,6 +788,27 @@ int plan_from_text(const std::string& text, int mode, Plan& out) {
     int st = p.parse(text);
     if (st) return st;
     return finish_plan(p, mode, out);
+}
+
+int plan_from_dplan(const DPlan& d, const uint32_t* labels, Plan& out) {
+    if (d.status != DPLAN_OK) return fail(GVA_ERR_ARG, "query was left to the host planner");
+    Plan plan;
+    plan.mode = GVA_MODE_DV;
+    plan.vnum = d.vnum;
+    plan.qlabel.assign(labels, labels + d.vnum);
+    plan.phases.resize(d.nphase);
+    for (uint32_t p = 0; p < d.nphase; ++p) {
+        Phase& ph = plan.phases[p];
+        ph.type = (char)d.ph_type[p];
+        ph.edge_label = d.ph_el[p];
+        ph.pairs.assign(d.pairs + d.ph_at[p], d.pairs + d.ph_at[p] + 2 * d.ph_np[p]);
+    }
+    plan.restricts.assign(d.restricts, d.restricts + d.vnum + 1);
+    for (uint32_t i = 0; i < d.nrep; ++i) plan.repeat_flag.emplace_hint(plan.repeat_flag.end(), d.rep_key[i], d.rep_val[i]);
+    for (uint32_t i = 0; i < d.nstat; ++i) plan.record_stat[d.stat_el[i]].push_back(d.stat_vl[i]);
+    plan.columns.assign(d.columns, d.columns + d.ncol);
+    out = std::move(plan);
+    return GVA_OK;
 }
 
 int plan_from_query(uint32_t n, const uint32_t* labels, const uint32_t* sdl, size_t ne, int mode, Plan& out) {
