@@ -123,20 +123,20 @@ struct DPlanner {
     const DPlanQuery& q;
     DPlan& out;
     uint32_t n = 0;
-    uint32_t adj[kDpV][kDpV];
+    uint8_t adj[kDpV][kDpV];  // index of the distinct edge (es, ee, el), 0xff: none
     uint32_t nbr_full[kDpV], live[kDpV];
     Group groups[2 * kDpLines];
     uint32_t ngroups = 0, goff[kDpV + 1];
     uint32_t es[kDpLines], ee[kDpLines], el[kDpLines], nedges = 0;  // distinct edges, first label wins
     uint32_t order[kDpV], norder = 0, visited = 0;
-    KeyCount ext_keys[kDpKeys], other_keys[kDpKeys];
+    KeyCount ext_keys[kDpV], other_keys[kDpLines];  // one per matched vertex / planned edge at most
     uint32_t next_keys = 0, nother_keys = 0;
     RedRef red[2 * kDpLines];  // two per reduce pair; a pair is a planned edge
     uint32_t nred = 0;
 
     GVA_HD DPlanner(const DPlanQuery& q_, DPlan& out_) : q(q_), out(out_) {}
 
-    GVA_HD uint32_t E(uint32_t a, uint32_t b) const { return adj[a][b]; }
+    GVA_HD uint32_t E(uint32_t a, uint32_t b) const { return adj[a][b] == 0xff ? kDpNone : el[adj[a][b]]; }
     GVA_HD uint32_t ql(uint32_t v) const { return q.label[v]; }
     GVA_HD static uint64_t key(uint32_t e, uint32_t v) { return ((uint64_t)e << 32) | v; }
     GVA_HD uint32_t group_mask(uint32_t v, uint32_t label) const {
@@ -150,7 +150,7 @@ struct DPlanner {
         if (n == 0 || n > (uint32_t)kDpV || q.lines == 0 || q.lines > (uint32_t)kDpLines) return false;
         for (uint32_t a = 0; a < n; ++a) {
             nbr_full[a] = live[a] = 0;
-            for (uint32_t b = 0; b < n; ++b) adj[a][b] = kDpNone;
+            for (uint32_t b = 0; b < n; ++b) adj[a][b] = 0xff;
         }
         for (uint32_t i = 0; i < q.lines; ++i) {
             const uint32_t s = q.s[i], d = q.d[i], l = q.l[i];
@@ -159,11 +159,12 @@ struct DPlanner {
             nbr_full[d] |= bit(s);
             groups[ngroups++] = {s, l, 1, bit(d)};
             groups[ngroups++] = {d, l, 1, bit(s)};
-            if (adj[s][d] == kDpNone) {
+            if (adj[s][d] == 0xff) {
                 es[nedges] = s < d ? s : d;
                 ee[nedges] = s < d ? d : s;
-                el[nedges++] = l;
-                adj[s][d] = adj[d][s] = l;
+                el[nedges] = l;
+                adj[s][d] = adj[d][s] = (uint8_t)nedges;
+                ++nedges;
             }
             live[s] |= bit(d);
             live[d] |= bit(s);
@@ -199,14 +200,14 @@ struct DPlanner {
         order[norder++] = v;
         return true;
     }
-    GVA_HD bool add_key(KeyCount* keys, uint32_t& nk, uint64_t k) {  // keys[k] += 1, ascending
+    GVA_HD bool add_key(KeyCount* keys, uint32_t& nk, uint64_t k, uint32_t cap) {  // keys[k] += 1, ascending
         uint32_t i = 0;
         while (i < nk && keys[i].key < k) ++i;
         if (i < nk && keys[i].key == k) {
             keys[i].count += 1;
             return true;
         }
-        if (nk >= (uint32_t)kDpKeys) return false;
+        if (nk >= cap) return false;
         for (uint32_t j = nk; j > i; --j) keys[j] = keys[j - 1];
         keys[i] = {k, 1};
         ++nk;
@@ -237,7 +238,7 @@ struct DPlanner {
         }
         if (!new_phase('E', E(s1, e1))) return false;
         auto take = [&](uint32_t s, uint32_t e) {
-            if (!add_pair(s, e) || !add_key(ext_keys, next_keys, key(E(s, e), ql(e)))) return false;
+            if (!add_pair(s, e) || !add_key(ext_keys, next_keys, key(E(s, e), ql(e)), kDpV)) return false;
             visited |= bit(e);
             if (!push_order(e)) return false;
             live[s] &= ~bit(e);
@@ -261,7 +262,7 @@ struct DPlanner {
             out.ph_el[idx] = E(a, b);
             const uint64_t kb = key(E(a, b), ql(b)), ka = key(E(a, b), ql(a));
             if (kb == ka) {
-                if (!add_key(other_keys, nother_keys, kb)) return false;
+                if (!add_key(other_keys, nother_keys, kb, kDpLines)) return false;
             } else {
                 if (nred + 2 > (uint32_t)(2 * kDpLines)) return false;
                 red[nred++] = {kb, idx, i};
@@ -300,8 +301,12 @@ struct DPlanner {
     GVA_HD void seed_without_triangle(uint32_t& s_out, uint32_t& e1_out, uint32_t& e2_out) const {
         // a group's members are its mask bits: at most two per edge line in all
         constexpr uint32_t kCap = 2 * kDpLines;
+        // entries: a same-edge-and-end-label list has two or more members,
+        // a same-edge-label list one per group, a same-source list one per vertex
+        const uint32_t list_cap[3] = {kCap / 2, kCap, (uint32_t)kDpV};
         uint32_t members[3][kCap];
-        SeedEntry list[3][kCap];
+        SeedEntry list0[kCap / 2], list1[kCap], list2[kDpV];
+        SeedEntry* list[3] = {list0, list1, list2};
         uint32_t used[3] = {0, 0, 0}, cnt[3] = {0, 0, 0};
         enum { SAME_EL_VL = 0, SAME_EL = 1, SAME_SRC = 2 };
         bool overflow = false;
@@ -312,7 +317,8 @@ struct DPlanner {
                 const uint32_t mask = groups[gi].mask;
                 const uint32_t pm = popc(mask);
                 if (used[SAME_EL_VL] + pm > kCap || used[SAME_EL] + pm > kCap || used[SAME_SRC] + pm > kCap ||
-                    cnt[SAME_EL_VL] + pm > kCap || cnt[SAME_EL] + 1 > kCap || cnt[SAME_SRC] + 1 > kCap) {
+                    cnt[SAME_EL_VL] + pm / 2 > list_cap[SAME_EL_VL] || cnt[SAME_EL] + 1 > list_cap[SAME_EL] ||
+                    cnt[SAME_SRC] + 1 > list_cap[SAME_SRC]) {
                     overflow = true;
                     break;
                 }
