@@ -355,30 +355,11 @@ int upload_graph(HostGraph& g, int device, DevDB*& out) {
     int prc = ensure_pool(device);
     if (prc) return prc;
     const uint32_t L = g.num_labels();
-    // vertices grouped by dense label: the seed frontiers of init phases
-    std::vector<uint32_t> seed_off(L + 1, 0), seed_verts;
-    for (uint32_t v = 1; v <= g.max_id; ++v)
-        if (g.dlabel[v] != kNone) seed_off[g.dlabel[v] + 1]++;
-    for (uint32_t l = 0; l < L; ++l) seed_off[l + 1] += seed_off[l];
-    seed_verts.resize(seed_off[L]);
-    {
-        std::vector<uint32_t> fill(seed_off.begin(), seed_off.end() - 1);
-        for (uint32_t v = 1; v <= g.max_id; ++v)
-            if (g.dlabel[v] != kNone) seed_verts[fill[g.dlabel[v]]++] = v;
-    }
-    // the same groups ordered by total degree (descending, then id): rooted
-    // existence searches try the vertices most likely to succeed first
-    std::vector<uint32_t> seed_deg(seed_verts);
-    {
-        std::vector<uint32_t> deg(g.max_id + 1, 0);
-        for (auto& p : g.parts)
-            if (!p.off.empty())
-                for (uint32_t v = 0; v <= g.max_id; ++v)
-                    deg[v] += p.off[(uint64_t)(v + 1) * L] - p.off[(uint64_t)v * L];
-        for (uint32_t l = 0; l < L; ++l)
-            std::sort(seed_deg.begin() + seed_off[l], seed_deg.begin() + seed_off[l + 1],
-                      [&](uint32_t a, uint32_t b) { return deg[a] != deg[b] ? deg[a] > deg[b] : a < b; });
-    }
+    // vertices grouped by dense label: the seed frontiers of init phases; the
+    // same groups by total degree for rooted existence searches, which try
+    // the vertices most likely to succeed first
+    std::vector<uint32_t> seed_off, seed_verts, seed_deg;
+    seed_groups(g, seed_off, seed_verts, seed_deg);
     size_t bytes = 2 * align256(seed_verts.size() * 4 + 4);
     for (auto& p : g.parts) bytes += align256(p.off.size() * 4) + align256(p.adj.size() * 4 + 4);
     void* arena = nullptr;

@@ -63,15 +63,45 @@ int build_partition(HostGraph& g, uint32_t edge_label, const std::vector<std::ve
     return GVA_OK;
 }
 
+// Sorted distinct labels and each vertex's dense label.  Labels are few
+// against vertices: they are collected in an open-addressing table (label ->
+// dense index, filled in once the distinct labels are sorted).
 void finish_labels(HostGraph& g) {
+    std::vector<uint64_t> tab(64, ~0ull);  // label << 32 | dense index; ~0: empty
+    size_t count = 0;
+    auto slot = [&](uint32_t l) -> uint64_t& {
+        const size_t m = tab.size() - 1;
+        size_t i = (size_t)((l * 0x9e3779b97f4a7c15ull) >> 32) & m;
+        while (tab[i] != ~0ull && (uint32_t)(tab[i] >> 32) != l) i = (i + 1) & m;
+        return tab[i];
+    };
     std::vector<uint32_t> ls;
-    for (uint32_t v = 1; v <= g.max_id; ++v)
-        if (g.vlabel[v] != kNone) ls.push_back(g.vlabel[v]);
+    uint32_t last = kNone;
+    for (uint32_t v = 1; v <= g.max_id; ++v) {
+        const uint32_t l = g.vlabel[v];
+        if (l == kNone || l == last) continue;
+        last = l;
+        uint64_t& t = slot(l);
+        if (t != ~0ull) continue;
+        t = (uint64_t)l << 32;
+        ls.push_back(l);
+        if (2 * ++count > tab.size()) {  // grow: re-file the labels seen so far
+            tab.assign(tab.size() * 2, ~0ull);
+            for (uint32_t x : ls) slot(x) = (uint64_t)x << 32;
+        }
+    }
     std::sort(ls.begin(), ls.end());
-    ls.erase(std::unique(ls.begin(), ls.end()), ls.end());
+    for (size_t i = 0; i < ls.size(); ++i) slot(ls[i]) = ((uint64_t)ls[i] << 32) | i;
     g.labels = ls;
     g.dlabel.assign(g.max_id + 1, kNone);
-    for (uint32_t v = 1; v <= g.max_id; ++v) g.dlabel[v] = g.dense_label(g.vlabel[v]);
+    last = kNone;
+    uint32_t last_dense = kNone;
+    for (uint32_t v = 1; v <= g.max_id; ++v) {
+        const uint32_t l = g.vlabel[v];
+        if (l == kNone) continue;
+        if (l != last) last = l, last_dense = (uint32_t)(slot(l) & 0xffffffffu);
+        g.dlabel[v] = last_dense;
+    }
 }
 
 // Number of index vertices genDatabase prepends to a label group of raw
@@ -171,6 +201,39 @@ int load_mygraph(const std::string& mygraph, const std::string& metadata, HostGr
     return GVA_OK;
 }
 
+void seed_groups(const HostGraph& g, std::vector<uint32_t>& seed_off, std::vector<uint32_t>& seed_verts,
+                 std::vector<uint32_t>& seed_by_degree) {
+    const uint32_t L = g.num_labels();
+    seed_off.assign(L + 1, 0);
+    for (uint32_t v = 1; v <= g.max_id; ++v)
+        if (g.dlabel[v] != kNone) seed_off[g.dlabel[v] + 1]++;
+    for (uint32_t l = 0; l < L; ++l) seed_off[l + 1] += seed_off[l];
+    seed_verts.resize(seed_off[L]);
+    {
+        std::vector<uint32_t> fill(seed_off.begin(), seed_off.end() - 1);
+        for (uint32_t v = 1; v <= g.max_id; ++v)
+            if (g.dlabel[v] != kNone) seed_verts[fill[g.dlabel[v]]++] = v;
+    }
+    // total degree over all edge labels; within a label group the vertices
+    // are in ascending id, so a stable counting sort by degree (largest
+    // first) gives (degree descending, id ascending)
+    std::vector<uint32_t> deg(g.max_id + 1, 0);
+    for (auto& p : g.parts)
+        if (!p.off.empty())
+            for (uint32_t v = 0; v <= g.max_id; ++v) deg[v] += p.off[(uint64_t)(v + 1) * L] - p.off[(uint64_t)v * L];
+    seed_by_degree.resize(seed_verts.size());
+    std::vector<uint32_t> cnt;
+    for (uint32_t l = 0; l < L; ++l) {
+        const uint32_t b = seed_off[l], e = seed_off[l + 1];
+        uint32_t dmax = 0;
+        for (uint32_t i = b; i < e; ++i) dmax = std::max(dmax, deg[seed_verts[i]]);
+        cnt.assign((size_t)dmax + 2, 0);
+        for (uint32_t i = b; i < e; ++i) cnt[dmax - deg[seed_verts[i]] + 1]++;  // rank 0 = largest degree
+        for (size_t r = 1; r < cnt.size(); ++r) cnt[r] += cnt[r - 1];
+        for (uint32_t i = b; i < e; ++i) seed_by_degree[b + cnt[dmax - deg[seed_verts[i]]]++] = seed_verts[i];
+    }
+}
+
 int graph_from_edges(const uint32_t* vlabels, uint32_t max_id, const uint32_t* src, const uint32_t* dst,
                      const uint32_t* elabel, uint64_t ne, HostGraph& g) {
     if (!vlabels || (ne && (!src || !dst || !elabel))) return fail(GVA_ERR_ARG, "null array");
@@ -200,21 +263,32 @@ int graph_from_edges(const uint32_t* vlabels, uint32_t max_id, const uint32_t* s
     const unsigned nth = std::max(1u, std::min(64u, std::thread::hardware_concurrency()));
     const uint64_t V = (uint64_t)max_id + 1;
     g.parts.resize(P);
-    std::vector<uint64_t> pos(V + 1), len(V);
-    for (uint32_t p = 1; p <= P; ++p) {
-        std::fill(pos.begin(), pos.end(), 0);
-        for (uint64_t i = 0; i < ne; ++i)
-            if (elabel[i] == p) pos[src[i] + 1]++, pos[dst[i] + 1]++;
-        for (uint64_t v = 0; v < V; ++v) pos[v + 1] += pos[v];
-        std::vector<uint64_t> keys(pos[V]);  // (dense label << 32) | neighbour
-        {
-            std::vector<uint64_t> cur(pos.begin(), pos.end() - 1);
-            for (uint64_t i = 0; i < ne; ++i) {
-                if (elabel[i] != p) continue;
-                keys[cur[src[i]]++] = ((uint64_t)g.dlabel[dst[i]] << 32) | dst[i];
-                keys[cur[dst[i]]++] = ((uint64_t)g.dlabel[src[i]] << 32) | src[i];
-            }
+    // every partition's entries bucketed by source in one pass over the edges:
+    // pos_all[p - 1][v] is where vertex v's bucket starts in keys_all[p - 1]
+    std::vector<std::vector<uint64_t>> pos_all(P, std::vector<uint64_t>(V + 1, 0)), keys_all(P);
+    for (uint64_t i = 0; i < ne; ++i) {
+        std::vector<uint64_t>& c = pos_all[elabel[i] - 1];
+        c[src[i] + 1]++, c[dst[i] + 1]++;
+    }
+    for (uint32_t p = 0; p < P; ++p) {
+        std::vector<uint64_t>& c = pos_all[p];
+        for (uint64_t v = 0; v < V; ++v) c[v + 1] += c[v];
+        keys_all[p].resize(c[V]);
+    }
+    {
+        std::vector<std::vector<uint64_t>> cur(P);
+        for (uint32_t p = 0; p < P; ++p) cur[p].assign(pos_all[p].begin(), pos_all[p].end() - 1);
+        for (uint64_t i = 0; i < ne; ++i) {  // (dense label << 32) | neighbour
+            const uint32_t p = elabel[i] - 1;
+            keys_all[p][cur[p][src[i]]++] = ((uint64_t)g.dlabel[dst[i]] << 32) | dst[i];
+            keys_all[p][cur[p][dst[i]]++] = ((uint64_t)g.dlabel[src[i]] << 32) | src[i];
         }
+    }
+    std::vector<uint64_t> len(V), start(V);
+    for (uint32_t p = 1; p <= P; ++p) {
+        const std::vector<uint64_t>& pos = pos_all[p - 1];
+        std::vector<uint64_t> keys;
+        keys.swap(keys_all[p - 1]);
         auto sort_range = [&](uint64_t v0, uint64_t v1) {
             for (uint64_t v = v0; v < v1; ++v) {
                 uint64_t* a = keys.data() + pos[v];
@@ -223,7 +297,7 @@ int graph_from_edges(const uint32_t* vlabels, uint32_t max_id, const uint32_t* s
                 len[v] = (uint64_t)(std::unique(a, b) - a);
             }
         };
-        if (nth == 1 || keys.size() < (1u << 20)) {
+        if (nth == 1 || keys.size() < (1u << 16)) {
             sort_range(0, V);
         } else {
             // vertex ranges of about equal entry counts
@@ -238,22 +312,41 @@ int graph_from_edges(const uint32_t* vlabels, uint32_t max_id, const uint32_t* s
             }
             for (auto& th : pool) th.join();
         }
-        uint64_t total = 0;
-        for (uint64_t v = 0; v < V; ++v) total += len[v];
+        uint64_t total = 0;  // start[v]: where vertex v's list starts in adj
+        for (uint64_t v = 0; v < V; ++v) {
+            const uint64_t l = len[v];
+            start[v] = total;
+            total += l;
+        }
         if (total >= 0xffffffffull) return fail(GVA_ERR_UNSUPPORTED, "partition has 2^32 or more adjacency entries");
         HostPartition& part = g.parts[p - 1];
         part.edge_label = p;
-        part.off.assign(entries, 0);  // group (v, l) starts at off[v * L + l]
+        part.off.resize(entries);  // group (v, l) starts at off[v * L + l]
         part.adj.resize(total);
-        uint64_t k = 0;
-        for (uint64_t v = 0; v < V; ++v) {
-            const uint64_t* a = keys.data() + pos[v];
-            for (uint64_t j = 0; j < len[v]; ++j) {
-                part.off[v * L + (a[j] >> 32) + 1]++;
-                part.adj[k++] = (uint32_t)a[j];
+        // each vertex's offsets and list, written by vertex ranges: its list
+        // is sorted by label, so group l starts after the entries of labels < l
+        auto fill_range = [&](uint64_t v0, uint64_t v1) {
+            for (uint64_t v = v0; v < v1; ++v) {
+                const uint64_t* a = keys.data() + pos[v];
+                const uint64_t at = start[v], n = len[v];
+                uint64_t j = 0;
+                for (uint64_t l = 0; l < L; ++l) {
+                    part.off[v * L + l] = (uint32_t)(at + j);
+                    while (j < n && (a[j] >> 32) == l) {
+                        part.adj[at + j] = (uint32_t)a[j];
+                        ++j;
+                    }
+                }
             }
+        };
+        if (nth == 1 || V < (1u << 16)) {
+            fill_range(0, V);
+        } else {
+            std::vector<std::thread> pool;
+            for (unsigned t = 0; t < nth; ++t) pool.emplace_back(fill_range, V * t / nth, V * (t + 1) / nth);
+            for (auto& th : pool) th.join();
         }
-        for (uint64_t t = 1; t < entries; ++t) part.off[t] += part.off[t - 1];
+        part.off[entries - 1] = (uint32_t)total;
     }
     if (g.parts.empty()) g.parts.resize(1);
     return GVA_OK;

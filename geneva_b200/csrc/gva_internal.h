@@ -3,6 +3,8 @@
 
 #include <cstdint>
 #include <map>
+#include <memory>
+#include <utility>
 #include <string>
 #include <vector>
 
@@ -20,10 +22,33 @@ const char* last_error_cstr();                        // this thread's last mess
 // Host copy of one database: per edge label a CSR whose per-vertex lists are
 // sorted by (dense vertex label, vertex id), plus a dense (vertex, label) ->
 // offset table.  seg(v, l) = adj[off[v*L + l] .. off[v*L + l + 1]).
+// Allocator whose default construction leaves plain values uninitialised:
+// the offset tables below are written in full by their builders, so zeroing
+// them first would only add a pass over memory (and its page faults on one
+// thread).
+template <typename T>
+struct NoInitAlloc : std::allocator<T> {
+    template <typename U>
+    struct rebind {
+        using other = NoInitAlloc<U>;
+    };
+    NoInitAlloc() = default;
+    template <typename U>
+    NoInitAlloc(const NoInitAlloc<U>&) noexcept {}
+    template <typename U>
+    void construct(U* p) noexcept {
+        ::new ((void*)p) U;
+    }
+    template <typename U, typename... A>
+    void construct(U* p, A&&... a) {
+        ::new ((void*)p) U(std::forward<A>(a)...);
+    }
+};
+
 struct HostPartition {
-    uint32_t edge_label = 0;       // 1..P
-    std::vector<uint32_t> off;     // (max_id + 1) * L + 1 entries
-    std::vector<uint32_t> adj;     // neighbour ids
+    uint32_t edge_label = 0;                            // 1..P
+    std::vector<uint32_t, NoInitAlloc<uint32_t>> off;   // (max_id + 1) * L + 1 entries, each written by the builder
+    std::vector<uint32_t> adj;                          // neighbour ids
 };
 
 struct HostGraph {
@@ -43,6 +68,12 @@ int load_mygraph(const std::string& mygraph, const std::string& metadata, HostGr
 // Builds from an edge list (tools/genDatabase.cpp:600-667 semantics, no renumbering).
 int graph_from_edges(const uint32_t* vlabels, uint32_t max_id, const uint32_t* src, const uint32_t* dst,
                      const uint32_t* elabel, uint64_t ne, HostGraph& g);
+
+// Init-phase frontiers: vertices grouped by dense label (seed_off[l] ..
+// seed_off[l + 1] of seed_verts, ascending id) and the same groups ordered by
+// total degree, largest first, ties by id (seed_by_degree).
+void seed_groups(const HostGraph& g, std::vector<uint32_t>& seed_off, std::vector<uint32_t>& seed_verts,
+                 std::vector<uint32_t>& seed_by_degree);
 
 // .g -> .mygraph/.metadata/.reorder exactly as tools/genDatabase.cpp writes them.
 int convert_g(const std::string& g_path, const std::string& mygraph, const std::string& metadata,
