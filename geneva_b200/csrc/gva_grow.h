@@ -1,7 +1,9 @@
 // Pattern growth for level-wise mining, host only: labelled patterns,
-// canonical codes, code sets and one level of candidate generation with its
-// anti-monotone pruning.  Shared by the miner (gva_mine.cpp) and a CPU test
-// that checks grow_level against a brute-force candidate generator.
+// canonical codes, code sets, one level of candidate generation with its
+// anti-monotone pruning (grow_level) and the level loop around it with the
+// evaluator as a callback (mine_levels).  Shared by the miner (gva_mine.cpp,
+// whose evaluator runs the batched matcher) and a CPU test that checks both
+// against a brute-force miner.
 #pragma once
 
 #include <algorithm>

@@ -13,7 +13,10 @@
 // and each level's candidates are matched in one gva_batch_count-style run
 // (shared step prefixes, per-graph bitmaps) whose supports decide the next
 // level.  Each candidate is matched with the planner's own plan for its
-// query text, so embedding counts are the reference's row counts.
+// query text (computed from the pattern by the heap-free planner, gva_dplan.h,
+// or the host planner for the queries it leaves), so embedding counts are the
+// reference's row counts.  The level loop is mine_levels (gva_grow.h); this
+// file supplies its evaluators (graph supports, MNI supports).
 #include <algorithm>
 #include <cstdio>
 #include <cstdlib>
