@@ -9,6 +9,7 @@
 #include <sstream>
 
 #include "../../include/geneva.h"
+#include "gva_dplan.h"
 #include "gva_internal.h"
 
 namespace gva {
@@ -363,14 +364,53 @@ int graph_from_edges(const uint32_t* vlabels, uint32_t max_id, const uint32_t* s
 //                               (src/cpumine.cpp:298-435)
 //   R                         : reduce over all pairs (src/cpumine.cpp:486-584); more than
 //                               16 pairs empties the frontier as the reference does (:499-502)
-int lower_plan(const Plan& plan, const HostGraph& g, std::vector<Step>& steps, bool fuse_reductions) {
+// The plan read through a small view, so that host plans and plans from the
+// heap-free planner (gva_dplan.h) lower through the same code.
+struct PlanView {
+    const Plan& p;
+    struct Ph {
+        const Phase& ph;
+        char type() const { return ph.type; }
+        uint32_t edge_label() const { return ph.edge_label; }
+        size_t npairs() const { return ph.pairs.size() / 2; }
+        uint32_t pair(size_t k) const { return ph.pairs[k]; }
+    };
+    uint32_t vnum() const { return p.vnum; }
+    int mode() const { return p.mode; }
+    uint32_t qlabel(uint32_t v) const { return p.qlabel[v]; }
+    uint32_t restrict_of(uint32_t v) const { return p.restricts[v]; }
+    size_t nphase() const { return p.phases.size(); }
+    Ph phase(size_t i) const { return Ph{p.phases[i]}; }
+};
+
+struct DPlanView {
+    const DPlan& d;
+    const uint32_t* labels;
+    struct Ph {
+        const DPlan& d;
+        size_t i;
+        char type() const { return (char)d.ph_type[i]; }
+        uint32_t edge_label() const { return d.ph_el[i]; }
+        size_t npairs() const { return d.ph_np[i]; }
+        uint32_t pair(size_t k) const { return d.pairs[d.ph_at[i] + k]; }
+    };
+    uint32_t vnum() const { return d.vnum; }
+    int mode() const { return GVA_MODE_DV; }
+    uint32_t qlabel(uint32_t v) const { return labels[v]; }
+    uint32_t restrict_of(uint32_t v) const { return d.restricts[v]; }
+    size_t nphase() const { return d.nphase; }
+    Ph phase(size_t i) const { return Ph{d, i}; }
+};
+
+template <typename View>
+int lower_core(const View& plan, const HostGraph& g, std::vector<Step>& steps, bool fuse_reductions) {
     steps.clear();
-    steps.reserve(plan.phases.size() + 2);
+    steps.reserve(plan.nphase() + 2);
     int newest = -1;  // query vertex added by the last extension step
     const uint32_t P = (uint32_t)g.parts.size();
-    if (plan.vnum > (uint32_t)kMaxCols) return fail(GVA_ERR_UNSUPPORTED, "query has more than 32 vertices");
+    if (plan.vnum() > (uint32_t)kMaxCols) return fail(GVA_ERR_UNSUPPORTED, "query has more than 32 vertices");
     int col[kMaxCols];
-    for (uint32_t v = 0; v < plan.vnum; ++v) col[v] = -1;
+    for (uint32_t v = 0; v < plan.vnum(); ++v) col[v] = -1;
     int width = 0;
     auto part_of = [&](uint32_t el) -> uint32_t { return (el >= 1 && el <= P && !g.parts[el - 1].off.empty()) ? el : 0; };
     struct EqCols {  // columns of matched vertices with the new vertex's label, ascending
@@ -382,7 +422,7 @@ int lower_plan(const Plan& plan, const HostGraph& g, std::vector<Step>& steps, b
         st.kind = STEP_EXT;
         st.width_in = (uint32_t)width;
         st.part = part_of(el);
-        st.label = g.dense_label(plan.qlabel[e]);
+        st.label = g.dense_label(plan.qlabel(e));
         st.src_col = col[s];
         st.bound_col = bound_col;
         st.bound_inclusive = incl ? 1 : 0;
@@ -395,51 +435,51 @@ int lower_plan(const Plan& plan, const HostGraph& g, std::vector<Step>& steps, b
     };
     auto same_label_cols = [&](uint32_t e) {
         EqCols eq;
-        for (uint32_t v = 0; v < plan.vnum; ++v)
-            if (col[v] >= 0 && plan.qlabel[v] == plan.qlabel[e]) eq.c[eq.n++] = col[v];
+        for (uint32_t v = 0; v < plan.vnum(); ++v)
+            if (col[v] >= 0 && plan.qlabel(v) == plan.qlabel(e)) eq.c[eq.n++] = col[v];
         std::sort(eq.c, eq.c + eq.n);
         return eq;
     };
-    for (size_t pi = 0; pi < plan.phases.size(); ++pi) {
-        const Phase& ph = plan.phases[pi];
-        const size_t np = ph.pairs.size() / 2;
+    for (size_t pi = 0; pi < plan.nphase(); ++pi) {
+        const auto ph = plan.phase(pi);
+        const size_t np = ph.npairs();
         if (pi == 0) {
-            if (ph.type != 'E' || np < 1 || np > 2) return fail(GVA_ERR_FORMAT, "first phase must extend 1 or 2 vertices");
-            const uint32_t s = ph.pairs[0];
+            if (ph.type() != 'E' || np < 1 || np > 2) return fail(GVA_ERR_FORMAT, "first phase must extend 1 or 2 vertices");
+            const uint32_t s = ph.pair(0);
             Step seed;
             seed.kind = STEP_SEED;
             seed.width_in = 0;
-            seed.part = part_of(ph.edge_label);
-            seed.label = g.dense_label(plan.qlabel[s]);
+            seed.part = part_of(ph.edge_label());
+            seed.label = g.dense_label(plan.qlabel(s));
             seed.always_empty = (seed.part == 0 || seed.label == kNone) ? 1 : 0;
             steps.push_back(seed);
             col[s] = width++;
-            if (np == 1 || plan.mode == GVA_MODE_SV) {
-                const uint32_t e = ph.pairs[1];
-                ext(ph.edge_label, s, e, plan.restricts[e] == s ? 0 : -1, false, EqCols());
+            if (np == 1 || plan.mode() == GVA_MODE_SV) {
+                const uint32_t e = ph.pair(1);
+                ext(ph.edge_label(), s, e, plan.restrict_of(e) == s ? 0 : -1, false, EqCols());
             } else {
-                const uint32_t e1 = ph.pairs[1], e2 = ph.pairs[3];
-                ext(ph.edge_label, s, e1, plan.restricts[e1] != kNone ? 0 : -1, true, EqCols());
+                const uint32_t e1 = ph.pair(1), e2 = ph.pair(3);
+                ext(ph.edge_label(), s, e1, plan.restrict_of(e1) != kNone ? 0 : -1, true, EqCols());
                 EqCols eq;
-                if (plan.qlabel[e2] == plan.qlabel[e1]) eq.c[eq.n++] = col[e1];
-                if (plan.restricts[e2] == e1)
-                    ext(ph.edge_label, s, e2, col[e1], false, eq);
+                if (plan.qlabel(e2) == plan.qlabel(e1)) eq.c[eq.n++] = col[e1];
+                if (plan.restrict_of(e2) == e1)
+                    ext(ph.edge_label(), s, e2, col[e1], false, eq);
                 else
-                    ext(ph.edge_label, s, e2, plan.restricts[e2] != kNone ? 0 : -1, true, eq);
+                    ext(ph.edge_label(), s, e2, plan.restrict_of(e2) != kNone ? 0 : -1, true, eq);
             }
             steps.back().phase_end = 0;
             continue;
         }
-        if (ph.type == 'E') {
+        if (ph.type() == 'E') {
             for (size_t i = 0; i < np; ++i) {
-                const uint32_t s = ph.pairs[2 * i], e = ph.pairs[2 * i + 1];
+                const uint32_t s = ph.pair(2 * i), e = ph.pair(2 * i + 1);
                 if (col[s] < 0) return fail(GVA_ERR_FORMAT, "extension from an unmatched vertex");
                 int bc = -1;
-                if (plan.restricts[e] != kNone) {
-                    bc = col[plan.restricts[e]];
+                if (plan.restrict_of(e) != kNone) {
+                    bc = col[plan.restrict_of(e)];
                     if (bc < 0) return fail(GVA_ERR_FORMAT, "restriction names an unmatched vertex");
                 }
-                ext(ph.edge_label, s, e, bc, false, same_label_cols(e));
+                ext(ph.edge_label(), s, e, bc, false, same_label_cols(e));
             }
         } else {
             // fold into the previous extension when every pair touches its new vertex
@@ -447,19 +487,19 @@ int lower_plan(const Plan& plan, const HostGraph& g, std::vector<Step>& steps, b
                 !steps.back().always_empty && np <= 8 - steps.back().n_chk && np <= GVA_MAX_REDUCE_PAIRS) {
                 bool ok = true;
                 for (size_t i = 0; i < np && ok; ++i)
-                    ok = (int)ph.pairs[2 * i] == newest || (int)ph.pairs[2 * i + 1] == newest;
+                    ok = (int)ph.pair(2 * i) == newest || (int)ph.pair(2 * i + 1) == newest;
                 if (ok) {
                     Step& st = steps.back();
-                    const uint32_t part = part_of(ph.edge_label);
+                    const uint32_t part = part_of(ph.edge_label());
                     if (part == 0) st.always_empty = 1;
                     for (size_t i = 0; i < np; ++i) {
-                        const uint32_t a = ph.pairs[2 * i], b = ph.pairs[2 * i + 1];
+                        const uint32_t a = ph.pair(2 * i), b = ph.pair(2 * i + 1);
                         const bool new_is_b = (int)b == newest;  // pair checks b in adj(a) with label(b)
                         const uint32_t other = new_is_b ? a : b;
                         st.chk_col[st.n_chk] = (uint8_t)col[other];
                         st.chk_dir[st.n_chk] = new_is_b ? 0 : 1;
                         st.chk_part[st.n_chk] = part;
-                        st.chk_lab[st.n_chk] = g.dense_label(plan.qlabel[b]);
+                        st.chk_lab[st.n_chk] = g.dense_label(plan.qlabel(b));
                         if (st.chk_lab[st.n_chk] == kNone) st.always_empty = 1;
                         st.n_chk++;
                     }
@@ -470,17 +510,17 @@ int lower_plan(const Plan& plan, const HostGraph& g, std::vector<Step>& steps, b
             Step st;
             st.kind = STEP_REDUCE;
             st.width_in = (uint32_t)width;
-            st.part = part_of(ph.edge_label);
+            st.part = part_of(ph.edge_label());
             if (np > GVA_MAX_REDUCE_PAIRS) {
                 st.always_empty = 1;
             } else {
                 st.n_pairs = (uint32_t)np;
                 for (size_t i = 0; i < np; ++i) {
-                    const uint32_t a = ph.pairs[2 * i], b = ph.pairs[2 * i + 1];
+                    const uint32_t a = ph.pair(2 * i), b = ph.pair(2 * i + 1);
                     if (col[a] < 0 || col[b] < 0) return fail(GVA_ERR_FORMAT, "reduction over an unmatched vertex");
                     st.rs_col[i] = (uint8_t)col[a];
                     st.re_col[i] = (uint8_t)col[b];
-                    st.re_label[i] = g.dense_label(plan.qlabel[b]);
+                    st.re_label[i] = g.dense_label(plan.qlabel(b));
                     if (st.re_label[i] == kNone) st.always_empty = 1;
                 }
                 if (st.part == 0) st.always_empty = 1;
@@ -490,6 +530,16 @@ int lower_plan(const Plan& plan, const HostGraph& g, std::vector<Step>& steps, b
         steps.back().phase_end = (int)pi;
     }
     return GVA_OK;
+}
+
+int lower_plan(const Plan& plan, const HostGraph& g, std::vector<Step>& steps, bool fuse_reductions) {
+    return lower_core(PlanView{plan}, g, steps, fuse_reductions);
+}
+
+int lower_dplan(const DPlan& plan, const uint32_t* labels, const HostGraph& g, std::vector<Step>& steps,
+                bool fuse_reductions) {
+    if (plan.status != DPLAN_OK) return fail(GVA_ERR_ARG, "query was left to the host planner");
+    return lower_core(DPlanView{plan, labels}, g, steps, fuse_reductions);
 }
 
 }  // namespace gva

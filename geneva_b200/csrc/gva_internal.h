@@ -141,6 +141,10 @@ struct Step {
 // just added into that extension (same final rows, fewer steps; per-phase
 // counts of the folded phases are then not observable).
 int lower_plan(const Plan& plan, const HostGraph& g, std::vector<Step>& steps, bool fuse_reductions = false);
+// The same steps for a plan of the heap-free planner (status DPLAN_OK) over
+// the query's labels, without building the host plan.
+int lower_dplan(const DPlan& plan, const uint32_t* labels, const HostGraph& g, std::vector<Step>& steps,
+                bool fuse_reductions = false);
 
 // ---------------------------------------------------------------- mining ---
 struct MinedPattern {

@@ -95,10 +95,14 @@ int run_mine(DevDB& db, cudaStream_t s, uint64_t budget, uint32_t max_edges, uin
                         dq->l[e] = sdl[3 * e + 2] = c.edges[e].el;
                     }
                     dplan(*dq, *dp);
-                    Plan plan;
-                    int r = dp->status == DPLAN_OK ? plan_from_dplan(*dp, dq->label, plan)
-                                                   : plan_from_query(c.n, dq->label, sdl, c.ne, GVA_MODE_DV, plan);
-                    if (!r) r = lower_plan(plan, db.meta, steps[i - b0], true);
+                    int r;
+                    if (dp->status == DPLAN_OK) {
+                        r = lower_dplan(*dp, dq->label, db.meta, steps[i - b0], true);
+                    } else {
+                        Plan plan;
+                        r = plan_from_query(c.n, dq->label, sdl, c.ne, GVA_MODE_DV, plan);
+                        if (!r) r = lower_plan(plan, db.meta, steps[i - b0], true);
+                    }
                     if (r) {
                         rcs[t] = r;
                         msgs[t] = last_error_cstr();

@@ -4,7 +4,8 @@
 // query dplan accepts must get the host planner's plan (phases, pair
 // orientation, restrictions, repeat flags, record stats, columns); the others
 // must be ones it may leave to the host (a list longer than 16 entries, a
-// capacity, or a query the host planner rejects).
+// capacity, or a query the host planner rejects).  Its plans lowered
+// directly (lower_dplan) must give the host plan's steps.
 //
 // usage: dplan_check queries seed max_vertices
 #include <cstdio>
@@ -32,6 +33,15 @@ int main(int argc, char** argv) {
     };
     static DPlanQuery dq;
     static DPlan dp;
+    // a database with labels 1..4 and partitions 1..3, for lowering
+    HostGraph g;
+    {
+        std::vector<uint32_t> vl(13), sv, dv, el;
+        for (uint32_t v = 1; v <= 12; ++v) vl[v] = 1 + (v - 1) % 4;
+        for (uint32_t v = 1; v <= 12; ++v)
+            for (uint32_t u = v + 1; u <= 12; ++u) sv.push_back(v), dv.push_back(u), el.push_back(1 + (u + v) % 3);
+        if (graph_from_edges(vl.data(), 12, sv.data(), dv.data(), el.data(), sv.size(), g)) return 2;
+    }
     int accepted = 0, host_only = 0;
     for (int qi = 0; qi < nq; ++qi) {
         const uint32_t n = 2 + rnd() % (maxv - 1), nl = 1 + rnd() % 4, nel = 1 + rnd() % 3;
@@ -79,6 +89,12 @@ int main(int argc, char** argv) {
                 t += "e " + std::to_string(dq.s[i]) + " " + std::to_string(dq.d[i]) + " " + std::to_string(dq.l[i]) + "\n";
             printf("query %d: plans differ\n%s--- host\n%s--- dplan\n%s", qi, t.c_str(), want.describe().c_str(),
                    got.describe().c_str());
+            return 1;
+        }
+        std::vector<Step> sa, sb;
+        if (lower_plan(want, g, sa, true) || lower_dplan(dp, dq.label, g, sb, true) || sa.size() != sb.size() ||
+            (!sa.empty() && std::memcmp(sa.data(), sb.data(), sa.size() * sizeof(Step)) != 0)) {
+            printf("query %d: lowered steps differ\n", qi);
             return 1;
         }
         ++accepted;
