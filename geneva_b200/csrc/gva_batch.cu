@@ -564,13 +564,17 @@ int BatchSession::submit(const std::vector<std::vector<Step>>& steps, const std:
     if (!presorted) index.reserve(steps.size() * 4);
     const int first_node = (int)nodes.size();
     uint8_t kb[512], kb2[512];
-    {  // room for the wave: a plan mostly adds a node or two past its shared prefix
+    {  // room for the wave (a plan mostly adds a node or two past its shared
+       // prefix), growing geometrically: a session may take many waves
         size_t total = 0;
         for (const auto& st : steps) total += st.size();
         const size_t guess = std::min(total, 2 * steps.size() + 64);
-        nodes.reserve(nodes.size() + guess);
-        node_steps.reserve(node_steps.size() + guess);
-        plans.reserve(plans.size() + steps.size());
+        auto room = [](auto& v, size_t more) {
+            if (v.capacity() < v.size() + more) v.reserve(std::max(v.size() + more, 2 * v.capacity()));
+        };
+        room(nodes, guess);
+        room(node_steps, guess);
+        room(plans, steps.size());
     }
     // a new node for step `st` at `depth` under `parent` (-1: a root)
     auto new_node = [&](const Step& st, int parent, int depth) {
