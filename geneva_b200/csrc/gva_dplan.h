@@ -7,9 +7,10 @@
 // insertion sort, which is what libstdc++'s std::sort does for 16 entries or
 // fewer; a query whose edge, neighbour or back-edge lists grow longer, or
 // that exceeds a fixed capacity below, is answered with DPLAN_HOST and left
-// to the host planner.  Restrictions are gathered while automorphisms are
-// enumerated: an automorphism contributes only at the first vertex (in plan
-// order) that it moves, so none has to be stored.
+// to the host planner, as is one whose automorphism search grows past fixed
+// bounds (so that a call's time is bounded).  Restrictions are gathered
+// while automorphisms are enumerated: an automorphism contributes only at the
+// first vertex (in plan order) that it moves, so none has to be stored.
 #pragma once
 
 #include <cstdint>
@@ -29,7 +30,8 @@ constexpr int kDpPhases = 96;     // E phases <= vertices, R phases <= edges
 constexpr int kDpPairs = 256;     // vertex ids over all phases
 constexpr int kDpKeys = 256;      // (edge label, vertex label) keys
 constexpr int kDpSort = 16;       // longest list sorted as std::sort would
-constexpr uint64_t kDpMaxAut = 1u << 20;  // automorphisms enumerated at most
+constexpr uint64_t kDpMaxAut = 1u << 20;    // automorphisms enumerated at most
+constexpr uint64_t kDpMaxSearch = 1u << 22;  // partial maps tried at most (bounds the search's time)
 
 enum : uint32_t { DPLAN_OK = 0, DPLAN_HOST = 1 };
 
@@ -570,7 +572,7 @@ struct DPlanner {
         for (uint32_t v = 0; v <= n; ++v) out.restricts[v] = kDpNone;
         // depth-first over partial maps cand[0..depth) (vertex i -> cand[i])
         uint32_t cand[kDpV], nextv[kDpV], used = 0;
-        uint64_t found = 0;
+        uint64_t found = 0, tried = 0;
         uint32_t depth = 0;
         nextv[0] = 0;
         bool identity[kDpV + 1];  // the map so far is the identity
@@ -588,6 +590,7 @@ struct DPlanner {
                 nextv[depth] = v + 1;
                 continue;
             }
+            if (++tried > kDpMaxSearch) return false;
             bool ok = (eq[depth] >> v) & 1;
             for (uint32_t i = 0; i < depth && ok; ++i) ok = E(i, depth) == E(cand[i], v);
             if (depth + 1 == n) {
