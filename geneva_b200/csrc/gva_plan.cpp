@@ -143,6 +143,8 @@ public:
     FlatMap<ReduceKey> red_keys;
     std::vector<uint32_t> auts;  // automorphisms, n entries each
     uint32_t eqmask[32] = {};    // eqmask[a] bit b: equivalent(a, b)
+    uint64_t aut_steps = 0;      // vertex tries of the automorphism search
+    bool aut_over = false;       // the search passed its bounds
 
     uint32_t E(uint32_t a, uint32_t b) const { return adj[(size_t)a * n + b]; }
     static uint64_t key(uint32_t el, uint32_t vl) { return ((uint64_t)el << 32) | vl; }
@@ -472,7 +474,13 @@ bool Planner::possible(const std::vector<uint32_t>& cand, uint32_t nid) const {
 }
 
 // src/genMatchOrderCPU.cpp:433-462: every non-identity automorphism.
+// The reference enumerates without bound; here a query whose search passes
+// kMaxAutSteps vertex tries or kMaxAuts automorphisms is rejected instead of
+// holding the caller (and memory) indefinitely.
+constexpr uint64_t kMaxAutSteps = 1ull << 27, kMaxAuts = 1ull << 20;
+
 void Planner::automorphisms(std::vector<uint32_t>& cand, bool identity) {
+    if (aut_over) return;
     uint32_t used = 0;
     for (uint32_t v : cand) used |= bit(v);
     if (cand.size() + 1 == n) {
@@ -480,6 +488,10 @@ void Planner::automorphisms(std::vector<uint32_t>& cand, bool identity) {
             if (used & bit(v)) continue;
             if (identity && v == cand.size()) return;
             if (possible(cand, v)) {
+                if (auts.size() / n >= kMaxAuts) {
+                    aut_over = true;
+                    return;
+                }
                 cand.push_back(v);
                 auts.insert(auts.end(), cand.begin(), cand.end());
                 cand.pop_back();
@@ -488,8 +500,12 @@ void Planner::automorphisms(std::vector<uint32_t>& cand, bool identity) {
         }
         return;
     }
-    for (uint32_t v = 0; v < n; ++v) {
+    for (uint32_t v = 0; v < n && !aut_over; ++v) {
         if (used & bit(v)) continue;
+        if (++aut_steps > kMaxAutSteps) {
+            aut_over = true;
+            return;
+        }
         if (!possible(cand, v)) continue;
         bool id = identity && v == cand.size();
         cand.push_back(v);
@@ -721,6 +737,7 @@ int Planner::run(Plan& out) {
     std::vector<uint32_t> cand;
     cand.reserve(n);
     automorphisms(cand, true);
+    if (aut_over) return fail(GVA_ERR_UNSUPPORTED, "query has too many symmetric vertex maps to enumerate");
     rearrange(out);
     restrictions(out);
     return GVA_OK;

@@ -65,6 +65,24 @@ def test_planner_errors(native, text, status):
     assert ei.value.status in (2, 6)
 
 
+def test_huge_symmetry_is_rejected_not_enumerated(native):
+    """A 14-vertex clique of one label has 14! automorphisms: the reference
+    would enumerate them for ever; the planner stops at a bound and reports
+    the query as unsupported, quickly."""
+    import time
+    n = 14
+    text = "".join(f"v {i} 1\n" for i in range(n)) + "".join(
+        f"e {i} {j} 1\n" for i in range(n) for j in range(i + 1, n))
+    t0 = time.perf_counter()
+    with pytest.raises(gv.GenevaError) as e:
+        gv.Plan.from_text(text)
+    assert e.value.status == 6 and "symmetric" in str(e.value)
+    assert time.perf_counter() - t0 < 30
+    # symmetric but small: planned as usual (a 7-vertex star, 6! automorphisms)
+    star = "".join(f"v {i} 1\n" for i in range(7)) + "".join(f"e 0 {j} 1\n" for j in range(1, 7))
+    assert gv.Plan.from_text(star).num_phases > 0
+
+
 def test_bad_mode_rejected(native):
     with pytest.raises(gv.GenevaError) as ei:
         gv.Plan.from_text("v 0 1\nv 1 1\ne 0 1 1\n", 7)
