@@ -52,8 +52,9 @@ struct Pattern {
 // (n, vertex labels, upper-triangle edge labels) over vertex orders that sort
 // vertices by an isomorphism-invariant key (label, degree, hash of the sorted
 // (edge label, neighbour label) list); only orders within equal-key cells are
-// tried.  Equal keys of non-equivalent vertices only enlarge a cell, which
-// costs time, not correctness.  Values are written `width` bytes each (1 when
+// tried, and twins (interchangeable by an automorphism) in one fixed order.
+// Equal keys of non-equivalent vertices only enlarge a cell, which costs
+// time, not correctness.  Values are written `width` bytes each (1 when
 // labels and edge labels fit a byte).
 struct CodeBuf {
     uint32_t len = 0;  // bytes
@@ -112,6 +113,52 @@ void canonical(const Pattern& p, uint32_t width, CodeBuf& out, uint32_t* order_o
         ce[nc++] = j;
         i = j;
     }
+    // twins (same label, same edge label to every other vertex) can be
+    // swapped by an automorphism, which leaves every code unchanged: orders
+    // that differ only in how twins are placed give the same code, so cells
+    // are permuted as multisets of twin classes, each class filled with its
+    // vertices in ascending id (a star's k equal leaves: one order, not k!)
+    uint32_t cls[GVA_MAX_QUERY_VERTICES];      // twin class at each position
+    uint32_t members[GVA_MAX_QUERY_VERTICES];  // class c: members[mat[c] .. mat[c] + mcnt[c]), ascending id
+    uint32_t mat[GVA_MAX_QUERY_VERTICES], mcnt[GVA_MAX_QUERY_VERTICES], ncls = 0;
+    if (!trivial) {
+        uint32_t vcls[GVA_MAX_QUERY_VERTICES], rep[GVA_MAX_QUERY_VERTICES];  // rep: a class's first vertex
+        for (uint32_t c = 0; c < nc; ++c) {
+            const uint32_t first = ncls;
+            for (uint32_t i = cb[c]; i < ce[c]; ++i) {  // ascending id within the cell
+                const uint32_t v = ord[i];
+                uint32_t k = first;
+                for (; k < ncls; ++k) {
+                    const uint32_t u = rep[k];
+                    bool twin = p.vl[u] == p.vl[v];
+                    for (uint32_t w = 0; w < n && twin; ++w)
+                        if (w != u && w != v) twin = adj[u][w] == adj[v][w];
+                    if (twin) break;
+                }
+                if (k == ncls) {
+                    rep[k] = v;
+                    mcnt[k] = 0;
+                    ++ncls;
+                }
+                vcls[i] = k;
+            }
+            // lay the cell's classes out contiguously, members in ascending id
+            uint32_t at = cb[c];
+            for (uint32_t k = first; k < ncls; ++k) {
+                mat[k] = at;
+                for (uint32_t i = cb[c]; i < ce[c]; ++i)
+                    if (vcls[i] == k) members[at++] = ord[i], mcnt[k]++;
+            }
+            for (uint32_t k = first, i = cb[c]; k < ncls; ++k)
+                for (uint32_t m = 0; m < mcnt[k]; ++m) cls[i++] = k;  // ascending: the first arrangement
+        }
+    }
+    auto arrange = [&]() {  // ord from the class arrangement
+        uint32_t used_of[GVA_MAX_QUERY_VERTICES];
+        for (uint32_t k = 0; k < ncls; ++k) used_of[k] = 0;
+        for (uint32_t i = 0; i < n; ++i) ord[i] = members[mat[cls[i]] + used_of[cls[i]]++];
+    };
+    if (!trivial) arrange();
     const uint32_t len = 1 + n + n * (n - 1) / 2;
     uint32_t best[kMaxCode], cur[kMaxCode];
     uint32_t best_ord[GVA_MAX_QUERY_VERTICES];
@@ -138,8 +185,9 @@ void canonical(const Pattern& p, uint32_t width, CodeBuf& out, uint32_t* order_o
         if (trivial) break;
         int c = (int)nc - 1;
         for (; c >= 0; --c)
-            if (std::next_permutation(ord + cb[c], ord + ce[c])) break;
+            if (std::next_permutation(cls + cb[c], cls + ce[c])) break;
         if (c < 0) break;
+        arrange();
     }
     if (order_out) std::memcpy(order_out, best_ord, sizeof(uint32_t) * n);
     out.len = len * width;

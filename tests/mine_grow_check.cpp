@@ -17,8 +17,10 @@
 // their supports, over the original labels.
 //
 // usage: mine_grow_check L P max_edges seed threshold threads
+#include <algorithm>
 #include <cstdio>
 #include <cstdlib>
+#include <cstring>
 #include <map>
 #include <random>
 #include <set>
@@ -82,12 +84,73 @@ Pattern without(const Pattern& p, uint32_t skip) {
 
 }  // namespace
 
+// Canonical codes of large symmetric patterns (stars and cliques beyond what
+// the brute force can enumerate, a double star) must not depend on the
+// vertex numbering.  Twins make stars and cliques fast; equivalent vertices
+// that are not twins (the two leaf sets of a double star) are still searched
+// over all their arrangements.
+int symmetric_check(std::mt19937& rng) {
+    auto shuffled = [&](const Pattern& p) {
+        uint32_t perm[GVA_MAX_QUERY_VERTICES];
+        for (uint32_t i = 0; i < p.n; ++i) perm[i] = i;
+        std::shuffle(perm, perm + p.n, rng);
+        Pattern q;
+        q.n = p.n;
+        for (uint32_t v = 0; v < p.n; ++v) q.vl[perm[v]] = p.vl[v];
+        for (uint32_t e = 0; e < p.ne; ++e) q.add_edge(perm[p.edges[e].u], perm[p.edges[e].v], p.edges[e].el);
+        return q;
+    };
+    std::vector<Pattern> pats;
+    for (uint32_t k : {8u, 16u, 24u, 31u}) {  // stars, one leaf label or two
+        for (uint32_t two = 0; two < 2; ++two) {
+            Pattern p;
+            p.n = k + 1;
+            p.vl[0] = 0;
+            for (uint32_t v = 1; v <= k; ++v) p.vl[v] = two ? v % 2 : 0, p.add_edge(0, v, 1);
+            pats.push_back(p);
+        }
+    }
+    for (uint32_t k : {6u, 8u}) {  // cliques (k(k-1)/2 <= 31 edges)
+        Pattern p;
+        p.n = k;
+        for (uint32_t v = 0; v < k; ++v) p.vl[v] = 0;
+        for (uint32_t a = 0; a < k; ++a)
+            for (uint32_t b = a + 1; b < k; ++b) p.add_edge(a, b, 1);
+        pats.push_back(p);
+    }
+    {  // double star: two centres, 6 equal leaves each (leaves of different
+       // centres share a cell but are not twins: C(12, 6) arrangements)
+        Pattern p;
+        p.n = 14;
+        for (uint32_t v = 0; v < 14; ++v) p.vl[v] = 0;
+        p.add_edge(0, 1, 2);
+        for (uint32_t v = 2; v < 14; ++v) p.add_edge(v < 8 ? 0 : 1, v, 1);
+        pats.push_back(p);
+    }
+    CodeBuf a, b;
+    for (const Pattern& p : pats) {
+        canonical(p, 1, a);
+        for (int r = 0; r < 5; ++r) {
+            canonical(shuffled(p), 1, b);
+            if (a.len != b.len || std::memcmp(a.b, b.b, a.len) != 0) {
+                printf("symmetric pattern of %u vertices: code depends on the numbering\n", p.n);
+                return 1;
+            }
+        }
+    }
+    return 0;
+}
+
 int main(int argc, char** argv) {
     if (argc < 7) return 2;
     const uint32_t L = atoi(argv[1]), P = atoi(argv[2]), max_edges = atoi(argv[3]);
     const uint32_t seed = atoi(argv[4]);
     const double thr = atof(argv[5]);
     const unsigned nthreads = atoi(argv[6]);
+    {
+        std::mt19937 srng(seed + 1000);  // its own stream: the supports below stay the same
+        if (symmetric_check(srng)) return 1;
+    }
     std::mt19937 rng(seed);
     std::uniform_real_distribution<double> uni(0.3, 1.0);
     std::vector<double> w((size_t)L * L * (P + 1));
