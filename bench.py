@@ -41,6 +41,7 @@ import argparse
 import json
 import os
 import statistics
+import shutil
 import subprocess
 import sys
 import tempfile
@@ -194,68 +195,71 @@ def reference_arm(args, db, queries, workload):
     if not (ref / "cpumine").exists() or not (ref / "genDatabase").exists():
         return {"impl": "reference", "unavailable": "oracle/_ref binaries not built (reference sources absent at build)"}
     work = Path(tempfile.mkdtemp(prefix="geneva_ref_"))
-    (work / "datasets").mkdir()
-    (work / "run").mkdir()
-    (work / "datasets" / f"{db.name}.g").write_text(db.to_g_text())
-    t_conv = time.perf_counter()
-    subprocess.run([str(ref / "genDatabase"), db.name], cwd=work / "run", check=True,
-                   stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
-    t_conv = time.perf_counter() - t_conv
-    ds = work / "datasets"
-    reorder = work / "run" / f"{db.name}.reorder"
-    meta = np.loadtxt(ds / f"{db.name}.metadata", dtype=np.int64)  # new id, label, old id (0-based .g id)
-    new_to_old = np.zeros(int(meta[:, 0].max()) + 1, dtype=np.int64)
-    new_to_old[meta[:, 0]] = meta[:, 2]
-    cores = os.cpu_count() or 1
-    wave = max(1, min(cores, len(queries), 64))  # one cpumine process per host core
+    try:
+        (work / "datasets").mkdir()
+        (work / "run").mkdir()
+        (work / "datasets" / f"{db.name}.g").write_text(db.to_g_text())
+        t_conv = time.perf_counter()
+        subprocess.run([str(ref / "genDatabase"), db.name], cwd=work / "run", check=True,
+                       stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
+        t_conv = time.perf_counter() - t_conv
+        ds = work / "datasets"
+        reorder = work / "run" / f"{db.name}.reorder"
+        meta = np.loadtxt(ds / f"{db.name}.metadata", dtype=np.int64)  # new id, label, old id (0-based .g id)
+        new_to_old = np.zeros(int(meta[:, 0].max()) + 1, dtype=np.int64)
+        new_to_old[meta[:, 0]] = meta[:, 2]
+        cores = os.cpu_count() or 1
+        wave = max(1, min(cores, len(queries), 64))  # one cpumine process per host core
 
-    def one(i_q):
-        i, q = i_q
-        d = work / f"q{i}"
-        d.mkdir(exist_ok=True)
-        (d / "q.query").write_text(q)
-        subprocess.run([str(ref / "cpumine"), str(reorder), "q.query", str(ds / f"{db.name}.mygraph"),
-                        str(ds / f"{db.name}.metadata")], cwd=d, stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL,
-                       check=True)
-        rows = [l.split() for l in open(d / "partialResultsCPU.txt") if l.strip()]
-        if not rows:
-            return 0, 0
-        r = np.unique(np.array(rows, dtype=np.int64), axis=0)  # cpumine repeats rows via index vertices
-        support = len(np.unique(db.graph_of(new_to_old[r[:, 0]] + 1)))
-        return r.shape[0], support
+        def one(i_q):
+            i, q = i_q
+            d = work / f"q{i}"
+            d.mkdir(exist_ok=True)
+            (d / "q.query").write_text(q)
+            subprocess.run([str(ref / "cpumine"), str(reorder), "q.query", str(ds / f"{db.name}.mygraph"),
+                            str(ds / f"{db.name}.metadata")], cwd=d, stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL,
+                           check=True)
+            rows = [l.split() for l in open(d / "partialResultsCPU.txt") if l.strip()]
+            if not rows:
+                return 0, 0
+            r = np.unique(np.array(rows, dtype=np.int64), axis=0)  # cpumine repeats rows via index vertices
+            support = len(np.unique(db.graph_of(new_to_old[r[:, 0]] + 1)))
+            return r.shape[0], support
 
-    steps_done = [0]
+        steps_done = [0]
 
-    def step():
-        k = steps_done[0]
-        steps_done[0] += 1
-        batch = [(k * wave + j, queries[(k * wave + j) % len(queries)]) for j in range(wave)]
-        t0 = time.perf_counter()
-        with ThreadPoolExecutor(max_workers=wave) as ex:
-            res = list(ex.map(one, batch))
-        return sum(r for r, _ in res), len(res), time.perf_counter() - t0
+        def step():
+            k = steps_done[0]
+            steps_done[0] += 1
+            batch = [(k * wave + j, queries[(k * wave + j) % len(queries)]) for j in range(wave)]
+            t0 = time.perf_counter()
+            with ThreadPoolExecutor(max_workers=wave) as ex:
+                res = list(ex.map(one, batch))
+            return sum(r for r, _ in res), len(res), time.perf_counter() - t0
 
-    for _ in range(args.warmup):
-        step()
-    tot_rows, tot_pats, tot_t = 0, 0, 0.0
-    for _ in range(args.steps):
-        r, n, t = step()
-        tot_rows += r
-        tot_pats += n
-        tot_t += t
-    value = tot_rows / tot_t
-    return {
-        "metric": "embeddings/s", "value": value, "unit": "embeddings/s", "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * tot_t / args.steps,
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
-        "impl": "reference", "patterns_per_s": tot_pats / tot_t,
-        "config": {"workload": workload, "seed": db.params.get("seed", args.seed), "patterns_per_step": wave,
-                   "database_conversion_s": t_conv},
-        "cpu_baseline": {"value": value, "unit": "embeddings/s", "cores": wave, "kind": "reference",
-                         "sample": f"{wave} seeded patterns per step sampled from the {db.name} database, one "
-                                   f"cpumine process each (it reloads the database per pattern)"},
-        "e2e": {"value": value, "unit": "embeddings/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-    }
+        for _ in range(args.warmup):
+            step()
+        tot_rows, tot_pats, tot_t = 0, 0, 0.0
+        for _ in range(args.steps):
+            r, n, t = step()
+            tot_rows += r
+            tot_pats += n
+            tot_t += t
+        value = tot_rows / tot_t
+        return {
+            "metric": "embeddings/s", "value": value, "unit": "embeddings/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * tot_t / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
+            "impl": "reference", "patterns_per_s": tot_pats / tot_t,
+            "config": {"workload": workload, "seed": db.params.get("seed", args.seed), "patterns_per_step": wave,
+                       "database_conversion_s": t_conv},
+            "cpu_baseline": {"value": value, "unit": "embeddings/s", "cores": wave, "kind": "reference",
+                             "sample": f"{wave} seeded patterns per step sampled from the {db.name} database, one "
+                                       f"cpumine process each (it reloads the database per pattern)"},
+            "e2e": {"value": value, "unit": "embeddings/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        }
+    finally:
+        shutil.rmtree(work, ignore_errors=True)  # the converted database and per-pattern outputs
 
 
 # -------------------------------------------------------------- serving arm ----
