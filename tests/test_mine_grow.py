@@ -27,6 +27,7 @@ CASES = [
     (2, 3, 4, 4, 0.05, 3),      # several edge labels between the same vertex labels
     (1, 1, 6, 2, 0.0, 4),       # unlabelled: every connected graph up to 6 edges (large symmetric cells)
     (260, 1, 4, 11, 0.999, 4),  # more than 256 labels: 2-byte codes
+    (3, 2, 4, 5, 0.2, 1),       # one host thread
 ]
 
 
