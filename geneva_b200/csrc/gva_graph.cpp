@@ -264,90 +264,103 @@ int graph_from_edges(const uint32_t* vlabels, uint32_t max_id, const uint32_t* s
     const unsigned nth = std::max(1u, std::min(64u, std::thread::hardware_concurrency()));
     const uint64_t V = (uint64_t)max_id + 1;
     g.parts.resize(P);
-    // every partition's entries bucketed by source in one pass over the edges:
-    // pos_all[p - 1][v] is where vertex v's bucket starts in keys_all[p - 1]
-    std::vector<std::vector<uint64_t>> pos_all(P, std::vector<uint64_t>(V + 1, 0)), keys_all(P);
-    for (uint64_t i = 0; i < ne; ++i) {
-        std::vector<uint64_t>& c = pos_all[elabel[i] - 1];
-        c[src[i] + 1]++, c[dst[i] + 1]++;
-    }
-    for (uint32_t p = 0; p < P; ++p) {
-        std::vector<uint64_t>& c = pos_all[p];
-        for (uint64_t v = 0; v < V; ++v) c[v + 1] += c[v];
-        keys_all[p].resize(c[V]);
-    }
-    {
-        std::vector<std::vector<uint64_t>> cur(P);
-        for (uint32_t p = 0; p < P; ++p) cur[p].assign(pos_all[p].begin(), pos_all[p].end() - 1);
-        for (uint64_t i = 0; i < ne; ++i) {  // (dense label << 32) | neighbour
-            const uint32_t p = elabel[i] - 1;
-            keys_all[p][cur[p][src[i]]++] = ((uint64_t)g.dlabel[dst[i]] << 32) | dst[i];
-            keys_all[p][cur[p][dst[i]]++] = ((uint64_t)g.dlabel[src[i]] << 32) | src[i];
-        }
-    }
+    // Edge labels in groups whose bucket tables and entries stay within a
+    // memory bound; each group's entries are bucketed by source in one
+    // counting and one scatter pass over the edges: pos_all[p - p0][v] is
+    // where vertex v's bucket starts in keys_all[p - p0]
+    std::vector<uint64_t> per_label(P + 1, 0);
+    for (uint64_t i = 0; i < ne; ++i) per_label[elabel[i]]++;
+    constexpr uint64_t kGroupBytes = 1ull << 30;
     std::vector<uint64_t> len(V), start(V);
-    for (uint32_t p = 1; p <= P; ++p) {
-        const std::vector<uint64_t>& pos = pos_all[p - 1];
-        std::vector<uint64_t> keys;
-        keys.swap(keys_all[p - 1]);
-        auto sort_range = [&](uint64_t v0, uint64_t v1) {
-            for (uint64_t v = v0; v < v1; ++v) {
-                uint64_t* a = keys.data() + pos[v];
-                uint64_t* b = keys.data() + pos[v + 1];
-                std::sort(a, b);
-                len[v] = (uint64_t)(std::unique(a, b) - a);
-            }
-        };
-        if (nth == 1 || keys.size() < (1u << 16)) {
-            sort_range(0, V);
-        } else {
-            // vertex ranges of about equal entry counts
-            std::vector<std::thread> pool;
-            uint64_t v0 = 0;
-            for (unsigned t = 0; t < nth; ++t) {
-                const uint64_t target = pos[V] * (t + 1) / nth;
-                uint64_t v1 = t + 1 == nth ? V : (uint64_t)(std::lower_bound(pos.begin(), pos.end(), target) - pos.begin());
-                v1 = std::min(std::max(v1, v0), V);
-                pool.emplace_back(sort_range, v0, v1);
-                v0 = v1;
-            }
-            for (auto& th : pool) th.join();
+    for (uint32_t p0 = 1, p1; p0 <= P; p0 = p1 + 1) {
+        uint64_t bytes = (V + 1) * 8 + 16 * per_label[p0];
+        for (p1 = p0; p1 < P && bytes + (V + 1) * 8 + 16 * per_label[p1 + 1] <= kGroupBytes; ++p1)
+            bytes += (V + 1) * 8 + 16 * per_label[p1 + 1];
+        const uint32_t G = p1 - p0 + 1;
+        std::vector<std::vector<uint64_t>> pos_all(G, std::vector<uint64_t>(V + 1, 0)), keys_all(G);
+        for (uint64_t i = 0; i < ne; ++i) {
+            if (elabel[i] < p0 || elabel[i] > p1) continue;
+            std::vector<uint64_t>& c = pos_all[elabel[i] - p0];
+            c[src[i] + 1]++, c[dst[i] + 1]++;
         }
-        uint64_t total = 0;  // start[v]: where vertex v's list starts in adj
-        for (uint64_t v = 0; v < V; ++v) {
-            const uint64_t l = len[v];
-            start[v] = total;
-            total += l;
+        for (uint32_t q = 0; q < G; ++q) {
+            std::vector<uint64_t>& c = pos_all[q];
+            for (uint64_t v = 0; v < V; ++v) c[v + 1] += c[v];
+            keys_all[q].resize(c[V]);
         }
-        if (total >= 0xffffffffull) return fail(GVA_ERR_UNSUPPORTED, "partition has 2^32 or more adjacency entries");
-        HostPartition& part = g.parts[p - 1];
-        part.edge_label = p;
-        part.off.resize(entries);  // group (v, l) starts at off[v * L + l]
-        part.adj.resize(total);
-        // each vertex's offsets and list, written by vertex ranges: its list
-        // is sorted by label, so group l starts after the entries of labels < l
-        auto fill_range = [&](uint64_t v0, uint64_t v1) {
-            for (uint64_t v = v0; v < v1; ++v) {
-                const uint64_t* a = keys.data() + pos[v];
-                const uint64_t at = start[v], n = len[v];
-                uint64_t j = 0;
-                for (uint64_t l = 0; l < L; ++l) {
-                    part.off[v * L + l] = (uint32_t)(at + j);
-                    while (j < n && (a[j] >> 32) == l) {
-                        part.adj[at + j] = (uint32_t)a[j];
-                        ++j;
+        {
+            std::vector<std::vector<uint64_t>> cur(G);
+            for (uint32_t q = 0; q < G; ++q) cur[q].assign(pos_all[q].begin(), pos_all[q].end() - 1);
+            for (uint64_t i = 0; i < ne; ++i) {  // (dense label << 32) | neighbour
+                if (elabel[i] < p0 || elabel[i] > p1) continue;
+                const uint32_t q = elabel[i] - p0;
+                keys_all[q][cur[q][src[i]]++] = ((uint64_t)g.dlabel[dst[i]] << 32) | dst[i];
+                keys_all[q][cur[q][dst[i]]++] = ((uint64_t)g.dlabel[src[i]] << 32) | src[i];
+            }
+        }
+        for (uint32_t p = p0; p <= p1; ++p) {
+            const std::vector<uint64_t>& pos = pos_all[p - p0];
+            std::vector<uint64_t> keys;
+            keys.swap(keys_all[p - p0]);
+            auto sort_range = [&](uint64_t v0, uint64_t v1) {
+                for (uint64_t v = v0; v < v1; ++v) {
+                    uint64_t* a = keys.data() + pos[v];
+                    uint64_t* b = keys.data() + pos[v + 1];
+                    std::sort(a, b);
+                    len[v] = (uint64_t)(std::unique(a, b) - a);
+                }
+            };
+            if (nth == 1 || keys.size() < (1u << 16)) {
+                sort_range(0, V);
+            } else {
+                // vertex ranges of about equal entry counts
+                std::vector<std::thread> pool;
+                uint64_t v0 = 0;
+                for (unsigned t = 0; t < nth; ++t) {
+                    const uint64_t target = pos[V] * (t + 1) / nth;
+                    uint64_t v1 = t + 1 == nth ? V : (uint64_t)(std::lower_bound(pos.begin(), pos.end(), target) - pos.begin());
+                    v1 = std::min(std::max(v1, v0), V);
+                    pool.emplace_back(sort_range, v0, v1);
+                    v0 = v1;
+                }
+                for (auto& th : pool) th.join();
+            }
+            uint64_t total = 0;  // start[v]: where vertex v's list starts in adj
+            for (uint64_t v = 0; v < V; ++v) {
+                const uint64_t l = len[v];
+                start[v] = total;
+                total += l;
+            }
+            if (total >= 0xffffffffull) return fail(GVA_ERR_UNSUPPORTED, "partition has 2^32 or more adjacency entries");
+            HostPartition& part = g.parts[p - 1];
+            part.edge_label = p;
+            part.off.resize(entries);  // group (v, l) starts at off[v * L + l]
+            part.adj.resize(total);
+            // each vertex's offsets and list, written by vertex ranges: its list
+            // is sorted by label, so group l starts after the entries of labels < l
+            auto fill_range = [&](uint64_t v0, uint64_t v1) {
+                for (uint64_t v = v0; v < v1; ++v) {
+                    const uint64_t* a = keys.data() + pos[v];
+                    const uint64_t at = start[v], n = len[v];
+                    uint64_t j = 0;
+                    for (uint64_t l = 0; l < L; ++l) {
+                        part.off[v * L + l] = (uint32_t)(at + j);
+                        while (j < n && (a[j] >> 32) == l) {
+                            part.adj[at + j] = (uint32_t)a[j];
+                            ++j;
+                        }
                     }
                 }
+            };
+            if (nth == 1 || V < (1u << 16)) {
+                fill_range(0, V);
+            } else {
+                std::vector<std::thread> pool;
+                for (unsigned t = 0; t < nth; ++t) pool.emplace_back(fill_range, V * t / nth, V * (t + 1) / nth);
+                for (auto& th : pool) th.join();
             }
-        };
-        if (nth == 1 || V < (1u << 16)) {
-            fill_range(0, V);
-        } else {
-            std::vector<std::thread> pool;
-            for (unsigned t = 0; t < nth; ++t) pool.emplace_back(fill_range, V * t / nth, V * (t + 1) / nth);
-            for (auto& th : pool) th.join();
+            part.off[entries - 1] = (uint32_t)total;
         }
-        part.off[entries - 1] = (uint32_t)total;
     }
     if (g.parts.empty()) g.parts.resize(1);
     return GVA_OK;
