@@ -1,6 +1,7 @@
 // Host side of the database: .mygraph/.metadata parsing, edge-list builder,
 // and the lowering of a plan to engine steps.
 #include <algorithm>
+#include <atomic>
 #include <thread>
 #include <cstdio>
 #include <cstring>
@@ -33,36 +34,6 @@ uint32_t HostGraph::dense_label(uint32_t orig) const {
 }
 
 namespace {
-
-// Per-partition adjacency in (vertex, label, id) order -> dense offset table.
-// lists[v] holds the already-sorted neighbours of v; their dense labels are
-// non-decreasing.
-int build_partition(HostGraph& g, uint32_t edge_label, const std::vector<std::vector<uint32_t>>& lists) {
-    const uint64_t L = g.num_labels();
-    const uint64_t entries = (uint64_t)(g.max_id + 1) * L + 1;
-    if (entries >= 0xffffffffull) return fail(GVA_ERR_UNSUPPORTED, "vertex count x label count exceeds 2^32");
-    HostPartition p;
-    p.edge_label = edge_label;
-    uint64_t total = 0;
-    for (auto& l : lists) total += l.size();
-    if (total >= 0xffffffffull) return fail(GVA_ERR_UNSUPPORTED, "partition has 2^32 or more adjacency entries");
-    p.off.resize(entries);
-    p.adj.reserve(total);
-    for (uint32_t v = 0; v <= g.max_id; ++v) {
-        const std::vector<uint32_t>* lst = v < lists.size() ? &lists[v] : nullptr;
-        size_t j = 0;
-        for (uint32_t l = 0; l < L; ++l) {
-            p.off[(uint64_t)v * L + l] = (uint32_t)p.adj.size();
-            if (!lst) continue;
-            while (j < lst->size() && g.dlabel[(*lst)[j]] == l) p.adj.push_back((*lst)[j++]);
-        }
-        if (lst && j != lst->size()) return fail(GVA_ERR_FORMAT, "neighbour list is not grouped by vertex label");
-    }
-    p.off[entries - 1] = (uint32_t)p.adj.size();
-    if (g.parts.size() < edge_label) g.parts.resize(edge_label);
-    g.parts[edge_label - 1] = std::move(p);
-    return GVA_OK;
-}
 
 // Sorted distinct labels and each vertex's dense label.  Labels are few
 // against vertices: they are collected in an open-addressing table (label ->
@@ -115,15 +86,49 @@ uint32_t index_prefix(uint32_t n) {
 
 }  // namespace
 
+namespace {
+
+// istream >> uint32_t on text held in memory: leading white space, an
+// optional sign ('-' negates modulo 2^32), at least one digit; false where
+// the stream would fail (no digit, or a value above 2^32 - 1).
+bool read_u32(const char*& p, const char* end, uint32_t& out) {
+    while (p < end && (*p == ' ' || *p == '\t' || *p == '\n' || *p == '\r' || *p == '\v' || *p == '\f')) ++p;
+    if (p == end) return false;
+    bool neg = false;
+    if (*p == '+' || *p == '-') neg = *p++ == '-';
+    if (p == end || *p < '0' || *p > '9') return false;
+    uint64_t x = 0;
+    while (p < end && *p >= '0' && *p <= '9') {
+        x = x * 10 + (uint64_t)(*p++ - '0');
+        if (x > 0xffffffffull) return false;
+    }
+    out = neg ? (uint32_t)(0u - (uint32_t)x) : (uint32_t)x;
+    return true;
+}
+
+}  // namespace
+
 int load_mygraph(const std::string& mygraph, const std::string& metadata, HostGraph& g, std::string* warnings) {
     // ---- .metadata: "newid label oldid" (src/loadDataBase.cpp:320-340) ----
-    std::ifstream mf(metadata);
+    std::ifstream mf(metadata, std::ios::binary | std::ios::ate);
     if (!mf.is_open()) return fail(GVA_ERR_IO, "cannot open metadata file " + metadata);
+    std::string text;
+    {
+        const std::streamoff size = mf.tellg();
+        text.resize(size > 0 ? (size_t)size : 0);
+        mf.seekg(0);
+        if (size > 0 && !mf.read(&text[0], size)) return fail(GVA_ERR_IO, "cannot read metadata file " + metadata);
+    }
     std::vector<std::pair<uint32_t, uint32_t>> vl;
-    uint32_t nid, lab, oid, maxid = 0;
-    while (mf >> nid >> lab >> oid) {
-        vl.push_back({nid, lab});
-        maxid = std::max(maxid, nid);
+    uint32_t maxid = 0;
+    {
+        const char* p = text.data();
+        const char* end = p + text.size();
+        uint32_t nid, lab, oid;
+        while (read_u32(p, end, nid) && read_u32(p, end, lab) && read_u32(p, end, oid)) {
+            vl.push_back({nid, lab});
+            maxid = std::max(maxid, nid);
+        }
     }
     if (vl.empty()) return fail(GVA_ERR_FORMAT, "metadata file has no vertices");
     g = HostGraph();
@@ -138,7 +143,11 @@ int load_mygraph(const std::string& mygraph, const std::string& metadata, HostGr
     if (!gf.is_open()) return fail(GVA_ERR_IO, "cannot open graph file " + mygraph);
     uint32_t P = 0;
     if (!gf.read((char*)&P, 4)) return fail(GVA_ERR_FORMAT, "graph file is empty");
+    const uint64_t V = (uint64_t)maxid + 1, L = g.num_labels();
+    const unsigned nth = std::max(1u, std::min(64u, std::thread::hardware_concurrency()));
     std::vector<uint32_t> part;
+    std::vector<uint64_t> cnt(V), start(V + 1);
+    std::vector<uint32_t> last(V);
     for (uint32_t key = 1; key <= P; ++key) {
         uint32_t tot = 0;
         if (!gf.read((char*)&tot, 4)) {
@@ -148,7 +157,7 @@ int load_mygraph(const std::string& mygraph, const std::string& metadata, HostGr
             break;
         }
         if (tot < 5) return fail(GVA_ERR_FORMAT, "partition shorter than its header");
-        part.assign(tot, 0);
+        part.resize(tot);
         part[0] = tot;
         if (!gf.read((char*)&part[1], (std::streamsize)(tot - 1) * 4)) return fail(GVA_ERR_FORMAT, "truncated partition");
         // header: [1] source slots, [2] intervals, [3]/[4] hash/neighbour offsets from word 5
@@ -158,7 +167,7 @@ int load_mygraph(const std::string& mygraph, const std::string& metadata, HostGr
         if (slots_at + nslot + 1 > tot || nbr_at > tot || 5 + 2 * nint + 1 > tot)
             return fail(GVA_ERR_FORMAT, "partition offsets out of range");
         const uint64_t nnbr = tot - nbr_at;
-        const uint32_t* start = &part[5];
+        const uint32_t* start_v = &part[5];
         const uint32_t* cum = &part[5 + nint + 1];
         const uint32_t* soff = &part[slots_at];
         const uint32_t* nbr = &part[nbr_at];
@@ -166,37 +175,87 @@ int load_mygraph(const std::string& mygraph, const std::string& metadata, HostGr
         if (soff[nslot] < nnbr && warnings)
             *warnings += "partition " + std::to_string(key) +
                          " holds neighbours of sources beyond its 256 intervals (dropped, as the reference)\n";
-        std::vector<std::vector<uint32_t>> lists(maxid + 1);
-        uint32_t prev = 0;
-        for (uint64_t i = 0; i < nint; ++i) {
-            if (cum[i] < prev || cum[i] > nslot) return fail(GVA_ERR_FORMAT, "interval lengths not cumulative");
-            for (uint32_t s = prev; s < cum[i]; ++s) {
-                const uint64_t v = (uint64_t)start[i] + (s - prev);
-                if (v == 0 || v > maxid) return fail(GVA_ERR_FORMAT, "source vertex id outside metadata");
-                uint32_t b = soff[s], e = soff[s + 1];
-                if (b > e || e > nnbr) return fail(GVA_ERR_FORMAT, "bad neighbour range");
-                std::vector<uint32_t>& out = lists[v];
-                // split into vertex-label groups, dropping each group's index prefix
-                uint32_t j = b;
-                while (j < e) {
-                    const uint32_t u0 = nbr[j];
-                    if (u0 == 0 || u0 > maxid || g.vlabel[u0] == kNone)
-                        return fail(GVA_ERR_FORMAT, "neighbour id outside metadata");
-                    uint32_t k = j;
-                    while (k < e && nbr[k] != 0 && nbr[k] <= maxid && g.vlabel[nbr[k]] == g.vlabel[u0]) ++k;
-                    const uint32_t skip = index_prefix(k - j);
-                    for (uint32_t t = j + skip; t < k; ++t) {
-                        if (!out.empty() && g.dlabel[out.back()] == g.dlabel[nbr[t]] && out.back() >= nbr[t])
-                            return fail(GVA_ERR_FORMAT, "neighbour group not strictly ascending");
-                        out.push_back(nbr[t]);
+        // every source slot's neighbours, split into vertex-label groups, each
+        // group without its index prefix; `visit(v, x)` gets them in order
+        auto walk = [&](bool check, auto&& visit) -> int {
+            uint32_t prev = 0;
+            for (uint64_t i = 0; i < nint; ++i) {
+                if (check && (cum[i] < prev || cum[i] > nslot)) return fail(GVA_ERR_FORMAT, "interval lengths not cumulative");
+                for (uint32_t s = prev; s < cum[i]; ++s) {
+                    const uint64_t v = (uint64_t)start_v[i] + (s - prev);
+                    if (check && (v == 0 || v > maxid)) return fail(GVA_ERR_FORMAT, "source vertex id outside metadata");
+                    const uint32_t b = soff[s], e = soff[s + 1];
+                    if (check && (b > e || e > nnbr)) return fail(GVA_ERR_FORMAT, "bad neighbour range");
+                    uint32_t j = b;
+                    while (j < e) {
+                        const uint32_t u0 = nbr[j];
+                        if (check && (u0 == 0 || u0 > maxid || g.vlabel[u0] == kNone))
+                            return fail(GVA_ERR_FORMAT, "neighbour id outside metadata");
+                        uint32_t k = j;
+                        while (k < e && nbr[k] != 0 && nbr[k] <= maxid && g.vlabel[nbr[k]] == g.vlabel[u0]) ++k;
+                        for (uint32_t t = j + index_prefix(k - j); t < k; ++t)
+                            if (int rc = visit(v, nbr[t])) return rc;
+                        j = k;
                     }
-                    j = k;
                 }
+                prev = cum[i];
             }
-            prev = cum[i];
+            return GVA_OK;
+        };
+        // pass 1: checks and list lengths (a list's groups must ascend
+        // strictly within a label, as the lists are appended slot by slot)
+        std::fill(cnt.begin(), cnt.end(), 0);
+        std::fill(last.begin(), last.end(), 0);
+        int rc = walk(true, [&](uint64_t v, uint32_t x) -> int {
+            const uint32_t b = last[v];
+            if (b != 0 && g.dlabel[b] == g.dlabel[x] && b >= x)
+                return fail(GVA_ERR_FORMAT, "neighbour group not strictly ascending");
+            last[v] = x;
+            cnt[v]++;
+            return GVA_OK;
+        });
+        if (rc) return rc;
+        start[0] = 0;
+        for (uint64_t v = 0; v < V; ++v) start[v + 1] = start[v] + cnt[v];
+        const uint64_t total = start[V];
+        const uint64_t entries = V * L + 1;
+        if (entries >= 0xffffffffull) return fail(GVA_ERR_UNSUPPORTED, "vertex count x label count exceeds 2^32");
+        if (total >= 0xffffffffull) return fail(GVA_ERR_UNSUPPORTED, "partition has 2^32 or more adjacency entries");
+        HostPartition hp;
+        hp.edge_label = key;
+        hp.adj.resize(total);
+        // pass 2: the lists, flat in vertex order
+        std::fill(cnt.begin(), cnt.end(), 0);
+        walk(false, [&](uint64_t v, uint32_t x) -> int {
+            hp.adj[start[v] + cnt[v]++] = x;
+            return GVA_OK;
+        });
+        // (vertex, label) offsets by vertex ranges; a list must be grouped by
+        // non-decreasing dense label
+        hp.off.resize(entries);
+        std::atomic<bool> ungrouped{false};
+        auto fill_range = [&](uint64_t v0, uint64_t v1) {
+            for (uint64_t v = v0; v < v1; ++v) {
+                const uint64_t at = start[v], n = start[v + 1] - at;
+                uint64_t j = 0;
+                for (uint64_t l = 0; l < L; ++l) {
+                    hp.off[v * L + l] = (uint32_t)(at + j);
+                    while (j < n && g.dlabel[hp.adj[at + j]] == l) ++j;
+                }
+                if (j != n) ungrouped = true;
+            }
+        };
+        if (nth == 1 || V < (1u << 16)) {
+            fill_range(0, V);
+        } else {
+            std::vector<std::thread> pool;
+            for (unsigned t = 0; t < nth; ++t) pool.emplace_back(fill_range, V * t / nth, V * (t + 1) / nth);
+            for (auto& th : pool) th.join();
         }
-        int st = build_partition(g, key, lists);
-        if (st) return st;
+        if (ungrouped) return fail(GVA_ERR_FORMAT, "neighbour list is not grouped by vertex label");
+        hp.off[entries - 1] = (uint32_t)total;
+        if (g.parts.size() < key) g.parts.resize(key);
+        g.parts[key - 1] = std::move(hp);
     }
     if (g.parts.empty()) return fail(GVA_ERR_FORMAT, "graph file holds no partition");
     return GVA_OK;

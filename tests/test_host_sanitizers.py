@@ -20,6 +20,8 @@ DRIVERS = {
     "dplan_check": [TESTS / "dplan_check.cpp", CSRC / "gva_plan.cpp", CSRC / "gva_graph.cpp"],
     "plan_query_check": [TESTS / "plan_query_check.cpp", CSRC / "gva_plan.cpp", CSRC / "gva_graph.cpp"],
     "graph_build_check": [TESTS / "graph_build_check.cpp", CSRC / "gva_graph.cpp", CSRC / "gva_plan.cpp"],
+    "mygraph_roundtrip_check": [TESTS / "mygraph_roundtrip_check.cpp", CSRC / "gva_convert.cpp", CSRC / "gva_graph.cpp",
+                                CSRC / "gva_plan.cpp"],
 }
 RUNS = [
     ("mine_grow_check", ["3", "2", "4", "7", "0.3", "4"]),
@@ -29,6 +31,7 @@ RUNS = [
     ("plan_query_check", ["1000", "1"]),
     ("graph_build_check", ["20", "1", "3000"]),
     ("graph_build_check", ["1", "2", "70000"]),  # the threaded sort and fill
+    ("mygraph_roundtrip_check", ["10", "3", None]),  # None: a scratch directory
 ]
 
 
@@ -54,10 +57,11 @@ def sanitized(tmp_path_factory):
         return dict(ex.map(build, DRIVERS.items()))
 
 
-@pytest.mark.parametrize("name,args", RUNS, ids=lambda x: x if isinstance(x, str) else "-".join(x))
-def test_host_code_is_sanitizer_clean(sanitized, name, args):
+@pytest.mark.parametrize("name,args", RUNS, ids=lambda x: x if isinstance(x, str) else "-".join(a or "dir" for a in x))
+def test_host_code_is_sanitizer_clean(sanitized, name, args, tmp_path):
     env = dict(os.environ, ASAN_OPTIONS="detect_leaks=1:abort_on_error=0",
                UBSAN_OPTIONS="print_stacktrace=1:halt_on_error=1")
+    args = [str(tmp_path) if a is None else a for a in args]
     r = subprocess.run([str(sanitized[name]), *args], capture_output=True, text=True, timeout=600, env=env)
     assert r.returncode == 0, (r.stdout + r.stderr)[-3000:]
     assert r.stdout.strip().splitlines()[-1].startswith("ok"), r.stdout[-2000:]
