@@ -335,10 +335,11 @@ int gva_result_write_text(const gva_result* res, const char* path) {
     if (!res || !path) return fail(GVA_ERR_ARG, "null argument");
     FILE* f = fopen(path, "w");
     if (!f) return fail(GVA_ERR_IO, std::string("cannot write ") + path);
-    const uint64_t chunk = 1 << 20;
+    const uint64_t chunk = 1 << 22;
     const uint32_t w = res->r.width;
+    const unsigned threads = std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
     std::vector<uint32_t> buf;
-    std::string line;
+    std::vector<std::string> parts;
     for (uint64_t r0 = 0; r0 < res->r.rows; r0 += chunk) {
         const uint64_t n = std::min<uint64_t>(chunk, res->r.rows - r0);
         buf.resize(n * w);
@@ -347,17 +348,14 @@ int gva_result_write_text(const gva_result* res, const char* path) {
             fclose(f);
             return st;
         }
-        for (uint64_t i = 0; i < n; ++i) {
-            line.clear();
-            for (uint32_t c = 0; c < w; ++c) {
-                if (c) line.push_back(' ');
-                line += std::to_string(buf[i * w + c]);
+        format_rows(buf.data(), n, w, threads, parts);
+        for (const std::string& part : parts)
+            if (fwrite(part.data(), 1, part.size(), f) != part.size()) {
+                fclose(f);
+                return fail(GVA_ERR_IO, std::string("cannot write ") + path);
             }
-            line.push_back('\n');
-            fwrite(line.data(), 1, line.size(), f);
-        }
     }
-    fclose(f);
+    if (fclose(f) != 0) return fail(GVA_ERR_IO, std::string("cannot write ") + path);
     return GVA_OK;
 }
 

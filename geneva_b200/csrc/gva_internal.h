@@ -146,6 +146,12 @@ int lower_plan(const Plan& plan, const HostGraph& g, std::vector<Step>& steps, b
 int lower_dplan(const DPlan& plan, const uint32_t* labels, const HostGraph& g, std::vector<Step>& steps,
                 bool fuse_reductions = false);
 
+// ----------------------------------------------------------------- text ----
+// Rows [0, n) of `width` values as text (one line per row, decimal values
+// separated by single spaces), formatted on up to `threads` threads; the
+// text is the concatenation of `parts` in order.
+void format_rows(const uint32_t* rows, uint64_t n, uint32_t width, unsigned threads, std::vector<std::string>& parts);
+
 // ---------------------------------------------------------------- mining ---
 struct MinedPattern {
     std::string text;  // query text, vertices in canonical order

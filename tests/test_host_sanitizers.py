@@ -22,6 +22,7 @@ DRIVERS = {
     "graph_build_check": [TESTS / "graph_build_check.cpp", CSRC / "gva_graph.cpp", CSRC / "gva_plan.cpp"],
     "mygraph_roundtrip_check": [TESTS / "mygraph_roundtrip_check.cpp", CSRC / "gva_convert.cpp", CSRC / "gva_graph.cpp",
                                 CSRC / "gva_plan.cpp"],
+    "text_format_check": [TESTS / "text_format_check.cpp", CSRC / "gva_text.cpp"],
 }
 RUNS = [
     ("mine_grow_check", ["3", "2", "4", "7", "0.3", "4"]),
@@ -32,6 +33,7 @@ RUNS = [
     ("graph_build_check", ["20", "1", "3000"]),
     ("graph_build_check", ["1", "2", "70000"]),  # the threaded sort and fill
     ("mygraph_roundtrip_check", ["10", "3", None]),  # None: a scratch directory
+    ("text_format_check", ["2"]),
 ]
 
 
