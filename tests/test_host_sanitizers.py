@@ -33,7 +33,7 @@ RUNS = [
     ("graph_build_check", ["20", "1", "3000"]),
     ("graph_build_check", ["1", "2", "70000"]),  # the threaded sort and fill
     ("mygraph_roundtrip_check", ["10", "3", None]),  # None: a scratch directory
-    ("text_format_check", ["2"]),
+    ("text_format_check", ["2", "8000"]),
 ]
 
 

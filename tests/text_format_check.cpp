@@ -3,7 +3,7 @@
 // std::to_string, for random rows of every width 1..32 (values including 0
 // and 2^32 - 1), several thread counts and row counts around the split sizes.
 //
-// usage: text_format_check seed
+// usage: text_format_check seed [max_rows]
 #include <cstdio>
 #include <cstdlib>
 #include <random>
@@ -15,10 +15,11 @@
 int main(int argc, char** argv) {
     if (argc < 2) return 2;
     std::mt19937 rng(atoi(argv[1]));
+    const uint64_t max_rows = argc > 2 ? strtoull(argv[2], nullptr, 10) : ~0ull;
     int cases = 0;
     for (uint32_t w = 1; w <= 32; ++w)
         for (uint64_t n : {0ull, 1ull, 7ull, 65535ull, 65537ull, 200001ull}) {
-            if (n > 70000 && w > 2) continue;
+            if ((n > 70000 && w > 2) || n > max_rows) continue;
             std::vector<uint32_t> rows(n * w);
             for (auto& x : rows) {
                 const uint32_t k = rng() % 4;
