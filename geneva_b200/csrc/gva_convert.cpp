@@ -44,13 +44,13 @@ namespace gva {
 namespace {
 
 // first three unsigned integers of a line (tools/genDatabase.cpp:69-92)
-int parse_uints(const std::string& line, uint32_t* out, int want) {
+int parse_uints(const char* line, size_t len, uint32_t* out, int want) {
     int n = 0;
     size_t i = 0;
-    while (i < line.size() && n < want) {
+    while (i < len && n < want) {
         if (line[i] >= '0' && line[i] <= '9') {
             uint64_t x = 0;
-            while (i < line.size() && line[i] >= '0' && line[i] <= '9') x = x * 10 + (uint64_t)(line[i++] - '0');
+            while (i < len && line[i] >= '0' && line[i] <= '9') x = x * 10 + (uint64_t)(line[i++] - '0');
             out[n++] = (uint32_t)x;
         } else {
             ++i;
@@ -59,15 +59,29 @@ int parse_uints(const std::string& line, uint32_t* out, int want) {
     return n;
 }
 
+// A partition's set of source vertices during the renumbering, over ranks
+// of the source ids (rank order = id order): the ranks it ever held,
+// ascending, and a bitset of those it still holds.  Iteration visits the
+// held ranks in ascending order, as std::set would.
+struct RankSet {
+    std::vector<uint32_t> items;
+    std::vector<uint64_t> bits;
+    size_t count = 0;
+    bool has(uint32_t r) const { return bits[r >> 6] >> (r & 63) & 1; }
+    void erase(uint32_t r) {
+        if (has(r)) bits[r >> 6] &= ~(1ull << (r & 63)), --count;
+    }
+};
+
 // Step 2 of the renumbering for one other partition `cur`.
-void split_by(std::set<uint32_t>& base, const std::set<uint32_t>& cur, std::vector<std::vector<uint32_t>>& subs) {
+void split_by(RankSet& base, const RankSet& cur, std::vector<std::vector<uint32_t>>& subs) {
     std::vector<uint32_t> common;
-    for (uint32_t v : base)
-        if (cur.count(v)) common.push_back(v);
+    for (uint32_t v : base.items)
+        if (base.has(v) && cur.has(v)) common.push_back(v);
     const size_t before = subs.size();
     for (size_t i = 0; i < before; ++i) {
         std::vector<uint32_t> in, out;
-        for (uint32_t v : subs[i]) (cur.count(v) ? in : out).push_back(v);
+        for (uint32_t v : subs[i]) (cur.has(v) ? in : out).push_back(v);
         if (in.size() == subs[i].size() || out.size() == subs[i].size()) continue;
         subs[i] = out;
         subs.push_back(in);
@@ -76,25 +90,48 @@ void split_by(std::set<uint32_t>& base, const std::set<uint32_t>& cur, std::vect
     for (uint32_t v : common) base.erase(v);
 }
 
-std::map<uint32_t, uint32_t> renumber(const std::vector<std::vector<uint32_t>>& sources) {
-    std::vector<std::set<uint32_t>> parts;
-    for (const std::vector<uint32_t>& src : sources) parts.emplace_back(src.begin(), src.end());
-    auto by_size = [](const std::set<uint32_t>& a, const std::set<uint32_t>& b) { return a.size() > b.size(); };
+// The new id of every source vertex, as (old id, new id) by ascending old id.
+std::vector<std::pair<uint32_t, uint32_t>> renumber(const std::vector<std::vector<uint32_t>>& sources) {
+    // ranks: the sorted union of all partitions' (sorted) source ids
+    std::vector<uint32_t> ids;
+    for (const std::vector<uint32_t>& src : sources) ids.insert(ids.end(), src.begin(), src.end());
+    std::sort(ids.begin(), ids.end());
+    ids.erase(std::unique(ids.begin(), ids.end()), ids.end());
+    const size_t nr = ids.size(), words = (nr + 63) / 64;
+    std::vector<RankSet> parts(sources.size());
+    for (size_t p = 0; p < sources.size(); ++p) {
+        RankSet& rs = parts[p];
+        rs.bits.assign(words, 0);
+        rs.items.reserve(sources[p].size());
+        size_t k = 0;  // sources[p] is sorted: a merge walk gives the ranks
+        for (uint32_t v : sources[p]) {
+            while (ids[k] < v) ++k;
+            if (rs.items.empty() || rs.items.back() != k) {
+                rs.items.push_back((uint32_t)k);
+                rs.bits[k >> 6] |= 1ull << (k & 63);
+                ++rs.count;
+            }
+        }
+    }
+    auto by_size = [](const RankSet& a, const RankSet& b) { return a.count > b.count; };
     std::stable_sort(parts.begin(), parts.end(), by_size);
-    std::map<uint32_t, uint32_t> newid;  // old -> new
+    std::vector<uint32_t> newid(nr, 0);  // by rank; 0: not numbered yet (ids start at 1)
+    auto assign = [&](uint32_t r, uint32_t id) {
+        if (!newid[r]) newid[r] = id;  // first one wins, as map::emplace
+    };
     uint32_t numbered = 0;
     const size_t rounds = parts.size();
     for (size_t r = 0; r < rounds; ++r) {
-        std::set<uint32_t>& base = parts[0];
-        uint32_t top = numbered + (uint32_t)base.size();
-        numbered += (uint32_t)base.size();
+        RankSet& base = parts[0];
+        uint32_t top = numbered + (uint32_t)base.count;
+        numbered += (uint32_t)base.count;
         std::vector<std::vector<uint32_t>> subs;
         for (size_t i = 1; i < parts.size(); ++i) split_by(base, parts[i], subs);
         std::map<size_t, std::set<size_t>> overlaps;  // other partition -> sub-parts it touches
         for (size_t i = 0; i < subs.size(); ++i) {
             const uint32_t probe = subs[i][0];
             for (size_t j = 1; j < parts.size(); ++j)
-                if (parts[j].count(probe)) overlaps[j].insert(i);
+                if (parts[j].has(probe)) overlaps[j].insert(i);
             for (uint32_t v : subs[i])
                 for (size_t k = 1; k < parts.size(); ++k) parts[k].erase(v);
         }
@@ -125,15 +162,20 @@ std::map<uint32_t, uint32_t> renumber(const std::vector<std::vector<uint32_t>>& 
             for (auto& gr : groups) {
                 uint32_t id = gr.second;
                 for (size_t sid : gr.first)
-                    for (uint32_t v : subs[sid]) newid.emplace(v, id--);
+                    for (uint32_t v : subs[sid]) assign(v, id--);
             }
         }
-        uint32_t id = top - (uint32_t)base.size() + 1;
-        for (uint32_t v : base) newid.emplace(v, id++);
+        uint32_t id = top - (uint32_t)base.count + 1;
+        for (uint32_t v : base.items)
+            if (base.has(v)) assign(v, id++);
         parts.erase(parts.begin());
         std::stable_sort(parts.begin(), parts.end(), by_size);
     }
-    return newid;
+    std::vector<std::pair<uint32_t, uint32_t>> out;
+    out.reserve(nr);
+    for (size_t k = 0; k < nr; ++k)
+        if (newid[k]) out.push_back({ids[k], newid[k]});
+    return out;
 }
 
 // tools/genDatabase.cpp:415-436
@@ -220,24 +262,28 @@ int convert_g(const std::string& g_path, const std::string& mygraph, const std::
         while ((k = fread(buf, 1, sizeof buf, f)) > 0) text.append(buf, k);
         fclose(f);
     }
-    std::map<uint32_t, uint32_t> vlabel;
+    std::unordered_map<uint32_t, uint32_t> vlabel;  // first definition wins; only looked up
     uint32_t x[3];
     size_t pos = 0;
-    auto next_line = [&](std::string& line) {
+    const char* line = nullptr;  // the current line, [line, line + len), in `text`
+    size_t len = 0;
+    auto next_line = [&]() {
         if (pos >= text.size()) return false;
-        size_t e = text.find('\n', pos);
-        if (e == std::string::npos) e = text.size();
-        line.assign(text, pos, e - pos);
+        const char* b = text.data() + pos;
+        const void* nl = std::memchr(b, '\n', text.size() - pos);
+        const size_t e = nl ? (size_t)((const char*)nl - text.data()) : text.size();
+        line = b;
+        len = e - pos;
         pos = e + 1;
         return true;
     };
-    std::string line;
     // vertex section (tools/genDatabase.cpp:769-778): up to the first `e` line
     bool have_edge = false;
-    while (next_line(line)) {
-        if (line.empty() || line[0] == 't') continue;
+    vlabel.reserve(text.size() / 16);
+    while (next_line()) {
+        if (len == 0 || line[0] == 't') continue;
         if (line[0] == 'v') {
-            if (parse_uints(line, x, 2) == 2) vlabel.emplace(x[0], x[1]);
+            if (parse_uints(line, len, x, 2) == 2) vlabel.emplace(x[0], x[1]);
         } else if (line[0] == 'e') {
             have_edge = true;
             break;
@@ -247,13 +293,14 @@ int convert_g(const std::string& g_path, const std::string& mygraph, const std::
     size_t P = 0;
     uint32_t max_id = 0;
     while (have_edge) {
-        if (!line.empty() && line[0] == 'e') {
-            if (parse_uints(line, x, 3) < 3) return fail(GVA_ERR_FORMAT, "malformed edge line: " + line);
+        if (len != 0 && line[0] == 'e') {
+            if (parse_uints(line, len, x, 3) < 3)
+                return fail(GVA_ERR_FORMAT, "malformed edge line: " + std::string(line, len));
             P = std::max<size_t>(P, (size_t)x[2] + 1);
             max_id = std::max(max_id, std::max(x[0], x[1]));
             edges.push_back({x[2], x[0], x[1]});
         }
-        if (!next_line(line)) break;
+        if (!next_line()) break;
     }
     text.clear();
     text.shrink_to_fit();
@@ -292,7 +339,7 @@ int convert_g(const std::string& g_path, const std::string& mygraph, const std::
         for (const Half& h : part[p])
             if (sources[p].empty() || sources[p].back() != h.a) sources[p].push_back(h.a);
     }
-    const std::map<uint32_t, uint32_t> newid = renumber(sources);
+    const std::vector<std::pair<uint32_t, uint32_t>> newid = renumber(sources);  // by old id
     std::vector<uint32_t> nid_dense;
     std::unordered_map<uint32_t, uint32_t> nid_hash;
     if (dense) {
