@@ -83,3 +83,27 @@ def test_converter_repeated_edges_match_reference_binary(native, tmp_path):
     assert filecmp.cmp(tmp_path / "mine.reorder", tmp_path / "run" / "d.reorder", shallow=False)
     assert filecmp.cmp(tmp_path / "mine.mygraph", tmp_path / "datasets" / "d.mygraph", shallow=False)
     assert filecmp.cmp(tmp_path / "mine.metadata", tmp_path / "datasets" / "d.metadata", shallow=False)
+
+
+@pytest.mark.parametrize("seed", range(6))
+def test_converter_random_graphs_match_reference_binary(native, tmp_path, seed):
+    """Random graphs with up to 6 edge labels (the renumbering splits the
+    largest partition by every other one) and hubs: all three files equal the
+    reference converter's."""
+    import random
+    ref = ROOT / "oracle" / "_ref" / "genDatabase"
+    if not ref.exists():
+        pytest.skip("reference converter not built here")
+    rng = random.Random(seed)
+    spec = dict(name=f"r{seed}", n=rng.choice([300, 2000, 5000]), avg_deg=rng.choice([1.5, 3.0, 6.0]),
+                vlabels=rng.randint(1, 5), elabels=rng.randint(2, 6), seed=500 + seed,
+                hub=rng.choice([0, 1]) * rng.randint(150, 280))
+    vl, edges = make_graph(spec)
+    (tmp_path / "datasets").mkdir()
+    (tmp_path / "run").mkdir()
+    (tmp_path / "datasets" / "r.g").write_text(write_g(vl, edges))
+    subprocess.run([str(ref), "r"], cwd=tmp_path / "run", check=True, capture_output=True)
+    gv.convert_g(tmp_path / "datasets" / "r.g", tmp_path / "mine")
+    assert filecmp.cmp(tmp_path / "mine.reorder", tmp_path / "run" / "r.reorder", shallow=False)
+    assert filecmp.cmp(tmp_path / "mine.mygraph", tmp_path / "datasets" / "r.mygraph", shallow=False)
+    assert filecmp.cmp(tmp_path / "mine.metadata", tmp_path / "datasets" / "r.metadata", shallow=False)
