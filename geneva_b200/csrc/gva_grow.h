@@ -469,6 +469,8 @@ template <typename Freq>
 void grow_level(const std::vector<Pattern>& level, const CodeSet& level_codes, Freq freq, uint32_t L, uint32_t P,
                 uint32_t width, uint32_t max_edges, unsigned nthreads, const WedgeTab* wedges,
                 std::vector<Pattern>& next, GrowStats& gt) {
+    // small levels on few threads: starting a thread costs more than a few patterns
+    nthreads = std::max(1u, std::min<unsigned>(nthreads, (unsigned)((level.size() + 15) / 16)));
     auto t_gen = std::chrono::steady_clock::now();
     std::vector<uint64_t> pinv(level.size());
     for (size_t i = 0; i < level.size(); ++i) pinv[i] = pattern_inv(level[i]);
@@ -778,14 +780,15 @@ int mine_levels(uint32_t L, uint32_t P, const std::vector<char>& has_part, const
         for (size_t i = 0; i < next.size(); ++i)
             if (sup[i] >= min_support) fi.push_back((uint32_t)i);
         std::vector<std::string> texts(fi.size());
-        std::vector<std::vector<uint8_t>> code_arena(nthreads);
+        const unsigned pt = std::max(1u, std::min<unsigned>(nthreads, (unsigned)(fi.size() / 256 + 1)));
+        std::vector<std::vector<uint8_t>> code_arena(pt);
         std::vector<uint32_t> code_at(fi.size()), code_len(fi.size());
         std::vector<uint8_t> code_thread(fi.size());
         std::vector<std::thread> pool;
-        for (unsigned t = 0; t < nthreads; ++t)
+        for (unsigned t = 0; t < pt; ++t)
             pool.emplace_back([&, t]() {
                 CodeBuf cb;
-                for (size_t j = t; j < fi.size(); j += nthreads) {
+                for (size_t j = t; j < fi.size(); j += pt) {
                     canonical(next[fi[j]], width, cb);
                     code_at[j] = (uint32_t)code_arena[t].size();
                     code_len[j] = cb.len;

@@ -74,15 +74,16 @@ int run_mine(DevDB& db, cudaStream_t s, uint64_t budget, uint32_t max_edges, uin
                           std::vector<std::vector<Step>>& steps, std::string& msg) -> int {
         auto t0 = std::chrono::steady_clock::now();
         steps.assign(b1 - b0, {});
-        std::vector<int> rcs(nthreads, GVA_OK);
-        std::vector<std::string> msgs(nthreads);
+        const unsigned pt = std::max(1u, std::min<unsigned>(nthreads, (unsigned)((b1 - b0) / 64 + 1)));
+        std::vector<int> rcs(pt, GVA_OK);
+        std::vector<std::string> msgs(pt);
         std::vector<std::thread> pool;
-        for (unsigned t = 0; t < nthreads; ++t)
+        for (unsigned t = 0; t < pt; ++t)
             pool.emplace_back([&, t]() {
                 uint32_t sdl[3 * kMaxPatEdges];
                 std::unique_ptr<DPlanQuery> dq(new DPlanQuery());
                 std::unique_ptr<DPlan> dp(new DPlan());
-                for (size_t i = b0 + t; i < b1; i += nthreads) {
+                for (size_t i = b0 + t; i < b1; i += pt) {
                     // the plan of the candidate's query text, built from the
                     // pattern by the heap-free planner, else by the host planner
                     const Pattern& c = cands[i];
@@ -112,7 +113,7 @@ int run_mine(DevDB& db, cudaStream_t s, uint64_t budget, uint32_t max_edges, uin
             });
         for (auto& th : pool) th.join();
         st.plan_ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
-        for (unsigned t = 0; t < nthreads; ++t)
+        for (unsigned t = 0; t < pt; ++t)
             if (rcs[t]) {
                 msg = msgs[t];
                 return rcs[t];
@@ -187,11 +188,12 @@ int run_mine(DevDB& db, cudaStream_t s, uint64_t budget, uint32_t max_edges, uin
         for (auto& v : all) width_k = std::max(width_k, v.size());
         std::vector<uint64_t> key(n * width_k, 0);
         {
+            const unsigned kt = std::max(1u, std::min<unsigned>(nthreads, (unsigned)(n / 256 + 1)));
             std::vector<std::thread> pool;
-            for (unsigned t = 0; t < nthreads; ++t)
+            for (unsigned t = 0; t < kt; ++t)
                 pool.emplace_back([&, t]() {
                     uint8_t kb[512];
-                    for (size_t i = t; i < n; i += nthreads)
+                    for (size_t i = t; i < n; i += kt)
                         for (size_t j = 0; j < all[i].size(); ++j) {
                             const size_t len = step_key_bytes(all[i][j], kb);
                             key[i * width_k + j] = code_hash(kb, (uint32_t)len) | 1;  // 0 marks the end
