@@ -3,13 +3,23 @@
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl geneva|reference] [--workload mine|match|mni|serve]
 
-Workload (default, "mine"): the 20,000-graph database (|V|~U[20,60], average
-degree 4, 16 vertex labels Zipf(1.2), 3 edge labels; seeded, synthetic)
-resident in HBM; one step mines every connected pattern of up to 6 edges with
-support >= 2% (400 graphs).  Every candidate of every level is matched on the
-GPU (all embeddings enumerated, per-graph support bitmaps).  Metric:
-embeddings/s = embeddings enumerated over all candidates / step time;
-patterns/s (candidates whose support was decided / step time) rides along.
+Workload (default, "batch"): the 20,000-graph database (|V|~U[20,60],
+average degree 4, 16 vertex labels Zipf(1.2), 3 edge labels; seeded,
+synthetic) resident in HBM and a seeded list of 16,384 connected patterns of
+2-7 vertices sampled from its graphs; one step matches every pattern in one
+batched run (gva_batch_count): the int64 embedding count and the supporting
+graphs of every pattern, copied to host memory.  Metric: embeddings/s =
+embeddings of all patterns / step time; patterns/s rides along.  The same
+patterns go through the plain per-pattern path (a sample), the oracle (parity
+check and CPU baseline, on the host's cores) and, in the reference arm, the
+reference's cpumine.  A complete mining run of the same database (patterns up
+to 6 edges, support >= 2%) is timed beside it (key "mining").
+
+"mine": one step mines every connected pattern of up to 6 edges with support
+>= 2% (400 graphs) of the 20,000-graph database (or, --db config1, up to 4
+edges with support >= 5% of the 1,000-graph database); every candidate of
+every level is matched on the GPU (all embeddings enumerated, per-graph
+support bitmaps).  embeddings/s over all candidates; patterns/s alongside.
 
 "match": 4,096 query patterns of 3-8 vertices, connected induced subgraphs
 sampled from the 1,000-graph database (|V|~U[10,30], average degree 3, 4
@@ -33,7 +43,8 @@ step time is the max over ranks.
 --impl reference times the reference CPU matcher (oracle/_ref/cpumine, built
 from the reference sources) on the same database and patterns, one process
 per pattern over the host cores (the reference has no miner: each pattern is
-a separate cpumine run, support from its rows' graph ids).
+a separate cpumine run, support from its rows' graph ids); each step is a
+bounded sample of the pattern list.
 """
 from __future__ import annotations
 
@@ -58,6 +69,11 @@ import numpy as np  # noqa: E402
 MINE_WORKLOAD = ("config-2 mining: 20000 graphs per rank, |V|~U[20,60], avg degree 4, 16 vertex labels Zipf(1.2), "
                  "3 edge labels; all connected patterns of up to {me} edges with support >= {ms:g} of the graphs; "
                  "every candidate matched, all embeddings enumerated")
+BATCH_WORKLOAD = ("config-2 batched matching: seeded list of connected patterns of 2-7 vertices, each grown inside "
+                  "a random graph of the config-2 database (20000 graphs, |V|~U[20,60], avg degree 4, 16 vertex "
+                  "labels Zipf(1.2), 3 edge labels, seed 2) with each further induced edge kept with probability "
+                  "1/2, matched (non-induced, the reference's row semantics) against that database; int64 embedding "
+                  "count and supporting graphs of every pattern")
 WORKLOAD = ("config-3 batched matching: 4096 query patterns of 3-8 vertices, each a connected induced subgraph "
             "sampled from a config-1 graph, matched (non-induced) against the config-1 database (1000 graphs, "
             "|V|~U[10,30], avg degree 3, 4 uniform vertex labels, unlabeled edges, seed 1); int64 embedding counts "
@@ -70,7 +86,10 @@ def parse_args():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="geneva", choices=["geneva", "reference"])
-    ap.add_argument("--workload", default="mine", choices=["mine", "match", "serve", "mni"])
+    ap.add_argument("--workload", default="batch", choices=["batch", "mine", "match", "serve", "mni"])
+    ap.add_argument("--patterns", type=int, default=16384, help="batch workload: patterns per rank per step")
+    ap.add_argument("--mining-steps", type=int, default=3,
+                    help="batch workload: timed steps of the mining run reported beside it (0: none)")
     ap.add_argument("--rates", default="10,100,500,2000", help="serve workload: arrival rates (req/s)")
     ap.add_argument("--duration", type=float, default=2.0, help="serve workload: seconds of arrivals per rate")
     ap.add_argument("--drain", type=float, default=30.0, help="serve workload: seconds to wait for results per rate")
@@ -186,7 +205,7 @@ def cpu_baseline_port(db, queries, budget_s=15.0):
                       f"{rows} embeddings in {dt:.2f} s"}
 
 
-def reference_arm(args, db, queries, workload):
+def reference_arm(args, db, queries, workload, config=None):
     """oracle/_ref/cpumine (the reference CPU matcher built from source) on the
     same database (converted by oracle/_ref/genDatabase) and patterns, one
     process per pattern, a wave of processes per step over the host cores;
@@ -211,14 +230,18 @@ def reference_arm(args, db, queries, workload):
         cores = os.cpu_count() or 1
         wave = max(1, min(cores, len(queries), 64))  # one cpumine process per host core
 
+        proc_s = []
+
         def one(i_q):
             i, q = i_q
             d = work / f"q{i}"
             d.mkdir(exist_ok=True)
             (d / "q.query").write_text(q)
+            tp = time.perf_counter()
             subprocess.run([str(ref / "cpumine"), str(reorder), "q.query", str(ds / f"{db.name}.mygraph"),
                             str(ds / f"{db.name}.metadata")], cwd=d, stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL,
                            check=True)
+            proc_s.append(time.perf_counter() - tp)
             rows = [l.split() for l in open(d / "partialResultsCPU.txt") if l.strip()]
             if not rows:
                 return 0, 0
@@ -239,6 +262,7 @@ def reference_arm(args, db, queries, workload):
 
         for _ in range(args.warmup):
             step()
+        proc_s.clear()
         tot_rows, tot_pats, tot_t = 0, 0, 0.0
         for _ in range(args.steps):
             r, n, t = step()
@@ -251,11 +275,18 @@ def reference_arm(args, db, queries, workload):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * tot_t / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
             "impl": "reference", "patterns_per_s": tot_pats / tot_t,
-            "config": {"workload": workload, "seed": db.params.get("seed", args.seed), "patterns_per_step": wave,
-                       "database_conversion_s": t_conv},
+            "config": config if config is not None else {"workload": workload,
+                                                         "seed": db.params.get("seed", args.seed)},
             "cpu_baseline": {"value": value, "unit": "embeddings/s", "cores": wave, "kind": "reference",
-                             "sample": f"{wave} seeded patterns per step sampled from the {db.name} database, one "
-                                       f"cpumine process each (it reloads the database per pattern)"},
+                             "sample": f"{wave} patterns of the list per step (patterns {args.warmup * wave}.."
+                                       f"{(args.warmup + args.steps) * wave - 1} over the timed steps, modulo the "
+                                       f"list), one cpumine process each on its own host core; cpumine "
+                                       f"reloads the database in every process",
+                             "process_s_min": min(proc_s) if proc_s else None,
+                             "process_s_mean": statistics.mean(proc_s) if proc_s else None,
+                             "process_note": "wall time of one cpumine process (database load + match + row "
+                                             "file); the smallest is about the database load alone",
+                             "database_conversion_s": t_conv},
             "e2e": {"value": value, "unit": "embeddings/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         }
     finally:
@@ -677,6 +708,260 @@ def cpu_baseline_mine(db, sample, budget_s=15.0):
                       f"support, {rows} embeddings in {dt:.2f} s"}
 
 
+# ------------------------------------------------------------ batch (default) ----
+def batch_config(args, world: int) -> dict:
+    """The workload description both arms print (identical by construction)."""
+    return {"workload": BATCH_WORKLOAD, "patterns_per_rank": args.patterns, "database_seed": args.seed,
+            "pattern_seed": 1000, "pattern_vertices": [2, 7],
+            "outputs": "int64 embedding count and supporting-graph count of every pattern, in host memory",
+            "l2": "GPU arm: flushed between steps (512 MiB write); CPU arms: not applicable",
+            "parallelism": f"database replicated on {world} rank(s), pattern list sharded (no collective on the "
+                           f"data path)"}
+
+
+def batch_patterns(args, db, rank: int, world: int, workloads):
+    """This rank's share of the pattern list (weak scaling: --patterns per rank)."""
+    allq = workloads.config2_patterns(db, args.patterns * world, seed=1000)
+    return allq[rank * args.patterns:(rank + 1) * args.patterns]
+
+
+def oracle_check(db, queries, counts, supports, budget_s=20.0):
+    """The oracle (cpumine restated, rows mapped to graph ids) on all host
+    cores over a bounded prefix of the patterns: the parity check of the GPU
+    results and, timed, the CPU baseline (kind "port")."""
+    sys.path.insert(0, str(ROOT / "tests"))
+    from oracle_lib import Oracle
+    o = Oracle.get()
+    g = o.from_edges(db.vlabels, db.src, db.dst, db.elabels)
+    cores = os.cpu_count() or 1
+    done, rows, mism, first_bad = 0, 0, 0, None
+    t0 = time.perf_counter()
+    chunk = 4 * cores
+    while done < len(queries) and time.perf_counter() - t0 < budget_s:
+        part = queries[done:done + chunk]
+        c, sup, _ = o.many_graph_counts(g, part, db.first, threads=cores)
+        for i in range(len(part)):
+            if int(c[i]) != int(counts[done + i]) or int(sup[i]) != int(supports[done + i]):
+                mism += 1
+                if first_bad is None:
+                    first_bad = done + i
+        rows += int(c.sum())
+        done += len(part)
+    dt = time.perf_counter() - t0
+    o.free(g)
+    parity = {"checked": done, "mismatches": mism, "first_mismatch": first_bad,
+              "against": "oracle (cpumine restated) per pattern, rows mapped to graph ids: embedding count and "
+                         "support of every checked pattern, exact"}
+    base = {"value": rows / dt, "unit": "embeddings/s", "cores": cores, "kind": "port",
+            "patterns_per_s": done / dt,
+            "sample": f"first {done} of the {len(queries)} patterns of one step, oracle restatement of cpumine on "
+                      f"{cores} host threads (one pattern per thread), {rows} embeddings in {dt:.2f} s, supports "
+                      f"from graph ids"}
+    return parity, base
+
+
+def batch_bench(args, rank, world, local, dist, torch, gv, workloads):
+    """One step = every pattern of this rank's list matched in one batched run
+    (gva_batch_count with supports), results in host memory."""
+    db = workloads.config2(seed=args.seed)
+    queries = batch_patterns(args, db, rank, world, workloads)
+    t0 = time.perf_counter()
+    gdb = gv.Database.from_edges(db.vlabels, db.src, db.dst, db.elabels, device=local)
+    gdb.set_graphs(db.first)
+    build_s = time.perf_counter() - t0
+    plans = gv.Plan.batch_from_texts(queries)
+    stream = torch.cuda.Stream()
+    sp = stream.cuda_stream
+    flush = torch.empty(512 << 20, dtype=torch.uint8, device="cuda")
+
+    def step(profile=False):
+        counts, sup, stats = gv.batch_count(gdb, plans, stream=sp, support=True, profile=profile)
+        return counts, sup, stats
+
+    for _ in range(max(args.warmup, 3)):
+        step()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    clocks = ClockSampler(local)
+    clocks.start()
+    launches0 = gv.kernel_launches()
+    ms, emb_local = [], 0
+    counts = sup = None
+    for _ in range(args.steps):
+        with torch.cuda.stream(stream):
+            flush.zero_()  # evict L2 between steps (outside the timed events)
+        stream.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        counts, sup, _ = step()
+        e1.record(stream)
+        e1.synchronize()
+        ms.append(e0.elapsed_time(e1))
+        emb_local += int(counts.sum())
+    launches = gv.kernel_launches() - launches0
+    clk = clocks.stop()
+    if dist:
+        dist.barrier()
+
+    def red(x, op):
+        if not dist:
+            return x
+        t = torch.tensor([float(x)], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=op)
+        return float(t.item())
+
+    t_sum = red(sum(ms), dist.ReduceOp.MAX if dist else None)
+    emb_all = red(emb_local, dist.ReduceOp.SUM if dist else None)
+    value = emb_all / (t_sum / 1000.0)
+    patterns_per_s = len(queries) * world * args.steps / (t_sum / 1000.0)
+
+    # ---- one profiled step: per-kernel CUDA events for the roofline
+    with torch.cuda.stream(stream):
+        flush.zero_()
+    stream.synchronize()
+    torch.cuda.nvtx.range_push("profiled_step")
+    _, _, pstats = step(profile=True)
+    torch.cuda.nvtx.range_pop()
+    kstats = {k: v for k, v in pstats["kernels"].items() if v["launches"]}
+
+    # ---- plain per-pattern GPU path on a sample of the same patterns
+    sample = plans[:args.sample]
+
+    def wall(fn, reps=3):
+        fn()
+        fn()
+        ts, out = [], None
+        for _ in range(reps):
+            torch.cuda.synchronize()
+            t1 = time.perf_counter()
+            out = fn()
+            torch.cuda.synchronize()
+            ts.append(time.perf_counter() - t1)
+        return statistics.mean(ts), out
+
+    def batched_sample():
+        c, s2, _ = gv.batch_count(gdb, sample, stream=sp, support=True)
+        return int(c.sum()), s2
+
+    def plain_sample():
+        n, s2 = 0, []
+        for p in sample:
+            r = gv.match(gdb, p, stream=sp)
+            rows = r.rows()
+            n += rows.shape[0]
+            s2.append(len(np.unique(db.graph_of(rows[:, 0].astype(np.int64)))) if rows.size else 0)
+            r.close()
+        return n, s2
+
+    def plain_count_sample():
+        n = 0
+        for p in sample:
+            r = gv.match(gdb, p, stream=sp, count_only=True)
+            n += r.num_rows
+            r.close()
+        return n
+
+    t_b, (n_b, s_b) = wall(batched_sample)
+    t_p, (n_p, s_p) = wall(plain_sample)
+    t_pc, n_pc = wall(plain_count_sample)
+    plain_ok = n_b == n_p == n_pc and list(s_b) == list(s_p)
+
+    # ---- end to end through the public API: pattern texts in (planned on the
+    # host's cores), counts and supports out to host memory; database resident
+    e2e_steps = max(1, args.steps)
+    h2d = sum(len(q.encode()) for q in queries)
+    d2h = len(queries) * (8 + 4)
+    torch.cuda.synchronize()
+    t1 = time.perf_counter()
+    e2e_emb = 0
+    for _ in range(e2e_steps):
+        ps = gv.Plan.batch_from_texts(queries)
+        c, _, _ = gv.batch_count(gdb, ps, stream=sp, support=True)
+        e2e_emb += int(c.sum())
+        for p in ps:
+            p.close()
+    torch.cuda.synchronize()
+    e2e_t = red(time.perf_counter() - t1, dist.ReduceOp.MAX if dist else None)
+    e2e_value = red(e2e_emb, dist.ReduceOp.SUM if dist else None) / e2e_t
+
+    peak, peak_kind = measured_peak_gbs()
+    name, s = max(kstats.items(), key=lambda kv: kv[1]["ms"]) if kstats else ("none", {"launches": 0, "ms": 0, "bytes": 0})
+    per_launch_ms = s["ms"] / max(s["launches"], 1)
+    achieved = (s["bytes"] / max(s["launches"], 1)) / (per_launch_ms / 1000.0) / 1e9 if per_launch_ms else 0.0
+    out = {
+        "metric": "embeddings/s", "value": value, "unit": "embeddings/s", "n_gpus": world,
+        "steps": args.steps, "warmup": max(args.warmup, 3), "ms_per_step": t_sum / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
+        "data": "synthetic (seeded generator of the configuration's shapes)",
+        "patterns_per_s": patterns_per_s,
+        "config": batch_config(args, world),
+        "embeddings_per_step": emb_all / args.steps,
+        "database": {"vertices": db.num_vertices, "edges": db.num_edges, "graphs": len(db.first) - 1,
+                     "build_upload_s": build_s, "device_bytes": gdb.info()["device_bytes"]},
+        "plain": {"sample": f"first {len(sample)} patterns of the list",
+                  "batched_embeddings_per_s": n_b / t_b, "plain_embeddings_per_s": n_p / t_p,
+                  "batched_over_plain": t_p / t_b,
+                  "plain_count_only_embeddings_per_s": n_pc / t_pc, "batched_over_plain_count_only": t_pc / t_b,
+                  "agree": plain_ok,
+                  "timing": "wall clock, mean of 3 calls after 2 warm-up calls per path",
+                  "path": "batched = one gva_batch_count with supports; plain = one gva_match per pattern, rows "
+                          "to host, support from their graph ids (count_only: embeddings only)"},
+        "roofline": {"bound": "hbm", "kernel": name, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "peak_source": peak_kind, "traffic": ncu_traffic(name, s),
+                     "launches": s["launches"], "kernel_ms": s["ms"]},
+        "kernels": kstats,
+        "batch": {k: pstats[k] for k in ("rounds", "splits", "launches", "trie_nodes")},
+        "e2e": {"value": e2e_value, "unit": "embeddings/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                "note": "pattern texts planned on the host's cores each step (gva_plan_batch), matched, counts and "
+                        "supports copied to host memory; database resident"},
+        "gpu_launches": launches,
+        "clocks": clk,
+    }
+    gdb.close()
+    del flush
+    if rank == 0 and world == 1:
+        parity, base = oracle_check(db, queries, counts, sup)
+        out["parity"] = parity
+        out["cpu_baseline"] = base
+        if args.mining_steps > 0:
+            out["mining"] = mining_extra(args, local, torch, gv, db)
+    return out
+
+
+def mining_extra(args, local, torch, gv, db):
+    """A complete mining run of the same database (patterns up to 6 edges,
+    support >= 2 %), timed with CUDA events over --mining-steps steps."""
+    gdb = gv.Database.from_edges(db.vlabels, db.src, db.dst, db.elabels, device=local)
+    gdb.set_graphs(db.first)
+    G = len(db.first) - 1
+    minsup = int(np.ceil(0.02 * G))
+    stream = torch.cuda.Stream()
+    sp = stream.cuda_stream
+    for _ in range(3):
+        gv.mine(gdb, 6, minsup, stream=sp)
+    ms, emb, cands, stats, pats = [], 0, 0, None, None
+    for _ in range(args.mining_steps):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        pats, stats = gv.mine(gdb, 6, minsup, stream=sp)
+        e1.record(stream)
+        e1.synchronize()
+        ms.append(e0.elapsed_time(e1))
+        emb += stats["embeddings"]
+        cands += stats["candidates"]
+    t = sum(ms) / 1000.0
+    gdb.close()
+    return dict({"workload": MINE_WORKLOAD.format(me=6, ms=0.02), "steps": args.mining_steps,
+                 "ms_per_step": 1000 * t / args.mining_steps, "embeddings_per_s": emb / t,
+                 "patterns_per_s": cands / t, "frequent_patterns": len(pats), "min_support_graphs": minsup},
+                **{k: stats[k] for k in ("levels", "candidates", "frequent", "pruned", "gpu_ms", "host_ms", "gen_ms",
+                                         "plan_ms", "eval_ms", "merge_ms", "submit_ms", "round_host_ms", "wait_ms")},
+                host_cpus=os.cpu_count())
+
+
 # ------------------------------------------------------------------ GPU arm ----
 def main():
     args = parse_args()
@@ -687,6 +972,12 @@ def main():
 
     if args.impl == "reference":
         if rank != 0:
+            return 0
+        if args.workload == "batch":
+            db = workloads.config2(seed=args.seed)
+            queries = batch_patterns(args, db, 0, world, workloads)
+            print(json.dumps(reference_arm(args, db, queries, BATCH_WORKLOAD, config=batch_config(args, world))),
+                  flush=True)
             return 0
         if args.workload == "mine":
             c1 = args.db == "config1"
@@ -719,6 +1010,17 @@ def main():
             dist.destroy_process_group()
         if rank == 0:
             print(json.dumps(mni_bench(args, local, torch, gv, workloads)), flush=True)
+        return 0
+    if args.workload == "batch":
+        out = batch_bench(args, rank, world, local, dist, torch, gv, workloads)
+        if dist:
+            dist.barrier()
+            dist.destroy_process_group()
+        if rank == 0:
+            print(json.dumps(out), flush=True)
+            if out.get("parity", {}).get("mismatches"):
+                print(f"parity mismatch: {out['parity']}", file=sys.stderr)
+                return 1
         return 0
     if args.workload == "mine":
         from geneva_b200 import shard

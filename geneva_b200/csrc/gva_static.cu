@@ -11,15 +11,19 @@
 // Limits and rules:
 //   * in_rows <= GVA_STATIC_MAX_ROWS (16,777,216); larger inputs are rejected
 //     with GVA_ERR_ARG before anything is launched.  The array takes
-//     (GVA_STATIC_MAX_ROWS / 256 + 1) * 8 bytes = 512 KiB + 8 bytes on every
-//     GPU that loads this library, held until the process exits.
+//     (GVA_STATIC_MAX_ROWS / 256 + 1) * 8 bytes rounded up to 256 bytes
+//     = 512 KiB + 256 bytes on every GPU that loads this library, held until
+//     the process exits.
 //   * Every call on a device shares that array, and it keeps whatever the
 //     previous call left in it.  Nothing needs clearing: the count kernel
 //     writes every block total it later scans.  Calls whose kernels overlap
 //     on the GPU (two streams, two threads) race on the array; serialise them.
 //   * The first call on a device looks up the array's device address with
 //     cudaGetSymbolAddress (that device current), once, and caches it; make
-//     that first call before any stream capture.
+//     that first call before any stream capture.  The cached address belongs
+//     to the device's current context: a caller that ends that context
+//     (cudaDeviceReset) must not call this entry point again in the same
+//     process.
 #include <cuda_runtime.h>
 
 #include <mutex>
@@ -33,9 +37,11 @@ namespace {
 
 constexpr uint64_t kStaticBlocks = (uint64_t)GVA_STATIC_MAX_ROWS / 256;  // 256 rows per count block
 
-// Block totals of one step (+1 slot for the grand total).  In host code this
-// name is only a stand-in for the symbol, never a device address.
-static __device__ __align__(256) uint64_t g_step_scratch[kStaticBlocks + 1];
+// Block totals of one step (+1 slot for the grand total), rounded up to the
+// 256-byte granule that run_step asks of every scratch buffer.  In host code
+// this name is only a stand-in for the symbol, never a device address.
+constexpr uint64_t kStaticScratchBytes = ((kStaticBlocks + 1) * sizeof(uint64_t) + 255) & ~(uint64_t)255;
+static __device__ __align__(256) uint64_t g_step_scratch[kStaticScratchBytes / sizeof(uint64_t)];
 
 std::mutex g_mu;
 void* g_scratch_addr[64] = {};
@@ -68,8 +74,7 @@ int run_step_static(DevDB& db, const Step& st, const uint32_t* in, uint64_t in_r
     void* scratch = nullptr;
     int rc = static_scratch(db.device, &scratch);
     if (rc) return rc;
-    return run_step(db, st, in, in_rows, out, out_cap, out_rows, scratch, (kStaticBlocks + 1) * sizeof(uint64_t),
-                    stream);
+    return run_step(db, st, in, in_rows, out, out_cap, out_rows, scratch, kStaticScratchBytes, stream);
 }
 
 }  // namespace gva

@@ -29,6 +29,7 @@ class GraphDB:
     elabels: np.ndarray          # uint32, 1..P
     first: np.ndarray            # int64, len G+1: graph g owns ids [first[g], first[g+1])
     params: Dict = field(default_factory=dict)
+    cache: Dict = field(default_factory=dict, repr=False, compare=False)  # derived lookups, built on first use
 
     @property
     def num_vertices(self) -> int:
@@ -131,11 +132,25 @@ def config2(seed: int = 2) -> GraphDB:
     return graph_database(20000, 20, 60, 4.0, 16, 1.2, 3, seed, "config2")
 
 
+def _edges_by_graph(db: GraphDB) -> Tuple[np.ndarray, np.ndarray]:
+    """Edge indices grouped by the graph of their source (a stable sort, so
+    each graph's edges keep their order in the edge arrays) and each graph's
+    range in that list; computed once per database."""
+    cached = db.cache.get("edges_by_graph")
+    if cached is None:
+        gsrc = db.graph_of(db.src.astype(np.int64))
+        order = np.argsort(gsrc, kind="stable")
+        bounds = np.searchsorted(gsrc[order], np.arange(len(db.first)))
+        cached = (order, bounds)
+        db.cache["edges_by_graph"] = cached
+    return cached
+
+
 def _adjacency(db: GraphDB, g: int):
-    lo, hi = int(db.first[g]), int(db.first[g + 1])
-    m = (db.src >= lo) & (db.src < hi)
+    order, bounds = _edges_by_graph(db)
+    idx = order[bounds[g]:bounds[g + 1]]
     adj: Dict[int, Dict[int, int]] = {}
-    for a, b, l in zip(db.src[m].tolist(), db.dst[m].tolist(), db.elabels[m].tolist()):
+    for a, b, l in zip(db.src[idx].tolist(), db.dst[idx].tolist(), db.elabels[idx].tolist()):
         adj.setdefault(a, {})[b] = l
         adj.setdefault(b, {})[a] = l
     return adj
@@ -176,6 +191,14 @@ def sample_patterns(db: GraphDB, count: int, vmin: int, vmax: int, seed: int, p_
         lines += [f"e {a} {b} {l}" for (a, b), l in sorted(es.items())]
         out.append("\n".join(lines) + "\n")
     return out
+
+
+def config2_patterns(db: GraphDB, count: int = 16384, seed: int = 1000) -> List[str]:
+    """The pattern list matched against the 20,000-graph database: `count`
+    connected patterns of 2-7 vertices (a random growth tree inside a random
+    graph plus each other edge among the chosen vertices with probability
+    1/2, labels copied), so every pattern has at least one embedding."""
+    return sample_patterns(db, count, 2, 7, seed=seed)
 
 
 def config3_queries(db: GraphDB, count: int = 4096, seed: int = 1000) -> List[str]:

@@ -337,13 +337,15 @@ int gva_step_run(gva_db* db, const gva_plan* plan, int step, const uint32_t* in_
  * (a request path that must not reach cudaMalloc, or a host runtime that owns
  * all device memory); it has no counterpart in the reference.  Same
  * arguments and results as gva_step_run minus the scratch buffer: the step's
- * scratch is a fixed array in the library's device memory (512 KiB + 8 bytes
- * per GPU, held until exit), so in_rows may not exceed GVA_STATIC_MAX_ROWS
+ * scratch is a fixed array in the library's device memory (512 KiB + 256
+ * bytes per GPU, held until exit), so in_rows may not exceed GVA_STATIC_MAX_ROWS
  * (GVA_ERR_ARG otherwise, nothing launched).  It allocates no device memory.
  * Every call on a device shares the array: calls whose kernels overlap on the
  * GPU race, so serialise them.  The first call on a device looks up the
  * array's address (cudaGetSymbolAddress) once; make it before any stream
- * capture. */
+ * capture.  That address belongs to the device's context: after the caller
+ * ends the context (cudaDeviceReset) this entry point must not be called
+ * again in the same process. */
 #define GVA_STATIC_MAX_ROWS 16777216u
 int gva_step_run_static(gva_db* db, const gva_plan* plan, int step, const uint32_t* in_dev, uint64_t in_rows,
                         uint32_t* out_dev, uint64_t out_capacity_rows, uint64_t* out_rows, void* stream);

@@ -872,6 +872,25 @@ int oracle_count_capped(const oracle_graph* g, const char* text, uint64_t cap_ro
     return 0;
 }
 
+int oracle_graph_counts(const oracle_graph* g, const char* text, const int64_t* first, uint32_t G, uint64_t* counts,
+                        uint64_t* nrows) {
+    Planner p;
+    if (!p.plan(text)) return fail("planner failed");
+    Matcher m(*g, p);
+    m.run();
+    for (uint32_t i = 0; i < G; ++i) counts[i] = 0;
+    const uint64_t n = m.width ? m.cur.size() / m.width : 0;
+    *nrows = n;
+    for (uint64_t r = 0; r < n; ++r) {
+        const int64_t v = m.cur[r * m.width];
+        // graph of v: the last i with first[i] <= v
+        const int64_t* it = std::upper_bound(first, first + G + 1, v);
+        const int64_t i = (it - first) - 1;
+        if (i >= 0 && i < (int64_t)G) ++counts[i];
+    }
+    return 0;
+}
+
 void oracle_free(void* p) { free(p); }
 
 }  // extern "C"

@@ -39,6 +39,15 @@ int oracle_match(const oracle_graph* g, const char* query_text, uint32_t** rows,
 int oracle_count(const oracle_graph* g, const char* query_text, uint64_t* nrows);
 /* Same, giving up (returns 2) once any frontier holds about cap_rows rows. */
 int oracle_count_capped(const oracle_graph* g, const char* query_text, uint64_t cap_rows, uint64_t* nrows);
+/* Embeddings per graph of a graph database: graph i owns the vertex ids
+ * [first[i], first[i+1]) (first has G + 1 ascending entries); counts[i]
+ * receives the final rows whose first column lies in graph i, *nrows all
+ * final rows (rows outside every graph are counted only there).  The query's
+ * support is the number of graphs with a nonzero count.  This is the
+ * post-process that maps cpumine's rows to graph ids, done without handing
+ * the rows out. */
+int oracle_graph_counts(const oracle_graph* g, const char* query_text, const int64_t* first, uint32_t G,
+                        uint64_t* counts, uint64_t* nrows);
 void oracle_free(void* p);
 const char* oracle_last_error(void);
 

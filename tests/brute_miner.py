@@ -81,3 +81,38 @@ def mine(db, max_edges: int, min_support: int) -> Dict[Tuple, int]:
         for c in found:
             support[c] += 1
     return {c: s for c, s in support.items() if s >= min_support}
+
+
+def build_native(workdir) -> str:
+    """Compiles tests/brute_mine.cpp (the same definition in C++, for databases
+    of a thousand graphs) into workdir; returns the executable's path."""
+    import shutil
+    import subprocess
+    from pathlib import Path
+    exe = Path(workdir) / "brute_mine"
+    if not exe.exists():
+        cxx = shutil.which("g++") or "g++"
+        subprocess.run([cxx, "-O2", "-std=c++17", "-o", str(exe), str(Path(__file__).with_name("brute_mine.cpp"))],
+                       check=True, capture_output=True, text=True)
+    return str(exe)
+
+
+def mine_native(db, max_edges: int, min_support: int, exe: str, workdir) -> Dict[Tuple, int]:
+    """mine() computed by the C++ brute force: {canonical code: support}."""
+    import subprocess
+    from pathlib import Path
+    inp = Path(workdir) / f"brute_{db.name}.txt"
+    with open(inp, "w") as f:
+        V = len(db.vlabels) - 1
+        G = len(db.first) - 1
+        f.write(f"{V} {len(db.src)} {G}\n")
+        f.write(" ".join(map(str, db.vlabels[1:].tolist())) + "\n")
+        for a, b, l in zip(db.src.tolist(), db.dst.tolist(), db.elabels.tolist()):
+            f.write(f"{a} {b} {l}\n")
+        f.write(" ".join(map(str, db.first.tolist())) + "\n")
+    r = subprocess.run([exe, str(inp), str(max_edges), str(min_support)], capture_output=True, text=True, check=True)
+    out: Dict[Tuple, int] = {}
+    for line in r.stdout.splitlines():
+        t = list(map(int, line.split()))
+        out[tuple(t[1:])] = t[0]
+    return out

@@ -47,6 +47,7 @@ class Oracle:
                                      ctypes.c_int, P(ctypes.c_int)]
         lib.oracle_count.argtypes = [vp, ctypes.c_char_p, P(u64)]
         lib.oracle_count_capped.argtypes = [vp, ctypes.c_char_p, u64, P(u64)]
+        lib.oracle_graph_counts.argtypes = [vp, ctypes.c_char_p, vp, u32, vp, P(u64)]
         lib.oracle_free.argtypes = [vp]
         lib.oracle_last_error.restype = ctypes.c_char_p
         lib.oracle_mni_graph_from_edges.argtypes = [vp, u32, vp, vp, vp, u64, P(vp)]
@@ -103,6 +104,30 @@ class Oracle:
         if st:
             raise RuntimeError(self.lib.oracle_last_error().decode())
         return int(n.value)
+
+    def graph_counts(self, g, query_text: str, first):
+        """-> (embeddings per graph [G] uint64, support) for a graph database
+        whose graph i owns the vertex ids [first[i], first[i+1])."""
+        f = np.ascontiguousarray(first, dtype=np.int64)
+        G = len(f) - 1
+        out = np.zeros(max(G, 1), dtype=np.uint64)
+        n = ctypes.c_uint64()
+        if self.lib.oracle_graph_counts(g, query_text.encode(), f.ctypes.data, G, out.ctypes.data, ctypes.byref(n)):
+            raise RuntimeError(self.lib.oracle_last_error().decode())
+        out = out[:G]
+        return out, int((out > 0).sum())
+
+    def many_graph_counts(self, g, texts, first, threads: int = 0):
+        """graph_counts of every text on a thread pool (the calls release the
+        interpreter lock): -> (counts [n] uint64, supports [n] uint32)."""
+        import os
+        from concurrent.futures import ThreadPoolExecutor
+        threads = threads or (os.cpu_count() or 1)
+        with ThreadPoolExecutor(max_workers=threads) as ex:
+            res = list(ex.map(lambda t: self.graph_counts(g, t, first), texts))
+        counts = np.array([int(c.sum()) for c, _ in res], dtype=np.uint64)
+        sup = np.array([s for _, s in res], dtype=np.uint32)
+        return counts, sup, [c for c, _ in res]
 
     # ---- MNI on one data graph (CPU existence search) ----
     def mni_graph(self, vlabels, src, dst, elabel):

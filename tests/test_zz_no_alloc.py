@@ -84,3 +84,42 @@ def test_static_scratch_rejects_oversized_input(native):
     assert st == 5
     assert b"GVA_STATIC_MAX_ROWS" in lib.gva_last_error()
     db.close()
+
+
+def test_static_scratch_accepts_the_maximum_input(native):
+    """Exactly GVA_STATIC_MAX_ROWS input rows fit the fixed array: the step runs
+    (count pass over every row) and reports the rows it would write instead of
+    an argument error."""
+    torch = pytest.importorskip("torch")
+    lib = _declare(native)
+    g = GOLDEN / "graphs"
+    db = gv.loadDataBase(g / "syn_hub.mygraph", g / "syn_hub.metadata")
+    plan = gv.Plan.from_text(QUERY)
+    assert lib.gva_plan_step_width_in(plan._h, db._h, 1) == 1
+    max_rows = 1 << 24
+    # the seed step's vertices repeated up to the maximum row count
+    n0 = ctypes.c_uint64()
+    seed = torch.empty(1 << 16, dtype=torch.int32, device="cuda")
+    stream = torch.cuda.current_stream().cuda_stream
+    st = lib.gva_step_run_static(db._h, plan._h, 0, None, 0, seed.data_ptr(), seed.numel(), ctypes.byref(n0), stream)
+    assert st == 0 and n0.value > 0, lib.gva_last_error()
+    base = seed[: n0.value]
+    inp = base.repeat((max_rows + n0.value - 1) // n0.value)[:max_rows].contiguous()
+    torch.cuda.synchronize()
+    n = ctypes.c_uint64()
+    st = lib.gva_step_run_static(db._h, plan._h, 1, inp.data_ptr(), max_rows, None, 0, ctypes.byref(n), stream)
+    # the same step on one copy of the seed rows, caller scratch
+    n1 = ctypes.c_uint64()
+    scratch = torch.empty(lib.gva_step_scratch_bytes(n0.value), dtype=torch.uint8, device="cuda")
+    st1 = lib.gva_step_run(db._h, plan._h, 1, base.data_ptr(), n0.value, None, 0, ctypes.byref(n1),
+                           scratch.data_ptr(), scratch.numel(), stream)
+    assert st1 in (0, 4), lib.gva_last_error()
+    assert st in (0, 4), lib.gva_last_error()  # 4: the output does not fit (capacity 0); never an argument error
+    reps, rest = divmod(max_rows, n0.value)
+    n_rest = ctypes.c_uint64()
+    if rest:
+        st2 = lib.gva_step_run(db._h, plan._h, 1, base.data_ptr(), rest, None, 0, ctypes.byref(n_rest),
+                               scratch.data_ptr(), scratch.numel(), stream)
+        assert st2 in (0, 4), lib.gva_last_error()
+    assert n.value == reps * n1.value + n_rest.value
+    db.close()
