@@ -24,7 +24,7 @@ from typing import List, Optional, Sequence
 import numpy as np
 
 __all__ = [
-    "GenevaError", "Database", "probe_graph", "convert_g", "batch_count", "kernel_launches", "mine", "mni_support", "MinedPatterns", "MinedPattern", "Plan", "Result", "MODE_DV", "MODE_SV", "library", "library_path",
+    "GenevaError", "Database", "probe_graph", "convert_g", "batch_count", "kernel_launches", "mine", "mine_host", "mni_support", "MinedPatterns", "MinedPattern", "Plan", "Result", "MODE_DV", "MODE_SV", "library", "library_path",
     "loadDataBase", "genMatchOrder", "genMatchOrderSingleV", "match", "gpumine", "gpumineSV",
 ]
 
@@ -64,6 +64,9 @@ class _KernelStat(ctypes.Structure):
 REDUCE_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.POINTER(ctypes.c_uint32), ctypes.POINTER(ctypes.c_uint64),
                              ctypes.c_uint64, ctypes.c_void_p)
 
+
+EVAL_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.POINTER(ctypes.c_uint64), ctypes.c_uint64,
+                           ctypes.POINTER(ctypes.c_uint32), ctypes.POINTER(ctypes.c_uint64), ctypes.c_void_p)
 
 SUPPORT_GRAPHS = 0
 SUPPORT_MNI = 1
@@ -148,6 +151,7 @@ def _declare(lib):
         "gva_db_set_graphs": (i32, [vp, vp, u32]),
         "gva_convert_g": (i32, [cp, cp, cp, cp]),
         "gva_mine": (i32, [vp, P(_MineOpts), P(vp)]),
+        "gva_mine_host": (i32, [u32, vp, u32, vp, u32, u32, u32, EVAL_FN, vp, REDUCE_FN, vp, P(vp)]),
         "gva_mine_num_patterns": (i32, [vp]),
         "gva_mine_get": (i32, [vp, i32, P(u32), P(u32), P(u64)]),
         "gva_mine_pattern_text": (sz, [vp, i32, ctypes.c_char_p, sz]),
@@ -476,22 +480,63 @@ def mine(db: Database, max_edges: int, min_support: int, stream: Optional[int] =
     so that a server's other work keeps running.  Returns (patterns, stats);
     stats["kernels"] is filled when profiling."""
     lib = library()
-    cb = REDUCE_FN(0)
-    if reduce is not None:
-        def _cb(sp, ep, n, user):
-            try:
-                sup = np.ctypeslib.as_array(sp, shape=(n,))
-                emb = np.ctypeslib.as_array(ep, shape=(n,))
-                reduce(sup, emb)
-                return 0
-            except Exception:
-                return 1
-        cb = REDUCE_FN(_cb)
+    cb = _reduce_callback(reduce)
     mode = {"graphs": SUPPORT_GRAPHS, "mni": SUPPORT_MNI}[support]
     o = _MineOpts(stream or None, budget_bytes, max_edges, min_support, batch_limit, 1 if profile else 0, cb, None,
                   mode, mni_cap, ctypes.addressof(cancel) if cancel is not None else None, sm_percent, host_threads)
     h = ctypes.c_void_p()
     _check(lib.gva_mine(db._h, ctypes.byref(o), ctypes.byref(h)))
+    return _mine_result(h)
+
+
+def _reduce_callback(reduce):
+    if reduce is None:
+        return REDUCE_FN(0)
+
+    def _cb(sp, ep, n, user):
+        try:
+            sup = np.ctypeslib.as_array(sp, shape=(n,))
+            emb = np.ctypeslib.as_array(ep, shape=(n,))
+            reduce(sup, emb)
+            return 0
+        except Exception:
+            return 1
+    return REDUCE_FN(_cb)
+
+
+def mine_host(labels, num_edge_labels: int, max_edges: int, min_support: int, evaluate, reduce=None,
+              edge_labels=None, host_threads: int = 0):
+    """gva_mine's level loop on the host with a Python evaluator
+    (gva_mine_host): evaluate(texts) -> (supports, embeddings) for a list of
+    candidate query texts; reduce(supports, embeddings) as in mine().  labels
+    are the ascending vertex labels, edge labels 1..num_edge_labels (those in
+    edge_labels when given).  Returns (patterns, stats)."""
+    lib = library()
+    lab = np.ascontiguousarray(labels, dtype=np.uint32)
+    has = np.zeros(num_edge_labels + 1, dtype=np.uint8)
+    for el in (edge_labels if edge_labels is not None else range(1, num_edge_labels + 1)):
+        has[el] = 1
+
+    def _eval(tp, op, n, sp, ep, user):
+        try:
+            offs = np.ctypeslib.as_array(op, shape=(n,)).copy()
+            texts = [ctypes.string_at(tp + int(o)).decode() for o in offs]
+            sup, emb = evaluate(texts)
+            np.ctypeslib.as_array(sp, shape=(n,))[:] = np.asarray(sup, dtype=np.uint32)
+            np.ctypeslib.as_array(ep, shape=(n,))[:] = np.asarray(emb, dtype=np.uint64)
+            return 0
+        except Exception:
+            return 1
+    ecb = EVAL_FN(_eval)
+    rcb = _reduce_callback(reduce)
+    h = ctypes.c_void_p()
+    _check(lib.gva_mine_host(len(lab), lab.ctypes.data, num_edge_labels, has.ctypes.data, max_edges, min_support,
+                             host_threads, ecb, None, rcb, None, ctypes.byref(h)))
+    return _mine_result(h)
+
+
+def _mine_result(h):
+    lib = library()
     try:
         n = lib.gva_mine_num_patterns(h)
         need = lib.gva_mine_export(h, None, 0, None, None, None, None)

@@ -421,6 +421,24 @@ int gva_mine(gva_db* db, const gva_mine_opts* opts, gva_mine_result** out) {
     return GVA_OK;
 }
 
+int gva_mine_host(uint32_t num_labels, const uint32_t* labels, uint32_t num_edge_labels,
+                  const uint8_t* has_edge_label, uint32_t max_edges, uint32_t min_support, uint32_t host_threads,
+                  gva_eval_fn evaluate, void* eval_user, gva_reduce_fn reduce, void* reduce_user,
+                  gva_mine_result** out) {
+    if (!out || !labels || !has_edge_label) return fail(GVA_ERR_ARG, "null argument");
+    *out = nullptr;
+    gva_mine_result* r = new gva_mine_result();
+    std::vector<uint32_t> lab(labels, labels + num_labels);
+    int st = run_mine_host(lab, num_edge_labels, has_edge_label, max_edges, min_support, host_threads, evaluate,
+                           eval_user, reduce, reduce_user, r->pats, r->stats);
+    if (st) {
+        delete r;
+        return st;
+    }
+    *out = r;
+    return GVA_OK;
+}
+
 int gva_mine_num_patterns(const gva_mine_result* res) { return res ? (int)res->pats.size() : -1; }
 
 int gva_mine_get(const gva_mine_result* res, int index, uint32_t* edges, uint32_t* support, uint64_t* embeddings) {

@@ -252,6 +252,14 @@ int run_mine(DevDB& db, cudaStream_t s, uint64_t budget, uint32_t max_edges, uin
              uint32_t mni_cap, std::vector<MinedPattern>& out, MineStats& st, const volatile int* cancel = nullptr,
              uint32_t sm_percent = 0, uint32_t host_threads = 0);
 
+// mine_levels with a caller-supplied evaluator of candidate query texts
+// (host only; gva_mine_host).
+typedef int (*TextEvalFn)(const char* text, const uint64_t* offsets, uint64_t n, uint32_t* supports,
+                          uint64_t* embeddings, void* user);
+int run_mine_host(const std::vector<uint32_t>& labels, uint32_t num_edge_labels, const uint8_t* has_edge_label,
+                  uint32_t max_edges, uint32_t min_support, uint32_t host_threads, TextEvalFn evaluate,
+                  void* eval_user, ReduceFn reduce, void* reduce_user, std::vector<MinedPattern>& out, MineStats& st);
+
 // ---- single-graph MNI support (gva_mni.cu) ----
 constexpr int kMniMaxVertices = 8;
 // A connected pattern: dense vertex labels, el[a][b] = partition (1-based

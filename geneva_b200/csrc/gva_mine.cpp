@@ -290,4 +290,56 @@ int run_mine(DevDB& db, cudaStream_t s, uint64_t budget, uint32_t max_edges, uin
     return GVA_OK;
 }
 
+int run_mine_host(const std::vector<uint32_t>& labels, uint32_t num_edge_labels, const uint8_t* has_edge_label,
+                  uint32_t max_edges, uint32_t min_support, uint32_t host_threads, TextEvalFn evaluate,
+                  void* eval_user, ReduceFn reduce, void* reduce_user, std::vector<MinedPattern>& out, MineStats& st) {
+    out.clear();
+    st = MineStats();
+    if (!evaluate) return fail(GVA_ERR_ARG, "no evaluator");
+    if (labels.empty() || num_edge_labels == 0 || !has_edge_label) return fail(GVA_ERR_ARG, "no labels");
+    for (size_t i = 1; i < labels.size(); ++i)
+        if (labels[i] <= labels[i - 1]) return fail(GVA_ERR_ARG, "vertex labels must be ascending and distinct");
+    if (max_edges == 0 || max_edges + 1 > (uint32_t)GVA_MAX_QUERY_VERTICES)
+        return fail(GVA_ERR_ARG, "max_edges out of range");
+    const auto t0 = std::chrono::steady_clock::now();
+    const unsigned nthreads =
+        host_threads ? host_threads : std::max(1u, (unsigned)std::thread::hardware_concurrency());
+    std::vector<char> has_part(num_edge_labels + 1, 0);
+    for (uint32_t el = 1; el <= num_edge_labels; ++el) has_part[el] = has_edge_label[el] != 0;
+    std::string blob;
+    std::vector<uint64_t> offsets;
+    auto eval = [&](const std::vector<Pattern>& cands, std::vector<uint32_t>& sup, std::vector<uint64_t>& emb) -> int {
+        const size_t n = cands.size();
+        sup.assign(n, 0);
+        emb.assign(n, 0);
+        if (n == 0) return GVA_OK;
+        blob.clear();
+        offsets.resize(n);
+        for (size_t i = 0; i < n; ++i) {
+            offsets[i] = blob.size();
+            blob += query_text(cands[i], labels);
+            blob.push_back('\0');
+        }
+        if (evaluate(blob.data(), offsets.data(), n, sup.data(), emb.data(), eval_user))
+            return fail(GVA_ERR_ARG, "candidate evaluation failed");
+        st.candidates += n;
+        for (uint64_t e : emb) st.embeddings += e;  // this process's share
+        if (reduce && reduce(sup.data(), emb.data(), n, reduce_user))
+            return fail(GVA_ERR_ARG, "support reduction across processes failed");
+        return GVA_OK;
+    };
+    LevelStats ls;
+    int rc = mine_levels((uint32_t)labels.size(), num_edge_labels, has_part, labels, max_edges, min_support, nthreads,
+                         nullptr, eval, out, ls);
+    if (rc) return rc;
+    st.pruned = ls.pruned;
+    st.gen_ms = ls.gen_ms;
+    st.merge_ms = ls.merge_ms;
+    st.eval_ms = ls.eval_ms;
+    st.levels = ls.levels;
+    st.frequent = out.size();
+    st.host_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    return GVA_OK;
+}
+
 }  // namespace gva

@@ -266,6 +266,27 @@ typedef struct gva_mine_stats {
 
 typedef struct gva_mine_result gva_mine_result;
 
+/* Gives the support and embedding count of n candidate patterns, passed as
+ * query texts (text + offsets[i], NUL-terminated, original vertex and edge
+ * labels); return 0 on success. */
+typedef int (*gva_eval_fn)(const char* text, const uint64_t* offsets, uint64_t n, uint32_t* supports,
+                           uint64_t* embeddings, void* user);
+
+/* gva_mine's level loop on the host with the caller's evaluator instead of
+ * the GPU matcher: the same candidates (level-wise growth over the vertex
+ * labels labels[0..num_labels) (ascending, distinct) and the edge labels
+ * 1..num_edge_labels with has_edge_label[el] != 0, canonical dedupe,
+ * anti-monotone pruning), each level evaluated by `evaluate` and then
+ * combined by `reduce` (optional, e.g. an all-reduce over processes holding
+ * disjoint graph shards), patterns returned as by gva_mine (no kernel
+ * statistics).  No device work: it serves evaluators elsewhere (another
+ * process, a CPU checker) and the multi-process level loop's tests.  The
+ * reference has no pattern generation; it has no counterpart there. */
+int gva_mine_host(uint32_t num_labels, const uint32_t* labels, uint32_t num_edge_labels,
+                  const uint8_t* has_edge_label, uint32_t max_edges, uint32_t min_support, uint32_t host_threads,
+                  gva_eval_fn evaluate, void* eval_user, gva_reduce_fn reduce, void* reduce_user,
+                  gva_mine_result** out);
+
 int gva_mine(gva_db* db, const gva_mine_opts* opts, gva_mine_result** out);
 int gva_mine_num_patterns(const gva_mine_result* res);
 int gva_mine_get(const gva_mine_result* res, int index, uint32_t* edges, uint32_t* support, uint64_t* embeddings);

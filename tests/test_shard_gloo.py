@@ -1,9 +1,13 @@
 """Multi-process path on CPU: graph-database sharding and the per-level
 support reduction (geneva_b200.shard) over a world-size-2 gloo group.
 
-Each rank counts pattern supports on its own shard (brute force stands in
-for the GPU matcher, which these ranks do not have); SupportReducer sums
-them; the result must equal the counts on the whole database.
+Each rank counts pattern supports on its own shard (brute force or the oracle
+stand in for the GPU matcher, which these ranks do not have); SupportReducer
+sums them; the result must equal the counts on the whole database.  The
+second test drives the miner's own level loop (gva_mine_host: the loop
+gva_mine runs, with its reduce hook) on both ranks: every level's candidates
+must be the same on both ranks and the mined patterns those of one process
+holding the whole database.
 """
 import os
 import socket
@@ -73,3 +77,63 @@ def test_support_reduction_over_gloo(tmp_path):
     out = tmp_path / "result.txt"
     mp.spawn(_rank_main, args=(2, _free_port(), str(out)), nprocs=2, join=True)
     assert out.read_text() == "ok"
+
+
+def _oracle_eval(oracle, og, db, seen):
+    """Evaluator of a rank: supports and embedding counts of the candidates on
+    this rank's graphs, by the oracle; records every level's candidates."""
+    def ev(texts):
+        seen.append(list(texts))
+        c, sup, _ = oracle.many_graph_counts(og, texts, db.first, threads=2)
+        return sup, c
+    return ev
+
+
+def _level_loop_rank(rank, world, port, out_dir):
+    import json
+    import torch.distributed as dist
+    import geneva_b200 as gv
+    from geneva_b200.shard import SupportReducer
+    from oracle_lib import Oracle
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    db = workloads.graph_database(80, 5, 12, 2.8, 3, None, 2, seed=23, name="t")
+    part = shard_database(db, rank, world)
+    oracle = Oracle.get()
+    og = oracle.from_edges(part.vlabels, part.src, part.dst, part.elabels)
+    seen = []
+    labels = np.unique(db.vlabels[1:])  # every rank mines over the database's labels
+    pats, st = gv.mine_host(labels, 2, 4, 6, _oracle_eval(oracle, og, part, seen), reduce=SupportReducer(),
+                            host_threads=2)
+    oracle.free(og)
+    with open(os.path.join(out_dir, f"rank{rank}.json"), "w") as f:
+        json.dump({"levels": seen, "patterns": [[p.text, p.support, p.embeddings] for p in pats],
+                   "candidates": st["candidates"]}, f)
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+def test_mining_level_loop_over_gloo(tmp_path):
+    import json
+    import geneva_b200 as gv
+    from brute_miner import mine as brute_mine, pattern_from_text
+    from oracle_lib import Oracle
+    mp = pytest.importorskip("torch.multiprocessing")
+    mp.spawn(_level_loop_rank, args=(2, _free_port(), str(tmp_path)), nprocs=2, join=True)
+    r0 = json.loads((tmp_path / "rank0.json").read_text())
+    r1 = json.loads((tmp_path / "rank1.json").read_text())
+    # both ranks evaluated the same candidates, level by level, and took the same decisions
+    assert r0["levels"] == r1["levels"] and len(r0["levels"]) >= 3
+    assert r0["patterns"] == r1["patterns"]
+    # and those of one process holding every graph
+    db = workloads.graph_database(80, 5, 12, 2.8, 3, None, 2, seed=23, name="t")
+    oracle = Oracle.get()
+    og = oracle.from_edges(db.vlabels, db.src, db.dst, db.elabels)
+    seen = []
+    pats, _ = gv.mine_host(np.unique(db.vlabels[1:]), 2, 4, 6, _oracle_eval(oracle, og, db, seen), host_threads=2)
+    oracle.free(og)
+    assert seen == r0["levels"]
+    assert [[p.text, p.support, p.embeddings] for p in pats] == r0["patterns"]
+    # embedding counts summed through the reduce hook (uint64 through int64) equal the whole database's
+    want = brute_mine(db, 4, 6)
+    assert {pattern_from_text(t): s for t, s, _ in r0["patterns"]} == want
