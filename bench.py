@@ -88,6 +88,8 @@ def parse_args():
     ap.add_argument("--impl", default="geneva", choices=["geneva", "reference"])
     ap.add_argument("--workload", default="batch", choices=["batch", "mine", "match", "serve", "mni"])
     ap.add_argument("--patterns", type=int, default=16384, help="batch workload: patterns per rank per step")
+    ap.add_argument("--tune-patterns", type=int, default=2048,
+                    help="batch workload: patterns of the autotuner's calibration batch (0: default launch shape)")
     ap.add_argument("--mining-steps", type=int, default=3,
                     help="batch workload: timed steps of the mining run reported beside it (0: none)")
     ap.add_argument("--rates", default="10,100,500,2000", help="serve workload: arrival rates (req/s)")
@@ -773,6 +775,9 @@ def batch_bench(args, rank, world, local, dist, torch, gv, workloads):
     stream = torch.cuda.Stream()
     sp = stream.cuda_stream
     flush = torch.empty(512 << 20, dtype=torch.uint8, device="cuda")
+    # launch shape of the round kernels: chosen on a calibration slice of the
+    # list (untimed), kept for every step
+    tuning = gdb.autotune(plans[:args.tune_patterns], stream=sp) if args.tune_patterns > 0 else gdb.tuning
 
     def step(profile=False):
         counts, sup, stats = gv.batch_count(gdb, plans, stream=sp, support=True, profile=profile)
@@ -912,7 +917,10 @@ def batch_bench(args, rank, world, local, dist, torch, gv, workloads):
                      "frac": achieved / peak, "peak_source": peak_kind, "traffic": ncu_traffic(name, s),
                      "launches": s["launches"], "kernel_ms": s["ms"]},
         "kernels": kstats,
-        "batch": {k: pstats[k] for k in ("rounds", "splits", "launches", "trie_nodes")},
+        "batch": {k: pstats[k] for k in ("rounds", "splits", "launches", "trie_nodes", "gpu_ms", "lower_ms",
+                                         "submit_ms", "round_host_ms", "wait_ms", "session_ms")},
+        "tuning": dict(tuning, calibration=f"first {min(args.tune_patterns, len(plans))} patterns of the list, "
+                                           f"counted with supports, each launch shape twice (gva_db_autotune)"),
         "e2e": {"value": e2e_value, "unit": "embeddings/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "note": "pattern texts planned on the host's cores each step (gva_plan_batch), matched, counts and "
                         "supports copied to host memory; database resident"},

@@ -99,9 +99,16 @@ class _BatchOpts(ctypes.Structure):
                 ("reserved", ctypes.c_int)]
 
 
+class _Tuning(ctypes.Structure):
+    _fields_ = [("rows_per_item", ctypes.c_uint32), ("hub", ctypes.c_uint32), ("ms", ctypes.c_double),
+                ("default_ms", ctypes.c_double), ("tried", ctypes.c_uint32), ("reserved", ctypes.c_uint32)]
+
+
 class _BatchStats(ctypes.Structure):
     _fields_ = [("gpu_ms", ctypes.c_double), ("rounds", ctypes.c_uint64), ("splits", ctypes.c_uint64),
-                ("launches", ctypes.c_uint64), ("trie_nodes", ctypes.c_uint64), ("kernels", _KernelStat * 5)]
+                ("launches", ctypes.c_uint64), ("trie_nodes", ctypes.c_uint64), ("kernels", _KernelStat * 5),
+                ("lower_ms", ctypes.c_double), ("submit_ms", ctypes.c_double), ("round_host_ms", ctypes.c_double),
+                ("wait_ms", ctypes.c_double), ("session_ms", ctypes.c_double)]
 
 
 class _MniStats(ctypes.Structure):
@@ -151,6 +158,9 @@ def _declare(lib):
         "gva_db_set_graphs": (i32, [vp, vp, u32]),
         "gva_convert_g": (i32, [cp, cp, cp, cp]),
         "gva_mine": (i32, [vp, P(_MineOpts), P(vp)]),
+        "gva_db_get_tuning": (i32, [vp, P(_Tuning)]),
+        "gva_db_set_tuning": (i32, [vp, P(_Tuning)]),
+        "gva_db_autotune": (i32, [vp, vp, i32, vp, P(_Tuning)]),
         "gva_mine_host": (i32, [u32, vp, u32, vp, u32, u32, u32, EVAL_FN, vp, REDUCE_FN, vp, P(vp)]),
         "gva_mine_num_patterns": (i32, [vp]),
         "gva_mine_get": (i32, [vp, i32, P(u32), P(u32), P(u64)]),
@@ -224,6 +234,26 @@ class Database:
         f = np.ascontiguousarray(first, dtype=np.uint64)
         _check(library().gva_db_set_graphs(self._h, f.ctypes.data, len(f) - 1))
         self.num_graphs = len(f) - 1
+
+    @property
+    def tuning(self) -> dict:
+        """Launch shape of the batched engine's round kernels on this database."""
+        t = _Tuning()
+        _check(library().gva_db_get_tuning(self._h, ctypes.byref(t)))
+        return {"rows_per_item": int(t.rows_per_item), "hub": int(t.hub)}
+
+    def set_tuning(self, rows_per_item: int, hub: int) -> None:
+        t = _Tuning(rows_per_item, hub, 0.0, 0.0, 0, 0)
+        _check(library().gva_db_set_tuning(self._h, ctypes.byref(t)))
+
+    def autotune(self, plans, stream: Optional[int] = None) -> dict:
+        """Times a calibration batch under each candidate launch shape and keeps
+        the fastest (gva_db_autotune)."""
+        arr = (ctypes.c_void_p * max(len(plans), 1))(*[p._h.value for p in plans])
+        t = _Tuning()
+        _check(library().gva_db_autotune(self._h, arr, len(plans), stream or None, ctypes.byref(t)))
+        return {"rows_per_item": int(t.rows_per_item), "hub": int(t.hub), "ms": float(t.ms),
+                "default_ms": float(t.default_ms), "shapes_tried": int(t.tried)}
 
     def close(self):
         if self._h:
@@ -410,7 +440,8 @@ def batch_count(db: Database, plans: Sequence[Plan], stream: Optional[int] = Non
                                      gc.ctypes.data if gc is not None else None,
                                      sup.ctypes.data if sup is not None else None, ctypes.byref(st)))
     stats = {"gpu_ms": st.gpu_ms, "rounds": int(st.rounds), "splits": int(st.splits), "launches": int(st.launches),
-             "trie_nodes": int(st.trie_nodes),
+             "trie_nodes": int(st.trie_nodes), "lower_ms": st.lower_ms, "submit_ms": st.submit_ms,
+             "round_host_ms": st.round_host_ms, "wait_ms": st.wait_ms, "session_ms": st.session_ms,
              "kernels": {st.kernels[i].name.decode(): dict(launches=int(st.kernels[i].launches),
                                                            ms=float(st.kernels[i].ms), bytes=float(st.kernels[i].bytes),
                                                            rows=float(st.kernels[i].rows))

@@ -50,12 +50,14 @@ namespace {
 // needs per-graph accounting (slot `query`).
 enum TaskMode : uint32_t { MODE_WRITE = 0, MODE_COUNT = 1, MODE_COUNT_GRAPHS = 2, MODE_WRITE_AND_GRAPHS = 3 };
 
+// Step parameters of one trie node, uploaded once per node.  The frontier
+// fields of the argument blocks (in, nrows, out) are unused here: a task's
+// frontier slice comes with its TaskRef.
 struct TaskDesc {
     uint32_t kind;     // STEP_EXT / STEP_REDUCE
     uint32_t mode;     // TaskMode
-    uint32_t query;    // index into the batch
+    uint32_t query;    // per-graph result slot
     uint32_t pad;
-    uint64_t block0;   // first global block of this task
     union {
         ExtArgs e;
         RedArgs r;
@@ -70,44 +72,44 @@ struct BatchCtx {
     uint32_t words;           // bitmap words per query
 };
 
-// Per-round task reference: the step parameters live in a per-node
-// descriptor uploaded once per submitted wave; a round uploads only these.
+// Per-round task reference: a node's descriptor and a frontier slice.  The
+// slice is cut into items of `rows_per_item` rows; task t owns the count
+// pass's items [item0[t], item0[t + 1]).
 struct TaskRef {
     uint32_t node;
     uint32_t pad;
-    uint64_t block0;
     const uint32_t* in;
     uint64_t nrows;
 };
 
-// Descriptor of task t: its node's parameters patched, while they are copied,
-// with the task's frontier slice (ExtArgs and RedArgs both start with `in`,
-// `nrows`), so one barrier makes the copy visible.
-__device__ __forceinline__ void load_task(TaskDesc& d, const TaskDesc* __restrict__ nodes,
-                                          const TaskRef* __restrict__ refs, int t) {
-    constexpr int kB0 = (int)(offsetof(TaskDesc, block0) / 4);
-    constexpr int kIn = (int)((offsetof(TaskDesc, e) + offsetof(ExtArgs, in)) / 4);
-    constexpr int kNr = (int)((offsetof(TaskDesc, e) + offsetof(ExtArgs, nrows)) / 4);
-    static_assert(offsetof(ExtArgs, in) == offsetof(RedArgs, in) && offsetof(ExtArgs, nrows) == offsetof(RedArgs, nrows),
-                  "extension and reduction arguments share their frontier fields");
-    const TaskRef r = refs[t];
-    const uint32_t* s = reinterpret_cast<const uint32_t*>(nodes + r.node);
-    uint32_t* dw = reinterpret_cast<uint32_t*>(&d);
-    const uint64_t in = (uint64_t)r.in;
-    for (int i = threadIdx.x; i < (int)(sizeof(TaskDesc) / 4); i += blockDim.x) {
-        uint32_t v;
-        if (i == kB0 || i == kB0 + 1)
-            v = (uint32_t)(r.block0 >> (32 * (i - kB0)));
-        else if (i == kIn || i == kIn + 1)
-            v = (uint32_t)(in >> (32 * (i - kIn)));
-        else if (i == kNr || i == kNr + 1)
-            v = (uint32_t)(r.nrows >> (32 * (i - kNr)));
-        else
-            v = __ldg(s + i);
-        dw[i] = v;
-    }
-    __syncthreads();
-}
+constexpr int kRoundWarps = 8;          // warps per CTA of the round kernels
+constexpr int kMaxItemRows = 128;       // rows of one work item (a multiple of 32)
+constexpr int kTileRows = 64;           // output rows staged per warp before a coalesced flush
+constexpr int kScanChunk = 4096;        // items per CTA of the item scan
+constexpr int kScanChunkLog2 = 12;
+
+struct RoundArgs {
+    const TaskDesc* nodes;
+    const TaskRef* refs;
+    const uint64_t* item0;        // [nt + 1] count-pass item prefix
+    uint64_t n_items;             // items of this launch (count: all tasks; write: the writing tasks)
+    const uint32_t* wtask;        // write: task of each writing task slot (null for the count pass)
+    const uint64_t* witem0;       // write: [nw + 1] item prefix over the writing tasks
+    uint32_t nt;                  // tasks (count) or writing tasks (write)
+    uint32_t rows_per_item;       // multiple of 32, <= kMaxItemRows
+    uint32_t hub;                 // candidate lists longer than this are shared by the whole warp
+    uint32_t kmax;                // widest input row of the round (shared-memory layout)
+    uint64_t* items;              // count: per-item output rows; write: their exclusive scan
+    const uint64_t* chunks;       // write: exclusive scan of the per-chunk sums, chunks[n_chunks] = total
+    uint64_t n_count_items;       // write: items of the count pass
+    uint64_t n_chunks;            // write: scan chunks of the count pass
+    unsigned long long* queue;    // work-queue head (zeroed before the launch)
+    uint32_t total_warps;         // resident warps of the persistent grid
+    uint32_t pad2;
+    uint32_t* const* task_out;    // write: output base of each task (null: not written this round)
+    unsigned long long* read_words;  // optional: candidate-list words read (profiling)
+    BatchCtx ctx;
+};
 
 // Per-(query, graph) accounting of a final-step row: lanes of a warp whose
 // rows lie in the same graph (rows arrive grouped by their first vertex)
@@ -127,213 +129,445 @@ __device__ __forceinline__ void add_graph_count(const BatchCtx& c, uint32_t quer
     }
 }
 
-__global__ void __launch_bounds__(kThreads)
-batch_count_kernel(const TaskDesc* __restrict__ nodes, const TaskRef* __restrict__ refs,
-                   const uint32_t* __restrict__ blk_task, uint64_t* __restrict__ block_sums, BatchCtx ctx) {
-    __shared__ TaskDesc d;
-    const uint64_t b = blockIdx.x;
-    const int t = (int)__ldg(blk_task + b);
-    load_task(d, nodes, refs, t);
-    const uint64_t r = (b - d.block0) * kRowsPerBlock + threadIdx.x;
-    uint32_t c = 0;
-    uint32_t first = 0;
-    bool valid = false;
-    if (d.kind == STEP_EXT) {
-        valid = r < d.e.nrows;
-        if (valid) {
-            const uint32_t* row = d.e.in + r * d.e.k;
-            c = ext_count_row(d.e, row);
-            first = row[0];
-        }
-    } else {
-        valid = r < d.r.nrows;
-        if (valid) {
-            const uint32_t* row = d.r.in + r * d.r.k;
-            c = red_keep_row(d.r, row) ? 1u : 0u;
-            first = row[0];
+// Guided self-scheduling over a device work queue: a warp takes a chunk of
+// about 1/(2 x resident warps) of the items left (at least one), so the
+// queue sees few atomics while the last items still spread over every SM.
+__device__ __forceinline__ bool next_chunk(const RoundArgs& a, uint64_t& begin, uint64_t& end) {
+    const int lane = threadIdx.x & 31;
+    unsigned long long b = 0, n = 0;
+    if (lane == 0) {
+        const unsigned long long head = *(volatile unsigned long long*)a.queue;
+        if (head < a.n_items) {
+            n = (a.n_items - head) / (2ull * a.total_warps);
+            if (n == 0) n = 1;
+            b = atomicAdd(a.queue, n);
+        } else {
+            b = a.n_items;
         }
     }
-    if (d.mode == MODE_COUNT_GRAPHS || d.mode == MODE_WRITE_AND_GRAPHS) add_graph_count(ctx, d.query, first, c, valid);
-    // block total without a barrier: each warp adds its share (sums zeroed before the launch)
-    const uint64_t ws = warp_sum((uint64_t)c);
-    if ((threadIdx.x & 31) == 0 && ws) atomicAdd((unsigned long long*)(block_sums + b), (unsigned long long)ws);
+    b = __shfl_sync(0xffffffffu, b, 0);
+    n = __shfl_sync(0xffffffffu, n, 0);
+    begin = b;
+    end = b + n < a.n_items ? b + n : a.n_items;
+    return begin < a.n_items;
 }
 
-__global__ void task_totals_kernel(const uint64_t* __restrict__ block0, int ntasks, const uint64_t* __restrict__ sums,
-                                   uint64_t* __restrict__ totals) {
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t < ntasks) totals[t] = sums[block0[t + 1]] - sums[block0[t]];
+// last t in [0, n) with pfx[t] <= x (pfx ascending, pfx[0] <= x)
+__device__ __forceinline__ uint32_t find_slot(const uint64_t* __restrict__ pfx, uint32_t n, uint64_t x) {
+    uint32_t lo = 0, hi = n;
+    while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (__ldg(pfx + mid) <= x)
+            lo = mid;
+        else
+            hi = mid;
+    }
+    return lo;
 }
 
-// Persistent: each CTA repeatedly takes the next 256-row item.
-__global__ void __launch_bounds__(kThreads)
-batch_write_kernel(const TaskDesc* __restrict__ nodes, const TaskRef* __restrict__ refs,
-                   const uint64_t* __restrict__ block0, const uint32_t* __restrict__ blk_task, uint64_t nblocks,
-                   const uint64_t* __restrict__ sums, uint32_t* __restrict__ const* __restrict__ task_out,
-                   unsigned long long* __restrict__ queue) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    __shared__ TaskDesc d;
-    __shared__ unsigned long long item_s;
-    __shared__ uint64_t base_s;
-    for (;;) {
-        if (threadIdx.x == 0) item_s = atomicAdd(queue, 1ull);
-        __syncthreads();
-        const uint64_t b = item_s;
-        if (b >= nblocks) return;
-        const int t = (int)__ldg(blk_task + b);
-        uint32_t* out = task_out[t];
-        if (out == nullptr) {  // task deferred or counted only: nothing to write
-            __syncthreads();
-            continue;
-        }
-        if (threadIdx.x == 0) base_s = sums[b] - sums[block0[t]];  // task-local output row of this item
-        load_task(d, nodes, refs, t);
-        const uint64_t row0 = (b - d.block0) * kRowsPerBlock;
-        const uint64_t out0 = base_s;
-        if (d.kind == STEP_EXT && d.e.n_chk) {
-            // fused back-edge checks: each thread walks its row's generator
-            // segment twice (count, then write) and stores survivors directly
-            const ExtArgs& p = d.e;
-            const uint32_t k = p.k, k1 = p.k + 1;
-            uint32_t* rows_s = reinterpret_cast<uint32_t*>(smem_raw);
-            const uint32_t nr = (uint32_t)umin64((uint64_t)kRowsPerBlock, p.nrows - row0);
-            const uint32_t* gin = p.in + row0 * k;
-            for (uint32_t w = threadIdx.x; w < nr * k; w += kThreads) rows_s[w] = gin[w];
-            __syncthreads();
-            const uint32_t* row = rows_s + threadIdx.x * k;
+// One warp's copy of a node descriptor.
+__device__ __forceinline__ void load_desc(TaskDesc& d, const TaskDesc* __restrict__ src) {
+    const uint32_t* s = reinterpret_cast<const uint32_t*>(src);
+    uint32_t* dw = reinterpret_cast<uint32_t*>(&d);
+    for (int i = threadIdx.x & 31; i < (int)(sizeof(TaskDesc) / 4); i += 32) dw[i] = __ldg(s + i);
+    __syncwarp();
+}
+
+// Rows [row0, row0 + nr) of a frontier of width k into shared memory,
+// coalesced (16-byte loads when the slice is 16-byte aligned).
+__device__ __forceinline__ void stage_rows(uint32_t* rows_s, const uint32_t* __restrict__ in, uint64_t row0, uint32_t nr,
+                                           uint32_t k) {
+    const int lane = threadIdx.x & 31;
+    const uint32_t* src = in + row0 * k;
+    const uint32_t nw = nr * k;
+    uint32_t w0 = 0;
+    if ((((uintptr_t)src | (uintptr_t)rows_s) & 15) == 0) {
+        const uint32_t nv = nw >> 2;
+        const uint4* s4 = reinterpret_cast<const uint4*>(src);
+        uint4* d4 = reinterpret_cast<uint4*>(rows_s);
+        for (uint32_t v = lane; v < nv; v += 32) d4[v] = __ldg(s4 + v);
+        w0 = nv << 2;
+    }
+    for (uint32_t w = w0 + lane; w < nw; w += 32) rows_s[w] = __ldg(src + w);
+    __syncwarp();
+}
+
+// Broadcast of lane h's generator state (hub rows are processed by the whole warp).
+__device__ __forceinline__ GenState shfl_gen(const GenState& g, int h, uint32_t n_chk) {
+    GenState o;
+    o.lo = __shfl_sync(0xffffffffu, g.lo, h);
+    o.hi = __shfl_sync(0xffffffffu, g.hi, h);
+    o.which = __shfl_sync(0xffffffffu, g.which, h);
+    o.slo = __shfl_sync(0xffffffffu, g.slo, h);
+    o.shi = __shfl_sync(0xffffffffu, g.shi, h);
+    o.gadj = reinterpret_cast<const uint32_t*>(
+        __shfl_sync(0xffffffffu, (unsigned long long)reinterpret_cast<uintptr_t>(g.gadj), h));
+#pragma unroll
+    for (int i = 0; i < kMaxChecks; ++i) {
+        o.clo[i] = __shfl_sync(0xffffffffu, g.clo[i], h);
+        o.chi[i] = __shfl_sync(0xffffffffu, g.chi[i], h);
+    }
+    (void)n_chk;
+    return o;
+}
+
+// Candidate test of the plain extension (no fused checks): injectivity only;
+// the restriction bound is already applied to the range.
+__device__ __forceinline__ bool ext_injective(const ExtArgs& p, const uint32_t* row, uint32_t c) {
+    for (uint32_t j = 0; j < p.n_eq; ++j)
+        if (row[p.eq_cols[j]] == c) return false;
+    return true;
+}
+
+// Output staging of one warp: accepted (row, candidate) pairs are appended
+// in ballot order to a shared tile of kTileRows rows and flushed 32 rows at a
+// time with coalesced stores.
+struct Tile {
+    uint32_t* t;      // kTileRows * w words
+    uint32_t w;       // output row width
+    uint32_t n;       // rows held
+    uint32_t* out;    // next output row in global memory
+    uint64_t room;    // rows this item may still write (its count from the count pass)
+};
+
+__device__ __forceinline__ void tile_flush(Tile& tl, uint32_t rows) {
+    const int lane = threadIdx.x & 31;
+    const uint32_t nw = rows * tl.w;
+    // never past the item's counted rows, whatever the data (e.g. repeated
+    // neighbours, which the count and write tests would see differently)
+    const uint32_t keep = (uint32_t)umin64(rows, tl.room);
+    const uint32_t kw = keep * tl.w;
+    for (uint32_t w = lane; w < kw; w += 32) tl.out[w] = tl.t[w];
+    tl.out += kw;
+    tl.room -= keep;
+    __syncwarp();
+    const uint32_t rest = (tl.n - rows) * tl.w;
+    for (uint32_t w = lane; w < rest; w += 32) tl.t[w] = tl.t[nw + w];
+    tl.n -= rows;
+    __syncwarp();
+}
+
+// Appends, for every lane with `take`, its row (k words of `row`) followed by
+// `c` when `extend` (output width k + 1), else the row alone.
+__device__ __forceinline__ void tile_append(Tile& tl, bool take, const uint32_t* row, uint32_t k, uint32_t c,
+                                            bool extend) {
+    const int lane = threadIdx.x & 31;
+    const uint32_t m = __ballot_sync(0xffffffffu, take);
+    if (take) {
+        const uint32_t pos = tl.n + __popc(m & ((1u << lane) - 1u));
+        uint32_t* dst = tl.t + pos * tl.w;
+        for (uint32_t q = 0; q < k; ++q) dst[q] = row[q];
+        if (extend) dst[k] = c;
+    }
+    tl.n += __popc(m);
+    __syncwarp();
+    if (tl.n >= 32) tile_flush(tl, 32);
+}
+
+// ------------------------------------------------------------ one item ----
+// Extension step over the item's rows (staged in rows_s).  Each lane owns
+// rows lane, lane + 32, ...; a row's candidates come from its generator
+// segment (ext_generator); rows whose list is at most `hub` long are walked by
+// their lane, longer ones by the whole warp, 32 candidates per step.  COUNT
+// returns the item's accepted candidates (valid in every lane) and does the
+// per-graph accounting; WRITE appends every accepted (row, candidate) to the
+// tile.  Both visit the same candidates with the same test.
+template <bool WRITE>
+__device__ __forceinline__ uint64_t ext_item(const TaskDesc& d, const uint32_t* rows_s, uint32_t nr, uint32_t hub,
+                                             const BatchCtx& ctx, Tile* tl, unsigned long long* read_words) {
+    const ExtArgs& p = d.e;
+    const int lane = threadIdx.x & 31;
+    const uint32_t k = p.k;
+    const bool graphs = !WRITE && (d.mode == MODE_COUNT_GRAPHS || d.mode == MODE_WRITE_AND_GRAPHS);
+    uint64_t total = 0;
+    uint64_t words = 0;
+    for (uint32_t base = 0; base < nr; base += 32) {
+        const uint32_t r = base + lane;
+        const bool valid = r < nr;
+        const uint32_t* row = rows_s + (valid ? r : 0) * k;
+        uint32_t cnt = 0;
+        if (!WRITE && p.n_chk == 0) {
+            // plain extension: the segment minus the matched vertices in it
+            if (valid) cnt = ext_count_row(p, row);
+        } else {
             GenState g;
             g.lo = g.hi = 0;
-            uint32_t cnt = 0, acc = 0;  // acc: verdicts of the first 32 candidates
-            if (threadIdx.x < nr) {
-                ext_generator(p, row, g);
-                for (uint32_t j = g.lo; j < g.hi; ++j) {
-                    const bool ok = ext_accept(p, row, __ldg(g.gadj + j), g);
-                    cnt += ok ? 1u : 0u;
-                    if (ok && j - g.lo < 32) acc |= 1u << (j - g.lo);
+            if (valid) {
+                if (p.n_chk) {
+                    ext_generator(p, row, g);
+                } else {
+                    ext_range(p, row, g.lo, g.hi);
+                    g.gadj = p.adj;
+                    g.which = -1;
                 }
             }
-            uint64_t total;
-            const uint64_t before = block_exclusive_scan(cnt, &total);
-            if (cnt) {
-                uint32_t* dst = out + (out0 + before) * k1;
-                for (uint32_t j = g.lo; j < g.hi; ++j) {
-                    const bool early = j - g.lo < 32;
-                    if (early && !(acc >> (j - g.lo) & 1)) continue;
-                    const uint32_t c = __ldg(g.gadj + j);
-                    if (!early && !ext_accept(p, row, c, g)) continue;
-                    for (uint32_t q = 0; q < k; ++q) dst[q] = row[q];
-                    dst[k] = c;
-                    dst += k1;
+            const uint32_t len = g.hi > g.lo ? g.hi - g.lo : 0;
+            const bool is_hub = len > hub;
+            const uint32_t mine = is_hub ? 0 : len;
+            words += mine;
+            // own rows: lanes step through their lists together
+            const uint32_t steps = __reduce_max_sync(0xffffffffu, mine);
+            for (uint32_t s = 0; s < steps; ++s) {
+                bool ok = false;
+                uint32_t c = 0;
+                if (s < mine) {
+                    c = __ldg(g.gadj + g.lo + s);
+                    ok = p.n_chk ? ext_accept(p, row, c, g) : ext_injective(p, row, c);
                 }
+                cnt += ok ? 1u : 0u;
+                if (WRITE) tile_append(*tl, ok, row, k, c, true);
             }
-            __syncthreads();
-        } else if (d.kind == STEP_EXT) {
-            const ExtArgs& p = d.e;
-            const uint32_t k = p.k, k1 = p.k + 1;
-            uint64_t* offs_s = reinterpret_cast<uint64_t*>(smem_raw);
-            uint32_t* rows_s = reinterpret_cast<uint32_t*>(offs_s + kRowsPerBlock + 1);
-            uint32_t* lo_s = rows_s + kRowsPerBlock * k;
-            uint32_t* ncol_s = lo_s + kRowsPerBlock;
-            uint32_t* coll_s = ncol_s + kRowsPerBlock;
-            uint32_t* out_s = coll_s + kRowsPerBlock * p.n_eq;
-            const uint32_t nr = (uint32_t)umin64((uint64_t)kRowsPerBlock, p.nrows - row0);
-            const uint32_t* gin = p.in + row0 * k;
-            for (uint32_t w = threadIdx.x; w < nr * k; w += kThreads) rows_s[w] = gin[w];
-            __syncthreads();
-            uint64_t cnt = 0;
-            if (threadIdx.x < nr) {
-                const uint32_t* row = rows_s + threadIdx.x * k;
-                uint32_t lo, hi;
-                ext_range(p, row, lo, hi);
-                uint32_t nc = 0;
-                uint32_t* mine = coll_s + threadIdx.x * p.n_eq;
-                if (lo < hi) {
-                    for (uint32_t j = 0; j < p.n_eq; ++j) {
-                        const uint32_t pos = find_in(p.adj, lo, hi, row[p.eq_cols[j]]);
-                        if (pos == 0xffffffffu) continue;
-                        bool dup = false;
-                        for (uint32_t i = 0; i < nc; ++i) dup |= (mine[i] == pos);
-                        if (dup) continue;
-                        uint32_t i = nc++;
-                        while (i > 0 && mine[i - 1] > pos) {
-                            mine[i] = mine[i - 1];
-                            --i;
-                        }
-                        mine[i] = pos;
+            // hub rows: the whole warp, 32 candidates per step
+            uint32_t hubs = __ballot_sync(0xffffffffu, is_hub);
+            while (hubs) {
+                const int h = __ffs(hubs) - 1;
+                hubs &= hubs - 1;
+                const GenState gh = shfl_gen(g, h, p.n_chk);
+                const uint32_t* hrow = rows_s + (base + h) * k;
+                uint32_t hc = 0;
+                for (uint32_t j0 = gh.lo; j0 < gh.hi; j0 += 32) {
+                    const uint32_t j = j0 + lane;
+                    bool ok = false;
+                    uint32_t c = 0;
+                    if (j < gh.hi) {
+                        c = __ldg(gh.gadj + j);
+                        ok = p.n_chk ? ext_accept(p, hrow, c, gh) : ext_injective(p, hrow, c);
                     }
-                    cnt = hi - lo - nc;
+                    hc += ok ? 1u : 0u;
+                    if (WRITE) tile_append(*tl, ok, hrow, k, c, true);
                 }
-                lo_s[threadIdx.x] = lo;
-                ncol_s[threadIdx.x] = nc;
+                hc = __reduce_add_sync(0xffffffffu, hc);
+                if (lane == h) cnt += hc;
+                if (lane == 0) words += gh.hi - gh.lo;
             }
-            uint64_t total;
-            const uint64_t before = block_exclusive_scan(cnt, &total);
-            offs_s[threadIdx.x] = before;
-            if (threadIdx.x == 0) offs_s[nr] = total;
-            __syncthreads();
-            for (uint64_t base = 0; base < total; base += kThreads) {
-                const uint64_t o = base + threadIdx.x;
-                if (o < total) {
-                    int a = 0, z = (int)nr - 1;
-                    while (a < z) {
-                        const int m = (a + z + 1) >> 1;
-                        if (offs_s[m] <= o)
-                            a = m;
-                        else
-                            z = m - 1;
-                    }
-                    uint32_t j = lo_s[a] + (uint32_t)(o - offs_s[a]);
-                    const uint32_t* mine = coll_s + a * p.n_eq;
-                    for (uint32_t c = 0; c < ncol_s[a]; ++c) j += (mine[c] <= j) ? 1u : 0u;
-                    uint32_t* dst = out_s + threadIdx.x * k1;
-                    const uint32_t* src = rows_s + a * k;
-                    for (uint32_t c = 0; c < k; ++c) dst[c] = src[c];
-                    dst[k] = __ldg(p.adj + j);
-                }
-                __syncthreads();
-                const uint32_t n_tile = (uint32_t)umin64((uint64_t)kThreads, total - base);
-                uint32_t* gout = out + (out0 + base) * k1;
-                for (uint32_t w = threadIdx.x; w < n_tile * k1; w += kThreads) gout[w] = out_s[w];
-                __syncthreads();
+        }
+        if (graphs) add_graph_count(ctx, d.query, row[0], cnt, valid);
+        total += cnt;
+    }
+    if (read_words) {
+        words = warp_sum(words);
+        if (lane == 0 && words) atomicAdd(read_words, (unsigned long long)words);
+    }
+    return warp_sum(total);
+}
+
+template <bool WRITE>
+__device__ __forceinline__ uint64_t red_item(const TaskDesc& d, const uint32_t* rows_s, uint32_t nr,
+                                             const BatchCtx& ctx, Tile* tl) {
+    const RedArgs& p = d.r;
+    const int lane = threadIdx.x & 31;
+    const uint32_t k = p.k;
+    const bool graphs = !WRITE && (d.mode == MODE_COUNT_GRAPHS || d.mode == MODE_WRITE_AND_GRAPHS);
+    uint64_t total = 0;
+    for (uint32_t base = 0; base < nr; base += 32) {
+        const uint32_t r = base + lane;
+        const bool valid = r < nr;
+        const uint32_t* row = rows_s + (valid ? r : 0) * k;
+        const bool keep = valid && red_keep_row(p, row);
+        if (WRITE) tile_append(*tl, keep, row, k, 0, false);
+        if (graphs) add_graph_count(ctx, d.query, row[0], keep ? 1u : 0u, valid);
+        total += keep ? 1u : 0u;
+    }
+    return warp_sum(total);
+}
+
+// Shared memory of one warp: its descriptor copy, the item's rows and the
+// output tile.
+__host__ __device__ constexpr size_t round_warp_words(uint32_t rows_per_item, uint32_t kmax) {
+    return (size_t)rows_per_item * kmax + (size_t)kTileRows * (kmax + 1);
+}
+size_t round_smem_bytes(uint32_t rows_per_item, uint32_t kmax) {
+    return (size_t)kRoundWarps * (sizeof(TaskDesc) + 4 * ((round_warp_words(rows_per_item, kmax) + 3) & ~(size_t)3));
+}
+
+// ---------------------------------------------------------- count pass ----
+// Persistent: warps pull chunks of items from the work queue; each item's
+// accepted rows go to items[item] (no atomics, no block barrier).
+__global__ void __launch_bounds__(kRoundWarps * 32, 4)
+round_count_kernel(RoundArgs a) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    TaskDesc* descs = reinterpret_cast<TaskDesc*>(smem_raw);
+    TaskDesc& d = descs[warp];
+    const size_t ww = (round_warp_words(a.rows_per_item, a.kmax) + 3) & ~(size_t)3;
+    uint32_t* rows_s = reinterpret_cast<uint32_t*>(smem_raw + kRoundWarps * sizeof(TaskDesc)) + warp * ww;
+    uint32_t t = 0xffffffffu;
+    uint64_t t_lo = 0, t_hi = 0;
+    const uint32_t* in = nullptr;
+    uint64_t nrows = 0;
+    uint64_t begin, end;
+    while (next_chunk(a, begin, end)) {
+        for (uint64_t item = begin; item < end; ++item) {
+            if (item >= t_hi || item < t_lo) {
+                t = find_slot(a.item0, a.nt + 1, item);
+                t_lo = __ldg(a.item0 + t);
+                t_hi = __ldg(a.item0 + t + 1);
+                const TaskRef& ref = a.refs[t];
+                in = ref.in;
+                nrows = ref.nrows;
+                __syncwarp();
+                load_desc(d, a.nodes + ref.node);
             }
-        } else {
-            const RedArgs& p = d.r;
-            const uint32_t k = p.k;
-            uint32_t* rows_s = reinterpret_cast<uint32_t*>(smem_raw);
-            uint32_t* out_s = rows_s + kRowsPerBlock * k;
-            const uint32_t nr = (uint32_t)umin64((uint64_t)kRowsPerBlock, p.nrows - row0);
-            const uint32_t* gin = p.in + row0 * k;
-            for (uint32_t w = threadIdx.x; w < nr * k; w += kThreads) rows_s[w] = gin[w];
-            __syncthreads();
-            bool keep = false;
-            if (threadIdx.x < nr) keep = red_keep_row(p, rows_s + threadIdx.x * k);
-            uint64_t total;
-            const uint64_t before = block_exclusive_scan(keep ? 1 : 0, &total);
-            if (keep)
-                for (uint32_t c = 0; c < k; ++c) out_s[before * k + c] = rows_s[threadIdx.x * k + c];
-            __syncthreads();
-            uint32_t* gout = out + out0 * k;
-            for (uint32_t w = threadIdx.x; w < (uint32_t)total * k; w += kThreads) gout[w] = out_s[w];
-            __syncthreads();
+            const uint64_t row0 = (item - t_lo) * a.rows_per_item;
+            const uint32_t nr = (uint32_t)umin64(a.rows_per_item, nrows - row0);
+            const uint32_t k = d.kind == STEP_EXT ? d.e.k : d.r.k;
+            __syncwarp();
+            stage_rows(rows_s, in, row0, nr, k);
+            const uint64_t c = d.kind == STEP_EXT ? ext_item<false>(d, rows_s, nr, a.hub, a.ctx, nullptr, a.read_words)
+                                                  : red_item<false>(d, rows_s, nr, a.ctx, nullptr);
+            if (lane == 0) a.items[item] = c;
         }
     }
 }
 
-size_t batch_smem_bytes() {
-    // the larger of the extension layout at k = 31, n_eq = 32 and the reduction layout at k = 32
-    const size_t ext = sizeof(uint64_t) * (kRowsPerBlock + 1) +
-                       sizeof(uint32_t) * ((size_t)kRowsPerBlock * 31 + 2 * kRowsPerBlock + (size_t)kRowsPerBlock * 32 +
-                                           (size_t)kRowsPerBlock * 32);
-    const size_t red = sizeof(uint32_t) * 2 * (size_t)kRowsPerBlock * 32;
-    return std::max(ext, red);
+// --------------------------------------------------------- item scans ----
+// Exclusive scan of per-item counts in chunks of kScanChunk (in place);
+// chunks[c] receives chunk c's sum.
+__global__ void __launch_bounds__(1024) scan_items_local_kernel(uint64_t* __restrict__ v, uint64_t n,
+                                                               uint64_t* __restrict__ chunks) {
+    __shared__ uint64_t ws[32];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const uint64_t base = (uint64_t)blockIdx.x * kScanChunk + (uint64_t)threadIdx.x * 4;
+    uint64_t x[4];
+    uint64_t sum = 0;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        x[i] = base + i < n ? v[base + i] : 0;
+        sum += x[i];
+    }
+    uint64_t inc = sum;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint64_t y = __shfl_up_sync(0xffffffffu, inc, o);
+        if (lane >= o) inc += y;
+    }
+    if (lane == 31) ws[wid] = inc;
+    __syncthreads();
+    if (wid == 0) {
+        uint64_t w = ws[lane];
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint64_t y = __shfl_up_sync(0xffffffffu, w, o);
+            if (lane >= o) w += y;
+        }
+        ws[lane] = w;
+    }
+    __syncthreads();
+    uint64_t run = (wid > 0 ? ws[wid - 1] : 0) + inc - sum;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        if (base + i < n) v[base + i] = run;
+        run += x[i];
+    }
+    if (threadIdx.x == 1023) chunks[blockIdx.x] = ws[31];
 }
 
-size_t batch_smem_bytes_for(uint32_t kmax, uint32_t eqmax) {
-    const size_t ext = sizeof(uint64_t) * (kRowsPerBlock + 1) +
-                       sizeof(uint32_t) * ((size_t)kRowsPerBlock * kmax + 2 * kRowsPerBlock +
-                                           (size_t)kRowsPerBlock * eqmax + (size_t)kRowsPerBlock * (kmax + 1));
-    const size_t red = sizeof(uint32_t) * 2 * (size_t)kRowsPerBlock * (kmax + 1);
-    return std::max(ext, red);
+// Exclusive scan of the chunk sums (chunks[nc] = grand total), then each
+// task's output rows: totals[t] = offset(item0[t + 1]) - offset(item0[t]).
+__global__ void __launch_bounds__(1024) scan_items_top_kernel(uint64_t* __restrict__ chunks, uint64_t nc,
+                                                             const uint64_t* __restrict__ v, uint64_t n,
+                                                             const uint64_t* __restrict__ item0, uint32_t nt,
+                                                             uint64_t* __restrict__ totals) {
+    __shared__ uint64_t ws[32];
+    __shared__ uint64_t carry_s;
+    if (threadIdx.x == 0) carry_s = 0;
+    __syncthreads();
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    for (uint64_t b = 0; b < nc; b += 1024) {
+        const uint64_t i = b + threadIdx.x;
+        const uint64_t x = i < nc ? chunks[i] : 0;
+        uint64_t inc = x;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint64_t y = __shfl_up_sync(0xffffffffu, inc, o);
+            if (lane >= o) inc += y;
+        }
+        if (lane == 31) ws[wid] = inc;
+        __syncthreads();
+        if (wid == 0) {
+            uint64_t w = ws[lane];
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint64_t y = __shfl_up_sync(0xffffffffu, w, o);
+                if (lane >= o) w += y;
+            }
+            ws[lane] = w;
+        }
+        __syncthreads();
+        const uint64_t carry = carry_s;
+        if (i < nc) chunks[i] = carry + (wid > 0 ? ws[wid - 1] : 0) + inc - x;
+        __syncthreads();
+        if (threadIdx.x == 0) carry_s = carry + ws[31];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) chunks[nc] = carry_s;
+    __syncthreads();
+    const uint64_t grand = carry_s;
+    auto off = [&](uint64_t i) -> uint64_t { return i >= n ? grand : v[i] + chunks[i >> kScanChunkLog2]; };
+    for (uint32_t t = threadIdx.x; t < nt; t += 1024) totals[t] = off(item0[t + 1]) - off(item0[t]);
+}
+
+// ---------------------------------------------------------- write pass ----
+// Persistent, over the items of the tasks that write this round: each item's
+// output rows go to its task's buffer at the item's scanned offset, in the
+// order the count pass counted them.  Items without output are skipped.
+__global__ void __launch_bounds__(kRoundWarps * 32, 4)
+round_write_kernel(RoundArgs a) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int warp = threadIdx.x >> 5;
+    TaskDesc* descs = reinterpret_cast<TaskDesc*>(smem_raw);
+    TaskDesc& d = descs[warp];
+    const size_t ww = (round_warp_words(a.rows_per_item, a.kmax) + 3) & ~(size_t)3;
+    uint32_t* rows_s = reinterpret_cast<uint32_t*>(smem_raw + kRoundWarps * sizeof(TaskDesc)) + warp * ww;
+    uint32_t* tile_s = rows_s + (size_t)a.rows_per_item * a.kmax;
+    uint64_t w_lo = 0, w_hi = 0;
+    uint32_t t = 0;
+    uint64_t t_item0 = 0, t_off0 = 0;
+    uint32_t* out = nullptr;
+    const uint32_t* in = nullptr;
+    uint64_t nrows = 0;
+    uint64_t begin, end;
+    while (next_chunk(a, begin, end)) {
+        for (uint64_t wi = begin; wi < end; ++wi) {
+            if (wi >= w_hi || wi < w_lo) {
+                const uint32_t slot = find_slot(a.witem0, a.nt + 1, wi);
+                w_lo = __ldg(a.witem0 + slot);
+                w_hi = __ldg(a.witem0 + slot + 1);
+                t = __ldg(a.wtask + slot);
+                t_item0 = __ldg(a.item0 + t);
+                const TaskRef& ref = a.refs[t];
+                in = ref.in;
+                nrows = ref.nrows;
+                out = a.task_out[t];
+                __syncwarp();
+                load_desc(d, a.nodes + ref.node);
+                t_off0 = a.items[t_item0] + a.chunks[t_item0 >> kScanChunkLog2];
+            }
+            const uint64_t item = t_item0 + (wi - w_lo);
+            const uint64_t off = a.items[item] + a.chunks[item >> kScanChunkLog2];
+            const uint64_t off_next = item + 1 >= a.n_count_items
+                                          ? a.chunks[a.n_chunks]
+                                          : a.items[item + 1] + a.chunks[(item + 1) >> kScanChunkLog2];
+            if (off_next == off) continue;  // nothing accepted in this item
+            const uint64_t row0 = (wi - w_lo) * a.rows_per_item;
+            const uint32_t nr = (uint32_t)umin64(a.rows_per_item, nrows - row0);
+            const bool ext = d.kind == STEP_EXT;
+            const uint32_t k = ext ? d.e.k : d.r.k;
+            Tile tl;
+            tl.t = tile_s;
+            tl.w = ext ? k + 1 : k;
+            tl.n = 0;
+            tl.out = out + (off - t_off0) * tl.w;
+            tl.room = off_next - off;
+            __syncwarp();
+            stage_rows(rows_s, in, row0, nr, k);
+            if (ext)
+                ext_item<true>(d, rows_s, nr, a.hub, a.ctx, &tl, nullptr);
+            else
+                red_item<true>(d, rows_s, nr, a.ctx, &tl);
+            if (tl.n) tile_flush(tl, tl.n);
+        }
+    }
 }
 
 std::atomic<uint64_t> g_batch_launches{0};
@@ -396,13 +630,16 @@ Staging::~Staging() { pin_give(p, cap); }
 // the serving loop submits new waves between rounds.
 BatchSession::BatchSession(DevDB& db_, cudaStream_t s_, uint64_t budget_, uint32_t slots_, bool graph_counts_,
                            bool profile_)
-    : db(db_), s(s_), budget(budget_), nslots(slots_), want_graph_counts(graph_counts_), profile(profile_) {}
+    : db(db_), s(s_), budget(budget_), nslots(slots_), want_graph_counts(graph_counts_), profile(profile_) {
+    tune.rows_per_item = db.tune_rows_per_item;
+    tune.hub = db.tune_hub;
+}
 
 BatchSession::~BatchSession() {
     cudaSetDevice(db.device);
     active.clear();
     if (staged) cudaEventDestroy(staged);
-    for (void* p : {(void*)d_desc, (void*)d_sums, (void*)d_small, (void*)d_blk, acc, d_nodes})
+    for (void* p : {(void*)d_desc, (void*)d_items, (void*)d_small, (void*)d_chunks, (void*)d_read, acc, d_nodes})
         if (p) cudaFreeAsync(p, s);
     cudaStreamSynchronize(s);
 }
@@ -428,8 +665,9 @@ int BatchSession::init() {
     static std::atomic<bool> smem_set[64];  // sessions may start on several threads (server, miner)
     if (dev < 0 || dev >= 64) return fail(GVA_ERR_ARG, "device index out of range");
     if (!smem_set[dev].load(std::memory_order_acquire)) {
-        GVA_CUDA_B(cudaFuncSetAttribute(batch_write_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        (int)batch_smem_bytes()));
+        const int most = (int)round_smem_bytes(kMaxItemRows / 4, kMaxCols);  // rows per item shrink as rows widen
+        GVA_CUDA_B(cudaFuncSetAttribute(round_count_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, most));
+        GVA_CUDA_B(cudaFuncSetAttribute(round_write_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, most));
         smem_set[dev].store(true, std::memory_order_release);
     }
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
@@ -724,22 +962,28 @@ int BatchSession::round() {
     ctx.graph_counts = graph_counts_dev();
     ctx.graph_bits = graph_bits_dev();
     const int nt = (int)active.size();
-    // staging: refs[nt] | new node descriptors (<= nt) | block0[nt+1] | totals[nt] | outs[nt] + queue
+    // rows per work item: as many as fit 1024 words of rows (the widest task
+    // of the round sets the shared-memory layout), a multiple of 32
+    uint32_t kmax = 1;
+    for (int t = 0; t < nt; ++t) kmax = std::max(kmax, nodes[active[t].node].width_in);
+    uint32_t R = std::min<uint32_t>(tune.rows_per_item, std::max<uint32_t>(32, (1024 / kmax) & ~31u));
+    // staging: refs[nt] | new node descriptors (<= nt) | item0[nt+1] | totals[nt] | outs[nt] | wtask[nt] | witem0[nt+1]
     const size_t ref_bytes = (size_t)nt * sizeof(TaskRef);
     const size_t desc_max = (size_t)nt * sizeof(TaskDesc);
-    const size_t small_words = (size_t)(nt + 1) + nt + nt + 1;
+    const size_t small_words = (size_t)(nt + 1) + nt + nt + 2 + nt + (nt + 1);
     char* h = staging.get(ref_bytes + desc_max + small_words * 8);
     if (!h) return fail(GVA_ERR_NOMEM, "pinned staging allocation failed");
     TaskRef* refs = (TaskRef*)h;
     char* new_desc = h + ref_bytes;
-    uint64_t* h_block0 = (uint64_t*)(h + ref_bytes + desc_max);
-    uint64_t* h_totals = h_block0 + (nt + 1);
+    uint64_t* h_item0 = (uint64_t*)(h + ref_bytes + desc_max);
+    uint64_t* h_totals = h_item0 + (nt + 1);
     uint32_t** h_outs = (uint32_t**)(h_totals + nt);
+    uint64_t* h_wtask = h_totals + 2 * nt + 2;  // nt 8-byte words holding uint32 task indices
+    uint64_t* h_witem0 = h_wtask + nt;
     const int dev_first = dev_count;
-    uint32_t kmax = 1, eqmax = 0;
     double cbytes = 0, crows = 0;
-    uint64_t nb = 0;
-    h_block0[0] = 0;
+    uint64_t ni = 0;
+    h_item0[0] = 0;
     for (int t = 0; t < nt; ++t) {
         const BTask& tk = active[t];
         BNode& nd = nodes[tk.node];
@@ -747,21 +991,14 @@ int BatchSession::round() {
             nd.dev = dev_count++;
             fill_node_desc(tk.node, new_desc + (size_t)(nd.dev - dev_first) * sizeof(TaskDesc));
         }
-        const BNode& st = nd;
-        refs[t] = TaskRef{(uint32_t)nd.dev, 0u, nb, tk.in, tk.rows};
-        kmax = std::max(kmax, st.width_in);
-        if (st.kind == STEP_EXT) eqmax = std::max(eqmax, st.n_eq);
-        nb += (tk.rows + kRowsPerBlock - 1) / kRowsPerBlock;
-        h_block0[t + 1] = nb;
-        cbytes += (4.0 * st.width_in + 8.0 * (st.kind == STEP_EXT ? 1 : st.n_pairs)) * (double)tk.rows;
+        refs[t] = TaskRef{(uint32_t)nd.dev, 0u, tk.in, tk.rows};
+        ni += (tk.rows + R - 1) / R;
+        h_item0[t + 1] = ni;
+        cbytes += (4.0 * nd.width_in + 8.0 * (nd.kind == STEP_EXT ? 1 : nd.n_pairs)) * (double)tk.rows;
         crows += (double)tk.rows;
     }
-    if (nb > 0x7fffffffull) return fail(GVA_ERR_UNSUPPORTED, "round too large for one launch");
-    // block -> task, so that no block searches block0
-    uint32_t* h_blk = (uint32_t*)staging_blk.get(nb * 4);
-    if (!h_blk) return fail(GVA_ERR_NOMEM, "pinned staging allocation failed");
-    for (int t = 0; t < nt; ++t)
-        for (uint64_t b = h_block0[t]; b < h_block0[t + 1]; ++b) h_blk[b] = (uint32_t)t;
+    if (ni == 0) return fail(GVA_ERR_ARG, "round without frontier rows");  // tasks always hold rows
+    const uint64_t nc = (ni + kScanChunk - 1) / kScanChunk;
     auto grow = [&](void** p, size_t& cap, size_t need) -> bool {
         if (need <= cap) return true;
         if (*p) cudaFreeAsync(*p, s);
@@ -785,35 +1022,62 @@ int BatchSession::round() {
         d_nodes = p;
         node_cap = cap;
     }
-    if (!grow(&d_desc, desc_cap, ref_bytes) || !grow((void**)&d_sums, sums_cap, (nb + 1) * 8) ||
-        !grow((void**)&d_small, small_cap, small_words * 8) || !grow((void**)&d_blk, blk_cap, nb * 4))
+    size_t read_cap = d_read ? 8 : 0;
+    if (!grow(&d_desc, desc_cap, ref_bytes) || !grow((void**)&d_items, items_cap, std::max<uint64_t>(ni, 1) * 8) ||
+        !grow((void**)&d_small, small_cap, small_words * 8) ||
+        !grow((void**)&d_chunks, chunks_cap, (nc + 1) * 8) || (pf && !grow((void**)&d_read, read_cap, 8)))
         return fail(GVA_ERR_NOMEM, "batch bookkeeping allocation failed");
-    uint64_t* d_block0 = d_small;
-    uint64_t* d_totals = d_block0 + (nt + 1);
+    uint64_t* d_item0 = d_small;
+    uint64_t* d_totals = d_item0 + (nt + 1);
     uint32_t** d_outs = (uint32_t**)(d_totals + nt);
-    unsigned long long* d_queue = (unsigned long long*)(d_totals + 2 * nt);
+    unsigned long long* d_queue = (unsigned long long*)(d_totals + 2 * nt);  // two heads: count, write
+    uint64_t* d_wtask = d_totals + 2 * nt + 2;
+    uint64_t* d_witem0 = d_wtask + nt;
     if (dev_count > dev_first)
         GVA_CUDA_B(cudaMemcpyAsync((char*)d_nodes + (size_t)dev_first * sizeof(TaskDesc), new_desc,
                                    (size_t)(dev_count - dev_first) * sizeof(TaskDesc), cudaMemcpyHostToDevice, s));
     GVA_CUDA_B(cudaMemcpyAsync(d_desc, refs, ref_bytes, cudaMemcpyHostToDevice, s));
-    GVA_CUDA_B(cudaMemcpyAsync(d_block0, h_block0, (nt + 1) * 8, cudaMemcpyHostToDevice, s));
-    GVA_CUDA_B(cudaMemcpyAsync(d_blk, h_blk, nb * 4, cudaMemcpyHostToDevice, s));
-
-    GVA_CUDA_B(cudaMemsetAsync(d_sums, 0, (nb + 1) * 8, s));
+    GVA_CUDA_B(cudaMemcpyAsync(d_item0, h_item0, (nt + 1) * 8, cudaMemcpyHostToDevice, s));
+    GVA_CUDA_B(cudaMemsetAsync(d_queue, 0, 16, s));
+    if (pf) GVA_CUDA_B(cudaMemsetAsync(d_read, 0, 8, s));
     lap(0);
+    const size_t smem = round_smem_bytes(R, kmax);
+    RoundArgs ra{};
+    ra.nodes = (const TaskDesc*)d_nodes;
+    ra.refs = (const TaskRef*)d_desc;
+    ra.item0 = d_item0;
+    ra.n_items = ni;
+    ra.nt = (uint32_t)nt;
+    ra.rows_per_item = R;
+    ra.hub = tune.hub;
+    ra.kmax = kmax;
+    ra.items = d_items;
+    ra.queue = d_queue;
+    ra.read_words = pf ? d_read : nullptr;
+    ra.ctx = ctx;
+    auto grid_for = [&](const void* fn) -> uint32_t {
+        int per_sm = 1;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kRoundWarps * 32, smem);
+        return (uint32_t)std::max(per_sm, 1) * (uint32_t)sms;
+    };
+    const uint32_t cgrid = (uint32_t)std::min<uint64_t>(grid_for((const void*)round_count_kernel),
+                                                        (ni + kRoundWarps - 1) / kRoundWarps);
+    ra.total_warps = cgrid * kRoundWarps;
     cudaEvent_t ev = nullptr;
     if (pf) pf->begin(K_EXT_COUNT, cbytes, s, ev);
-    batch_count_kernel<<<(unsigned)nb, kThreads, 0, s>>>((const TaskDesc*)d_nodes, (const TaskRef*)d_desc, d_blk,
-                                                         d_sums, ctx);
+    round_count_kernel<<<cgrid, kRoundWarps * 32, smem, s>>>(ra);
     if (pf) pf->end(ev, K_EXT_COUNT, cbytes, s, crows);
-    if (pf) pf->begin(K_SCAN, 16.0 * nb, s, ev);
-    scan_block_sums_kernel<<<1, kScanThreads, 0, s>>>(d_sums, nb);
-    if (pf) pf->end(ev, K_SCAN, 16.0 * nb, s, (double)nb);
-    task_totals_kernel<<<(nt + 255) / 256, 256, 0, s>>>(d_block0, nt, d_sums, d_totals);
+    if (pf) pf->begin(K_SCAN, 16.0 * ni, s, ev);
+    scan_items_local_kernel<<<(unsigned)nc, 1024, 0, s>>>(d_items, ni, d_chunks);
+    scan_items_top_kernel<<<1, 1024, 0, s>>>(d_chunks, nc, d_items, ni, d_item0, (uint32_t)nt, d_totals);
+    if (pf) pf->end(ev, K_SCAN, 16.0 * ni, s, (double)ni);
     launches += 3;
     g_batch_launches += 3;
     GVA_CUDA_B(cudaGetLastError());
     GVA_CUDA_B(cudaMemcpyAsync(h_totals, d_totals, nt * 8, cudaMemcpyDeviceToHost, s));
+    uint64_t h_read_count = 0;
+    uint64_t* h_read = pf ? (uint64_t*)staging_read.get(8) : nullptr;
+    if (pf && h_read) GVA_CUDA_B(cudaMemcpyAsync(h_read, d_read, 8, cudaMemcpyDeviceToHost, s));
     lap(1);
     {
         const auto w0 = std::chrono::steady_clock::now();
@@ -821,6 +1085,11 @@ int BatchSession::round() {
         wait_ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - w0).count();
         if (e != cudaSuccess) return fail(GVA_ERR_CUDA, cudaGetErrorString(e));
         t_lap = std::chrono::steady_clock::now();
+    }
+    if (pf && h_read) {
+        h_read_count = *h_read;
+        for (auto& pe : pf->pending)
+            if (pe.kind == K_EXT_COUNT) pe.bytes += 4.0 * (double)h_read_count;
     }
 
     // which tasks write this round: all when the outputs fit the budget,
@@ -886,9 +1155,16 @@ int BatchSession::round() {
         cudaStream_t ss = s;
         buf = std::shared_ptr<void>(p, [ss](void* q) { cudaFreeAsync(q, ss); });
         double wbytes = 0, wrows = 0;
+        uint32_t nw = 0;
+        uint64_t wi = 0;
+        uint32_t* h_wt = (uint32_t*)h_wtask;  // task index per writing slot (uint32)
+        h_witem0[0] = 0;
         for (int t = 0; t < nt; ++t) {
             h_outs[t] = chosen_flag[t] == 1 ? (uint32_t*)p + off_words[t] : nullptr;
             if (chosen_flag[t] != 1) continue;
+            h_wt[nw] = (uint32_t)t;
+            wi += h_item0[t + 1] - h_item0[t];
+            h_witem0[++nw] = wi;
             wrows += (double)active[t].rows;
             const BNode& st = nodes[active[t].node];
             const double k = st.width_in;
@@ -896,15 +1172,24 @@ int BatchSession::round() {
                       (st.kind == STEP_EXT ? (4.0 + 4.0 * (k + 1)) : 4.0 * k) * (double)h_totals[t];
         }
         GVA_CUDA_B(cudaMemcpyAsync(d_outs, h_outs, nt * sizeof(uint32_t*), cudaMemcpyHostToDevice, s));
+        GVA_CUDA_B(cudaMemcpyAsync(d_wtask, h_wtask, (size_t)(2 * nt + 1) * 8, cudaMemcpyHostToDevice, s));
         GVA_CUDA_B(cudaEventRecord(staged, s));  // the last read of the staging area this round
-        GVA_CUDA_B(cudaMemsetAsync(d_queue, 0, 8, s));
-        const size_t smem = batch_smem_bytes_for(kmax, std::max(eqmax, 1u));
-        int per_sm = 1;
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_write_kernel, kThreads, smem);
-        const uint64_t grid = std::min<uint64_t>(nb, (uint64_t)std::max(per_sm, 1) * sms);
+        RoundArgs wa = ra;
+        wa.n_items = wi;
+        wa.wtask = (const uint32_t*)d_wtask;
+        wa.witem0 = d_witem0;
+        wa.nt = nw;
+        wa.chunks = d_chunks;
+        wa.n_count_items = ni;
+        wa.n_chunks = nc;
+        wa.queue = d_queue + 1;
+        wa.task_out = d_outs;
+        wa.read_words = nullptr;
+        const uint32_t wgrid = (uint32_t)std::min<uint64_t>(grid_for((const void*)round_write_kernel),
+                                                            (wi + kRoundWarps - 1) / kRoundWarps);
+        wa.total_warps = wgrid * kRoundWarps;
         if (pf) pf->begin(K_EXT_WRITE, wbytes, s, ev);
-        batch_write_kernel<<<(unsigned)grid, kThreads, smem, s>>>((const TaskDesc*)d_nodes, (const TaskRef*)d_desc,
-                                                                  d_block0, d_blk, nb, d_sums, d_outs, d_queue);
+        round_write_kernel<<<wgrid, kRoundWarps * 32, smem, s>>>(wa);
         if (pf) pf->end(ev, K_EXT_WRITE, wbytes, s, wrows);
         launches += 1;
         g_batch_launches += 1;
@@ -1122,6 +1407,59 @@ int run_batch(DevDB& db, const std::vector<std::vector<Step>>& steps, cudaStream
                            profile, pb);
     if (rc) return rc;
     return finish_batch(db, pb, counts, graph_counts_host, support_host, stats);
+}
+
+// Candidate launch shapes: rows per work item x the list length from which a
+// row's candidates are shared by its warp (1 << 30: never).  Each shape runs
+// the calibration batch twice; the faster run counts.
+int autotune_batch(DevDB& db, const std::vector<std::vector<Step>>& steps, cudaStream_t s, bool per_graph,
+                   TuneResult& out) {
+    out = TuneResult();
+    if (steps.empty()) return fail(GVA_ERR_ARG, "empty calibration batch");
+    const uint32_t keep_r = db.tune_rows_per_item, keep_h = db.tune_hub;
+    const uint32_t rows[] = {32, 64, 128};
+    const uint32_t hubs[] = {16, 32, 64, 1u << 30};
+    std::vector<uint64_t> counts(steps.size()), first_counts;
+    std::vector<uint32_t> sup(per_graph ? steps.size() : 0);
+    double best = 1e300;
+    int rc = GVA_OK;
+    for (uint32_t r : rows) {
+        for (uint32_t hb : hubs) {
+            db.tune_rows_per_item = r;
+            db.tune_hub = hb;
+            double t = 1e300;
+            for (int rep = 0; rep < 2 && !rc; ++rep) {
+                BatchStats bs;
+                rc = run_batch(db, steps, s, 0, nullptr, 0, counts.data(), nullptr, per_graph ? sup.data() : nullptr,
+                               false, &bs);
+                t = std::min(t, bs.gpu_ms);
+            }
+            if (rc) break;
+            if (first_counts.empty()) {
+                first_counts = counts;
+            } else if (counts != first_counts) {  // every shape counts the same rows
+                rc = fail(GVA_ERR_CUDA, "launch shapes disagree on the calibration counts");
+                break;
+            }
+            out.tried.push_back({(double)r, (double)hb, t});
+            if (r == 64 && hb == 32) out.default_ms = t;
+            if (t < best) {
+                best = t;
+                out.rows_per_item = r;
+                out.hub = hb;
+            }
+        }
+        if (rc) break;
+    }
+    if (rc) {
+        db.tune_rows_per_item = keep_r;
+        db.tune_hub = keep_h;
+        return rc;
+    }
+    out.ms = best;
+    db.tune_rows_per_item = out.rows_per_item;
+    db.tune_hub = out.hub;
+    return GVA_OK;
 }
 
 int set_graph_ids(DevDB& db, const uint64_t* first, uint32_t num_graphs) {

@@ -4,6 +4,7 @@
 
 #include <algorithm>
 #include <cstdio>
+#include <chrono>
 #include <cstring>
 #include <fstream>
 #include <sstream>
@@ -381,10 +382,12 @@ int gva_batch_count(gva_db* db, const gva_plan* const* plans, int nplans, const 
     std::vector<std::vector<Step>> steps(nplans);
     for (int i = 0; i < nplans; ++i)
         if (!plans[i]) return fail(GVA_ERR_ARG, "null plan");
+    const auto t_lower = std::chrono::steady_clock::now();
     {
         int st = parallel_for(nplans, [&](int i) { return lower_plan(plans[i]->plan, db->dev->meta, steps[i], true); });
         if (st) return st;
     }
+    const double lower_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_lower).count();
     BatchStats bs;
     int st = run_batch(*db->dev, steps, (cudaStream_t)o.stream, o.budget_bytes, db->dev->vgraph, db->dev->num_graphs,
                        counts, graph_counts, graph_support, o.profile != 0, &bs);
@@ -395,6 +398,11 @@ int gva_batch_count(gva_db* db, const gva_plan* const* plans, int nplans, const 
         stats->splits = bs.splits;
         stats->launches = bs.launches;
         stats->trie_nodes = bs.nodes;
+        stats->lower_ms = lower_ms;
+        stats->submit_ms = bs.submit_ms;
+        stats->round_host_ms = bs.round_host_ms;
+        stats->wait_ms = bs.wait_ms;
+        stats->session_ms = bs.session_ms;
         for (int i = 0; i < K_NUM && i < 5; ++i) {
             strncpy(stats->kernels[i].name, kKernelNames[i], sizeof stats->kernels[i].name - 1);
             stats->kernels[i].launches = bs.kstat[i].launches;
@@ -404,6 +412,44 @@ int gva_batch_count(gva_db* db, const gva_plan* const* plans, int nplans, const 
         }
     }
     return st;
+}
+
+int gva_db_get_tuning(const gva_db* db, gva_tuning* out) {
+    if (!db || !out) return fail(GVA_ERR_ARG, "null argument");
+    memset(out, 0, sizeof *out);
+    out->rows_per_item = db->dev->tune_rows_per_item;
+    out->hub = db->dev->tune_hub;
+    return GVA_OK;
+}
+
+int gva_db_set_tuning(gva_db* db, const gva_tuning* t) {
+    if (!db || !t) return fail(GVA_ERR_ARG, "null argument");
+    if (t->rows_per_item != 32 && t->rows_per_item != 64 && t->rows_per_item != 128)
+        return fail(GVA_ERR_ARG, "rows_per_item must be 32, 64 or 128");  // hub: any value (0: every row shared)
+    db->dev->tune_rows_per_item = t->rows_per_item;
+    db->dev->tune_hub = t->hub;
+    return GVA_OK;
+}
+
+int gva_db_autotune(gva_db* db, const gva_plan* const* plans, int nplans, void* stream, gva_tuning* out) {
+    if (!db || nplans <= 0 || !plans) return fail(GVA_ERR_ARG, "null argument");
+    std::vector<std::vector<Step>> steps(nplans);
+    for (int i = 0; i < nplans; ++i)
+        if (!plans[i]) return fail(GVA_ERR_ARG, "null plan");
+    int st = parallel_for(nplans, [&](int i) { return lower_plan(plans[i]->plan, db->dev->meta, steps[i], true); });
+    if (st) return st;
+    TuneResult tr;
+    st = autotune_batch(*db->dev, steps, (cudaStream_t)stream, db->dev->vgraph != nullptr, tr);
+    if (st) return st;
+    if (out) {
+        memset(out, 0, sizeof *out);
+        out->rows_per_item = tr.rows_per_item;
+        out->hub = tr.hub;
+        out->ms = tr.ms;
+        out->default_ms = tr.default_ms;
+        out->tried = (uint32_t)tr.tried.size();
+    }
+    return GVA_OK;
 }
 
 int gva_mine(gva_db* db, const gva_mine_opts* opts, gva_mine_result** out) {

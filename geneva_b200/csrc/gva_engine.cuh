@@ -3,6 +3,7 @@
 
 #include <cuda_runtime.h>
 
+#include <array>
 #include <cstdint>
 #include <memory>
 #include <string>
@@ -35,6 +36,8 @@ struct DevDB {
     HostGraph meta;                       // labels/partition presence for lowering (no adjacency)
     uint32_t* vgraph = nullptr;           // optional vertex -> graph id map (graph databases)
     uint32_t num_graphs = 0;
+    // launch shape of the batched engine's round kernels (autotune_batch)
+    uint32_t tune_rows_per_item = 64, tune_hub = 32;
 };
 
 int upload_graph(HostGraph& g, int device, DevDB*& out);
@@ -168,6 +171,14 @@ public:
     uint64_t* graph_counts_dev() const;
     uint32_t* graph_bits_dev() const;
 
+    // Launch shape of the round kernels: rows per work item (a multiple of
+    // 32, at most 128; fewer when rows are wide) and the candidate-list length
+    // above which a row's candidates are shared by its whole warp.
+    struct Tuning {
+        uint32_t rows_per_item = 64;
+        uint32_t hub = 32;
+    } tune;
+
     uint64_t rounds = 0, splits = 0, launches = 0;
     double submit_ms = 0, round_host_ms = 0, wait_ms = 0;  // host time split
     // round_host_ms by part: task scan + uploads, count launches, totals and
@@ -207,13 +218,13 @@ private:
     std::vector<uint64_t> scratch_off;
     void* d_desc = nullptr;  // per-round task references
     size_t desc_cap = 0;
-    uint64_t* d_sums = nullptr;
-    size_t sums_cap = 0;
+    uint64_t* d_items = nullptr;  // per-round item counts, scanned in place
+    size_t items_cap = 0;
+    uint64_t* d_chunks = nullptr;  // per-round scan chunk sums
+    size_t chunks_cap = 0;
     uint64_t* d_small = nullptr;
     size_t small_cap = 0;
-    uint32_t* d_blk = nullptr;  // per-round block -> task
-    size_t blk_cap = 0;
-    Staging staging_blk;
+    unsigned long long* d_read = nullptr;  // profiling: candidate-list words read
     Staging staging_read;  // pinned landing area of per-plan support read-backs
 };
 // run_batch in two halves, so that a caller can build the next batch's
@@ -231,6 +242,16 @@ int prepare_batch(DevDB& db, const std::vector<std::vector<Step>>& steps, cudaSt
 int finish_batch(DevDB& db, PreparedBatch& pb, uint64_t* counts, uint64_t* graph_counts_host, uint32_t* support_host,
                  BatchStats* stats, const volatile int* cancel = nullptr);
 int set_graph_ids(DevDB& db, const uint64_t* first, uint32_t num_graphs);
+
+// Times the batched count of `steps` (a calibration batch) under each
+// candidate launch shape of the round kernels and stores the fastest in db.
+struct TuneResult {
+    uint32_t rows_per_item = 64, hub = 32;
+    double ms = 0.0, default_ms = 0.0;
+    std::vector<std::array<double, 3>> tried;  // rows per item, hub, ms
+};
+int autotune_batch(DevDB& db, const std::vector<std::vector<Step>>& steps, cudaStream_t s, bool per_graph,
+                   TuneResult& out);
 
 struct MineStats {
     uint64_t candidates = 0, frequent = 0, embeddings = 0, levels = 0, pruned = 0;

@@ -177,6 +177,10 @@ typedef struct gva_batch_stats {
     uint64_t rounds, splits, launches;
     uint64_t trie_nodes; /* distinct step prefixes: plans sharing a prefix share its frontier */
     gva_kernel_stat kernels[5];
+    /* host time (ms): lowering plans to steps, building the step trie,
+     * rounds' host work (task lists, launches, budget choice), waiting for
+     * the device, session set-up / read-back / tear-down */
+    double lower_ms, submit_ms, round_host_ms, wait_ms, session_ms;
 } gva_batch_stats;
 
 /* Declares the database a union of graphs: graph g owns vertex ids
@@ -189,6 +193,28 @@ int gva_db_set_graphs(gva_db* db, const uint64_t* first, uint32_t num_graphs);
  * (optional): graphs holding at least one embedding. */
 int gva_batch_count(gva_db* db, const gva_plan* const* plans, int nplans, const gva_batch_opts* opts,
                     uint64_t* counts, uint64_t* graph_counts, uint32_t* graph_support, gva_batch_stats* stats);
+
+/* Launch shape of the batched engine's round kernels on one database: rows
+ * per work item (32, 64 or 128; fewer when rows are wide) and the candidate
+ * list length above which a frontier row's candidates are shared by a whole
+ * warp instead of walked by one lane.  Defaults 64 / 32.  The reference's
+ * launch shape is fixed (a persistent grid of GPU_SM_NUM blocks,
+ * src/miningPattern.cu:3350-3377); here it is chosen per database. */
+typedef struct gva_tuning {
+    uint32_t rows_per_item;
+    uint32_t hub;
+    double ms;          /* gva_db_autotune: calibration time of the chosen shape */
+    double default_ms;  /* gva_db_autotune: calibration time of the default shape */
+    uint32_t tried;     /* gva_db_autotune: shapes timed */
+    uint32_t reserved;
+} gva_tuning;
+int gva_db_get_tuning(const gva_db* db, gva_tuning* out);
+int gva_db_set_tuning(gva_db* db, const gva_tuning* tuning);
+/* Counts a calibration batch (as gva_batch_count does, with supports when
+ * the database has graph ids) under each candidate launch shape, twice each,
+ * and keeps the fastest for every later batched run, mining run and session
+ * on this database.  Every shape must give the same counts. */
+int gva_db_autotune(gva_db* db, const gva_plan* const* plans, int nplans, void* stream, gva_tuning* out);
 
 /* ---- serving: a persistent batch -------------------------------------------
  * The batched engine kept open: plans may be submitted at any time and join

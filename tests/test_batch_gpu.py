@@ -93,3 +93,38 @@ def test_enron_batch(native, enron_dir):
     with pytest.raises(gv.GenevaError):
         gv.batch_count(db, plans, support=True)  # no graph ids declared
     db.close()
+
+
+@pytest.mark.parametrize("rows_per_item,hub", [(32, 0), (64, 0), (128, 1), (64, 1 << 30), (32, 5), (128, 32)])
+def test_launch_shapes_give_the_oracle_counts(small_db, oracle, rows_per_item, hub):
+    """Every launch shape of the round kernels counts (and writes the
+    intermediate frontiers of) the same rows: hub 0 sends every row's
+    candidates through the warp-shared path, 1 << 30 none."""
+    db, gdb, og = small_db
+    pats = [p for p in _patterns(db, 60, 21) if oracle.count(og, p, cap_rows=1_000_000) is not None]
+    plans = [gv.Plan.from_text(p) for p in pats]
+    keep = gdb.tuning
+    try:
+        gdb.set_tuning(rows_per_item, hub)
+        assert gdb.tuning == {"rows_per_item": rows_per_item, "hub": hub}
+        counts, (gc, sup), _ = gv.batch_count(gdb, plans, graph_counts=True, support=True)
+    finally:
+        gdb.set_tuning(keep["rows_per_item"], keep["hub"])
+    want_counts, want_sup, want_gc = oracle.many_graph_counts(og, pats, db.first)
+    assert np.array_equal(counts, want_counts)
+    assert np.array_equal(sup, want_sup)
+    for i in range(len(pats)):
+        assert np.array_equal(gc[i], want_gc[i]), pats[i]
+
+
+def test_autotune_keeps_a_valid_shape(small_db, oracle):
+    db, gdb, og = small_db
+    pats = workloads.sample_patterns(db, 200, 3, 6, seed=31)
+    plans = gv.Plan.batch_from_texts(pats)
+    t = gdb.autotune(plans)
+    assert t["rows_per_item"] in (32, 64, 128) and t["shapes_tried"] == 12
+    assert 0 < t["ms"] <= t["default_ms"]
+    assert gdb.tuning == {"rows_per_item": t["rows_per_item"], "hub": t["hub"]}
+    counts, _, _ = gv.batch_count(gdb, plans)
+    want, _, _ = oracle.many_graph_counts(og, pats, db.first)
+    assert np.array_equal(counts, want)
