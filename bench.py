@@ -90,6 +90,8 @@ def parse_args():
     ap.add_argument("--patterns", type=int, default=16384, help="batch workload: patterns per rank per step")
     ap.add_argument("--tune-patterns", type=int, default=2048,
                     help="batch workload: patterns of the autotuner's calibration batch (0: default launch shape)")
+    ap.add_argument("--serve-rates", default="100,1000",
+                    help="batch workload: arrival rates of the serving sweep reported beside it (empty: none)")
     ap.add_argument("--mining-steps", type=int, default=3,
                     help="batch workload: timed steps of the mining run reported beside it (0: none)")
     ap.add_argument("--rates", default="10,100,500,2000", help="serve workload: arrival rates (req/s)")
@@ -296,15 +298,21 @@ def reference_arm(args, db, queries, workload, config=None):
 
 
 # -------------------------------------------------------------- serving arm ----
-def serve_bench(args, local, torch, gv, workloads):
+def serve_bench(args, local, torch, gv, workloads, db=None, rates=None, duration=None, drain=None):
     """Poisson arrivals at each rate: 80% matching requests (3-10 vertex
     patterns sampled from the resident config-2 database), 20% mining
     requests (max edges 3-5, minimum MNI support 1-5% of the vertices) against
     the resident config-4 graph; continuous batching with a 150 GB admission
-    budget; matching on a high-priority stream, mining on its own stream."""
+    budget; matching on a high-priority stream, mining on its own stream; at
+    most 2 mining requests wait behind the running one, later ones are
+    rejected at arrival."""
     import random
     from geneva_b200.serve import Server, percentile
-    db = workloads.config2(seed=args.seed)
+    rates = rates if rates is not None else args.rates
+    duration = duration if duration is not None else args.duration
+    drain = drain if drain is not None else args.drain
+    if db is None:
+        db = workloads.config2(seed=args.seed)
     gdb = gv.Database.from_edges(db.vlabels, db.src, db.dst, db.elabels, device=local)
     gdb.set_graphs(db.first)
     g4 = workloads.config4()
@@ -322,11 +330,11 @@ def serve_bench(args, local, torch, gv, workloads):
         r.future.result(timeout=600)
     srv.close()
     points = []
-    for rate in [float(x) for x in args.rates.split(",")]:
+    for rate in [float(x) for x in rates.split(",")]:
         srv = mk()
         rng = random.Random(int(rate))
         reqs = []
-        t_end = time.perf_counter() + args.duration
+        t_end = time.perf_counter() + duration
         nxt = time.perf_counter()
         while nxt < t_end:
             gap = nxt - time.perf_counter()
@@ -339,7 +347,7 @@ def serve_bench(args, local, torch, gv, workloads):
             else:
                 reqs.append(srv.submit_mine(rng.randint(3, 5), int(V4 * rng.uniform(0.01, 0.05))))
             nxt += rng.expovariate(rate)
-        deadline = time.perf_counter() + args.drain
+        deadline = time.perf_counter() + drain
         for r in reqs:
             try:
                 r.future.result(timeout=max(0.0, deadline - time.perf_counter()))
@@ -356,6 +364,7 @@ def serve_bench(args, local, torch, gv, workloads):
         points.append({"rate": rate, "requests": len(reqs), "completed": len(done),
                        "match_requests": sum(r.kind == "match" for r in reqs), "match_completed": len(lm),
                        "mine_requests": sum(r.kind == "mine" for r in reqs), "mine_completed": len(ln),
+                       "mine_rejected": srv.mine_rejected,
                        "match_p50_ms": 1e3 * percentile(lm, 50) if lm else None,
                        "match_p99_ms": 1e3 * percentile(lm, 99) if lm else None,
                        "match_admission_wait_p50_ms": 1e3 * percentile(wait_m, 50) if wait_m else None,
@@ -372,7 +381,9 @@ def serve_bench(args, local, torch, gv, workloads):
             "workload": "config-5 serving sweep: Poisson arrivals, 80% matching queries (3-10 vertices) against the "
                         "config-2 database, 20% MNI mining requests (max edges 3-5, min support 1-5% of |V|) against "
                         "the config-4 graph; 150 GB admission budget",
-            "duration_s_per_rate": args.duration, "drain_s": args.drain, "points": points}
+            "duration_s_per_rate": duration, "drain_s": drain,
+            "mine_admission": "at most 2 mining requests wait behind the running one; later ones rejected at arrival",
+            "points": points}
 
 
 # ------------------------------------------------------------ MNI mining arm ----
@@ -918,7 +929,8 @@ def batch_bench(args, rank, world, local, dist, torch, gv, workloads):
                      "launches": s["launches"], "kernel_ms": s["ms"]},
         "kernels": kstats,
         "batch": {k: pstats[k] for k in ("rounds", "splits", "launches", "trie_nodes", "gpu_ms", "lower_ms",
-                                         "submit_ms", "round_host_ms", "wait_ms", "session_ms")},
+                                         "submit_ms", "round_host_ms", "round_phase_ms", "wait_ms",
+                                         "session_ms")},
         "tuning": dict(tuning, calibration=f"first {min(args.tune_patterns, len(plans))} patterns of the list, "
                                            f"counted with supports, each launch shape twice (gva_db_autotune)"),
         "e2e": {"value": e2e_value, "unit": "embeddings/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
@@ -935,6 +947,9 @@ def batch_bench(args, rank, world, local, dist, torch, gv, workloads):
         out["cpu_baseline"] = base
         if args.mining_steps > 0:
             out["mining"] = mining_extra(args, local, torch, gv, db)
+        if args.serve_rates:
+            out["serving"] = serve_bench(args, local, torch, gv, workloads, db=db, rates=args.serve_rates,
+                                         duration=1.0, drain=20.0)
     return out
 
 

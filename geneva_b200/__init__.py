@@ -108,7 +108,8 @@ class _BatchStats(ctypes.Structure):
     _fields_ = [("gpu_ms", ctypes.c_double), ("rounds", ctypes.c_uint64), ("splits", ctypes.c_uint64),
                 ("launches", ctypes.c_uint64), ("trie_nodes", ctypes.c_uint64), ("kernels", _KernelStat * 5),
                 ("lower_ms", ctypes.c_double), ("submit_ms", ctypes.c_double), ("round_host_ms", ctypes.c_double),
-                ("wait_ms", ctypes.c_double), ("session_ms", ctypes.c_double)]
+                ("wait_ms", ctypes.c_double), ("session_ms", ctypes.c_double),
+                ("round_phase_ms", ctypes.c_double * 5)]
 
 
 class _MniStats(ctypes.Structure):
@@ -442,6 +443,7 @@ def batch_count(db: Database, plans: Sequence[Plan], stream: Optional[int] = Non
     stats = {"gpu_ms": st.gpu_ms, "rounds": int(st.rounds), "splits": int(st.splits), "launches": int(st.launches),
              "trie_nodes": int(st.trie_nodes), "lower_ms": st.lower_ms, "submit_ms": st.submit_ms,
              "round_host_ms": st.round_host_ms, "wait_ms": st.wait_ms, "session_ms": st.session_ms,
+             "round_phase_ms": [float(x) for x in st.round_phase_ms],
              "kernels": {st.kernels[i].name.decode(): dict(launches=int(st.kernels[i].launches),
                                                            ms=float(st.kernels[i].ms), bytes=float(st.kernels[i].bytes),
                                                            rows=float(st.kernels[i].rows))

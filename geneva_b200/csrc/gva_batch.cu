@@ -29,6 +29,7 @@
 #include <unordered_map>
 #include <numeric>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/geneva.h"
@@ -92,7 +93,8 @@ struct RoundArgs {
     const TaskDesc* nodes;
     const TaskRef* refs;
     const uint64_t* item0;        // [nt + 1] count-pass item prefix
-    uint64_t n_items;             // items of this launch (count: all tasks; write: the writing tasks)
+    uint64_t item_base;           // first item of this launch (its task class's range)
+    uint64_t n_items;             // items of this launch
     const uint32_t* wtask;        // write: task of each writing task slot (null for the count pass)
     const uint64_t* witem0;       // write: [nw + 1] item prefix over the writing tasks
     uint32_t nt;                  // tasks (count) or writing tasks (write)
@@ -192,25 +194,6 @@ __device__ __forceinline__ void stage_rows(uint32_t* rows_s, const uint32_t* __r
     __syncwarp();
 }
 
-// Broadcast of lane h's generator state (hub rows are processed by the whole warp).
-__device__ __forceinline__ GenState shfl_gen(const GenState& g, int h, uint32_t n_chk) {
-    GenState o;
-    o.lo = __shfl_sync(0xffffffffu, g.lo, h);
-    o.hi = __shfl_sync(0xffffffffu, g.hi, h);
-    o.which = __shfl_sync(0xffffffffu, g.which, h);
-    o.slo = __shfl_sync(0xffffffffu, g.slo, h);
-    o.shi = __shfl_sync(0xffffffffu, g.shi, h);
-    o.gadj = reinterpret_cast<const uint32_t*>(
-        __shfl_sync(0xffffffffu, (unsigned long long)reinterpret_cast<uintptr_t>(g.gadj), h));
-#pragma unroll
-    for (int i = 0; i < kMaxChecks; ++i) {
-        o.clo[i] = __shfl_sync(0xffffffffu, g.clo[i], h);
-        o.chi[i] = __shfl_sync(0xffffffffu, g.chi[i], h);
-    }
-    (void)n_chk;
-    return o;
-}
-
 // Candidate test of the plain extension (no fused checks): injectivity only;
 // the restriction bound is already applied to the range.
 __device__ __forceinline__ bool ext_injective(const ExtArgs& p, const uint32_t* row, uint32_t c) {
@@ -265,16 +248,22 @@ __device__ __forceinline__ void tile_append(Tile& tl, bool take, const uint32_t*
 }
 
 // ------------------------------------------------------------ one item ----
-// Extension step over the item's rows (staged in rows_s).  Each lane owns
-// rows lane, lane + 32, ...; a row's candidates come from its generator
-// segment (ext_generator); rows whose list is at most `hub` long are walked by
-// their lane, longer ones by the whole warp, 32 candidates per step.  COUNT
+// Tasks come in two classes with their own kernels (so that each gets the
+// registers, and the occupancy, its work needs):
+//   light  plain extensions (no fused checks) and reductions: a lane per row;
+//   fused  extensions with fused back-edge checks: a row's candidates come
+//          from its generator segment (ext_generator) and every candidate is
+//          tested against the other segments; each lane's generator state
+//          lives in shared memory, where the whole warp can read it.
+// In both, a row whose candidate list is at most `hub` long is walked by its
+// lane; longer lists are shared by the warp, 32 candidates per step.  COUNT
 // returns the item's accepted candidates (valid in every lane) and does the
 // per-graph accounting; WRITE appends every accepted (row, candidate) to the
-// tile.  Both visit the same candidates with the same test.
-template <bool WRITE>
+// tile.  Both passes visit the same candidates with the same test.
+template <bool WRITE, bool FUSED>
 __device__ __forceinline__ uint64_t ext_item(const TaskDesc& d, const uint32_t* rows_s, uint32_t nr, uint32_t hub,
-                                             const BatchCtx& ctx, Tile* tl, unsigned long long* read_words) {
+                                             const BatchCtx& ctx, Tile* tl, GenState* gen_s,
+                                             unsigned long long* read_words) {
     const ExtArgs& p = d.e;
     const int lane = threadIdx.x & 31;
     const uint32_t k = p.k;
@@ -286,60 +275,64 @@ __device__ __forceinline__ uint64_t ext_item(const TaskDesc& d, const uint32_t* 
         const bool valid = r < nr;
         const uint32_t* row = rows_s + (valid ? r : 0) * k;
         uint32_t cnt = 0;
-        if (!WRITE && p.n_chk == 0) {
+        if (!FUSED && !WRITE) {
             // plain extension: the segment minus the matched vertices in it
             if (valid) cnt = ext_count_row(p, row);
         } else {
-            GenState g;
-            g.lo = g.hi = 0;
-            if (valid) {
-                if (p.n_chk) {
+            uint32_t lo = 0, hi = 0;
+            if (FUSED) {
+                GenState& g = gen_s[lane];
+                if (valid) {
                     ext_generator(p, row, g);
-                } else {
-                    ext_range(p, row, g.lo, g.hi);
-                    g.gadj = p.adj;
-                    g.which = -1;
+                    lo = g.lo;
+                    hi = g.hi;
                 }
+            } else if (valid) {
+                ext_range(p, row, lo, hi);
             }
-            const uint32_t len = g.hi > g.lo ? g.hi - g.lo : 0;
+            const uint32_t len = hi > lo ? hi - lo : 0;
             const bool is_hub = len > hub;
             const uint32_t mine = is_hub ? 0 : len;
             words += mine;
+            const uint32_t* gadj = FUSED ? gen_s[lane].gadj : p.adj;
             // own rows: lanes step through their lists together
             const uint32_t steps = __reduce_max_sync(0xffffffffu, mine);
             for (uint32_t s = 0; s < steps; ++s) {
                 bool ok = false;
                 uint32_t c = 0;
                 if (s < mine) {
-                    c = __ldg(g.gadj + g.lo + s);
-                    ok = p.n_chk ? ext_accept(p, row, c, g) : ext_injective(p, row, c);
+                    c = __ldg(gadj + lo + s);
+                    ok = FUSED ? ext_accept(p, row, c, gen_s[lane]) : ext_injective(p, row, c);
                 }
                 cnt += ok ? 1u : 0u;
                 if (WRITE) tile_append(*tl, ok, row, k, c, true);
             }
             // hub rows: the whole warp, 32 candidates per step
             uint32_t hubs = __ballot_sync(0xffffffffu, is_hub);
+            if (FUSED) __syncwarp();  // generator states written before other lanes read them
             while (hubs) {
                 const int h = __ffs(hubs) - 1;
                 hubs &= hubs - 1;
-                const GenState gh = shfl_gen(g, h, p.n_chk);
+                const uint32_t hlo = __shfl_sync(0xffffffffu, lo, h), hhi = __shfl_sync(0xffffffffu, hi, h);
                 const uint32_t* hrow = rows_s + (base + h) * k;
+                const uint32_t* hadj = FUSED ? gen_s[h].gadj : p.adj;
                 uint32_t hc = 0;
-                for (uint32_t j0 = gh.lo; j0 < gh.hi; j0 += 32) {
+                for (uint32_t j0 = hlo; j0 < hhi; j0 += 32) {
                     const uint32_t j = j0 + lane;
                     bool ok = false;
                     uint32_t c = 0;
-                    if (j < gh.hi) {
-                        c = __ldg(gh.gadj + j);
-                        ok = p.n_chk ? ext_accept(p, hrow, c, gh) : ext_injective(p, hrow, c);
+                    if (j < hhi) {
+                        c = __ldg(hadj + j);
+                        ok = FUSED ? ext_accept(p, hrow, c, gen_s[h]) : ext_injective(p, hrow, c);
                     }
                     hc += ok ? 1u : 0u;
                     if (WRITE) tile_append(*tl, ok, hrow, k, c, true);
                 }
                 hc = __reduce_add_sync(0xffffffffu, hc);
                 if (lane == h) cnt += hc;
-                if (lane == 0) words += gh.hi - gh.lo;
+                if (lane == 0) words += hhi - hlo;
             }
+            if (FUSED) __syncwarp();  // every lane done with the states before the next rows overwrite them
         }
         if (graphs) add_graph_count(ctx, d.query, row[0], cnt, valid);
         total += cnt;
@@ -371,33 +364,60 @@ __device__ __forceinline__ uint64_t red_item(const TaskDesc& d, const uint32_t* 
     return warp_sum(total);
 }
 
-// Shared memory of one warp: its descriptor copy, the item's rows and the
-// output tile.
-__host__ __device__ constexpr size_t round_warp_words(uint32_t rows_per_item, uint32_t kmax) {
-    return (size_t)rows_per_item * kmax + (size_t)kTileRows * (kmax + 1);
+// Class of a task: fused extensions apart from everything else.
+__host__ __device__ __forceinline__ bool fused_class(uint32_t kind, uint32_t n_chk) {
+    return kind == STEP_EXT && n_chk > 0;
 }
-size_t round_smem_bytes(uint32_t rows_per_item, uint32_t kmax) {
-    return (size_t)kRoundWarps * (sizeof(TaskDesc) + 4 * ((round_warp_words(rows_per_item, kmax) + 3) & ~(size_t)3));
+
+// Shared memory of one warp: the item's rows, (write pass) the output tile
+// and (fused class) the lanes' generator states; before them, one descriptor
+// copy per warp.
+constexpr size_t kGenBytes = 32 * sizeof(GenState);  // per warp
+__host__ __device__ constexpr size_t round_warp_words(uint32_t rows_per_item, uint32_t kmax, bool write) {
+    return (((size_t)rows_per_item * kmax + (write ? (size_t)kTileRows * (kmax + 1) : 0)) + 3) & ~(size_t)3;
+}
+size_t round_smem_bytes(uint32_t rows_per_item, uint32_t kmax, bool write, bool fused) {
+    return (size_t)kRoundWarps *
+           (sizeof(TaskDesc) + (fused ? kGenBytes : 0) + 4 * round_warp_words(rows_per_item, kmax, write));
+}
+
+struct WarpSmem {
+    TaskDesc* d;
+    uint32_t* rows;
+    uint32_t* tile;
+    GenState* gen;
+};
+template <bool WRITE, bool FUSED>
+__device__ __forceinline__ WarpSmem warp_smem(unsigned char* raw, const RoundArgs& a) {
+    const int warp = threadIdx.x >> 5;
+    WarpSmem w;
+    w.d = reinterpret_cast<TaskDesc*>(raw) + warp;
+    unsigned char* area = raw + kRoundWarps * sizeof(TaskDesc);  // 8-byte aligned: TaskDesc holds pointers
+    w.gen = FUSED ? reinterpret_cast<GenState*>(area) + 32 * warp : nullptr;
+    uint32_t* words = reinterpret_cast<uint32_t*>(area + (FUSED ? kRoundWarps * kGenBytes : 0));
+    w.rows = words + warp * round_warp_words(a.rows_per_item, a.kmax, WRITE);
+    w.tile = w.rows + (size_t)a.rows_per_item * a.kmax;
+    return w;
 }
 
 // ---------------------------------------------------------- count pass ----
 // Persistent: warps pull chunks of items from the work queue; each item's
-// accepted rows go to items[item] (no atomics, no block barrier).
-__global__ void __launch_bounds__(kRoundWarps * 32, 4)
+// accepted rows go to items[item] (no atomics, no block barrier).  One
+// instance per task class over that class's range of items.
+template <bool FUSED>
+__global__ void __launch_bounds__(kRoundWarps * 32, FUSED ? 5 : 6)
 round_count_kernel(RoundArgs a) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    TaskDesc* descs = reinterpret_cast<TaskDesc*>(smem_raw);
-    TaskDesc& d = descs[warp];
-    const size_t ww = (round_warp_words(a.rows_per_item, a.kmax) + 3) & ~(size_t)3;
-    uint32_t* rows_s = reinterpret_cast<uint32_t*>(smem_raw + kRoundWarps * sizeof(TaskDesc)) + warp * ww;
+    const int lane = threadIdx.x & 31;
+    const WarpSmem ws = warp_smem<false, FUSED>(smem_raw, a);
+    TaskDesc& d = *ws.d;
     uint32_t t = 0xffffffffu;
     uint64_t t_lo = 0, t_hi = 0;
     const uint32_t* in = nullptr;
     uint64_t nrows = 0;
     uint64_t begin, end;
     while (next_chunk(a, begin, end)) {
-        for (uint64_t item = begin; item < end; ++item) {
+        for (uint64_t item = a.item_base + begin; item < a.item_base + end; ++item) {
             if (item >= t_hi || item < t_lo) {
                 t = find_slot(a.item0, a.nt + 1, item);
                 t_lo = __ldg(a.item0 + t);
@@ -412,9 +432,14 @@ round_count_kernel(RoundArgs a) {
             const uint32_t nr = (uint32_t)umin64(a.rows_per_item, nrows - row0);
             const uint32_t k = d.kind == STEP_EXT ? d.e.k : d.r.k;
             __syncwarp();
-            stage_rows(rows_s, in, row0, nr, k);
-            const uint64_t c = d.kind == STEP_EXT ? ext_item<false>(d, rows_s, nr, a.hub, a.ctx, nullptr, a.read_words)
-                                                  : red_item<false>(d, rows_s, nr, a.ctx, nullptr);
+            stage_rows(ws.rows, in, row0, nr, k);
+            uint64_t c;
+            if (FUSED)
+                c = ext_item<false, true>(d, ws.rows, nr, a.hub, a.ctx, nullptr, ws.gen, a.read_words);
+            else if (d.kind == STEP_EXT)
+                c = ext_item<false, false>(d, ws.rows, nr, a.hub, a.ctx, nullptr, nullptr, a.read_words);
+            else
+                c = red_item<false>(d, ws.rows, nr, a.ctx, nullptr);
             if (lane == 0) a.items[item] = c;
         }
     }
@@ -508,18 +533,16 @@ __global__ void __launch_bounds__(1024) scan_items_top_kernel(uint64_t* __restri
 }
 
 // ---------------------------------------------------------- write pass ----
-// Persistent, over the items of the tasks that write this round: each item's
-// output rows go to its task's buffer at the item's scanned offset, in the
-// order the count pass counted them.  Items without output are skipped.
-__global__ void __launch_bounds__(kRoundWarps * 32, 4)
+// Persistent, over the items of the tasks that write this round (one
+// instance per task class): each item's output rows go to its task's buffer
+// at the item's scanned offset, in the order the count pass counted them.
+// Items without output are skipped.
+template <bool FUSED>
+__global__ void __launch_bounds__(kRoundWarps * 32, FUSED ? 4 : 6)
 round_write_kernel(RoundArgs a) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    const int warp = threadIdx.x >> 5;
-    TaskDesc* descs = reinterpret_cast<TaskDesc*>(smem_raw);
-    TaskDesc& d = descs[warp];
-    const size_t ww = (round_warp_words(a.rows_per_item, a.kmax) + 3) & ~(size_t)3;
-    uint32_t* rows_s = reinterpret_cast<uint32_t*>(smem_raw + kRoundWarps * sizeof(TaskDesc)) + warp * ww;
-    uint32_t* tile_s = rows_s + (size_t)a.rows_per_item * a.kmax;
+    const WarpSmem ws = warp_smem<true, FUSED>(smem_raw, a);
+    TaskDesc& d = *ws.d;
     uint64_t w_lo = 0, w_hi = 0;
     uint32_t t = 0;
     uint64_t t_item0 = 0, t_off0 = 0;
@@ -528,7 +551,7 @@ round_write_kernel(RoundArgs a) {
     uint64_t nrows = 0;
     uint64_t begin, end;
     while (next_chunk(a, begin, end)) {
-        for (uint64_t wi = begin; wi < end; ++wi) {
+        for (uint64_t wi = a.item_base + begin; wi < a.item_base + end; ++wi) {
             if (wi >= w_hi || wi < w_lo) {
                 const uint32_t slot = find_slot(a.witem0, a.nt + 1, wi);
                 w_lo = __ldg(a.witem0 + slot);
@@ -554,17 +577,19 @@ round_write_kernel(RoundArgs a) {
             const bool ext = d.kind == STEP_EXT;
             const uint32_t k = ext ? d.e.k : d.r.k;
             Tile tl;
-            tl.t = tile_s;
+            tl.t = ws.tile;
             tl.w = ext ? k + 1 : k;
             tl.n = 0;
             tl.out = out + (off - t_off0) * tl.w;
             tl.room = off_next - off;
             __syncwarp();
-            stage_rows(rows_s, in, row0, nr, k);
-            if (ext)
-                ext_item<true>(d, rows_s, nr, a.hub, a.ctx, &tl, nullptr);
+            stage_rows(ws.rows, in, row0, nr, k);
+            if (FUSED)
+                ext_item<true, true>(d, ws.rows, nr, a.hub, a.ctx, &tl, ws.gen, nullptr);
+            else if (ext)
+                ext_item<true, false>(d, ws.rows, nr, a.hub, a.ctx, &tl, nullptr, nullptr);
             else
-                red_item<true>(d, rows_s, nr, a.ctx, &tl);
+                red_item<true>(d, ws.rows, nr, a.ctx, &tl);
             if (tl.n) tile_flush(tl, tl.n);
         }
     }
@@ -665,9 +690,11 @@ int BatchSession::init() {
     static std::atomic<bool> smem_set[64];  // sessions may start on several threads (server, miner)
     if (dev < 0 || dev >= 64) return fail(GVA_ERR_ARG, "device index out of range");
     if (!smem_set[dev].load(std::memory_order_acquire)) {
-        const int most = (int)round_smem_bytes(kMaxItemRows / 4, kMaxCols);  // rows per item shrink as rows widen
-        GVA_CUDA_B(cudaFuncSetAttribute(round_count_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, most));
-        GVA_CUDA_B(cudaFuncSetAttribute(round_write_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, most));
+        const int most = (int)round_smem_bytes(kMaxItemRows / 4, kMaxCols, true, true);  // rows per item shrink as rows widen
+        GVA_CUDA_B(cudaFuncSetAttribute(round_count_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, most));
+        GVA_CUDA_B(cudaFuncSetAttribute(round_count_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, most));
+        GVA_CUDA_B(cudaFuncSetAttribute(round_write_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, most));
+        GVA_CUDA_B(cudaFuncSetAttribute(round_write_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, most));
         smem_set[dev].store(true, std::memory_order_release);
     }
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
@@ -740,7 +767,7 @@ void BatchSession::fill_node_desc(int id, void* out) const {
     const BNode& nd = nodes[id];
     TaskDesc& d = *reinterpret_cast<TaskDesc*>(out);
     memset(&d, 0, sizeof d);
-    const Step& st = node_steps[id];
+    const Step& st = *node_steps[id];
     d.kind = st.kind;
     d.mode = nd.first_child < 0 ? MODE_COUNT : MODE_WRITE;
     if (per_graph && nd.first_term >= 0) {
@@ -784,8 +811,10 @@ void BatchSession::fill_node_desc(int id, void* out) const {
     }
 }
 
-int BatchSession::submit(const std::vector<std::vector<Step>>& steps, const std::vector<uint64_t>& tags,
+int BatchSession::submit(std::vector<std::vector<Step>>&& wave, const std::vector<uint64_t>& tags,
                          std::vector<int>* ids, bool presorted) {
+    waves.push_back(std::move(wave));
+    const std::vector<std::vector<Step>>& steps = waves.back();
     const auto t_start = std::chrono::steady_clock::now();
     struct Timer {
         std::chrono::steady_clock::time_point t0;
@@ -798,8 +827,26 @@ int BatchSession::submit(const std::vector<std::vector<Step>>& steps, const std:
     // is matched against the previous plan only and keeps no index; a step
     // that only a non-adjacent plan shares gets a node of its own, which
     // costs sharing, not correctness.
-    std::unordered_multimap<uint64_t, int> index;
-    if (!presorted) index.reserve(steps.size() * 4);
+    // open addressing over (hash, node) slots; each new node's key bytes are
+    // kept in one arena so that a probe compares bytes without serialising
+    // the candidate node's step again
+    struct Slot {
+        uint64_t h;
+        int id;
+        uint32_t key_at;
+    };
+    std::vector<Slot> index;
+    std::vector<uint8_t> key_arena;
+    size_t index_mask = 0;
+    if (!presorted) {
+        size_t total = 0;
+        for (const auto& st : steps) total += st.size();
+        size_t cap = 64;
+        while (cap < 2 * total) cap <<= 1;
+        index.assign(cap, Slot{0, -1, 0});
+        index_mask = cap - 1;
+        key_arena.reserve(total * 64);
+    }
     const int first_node = (int)nodes.size();
     uint8_t kb[512], kb2[512];
     {  // room for the wave (a plan mostly adds a node or two past its shared
@@ -823,8 +870,9 @@ int BatchSession::submit(const std::vector<std::vector<Step>>& steps, const std:
         nd.n_eq = st.n_eq;
         nd.n_pairs = st.n_pairs;
         nd.always_empty = st.always_empty;
+        nd.fused = fused_class(st.kind, st.n_chk) ? 1u : 0u;
         nd.depth = depth;
-        node_steps.push_back(st);
+        node_steps.push_back(&st);
         nd.parent = parent;
         if (parent >= 0) {
             nd.next_sibling = nodes[parent].first_child;
@@ -878,16 +926,22 @@ int BatchSession::submit(const std::vector<std::vector<Step>>& steps, const std:
                 h = (h ^ w) * 1099511628211ull;
             }
             for (size_t j = n & ~(size_t)7; j < n; ++j) h = (h ^ kb[j]) * 1099511628211ull;
+            h ^= h >> 29;
             int id = -1;
-            auto range = index.equal_range(h);
-            for (auto it = range.first; it != range.second && id < 0; ++it) {
-                const BNode& cand = nodes[it->second];
-                if (cand.parent != cur) continue;
-                if (step_key_bytes(node_steps[it->second], kb2) == n && memcmp(kb, kb2, n) == 0) id = it->second;
+            size_t at = (size_t)h & index_mask;
+            for (; index[at].id >= 0; at = (at + 1) & index_mask) {
+                const Slot& sl = index[at];
+                if (sl.h != h || nodes[sl.id].parent != cur) continue;
+                if (key_arena[sl.key_at] == n && memcmp(key_arena.data() + sl.key_at + 1, kb, n) == 0) {
+                    id = sl.id;
+                    break;
+                }
             }
-            if (id < 0) {
+            if (id < 0) {  // `at` is the free slot that ended the probe
                 id = new_node(st[i], cur, (int)i);
-                index.emplace(h, id);
+                index[at] = Slot{h, id, (uint32_t)key_arena.size()};
+                key_arena.push_back((uint8_t)n);
+                key_arena.insert(key_arena.end(), kb, kb + n);
             }
             cur = id;
             path[i] = cur;
@@ -901,7 +955,7 @@ int BatchSession::submit(const std::vector<std::vector<Step>>& steps, const std:
     // seeds: the children of every seed node start from its vertex list
     for (int id = first_node; id < (int)nodes.size(); ++id) {
         if (nodes[id].parent != -1) continue;
-        const Step& sd = node_steps[id];
+        const Step& sd = *node_steps[id];
         uint64_t n = 0;
         if (!sd.always_empty) n = db.seed_off[sd.label + 1] - db.seed_off[sd.label];
         if (n)
@@ -947,6 +1001,9 @@ int BatchSession::round() {
     }
     if (active.empty()) return GVA_OK;
     ++rounds;
+    // tasks of the light class first, then the fused class: each class's
+    // items form one range, run by that class's kernels
+    std::stable_partition(active.begin(), active.end(), [&](const BTask& tk) { return !nodes[tk.node].fused; });
     // the previous round's host-to-device copies read the staging area
     if (staged) {
         GVA_CUDA_B(cudaEventSynchronize(staged));
@@ -970,7 +1027,7 @@ int BatchSession::round() {
     // staging: refs[nt] | new node descriptors (<= nt) | item0[nt+1] | totals[nt] | outs[nt] | wtask[nt] | witem0[nt+1]
     const size_t ref_bytes = (size_t)nt * sizeof(TaskRef);
     const size_t desc_max = (size_t)nt * sizeof(TaskDesc);
-    const size_t small_words = (size_t)(nt + 1) + nt + nt + 2 + nt + (nt + 1);
+    const size_t small_words = (size_t)(nt + 1) + nt + nt + 4 + nt + (nt + 1);
     char* h = staging.get(ref_bytes + desc_max + small_words * 8);
     if (!h) return fail(GVA_ERR_NOMEM, "pinned staging allocation failed");
     TaskRef* refs = (TaskRef*)h;
@@ -978,15 +1035,16 @@ int BatchSession::round() {
     uint64_t* h_item0 = (uint64_t*)(h + ref_bytes + desc_max);
     uint64_t* h_totals = h_item0 + (nt + 1);
     uint32_t** h_outs = (uint32_t**)(h_totals + nt);
-    uint64_t* h_wtask = h_totals + 2 * nt + 2;  // nt 8-byte words holding uint32 task indices
+    uint64_t* h_wtask = h_totals + 2 * nt + 4;  // nt 8-byte words holding uint32 task indices
     uint64_t* h_witem0 = h_wtask + nt;
     const int dev_first = dev_count;
     double cbytes = 0, crows = 0;
-    uint64_t ni = 0;
+    uint64_t ni = 0, ni_light = 0;
     h_item0[0] = 0;
     for (int t = 0; t < nt; ++t) {
         const BTask& tk = active[t];
         BNode& nd = nodes[tk.node];
+        if (!nd.fused) ni_light = ni + (tk.rows + R - 1) / R;
         if (nd.dev < 0) {  // first task of this node: ship its parameters
             nd.dev = dev_count++;
             fill_node_desc(tk.node, new_desc + (size_t)(nd.dev - dev_first) * sizeof(TaskDesc));
@@ -1030,18 +1088,18 @@ int BatchSession::round() {
     uint64_t* d_item0 = d_small;
     uint64_t* d_totals = d_item0 + (nt + 1);
     uint32_t** d_outs = (uint32_t**)(d_totals + nt);
-    unsigned long long* d_queue = (unsigned long long*)(d_totals + 2 * nt);  // two heads: count, write
-    uint64_t* d_wtask = d_totals + 2 * nt + 2;
+    unsigned long long* d_queue = (unsigned long long*)(d_totals + 2 * nt);  // four heads: count and write, per class
+    uint64_t* d_wtask = d_totals + 2 * nt + 4;
     uint64_t* d_witem0 = d_wtask + nt;
     if (dev_count > dev_first)
         GVA_CUDA_B(cudaMemcpyAsync((char*)d_nodes + (size_t)dev_first * sizeof(TaskDesc), new_desc,
                                    (size_t)(dev_count - dev_first) * sizeof(TaskDesc), cudaMemcpyHostToDevice, s));
     GVA_CUDA_B(cudaMemcpyAsync(d_desc, refs, ref_bytes, cudaMemcpyHostToDevice, s));
     GVA_CUDA_B(cudaMemcpyAsync(d_item0, h_item0, (nt + 1) * 8, cudaMemcpyHostToDevice, s));
-    GVA_CUDA_B(cudaMemsetAsync(d_queue, 0, 16, s));
+    GVA_CUDA_B(cudaMemsetAsync(d_queue, 0, 32, s));
     if (pf) GVA_CUDA_B(cudaMemsetAsync(d_read, 0, 8, s));
     lap(0);
-    const size_t smem = round_smem_bytes(R, kmax);
+
     RoundArgs ra{};
     ra.nodes = (const TaskDesc*)d_nodes;
     ra.refs = (const TaskRef*)d_desc;
@@ -1055,24 +1113,45 @@ int BatchSession::round() {
     ra.queue = d_queue;
     ra.read_words = pf ? d_read : nullptr;
     ra.ctx = ctx;
-    auto grid_for = [&](const void* fn) -> uint32_t {
+    auto grid_for = [&](const void* fn, uint64_t items, size_t smem) -> uint32_t {
         int per_sm = 1;
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kRoundWarps * 32, smem);
-        return (uint32_t)std::max(per_sm, 1) * (uint32_t)sms;
+        return (uint32_t)std::min<uint64_t>((uint64_t)std::max(per_sm, 1) * (uint64_t)sms,
+                                            (items + kRoundWarps - 1) / kRoundWarps);
     };
-    const uint32_t cgrid = (uint32_t)std::min<uint64_t>(grid_for((const void*)round_count_kernel),
-                                                        (ni + kRoundWarps - 1) / kRoundWarps);
-    ra.total_warps = cgrid * kRoundWarps;
     cudaEvent_t ev = nullptr;
     if (pf) pf->begin(K_EXT_COUNT, cbytes, s, ev);
-    round_count_kernel<<<cgrid, kRoundWarps * 32, smem, s>>>(ra);
+    if (ni_light > 0) {  // light class: items [0, ni_light)
+        RoundArgs la = ra;
+        la.item_base = 0;
+        la.n_items = ni_light;
+        la.queue = d_queue;
+        const size_t smem = round_smem_bytes(R, kmax, false, false);
+            const uint32_t g = grid_for((const void*)round_count_kernel<false>, ni_light, smem);
+        la.total_warps = g * kRoundWarps;
+        round_count_kernel<false><<<g, kRoundWarps * 32, smem, s>>>(la);
+        launches += 1;
+        g_batch_launches += 1;
+    }
+    if (ni > ni_light) {  // fused class: items [ni_light, ni)
+        RoundArgs fa = ra;
+        fa.item_base = ni_light;
+        fa.n_items = ni - ni_light;
+        fa.queue = d_queue + 1;
+        const size_t smem = round_smem_bytes(R, kmax, false, true);
+            const uint32_t g = grid_for((const void*)round_count_kernel<true>, ni - ni_light, smem);
+        fa.total_warps = g * kRoundWarps;
+        round_count_kernel<true><<<g, kRoundWarps * 32, smem, s>>>(fa);
+        launches += 1;
+        g_batch_launches += 1;
+    }
     if (pf) pf->end(ev, K_EXT_COUNT, cbytes, s, crows);
     if (pf) pf->begin(K_SCAN, 16.0 * ni, s, ev);
     scan_items_local_kernel<<<(unsigned)nc, 1024, 0, s>>>(d_items, ni, d_chunks);
     scan_items_top_kernel<<<1, 1024, 0, s>>>(d_chunks, nc, d_items, ni, d_item0, (uint32_t)nt, d_totals);
     if (pf) pf->end(ev, K_SCAN, 16.0 * ni, s, (double)ni);
-    launches += 3;
-    g_batch_launches += 3;
+    launches += 2;
+    g_batch_launches += 2;
     GVA_CUDA_B(cudaGetLastError());
     GVA_CUDA_B(cudaMemcpyAsync(h_totals, d_totals, nt * 8, cudaMemcpyDeviceToHost, s));
     uint64_t h_read_count = 0;
@@ -1156,7 +1235,7 @@ int BatchSession::round() {
         buf = std::shared_ptr<void>(p, [ss](void* q) { cudaFreeAsync(q, ss); });
         double wbytes = 0, wrows = 0;
         uint32_t nw = 0;
-        uint64_t wi = 0;
+        uint64_t wi = 0, wi_light = 0;
         uint32_t* h_wt = (uint32_t*)h_wtask;  // task index per writing slot (uint32)
         h_witem0[0] = 0;
         for (int t = 0; t < nt; ++t) {
@@ -1165,6 +1244,7 @@ int BatchSession::round() {
             h_wt[nw] = (uint32_t)t;
             wi += h_item0[t + 1] - h_item0[t];
             h_witem0[++nw] = wi;
+            if (!nodes[active[t].node].fused) wi_light = wi;
             wrows += (double)active[t].rows;
             const BNode& st = nodes[active[t].node];
             const double k = st.width_in;
@@ -1182,17 +1262,34 @@ int BatchSession::round() {
         wa.chunks = d_chunks;
         wa.n_count_items = ni;
         wa.n_chunks = nc;
-        wa.queue = d_queue + 1;
         wa.task_out = d_outs;
         wa.read_words = nullptr;
-        const uint32_t wgrid = (uint32_t)std::min<uint64_t>(grid_for((const void*)round_write_kernel),
-                                                            (wi + kRoundWarps - 1) / kRoundWarps);
-        wa.total_warps = wgrid * kRoundWarps;
         if (pf) pf->begin(K_EXT_WRITE, wbytes, s, ev);
-        round_write_kernel<<<wgrid, kRoundWarps * 32, smem, s>>>(wa);
+        if (wi_light > 0) {
+            RoundArgs la = wa;
+            la.item_base = 0;
+            la.n_items = wi_light;
+            la.queue = d_queue + 2;
+            const size_t smem = round_smem_bytes(R, kmax, true, false);
+            const uint32_t g = grid_for((const void*)round_write_kernel<false>, wi_light, smem);
+            la.total_warps = g * kRoundWarps;
+            round_write_kernel<false><<<g, kRoundWarps * 32, smem, s>>>(la);
+            launches += 1;
+            g_batch_launches += 1;
+        }
+        if (wi > wi_light) {
+            RoundArgs fa = wa;
+            fa.item_base = wi_light;
+            fa.n_items = wi - wi_light;
+            fa.queue = d_queue + 3;
+            const size_t smem = round_smem_bytes(R, kmax, true, true);
+            const uint32_t g = grid_for((const void*)round_write_kernel<true>, wi - wi_light, smem);
+            fa.total_warps = g * kRoundWarps;
+            round_write_kernel<true><<<g, kRoundWarps * 32, smem, s>>>(fa);
+            launches += 1;
+            g_batch_launches += 1;
+        }
         if (pf) pf->end(ev, K_EXT_WRITE, wbytes, s, wrows);
-        launches += 1;
-        g_batch_launches += 1;
         GVA_CUDA_B(cudaGetLastError());
     } else {
         GVA_CUDA_B(cudaEventRecord(staged, s));
@@ -1293,7 +1390,7 @@ __global__ void slot_popcount_kernel(const uint32_t* __restrict__ bits, uint32_t
     }
 }
 
-int prepare_batch(DevDB& db, const std::vector<std::vector<Step>>& steps, cudaStream_t s, uint64_t budget,
+int prepare_batch(DevDB& db, std::vector<std::vector<Step>>&& steps, cudaStream_t s, uint64_t budget,
                   bool per_graph, bool graph_counts, bool profile, PreparedBatch& out, bool presorted) {
     const auto t0 = std::chrono::steady_clock::now();
     GVA_CUDA_B(cudaSetDevice(db.device));
@@ -1304,7 +1401,7 @@ int prepare_batch(DevDB& db, const std::vector<std::vector<Step>>& steps, cudaSt
     if (out.nq == 0) return GVA_OK;
     out.ses.reset(new BatchSession(db, s, budget, per_graph ? (uint32_t)out.nq : 0, graph_counts, profile));
     int rc = out.ses->init();
-    if (!rc) rc = out.ses->submit(steps, {}, &out.ids, presorted);
+    if (!rc) rc = out.ses->submit(std::move(steps), {}, &out.ids, presorted);
     out.prep_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
     return rc;
 }
@@ -1397,16 +1494,100 @@ int finish_batch(DevDB& db, PreparedBatch& pb, uint64_t* counts, uint64_t* graph
     return rc;
 }
 
-int run_batch(DevDB& db, const std::vector<std::vector<Step>>& steps, cudaStream_t s, uint64_t budget,
+// Plans ordered by their sequences of step keys (64-bit hashes of the key
+// bytes), so that plans sharing a step prefix are adjacent and the trie is
+// built against the previous plan only (presorted submit), with the same
+// nodes as the indexed build.  Keys hashed and chunks sorted on the host's
+// cores.
+static void order_by_step_keys(const std::vector<std::vector<Step>>& steps, std::vector<uint32_t>& order) {
+    const size_t n = steps.size();
+    size_t w = 1;
+    for (const auto& v : steps) w = std::max(w, v.size());
+    std::vector<uint64_t> key(n * w, 0);  // 0 ends a plan's sequence
+    const unsigned nth = n < 2048 ? 1u : std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
+    auto run = [&](auto&& fn) {
+        if (nth == 1) {
+            fn(0u);
+            return;
+        }
+        std::vector<std::thread> pool;
+        for (unsigned t = 0; t < nth; ++t) pool.emplace_back(fn, t);
+        for (auto& th : pool) th.join();
+    };
+    run([&](unsigned t) {
+        uint8_t kb[512];
+        for (size_t i = t; i < n; i += nth)
+            for (size_t j = 0; j < steps[i].size(); ++j) {
+                const size_t len = step_key_bytes(steps[i][j], kb);
+                uint64_t h = 1469598103934665603ull;
+                for (size_t b = 0; b < len; ++b) h = (h ^ kb[b]) * 1099511628211ull;
+                key[i * w + j] = h | 1;
+            }
+    });
+    order.resize(n);
+    for (size_t i = 0; i < n; ++i) order[i] = (uint32_t)i;
+    auto less = [&](uint32_t a, uint32_t b) {
+        const uint64_t* ka = key.data() + (size_t)a * w;
+        const uint64_t* kb = key.data() + (size_t)b * w;
+        for (size_t j = 0; j < w; ++j)
+            if (ka[j] != kb[j]) return ka[j] < kb[j];
+        return a < b;
+    };
+    // sorted chunks, merged pairwise
+    size_t chunks = 1;
+    while (chunks * 2 <= nth && chunks < 32) chunks *= 2;
+    std::vector<size_t> cut(chunks + 1);
+    for (size_t c = 0; c <= chunks; ++c) cut[c] = n * c / chunks;
+    {
+        std::vector<std::thread> pool;
+        for (size_t c = 0; c < chunks; ++c)
+            pool.emplace_back([&, c]() { std::sort(order.begin() + cut[c], order.begin() + cut[c + 1], less); });
+        for (auto& th : pool) th.join();
+    }
+    for (size_t width = 1; width < chunks; width *= 2) {
+        std::vector<std::thread> pool;
+        for (size_t c = 0; c + width < chunks; c += 2 * width) {
+            const size_t lo = cut[c], mid = cut[c + width], hi = cut[std::min(chunks, c + 2 * width)];
+            pool.emplace_back([&, lo, mid, hi]() {
+                std::inplace_merge(order.begin() + lo, order.begin() + mid, order.begin() + hi, less);
+            });
+        }
+        for (auto& th : pool) th.join();
+    }
+}
+
+int run_batch(DevDB& db, std::vector<std::vector<Step>> steps, cudaStream_t s, uint64_t budget,
               const uint32_t* vgraph, uint32_t G, uint64_t* counts, uint64_t* graph_counts_host,
               uint32_t* support_host, bool profile, BatchStats* stats) {
     (void)vgraph;
     (void)G;
+    const auto t0 = std::chrono::steady_clock::now();
+    const size_t n = steps.size();
+    std::vector<uint32_t> order;
+    order_by_step_keys(steps, order);
+    std::vector<std::vector<Step>> sorted(n);
+    for (size_t i = 0; i < n; ++i) sorted[i] = std::move(steps[order[i]]);
+    const double order_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
     PreparedBatch pb;
-    int rc = prepare_batch(db, steps, s, budget, graph_counts_host || support_host, graph_counts_host != nullptr,
-                           profile, pb);
+    int rc = prepare_batch(db, std::move(sorted), s, budget, graph_counts_host || support_host,
+                           graph_counts_host != nullptr, profile, pb, true);
     if (rc) return rc;
-    return finish_batch(db, pb, counts, graph_counts_host, support_host, stats);
+    // results in submission (sorted) order, then back to the caller's order
+    std::vector<uint64_t> c2(n);
+    std::vector<uint32_t> s2(support_host ? n : 0);
+    std::vector<uint64_t> g2(graph_counts_host ? n * (size_t)db.num_graphs : 0);
+    rc = finish_batch(db, pb, c2.data(), graph_counts_host ? g2.data() : nullptr, support_host ? s2.data() : nullptr,
+                      stats);
+    if (rc) return rc;
+    const size_t Gn = db.num_graphs;
+    for (size_t i = 0; i < n; ++i) {
+        counts[order[i]] = c2[i];
+        if (support_host) support_host[order[i]] = s2[i];
+        if (graph_counts_host)
+            std::copy(g2.begin() + i * Gn, g2.begin() + (i + 1) * Gn, graph_counts_host + (size_t)order[i] * Gn);
+    }
+    if (stats) stats->submit_ms += order_ms;
+    return GVA_OK;
 }
 
 // Candidate launch shapes: rows per work item x the list length from which a

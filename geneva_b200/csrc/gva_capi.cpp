@@ -389,7 +389,8 @@ int gva_batch_count(gva_db* db, const gva_plan* const* plans, int nplans, const 
     }
     const double lower_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_lower).count();
     BatchStats bs;
-    int st = run_batch(*db->dev, steps, (cudaStream_t)o.stream, o.budget_bytes, db->dev->vgraph, db->dev->num_graphs,
+    int st = run_batch(*db->dev, std::move(steps), (cudaStream_t)o.stream, o.budget_bytes, db->dev->vgraph,
+                       db->dev->num_graphs,
                        counts, graph_counts, graph_support, o.profile != 0, &bs);
     if (stats) {
         memset(stats, 0, sizeof *stats);
@@ -403,6 +404,7 @@ int gva_batch_count(gva_db* db, const gva_plan* const* plans, int nplans, const 
         stats->round_host_ms = bs.round_host_ms;
         stats->wait_ms = bs.wait_ms;
         stats->session_ms = bs.session_ms;
+        for (int i = 0; i < 5; ++i) stats->round_phase_ms[i] = bs.phase_ms[i];
         for (int i = 0; i < K_NUM && i < 5; ++i) {
             strncpy(stats->kernels[i].name, kKernelNames[i], sizeof stats->kernels[i].name - 1);
             stats->kernels[i].launches = bs.kstat[i].launches;
@@ -630,7 +632,7 @@ int gva_session_submit(gva_session* s, const gva_plan* const* plans, const uint6
         if (st) return st;
         tg[i] = tags ? tags[i] : (uint64_t)i;
     }
-    return s->ses->submit(steps, tg, nullptr);
+    return s->ses->submit(std::move(steps), tg, nullptr);
 }
 
 int gva_session_round(gva_session* s, int* active_tasks) {

@@ -98,7 +98,7 @@ struct BatchStats {
 // parents agree.  buf must hold 512 bytes.
 size_t step_key_bytes(const Step& st, uint8_t* buf);
 
-int run_batch(DevDB& db, const std::vector<std::vector<Step>>& steps, cudaStream_t s, uint64_t budget,
+int run_batch(DevDB& db, std::vector<std::vector<Step>> steps, cudaStream_t s, uint64_t budget,
               const uint32_t* vgraph, uint32_t G, uint64_t* counts, uint64_t* graph_counts_host,
               uint32_t* support_host, bool profile, BatchStats* stats);
 uint64_t batch_kernel_launches();
@@ -122,6 +122,7 @@ public:
     struct BNode {
         uint32_t kind = 0, width_in = 0, n_eq = 0, n_pairs = 0;
         uint32_t always_empty = 0;
+        uint32_t fused = 0;  // an extension with fused back-edge checks (its own round kernels)
         int depth = 0;
         int parent = -1;
         int first_child = -1, next_sibling = -1;  // children as a linked list
@@ -151,8 +152,15 @@ public:
     int init();
     // presorted: the plans come in order of their step keys (plans sharing a
     // prefix are adjacent); the trie is then built without a hash index
-    int submit(const std::vector<std::vector<Step>>& steps, const std::vector<uint64_t>& tags, std::vector<int>* ids,
+    // The session keeps the submitted steps (moved in, not copied: trie nodes
+    // point at them).
+    int submit(std::vector<std::vector<Step>>&& steps, const std::vector<uint64_t>& tags, std::vector<int>* ids,
                bool presorted = false);
+    int submit(const std::vector<std::vector<Step>>& steps, const std::vector<uint64_t>& tags, std::vector<int>* ids,
+               bool presorted = false) {
+        std::vector<std::vector<Step>> copy(steps);
+        return submit(std::move(copy), tags, ids, presorted);
+    }
     int round();
     bool idle() const { return active.empty(); }
     std::vector<int> take_completed();
@@ -164,7 +172,7 @@ public:
     void release(int q);
     size_t num_nodes() const { return nodes.size(); }
     const BNode& node(int id) const { return nodes[id]; }           // trie introspection (host only)
-    const Step& node_step(int id) const { return node_steps[id]; }
+    const Step& node_step(int id) const { return *node_steps[id]; }
     cudaStream_t stream() const { return s; }
     size_t num_active() const { return active.size(); }
     uint32_t words() const { return ctx_words; }
@@ -204,7 +212,8 @@ private:
     void* acc = nullptr;
     std::vector<int> free_slots;
     std::vector<BNode> nodes;
-    std::vector<Step> node_steps;  // parallel to nodes
+    std::vector<const Step*> node_steps;  // parallel to nodes, into `waves`
+    std::vector<std::vector<std::vector<Step>>> waves;  // every submitted wave's steps
     std::vector<PlanRec> plans;
     std::vector<BTask> active;
     std::vector<int> completed;
@@ -237,7 +246,7 @@ struct PreparedBatch {
     bool per_graph = false, graph_counts = false;
     double prep_ms = 0.0;
 };
-int prepare_batch(DevDB& db, const std::vector<std::vector<Step>>& steps, cudaStream_t s, uint64_t budget,
+int prepare_batch(DevDB& db, std::vector<std::vector<Step>>&& steps, cudaStream_t s, uint64_t budget,
                   bool per_graph, bool graph_counts, bool profile, PreparedBatch& out, bool presorted = false);
 int finish_batch(DevDB& db, PreparedBatch& pb, uint64_t* counts, uint64_t* graph_counts_host, uint32_t* support_host,
                  BatchStats* stats, const volatile int* cancel = nullptr);

@@ -226,7 +226,7 @@ int run_mine(DevDB& db, cudaStream_t s, uint64_t budget, uint32_t max_edges, uin
             const size_t b0 = b * batch_limit, b1 = std::min(n, b0 + batch_limit);
             std::vector<std::vector<Step>> cur(b1 - b0);
             for (size_t i = b0; i < b1; ++i) cur[i - b0] = std::move(all[order[i]]);
-            p->rc = prepare_batch(db, cur, s, budget, true, false, profile, p->pb, true);  // ordered by step keys
+            p->rc = prepare_batch(db, std::move(cur), s, budget, true, false, profile, p->pb, true);  // ordered by step keys
             if (p->rc) p->err = last_error_cstr();
             return p;
         };

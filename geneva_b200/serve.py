@@ -10,7 +10,12 @@ server keeps one database resident and a batched session open (gva_session):
 * mining requests (max edges, min support) run on a worker thread with their
   own CUDA stream, so their rounds overlap the matching rounds on the device;
   they mine the graph database (graph support) or, when the server is given
-  one data graph for mining, that graph (MNI support).
+  one data graph for mining, that graph (MNI support).  A mining run takes
+  seconds, so at most `mine_queue_limit` of them wait behind the running one;
+  a mining request arriving when that many wait is rejected at once
+  (GenevaError, status REJECTED) instead of queueing without bound, which
+  keeps the latency of every admitted mining request bounded by about
+  (mine_queue_limit + 1) runs.
 
 Latency of a request = completion time - arrival time (host wall clock).
 """
@@ -28,6 +33,9 @@ from typing import List, Optional
 import numpy as np
 
 from . import Database, GenevaError, MODE_DV, Plan, _check, library, mine
+
+
+REJECTED = 8  # status of a mining request refused by the admission policy (queue full)
 
 
 @dataclass
@@ -67,13 +75,15 @@ class Server:
     def __init__(self, db: Database, budget_bytes: int = 150 << 30, support: bool = True,
                  slots: int = 4096, match_stream: Optional[int] = None, mine_stream: Optional[int] = None,
                  mine_db: Optional[Database] = None, mine_sm_percent: int = 50,
-                 mine_host_threads: Optional[int] = None):
+                 mine_host_threads: Optional[int] = None, mine_queue_limit: int = 2):
         """db: the graph database matching requests run against (and mining
         requests, with graph support, when mine_db is None).  mine_db: one
         data graph that mining requests run against with MNI support.
         Mining runs are long; they get at most mine_sm_percent of the SMs
         (MNI search kernel) and mine_host_threads host threads (default: half
-        the cores), so that matching rounds keep GPU and host time."""
+        the cores), so that matching rounds keep GPU and host time.
+        mine_queue_limit: mining requests that may wait behind the running
+        one; later ones are rejected at arrival (status REJECTED)."""
         self.lib = _declare(library())
         self.db = db
         self._max_vertex_id = db.info()["max_vertex_id"]
@@ -90,6 +100,8 @@ class Server:
         self._slots = slots
         self._arrivals: "queue.Queue[Request]" = queue.Queue()
         self._mine_q: "queue.Queue[Optional[Request]]" = queue.Queue()
+        self.mine_queue_limit = mine_queue_limit
+        self.mine_rejected = 0
         self._waiting: List[Request] = []
         self._inflight = {}
         self._reserved = 0
@@ -113,6 +125,11 @@ class Server:
 
     def submit_mine(self, max_edges: int, min_support: int) -> Request:
         r = Request("mine", (max_edges, min_support), arrival=time.perf_counter())
+        if self._mine_q.qsize() >= self.mine_queue_limit:
+            r.done = r.arrival
+            self.mine_rejected += 1
+            r.future.set_exception(GenevaError(REJECTED, "mining queue full: request rejected at admission"))
+            return r
         self._mine_q.put(r)
         return r
 

@@ -181,6 +181,9 @@ typedef struct gva_batch_stats {
      * rounds' host work (task lists, launches, budget choice), waiting for
      * the device, session set-up / read-back / tear-down */
     double lower_ms, submit_ms, round_host_ms, wait_ms, session_ms;
+    /* round_host_ms by part: task list and uploads, count launches, totals
+     * and budget choice, write launch, next tasks and completion */
+    double round_phase_ms[5];
 } gva_batch_stats;
 
 /* Declares the database a union of graphs: graph g owns vertex ids

@@ -157,3 +157,34 @@ def test_mni_eight_vertex_path_and_hub_star(native, oracle):
         assert int(s) == mni_from_rows(oracle, og, p), p
     oracle.free(og)
     gdb.close()
+
+
+@pytest.mark.gpu
+def test_mni_on_a_config4_shaped_rmat(native, oracle):
+    """R-MAT with the single-graph configuration's shape at 1/64 of its size
+    (a = 0.57, b = c = 0.19, average degree 32, 32 vertex labels Zipf(1.0)):
+    300 sampled patterns of 2-4 vertices, exact and capped at 1,000 (the
+    configuration's minimum support), batched and plain, against the oracle's
+    existence search; those with at most 500,000 oracle rows also against
+    the cpumine rows with automorphism orbits unioned."""
+    db = workloads.rmat_graph(16, 1 << 20, 32, 1.0, seed=44, name="c4_shape")
+    gdb = gv.Database.from_edges(db.vlabels, db.src, db.dst, db.elabels)
+    mg = oracle.mni_graph(db.vlabels, db.src, db.dst, db.elabels)
+    og = oracle.from_edges(db.vlabels, db.src, db.dst, db.elabels)
+    pats = workloads.sample_patterns(db, 300, 2, 4, seed=45)
+    exact = [oracle.mni(mg, p)[0] for p in pats]
+    sup, _ = gv.mni_support(gdb, pats, cap=0)
+    assert [int(x) for x in sup] == exact
+    for plain in (False, True):
+        capped, _ = gv.mni_support(gdb, pats, cap=1000, plain=plain)
+        assert [int(x) for x in capped] == [min(e, 1000) for e in exact]
+    rows_checked = 0
+    for p, e in zip(pats, exact):
+        if oracle.count(og, p, cap_rows=500_000) is None:
+            continue
+        assert mni_from_rows(oracle, og, p) == e, p
+        rows_checked += 1
+    assert rows_checked >= 100
+    oracle.mni_graph_free(mg)
+    oracle.free(og)
+    gdb.close()

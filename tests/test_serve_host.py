@@ -177,3 +177,34 @@ def test_close_cancels_mining(fake, monkeypatch):
     with pytest.raises(gv.GenevaError, match="closed"):
         queued.future.result(timeout=10)
     assert seen_cancel == [1]
+
+
+def test_mining_admission_rejects_beyond_the_queue_limit(fake, monkeypatch):
+    """At most mine_queue_limit mining requests wait behind the running one;
+    later ones are rejected at arrival (status REJECTED) and the admitted ones
+    all complete."""
+    release = threading.Event()
+    started = threading.Event()
+
+    def fake_mine(db, max_edges, min_support, stream=None, cancel=None, **kw):
+        started.set()
+        release.wait(10)
+        return ("patterns", {"candidates": max_edges})
+
+    monkeypatch.setattr(serve, "mine", fake_mine)
+    srv = serve.Server(FakeDb(), budget_bytes=1 << 40, slots=64, mine_queue_limit=2)
+    first = srv.submit_mine(3, 10)
+    assert started.wait(10)  # running, no longer queued
+    reqs = [srv.submit_mine(4, 10) for _ in range(6)]
+    rejected = [r for r in reqs if r.future.done()]
+    assert len(rejected) == 4 and srv.mine_rejected == 4
+    for r in rejected:
+        with pytest.raises(gv.GenevaError) as e:
+            r.future.result(timeout=1)
+        assert e.value.status == serve.REJECTED
+    release.set()
+    assert first.future.result(timeout=10)[1]["candidates"] == 3
+    for r in reqs:
+        if r not in rejected:
+            assert r.future.result(timeout=10)[1]["candidates"] == 4
+    srv.close()
