@@ -653,14 +653,41 @@ Staging::~Staging() { pin_give(p, cap); }
 // every round() advances all active tasks by one step; a plan completes when
 // no task on its path is left.  run_batch() is one wave run to completion;
 // the serving loop submits new waves between rounds.
+// Host containers of ended sessions, kept per thread for the next session:
+// a batched run's trie and plan records are rebuilt on every call, and fresh
+// vectors would pay a page fault per page on first touch.
+namespace {
+struct SessionSpare {
+    std::vector<BatchSession::BNode> nodes;
+    std::vector<const Step*> node_steps;
+    std::vector<BatchSession::PlanRec> plans;
+};
+thread_local SessionSpare t_spare;
+}  // namespace
+
 BatchSession::BatchSession(DevDB& db_, cudaStream_t s_, uint64_t budget_, uint32_t slots_, bool graph_counts_,
                            bool profile_)
     : db(db_), s(s_), budget(budget_), nslots(slots_), want_graph_counts(graph_counts_), profile(profile_) {
     tune.rows_per_item = db.tune_rows_per_item;
     tune.hub = db.tune_hub;
+    nodes.swap(t_spare.nodes);
+    node_steps.swap(t_spare.node_steps);
+    plans.swap(t_spare.plans);
+    nodes.clear();
+    node_steps.clear();
+    plans.clear();
 }
 
 BatchSession::~BatchSession() {
+    auto keep = [](auto& mine, auto& spare) {
+        if (mine.capacity() > spare.capacity()) {
+            mine.clear();
+            mine.swap(spare);
+        }
+    };
+    keep(nodes, t_spare.nodes);
+    keep(node_steps, t_spare.node_steps);
+    keep(plans, t_spare.plans);
     cudaSetDevice(db.device);
     active.clear();
     if (staged) cudaEventDestroy(staged);
@@ -774,7 +801,7 @@ void BatchSession::fill_node_desc(int id, void* out) const {
         d.mode = nd.first_child < 0 ? MODE_COUNT_GRAPHS : MODE_WRITE_AND_GRAPHS;
         d.query = (uint32_t)plans[nd.first_term].slot;
     }
-    if (st.kind == STEP_SEED || st.always_empty || st.part == 0) return;
+    if (st.kind == STEP_SEED || st.always_empty || st.part == 0 || st.part > db.parts.size()) return;
     const DevPart& P = db.parts[st.part - 1];
     if (st.kind == STEP_EXT) {
         ExtArgs& a = d.e;
@@ -793,6 +820,7 @@ void BatchSession::fill_node_desc(int id, void* out) const {
             a.chk_col[i] = st.chk_col[i];
             a.chk_dir[i] = st.chk_dir[i];
             a.chk_lab[i] = st.chk_lab[i];
+            if (st.chk_part[i] == 0 || st.chk_part[i] > db.parts.size()) continue;  // lowering marks such steps empty
             a.chk_off[i] = db.parts[st.chk_part[i] - 1].off;
             a.chk_adj[i] = db.parts[st.chk_part[i] - 1].adj;
         }
@@ -883,6 +911,173 @@ int BatchSession::submit(std::vector<std::vector<Step>>&& wave, const std::vecto
         }
         return id;
     };
+    // a presorted wave of many plans: cut into chunks at changes of the first
+    // two steps and built on the host's cores (only seed nodes, which cost
+    // nothing on the device, can repeat across chunks)
+    const unsigned hw = std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
+    if (presorted && steps.size() >= 4096 && hw > 1) {
+        const size_t np = steps.size();
+        for (const auto& st : steps)
+            if (st.size() < 2 || st[0].kind != STEP_SEED) return fail(GVA_ERR_ARG, "plan must start with a seed step");
+        if (per_graph && free_slots.size() < np) return fail(GVA_ERR_NOMEM, "no free per-graph result slot");
+        const int q0 = (int)plans.size();
+        for (size_t qi = 0; qi < np; ++qi) {
+            PlanRec pr;
+            pr.tag = qi < tags.size() ? tags[qi] : qi;
+            if (per_graph) {
+                pr.slot = free_slots.back();
+                free_slots.pop_back();
+            }
+            plans.push_back(pr);
+            if (ids) ids->push_back(q0 + (int)qi);
+        }
+        // seed nodes first, on this thread (presorted: equal seed steps are adjacent)
+        std::vector<int> root_of(np);
+        {
+            uint8_t ka[512], kc[512];
+            int root = -1;
+            for (size_t qi = 0; qi < np; ++qi) {
+                const Step& s0 = steps[qi][0];
+                bool same = false;
+                if (qi > 0) {
+                    const Step& p0 = steps[qi - 1][0];
+                    same = memcmp(&s0, &p0, sizeof(Step)) == 0;
+                    if (!same) {
+                        const size_t n = step_key_bytes(s0, ka);
+                        same = step_key_bytes(p0, kc) == n && memcmp(ka, kc, n) == 0;
+                    }
+                }
+                if (!same) {
+                    root = (int)nodes.size();
+                    BNode nd;
+                    nd.kind = s0.kind;
+                    nd.width_in = s0.width_in;
+                    nd.always_empty = s0.always_empty;
+                    nd.depth = 0;
+                    nodes.push_back(nd);
+                    node_steps.push_back(&s0);
+                }
+                root_of[qi] = root;
+            }
+        }
+        const int first_chunk_node = (int)nodes.size();
+        // chunks cut where the first two steps change, so that no node below
+        // a seed node is split across chunks
+        const unsigned T = std::max(1u, std::min<unsigned>(hw, (unsigned)(np / 1024)));
+        auto same01 = [&](size_t a, size_t b) {
+            return root_of[a] == root_of[b] && memcmp(&steps[a][1], &steps[b][1], sizeof(Step)) == 0;
+        };
+        std::vector<size_t> cut(T + 1, np);
+        cut[0] = 0;
+        for (unsigned t = 1; t < T; ++t) {
+            size_t c = std::max(np * t / T, cut[t - 1]);
+            while (c < np && c > cut[t - 1] && same01(c - 1, c)) ++c;
+            cut[t] = c;
+        }
+        // a chunk's nodes use local ids >= 0; a seed node is -2 - its id
+        struct Local {
+            std::vector<BNode> nodes;
+            std::vector<const Step*> steps;
+            std::vector<int> term;                       // terminal (local id) of each plan of the chunk
+            std::vector<std::pair<int, int>> root_list;  // (seed node, first local child) in order seen
+        };
+        std::vector<Local> loc(T);
+        auto build = [&](unsigned t) {
+            Local& L = loc[t];
+            const size_t a0 = cut[t], a1 = cut[t + 1];
+            L.nodes.reserve(2 * (a1 - a0) + 16);
+            L.steps.reserve(2 * (a1 - a0) + 16);
+            L.term.resize(a1 - a0);
+            uint8_t ka[512], kc[512];
+            const std::vector<Step>* prv = nullptr;
+            std::vector<int> pp, cp;
+            for (size_t qi = a0; qi < a1; ++qi) {
+                const std::vector<Step>& st = steps[qi];
+                if (cp.size() < st.size()) cp.resize(st.size());
+                int cur = -2 - root_of[qi];
+                cp[0] = cur;
+                for (size_t i = 1; i < st.size(); ++i) {
+                    const bool up = prv && i < pp.size() && i < prv->size() && cur == pp[i - 1];
+                    int id = -1;
+                    if (up && memcmp(&st[i], &(*prv)[i], sizeof(Step)) == 0) {
+                        id = pp[i];
+                    } else if (up) {
+                        const size_t n = step_key_bytes(st[i], ka);
+                        if (step_key_bytes((*prv)[i], kc) == n && memcmp(ka, kc, n) == 0) id = pp[i];
+                    }
+                    if (id < 0) {
+                        id = (int)L.nodes.size();
+                        BNode nd;
+                        nd.kind = st[i].kind;
+                        nd.width_in = st[i].width_in;
+                        nd.n_eq = st[i].n_eq;
+                        nd.n_pairs = st[i].n_pairs;
+                        nd.always_empty = st[i].always_empty;
+                        nd.fused = fused_class(st[i].kind, st[i].n_chk) ? 1u : 0u;
+                        nd.depth = (int)i;
+                        nd.parent = cur;
+                        if (cur >= 0) {
+                            nd.next_sibling = L.nodes[cur].first_child;
+                            L.nodes[cur].first_child = id;
+                        } else {  // child of a seed node: chained per seed node, spliced in on merge
+                            const int r = -2 - cur;
+                            if (L.root_list.empty() || L.root_list.back().first != r) L.root_list.push_back({r, -1});
+                            nd.next_sibling = L.root_list.back().second;
+                            L.root_list.back().second = id;
+                        }
+                        L.nodes.push_back(nd);
+                        L.steps.push_back(&st[i]);
+                    }
+                    cur = id;
+                    cp[i] = cur;
+                }
+                prv = &st;
+                pp.assign(cp.begin(), cp.begin() + st.size());
+                const int q = q0 + (int)qi;
+                L.term[qi - a0] = cur;
+                plans[q].next_term = L.nodes[cur].first_term;
+                L.nodes[cur].first_term = q;
+            }
+        };
+        {
+            std::vector<std::thread> pool;
+            for (unsigned t = 1; t < T; ++t) pool.emplace_back(build, t);
+            build(0);
+            for (auto& th : pool) th.join();
+        }
+        std::vector<size_t> off(T + 1, (size_t)first_chunk_node);
+        for (unsigned t = 0; t < T; ++t) off[t + 1] = off[t] + loc[t].nodes.size();
+        nodes.resize(off[T]);
+        node_steps.resize(off[T]);
+        auto place = [&](unsigned t) {
+            const int o = (int)off[t];
+            Local& L = loc[t];
+            for (size_t j = 0; j < L.nodes.size(); ++j) {
+                BNode nd = L.nodes[j];
+                nd.parent = nd.parent >= 0 ? nd.parent + o : -2 - nd.parent;
+                if (nd.first_child >= 0) nd.first_child += o;
+                if (nd.next_sibling >= 0) nd.next_sibling += o;
+                nodes[off[t] + j] = nd;
+                node_steps[off[t] + j] = L.steps[j];
+            }
+            for (size_t qi = cut[t]; qi < cut[t + 1]; ++qi) plans[q0 + (int)qi].terminal = L.term[qi - cut[t]] + o;
+        };
+        {
+            std::vector<std::thread> pool;
+            for (unsigned t = 1; t < T; ++t) pool.emplace_back(place, t);
+            place(0);
+            for (auto& th : pool) th.join();
+        }
+        // children of seed nodes: each chunk's chain joins its seed node's list
+        for (unsigned t = 0; t < T; ++t)
+            for (const auto& rl : loc[t].root_list) {
+                if (rl.second < 0) continue;
+                int last = rl.second + (int)off[t];
+                while (nodes[last].next_sibling >= 0) last = nodes[last].next_sibling;
+                nodes[last].next_sibling = nodes[rl.first].first_child;
+                nodes[rl.first].first_child = rl.second + (int)off[t];
+            }
+    } else {
     const std::vector<Step>* prev = nullptr;
     std::vector<int> prev_path, path;
     for (size_t qi = 0; qi < steps.size(); ++qi) {
@@ -951,6 +1146,25 @@ int BatchSession::submit(std::vector<std::vector<Step>>&& wave, const std::vecto
         plans[q].terminal = cur;
         plans[q].next_term = nodes[cur].first_term;
         nodes[cur].first_term = q;
+    }
+    }
+    // the new nodes' descriptors, on the host's cores, into pinned staging
+    // that the next round ships
+    {
+        const size_t nn = nodes.size();
+        // host memory only (no device call), so tries are built without a device;
+        // only descriptors not yet shipped are kept
+        if (desc_host.size() < (nn - shipped) * sizeof(TaskDesc)) desc_host.resize((nn - shipped) * sizeof(TaskDesc));
+        const size_t nnew = nn - (size_t)first_node;
+        const unsigned T = nnew >= 8192 ? hw : 1u;
+        auto fill = [&](unsigned t) {
+            for (size_t id = (size_t)first_node + t; id < nn; id += T)
+                fill_node_desc((int)id, desc_host.data() + (id - shipped) * sizeof(TaskDesc));
+        };
+        std::vector<std::thread> pool;
+        for (unsigned t = 1; t < T; ++t) pool.emplace_back(fill, t);
+        fill(0);
+        for (auto& th : pool) th.join();
     }
     // seeds: the children of every seed node start from its vertex list
     for (int id = first_node; id < (int)nodes.size(); ++id) {
@@ -1024,20 +1238,18 @@ int BatchSession::round() {
     uint32_t kmax = 1;
     for (int t = 0; t < nt; ++t) kmax = std::max(kmax, nodes[active[t].node].width_in);
     uint32_t R = std::min<uint32_t>(tune.rows_per_item, std::max<uint32_t>(32, (1024 / kmax) & ~31u));
-    // staging: refs[nt] | new node descriptors (<= nt) | item0[nt+1] | totals[nt] | outs[nt] | wtask[nt] | witem0[nt+1]
+    // staging: refs[nt] | item0[nt+1] | totals[nt] | outs[nt] | queue heads | wtask[nt] | witem0[nt+1]
     const size_t ref_bytes = (size_t)nt * sizeof(TaskRef);
-    const size_t desc_max = (size_t)nt * sizeof(TaskDesc);
+    const size_t desc_max = 0;
     const size_t small_words = (size_t)(nt + 1) + nt + nt + 4 + nt + (nt + 1);
     char* h = staging.get(ref_bytes + desc_max + small_words * 8);
     if (!h) return fail(GVA_ERR_NOMEM, "pinned staging allocation failed");
     TaskRef* refs = (TaskRef*)h;
-    char* new_desc = h + ref_bytes;
     uint64_t* h_item0 = (uint64_t*)(h + ref_bytes + desc_max);
     uint64_t* h_totals = h_item0 + (nt + 1);
     uint32_t** h_outs = (uint32_t**)(h_totals + nt);
     uint64_t* h_wtask = h_totals + 2 * nt + 4;  // nt 8-byte words holding uint32 task indices
     uint64_t* h_witem0 = h_wtask + nt;
-    const int dev_first = dev_count;
     double cbytes = 0, crows = 0;
     uint64_t ni = 0, ni_light = 0;
     h_item0[0] = 0;
@@ -1045,11 +1257,7 @@ int BatchSession::round() {
         const BTask& tk = active[t];
         BNode& nd = nodes[tk.node];
         if (!nd.fused) ni_light = ni + (tk.rows + R - 1) / R;
-        if (nd.dev < 0) {  // first task of this node: ship its parameters
-            nd.dev = dev_count++;
-            fill_node_desc(tk.node, new_desc + (size_t)(nd.dev - dev_first) * sizeof(TaskDesc));
-        }
-        refs[t] = TaskRef{(uint32_t)nd.dev, 0u, tk.in, tk.rows};
+        refs[t] = TaskRef{(uint32_t)tk.node, 0u, tk.in, tk.rows};
         ni += (tk.rows + R - 1) / R;
         h_item0[t + 1] = ni;
         cbytes += (4.0 * nd.width_in + 8.0 * (nd.kind == STEP_EXT ? 1 : nd.n_pairs)) * (double)tk.rows;
@@ -1069,13 +1277,13 @@ int BatchSession::round() {
         cap = c;
         return true;
     };
-    const size_t dev_need = (size_t)dev_count * sizeof(TaskDesc);
+    const size_t dev_need = nodes.size() * sizeof(TaskDesc);
     if (dev_need > node_cap) {  // keep the descriptors already shipped
         void* p = nullptr;
         const size_t cap = std::max(dev_need, node_cap * 2);
         if (cudaMallocAsync(&p, cap, s) != cudaSuccess) return fail(GVA_ERR_NOMEM, "node descriptor allocation failed");
-        if (d_nodes && dev_first > 0)
-            GVA_CUDA_B(cudaMemcpyAsync(p, d_nodes, (size_t)dev_first * sizeof(TaskDesc), cudaMemcpyDeviceToDevice, s));
+        if (d_nodes && shipped > 0)
+            GVA_CUDA_B(cudaMemcpyAsync(p, d_nodes, shipped * sizeof(TaskDesc), cudaMemcpyDeviceToDevice, s));
         if (d_nodes) cudaFreeAsync(d_nodes, s);
         d_nodes = p;
         node_cap = cap;
@@ -1091,9 +1299,13 @@ int BatchSession::round() {
     unsigned long long* d_queue = (unsigned long long*)(d_totals + 2 * nt);  // four heads: count and write, per class
     uint64_t* d_wtask = d_totals + 2 * nt + 4;
     uint64_t* d_witem0 = d_wtask + nt;
-    if (dev_count > dev_first)
-        GVA_CUDA_B(cudaMemcpyAsync((char*)d_nodes + (size_t)dev_first * sizeof(TaskDesc), new_desc,
-                                   (size_t)(dev_count - dev_first) * sizeof(TaskDesc), cudaMemcpyHostToDevice, s));
+    if (shipped < nodes.size()) {  // descriptors of the nodes submitted since the last round
+        // a pageable source: the copy is complete when the call returns, so
+        // the next wave may refill the buffer
+        GVA_CUDA_B(cudaMemcpyAsync((char*)d_nodes + shipped * sizeof(TaskDesc), desc_host.data(),
+                                   (nodes.size() - shipped) * sizeof(TaskDesc), cudaMemcpyHostToDevice, s));
+        shipped = nodes.size();
+    }
     GVA_CUDA_B(cudaMemcpyAsync(d_desc, refs, ref_bytes, cudaMemcpyHostToDevice, s));
     GVA_CUDA_B(cudaMemcpyAsync(d_item0, h_item0, (nt + 1) * 8, cudaMemcpyHostToDevice, s));
     GVA_CUDA_B(cudaMemsetAsync(d_queue, 0, 32, s));

@@ -128,7 +128,6 @@ public:
         int first_child = -1, next_sibling = -1;  // children as a linked list
         int first_term = -1;                       // plans ending here, linked through PlanRec::next_term
         int at = 0;                                // active tasks at this node
-        int dev = -1;                              // index of its descriptor on the device
         bool closed = false;
     };
     struct BTask {
@@ -219,9 +218,10 @@ private:
     std::vector<int> completed;
     Staging staging;
     cudaEvent_t staged = nullptr;  // marks the last copies out of `staging`
-    void* d_nodes = nullptr;       // per-node step descriptors (layout private to gva_batch.cu)
+    void* d_nodes = nullptr;       // per-node step descriptors (layout private to gva_batch.cu), by node id
     size_t node_cap = 0;
-    int dev_count = 0;
+    size_t shipped = 0;            // nodes whose descriptors are on the device
+    std::vector<unsigned char> desc_host;  // descriptors filled at submit, shipped by the next round
     std::vector<int> scratch_order;
     std::vector<char> scratch_flag;
     std::vector<uint64_t> scratch_off;
