@@ -194,6 +194,38 @@ __device__ __forceinline__ void stage_rows(uint32_t* rows_s, const uint32_t* __r
     __syncwarp();
 }
 
+// cp.async (sm_80+ asynchronous global -> shared copies): a warp issues the
+// next item's rows while it works on the current one.
+__device__ __forceinline__ void cp_async4(void* smem, const void* gmem) {
+    const uint32_t sa = (uint32_t)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+    const uint32_t sa = (uint32_t)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_one() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
+
+// Issues, without waiting, the copy of rows [row0, row0 + nr) of width k
+// into rows_s (16-byte copies when the slice is 16-byte aligned); each lane
+// commits one group.
+__device__ __forceinline__ void stage_rows_async(uint32_t* rows_s, const uint32_t* __restrict__ in, uint64_t row0,
+                                                 uint32_t nr, uint32_t k) {
+    const int lane = threadIdx.x & 31;
+    const uint32_t* src = in + row0 * k;
+    const uint32_t nw = nr * k;
+    uint32_t w0 = 0;
+    if ((((uintptr_t)src | (uintptr_t)rows_s) & 15) == 0) {
+        const uint32_t nv = nw >> 2;
+        for (uint32_t v = lane; v < nv; v += 32) cp_async16(rows_s + 4 * v, src + 4 * v);
+        w0 = nv << 2;
+    }
+    for (uint32_t w = w0 + lane; w < nw; w += 32) cp_async4(rows_s + w, src + w);
+    cp_async_commit();
+}
+
 // Candidate test of the plain extension (no fused checks): injectivity only;
 // the restriction bound is already applied to the range.
 __device__ __forceinline__ bool ext_injective(const ExtArgs& p, const uint32_t* row, uint32_t c) {
@@ -373,17 +405,23 @@ __host__ __device__ __forceinline__ bool fused_class(uint32_t kind, uint32_t n_c
 // and (fused class) the lanes' generator states; before them, one descriptor
 // copy per warp.
 constexpr size_t kGenBytes = 32 * sizeof(GenState);  // per warp
-__host__ __device__ constexpr size_t round_warp_words(uint32_t rows_per_item, uint32_t kmax, bool write) {
-    return (((size_t)rows_per_item * kmax + (write ? (size_t)kTileRows * (kmax + 1) : 0)) + 3) & ~(size_t)3;
+// The light class double-buffers the item rows (the next item's rows are
+// copied in while the current item is worked on); the fused class, whose
+// generator states already take shared memory, stages one item at a time.
+__host__ __device__ constexpr uint32_t row_buffers(bool fused) { return fused ? 1u : 2u; }
+__host__ __device__ constexpr size_t round_warp_words(uint32_t rows_per_item, uint32_t kmax, bool write, bool fused) {
+    return (((size_t)row_buffers(fused) * rows_per_item * kmax + (write ? (size_t)kTileRows * (kmax + 1) : 0)) + 3) &
+           ~(size_t)3;
 }
 size_t round_smem_bytes(uint32_t rows_per_item, uint32_t kmax, bool write, bool fused) {
     return (size_t)kRoundWarps *
-           (sizeof(TaskDesc) + (fused ? kGenBytes : 0) + 4 * round_warp_words(rows_per_item, kmax, write));
+           (sizeof(TaskDesc) + (fused ? kGenBytes : 0) + 4 * round_warp_words(rows_per_item, kmax, write, fused));
 }
 
 struct WarpSmem {
     TaskDesc* d;
-    uint32_t* rows;
+    uint32_t* rows;   // one or two buffers of rows_per_item * kmax words
+    uint32_t* rows2;  // the second buffer (light class)
     uint32_t* tile;
     GenState* gen;
 };
@@ -395,8 +433,9 @@ __device__ __forceinline__ WarpSmem warp_smem(unsigned char* raw, const RoundArg
     unsigned char* area = raw + kRoundWarps * sizeof(TaskDesc);  // 8-byte aligned: TaskDesc holds pointers
     w.gen = FUSED ? reinterpret_cast<GenState*>(area) + 32 * warp : nullptr;
     uint32_t* words = reinterpret_cast<uint32_t*>(area + (FUSED ? kRoundWarps * kGenBytes : 0));
-    w.rows = words + warp * round_warp_words(a.rows_per_item, a.kmax, WRITE);
-    w.tile = w.rows + (size_t)a.rows_per_item * a.kmax;
+    w.rows = words + warp * round_warp_words(a.rows_per_item, a.kmax, WRITE, FUSED);
+    w.rows2 = w.rows + (size_t)(row_buffers(FUSED) - 1) * a.rows_per_item * a.kmax;
+    w.tile = w.rows + (size_t)row_buffers(FUSED) * a.rows_per_item * a.kmax;
     return w;
 }
 
@@ -416,6 +455,8 @@ round_count_kernel(RoundArgs a) {
     const uint32_t* in = nullptr;
     uint64_t nrows = 0;
     uint64_t begin, end;
+    uint32_t cur = 0;    // light class: buffer of the current item
+    bool ready = false;  // light class: the current item's rows were issued with the previous item
     while (next_chunk(a, begin, end)) {
         for (uint64_t item = a.item_base + begin; item < a.item_base + end; ++item) {
             if (item >= t_hi || item < t_lo) {
@@ -431,16 +472,37 @@ round_count_kernel(RoundArgs a) {
             const uint64_t row0 = (item - t_lo) * a.rows_per_item;
             const uint32_t nr = (uint32_t)umin64(a.rows_per_item, nrows - row0);
             const uint32_t k = d.kind == STEP_EXT ? d.e.k : d.r.k;
-            __syncwarp();
-            stage_rows(ws.rows, in, row0, nr, k);
+            uint32_t* rows = ws.rows;
+            if (FUSED) {
+                __syncwarp();
+                stage_rows(rows, in, row0, nr, k);
+            } else {
+                rows = cur ? ws.rows2 : ws.rows;
+                if (!ready) {
+                    __syncwarp();
+                    stage_rows_async(rows, in, row0, nr, k);
+                }
+                // the next item of the same task and chunk: its rows are copied in meanwhile
+                ready = item + 1 < a.item_base + end && item + 1 < t_hi;
+                if (ready) {
+                    const uint64_t r1 = row0 + a.rows_per_item;
+                    stage_rows_async(cur ? ws.rows : ws.rows2, in, r1, (uint32_t)umin64(a.rows_per_item, nrows - r1), k);
+                    cp_async_wait_one();
+                } else {
+                    cp_async_wait_all();
+                }
+                __syncwarp();
+                cur ^= 1;
+            }
             uint64_t c;
             if (FUSED)
-                c = ext_item<false, true>(d, ws.rows, nr, a.hub, a.ctx, nullptr, ws.gen, a.read_words);
+                c = ext_item<false, true>(d, rows, nr, a.hub, a.ctx, nullptr, ws.gen, a.read_words);
             else if (d.kind == STEP_EXT)
-                c = ext_item<false, false>(d, ws.rows, nr, a.hub, a.ctx, nullptr, nullptr, a.read_words);
+                c = ext_item<false, false>(d, rows, nr, a.hub, a.ctx, nullptr, nullptr, a.read_words);
             else
-                c = red_item<false>(d, ws.rows, nr, a.ctx, nullptr);
+                c = red_item<false>(d, rows, nr, a.ctx, nullptr);
             if (lane == 0) a.items[item] = c;
+            __syncwarp();  // every lane done with these rows before the buffer is refilled
         }
     }
 }
@@ -550,6 +612,8 @@ round_write_kernel(RoundArgs a) {
     const uint32_t* in = nullptr;
     uint64_t nrows = 0;
     uint64_t begin, end;
+    uint32_t cur = 0;    // light class: buffer of the current item
+    bool ready = false;  // light class: the current item's rows were issued with the previous item
     while (next_chunk(a, begin, end)) {
         for (uint64_t wi = a.item_base + begin; wi < a.item_base + end; ++wi) {
             if (wi >= w_hi || wi < w_lo) {
@@ -571,26 +635,53 @@ round_write_kernel(RoundArgs a) {
             const uint64_t off_next = item + 1 >= a.n_count_items
                                           ? a.chunks[a.n_chunks]
                                           : a.items[item + 1] + a.chunks[(item + 1) >> kScanChunkLog2];
-            if (off_next == off) continue;  // nothing accepted in this item
             const uint64_t row0 = (wi - w_lo) * a.rows_per_item;
             const uint32_t nr = (uint32_t)umin64(a.rows_per_item, nrows - row0);
             const bool ext = d.kind == STEP_EXT;
             const uint32_t k = ext ? d.e.k : d.r.k;
+            if (off_next == off) {  // nothing accepted in this item
+                if (!FUSED && ready) {  // its rows were issued already: let them land before the buffer is reused
+                    cp_async_wait_all();
+                    __syncwarp();
+                    ready = false;
+                }
+                continue;
+            }
+            uint32_t* rows = ws.rows;
+            if (FUSED) {
+                __syncwarp();
+                stage_rows(rows, in, row0, nr, k);
+            } else {
+                rows = cur ? ws.rows2 : ws.rows;
+                if (!ready) {
+                    __syncwarp();
+                    stage_rows_async(rows, in, row0, nr, k);
+                }
+                ready = wi + 1 < a.item_base + end && wi + 1 < w_hi;
+                if (ready) {
+                    const uint64_t r1 = row0 + a.rows_per_item;
+                    stage_rows_async(cur ? ws.rows : ws.rows2, in, r1, (uint32_t)umin64(a.rows_per_item, nrows - r1), k);
+                    cp_async_wait_one();
+                } else {
+                    cp_async_wait_all();
+                }
+                __syncwarp();
+                cur ^= 1;
+            }
             Tile tl;
             tl.t = ws.tile;
             tl.w = ext ? k + 1 : k;
             tl.n = 0;
             tl.out = out + (off - t_off0) * tl.w;
             tl.room = off_next - off;
-            __syncwarp();
-            stage_rows(ws.rows, in, row0, nr, k);
             if (FUSED)
-                ext_item<true, true>(d, ws.rows, nr, a.hub, a.ctx, &tl, ws.gen, nullptr);
+                ext_item<true, true>(d, rows, nr, a.hub, a.ctx, &tl, ws.gen, nullptr);
             else if (ext)
-                ext_item<true, false>(d, ws.rows, nr, a.hub, a.ctx, &tl, nullptr, nullptr);
+                ext_item<true, false>(d, rows, nr, a.hub, a.ctx, &tl, nullptr, nullptr);
             else
-                red_item<true>(d, ws.rows, nr, a.ctx, &tl);
+                red_item<true>(d, rows, nr, a.ctx, &tl);
             if (tl.n) tile_flush(tl, tl.n);
+            __syncwarp();  // every lane done with these rows before the buffer is refilled
         }
     }
 }
@@ -717,7 +808,8 @@ int BatchSession::init() {
     static std::atomic<bool> smem_set[64];  // sessions may start on several threads (server, miner)
     if (dev < 0 || dev >= 64) return fail(GVA_ERR_ARG, "device index out of range");
     if (!smem_set[dev].load(std::memory_order_acquire)) {
-        const int most = (int)round_smem_bytes(kMaxItemRows / 4, kMaxCols, true, true);  // rows per item shrink as rows widen
+        const int most = (int)std::max(round_smem_bytes(kMaxItemRows / 4, kMaxCols, true, true),
+                                       round_smem_bytes(kMaxItemRows / 4, kMaxCols, true, false));  // rows per item shrink as rows widen
         GVA_CUDA_B(cudaFuncSetAttribute(round_count_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, most));
         GVA_CUDA_B(cudaFuncSetAttribute(round_count_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, most));
         GVA_CUDA_B(cudaFuncSetAttribute(round_write_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, most));
@@ -808,7 +900,7 @@ void BatchSession::fill_node_desc(int id, void* out) const {
         a.off = P.off;
         a.adj = P.adj;
         a.k = st.width_in;
-        a.L = db.L;
+        a.L = db.kernel_L();
         a.lab = st.label;
         a.src_col = st.src_col;
         a.bound_col = st.bound_col;
@@ -829,7 +921,7 @@ void BatchSession::fill_node_desc(int id, void* out) const {
         a.off = P.off;
         a.adj = P.adj;
         a.k = st.width_in;
-        a.L = db.L;
+        a.L = db.kernel_L();
         a.n_pairs = st.n_pairs;
         for (uint32_t i = 0; i < st.n_pairs; ++i) {
             a.rs[i] = st.rs_col[i];
@@ -1237,7 +1329,7 @@ int BatchSession::round() {
     // of the round sets the shared-memory layout), a multiple of 32
     uint32_t kmax = 1;
     for (int t = 0; t < nt; ++t) kmax = std::max(kmax, nodes[active[t].node].width_in);
-    uint32_t R = std::min<uint32_t>(tune.rows_per_item, std::max<uint32_t>(32, (1024 / kmax) & ~31u));
+    uint32_t R = std::min<uint32_t>(tune.rows_per_item, std::max<uint32_t>(32, (768 / kmax) & ~31u));
     // staging: refs[nt] | item0[nt+1] | totals[nt] | outs[nt] | queue heads | wtask[nt] | witem0[nt+1]
     const size_t ref_bytes = (size_t)nt * sizeof(TaskRef);
     const size_t desc_max = 0;

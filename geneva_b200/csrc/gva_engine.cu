@@ -188,7 +188,7 @@ void fill_ext(ExtArgs& a, const DevDB& db, const Step& st, const uint32_t* in, u
     a.off = P.off;
     a.adj = P.adj;
     a.k = st.width_in;
-    a.L = db.L;
+    a.L = db.kernel_L();
     a.lab = st.label;
     a.src_col = st.src_col;
     a.bound_col = st.bound_col;
@@ -206,7 +206,7 @@ void fill_red(RedArgs& a, const DevDB& db, const Step& st, const uint32_t* in, u
     a.off = P.off;
     a.adj = P.adj;
     a.k = st.width_in;
-    a.L = db.L;
+    a.L = db.kernel_L();
     a.n_pairs = st.n_pairs;
     for (uint32_t i = 0; i < st.n_pairs; ++i) {
         a.rs[i] = st.rs_col[i];
@@ -360,8 +360,45 @@ int upload_graph(HostGraph& g, int device, DevDB*& out) {
     // the vertices most likely to succeed first
     std::vector<uint32_t> seed_off, seed_verts, seed_deg;
     seed_groups(g, seed_off, seed_verts, seed_deg);
+    // segment index per partition: packed 32-byte vertex records when the
+    // label count allows (seg_of), else the dense (vertex, label) table
+    bool packed = L >= 1 && L <= 28;
+    for (auto& p : g.parts)
+        if (!p.off.empty() && p.adj.size() >= 0x80000000ull) packed = false;
+    std::vector<std::vector<uint32_t>> pidx(g.parts.size());
+    if (packed) {
+        const uint64_t nv = (uint64_t)g.max_id + 1;
+        for (size_t i = 0; i < g.parts.size(); ++i) {
+            const HostPartition& hp = g.parts[i];
+            if (hp.off.empty()) continue;
+            std::vector<uint32_t>& rec = pidx[i];
+            rec.assign(nv * 8, 0);
+            std::vector<uint32_t> wide;
+            for (uint64_t v = 0; v < nv; ++v) {
+                const uint32_t* o = hp.off.data() + v * L;
+                const uint32_t base = o[0];
+                uint32_t* r = rec.data() + v * 8;
+                if (o[L] - base > 255) {
+                    r[0] = base | 0x80000000u;
+                    r[1] = (uint32_t)(nv * 8 + wide.size());
+                    for (uint32_t j = 0; j <= L; ++j) wide.push_back(o[j] - base);
+                } else {
+                    r[0] = base;
+                    unsigned char* b = reinterpret_cast<unsigned char*>(r);
+                    for (uint32_t j = 1; j <= L; ++j) b[3 + j] = (unsigned char)(o[j] - base);
+                }
+            }
+            if (nv * 8 + wide.size() >= 0x80000000ull) {
+                packed = false;
+                break;
+            }
+            rec.insert(rec.end(), wide.begin(), wide.end());
+        }
+        if (!packed) pidx.assign(g.parts.size(), {});
+    }
     size_t bytes = 2 * align256(seed_verts.size() * 4 + 4);
-    for (auto& p : g.parts) bytes += align256(p.off.size() * 4) + align256(p.adj.size() * 4 + 4);
+    for (size_t i = 0; i < g.parts.size(); ++i)
+        bytes += align256((packed ? pidx[i].size() : g.parts[i].off.size()) * 4) + align256(g.parts[i].adj.size() * 4 + 4);
     void* arena = nullptr;
     cudaError_t e = cudaMalloc(&arena, bytes);
     if (e != cudaSuccess) return fail(GVA_ERR_NOMEM, std::string("database allocation failed: ") + cudaGetErrorString(e));
@@ -369,6 +406,7 @@ int upload_graph(HostGraph& g, int device, DevDB*& out) {
     db->device = device;
     db->max_id = g.max_id;
     db->L = L;
+    db->packed = packed;
     db->labels = g.labels;
     db->seed_off = seed_off;
     db->arena = arena;
@@ -387,8 +425,13 @@ int upload_graph(HostGraph& g, int device, DevDB*& out) {
         HostPartition& hp = g.parts[i];
         if (hp.off.empty()) continue;
         const uint32_t* off = (const uint32_t*)cur;
-        cudaMemcpy(cur, hp.off.data(), hp.off.size() * 4, cudaMemcpyHostToDevice);
-        cur += align256(hp.off.size() * 4);
+        if (packed) {
+            cudaMemcpy(cur, pidx[i].data(), pidx[i].size() * 4, cudaMemcpyHostToDevice);
+            cur += align256(pidx[i].size() * 4);
+        } else {
+            cudaMemcpy(cur, hp.off.data(), hp.off.size() * 4, cudaMemcpyHostToDevice);
+            cur += align256(hp.off.size() * 4);
+        }
         db->parts[i].off = off;
         db->parts[i].adj = put(hp.adj);
         db->parts[i].n_adj = hp.adj.size();

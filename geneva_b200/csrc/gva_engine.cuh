@@ -25,6 +25,8 @@ struct DevDB {
     int device = 0;
     uint32_t max_id = 0;
     uint32_t L = 0;                       // dense vertex labels
+    bool packed = false;                  // segment index layout (seg_of): packed records, else dense
+    uint32_t kernel_L() const { return L | (packed ? kPackedSeg : 0u); }  // the label count kernels take
     std::vector<uint32_t> labels;         // dense -> original label
     std::vector<DevPart> parts;           // parts[p - 1] = edge label p (off == nullptr: absent)
     std::vector<uint32_t> seed_off;       // host copy of seed_off

@@ -11,6 +11,9 @@
 namespace gva {
 
 constexpr uint32_t kNone = 0xffffffffu;
+// bit of the label count handed to kernels that marks a packed segment index
+// (seg_of in gva_kernels.cuh)
+constexpr uint32_t kPackedSeg = 0x80000000u;
 constexpr int kMaxCols = 32;
 
 // ---------------------------------------------------------------- errors ----

@@ -59,6 +59,48 @@ struct RedArgs {
 
 __device__ __forceinline__ uint64_t umin64(uint64_t a, uint64_t b) { return a < b ? a : b; }
 
+// Label segment [lo, hi) of (vertex v, dense label l) in one partition's
+// segment index.  Two layouts, chosen per database; bit 31 of L (kPackedSeg)
+// marks the packed one:
+//   dense   off[v * L + l] .. off[v * L + l + 1], (V + 1) * L + 1 words;
+//   packed  one 32-byte record per vertex (one sector): word 0 = where v's
+//           list starts in adj, bytes 4 .. 3 + L = cum[1 .. L], cum[j] = v's
+//           neighbours with a label below j (cum[0] = 0 is not stored); a
+//           vertex with more than 255 neighbours in the partition has bit 31
+//           of word 0 set and word 1 = the word index, from `off`, of its
+//           L + 1 uint32 cumulative counts.  For L <= 28.
+// The packed index of a 20,000-graph database with 16 labels takes half the
+// bytes of the dense one and every lookup is one sector, so the index of all
+// partitions stays in L2 beside the frontiers.
+__device__ __forceinline__ void seg_of(const uint32_t* __restrict__ off, uint32_t L, uint32_t v, uint32_t l,
+                                       uint32_t& lo, uint32_t& hi) {
+    if (!(L & kPackedSeg)) {
+        const uint64_t t = (uint64_t)v * L + l;
+        lo = __ldg(off + t);
+        hi = __ldg(off + t + 1);
+        return;
+    }
+    const uint32_t* rec = off + (uint64_t)v * 8;
+    const uint32_t w0 = __ldg(rec);
+    const uint32_t base = w0 & 0x7fffffffu;
+    if (w0 & 0x80000000u) {  // more than 255 neighbours: a row of cumulative words
+        const uint32_t* cw = off + __ldg(rec + 1);
+        lo = base + __ldg(cw + l);
+        hi = base + __ldg(cw + l + 1);
+        return;
+    }
+    const uint32_t bh = 4 + l;  // byte of cum[l + 1]
+    const uint32_t wh = __ldg(rec + (bh >> 2));
+    hi = base + ((wh >> (8 * (bh & 3))) & 0xffu);
+    uint32_t c = 0;
+    if (l > 0) {
+        const uint32_t bl = 3 + l;  // byte of cum[l]
+        const uint32_t wl = (bl >> 2) == (bh >> 2) ? wh : __ldg(rec + (bl >> 2));
+        c = (wl >> (8 * (bl & 3))) & 0xffu;
+    }
+    lo = base + c;
+}
+
 // first index in [lo, hi) with a[i] >= x (hi if none)
 __device__ __forceinline__ uint32_t lower_bound_u32(const uint32_t* __restrict__ a, uint32_t lo, uint32_t hi,
                                                     uint64_t x) {
@@ -75,10 +117,7 @@ __device__ __forceinline__ uint32_t lower_bound_u32(const uint32_t* __restrict__
 // Candidate range of one row: the (source, label) segment cut below the
 // restriction bound.
 __device__ __forceinline__ void ext_range(const ExtArgs& p, const uint32_t* row, uint32_t& lo, uint32_t& hi) {
-    const uint32_t s = row[p.src_col];
-    const uint64_t t = (uint64_t)s * p.L + p.lab;
-    lo = __ldg(p.off + t);
-    hi = __ldg(p.off + t + 1);
+    seg_of(p.off, p.L, row[p.src_col], p.lab, lo, hi);
     if (p.bound_col >= 0 && lo < hi) {
         const uint64_t b = (uint64_t)row[p.bound_col] + p.bound_incl;
         hi = lower_bound_u32(p.adj, lo, hi, b);
@@ -114,8 +153,8 @@ __device__ __forceinline__ void ext_generator(const ExtArgs& p, const uint32_t* 
     g.which = -1;
     for (uint32_t i = 0; i < p.n_chk && g.lo < g.hi; ++i) {
         if (p.chk_dir[i]) continue;
-        const uint64_t t = (uint64_t)row[p.chk_col[i]] * p.L + p.lab;
-        uint32_t l2 = __ldg(p.chk_off[i] + t), h2 = __ldg(p.chk_off[i] + t + 1);
+        uint32_t l2, h2;
+        seg_of(p.chk_off[i], p.L, row[p.chk_col[i]], p.lab, l2, h2);
         if (p.bound_col >= 0 && l2 < h2)
             h2 = lower_bound_u32(p.chk_adj[i], l2, h2, (uint64_t)row[p.bound_col] + p.bound_incl);
         g.clo[i] = l2;
@@ -131,8 +170,9 @@ __device__ __forceinline__ void ext_generator(const ExtArgs& p, const uint32_t* 
 
 __device__ __forceinline__ bool seg_has(const uint32_t* __restrict__ off, const uint32_t* __restrict__ adj, uint32_t L,
                                         uint32_t v, uint32_t lab, uint32_t w) {
-    const uint64_t t = (uint64_t)v * L + lab;
-    return find_in(adj, __ldg(off + t), __ldg(off + t + 1), w) != 0xffffffffu;
+    uint32_t lo, hi;
+    seg_of(off, L, v, lab, lo, hi);
+    return find_in(adj, lo, hi, w) != 0xffffffffu;
 }
 
 // Whether generated candidate c survives injectivity, the source edge (when
@@ -176,8 +216,8 @@ __device__ __forceinline__ bool red_keep_row(const RedArgs& p, const uint32_t* r
     for (uint32_t j = 0; j < p.n_pairs; ++j) {
         const uint32_t s = row[p.rs[j]];
         const uint32_t e = row[p.re[j]];
-        const uint64_t t = (uint64_t)s * p.L + p.rl[j];
-        const uint32_t lo = __ldg(p.off + t), hi = __ldg(p.off + t + 1);
+        uint32_t lo, hi;
+        seg_of(p.off, p.L, s, p.rl[j], lo, hi);
         if (find_in(p.adj, lo, hi, e) == 0xffffffffu) return false;
     }
     return true;

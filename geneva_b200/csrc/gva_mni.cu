@@ -108,8 +108,9 @@ __global__ void mni_expand_kernel(const uint64_t* __restrict__ item0, int nslots
 __device__ __forceinline__ bool root_ok(const MniTask& T, const PartPtr* __restrict__ parts, uint32_t L, uint32_t v) {
     for (uint32_t k = 0; k < T.n_rootf; ++k) {
         const PartPtr P = parts[T.root_part[k] - 1];
-        const uint64_t t = (uint64_t)v * L + T.root_lab[k];
-        if (__ldg(P.off + t + 1) - __ldg(P.off + t) < T.root_mult[k]) return false;
+        uint32_t lo, hi;
+        seg_of(P.off, L, v, T.root_lab[k], lo, hi);
+        if (hi - lo < T.root_mult[k]) return false;
     }
     return true;
 }
@@ -134,8 +135,8 @@ __device__ bool mni_dfs(const MniTask& T, const PartPtr* __restrict__ parts, uin
             const int j = __ffs(m) - 1;
             m &= m - 1;
             const PartPtr P = parts[T.part[lv][j] - 1];
-            const uint64_t t = (uint64_t)f[j] * L + T.lab[lv];
-            const uint32_t lo = __ldg(P.off + t), hi = __ldg(P.off + t + 1);
+            uint32_t lo, hi;
+            seg_of(P.off, L, f[j], T.lab[lv], lo, hi);
             if (!have || hi - lo < bhi - blo) {
                 blo = lo;
                 bhi = hi;
@@ -175,8 +176,9 @@ __device__ bool mni_dfs(const MniTask& T, const PartPtr* __restrict__ parts, uin
                 const int j = __ffs(m) - 1;
                 m &= m - 1;
                 const PartPtr P = parts[T.part[i][j] - 1];
-                const uint64_t t = (uint64_t)f[j] * L + T.lab[i];
-                ok = find_in(P.adj, __ldg(P.off + t), __ldg(P.off + t + 1), c) != 0xffffffffu;
+                uint32_t lo, hi;
+                seg_of(P.off, L, f[j], T.lab[i], lo, hi);
+                ok = find_in(P.adj, lo, hi, c) != 0xffffffffu;
                 cnt[P_CHECKS] += 1;
             }
         }
@@ -217,8 +219,8 @@ __device__ int lane_dfs(const MniTask& T, const PartPtr* __restrict__ parts, uin
             const int j = __ffs(m) - 1;
             m &= m - 1;
             const PartPtr P = parts[T.part[lv][j] - 1];
-            const uint64_t t = (uint64_t)f[j] * L + T.lab[lv];
-            const uint32_t lo = __ldg(P.off + t), hi = __ldg(P.off + t + 1);
+            uint32_t lo, hi;
+            seg_of(P.off, L, f[j], T.lab[lv], lo, hi);
             if (!have || hi - lo < bhi - blo) {
                 blo = lo;
                 bhi = hi;
@@ -257,8 +259,9 @@ __device__ int lane_dfs(const MniTask& T, const PartPtr* __restrict__ parts, uin
             const int j = __ffs(m) - 1;
             m &= m - 1;
             const PartPtr P = parts[T.part[i][j] - 1];
-            const uint64_t t = (uint64_t)f[j] * L + T.lab[i];
-            ok = find_in(P.adj, __ldg(P.off + t), __ldg(P.off + t + 1), c) != 0xffffffffu;
+            uint32_t lo, hi;
+            seg_of(P.off, L, f[j], T.lab[i], lo, hi);
+            ok = find_in(P.adj, lo, hi, c) != 0xffffffffu;
             cnt[P_CHECKS] += 1;
         }
         if (!ok) continue;
@@ -716,7 +719,7 @@ int mni_run_prepared(DevDB& db, const MniPrepared& prep, uint32_t cap, bool plai
                                                                                                   d_item_slot);
             if (profile) prof.begin(K_MNI, 0.0, s, ev);
             mni_search_kernel<<<(unsigned)std::max<uint64_t>(grid, 1), kMniWarps * 32, 0, s>>>(
-                d_tasks, d_slots, d_item0, d_item_slot, nitems, db.seed_by_degree, (uint32_t)item_len, d_parts, db.L,
+                d_tasks, d_slots, d_item0, d_item_slot, nitems, db.seed_by_degree, (uint32_t)item_len, d_parts, db.kernel_L(),
                 d_counts, d_queue,
                 profile ? d_prof : nullptr);
             if (profile) prof.end(ev, K_MNI, 0.0, s, rows);

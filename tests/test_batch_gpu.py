@@ -128,3 +128,44 @@ def test_autotune_keeps_a_valid_shape(small_db, oracle):
     counts, _, _ = gv.batch_count(gdb, plans)
     want, _, _ = oracle.many_graph_counts(og, pats, db.first)
     assert np.array_equal(counts, want)
+
+
+def test_hub_vertices_of_the_packed_segment_index(native, oracle):
+    """Vertices with more than 255 neighbours in a partition take the packed
+    index's wide records (a row of cumulative words instead of bytes): a
+    graph with a few such hubs, matched through the batched and the plain
+    path, against the oracle (counts per graph, supports, rows)."""
+    rng = np.random.default_rng(5)
+    V = 3000
+    vl = np.zeros(V + 1, dtype=np.uint32)
+    vl[1:] = rng.integers(1, 6, size=V)
+    edges = set()
+    for hub in (1, 2, 3):
+        for w in rng.choice(np.arange(4, V + 1), size=700, replace=False):
+            edges.add((hub, int(w), 1 + (int(w) % 2)))
+    while len(edges) < 2100 + 6000:
+        a, b = (int(x) for x in rng.integers(1, V + 1, size=2))
+        if a != b:
+            edges.add((min(a, b), max(a, b), int(rng.integers(1, 3))))
+    e = np.array(sorted(edges), dtype=np.uint32)
+    first = np.array([1, V + 1], dtype=np.int64)
+    gdb = gv.Database.from_edges(vl, e[:, 0], e[:, 1], e[:, 2])
+    gdb.set_graphs(first)
+    og = oracle.from_edges(vl, e[:, 0], e[:, 1], e[:, 2])
+    pats = ["v 0 %d\nv 1 %d\nv 2 %d\ne 0 1 1\ne 0 2 %d\n" % (int(vl[1]), a, b, el)
+            for a in (1, 3) for b in (2, 4) for el in (1, 2)]
+    pats += ["v 0 %d\nv 1 %d\nv 2 %d\nv 3 %d\ne 0 1 1\ne 1 2 2\ne 0 2 1\ne 2 3 %d\n" % (int(vl[2]), a, b, c, el)
+             for a in (1, 2) for b in (3, 5) for c in (1, 4) for el in (1, 2)]
+    pats = [p for p in pats if oracle.count(og, p, cap_rows=3_000_000) is not None]
+    assert len(pats) >= 10
+    plans = [gv.Plan.from_text(p) for p in pats]
+    counts, sup, _ = gv.batch_count(gdb, plans, support=True)
+    want, want_sup, _ = oracle.many_graph_counts(og, pats, first)
+    assert np.array_equal(counts, want) and np.array_equal(sup, want_sup)
+    from oracle_lib import rows_digest
+    for p, plan in list(zip(pats, plans))[:8]:
+        got = gv.match(gdb, plan).rows()
+        rows, _ = oracle.match(og, p)
+        assert rows_digest(got) == rows_digest(rows), p
+    oracle.free(og)
+    gdb.close()
