@@ -893,11 +893,8 @@ def batch_bench(args, rank, world, local, dist, torch, gv, workloads):
     t1 = time.perf_counter()
     e2e_emb = 0
     for _ in range(e2e_steps):
-        ps = gv.Plan.batch_from_texts(queries)
-        c, _, _ = gv.batch_count(gdb, ps, stream=sp, support=True)
+        c, _, _ = gv.batch_count_texts(gdb, queries, stream=sp, support=True)
         e2e_emb += int(c.sum())
-        for p in ps:
-            p.close()
     torch.cuda.synchronize()
     e2e_t = red(time.perf_counter() - t1, dist.ReduceOp.MAX if dist else None)
     e2e_value = red(e2e_emb, dist.ReduceOp.SUM if dist else None) / e2e_t
@@ -934,8 +931,8 @@ def batch_bench(args, rank, world, local, dist, torch, gv, workloads):
         "tuning": dict(tuning, calibration=f"first {min(args.tune_patterns, len(plans))} patterns of the list, "
                                            f"counted with supports, each launch shape twice (gva_db_autotune)"),
         "e2e": {"value": e2e_value, "unit": "embeddings/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-                "note": "pattern texts planned on the host's cores each step (gva_plan_batch), matched, counts and "
-                        "supports copied to host memory; database resident"},
+                "note": "pattern texts read, planned on the host's cores and matched in one call each step "
+                        "(gva_batch_count_texts), counts and supports copied to host memory; database resident"},
         "gpu_launches": launches,
         "clocks": clk,
     }

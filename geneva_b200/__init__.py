@@ -24,7 +24,7 @@ from typing import List, Optional, Sequence
 import numpy as np
 
 __all__ = [
-    "GenevaError", "Database", "probe_graph", "convert_g", "batch_count", "kernel_launches", "mine", "mine_host", "mni_support", "MinedPatterns", "MinedPattern", "Plan", "Result", "MODE_DV", "MODE_SV", "library", "library_path",
+    "GenevaError", "Database", "probe_graph", "convert_g", "batch_count", "batch_count_texts", "kernel_launches", "mine", "mine_host", "mni_support", "MinedPatterns", "MinedPattern", "Plan", "Result", "MODE_DV", "MODE_SV", "library", "library_path",
     "loadDataBase", "genMatchOrder", "genMatchOrderSingleV", "match", "gpumine", "gpumineSV",
 ]
 
@@ -94,9 +94,12 @@ class _MniOpts(ctypes.Structure):
                 ("profile", ctypes.c_int), ("reserved", ctypes.c_int)]
 
 
+BATCH_PLAN_ON_DEVICE = 1
+
+
 class _BatchOpts(ctypes.Structure):
     _fields_ = [("stream", ctypes.c_void_p), ("budget_bytes", ctypes.c_uint64), ("profile", ctypes.c_int),
-                ("reserved", ctypes.c_int)]
+                ("flags", ctypes.c_int)]
 
 
 class _Tuning(ctypes.Structure):
@@ -159,6 +162,8 @@ def _declare(lib):
         "gva_db_set_graphs": (i32, [vp, vp, u32]),
         "gva_convert_g": (i32, [cp, cp, cp, cp]),
         "gva_mine": (i32, [vp, P(_MineOpts), P(vp)]),
+        "gva_plan_batch_device": (i32, [i32, vp, i32, vp, vp]),
+        "gva_batch_count_texts": (i32, [vp, vp, i32, i32, P(_BatchOpts), vp, vp, vp, vp, P(_BatchStats)]),
         "gva_db_get_tuning": (i32, [vp, P(_Tuning)]),
         "gva_db_set_tuning": (i32, [vp, P(_Tuning)]),
         "gva_db_autotune": (i32, [vp, vp, i32, vp, P(_Tuning)]),
@@ -316,6 +321,25 @@ class Plan:
         return plans
 
     @classmethod
+    def batch_from_texts_device(cls, texts: Sequence[str], device: int = 0) -> List["Plan"]:
+        """DV plans of many queries computed by the device planner
+        (gva_plan_batch_device); the same plans as batch_from_texts."""
+        n = len(texts)
+        enc = (ctypes.c_char_p * max(n, 1))(*[t.encode() for t in texts])
+        out = (ctypes.c_void_p * max(n, 1))()
+        st = (ctypes.c_int * max(n, 1))()
+        rc = library().gva_plan_batch_device(device, ctypes.cast(enc, ctypes.c_void_p), n,
+                                             ctypes.cast(out, ctypes.c_void_p), ctypes.cast(st, ctypes.c_void_p))
+        plans = [cls(out[i]) if out[i] else None for i in range(n)]
+        if rc:
+            msg = library().gva_last_error().decode()
+            for p in plans:
+                if p is not None:
+                    p.close()
+            raise GenevaError(rc, msg)
+        return plans
+
+    @classmethod
     def from_file(cls, path: str, mode: int = MODE_DV) -> "Plan":
         h = ctypes.c_void_p()
         _check(library().gva_plan_from_file(str(path).encode(), mode, ctypes.byref(h)))
@@ -440,18 +464,47 @@ def batch_count(db: Database, plans: Sequence[Plan], stream: Optional[int] = Non
     _check(library().gva_batch_count(db._h, arr, n, ctypes.byref(o), counts.ctypes.data,
                                      gc.ctypes.data if gc is not None else None,
                                      sup.ctypes.data if sup is not None else None, ctypes.byref(st)))
-    stats = {"gpu_ms": st.gpu_ms, "rounds": int(st.rounds), "splits": int(st.splits), "launches": int(st.launches),
-             "trie_nodes": int(st.trie_nodes), "lower_ms": st.lower_ms, "submit_ms": st.submit_ms,
-             "round_host_ms": st.round_host_ms, "wait_ms": st.wait_ms, "session_ms": st.session_ms,
-             "round_phase_ms": [float(x) for x in st.round_phase_ms],
-             "kernels": {st.kernels[i].name.decode(): dict(launches=int(st.kernels[i].launches),
-                                                           ms=float(st.kernels[i].ms), bytes=float(st.kernels[i].bytes),
-                                                           rows=float(st.kernels[i].rows))
-                         for i in range(5)}}
     per_graph = gc if graph_counts else sup
     if graph_counts and support:
         per_graph = (gc, sup)
-    return counts, per_graph, stats
+    return counts, per_graph, _batch_stats_dict(st)
+
+
+def _batch_stats_dict(st) -> dict:
+    return {"gpu_ms": st.gpu_ms, "rounds": int(st.rounds), "splits": int(st.splits), "launches": int(st.launches),
+            "trie_nodes": int(st.trie_nodes), "lower_ms": st.lower_ms, "submit_ms": st.submit_ms,
+            "round_host_ms": st.round_host_ms, "wait_ms": st.wait_ms, "session_ms": st.session_ms,
+            "round_phase_ms": [float(x) for x in st.round_phase_ms],
+            "kernels": {st.kernels[i].name.decode(): dict(launches=int(st.kernels[i].launches),
+                                                          ms=float(st.kernels[i].ms), bytes=float(st.kernels[i].bytes),
+                                                          rows=float(st.kernels[i].rows))
+                        for i in range(5)}}
+
+
+def batch_count_texts(db: Database, texts: Sequence[str], mode: int = MODE_DV, stream: Optional[int] = None,
+                      budget_bytes: int = 0, graph_counts: bool = False, support: bool = False,
+                      profile: bool = False, plan_on_device: bool = False):
+    """Plans and counts query texts in one call (gva_batch_count_texts): no
+    plan handles; plan_on_device plans them with the device planner.
+    Returns (counts, per_graph, stats) as batch_count; a text that fails to
+    plan raises GenevaError after the others were counted."""
+    n = len(texts)
+    enc = [t.encode() for t in texts]
+    arr = (ctypes.c_char_p * max(n, 1))(*enc)
+    counts = np.zeros(n, dtype=np.uint64)
+    gc = np.zeros((n, db.num_graphs), dtype=np.uint64) if graph_counts else None
+    sup = np.zeros(n, dtype=np.uint32) if support else None
+    status = np.zeros(max(n, 1), dtype=np.int32)
+    o = _BatchOpts(stream or None, budget_bytes, 1 if profile else 0, BATCH_PLAN_ON_DEVICE if plan_on_device else 0)
+    st = _BatchStats()
+    _check(library().gva_batch_count_texts(db._h, ctypes.cast(arr, ctypes.c_void_p), n, mode, ctypes.byref(o),
+                                           counts.ctypes.data, gc.ctypes.data if gc is not None else None,
+                                           sup.ctypes.data if sup is not None else None, status.ctypes.data,
+                                           ctypes.byref(st)))
+    per_graph = gc if graph_counts else sup
+    if graph_counts and support:
+        per_graph = (gc, sup)
+    return counts, per_graph, _batch_stats_dict(st)
 
 
 @dataclass

@@ -25,7 +25,7 @@ NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompil
               "--expt-relaxed-constexpr", f"-I{ROOT / 'include'}"] + ARCH
 CXX_FLAGS = ["-O2", "-std=c++17", "-fPIC", "-Wall", "-Wno-sign-compare", f"-I{ROOT / 'include'}"]
 
-CU_SOURCES = ["gva_engine.cu", "gva_batch.cu", "gva_static.cu", "gva_mni.cu"]
+CU_SOURCES = ["gva_engine.cu", "gva_batch.cu", "gva_static.cu", "gva_mni.cu", "gva_dplan.cu"]
 CPP_SOURCES = ["gva_plan.cpp", "gva_graph.cpp", "gva_capi.cpp", "gva_mine.cpp", "gva_convert.cpp", "gva_text.cpp"]
 
 
@@ -58,7 +58,7 @@ def build(verbose: bool = False) -> Path:
     """Compile everything; returns the path of libgeneva.so."""
     LIB.mkdir(parents=True, exist_ok=True)
     OBJ.mkdir(parents=True, exist_ok=True)
-    headers = list(CSRC.glob("*.h")) + list(CSRC.glob("*.cuh")) + [ROOT / "include" / "geneva.h"]
+    headers = list(CSRC.glob("*.h")) + list(CSRC.glob("*.cuh")) + list(CSRC.glob("*.inc")) + [ROOT / "include" / "geneva.h"]
     jobs = []
     objs = []
     for src in CU_SOURCES:

@@ -7,6 +7,7 @@
 #include <chrono>
 #include <cstring>
 #include <fstream>
+#include <memory>
 #include <sstream>
 #include <string>
 #include <thread>
@@ -14,6 +15,7 @@
 
 #include "../../include/geneva.h"
 #include "gva_engine.cuh"
+#include "gva_dplan.h"
 #include "gva_internal.h"
 
 namespace gva {
@@ -243,6 +245,70 @@ int gva_plan_batch(const char* const* query_texts, int n, int mode, gva_plan** o
     return GVA_OK;
 }
 
+int gva_plan_batch_device(int device, const char* const* query_texts, int n, gva_plan** out, int* status) {
+    if (n < 0 || (n > 0 && (!query_texts || !out))) return fail(GVA_ERR_ARG, "null argument");
+    for (int i = 0; i < n; ++i) out[i] = nullptr;
+    std::vector<int> st(n, GVA_OK);
+    std::vector<std::string> msg(n);
+    std::vector<std::vector<uint32_t>> lab(n), sdl(n);
+    parallel_for(n, [&](int i) {
+        st[i] = query_texts[i] ? read_query_text(query_texts[i], lab[i], sdl[i]) : fail(GVA_ERR_ARG, "null query text");
+        if (st[i]) msg[i] = last_error_cstr();
+        return GVA_OK;
+    });
+    std::vector<DevPlanQuery> dq;
+    std::vector<int> slot(n, -1);
+    for (int i = 0; i < n; ++i) {
+        if (st[i]) continue;
+        bool ok = !sdl[i].empty() && lab[i].size() <= (size_t)kDevPlanV && sdl[i].size() / 3 <= (size_t)kDevPlanLines;
+        for (size_t e = 0; e + 2 < sdl[i].size() && ok; e += 3)
+            ok = sdl[i][e] < lab[i].size() && sdl[i][e + 1] < lab[i].size() && sdl[i][e] != sdl[i][e + 1];
+        if (!ok) continue;
+        DevPlanQuery q{};
+        q.n = (uint32_t)lab[i].size();
+        q.lines = (uint32_t)(sdl[i].size() / 3);
+        for (uint32_t v = 0; v < q.n; ++v) q.label[v] = lab[i][v];
+        for (uint32_t e = 0; e < q.lines; ++e) {
+            q.s[e] = (uint8_t)sdl[i][3 * e];
+            q.d[e] = (uint8_t)sdl[i][3 * e + 1];
+            q.l[e] = sdl[i][3 * e + 2];
+        }
+        slot[i] = (int)dq.size();
+        dq.push_back(q);
+    }
+    std::vector<DevPlanOut> res(dq.size());
+    int rc = plan_on_device(device, nullptr, dq.data(), (uint32_t)dq.size(), res.data());
+    if (rc) return rc;
+    parallel_for(n, [&](int i) {
+        if (st[i]) return GVA_OK;
+        gva_plan* p = new gva_plan();
+        int r;
+        if (slot[i] >= 0 && res[slot[i]].status == DPLAN_OK) {
+            thread_local std::unique_ptr<DPlan> dp(new DPlan());
+            dplan_from_device(res[slot[i]], *dp);
+            r = plan_from_dplan(*dp, lab[i].data(), p->plan);
+        } else {
+            r = plan_from_query((uint32_t)lab[i].size(), lab[i].data(), sdl[i].data(), sdl[i].size() / 3, GVA_MODE_DV,
+                                p->plan);
+        }
+        if (r) {
+            st[i] = r;
+            msg[i] = last_error_cstr();
+            delete p;
+        } else {
+            out[i] = p;
+        }
+        return GVA_OK;
+    });
+    int first = -1;
+    for (int i = 0; i < n; ++i) {
+        if (status) status[i] = st[i];
+        if (st[i] && first < 0) first = i;
+    }
+    if (first >= 0) return fail(st[first], "query " + std::to_string(first) + ": " + msg[first]);
+    return GVA_OK;
+}
+
 int gva_plan_from_text(const char* query_text, int mode, gva_plan** out) {
     if (!out || !query_text) return fail(GVA_ERR_ARG, "null argument");
     *out = nullptr;
@@ -374,6 +440,30 @@ int gva_db_set_graphs(gva_db* db, const uint64_t* first, uint32_t num_graphs) {
     return set_graph_ids(*db->dev, first, num_graphs);
 }
 
+namespace {
+void fill_batch_stats(const BatchStats& bs, double lower_ms, gva_batch_stats* stats) {
+    memset(stats, 0, sizeof *stats);
+    stats->gpu_ms = bs.gpu_ms;
+    stats->rounds = bs.rounds;
+    stats->splits = bs.splits;
+    stats->launches = bs.launches;
+    stats->trie_nodes = bs.nodes;
+    stats->lower_ms = lower_ms;
+    stats->submit_ms = bs.submit_ms;
+    stats->round_host_ms = bs.round_host_ms;
+    stats->wait_ms = bs.wait_ms;
+    stats->session_ms = bs.session_ms;
+    for (int i = 0; i < 5; ++i) stats->round_phase_ms[i] = bs.phase_ms[i];
+    for (int i = 0; i < K_NUM && i < 5; ++i) {
+        strncpy(stats->kernels[i].name, kKernelNames[i], sizeof stats->kernels[i].name - 1);
+        stats->kernels[i].launches = bs.kstat[i].launches;
+        stats->kernels[i].ms = bs.kstat[i].ms;
+        stats->kernels[i].bytes = bs.kstat[i].bytes;
+        stats->kernels[i].rows = bs.kstat[i].rows;
+    }
+}
+}  // namespace
+
 int gva_batch_count(gva_db* db, const gva_plan* const* plans, int nplans, const gva_batch_opts* opts,
                     uint64_t* counts, uint64_t* graph_counts, uint32_t* graph_support, gva_batch_stats* stats) {
     if (!db || (nplans > 0 && (!plans || !counts))) return fail(GVA_ERR_ARG, "null argument");
@@ -392,28 +482,136 @@ int gva_batch_count(gva_db* db, const gva_plan* const* plans, int nplans, const 
     int st = run_batch(*db->dev, std::move(steps), (cudaStream_t)o.stream, o.budget_bytes, db->dev->vgraph,
                        db->dev->num_graphs,
                        counts, graph_counts, graph_support, o.profile != 0, &bs);
-    if (stats) {
-        memset(stats, 0, sizeof *stats);
-        stats->gpu_ms = bs.gpu_ms;
-        stats->rounds = bs.rounds;
-        stats->splits = bs.splits;
-        stats->launches = bs.launches;
-        stats->trie_nodes = bs.nodes;
-        stats->lower_ms = lower_ms;
-        stats->submit_ms = bs.submit_ms;
-        stats->round_host_ms = bs.round_host_ms;
-        stats->wait_ms = bs.wait_ms;
-        stats->session_ms = bs.session_ms;
-        for (int i = 0; i < 5; ++i) stats->round_phase_ms[i] = bs.phase_ms[i];
-        for (int i = 0; i < K_NUM && i < 5; ++i) {
-            strncpy(stats->kernels[i].name, kKernelNames[i], sizeof stats->kernels[i].name - 1);
-            stats->kernels[i].launches = bs.kstat[i].launches;
-            stats->kernels[i].ms = bs.kstat[i].ms;
-            stats->kernels[i].bytes = bs.kstat[i].bytes;
-            stats->kernels[i].rows = bs.kstat[i].rows;
+    if (stats) fill_batch_stats(bs, lower_ms, stats);
+    return st;
+}
+
+int gva_batch_count_texts(gva_db* db, const char* const* texts, int n, int mode, const gva_batch_opts* opts,
+                          uint64_t* counts, uint64_t* graph_counts, uint32_t* graph_support, int* status,
+                          gva_batch_stats* stats) {
+    if (!db || n < 0 || (n > 0 && (!texts || !counts))) return fail(GVA_ERR_ARG, "null argument");
+    if (mode != GVA_MODE_DV && mode != GVA_MODE_SV) return fail(GVA_ERR_ARG, "mode must be GVA_MODE_DV or GVA_MODE_SV");
+    gva_batch_opts o{};
+    if (opts) o = *opts;
+    const auto t_lower = std::chrono::steady_clock::now();
+    std::vector<std::vector<Step>> steps(n);
+    std::vector<int> st(n, GVA_OK);
+    std::vector<std::string> msg(n);
+    const HostGraph& meta = db->dev->meta;
+    // device planning: queries read on the host, planned by the planning
+    // kernel, lowered on the host from the compact plans
+    const bool on_device = (o.flags & GVA_BATCH_PLAN_ON_DEVICE) && mode == GVA_MODE_DV;
+    std::vector<std::vector<uint32_t>> qlab(on_device ? n : 0), qsdl(on_device ? n : 0);
+    std::vector<int> dev_slot(on_device ? n : 0, -1);
+    std::vector<DevPlanOut> dev_out;
+    if (on_device) {
+        std::vector<int> rd(n, GVA_OK);
+        parallel_for(n, [&](int i) {
+            rd[i] = texts[i] ? read_query_text(texts[i], qlab[i], qsdl[i]) : fail(GVA_ERR_ARG, "null query text");
+            if (rd[i]) msg[i] = last_error_cstr();
+            return GVA_OK;
+        });
+        std::vector<DevPlanQuery> dq;
+        for (int i = 0; i < n; ++i) {
+            const std::vector<uint32_t>& lab = qlab[i];
+            const std::vector<uint32_t>& sdl = qsdl[i];
+            if (rd[i]) {
+                st[i] = rd[i];
+                continue;
+            }
+            bool ok = !sdl.empty() && lab.size() <= (size_t)kDevPlanV && sdl.size() / 3 <= (size_t)kDevPlanLines;
+            for (size_t e = 0; e + 2 < sdl.size() && ok; e += 3)
+                ok = sdl[e] < lab.size() && sdl[e + 1] < lab.size() && sdl[e] != sdl[e + 1];
+            if (!ok) continue;
+            DevPlanQuery q{};
+            q.n = (uint32_t)lab.size();
+            q.lines = (uint32_t)(sdl.size() / 3);
+            for (size_t v = 0; v < lab.size(); ++v) q.label[v] = lab[v];
+            for (uint32_t e = 0; e < q.lines; ++e) {
+                q.s[e] = (uint8_t)sdl[3 * e];
+                q.d[e] = (uint8_t)sdl[3 * e + 1];
+                q.l[e] = sdl[3 * e + 2];
+            }
+            dev_slot[i] = (int)dq.size();
+            dq.push_back(q);
+        }
+        dev_out.resize(dq.size());
+        const int rc = plan_on_device(db->dev->device, (cudaStream_t)o.stream, dq.data(), (uint32_t)dq.size(),
+                                      dev_out.data());
+        if (rc) return rc;
+    }
+    parallel_for(n, [&](int i) {
+        thread_local std::unique_ptr<DPlanQuery> dq(new DPlanQuery());
+        thread_local std::unique_ptr<DPlan> dp(new DPlan());
+        if (on_device && st[i]) return GVA_OK;  // the text could not be read (message kept)
+        std::vector<uint32_t> labels, sdl;
+        int r = GVA_OK;
+        if (on_device) {
+            labels.swap(qlab[i]);
+            sdl.swap(qsdl[i]);
+        } else {
+            r = texts[i] ? read_query_text(texts[i], labels, sdl) : fail(GVA_ERR_ARG, "null query text");
+        }
+        bool done = false;
+        if (!r && on_device && dev_slot[i] >= 0 && dev_out[dev_slot[i]].status == DPLAN_OK) {
+            dplan_from_device(dev_out[dev_slot[i]], *dp);
+            r = lower_dplan(*dp, labels.data(), meta, steps[i], true);
+            done = true;
+        }
+        if (!r && !done && !on_device && mode == GVA_MODE_DV && labels.size() <= (size_t)kDpV &&
+            sdl.size() / 3 <= (size_t)kDpLines) {
+            // edges the planner would reject go to it for their message
+            bool clean = !sdl.empty();
+            for (size_t e = 0; e + 2 < sdl.size() && clean; e += 3)
+                clean = sdl[e] < labels.size() && sdl[e + 1] < labels.size() && sdl[e] != sdl[e + 1];
+            if (clean) {
+                dq->n = (uint32_t)labels.size();
+                dq->lines = (uint32_t)(sdl.size() / 3);
+                for (size_t v = 0; v < labels.size(); ++v) dq->label[v] = labels[v];
+                for (uint32_t e = 0; e < dq->lines; ++e) {
+                    dq->s[e] = sdl[3 * e];
+                    dq->d[e] = sdl[3 * e + 1];
+                    dq->l[e] = sdl[3 * e + 2];
+                }
+                dplan(*dq, *dp);
+                if (dp->status == DPLAN_OK) {
+                    r = lower_dplan(*dp, dq->label, meta, steps[i], true);
+                    done = true;
+                }
+            }
+        }
+        if (!r && !done) {
+            Plan plan;
+            r = plan_from_query((uint32_t)labels.size(), labels.data(), sdl.data(), sdl.size() / 3, mode, plan);
+            if (!r) r = lower_plan(plan, meta, steps[i], true);
+        }
+        st[i] = r;
+        if (r) msg[i] = last_error_cstr();
+        return GVA_OK;  // per-query failures are reported in status
+    });
+    // texts that failed to plan are counted as a plan that cannot match
+    int first = -1;
+    for (int i = 0; i < n; ++i) {
+        if (status) status[i] = st[i];
+        if (st[i] && first < 0) first = i;
+        if (st[i]) {
+            Step seed;
+            seed.kind = STEP_SEED;
+            seed.always_empty = 1;
+            Step ext;
+            ext.always_empty = 1;
+            steps[i] = {seed, ext};
         }
     }
-    return st;
+    const double lower_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_lower).count();
+    BatchStats bs;
+    int rc = n ? run_batch(*db->dev, std::move(steps), (cudaStream_t)o.stream, o.budget_bytes, db->dev->vgraph,
+                           db->dev->num_graphs, counts, graph_counts, graph_support, o.profile != 0, &bs)
+               : GVA_OK;
+    if (stats) fill_batch_stats(bs, lower_ms, stats);
+    if (rc) return rc;
+    if (first >= 0) return fail(st[first], "query " + std::to_string(first) + ": " + msg[first]);
+    return GVA_OK;
 }
 
 int gva_db_get_tuning(const gva_db* db, gva_tuning* out) {

@@ -325,6 +325,35 @@ int mni_run_prepared(DevDB& db, const MniPrepared& prep, uint32_t cap, bool plai
                      std::vector<uint32_t>& support, MniStats& st, const volatile int* cancel = nullptr,
                      uint32_t sm_percent = 0);
 
+// ---- device-side planning (gva_dplan.cu) ----
+// Fixed-size query records and compact plans exchanged with the planning
+// kernel (dplan on the device, one query per thread).
+constexpr int kDevPlanV = 16, kDevPlanLines = 32, kDevPlanPhases = 32, kDevPlanPairs = 96, kDevPlanKeys = 64;
+struct DevPlanQuery {
+    uint32_t n, lines;
+    uint32_t label[kDevPlanV];
+    uint8_t s[kDevPlanLines], d[kDevPlanLines];
+    uint32_t l[kDevPlanLines];
+};
+struct DevPlanOut {
+    uint32_t status, vnum, nphase, npair;
+    uint32_t restricts[kDevPlanV + 1];
+    uint32_t ph_el[kDevPlanPhases];
+    uint8_t ph_type[kDevPlanPhases], ph_at[kDevPlanPhases], ph_np[kDevPlanPhases];
+    uint8_t pairs[kDevPlanPairs];
+    uint32_t nrep, nstat, ncol, pad;  // repeat flags, record stats and columns (the plan text; not lowered)
+    uint64_t rep_key[kDevPlanKeys];
+    uint32_t rep_val[kDevPlanKeys];
+    uint32_t stat_el[kDevPlanKeys], stat_vl[kDevPlanKeys];
+    uint8_t columns[kDevPlanV];
+};
+struct DPlan;
+// Plans n queries on `device` (blocking: the plans are on the host when it returns).
+int plan_on_device(int device, cudaStream_t s, const DevPlanQuery* qs, uint32_t n, DevPlanOut* outs);
+// The host-side DPlan of a device plan: the fields lowering reads.
+void dplan_from_device(const DevPlanOut& o, DPlan& p);
+uint64_t dplan_kernel_launches();
+
 size_t step_scratch_bytes(uint64_t in_rows);
 // run_step with the library's fixed device scratch array (no allocation).
 int run_step_static(DevDB& db, const Step& st, const uint32_t* in, uint64_t in_rows, uint32_t* out,

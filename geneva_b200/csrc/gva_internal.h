@@ -102,6 +102,10 @@ struct Plan {
 };
 
 int plan_from_text(const std::string& text, int mode, Plan& out);
+// A query text's vertex labels (by id 0..n-1, first definition wins) and edge
+// lines (source, target, label) in text order, read by the planner's rules;
+// the vertex checks of the planner are made here, the edge checks by it.
+int read_query_text(const std::string& text, std::vector<uint32_t>& labels, std::vector<uint32_t>& sdl);
 // The same plan for the query "v i labels[i]" (i < n) followed by the edges
 // "e sdl[3j] sdl[3j+1] sdl[3j+2]" (j < ne), without the text.
 int plan_from_query(uint32_t n, const uint32_t* labels, const uint32_t* sdl, size_t ne, int mode, Plan& out);

@@ -156,7 +156,6 @@ public:
         return none;
     }
     int parse(const std::string& text);
-    int set_vertices(const std::map<uint32_t, uint32_t>& labels);
     int set_vertices(uint32_t nv, const uint32_t* labels);  // vertex v labelled labels[v]
     int set_edges(const uint32_t* sdl, size_t ne);  // (svid, evid, label) triples in query order
     void count_triangle(uint32_t i, TriInfo& t) const;
@@ -172,48 +171,12 @@ public:
 };
 
 int Planner::parse(const std::string& text) {
-    Cursor c(text);
-    std::map<uint32_t, uint32_t> labels;  // vid -> label, first definition wins
-    char ch;
-    bool in_edges = false;
-    while (c.get(ch)) {
-        if (ch == 'v') {
-            uint32_t vid, lab;
-            if (!c.read_uint(vid) || !c.read_uint(lab)) break;
-            labels.emplace(vid, lab);
-        } else if (ch == 'e') {
-            --c.i;
-            in_edges = true;
-            break;
-        } else if (ch == '#') {
-            c.skip_line();
-        }
-    }
-    int st = set_vertices(labels);
+    std::vector<uint32_t> labels, sdl;
+    int st = read_query_text(text, labels, sdl);
     if (st) return st;
-    if (!in_edges) return fail(GVA_ERR_FORMAT, "query has no edges");
-    std::vector<uint32_t> sdl;
-    while (c.ok && c.get(ch)) {
-        if (ch != 'e') continue;
-        uint32_t s, d, l;
-        if (!c.read_uint(s) || !c.read_uint(d) || !c.read_uint(l)) break;
-        sdl.push_back(s);
-        sdl.push_back(d);
-        sdl.push_back(l);
-    }
+    st = set_vertices((uint32_t)labels.size(), labels.data());
+    if (st) return st;
     return set_edges(sdl.data(), sdl.size() / 3);
-}
-
-int Planner::set_vertices(const std::map<uint32_t, uint32_t>& labels) {
-    n = (uint32_t)labels.size();
-    if (n == 0) return fail(GVA_ERR_FORMAT, "query has no vertices");
-    if (n > GVA_MAX_QUERY_VERTICES) return fail(GVA_ERR_UNSUPPORTED, "query has more than 32 vertices");
-    uint32_t expect = 0;
-    for (auto& kv : labels) {
-        if (kv.first != expect++) return fail(GVA_ERR_FORMAT, "query vertex ids must be 0..n-1");
-        qlabel.push_back(kv.second);
-    }
-    return GVA_OK;
 }
 
 int Planner::set_vertices(uint32_t nv, const uint32_t* labels) {
@@ -798,6 +761,46 @@ int finish_plan(Planner& p, int mode, Plan& out) {
 }
 
 }  // namespace
+
+int read_query_text(const std::string& text, std::vector<uint32_t>& labels_out, std::vector<uint32_t>& sdl) {
+    Cursor c(text);
+    std::map<uint32_t, uint32_t> labels;  // vid -> label, first definition wins
+    char ch;
+    bool in_edges = false;
+    while (c.get(ch)) {
+        if (ch == 'v') {
+            uint32_t vid, lab;
+            if (!c.read_uint(vid) || !c.read_uint(lab)) break;
+            labels.emplace(vid, lab);
+        } else if (ch == 'e') {
+            --c.i;
+            in_edges = true;
+            break;
+        } else if (ch == '#') {
+            c.skip_line();
+        }
+    }
+    const uint32_t n = (uint32_t)labels.size();
+    if (n == 0) return fail(GVA_ERR_FORMAT, "query has no vertices");
+    if (n > GVA_MAX_QUERY_VERTICES) return fail(GVA_ERR_UNSUPPORTED, "query has more than 32 vertices");
+    labels_out.clear();
+    uint32_t expect = 0;
+    for (auto& kv : labels) {
+        if (kv.first != expect++) return fail(GVA_ERR_FORMAT, "query vertex ids must be 0..n-1");
+        labels_out.push_back(kv.second);
+    }
+    if (!in_edges) return fail(GVA_ERR_FORMAT, "query has no edges");
+    sdl.clear();
+    while (c.ok && c.get(ch)) {
+        if (ch != 'e') continue;
+        uint32_t s, d, l;
+        if (!c.read_uint(s) || !c.read_uint(d) || !c.read_uint(l)) break;
+        sdl.push_back(s);
+        sdl.push_back(d);
+        sdl.push_back(l);
+    }
+    return GVA_OK;
+}
 
 int plan_from_text(const std::string& text, int mode, Plan& out) {
     if (mode != GVA_MODE_DV && mode != GVA_MODE_SV) return fail(GVA_ERR_ARG, "mode must be GVA_MODE_DV or GVA_MODE_SV");

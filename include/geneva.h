@@ -123,6 +123,11 @@ int gva_convert_g(const char* g_path, const char* mygraph_path, const char* meta
  * restrictions and repeat flags for the same query text.  Host-only. */
 int gva_plan_from_file(const char* query_path, int mode, gva_plan** out);
 int gva_plan_from_text(const char* query_text, int mode, gva_plan** out);
+/* gva_plan_batch for DV plans computed on `device` by the device planner
+ * (the heap-free planner, one query per thread; queries of up to 16 vertices
+ * and 32 edge lines, others planned on the host): the same plans as the host
+ * planner (genMatchOrder, src/genMatchOrderCPU.cpp:670-983). */
+int gva_plan_batch_device(int device, const char* const* query_texts, int n, gva_plan** out, int* status);
 /* gva_plan_from_text for n queries at once on the host's cores (a batch or a
  * serving wave planned in one call): out[i] receives query i's plan (NULL on
  * failure) and status[i] (may be NULL) its status; the call returns the first
@@ -169,8 +174,12 @@ typedef struct gva_batch_opts {
     void* stream;          /* cudaStream_t; NULL = legacy default stream            */
     uint64_t budget_bytes; /* frontier memory cap (0 = 3/4 of free HBM)            */
     int profile;           /* 1: per-kernel CUDA-event timing in stats->kernels     */
-    int reserved;
+    int flags;             /* GVA_BATCH_* below; 0 = none                           */
 } gva_batch_opts;
+/* gva_batch_count_texts: plan the queries on the device (the heap-free
+ * planner, one query per thread; queries of up to 16 vertices and 32 edge
+ * lines, DV mode), the others on the host */
+#define GVA_BATCH_PLAN_ON_DEVICE 1
 
 typedef struct gva_batch_stats {
     double gpu_ms;
@@ -196,6 +205,18 @@ int gva_db_set_graphs(gva_db* db, const uint64_t* first, uint32_t num_graphs);
  * (optional): graphs holding at least one embedding. */
 int gva_batch_count(gva_db* db, const gva_plan* const* plans, int nplans, const gva_batch_opts* opts,
                     uint64_t* counts, uint64_t* graph_counts, uint32_t* graph_support, gva_batch_stats* stats);
+
+/* gva_batch_count for query texts, in one call: every text is read and
+ * planned on the host's cores (mode GVA_MODE_DV or GVA_MODE_SV; the planner
+ * without heap storage where it applies, else the host planner) and the plans
+ * counted in one batched run, without plan handles.  status[i] (optional)
+ * receives each text's planning status; a text that fails to plan gets
+ * count 0, and the call returns the first failure's status after counting
+ * the others.  Replaces running gpumine once per .query file
+ * (src/gpumine.cpp:866-1072). */
+int gva_batch_count_texts(gva_db* db, const char* const* query_texts, int n, int mode, const gva_batch_opts* opts,
+                          uint64_t* counts, uint64_t* graph_counts, uint32_t* graph_support, int* status,
+                          gva_batch_stats* stats);
 
 /* Launch shape of the batched engine's round kernels on one database: rows
  * per work item (32, 64 or 128; fewer when rows are wide) and the candidate

@@ -169,3 +169,33 @@ def test_hub_vertices_of_the_packed_segment_index(native, oracle):
         assert rows_digest(got) == rows_digest(rows), p
     oracle.free(og)
     gdb.close()
+
+
+def test_batch_count_texts_equals_planned_batch(small_db, oracle):
+    """gva_batch_count_texts (texts read and planned inside the call) gives the
+    counts of gva_batch_count over planned handles, in DV and SV mode; a text
+    the planner rejects fails alone (count 0, its status), after the others
+    were counted."""
+    import ctypes
+    db, gdb, og = small_db
+    pats = [p for p in _patterns(db, 120, 41) if oracle.count(og, p, cap_rows=1_000_000) is not None]
+    for mode in (gv.MODE_DV, gv.MODE_SV):
+        plans = [gv.Plan.from_text(p, mode) for p in pats]
+        want, (wgc, wsup), _ = gv.batch_count(gdb, plans, graph_counts=True, support=True)
+        got, (gc, sup), st = gv.batch_count_texts(gdb, pats, mode=mode, graph_counts=True, support=True)
+        assert np.array_equal(got, want) and np.array_equal(gc, wgc) and np.array_equal(sup, wsup)
+        assert st["trie_nodes"] > 0
+    bad = list(pats[:5]) + ["v 0 1\nv 1 1\ne 0 0 1\n", "v 0 1\nv 2 1\ne 0 2 1\n", "v 0 1\nv 1 2\n"] + list(pats[5:10])
+    lib = gv.library()
+    n = len(bad)
+    arr = (ctypes.c_char_p * n)(*[t.encode() for t in bad])
+    counts = np.zeros(n, dtype=np.uint64)
+    status = np.zeros(n, dtype=np.int32)
+    o = gv._BatchOpts(None, 0, 0, 0)
+    rc = lib.gva_batch_count_texts(gdb._h, ctypes.cast(arr, ctypes.c_void_p), n, gv.MODE_DV, ctypes.byref(o),
+                                   counts.ctypes.data, None, None, status.ctypes.data, None)
+    assert rc != 0 and b"query 5" in lib.gva_last_error()
+    assert list(status[5:8]) == [6, 2, 2]  # self-loop, ids not 0..n-1, no edges
+    want = [oracle.count(og, t) for t in pats[:10]]
+    assert [int(c) for i, c in enumerate(counts) if i not in (5, 6, 7)] == want
+    assert int(counts[5]) == int(counts[6]) == int(counts[7]) == 0
