@@ -29,6 +29,8 @@
 #include <unordered_map>
 #include <numeric>
 #include <string>
+#include <future>
+#include <tuple>
 #include <thread>
 #include <vector>
 
@@ -752,6 +754,7 @@ struct SessionSpare {
     std::vector<BatchSession::BNode> nodes;
     std::vector<const Step*> node_steps;
     std::vector<BatchSession::PlanRec> plans;
+    std::vector<unsigned char> desc_host;
 };
 thread_local SessionSpare t_spare;
 }  // namespace
@@ -764,6 +767,7 @@ BatchSession::BatchSession(DevDB& db_, cudaStream_t s_, uint64_t budget_, uint32
     nodes.swap(t_spare.nodes);
     node_steps.swap(t_spare.node_steps);
     plans.swap(t_spare.plans);
+    desc_host.swap(t_spare.desc_host);
     nodes.clear();
     node_steps.clear();
     plans.clear();
@@ -779,6 +783,7 @@ BatchSession::~BatchSession() {
     keep(nodes, t_spare.nodes);
     keep(node_steps, t_spare.node_steps);
     keep(plans, t_spare.plans);
+    if (desc_host.capacity() > t_spare.desc_host.capacity()) desc_host.swap(t_spare.desc_host);
     cudaSetDevice(db.device);
     active.clear();
     if (staged) cudaEventDestroy(staged);
@@ -790,9 +795,12 @@ BatchSession::~BatchSession() {
 int BatchSession::init() {
     GVA_CUDA_B(cudaSetDevice(db.device));
     if (budget == 0) {
-        size_t fr = 0, tot = 0;
-        GVA_CUDA_B(cudaMemGetInfo(&fr, &tot));
-        budget = (uint64_t)fr / 4 * 3;
+        if (db.default_budget == 0) {
+            size_t fr = 0, tot = 0;
+            GVA_CUDA_B(cudaMemGetInfo(&fr, &tot));
+            db.default_budget = (uint64_t)fr / 4 * 3;
+        }
+        budget = db.default_budget;
     }
     per_graph = nslots > 0;
     if (per_graph) {
@@ -1872,16 +1880,62 @@ int run_batch(DevDB& db, std::vector<std::vector<Step>> steps, cudaStream_t s, u
     std::vector<std::vector<Step>> sorted(n);
     for (size_t i = 0; i < n; ++i) sorted[i] = std::move(steps[order[i]]);
     const double order_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
-    PreparedBatch pb;
-    int rc = prepare_batch(db, std::move(sorted), s, budget, graph_counts_host || support_host,
-                           graph_counts_host != nullptr, profile, pb, true);
-    if (rc) return rc;
     // results in submission (sorted) order, then back to the caller's order
     std::vector<uint64_t> c2(n);
     std::vector<uint32_t> s2(support_host ? n : 0);
     std::vector<uint64_t> g2(graph_counts_host ? n * (size_t)db.num_graphs : 0);
-    rc = finish_batch(db, pb, c2.data(), graph_counts_host ? g2.data() : nullptr, support_host ? s2.data() : nullptr,
-                      stats);
+    // a large batch runs in K contiguous chunks of the sorted plans (they
+    // share prefixes within a chunk): chunk k + 1's session (device set-up,
+    // trie, descriptors; host work) is prepared on a helper thread while
+    // chunk k's rounds run, so that only the first chunk's set-up leaves the
+    // device idle
+    const size_t K = n >= 12288 ? 2 : 1;
+    std::vector<size_t> cut(K + 1);
+    for (size_t k = 0; k <= K; ++k) cut[k] = n * k / K;
+    const bool per_graph = graph_counts_host || support_host;
+    auto prepare = [&](size_t k) {
+        std::unique_ptr<PreparedBatch> pb(new PreparedBatch());
+        std::vector<std::vector<Step>> part(std::make_move_iterator(sorted.begin() + cut[k]),
+                                            std::make_move_iterator(sorted.begin() + cut[k + 1]));
+        int r = prepare_batch(db, std::move(part), s, budget, per_graph, graph_counts_host != nullptr, profile, *pb,
+                              true);
+        std::string err = r ? last_error_cstr() : std::string();
+        return std::make_tuple(std::move(pb), r, err);
+    };
+    auto cur = prepare(0);
+    if (std::get<1>(cur)) return std::get<1>(cur);
+    int rc = GVA_OK;
+    BatchStats total;
+    for (size_t k = 0; k < K && !rc; ++k) {
+        std::future<decltype(cur)> next;
+        if (k + 1 < K) next = std::async(std::launch::async, prepare, k + 1);
+        BatchStats bs;
+        const size_t a0 = cut[k];
+        rc = finish_batch(db, *std::get<0>(cur), c2.data() + a0,
+                          graph_counts_host ? g2.data() + a0 * (size_t)db.num_graphs : nullptr,
+                          support_host ? s2.data() + a0 : nullptr, &bs);
+        total.gpu_ms += bs.gpu_ms;
+        total.submit_ms += bs.submit_ms;
+        total.round_host_ms += bs.round_host_ms;
+        total.wait_ms += bs.wait_ms;
+        total.session_ms += bs.session_ms;
+        total.rounds += bs.rounds;
+        total.splits += bs.splits;
+        total.launches += bs.launches;
+        total.nodes += bs.nodes;
+        for (int i = 0; i < 5; ++i) total.phase_ms[i] += bs.phase_ms[i];
+        for (int i = 0; i < K_NUM; ++i) {
+            total.kstat[i].launches += bs.kstat[i].launches;
+            total.kstat[i].ms += bs.kstat[i].ms;
+            total.kstat[i].bytes += bs.kstat[i].bytes;
+            total.kstat[i].rows += bs.kstat[i].rows;
+        }
+        if (next.valid()) {
+            cur = next.get();
+            if (!rc && std::get<1>(cur)) rc = fail(std::get<1>(cur), std::get<2>(cur));
+        }
+    }
+    if (stats) *stats = total;
     if (rc) return rc;
     const size_t Gn = db.num_graphs;
     for (size_t i = 0; i < n; ++i) {

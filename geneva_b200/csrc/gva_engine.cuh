@@ -40,6 +40,9 @@ struct DevDB {
     uint32_t num_graphs = 0;
     // launch shape of the batched engine's round kernels (autotune_batch)
     uint32_t tune_rows_per_item = 64, tune_hub = 32;
+    // frontier budget of batched runs given none: 3/4 of the device memory
+    // free when the first such run started (querying it costs a driver call)
+    uint64_t default_budget = 0;
 };
 
 int upload_graph(HostGraph& g, int device, DevDB*& out);

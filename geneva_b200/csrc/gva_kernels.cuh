@@ -203,6 +203,23 @@ __device__ __forceinline__ uint32_t ext_count_row(const ExtArgs& p, const uint32
     ext_range(p, row, lo, hi);
     if (lo >= hi) return 0;
     uint32_t n = hi - lo;
+    if (n <= 8 && p.n_eq <= 8) {
+        // a short list: each candidate against the matched vertices, one
+        // pass over the list (a vertex in two columns still excludes its
+        // candidate once)
+        uint32_t eqv[8];
+#pragma unroll
+        for (int e = 0; e < 8; ++e) eqv[e] = e < (int)p.n_eq ? row[p.eq_cols[e]] : 0xffffffffu;
+        uint32_t m = 0;
+        for (uint32_t j = lo; j < hi; ++j) {
+            const uint32_t c = __ldg(p.adj + j);
+            bool coll = false;
+#pragma unroll
+            for (int e = 0; e < 8; ++e) coll |= c == eqv[e];
+            m += coll ? 0u : 1u;
+        }
+        return m;
+    }
     for (uint32_t j = 0; j < p.n_eq; ++j) {
         const uint32_t w = row[p.eq_cols[j]];
         bool dup = false;  // the same vertex in two columns collides once
