@@ -1719,9 +1719,11 @@ int prepare_batch(DevDB& db, std::vector<std::vector<Step>>&& steps, cudaStream_
 }
 
 int finish_batch(DevDB& db, PreparedBatch& pb, uint64_t* counts, uint64_t* graph_counts_host, uint32_t* support_host,
-                 BatchStats* stats, const volatile int* cancel) {
+                 BatchStats* stats, const volatile int* cancel, const uint32_t* order) {
     const int nq = pb.nq;
-    for (int q = 0; q < nq; ++q) counts[q] = 0;
+    // the result of submitted plan q goes to index at(q) of the caller's arrays
+    auto at = [&](int q) -> size_t { return order ? (size_t)order[q] : (size_t)q; };
+    for (int q = 0; q < nq; ++q) counts[at(q)] = 0;
     if (nq == 0) return GVA_OK;
     GVA_CUDA_B(cudaSetDevice(db.device));
     BatchSession& ses = *pb.ses;
@@ -1749,7 +1751,7 @@ int finish_batch(DevDB& db, PreparedBatch& pb, uint64_t* counts, uint64_t* graph
     const double loop_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_loop0).count();
     const std::vector<int>& ids = pb.ids;
     if (!rc) {
-        for (int q = 0; q < nq; ++q) counts[q] = ses.plan(ids[q]).count;
+        for (int q = 0; q < nq; ++q) counts[at(q)] = ses.plan(ids[q]).count;
         if (support_host || graph_counts_host) {
             // supports counted on the device; identical plans read their first one's slot
             uint32_t* d_pop = nullptr;
@@ -1766,18 +1768,23 @@ int finish_batch(DevDB& db, PreparedBatch& pb, uint64_t* counts, uint64_t* graph
                 cudaMemcpyAsync(pop, d_pop, (size_t)nq * 4, cudaMemcpyDeviceToHost, s);
                 cudaFreeAsync(d_pop, s);
             }
-            if (!rc && graph_counts_host)
-                cudaMemcpyAsync(graph_counts_host, ses.graph_counts_dev(), (size_t)nq * db.num_graphs * 8,
-                                cudaMemcpyDeviceToHost, s);
+            // per-graph counts by slot, landed in pinned staging (reused
+            // across runs), then each plan's row copied to its place
+            Staging gc_stage;
+            const size_t G = db.num_graphs;
+            uint64_t* gc = nullptr;
+            if (!rc && graph_counts_host) {
+                gc = (uint64_t*)gc_stage.get((size_t)nq * G * 8);
+                if (!gc) rc = fail(GVA_ERR_NOMEM, "pinned staging allocation failed");
+                if (!rc)
+                    cudaMemcpyAsync(gc, ses.graph_counts_dev(), (size_t)nq * G * 8, cudaMemcpyDeviceToHost, s);
+            }
             if (!rc)
                 rc = cudaStreamSynchronize(s) == cudaSuccess ? GVA_OK : fail(GVA_ERR_CUDA, "result read-back failed");
             for (int q = 0; q < nq && !rc; ++q) {
-                const int sl = ses.plan(ses.first_peer(ids[q])).slot, own = ses.plan(ids[q]).slot;
-                if (support_host) support_host[q] = pop[sl];
-                if (graph_counts_host && sl != own)
-                    std::copy(graph_counts_host + (size_t)sl * db.num_graphs,
-                              graph_counts_host + (size_t)(sl + 1) * db.num_graphs,
-                              graph_counts_host + (size_t)own * db.num_graphs);
+                const int sl = ses.plan(ses.first_peer(ids[q])).slot;
+                if (support_host) support_host[at(q)] = pop[sl];
+                if (gc) std::copy(gc + (size_t)sl * G, gc + (size_t)(sl + 1) * G, graph_counts_host + at(q) * G);
             }
         }
     }
@@ -1804,6 +1811,25 @@ int finish_batch(DevDB& db, PreparedBatch& pb, uint64_t* counts, uint64_t* graph
         stats->session_ms = (pb.prep_ms - stats->submit_ms) + (fin_ms - loop_ms);
     }
     return rc;
+}
+
+// A second stream of the device for the second half of a large batched run
+// (created once per device and kept), ordered after the work already on `s`.
+static int second_stream(int device, cudaStream_t s, cudaStream_t& out) {
+    static std::mutex mu;
+    static cudaStream_t aux[64] = {};
+    static cudaEvent_t ev[64] = {};
+    if (device < 0 || device >= 64) return fail(GVA_ERR_ARG, "device index out of range");
+    std::lock_guard<std::mutex> lock(mu);
+    GVA_CUDA_B(cudaSetDevice(device));
+    if (!aux[device]) {
+        GVA_CUDA_B(cudaStreamCreateWithFlags(&aux[device], cudaStreamNonBlocking));
+        GVA_CUDA_B(cudaEventCreateWithFlags(&ev[device], cudaEventDisableTiming));
+    }
+    GVA_CUDA_B(cudaEventRecord(ev[device], s));
+    GVA_CUDA_B(cudaStreamWaitEvent(aux[device], ev[device], 0));
+    out = aux[device];
+    return GVA_OK;
 }
 
 // Plans ordered by their sequences of step keys (64-bit hashes of the key
@@ -1880,41 +1906,46 @@ int run_batch(DevDB& db, std::vector<std::vector<Step>> steps, cudaStream_t s, u
     std::vector<std::vector<Step>> sorted(n);
     for (size_t i = 0; i < n; ++i) sorted[i] = std::move(steps[order[i]]);
     const double order_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
-    // results in submission (sorted) order, then back to the caller's order
-    std::vector<uint64_t> c2(n);
-    std::vector<uint32_t> s2(support_host ? n : 0);
-    std::vector<uint64_t> g2(graph_counts_host ? n * (size_t)db.num_graphs : 0);
-    // a large batch runs in K contiguous chunks of the sorted plans (they
-    // share prefixes within a chunk): chunk k + 1's session (device set-up,
-    // trie, descriptors; host work) is prepared on a helper thread while
-    // chunk k's rounds run, so that only the first chunk's set-up leaves the
-    // device idle
+    // a large batch runs as two contiguous halves of the sorted plans (plans
+    // share prefixes within a half), each prepared and run by its own host
+    // thread on its own stream: one half's host work (trie, descriptors,
+    // rounds' bookkeeping) overlaps the other's kernels, and the two halves'
+    // kernels fill each other's gaps on the device
     const size_t K = n >= 12288 ? 2 : 1;
     std::vector<size_t> cut(K + 1);
     for (size_t k = 0; k <= K; ++k) cut[k] = n * k / K;
     const bool per_graph = graph_counts_host || support_host;
-    auto prepare = [&](size_t k) {
-        std::unique_ptr<PreparedBatch> pb(new PreparedBatch());
+    cudaStream_t streams[2] = {s, s};
+    if (K == 2) {
+        int rc0 = second_stream(db.device, s, streams[1]);
+        if (rc0) return rc0;
+    }
+    std::vector<BatchStats> bss(K);
+    std::vector<int> rcs(K, GVA_OK);
+    std::vector<std::string> errs(K);
+    auto run_half = [&](size_t k) {
+        PreparedBatch pb;
         std::vector<std::vector<Step>> part(std::make_move_iterator(sorted.begin() + cut[k]),
                                             std::make_move_iterator(sorted.begin() + cut[k + 1]));
-        int r = prepare_batch(db, std::move(part), s, budget, per_graph, graph_counts_host != nullptr, profile, *pb,
-                              true);
-        std::string err = r ? last_error_cstr() : std::string();
-        return std::make_tuple(std::move(pb), r, err);
+        int r = prepare_batch(db, std::move(part), streams[k], budget, per_graph, graph_counts_host != nullptr,
+                              profile, pb, true);
+        // results straight to the caller's arrays, at each plan's index before sorting
+        if (!r) r = finish_batch(db, pb, counts, graph_counts_host, support_host, &bss[k], nullptr, order.data() + cut[k]);
+        rcs[k] = r;
+        if (r) errs[k] = last_error_cstr();
     };
-    auto cur = prepare(0);
-    if (std::get<1>(cur)) return std::get<1>(cur);
+    {
+        std::vector<std::thread> pool;
+        for (size_t k = 1; k < K; ++k) pool.emplace_back(run_half, k);
+        run_half(0);
+        for (auto& th : pool) th.join();
+    }
     int rc = GVA_OK;
+    for (size_t k = 0; k < K && !rc; ++k)
+        if (rcs[k]) rc = fail(rcs[k], errs[k]);
     BatchStats total;
-    for (size_t k = 0; k < K && !rc; ++k) {
-        std::future<decltype(cur)> next;
-        if (k + 1 < K) next = std::async(std::launch::async, prepare, k + 1);
-        BatchStats bs;
-        const size_t a0 = cut[k];
-        rc = finish_batch(db, *std::get<0>(cur), c2.data() + a0,
-                          graph_counts_host ? g2.data() + a0 * (size_t)db.num_graphs : nullptr,
-                          support_host ? s2.data() + a0 : nullptr, &bs);
-        total.gpu_ms += bs.gpu_ms;
+    for (const BatchStats& bs : bss) {
+        total.gpu_ms = std::max(total.gpu_ms, bs.gpu_ms);  // the halves overlap
         total.submit_ms += bs.submit_ms;
         total.round_host_ms += bs.round_host_ms;
         total.wait_ms += bs.wait_ms;
@@ -1930,20 +1961,9 @@ int run_batch(DevDB& db, std::vector<std::vector<Step>> steps, cudaStream_t s, u
             total.kstat[i].bytes += bs.kstat[i].bytes;
             total.kstat[i].rows += bs.kstat[i].rows;
         }
-        if (next.valid()) {
-            cur = next.get();
-            if (!rc && std::get<1>(cur)) rc = fail(std::get<1>(cur), std::get<2>(cur));
-        }
     }
     if (stats) *stats = total;
     if (rc) return rc;
-    const size_t Gn = db.num_graphs;
-    for (size_t i = 0; i < n; ++i) {
-        counts[order[i]] = c2[i];
-        if (support_host) support_host[order[i]] = s2[i];
-        if (graph_counts_host)
-            std::copy(g2.begin() + i * Gn, g2.begin() + (i + 1) * Gn, graph_counts_host + (size_t)order[i] * Gn);
-    }
     if (stats) stats->submit_ms += order_ms;
     return GVA_OK;
 }

@@ -510,10 +510,13 @@ int run_match(DevDB& db, const Plan& plan, const std::vector<Step>& steps, cudaS
     res.stream = s;
     res.columns = plan.columns;
     res.phase_rows.assign(plan.phases.size(), 0);
-    if (budget == 0) {
-        size_t fr = 0, tot = 0;
-        GVA_CUDA(cudaMemGetInfo(&fr, &tot));
-        budget = (uint64_t)fr / 4 * 3;
+    if (budget == 0) {  // 3/4 of the memory free at the database's first run (a driver query per call is costly)
+        if (db.default_budget == 0) {
+            size_t fr = 0, tot = 0;
+            GVA_CUDA(cudaMemGetInfo(&fr, &tot));
+            db.default_budget = (uint64_t)fr / 4 * 3;
+        }
+        budget = db.default_budget;
     }
     HostStage* hs = nullptr;
     rc = host_stage(db.device, hs);

@@ -253,8 +253,9 @@ struct PreparedBatch {
 };
 int prepare_batch(DevDB& db, std::vector<std::vector<Step>>&& steps, cudaStream_t s, uint64_t budget,
                   bool per_graph, bool graph_counts, bool profile, PreparedBatch& out, bool presorted = false);
+// order (optional): plan q's results go to index order[q] of the arrays
 int finish_batch(DevDB& db, PreparedBatch& pb, uint64_t* counts, uint64_t* graph_counts_host, uint32_t* support_host,
-                 BatchStats* stats, const volatile int* cancel = nullptr);
+                 BatchStats* stats, const volatile int* cancel = nullptr, const uint32_t* order = nullptr);
 int set_graph_ids(DevDB& db, const uint64_t* first, uint32_t num_graphs);
 
 // Times the batched count of `steps` (a calibration batch) under each

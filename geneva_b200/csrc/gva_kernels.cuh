@@ -80,8 +80,13 @@ __device__ __forceinline__ void seg_of(const uint32_t* __restrict__ off, uint32_
         hi = __ldg(off + t + 1);
         return;
     }
+    // the words holding word 0, cum[l] and cum[l + 1] are loaded together
+    // (independent loads of one sector): one round trip for a narrow record
     const uint32_t* rec = off + (uint64_t)v * 8;
+    const uint32_t bl = 3 + l, bh = 4 + l;  // bytes of cum[l] (l > 0) and cum[l + 1]
     const uint32_t w0 = __ldg(rec);
+    const uint32_t wl = __ldg(rec + (bl >> 2));
+    const uint32_t wh = __ldg(rec + (bh >> 2));
     const uint32_t base = w0 & 0x7fffffffu;
     if (w0 & 0x80000000u) {  // more than 255 neighbours: a row of cumulative words
         const uint32_t* cw = off + __ldg(rec + 1);
@@ -89,16 +94,8 @@ __device__ __forceinline__ void seg_of(const uint32_t* __restrict__ off, uint32_
         hi = base + __ldg(cw + l + 1);
         return;
     }
-    const uint32_t bh = 4 + l;  // byte of cum[l + 1]
-    const uint32_t wh = __ldg(rec + (bh >> 2));
     hi = base + ((wh >> (8 * (bh & 3))) & 0xffu);
-    uint32_t c = 0;
-    if (l > 0) {
-        const uint32_t bl = 3 + l;  // byte of cum[l]
-        const uint32_t wl = (bl >> 2) == (bh >> 2) ? wh : __ldg(rec + (bl >> 2));
-        c = (wl >> (8 * (bl & 3))) & 0xffu;
-    }
-    lo = base + c;
+    lo = base + (l > 0 ? (wl >> (8 * (bl & 3))) & 0xffu : 0u);
 }
 
 // first index in [lo, hi) with a[i] >= x (hi if none)
