@@ -311,7 +311,7 @@ __device__ __forceinline__ uint64_t ext_item(const TaskDesc& d, const uint32_t* 
         uint32_t cnt = 0;
         if (!FUSED && !WRITE) {
             // plain extension: the segment minus the matched vertices in it
-            if (valid) cnt = ext_count_row(p, row);
+            if (valid) cnt = ext_count_plain(p, row);
         } else {
             uint32_t lo = 0, hi = 0;
             if (FUSED) {
@@ -341,7 +341,13 @@ __device__ __forceinline__ uint64_t ext_item(const TaskDesc& d, const uint32_t* 
                 cnt += ok ? 1u : 0u;
                 if (WRITE) tile_append(*tl, ok, row, k, c, true);
             }
-            // hub rows: the whole warp, 32 candidates per step
+            // hub rows: the whole warp.  Lists of 128 candidates or more are
+            // read as 16-byte vectors (4 consecutive candidates per lane, 128
+            // per step) from the 16-byte boundary at or below the list's
+            // start: adjacency arrays start 16-byte aligned and end with 16
+            // bytes of slack, so the vectors around a list's ends stay inside
+            // the allocation.  Shorter ones go 32 candidates per step, one per
+            // lane, which keeps every lane busy on them.
             uint32_t hubs = __ballot_sync(0xffffffffu, is_hub);
             if (FUSED) __syncwarp();  // generator states written before other lanes read them
             while (hubs) {
@@ -351,16 +357,34 @@ __device__ __forceinline__ uint64_t ext_item(const TaskDesc& d, const uint32_t* 
                 const uint32_t* hrow = rows_s + (base + h) * k;
                 const uint32_t* hadj = FUSED ? gen_s[h].gadj : p.adj;
                 uint32_t hc = 0;
-                for (uint32_t j0 = hlo; j0 < hhi; j0 += 32) {
-                    const uint32_t j = j0 + lane;
-                    bool ok = false;
-                    uint32_t c = 0;
-                    if (j < hhi) {
-                        c = __ldg(hadj + j);
-                        ok = FUSED ? ext_accept(p, hrow, c, gen_s[h]) : ext_injective(p, hrow, c);
+                if (hhi - hlo >= 128) {
+                    for (uint32_t j0 = hlo & ~3u; j0 < hhi; j0 += 128) {
+                        const uint32_t j = j0 + 4 * lane;
+                        uint4 v4 = make_uint4(0, 0, 0, 0);
+                        if (j < hhi) v4 = __ldg(reinterpret_cast<const uint4*>(hadj + j));
+                        const uint32_t vv[4] = {v4.x, v4.y, v4.z, v4.w};
+#pragma unroll
+                        for (int q = 0; q < 4; ++q) {
+                            const uint32_t c = vv[q];
+                            bool ok = false;
+                            if (j + q >= hlo && j + q < hhi)
+                                ok = FUSED ? ext_accept(p, hrow, c, gen_s[h]) : ext_injective(p, hrow, c);
+                            hc += ok ? 1u : 0u;
+                            if (WRITE) tile_append(*tl, ok, hrow, k, c, true);
+                        }
                     }
-                    hc += ok ? 1u : 0u;
-                    if (WRITE) tile_append(*tl, ok, hrow, k, c, true);
+                } else {
+                    for (uint32_t j0 = hlo; j0 < hhi; j0 += 32) {
+                        const uint32_t j = j0 + lane;
+                        bool ok = false;
+                        uint32_t c = 0;
+                        if (j < hhi) {
+                            c = __ldg(hadj + j);
+                            ok = FUSED ? ext_accept(p, hrow, c, gen_s[h]) : ext_injective(p, hrow, c);
+                        }
+                        hc += ok ? 1u : 0u;
+                        if (WRITE) tile_append(*tl, ok, hrow, k, c, true);
+                    }
                 }
                 hc = __reduce_add_sync(0xffffffffu, hc);
                 if (lane == h) cnt += hc;
@@ -1911,7 +1935,9 @@ int run_batch(DevDB& db, std::vector<std::vector<Step>> steps, cudaStream_t s, u
     // thread on its own stream: one half's host work (trie, descriptors,
     // rounds' bookkeeping) overlaps the other's kernels, and the two halves'
     // kernels fill each other's gaps on the device
-    const size_t K = n >= 12288 ? 2 : 1;
+    // (a profiled run keeps one stream: per-kernel event timings of two
+    // overlapping streams would each include the other's kernels)
+    const size_t K = n >= 12288 && !profile ? 2 : 1;
     std::vector<size_t> cut(K + 1);
     for (size_t k = 0; k <= K; ++k) cut[k] = n * k / K;
     const bool per_graph = graph_counts_host || support_host;

@@ -396,9 +396,9 @@ int upload_graph(HostGraph& g, int device, DevDB*& out) {
         }
         if (!packed) pidx.assign(g.parts.size(), {});
     }
-    size_t bytes = 2 * align256(seed_verts.size() * 4 + 4);
+    size_t bytes = 2 * align256(seed_verts.size() * 4 + 16);
     for (size_t i = 0; i < g.parts.size(); ++i)
-        bytes += align256((packed ? pidx[i].size() : g.parts[i].off.size()) * 4) + align256(g.parts[i].adj.size() * 4 + 4);
+        bytes += align256((packed ? pidx[i].size() : g.parts[i].off.size()) * 4) + align256(g.parts[i].adj.size() * 4 + 16);
     void* arena = nullptr;
     cudaError_t e = cudaMalloc(&arena, bytes);
     if (e != cudaSuccess) return fail(GVA_ERR_NOMEM, std::string("database allocation failed: ") + cudaGetErrorString(e));
@@ -415,7 +415,7 @@ int upload_graph(HostGraph& g, int device, DevDB*& out) {
     auto put = [&](const std::vector<uint32_t>& v) -> const uint32_t* {
         const uint32_t* at = (const uint32_t*)cur;
         if (!v.empty()) cudaMemcpy(cur, v.data(), v.size() * 4, cudaMemcpyHostToDevice);
-        cur += align256(v.size() * 4 + 4);
+        cur += align256(v.size() * 4 + 16);
         return at;
     };
     db->seed_verts = put(seed_verts);

@@ -143,24 +143,43 @@ struct GenState {
 };
 
 __device__ __forceinline__ void ext_generator(const ExtArgs& p, const uint32_t* row, GenState& g) {
-    ext_range(p, row, g.slo, g.shi);
-    g.lo = g.slo;
-    g.hi = g.shi;
+    uint32_t slo, shi;
+    seg_of(p.off, p.L, row[p.src_col], p.lab, slo, shi);
     g.gadj = p.adj;
     g.which = -1;
-    for (uint32_t i = 0; i < p.n_chk && g.lo < g.hi; ++i) {
-        if (p.chk_dir[i]) continue;
-        uint32_t l2, h2;
-        seg_of(p.chk_off[i], p.L, row[p.chk_col[i]], p.lab, l2, h2);
-        if (p.bound_col >= 0 && l2 < h2)
-            h2 = lower_bound_u32(p.chk_adj[i], l2, h2, (uint64_t)row[p.bound_col] + p.bound_incl);
-        g.clo[i] = l2;
-        g.chi[i] = h2;
-        if (h2 - l2 < g.hi - g.lo) {
-            g.lo = l2;
-            g.hi = h2;
+    if (slo >= shi) {  // no candidate from the source: nothing else to look up
+        g.lo = g.hi = g.slo = g.shi = slo;
+        return;
+    }
+    // the partners' segments are looked up together (independent loads),
+    // then every segment is cut below the restriction bound
+    uint32_t l2[kMaxChecks], h2[kMaxChecks];
+#pragma unroll
+    for (int i = 0; i < kMaxChecks; ++i) {
+        l2[i] = h2[i] = 0;
+        if (i < (int)p.n_chk && !p.chk_dir[i]) seg_of(p.chk_off[i], p.L, row[p.chk_col[i]], p.lab, l2[i], h2[i]);
+    }
+    if (p.bound_col >= 0) {
+        const uint64_t b = (uint64_t)row[p.bound_col] + p.bound_incl;
+        shi = lower_bound_u32(p.adj, slo, shi, b);
+#pragma unroll
+        for (int i = 0; i < kMaxChecks; ++i)
+            if (i < (int)p.n_chk && !p.chk_dir[i] && l2[i] < h2[i]) h2[i] = lower_bound_u32(p.chk_adj[i], l2[i], h2[i], b);
+    }
+    g.slo = slo;
+    g.shi = shi;
+    g.lo = slo;
+    g.hi = shi;
+#pragma unroll
+    for (int i = 0; i < kMaxChecks; ++i) {
+        if (i >= (int)p.n_chk || p.chk_dir[i]) continue;
+        g.clo[i] = l2[i];
+        g.chi[i] = h2[i];
+        if (h2[i] - l2[i] < g.hi - g.lo) {
+            g.lo = l2[i];
+            g.hi = h2[i];
             g.gadj = p.chk_adj[i];
-            g.which = (int)i;
+            g.which = i;
         }
     }
 }
@@ -187,15 +206,9 @@ __device__ __forceinline__ bool ext_accept(const ExtArgs& p, const uint32_t* row
     return true;
 }
 
-// Number of candidates of one row (segment minus already-matched vertices).
-__device__ __forceinline__ uint32_t ext_count_row(const ExtArgs& p, const uint32_t* row) {
-    if (p.n_chk) {
-        GenState g;
-        ext_generator(p, row, g);
-        uint32_t n = 0;
-        for (uint32_t j = g.lo; j < g.hi; ++j) n += ext_accept(p, row, __ldg(g.gadj + j), g) ? 1u : 0u;
-        return n;
-    }
+// Number of candidates of one row of a plain extension (no fused checks):
+// the segment minus the already-matched vertices in it.
+__device__ __forceinline__ uint32_t ext_count_plain(const ExtArgs& p, const uint32_t* row) {
     uint32_t lo, hi;
     ext_range(p, row, lo, hi);
     if (lo >= hi) return 0;
@@ -224,6 +237,18 @@ __device__ __forceinline__ uint32_t ext_count_row(const ExtArgs& p, const uint32
         if (!dup && find_in(p.adj, lo, hi, w) != 0xffffffffu) --n;
     }
     return n;
+}
+
+// Number of candidates of one row, plain or with fused checks.
+__device__ __forceinline__ uint32_t ext_count_row(const ExtArgs& p, const uint32_t* row) {
+    if (p.n_chk) {
+        GenState g;
+        ext_generator(p, row, g);
+        uint32_t n = 0;
+        for (uint32_t j = g.lo; j < g.hi; ++j) n += ext_accept(p, row, __ldg(g.gadj + j), g) ? 1u : 0u;
+        return n;
+    }
+    return ext_count_plain(p, row);
 }
 
 __device__ __forceinline__ bool red_keep_row(const RedArgs& p, const uint32_t* row) {
