@@ -803,7 +803,7 @@ def batch_bench(args, rank, world, local, dist, torch, gv, workloads):
     clocks.start()
     launches0 = gv.kernel_launches()
     ms, emb_local = [], 0
-    counts = sup = None
+    counts = sup = tstats = None
     for _ in range(args.steps):
         with torch.cuda.stream(stream):
             flush.zero_()  # evict L2 between steps (outside the timed events)
@@ -811,7 +811,7 @@ def batch_bench(args, rank, world, local, dist, torch, gv, workloads):
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record(stream)
-        counts, sup, _ = step()
+        counts, sup, tstats = step()
         e1.record(stream)
         e1.synchronize()
         ms.append(e0.elapsed_time(e1))
@@ -832,6 +832,23 @@ def batch_bench(args, rank, world, local, dist, torch, gv, workloads):
     emb_all = red(emb_local, dist.ReduceOp.SUM if dist else None)
     value = emb_all / (t_sum / 1000.0)
     patterns_per_s = len(queries) * world * args.steps / (t_sum / 1000.0)
+
+    # ---- the same step with every round scheduled on the host (each round's
+    # totals read back before its write pass), for comparison
+    host_ms = []
+    for i in range(3):
+        with torch.cuda.stream(stream):
+            flush.zero_()
+        stream.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        c_h, s_h, _ = gv.batch_count(gdb, plans, stream=sp, support=True, host_rounds=True)
+        e1.record(stream)
+        e1.synchronize()
+        if i:
+            host_ms.append(e0.elapsed_time(e1))
+    host_rounds_agree = bool(np.array_equal(c_h, counts) and np.array_equal(s_h, sup))
 
     # ---- one profiled step: per-kernel CUDA events for the roofline
     with torch.cuda.stream(stream):
@@ -925,9 +942,18 @@ def batch_bench(args, rank, world, local, dist, torch, gv, workloads):
                      "frac": achieved / peak, "peak_source": peak_kind, "traffic": ncu_traffic(name, s),
                      "launches": s["launches"], "kernel_ms": s["ms"]},
         "kernels": kstats,
-        "batch": {k: pstats[k] for k in ("rounds", "splits", "launches", "trie_nodes", "gpu_ms", "lower_ms",
-                                         "submit_ms", "round_host_ms", "round_phase_ms", "wait_ms",
-                                         "session_ms")},
+        # host figures of the last timed step (the profiled step keeps one
+        # stream and synchronises around every kernel)
+        "batch": dict({k: pstats[k] for k in ("rounds", "splits", "launches", "trie_nodes")},
+                      **{k: tstats[k] for k in ("device_rounds", "gpu_ms", "lower_ms", "submit_ms", "round_host_ms",
+                                                "round_phase_ms", "wait_ms", "session_ms", "timeline_ms")},
+                      timeline="ms from the start of the batched run: plans ordered; per half: session prepared, "
+                               "rounds done, results read",
+                      host_rounds={"ms_per_step": statistics.mean(host_ms),
+                                   "embeddings_per_s": emb_local / args.steps / (statistics.mean(host_ms) / 1000.0),
+                                   "agree": host_rounds_agree,
+                                   "path": "the same step with every round scheduled on the host "
+                                           "(GVA_BATCH_HOST_ROUNDS), mean of 2 after 1 warm-up"}),
         "tuning": dict(tuning, calibration=f"first {min(args.tune_patterns, len(plans))} patterns of the list, "
                                            f"counted with supports, each launch shape twice (gva_db_autotune)"),
         "e2e": {"value": e2e_value, "unit": "embeddings/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,

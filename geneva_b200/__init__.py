@@ -91,10 +91,11 @@ class _MineStats(ctypes.Structure):
 
 class _MniOpts(ctypes.Structure):
     _fields_ = [("stream", ctypes.c_void_p), ("cap", ctypes.c_uint32), ("plain", ctypes.c_int),
-                ("profile", ctypes.c_int), ("reserved", ctypes.c_int)]
+                ("profile", ctypes.c_int), ("flags", ctypes.c_int)]
 
 
 BATCH_PLAN_ON_DEVICE = 1
+BATCH_HOST_ROUNDS = 2
 
 
 class _BatchOpts(ctypes.Structure):
@@ -104,7 +105,7 @@ class _BatchOpts(ctypes.Structure):
 
 class _Tuning(ctypes.Structure):
     _fields_ = [("rows_per_item", ctypes.c_uint32), ("hub", ctypes.c_uint32), ("ms", ctypes.c_double),
-                ("default_ms", ctypes.c_double), ("tried", ctypes.c_uint32), ("reserved", ctypes.c_uint32)]
+                ("default_ms", ctypes.c_double), ("tried", ctypes.c_uint32), ("round_region_mb", ctypes.c_uint32)]
 
 
 class _BatchStats(ctypes.Structure):
@@ -112,7 +113,8 @@ class _BatchStats(ctypes.Structure):
                 ("launches", ctypes.c_uint64), ("trie_nodes", ctypes.c_uint64), ("kernels", _KernelStat * 5),
                 ("lower_ms", ctypes.c_double), ("submit_ms", ctypes.c_double), ("round_host_ms", ctypes.c_double),
                 ("wait_ms", ctypes.c_double), ("session_ms", ctypes.c_double),
-                ("round_phase_ms", ctypes.c_double * 5)]
+                ("round_phase_ms", ctypes.c_double * 5), ("timeline_ms", ctypes.c_double * 7),
+                ("device_rounds", ctypes.c_uint64)]
 
 
 class _MniStats(ctypes.Structure):
@@ -246,10 +248,13 @@ class Database:
         """Launch shape of the batched engine's round kernels on this database."""
         t = _Tuning()
         _check(library().gva_db_get_tuning(self._h, ctypes.byref(t)))
-        return {"rows_per_item": int(t.rows_per_item), "hub": int(t.hub)}
+        return {"rows_per_item": int(t.rows_per_item), "hub": int(t.hub),
+                "round_region_mb": int(t.round_region_mb)}
 
-    def set_tuning(self, rows_per_item: int, hub: int) -> None:
-        t = _Tuning(rows_per_item, hub, 0.0, 0.0, 0, 0)
+    def set_tuning(self, rows_per_item: int, hub: int, round_region_mb: int = 0) -> None:
+        """round_region_mb: MiB of each frontier region of device-scheduled
+        rounds (0 keeps the current size)."""
+        t = _Tuning(rows_per_item, hub, 0.0, 0.0, 0, round_region_mb)
         _check(library().gva_db_set_tuning(self._h, ctypes.byref(t)))
 
     def autotune(self, plans, stream: Optional[int] = None) -> dict:
@@ -448,18 +453,20 @@ def match(db: Database, plan: Plan, stream: Optional[int] = None, budget_bytes: 
 
 
 def batch_count(db: Database, plans: Sequence[Plan], stream: Optional[int] = None, budget_bytes: int = 0,
-                graph_counts: bool = False, support: bool = False, profile: bool = False):
+                graph_counts: bool = False, support: bool = False, profile: bool = False,
+                host_rounds: bool = False):
     """Counts embeddings of many plans in shared rounds (gva_batch_count).
 
     Returns (counts[n] uint64, per_graph, stats) where per_graph is the
     [n, num_graphs] uint64 count matrix when graph_counts, else the [n]
-    uint32 supporting-graph counts when support, else None."""
+    uint32 supporting-graph counts when support, else None.  host_rounds:
+    schedule every round on the host (GVA_BATCH_HOST_ROUNDS)."""
     n = len(plans)
     arr = (ctypes.c_void_p * max(n, 1))(*[p._h.value for p in plans])
     counts = np.zeros(n, dtype=np.uint64)
     gc = np.zeros((n, db.num_graphs), dtype=np.uint64) if graph_counts else None
     sup = np.zeros(n, dtype=np.uint32) if support else None
-    o = _BatchOpts(stream or None, budget_bytes, 1 if profile else 0, 0)
+    o = _BatchOpts(stream or None, budget_bytes, 1 if profile else 0, BATCH_HOST_ROUNDS if host_rounds else 0)
     st = _BatchStats()
     _check(library().gva_batch_count(db._h, arr, n, ctypes.byref(o), counts.ctypes.data,
                                      gc.ctypes.data if gc is not None else None,
@@ -471,10 +478,12 @@ def batch_count(db: Database, plans: Sequence[Plan], stream: Optional[int] = Non
 
 
 def _batch_stats_dict(st) -> dict:
-    return {"gpu_ms": st.gpu_ms, "rounds": int(st.rounds), "splits": int(st.splits), "launches": int(st.launches),
+    return {"gpu_ms": st.gpu_ms, "rounds": int(st.rounds), "device_rounds": int(st.device_rounds),
+            "splits": int(st.splits), "launches": int(st.launches),
             "trie_nodes": int(st.trie_nodes), "lower_ms": st.lower_ms, "submit_ms": st.submit_ms,
             "round_host_ms": st.round_host_ms, "wait_ms": st.wait_ms, "session_ms": st.session_ms,
             "round_phase_ms": [float(x) for x in st.round_phase_ms],
+            "timeline_ms": [float(x) for x in st.timeline_ms],
             "kernels": {st.kernels[i].name.decode(): dict(launches=int(st.kernels[i].launches),
                                                           ms=float(st.kernels[i].ms), bytes=float(st.kernels[i].bytes),
                                                           rows=float(st.kernels[i].rows))

@@ -91,6 +91,21 @@ constexpr int kTileRows = 64;           // output rows staged per warp before a 
 constexpr int kScanChunk = 4096;        // items per CTA of the item scan
 constexpr int kScanChunkLog2 = 12;
 
+// Device-side state of one round when the rounds are scheduled on the device
+// (BatchSession::run_device): the count pass's tasks and items (written by
+// the previous round's planning kernel, or by the host for the first round),
+// the write pass's (written by this round's planning kernel) and the four
+// work-queue heads (zero when the state is created).  A set `overflow` makes
+// every later launch of the run find no work.
+struct RunState {
+    uint64_t ni, ni_light;  // count items: all, light class (the light class's items come first)
+    uint64_t wi, wi_light;  // write items: all, light class
+    uint32_t nt, nt_light;  // count tasks: all, light class
+    uint32_t nw;            // writing tasks
+    uint32_t overflow;      // frontier region, task or item capacity exceeded
+    unsigned long long heads[4];  // queue heads: count light, count fused, write light, write fused
+};
+
 struct RoundArgs {
     const TaskDesc* nodes;
     const TaskRef* refs;
@@ -108,12 +123,46 @@ struct RoundArgs {
     uint64_t n_count_items;       // write: items of the count pass
     uint64_t n_chunks;            // write: scan chunks of the count pass
     unsigned long long* queue;    // work-queue head (zeroed before the launch)
-    uint32_t total_warps;         // resident warps of the persistent grid
-    uint32_t pad2;
     uint32_t* const* task_out;    // write: output base of each task (null: not written this round)
     unsigned long long* read_words;  // optional: candidate-list words read (profiling)
     BatchCtx ctx;
+    RunState* dyn;                // device-scheduled rounds: item ranges, task counts and queue heads from
+                                  // here instead of the fields above (null: host-scheduled)
 };
+
+// The item range of one launch: from the arguments (host-scheduled rounds)
+// or from the round's device state.
+struct Span {
+    uint64_t base, n;              // items [base, base + n) of this launch
+    uint64_t n_count_items, n_chunks;  // write pass: items and scan chunks of the count pass
+    unsigned long long* queue;
+    uint32_t nt;                   // tasks (count) or writing tasks (write)
+    uint32_t warps;                // resident warps of the persistent grid
+};
+
+template <bool WRITE>
+__device__ __forceinline__ Span launch_span(const RoundArgs& a, bool fused) {
+    Span s;
+    s.warps = gridDim.x * kRoundWarps;
+    if (!a.dyn) {
+        s.base = a.item_base;
+        s.n = a.n_items;
+        s.nt = a.nt;
+        s.n_count_items = a.n_count_items;
+        s.n_chunks = a.n_chunks;
+        s.queue = a.queue;
+        return s;
+    }
+    const RunState& st = *a.dyn;
+    const uint64_t all = WRITE ? st.wi : st.ni, light = WRITE ? st.wi_light : st.ni_light;
+    s.base = fused ? light : 0;
+    s.n = fused ? all - light : light;
+    s.nt = WRITE ? st.nw : st.nt;
+    s.n_count_items = st.ni;
+    s.n_chunks = (st.ni + kScanChunk - 1) / kScanChunk;
+    s.queue = a.dyn->heads + (WRITE ? 2 : 0) + (fused ? 1 : 0);
+    return s;
+}
 
 // Per-(query, graph) accounting of a final-step row: lanes of a warp whose
 // rows lie in the same graph (rows arrive grouped by their first vertex)
@@ -136,24 +185,24 @@ __device__ __forceinline__ void add_graph_count(const BatchCtx& c, uint32_t quer
 // Guided self-scheduling over a device work queue: a warp takes a chunk of
 // about 1/(2 x resident warps) of the items left (at least one), so the
 // queue sees few atomics while the last items still spread over every SM.
-__device__ __forceinline__ bool next_chunk(const RoundArgs& a, uint64_t& begin, uint64_t& end) {
+__device__ __forceinline__ bool next_chunk(const Span& a, uint64_t& begin, uint64_t& end) {
     const int lane = threadIdx.x & 31;
     unsigned long long b = 0, n = 0;
     if (lane == 0) {
         const unsigned long long head = *(volatile unsigned long long*)a.queue;
-        if (head < a.n_items) {
-            n = (a.n_items - head) / (2ull * a.total_warps);
+        if (head < a.n) {
+            n = (a.n - head) / (2ull * a.warps);
             if (n == 0) n = 1;
             b = atomicAdd(a.queue, n);
         } else {
-            b = a.n_items;
+            b = a.n;
         }
     }
     b = __shfl_sync(0xffffffffu, b, 0);
     n = __shfl_sync(0xffffffffu, n, 0);
     begin = b;
-    end = b + n < a.n_items ? b + n : a.n_items;
-    return begin < a.n_items;
+    end = b + n < a.n ? b + n : a.n;
+    return begin < a.n;
 }
 
 // last t in [0, n) with pfx[t] <= x (pfx ascending, pfx[0] <= x)
@@ -483,10 +532,11 @@ round_count_kernel(RoundArgs a) {
     uint64_t begin, end;
     uint32_t cur = 0;    // light class: buffer of the current item
     bool ready = false;  // light class: the current item's rows were issued with the previous item
-    while (next_chunk(a, begin, end)) {
-        for (uint64_t item = a.item_base + begin; item < a.item_base + end; ++item) {
+    const Span sp = launch_span<false>(a, FUSED);
+    while (next_chunk(sp, begin, end)) {
+        for (uint64_t item = sp.base + begin; item < sp.base + end; ++item) {
             if (item >= t_hi || item < t_lo) {
-                t = find_slot(a.item0, a.nt + 1, item);
+                t = find_slot(a.item0, sp.nt + 1, item);
                 t_lo = __ldg(a.item0 + t);
                 t_hi = __ldg(a.item0 + t + 1);
                 const TaskRef& ref = a.refs[t];
@@ -509,7 +559,7 @@ round_count_kernel(RoundArgs a) {
                     stage_rows_async(rows, in, row0, nr, k);
                 }
                 // the next item of the same task and chunk: its rows are copied in meanwhile
-                ready = item + 1 < a.item_base + end && item + 1 < t_hi;
+                ready = item + 1 < sp.base + end && item + 1 < t_hi;
                 if (ready) {
                     const uint64_t r1 = row0 + a.rows_per_item;
                     stage_rows_async(cur ? ws.rows : ws.rows2, in, r1, (uint32_t)umin64(a.rows_per_item, nrows - r1), k);
@@ -535,12 +585,15 @@ round_count_kernel(RoundArgs a) {
 
 // --------------------------------------------------------- item scans ----
 // Exclusive scan of per-item counts in chunks of kScanChunk (in place);
-// chunks[c] receives chunk c's sum.
+// chunks[c] receives chunk c's sum.  A block per chunk, the grid striding
+// over the chunks (n from the round's device state when `dyn` is given).
 __global__ void __launch_bounds__(1024) scan_items_local_kernel(uint64_t* __restrict__ v, uint64_t n,
-                                                               uint64_t* __restrict__ chunks) {
+                                                               uint64_t* __restrict__ chunks, const RunState* dyn) {
     __shared__ uint64_t ws[32];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    const uint64_t base = (uint64_t)blockIdx.x * kScanChunk + (uint64_t)threadIdx.x * 4;
+    if (dyn) n = dyn->ni;
+    for (uint64_t c = blockIdx.x; c * kScanChunk < n; c += gridDim.x) {
+    const uint64_t base = c * kScanChunk + (uint64_t)threadIdx.x * 4;
     uint64_t x[4];
     uint64_t sum = 0;
 #pragma unroll
@@ -572,7 +625,9 @@ __global__ void __launch_bounds__(1024) scan_items_local_kernel(uint64_t* __rest
         if (base + i < n) v[base + i] = run;
         run += x[i];
     }
-    if (threadIdx.x == 1023) chunks[blockIdx.x] = ws[31];
+    if (threadIdx.x == 1023) chunks[c] = ws[31];
+    __syncthreads();  // ws read by every thread before the next chunk rewrites it
+    }
 }
 
 // Exclusive scan of the chunk sums (chunks[nc] = grand total), then each
@@ -580,8 +635,13 @@ __global__ void __launch_bounds__(1024) scan_items_local_kernel(uint64_t* __rest
 __global__ void __launch_bounds__(1024) scan_items_top_kernel(uint64_t* __restrict__ chunks, uint64_t nc,
                                                              const uint64_t* __restrict__ v, uint64_t n,
                                                              const uint64_t* __restrict__ item0, uint32_t nt,
-                                                             uint64_t* __restrict__ totals) {
+                                                             uint64_t* __restrict__ totals, const RunState* dyn) {
     __shared__ uint64_t ws[32];
+    if (dyn) {
+        n = dyn->ni;
+        nc = (n + kScanChunk - 1) / kScanChunk;
+        nt = dyn->nt;
+    }
     __shared__ uint64_t carry_s;
     if (threadIdx.x == 0) carry_s = 0;
     __syncthreads();
@@ -640,10 +700,11 @@ round_write_kernel(RoundArgs a) {
     uint64_t begin, end;
     uint32_t cur = 0;    // light class: buffer of the current item
     bool ready = false;  // light class: the current item's rows were issued with the previous item
-    while (next_chunk(a, begin, end)) {
-        for (uint64_t wi = a.item_base + begin; wi < a.item_base + end; ++wi) {
+    const Span sp = launch_span<true>(a, FUSED);
+    while (next_chunk(sp, begin, end)) {
+        for (uint64_t wi = sp.base + begin; wi < sp.base + end; ++wi) {
             if (wi >= w_hi || wi < w_lo) {
-                const uint32_t slot = find_slot(a.witem0, a.nt + 1, wi);
+                const uint32_t slot = find_slot(a.witem0, sp.nt + 1, wi);
                 w_lo = __ldg(a.witem0 + slot);
                 w_hi = __ldg(a.witem0 + slot + 1);
                 t = __ldg(a.wtask + slot);
@@ -658,8 +719,8 @@ round_write_kernel(RoundArgs a) {
             }
             const uint64_t item = t_item0 + (wi - w_lo);
             const uint64_t off = a.items[item] + a.chunks[item >> kScanChunkLog2];
-            const uint64_t off_next = item + 1 >= a.n_count_items
-                                          ? a.chunks[a.n_chunks]
+            const uint64_t off_next = item + 1 >= sp.n_count_items
+                                          ? a.chunks[sp.n_chunks]
                                           : a.items[item + 1] + a.chunks[(item + 1) >> kScanChunkLog2];
             const uint64_t row0 = (wi - w_lo) * a.rows_per_item;
             const uint32_t nr = (uint32_t)umin64(a.rows_per_item, nrows - row0);
@@ -683,7 +744,7 @@ round_write_kernel(RoundArgs a) {
                     __syncwarp();
                     stage_rows_async(rows, in, row0, nr, k);
                 }
-                ready = wi + 1 < a.item_base + end && wi + 1 < w_hi;
+                ready = wi + 1 < sp.base + end && wi + 1 < w_hi;
                 if (ready) {
                     const uint64_t r1 = row0 + a.rows_per_item;
                     stage_rows_async(cur ? ws.rows : ws.rows2, in, r1, (uint32_t)umin64(a.rows_per_item, nrows - r1), k);
@@ -709,6 +770,197 @@ round_write_kernel(RoundArgs a) {
             if (tl.n) tile_flush(tl, tl.n);
             __syncwarp();  // every lane done with these rows before the buffer is refilled
         }
+    }
+}
+
+// ------------------------------------------------- device-side planning ----
+// Rounds scheduled on the device (BatchSession::run_device).  Every task of
+// a round sits at the same trie depth (nothing is deferred or split), so a
+// round's tasks are the children of the previous round's writing tasks.
+// Per node: the children that can match, light class first, as a range of
+// the children array, and the words of one output row.
+struct NodeRun {
+    uint32_t child0;
+    uint16_t n_light, n_fused;
+    uint32_t out_w;  // EXT: width + 1; REDUCE: width
+    uint32_t pad;
+};
+
+struct PlanArgs {
+    RunState* st;              // this round
+    RunState* nx;              // the next round
+    const TaskRef* refs;       // this round's tasks (light class first)
+    const uint64_t* item0;     // [nt + 1] this round's count-pass item prefix
+    const uint64_t* totals;    // [nt] output rows per task
+    const NodeRun* info;
+    const uint32_t* children;
+    uint64_t* node_total;      // output rows per node (zeroed before the run)
+    uint32_t* region;          // this round's output frontier region
+    uint64_t region_words;
+    uint32_t** outs;           // [nt] output base per task (null: not written)
+    uint32_t* wtask;           // [nw] count-task index of each writing task
+    uint64_t* witem0;          // [nw + 1] item prefix over the writing tasks
+    TaskRef* next_refs;        // the next round's tasks
+    uint64_t* next_item0;      // [next nt + 1]
+    uint32_t refs_cap;         // capacity of next_refs
+    uint64_t items_cap;        // capacity of the per-item arrays
+    uint32_t rows_next;        // rows per item of the next round
+    uint32_t* overflow;        // set (never cleared) when a capacity is exceeded
+};
+
+constexpr int kPlanThreads = 512;
+constexpr int kPlanVals = 8;
+
+// Task t's contributions: 0 output words (rounded up to 16 bytes), 1 writes,
+// 2 write items, 3 write items of the light class, 4 / 5 light / fused child
+// tasks, 6 / 7 their items.  A task writes when it has output rows and a
+// child that can match.
+__device__ __forceinline__ void plan_values(const PlanArgs& p, uint32_t nt_light, uint32_t t, uint64_t v[kPlanVals],
+                                            uint32_t& node, uint64_t& tot, uint64_t& per) {
+    node = p.refs[t].node;
+    tot = p.totals[t];
+    const NodeRun nr = p.info[node];
+    const bool w = tot > 0 && nr.n_light + nr.n_fused > 0;
+    per = w ? (tot + p.rows_next - 1) / p.rows_next : 0;
+    const uint64_t items = p.item0[t + 1] - p.item0[t];
+    v[0] = w ? ((tot * nr.out_w + 3) & ~3ull) : 0;
+    v[1] = w ? 1 : 0;
+    v[2] = w ? items : 0;
+    v[3] = w && t < nt_light ? items : 0;
+    v[4] = w ? nr.n_light : 0;
+    v[5] = w ? nr.n_fused : 0;
+    v[6] = per * nr.n_light;
+    v[7] = per * nr.n_fused;
+}
+
+// Exclusive block scan of kPlanVals values per thread; sum receives the
+// block totals.
+__device__ __forceinline__ void plan_scan(const uint64_t v[kPlanVals], uint64_t ex[kPlanVals], uint64_t sum[kPlanVals],
+                                          uint64_t (*sh)[kPlanVals]) {
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    constexpr int W = kPlanThreads / 32;
+    uint64_t inc[kPlanVals];
+#pragma unroll
+    for (int k = 0; k < kPlanVals; ++k) {
+        inc[k] = v[k];
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint64_t y = __shfl_up_sync(0xffffffffu, inc[k], o);
+            if (lane >= o) inc[k] += y;
+        }
+    }
+    if (lane == 31)
+        for (int k = 0; k < kPlanVals; ++k) sh[wid][k] = inc[k];
+    __syncthreads();
+    if (wid == 0) {
+#pragma unroll
+        for (int k = 0; k < kPlanVals; ++k) {
+            uint64_t w = lane < W ? sh[lane][k] : 0;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint64_t y = __shfl_up_sync(0xffffffffu, w, o);
+                if (lane >= o) w += y;
+            }
+            if (lane < W) sh[lane][k] = w;
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < kPlanVals; ++k) {
+        ex[k] = (wid > 0 ? sh[wid - 1][k] : 0) + inc[k] - v[k];
+        sum[k] = sh[W - 1][k];
+    }
+    __syncthreads();  // sh read by every thread before the next scan rewrites it
+}
+
+// One block: records every task's output rows (node_total), places the
+// writing tasks' outputs in the round's region, lists them for the write
+// pass, and lists the next round's tasks (their children, light class
+// first) with their item prefix.  A region, task or item capacity exceeded
+// marks the run overflowed: no later launch of the run finds work, and the
+// host runs the session's rounds itself.
+__global__ void __launch_bounds__(kPlanThreads) round_plan_kernel(PlanArgs p) {
+    __shared__ uint64_t sh[kPlanThreads / 32][kPlanVals];
+    __shared__ uint64_t tot_s[kPlanVals];
+    __shared__ uint32_t bad_s;
+    RunState& st = *p.st;
+    RunState& nx = *p.nx;
+    const uint32_t nt = st.overflow ? 0u : st.nt;
+    const uint32_t ntl = st.nt_light;
+    uint64_t v[kPlanVals], ex[kPlanVals], sum[kPlanVals];
+    uint32_t node;
+    uint64_t tot, per;
+    // pass 1: the round's sums
+    uint64_t acc[kPlanVals] = {};
+    for (uint32_t t = threadIdx.x; t < nt; t += kPlanThreads) {
+        plan_values(p, ntl, t, v, node, tot, per);
+#pragma unroll
+        for (int k = 0; k < kPlanVals; ++k) acc[k] += v[k];
+    }
+    plan_scan(acc, ex, sum, sh);
+    if (threadIdx.x == 0) {
+        const bool bad = st.overflow || sum[0] > p.region_words || sum[4] + sum[5] > p.refs_cap ||
+                         sum[6] + sum[7] > p.items_cap;
+        bad_s = bad ? 1u : 0u;
+        if (bad) {
+            st.overflow = 1;
+            st.nw = 0;
+            st.wi = st.wi_light = 0;
+            nx.overflow = 1;
+            nx.nt = nx.nt_light = 0;
+            nx.ni = nx.ni_light = 0;
+            *p.overflow = 1;
+        } else {
+            st.nw = (uint32_t)sum[1];
+            st.wi = sum[2];
+            st.wi_light = sum[3];
+            nx.nt = (uint32_t)(sum[4] + sum[5]);
+            nx.nt_light = (uint32_t)sum[4];
+            nx.ni = sum[6] + sum[7];
+            nx.ni_light = sum[6];
+            p.witem0[sum[1]] = sum[2];
+            p.next_item0[sum[4] + sum[5]] = sum[6] + sum[7];
+        }
+#pragma unroll
+        for (int k = 0; k < kPlanVals; ++k) tot_s[k] = sum[k];
+    }
+    __syncthreads();
+    if (bad_s) return;
+    const uint64_t light_tasks = tot_s[4], light_items = tot_s[6];
+    // pass 2: prefixes, outputs and the next round's tasks
+    uint64_t carry[kPlanVals] = {};
+    for (uint32_t base = 0; base < nt; base += kPlanThreads) {
+        const uint32_t t = base + threadIdx.x;
+#pragma unroll
+        for (int k = 0; k < kPlanVals; ++k) v[k] = 0;
+        tot = per = 0;
+        node = 0;
+        if (t < nt) plan_values(p, ntl, t, v, node, tot, per);
+        plan_scan(v, ex, sum, sh);
+        if (t < nt) {
+            p.node_total[node] = tot;
+            uint32_t* out = nullptr;
+            if (v[1]) {
+                out = p.region + carry[0] + ex[0];
+                const uint64_t slot = carry[1] + ex[1];
+                p.wtask[slot] = t;
+                p.witem0[slot] = carry[2] + ex[2];
+                const NodeRun nr = p.info[node];
+                const uint64_t j0 = carry[4] + ex[4], i0 = carry[6] + ex[6];
+                for (uint32_t i = 0; i < nr.n_light; ++i) {
+                    p.next_refs[j0 + i] = TaskRef{__ldg(p.children + nr.child0 + i), 0u, out, tot};
+                    p.next_item0[j0 + i] = i0 + (uint64_t)i * per;
+                }
+                const uint64_t j1 = light_tasks + carry[5] + ex[5], i1 = light_items + carry[7] + ex[7];
+                for (uint32_t i = 0; i < nr.n_fused; ++i) {
+                    p.next_refs[j1 + i] = TaskRef{__ldg(p.children + nr.child0 + nr.n_light + i), 0u, out, tot};
+                    p.next_item0[j1 + i] = i1 + (uint64_t)i * per;
+                }
+            }
+            p.outs[t] = out;
+        }
+#pragma unroll
+        for (int k = 0; k < kPlanVals; ++k) carry[k] += sum[k];
     }
 }
 
@@ -832,6 +1084,7 @@ int BatchSession::init() {
             return fail(GVA_ERR_ARG, "per-graph results need the database's graph ids (gva_db_set_graphs)");
         ctx_words = (db.num_graphs + 31) / 32;
         const size_t bytes = (want_graph_counts ? (size_t)nslots * db.num_graphs * 8 : 0) + (size_t)nslots * ctx_words * 4;
+        acc_bytes = bytes;
         if (cudaMallocAsync(&acc, bytes, s) != cudaSuccess) return fail(GVA_ERR_NOMEM, "per-graph counters");
         GVA_CUDA_B(cudaMemsetAsync(acc, 0, bytes, s));
         for (uint32_t i = nslots; i > 0; --i) free_slots.push_back((int)i - 1);
@@ -1290,7 +1543,13 @@ int BatchSession::submit(std::vector<std::vector<Step>>&& wave, const std::vecto
         fill(0);
         for (auto& th : pool) th.join();
     }
-    // seeds: the children of every seed node start from its vertex list
+    start_seeds(first_node);
+    return GVA_OK;
+}
+
+// seeds: the children of every seed node from first_node on start from its
+// vertex list
+void BatchSession::start_seeds(int first_node) {
     for (int id = first_node; id < (int)nodes.size(); ++id) {
         if (nodes[id].parent != -1) continue;
         const Step& sd = *node_steps[id];
@@ -1301,7 +1560,6 @@ int BatchSession::submit(std::vector<std::vector<Step>>&& wave, const std::vecto
                 add_task(c, db.seed_verts + db.seed_off[sd.label], n, nullptr);
         try_close(id);
     }
-    return GVA_OK;
 }
 
 int BatchSession::round() {
@@ -1401,16 +1659,9 @@ int BatchSession::round() {
         cap = c;
         return true;
     };
-    const size_t dev_need = nodes.size() * sizeof(TaskDesc);
-    if (dev_need > node_cap) {  // keep the descriptors already shipped
-        void* p = nullptr;
-        const size_t cap = std::max(dev_need, node_cap * 2);
-        if (cudaMallocAsync(&p, cap, s) != cudaSuccess) return fail(GVA_ERR_NOMEM, "node descriptor allocation failed");
-        if (d_nodes && shipped > 0)
-            GVA_CUDA_B(cudaMemcpyAsync(p, d_nodes, shipped * sizeof(TaskDesc), cudaMemcpyDeviceToDevice, s));
-        if (d_nodes) cudaFreeAsync(d_nodes, s);
-        d_nodes = p;
-        node_cap = cap;
+    {
+        const int rc = ship_nodes();
+        if (rc) return rc;
     }
     size_t read_cap = d_read ? 8 : 0;
     if (!grow(&d_desc, desc_cap, ref_bytes) || !grow((void**)&d_items, items_cap, std::max<uint64_t>(ni, 1) * 8) ||
@@ -1423,13 +1674,6 @@ int BatchSession::round() {
     unsigned long long* d_queue = (unsigned long long*)(d_totals + 2 * nt);  // four heads: count and write, per class
     uint64_t* d_wtask = d_totals + 2 * nt + 4;
     uint64_t* d_witem0 = d_wtask + nt;
-    if (shipped < nodes.size()) {  // descriptors of the nodes submitted since the last round
-        // a pageable source: the copy is complete when the call returns, so
-        // the next wave may refill the buffer
-        GVA_CUDA_B(cudaMemcpyAsync((char*)d_nodes + shipped * sizeof(TaskDesc), desc_host.data(),
-                                   (nodes.size() - shipped) * sizeof(TaskDesc), cudaMemcpyHostToDevice, s));
-        shipped = nodes.size();
-    }
     GVA_CUDA_B(cudaMemcpyAsync(d_desc, refs, ref_bytes, cudaMemcpyHostToDevice, s));
     GVA_CUDA_B(cudaMemcpyAsync(d_item0, h_item0, (nt + 1) * 8, cudaMemcpyHostToDevice, s));
     GVA_CUDA_B(cudaMemsetAsync(d_queue, 0, 32, s));
@@ -1464,7 +1708,6 @@ int BatchSession::round() {
         la.queue = d_queue;
         const size_t smem = round_smem_bytes(R, kmax, false, false);
             const uint32_t g = grid_for((const void*)round_count_kernel<false>, ni_light, smem);
-        la.total_warps = g * kRoundWarps;
         round_count_kernel<false><<<g, kRoundWarps * 32, smem, s>>>(la);
         launches += 1;
         g_batch_launches += 1;
@@ -1476,15 +1719,14 @@ int BatchSession::round() {
         fa.queue = d_queue + 1;
         const size_t smem = round_smem_bytes(R, kmax, false, true);
             const uint32_t g = grid_for((const void*)round_count_kernel<true>, ni - ni_light, smem);
-        fa.total_warps = g * kRoundWarps;
         round_count_kernel<true><<<g, kRoundWarps * 32, smem, s>>>(fa);
         launches += 1;
         g_batch_launches += 1;
     }
     if (pf) pf->end(ev, K_EXT_COUNT, cbytes, s, crows);
     if (pf) pf->begin(K_SCAN, 16.0 * ni, s, ev);
-    scan_items_local_kernel<<<(unsigned)nc, 1024, 0, s>>>(d_items, ni, d_chunks);
-    scan_items_top_kernel<<<1, 1024, 0, s>>>(d_chunks, nc, d_items, ni, d_item0, (uint32_t)nt, d_totals);
+    scan_items_local_kernel<<<(unsigned)nc, 1024, 0, s>>>(d_items, ni, d_chunks, nullptr);
+    scan_items_top_kernel<<<1, 1024, 0, s>>>(d_chunks, nc, d_items, ni, d_item0, (uint32_t)nt, d_totals, nullptr);
     if (pf) pf->end(ev, K_SCAN, 16.0 * ni, s, (double)ni);
     launches += 2;
     g_batch_launches += 2;
@@ -1608,8 +1850,7 @@ int BatchSession::round() {
             la.queue = d_queue + 2;
             const size_t smem = round_smem_bytes(R, kmax, true, false);
             const uint32_t g = grid_for((const void*)round_write_kernel<false>, wi_light, smem);
-            la.total_warps = g * kRoundWarps;
-            round_write_kernel<false><<<g, kRoundWarps * 32, smem, s>>>(la);
+                round_write_kernel<false><<<g, kRoundWarps * 32, smem, s>>>(la);
             launches += 1;
             g_batch_launches += 1;
         }
@@ -1620,8 +1861,7 @@ int BatchSession::round() {
             fa.queue = d_queue + 3;
             const size_t smem = round_smem_bytes(R, kmax, true, true);
             const uint32_t g = grid_for((const void*)round_write_kernel<true>, wi - wi_light, smem);
-            fa.total_warps = g * kRoundWarps;
-            round_write_kernel<true><<<g, kRoundWarps * 32, smem, s>>>(fa);
+                round_write_kernel<true><<<g, kRoundWarps * 32, smem, s>>>(fa);
             launches += 1;
             g_batch_launches += 1;
         }
@@ -1654,6 +1894,308 @@ int BatchSession::round() {
             kstat[i].rows += pf->stat[i].rows;
         }
     }
+    return GVA_OK;
+}
+
+int BatchSession::ship_nodes() {
+    const size_t dev_need = nodes.size() * sizeof(TaskDesc);
+    if (dev_need > node_cap) {  // keep the descriptors already shipped
+        void* p = nullptr;
+        const size_t cap = std::max(dev_need, node_cap * 2);
+        if (cudaMallocAsync(&p, cap, s) != cudaSuccess) return fail(GVA_ERR_NOMEM, "node descriptor allocation failed");
+        if (d_nodes && shipped > 0)
+            GVA_CUDA_B(cudaMemcpyAsync(p, d_nodes, shipped * sizeof(TaskDesc), cudaMemcpyDeviceToDevice, s));
+        if (d_nodes) cudaFreeAsync(d_nodes, s);
+        d_nodes = p;
+        node_cap = cap;
+    }
+    if (shipped < nodes.size()) {  // descriptors of the nodes submitted since the last shipment
+        // a pageable source: the copy is complete when the call returns, so
+        // the next wave may refill the buffer
+        GVA_CUDA_B(cudaMemcpyAsync((char*)d_nodes + shipped * sizeof(TaskDesc), desc_host.data(),
+                                   (nodes.size() - shipped) * sizeof(TaskDesc), cudaMemcpyHostToDevice, s));
+        shipped = nodes.size();
+    }
+    return GVA_OK;
+}
+
+int BatchSession::run_device() {
+    if (host_rounds || profile || waves.size() != 1 || rounds != 0 || active.empty() || !db.seed_verts) return GVA_OK;
+    const auto t_start = std::chrono::steady_clock::now();
+    double wait_before = wait_ms;
+    struct Timer {
+        std::chrono::steady_clock::time_point t0;
+        double& acc;
+        double& wait;
+        double wait0;
+        ~Timer() {
+            acc += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count() -
+                   (wait - wait0);
+        }
+    } timer{t_start, round_host_ms, wait_ms, wait_before};
+    const size_t nn = nodes.size();
+    for (const BTask& tk : active)
+        if (nodes[tk.node].depth != 1) return GVA_OK;
+    int D = 0;
+    for (const BNode& nd : nodes) D = std::max(D, nd.depth);
+    if (D < 1) return GVA_OK;
+    // per depth: widest input row, nodes, nodes of each class
+    std::vector<uint32_t> kmax(D + 2, 1), at_depth(D + 2, 0), light_at(D + 2, 0), fused_at(D + 2, 0);
+    for (const BNode& nd : nodes) {
+        kmax[nd.depth] = std::max(kmax[nd.depth], nd.width_in);
+        at_depth[nd.depth]++;
+        (nd.fused ? fused_at : light_at)[nd.depth]++;
+    }
+    uint32_t refs_cap = 1;
+    for (int d = 1; d <= D; ++d) refs_cap = std::max(refs_cap, at_depth[d]);
+    std::vector<uint32_t> R(D + 2, 32);
+    for (int d = 1; d <= D; ++d)
+        R[d] = std::min<uint32_t>(tune.rows_per_item, std::max<uint32_t>(32, (768 / kmax[d]) & ~31u));
+    // children that can match, light class first
+    std::vector<NodeRun> info(nn);
+    std::vector<uint32_t> kids;
+    kids.reserve(nn);
+    for (size_t id = 0; id < nn; ++id) {
+        const BNode& nd = nodes[id];
+        NodeRun r{};
+        r.child0 = (uint32_t)kids.size();
+        r.out_w = nd.kind == STEP_EXT ? nd.width_in + 1 : nd.width_in;
+        size_t cnt[2] = {0, 0};
+        for (uint32_t f = 0; f < 2; ++f)
+            for (int c = nd.first_child; c >= 0; c = nodes[c].next_sibling)
+                if (!nodes[c].always_empty && nodes[c].fused == f) {
+                    kids.push_back((uint32_t)c);
+                    cnt[f]++;
+                }
+        if (cnt[0] > 0xffff || cnt[1] > 0xffff) return GVA_OK;  // beyond the schedule's child counts
+        r.n_light = (uint16_t)cnt[0];
+        r.n_fused = (uint16_t)cnt[1];
+        info[id] = r;
+    }
+    // the first round's tasks (depth 1, from the seed lists), light class first
+    std::vector<TaskRef> r0;
+    r0.reserve(active.size());
+    uint32_t nt_light0 = 0;
+    for (uint32_t f = 0; f < 2; ++f) {
+        for (const BTask& tk : active) {
+            const BNode& nd = nodes[tk.node];
+            if (nd.always_empty || nd.fused != f || tk.rows == 0) continue;
+            r0.push_back(TaskRef{(uint32_t)tk.node, 0u, tk.in, tk.rows});
+        }
+        if (f == 0) nt_light0 = (uint32_t)r0.size();
+    }
+    std::vector<uint64_t> i0(r0.size() + 1, 0);
+    uint64_t ni_light0 = 0;
+    for (size_t t = 0; t < r0.size(); ++t) {
+        i0[t + 1] = i0[t] + (r0[t].nrows + R[1] - 1) / R[1];
+        if (t + 1 == nt_light0) ni_light0 = i0[t + 1];
+    }
+    // two frontier regions (a round writes one while its tasks read the other)
+    uint64_t region = db.round_region_bytes.load();
+    if (region == 0) region = 2ull << 30;
+    if (2 * region > budget) return GVA_OK;
+    const uint64_t region_words = region / 4;
+    const uint64_t items_cap = std::max<uint64_t>(i0.back(), region_words / 64 + refs_cap) + 1;
+    const uint64_t chunks_cap = items_cap / kScanChunk + 2;
+    // one block for the schedule's small arrays
+    auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
+    const size_t o_state = 0;
+    const size_t o_refs0 = o_state + al((D + 2) * sizeof(RunState));
+    const size_t o_refs1 = o_refs0 + al((size_t)refs_cap * sizeof(TaskRef));
+    const size_t o_item00 = o_refs1 + al((size_t)refs_cap * sizeof(TaskRef));
+    const size_t o_item01 = o_item00 + al(((size_t)refs_cap + 1) * 8);
+    const size_t o_totals = o_item01 + al(((size_t)refs_cap + 1) * 8);
+    const size_t o_outs = o_totals + al((size_t)refs_cap * 8);
+    const size_t o_wtask = o_outs + al((size_t)refs_cap * 8);
+    const size_t o_witem0 = o_wtask + al((size_t)refs_cap * 4);
+    const size_t o_ntot = o_witem0 + al(((size_t)refs_cap + 1) * 8);
+    const size_t o_info = o_ntot + al(nn * 8);
+    const size_t o_kids = o_info + al(nn * sizeof(NodeRun));
+    const size_t o_flag = o_kids + al(std::max<size_t>(kids.size(), 1) * 4);
+    const size_t o_items = o_flag + 256;
+    const size_t o_chunks = o_items + al(items_cap * 8);
+    const size_t small_bytes = o_chunks + al((chunks_cap + 1) * 8);
+    {
+        const int rc = ship_nodes();
+        if (rc) return rc;
+    }
+    char* blk = nullptr;
+    void* reg[2] = {nullptr, nullptr};
+    if (cudaMallocAsync((void**)&blk, small_bytes, s) != cudaSuccess) {  // no room: host rounds
+        cudaGetLastError();
+        return GVA_OK;
+    }
+    if (cudaMallocAsync(&reg[0], region, s) != cudaSuccess || cudaMallocAsync(&reg[1], region, s) != cudaSuccess) {
+        cudaGetLastError();
+        for (void* q : {(void*)blk, reg[0], reg[1]})
+            if (q) cudaFreeAsync(q, s);
+        return GVA_OK;
+    }
+    auto free_all = [&]() {
+        for (void* q : {(void*)blk, reg[0], reg[1]}) cudaFreeAsync(q, s);
+    };
+    RunState* states = (RunState*)(blk + o_state);
+    TaskRef* refs[2] = {(TaskRef*)(blk + o_refs0), (TaskRef*)(blk + o_refs1)};
+    uint64_t* item0[2] = {(uint64_t*)(blk + o_item00), (uint64_t*)(blk + o_item01)};
+    uint64_t* totals = (uint64_t*)(blk + o_totals);
+    uint32_t** outs = (uint32_t**)(blk + o_outs);
+    uint32_t* wtask = (uint32_t*)(blk + o_wtask);
+    uint64_t* witem0 = (uint64_t*)(blk + o_witem0);
+    uint64_t* ntot = (uint64_t*)(blk + o_ntot);
+    NodeRun* d_info = (NodeRun*)(blk + o_info);
+    uint32_t* d_kids = (uint32_t*)(blk + o_kids);
+    uint32_t* d_flag = (uint32_t*)(blk + o_flag);
+    uint64_t* items = (uint64_t*)(blk + o_items);
+    uint64_t* chunks = (uint64_t*)(blk + o_chunks);
+    RunState s1{};
+    s1.ni = i0.back();
+    s1.ni_light = ni_light0;
+    s1.nt = (uint32_t)r0.size();
+    s1.nt_light = nt_light0;
+    // pageable sources: each copy is complete when its call returns
+    GVA_CUDA_B(cudaMemsetAsync(blk + o_state, 0, (D + 2) * sizeof(RunState), s));
+    GVA_CUDA_B(cudaMemsetAsync(ntot, 0, nn * 8, s));
+    GVA_CUDA_B(cudaMemsetAsync(d_flag, 0, 4, s));
+    GVA_CUDA_B(cudaMemcpyAsync(states + 1, &s1, sizeof s1, cudaMemcpyHostToDevice, s));
+    GVA_CUDA_B(cudaMemcpyAsync(d_info, info.data(), nn * sizeof(NodeRun), cudaMemcpyHostToDevice, s));
+    if (!kids.empty()) GVA_CUDA_B(cudaMemcpyAsync(d_kids, kids.data(), kids.size() * 4, cudaMemcpyHostToDevice, s));
+    if (!r0.empty()) GVA_CUDA_B(cudaMemcpyAsync(refs[1], r0.data(), r0.size() * sizeof(TaskRef), cudaMemcpyHostToDevice, s));
+    GVA_CUDA_B(cudaMemcpyAsync(item0[1], i0.data(), i0.size() * 8, cudaMemcpyHostToDevice, s));
+
+    BatchCtx ctx{};
+    ctx.vgraph = db.vgraph;
+    ctx.G = db.num_graphs;
+    ctx.words = ctx_words;
+    ctx.graph_counts = graph_counts_dev();
+    ctx.graph_bits = graph_bits_dev();
+    auto grid = [&](const void* fn, size_t smem) -> uint32_t {
+        int per_sm = 1;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kRoundWarps * 32, smem);
+        return (uint32_t)(std::max(per_sm, 1) * sms);
+    };
+    uint64_t nl = 0;
+    for (int d = 1; d <= D; ++d) {
+        const int b = d & 1;
+        RoundArgs ra{};
+        ra.nodes = (const TaskDesc*)d_nodes;
+        ra.refs = refs[b];
+        ra.item0 = item0[b];
+        ra.rows_per_item = R[d];
+        ra.hub = tune.hub;
+        ra.kmax = kmax[d];
+        ra.items = items;
+        ra.ctx = ctx;
+        ra.dyn = states + d;
+        if (light_at[d]) {
+            const size_t smem = round_smem_bytes(R[d], kmax[d], false, false);
+            round_count_kernel<false><<<grid((const void*)round_count_kernel<false>, smem), kRoundWarps * 32, smem, s>>>(ra);
+            ++nl;
+        }
+        if (fused_at[d]) {
+            const size_t smem = round_smem_bytes(R[d], kmax[d], false, true);
+            round_count_kernel<true><<<grid((const void*)round_count_kernel<true>, smem), kRoundWarps * 32, smem, s>>>(ra);
+            ++nl;
+        }
+        scan_items_local_kernel<<<2 * sms, 1024, 0, s>>>(items, 0, chunks, states + d);
+        scan_items_top_kernel<<<1, 1024, 0, s>>>(chunks, 0, items, 0, item0[b], 0, totals, states + d);
+        PlanArgs pa{};
+        pa.st = states + d;
+        pa.nx = states + d + 1;
+        pa.refs = refs[b];
+        pa.item0 = item0[b];
+        pa.totals = totals;
+        pa.info = d_info;
+        pa.children = d_kids;
+        pa.node_total = ntot;
+        pa.region = (uint32_t*)reg[b];
+        pa.region_words = region_words;
+        pa.outs = outs;
+        pa.wtask = wtask;
+        pa.witem0 = witem0;
+        pa.next_refs = refs[b ^ 1];
+        pa.next_item0 = item0[b ^ 1];
+        pa.refs_cap = refs_cap;
+        pa.items_cap = items_cap;
+        pa.rows_next = R[d + 1];
+        pa.overflow = d_flag;
+        round_plan_kernel<<<1, kPlanThreads, 0, s>>>(pa);
+        nl += 3;
+        if (d < D) {  // the deepest round's tasks have no children
+            RoundArgs wa = ra;
+            wa.wtask = wtask;
+            wa.witem0 = witem0;
+            wa.chunks = chunks;
+            wa.task_out = outs;
+            if (light_at[d]) {
+                const size_t smem = round_smem_bytes(R[d], kmax[d], true, false);
+                round_write_kernel<false><<<grid((const void*)round_write_kernel<false>, smem), kRoundWarps * 32, smem, s>>>(wa);
+                ++nl;
+            }
+            if (fused_at[d]) {
+                const size_t smem = round_smem_bytes(R[d], kmax[d], true, true);
+                round_write_kernel<true><<<grid((const void*)round_write_kernel<true>, smem), kRoundWarps * 32, smem, s>>>(wa);
+                ++nl;
+            }
+        }
+    }
+    launches += nl;
+    g_batch_launches += nl;
+    {
+        const cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) {
+            free_all();
+            return fail(GVA_ERR_CUDA, std::string("device-scheduled rounds: ") + cudaGetErrorString(e));
+        }
+    }
+    char* h = staging.get(nn * 8 + 16);
+    if (!h) {
+        free_all();
+        return fail(GVA_ERR_NOMEM, "pinned staging allocation failed");
+    }
+    uint64_t* h_tot = (uint64_t*)h;
+    uint32_t* h_flag = (uint32_t*)(h + nn * 8);
+    GVA_CUDA_B(cudaMemcpyAsync(h_tot, ntot, nn * 8, cudaMemcpyDeviceToHost, s));
+    GVA_CUDA_B(cudaMemcpyAsync(h_flag, d_flag, 4, cudaMemcpyDeviceToHost, s));
+    free_all();
+    {
+        const auto w0 = std::chrono::steady_clock::now();
+        const cudaError_t e = cudaStreamSynchronize(s);
+        wait_ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - w0).count();
+        if (e != cudaSuccess) return fail(GVA_ERR_CUDA, cudaGetErrorString(e));
+    }
+    if (*h_flag) {
+        // a round outgrew a region: later runs get regions twice as large, and
+        // this one starts over with host-scheduled rounds
+        uint64_t cur = db.round_region_bytes.load();
+        while (cur < 2 * region && !db.round_region_bytes.compare_exchange_weak(cur, 2 * region)) {
+        }
+        if (acc) GVA_CUDA_B(cudaMemsetAsync(acc, 0, acc_bytes, s));
+        for (BNode& nd : nodes) {
+            nd.at = 0;
+            nd.closed = false;
+        }
+        for (PlanRec& pr : plans) {
+            pr.count = 0;
+            pr.done = false;
+        }
+        completed.clear();
+        active.clear();
+        start_seeds(0);
+        return GVA_OK;
+    }
+    for (size_t q = 0; q < plans.size(); ++q) {
+        PlanRec& pr = plans[q];
+        pr.count = h_tot[pr.terminal];
+        pr.done = true;
+        completed.push_back((int)q);
+    }
+    for (BNode& nd : nodes) {
+        nd.at = 0;
+        nd.closed = true;
+    }
+    active.clear();
+    rounds += (uint64_t)D;
+    device_rounds += (uint64_t)D;
     return GVA_OK;
 }
 
@@ -1727,7 +2269,8 @@ __global__ void slot_popcount_kernel(const uint32_t* __restrict__ bits, uint32_t
 }
 
 int prepare_batch(DevDB& db, std::vector<std::vector<Step>>&& steps, cudaStream_t s, uint64_t budget,
-                  bool per_graph, bool graph_counts, bool profile, PreparedBatch& out, bool presorted) {
+                  bool per_graph, bool graph_counts, bool profile, PreparedBatch& out, bool presorted,
+                  bool host_rounds) {
     const auto t0 = std::chrono::steady_clock::now();
     GVA_CUDA_B(cudaSetDevice(db.device));
     out.nq = (int)steps.size();
@@ -1736,6 +2279,7 @@ int prepare_batch(DevDB& db, std::vector<std::vector<Step>>&& steps, cudaStream_
     out.ids.clear();
     if (out.nq == 0) return GVA_OK;
     out.ses.reset(new BatchSession(db, s, budget, per_graph ? (uint32_t)out.nq : 0, graph_counts, profile));
+    out.ses->host_rounds = host_rounds;
     int rc = out.ses->init();
     if (!rc) rc = out.ses->submit(std::move(steps), {}, &out.ids, presorted);
     out.prep_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
@@ -1765,6 +2309,7 @@ int finish_batch(DevDB& db, PreparedBatch& pb, uint64_t* counts, uint64_t* graph
     GVA_CUDA_B(cudaEventRecord(tev[dev][0], s));
     int rc = GVA_OK;
     const auto t_loop0 = std::chrono::steady_clock::now();
+    if (!(cancel && *cancel)) rc = ses.run_device();
     while (!rc && !ses.idle()) {
         if (cancel && *cancel) {
             rc = fail(GVA_ERR_CANCELLED, "cancelled");
@@ -1773,6 +2318,7 @@ int finish_batch(DevDB& db, PreparedBatch& pb, uint64_t* counts, uint64_t* graph
         rc = ses.round();
     }
     const double loop_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_loop0).count();
+    if (stats) stats->loop_end_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_fin0).count();
     const std::vector<int>& ids = pb.ids;
     if (!rc) {
         for (int q = 0; q < nq; ++q) counts[at(q)] = ses.plan(ids[q]).count;
@@ -1817,6 +2363,7 @@ int finish_batch(DevDB& db, PreparedBatch& pb, uint64_t* counts, uint64_t* graph
         stats->round_host_ms = ses.round_host_ms;
         stats->wait_ms = ses.wait_ms;
         stats->rounds = ses.rounds;
+        stats->device_rounds = ses.device_rounds;
         stats->splits = ses.splits;
         stats->launches = ses.launches;
         stats->nodes = ses.num_nodes();
@@ -1920,7 +2467,7 @@ static void order_by_step_keys(const std::vector<std::vector<Step>>& steps, std:
 
 int run_batch(DevDB& db, std::vector<std::vector<Step>> steps, cudaStream_t s, uint64_t budget,
               const uint32_t* vgraph, uint32_t G, uint64_t* counts, uint64_t* graph_counts_host,
-              uint32_t* support_host, bool profile, BatchStats* stats) {
+              uint32_t* support_host, bool profile, BatchStats* stats, bool host_rounds) {
     (void)vgraph;
     (void)G;
     const auto t0 = std::chrono::steady_clock::now();
@@ -1954,9 +2501,14 @@ int run_batch(DevDB& db, std::vector<std::vector<Step>> steps, cudaStream_t s, u
         std::vector<std::vector<Step>> part(std::make_move_iterator(sorted.begin() + cut[k]),
                                             std::make_move_iterator(sorted.begin() + cut[k + 1]));
         int r = prepare_batch(db, std::move(part), streams[k], budget, per_graph, graph_counts_host != nullptr,
-                              profile, pb, true);
+                              profile, pb, true, host_rounds);
+        const double t_prep = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
         // results straight to the caller's arrays, at each plan's index before sorting
         if (!r) r = finish_batch(db, pb, counts, graph_counts_host, support_host, &bss[k], nullptr, order.data() + cut[k]);
+        bss[k].timeline_ms[1 + 3 * k] = t_prep;
+        bss[k].timeline_ms[2 + 3 * k] = t_prep + bss[k].loop_end_ms;
+        bss[k].timeline_ms[3 + 3 * k] =
+            std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
         rcs[k] = r;
         if (r) errs[k] = last_error_cstr();
     };
@@ -1977,10 +2529,12 @@ int run_batch(DevDB& db, std::vector<std::vector<Step>> steps, cudaStream_t s, u
         total.wait_ms += bs.wait_ms;
         total.session_ms += bs.session_ms;
         total.rounds += bs.rounds;
+        total.device_rounds += bs.device_rounds;
         total.splits += bs.splits;
         total.launches += bs.launches;
         total.nodes += bs.nodes;
         for (int i = 0; i < 5; ++i) total.phase_ms[i] += bs.phase_ms[i];
+        for (int i = 1; i < 7; ++i) total.timeline_ms[i] += bs.timeline_ms[i];
         for (int i = 0; i < K_NUM; ++i) {
             total.kstat[i].launches += bs.kstat[i].launches;
             total.kstat[i].ms += bs.kstat[i].ms;
@@ -1988,6 +2542,7 @@ int run_batch(DevDB& db, std::vector<std::vector<Step>> steps, cudaStream_t s, u
             total.kstat[i].rows += bs.kstat[i].rows;
         }
     }
+    total.timeline_ms[0] = order_ms;
     if (stats) *stats = total;
     if (rc) return rc;
     if (stats) stats->submit_ms += order_ms;

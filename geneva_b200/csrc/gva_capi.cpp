@@ -454,6 +454,8 @@ void fill_batch_stats(const BatchStats& bs, double lower_ms, gva_batch_stats* st
     stats->wait_ms = bs.wait_ms;
     stats->session_ms = bs.session_ms;
     for (int i = 0; i < 5; ++i) stats->round_phase_ms[i] = bs.phase_ms[i];
+    for (int i = 0; i < 7; ++i) stats->timeline_ms[i] = bs.timeline_ms[i];
+    stats->device_rounds = bs.device_rounds;
     for (int i = 0; i < K_NUM && i < 5; ++i) {
         strncpy(stats->kernels[i].name, kKernelNames[i], sizeof stats->kernels[i].name - 1);
         stats->kernels[i].launches = bs.kstat[i].launches;
@@ -481,7 +483,8 @@ int gva_batch_count(gva_db* db, const gva_plan* const* plans, int nplans, const 
     BatchStats bs;
     int st = run_batch(*db->dev, std::move(steps), (cudaStream_t)o.stream, o.budget_bytes, db->dev->vgraph,
                        db->dev->num_graphs,
-                       counts, graph_counts, graph_support, o.profile != 0, &bs);
+                       counts, graph_counts, graph_support, o.profile != 0, &bs,
+                       (o.flags & GVA_BATCH_HOST_ROUNDS) != 0);
     if (stats) fill_batch_stats(bs, lower_ms, stats);
     return st;
 }
@@ -606,7 +609,8 @@ int gva_batch_count_texts(gva_db* db, const char* const* texts, int n, int mode,
     const double lower_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_lower).count();
     BatchStats bs;
     int rc = n ? run_batch(*db->dev, std::move(steps), (cudaStream_t)o.stream, o.budget_bytes, db->dev->vgraph,
-                           db->dev->num_graphs, counts, graph_counts, graph_support, o.profile != 0, &bs)
+                           db->dev->num_graphs, counts, graph_counts, graph_support, o.profile != 0, &bs,
+                           (o.flags & GVA_BATCH_HOST_ROUNDS) != 0)
                : GVA_OK;
     if (stats) fill_batch_stats(bs, lower_ms, stats);
     if (rc) return rc;
@@ -619,6 +623,8 @@ int gva_db_get_tuning(const gva_db* db, gva_tuning* out) {
     memset(out, 0, sizeof *out);
     out->rows_per_item = db->dev->tune_rows_per_item;
     out->hub = db->dev->tune_hub;
+    const uint64_t region = db->dev->round_region_bytes.load();
+    out->round_region_mb = (uint32_t)((region ? region : (2ull << 30)) >> 20);
     return GVA_OK;
 }
 
@@ -628,6 +634,7 @@ int gva_db_set_tuning(gva_db* db, const gva_tuning* t) {
         return fail(GVA_ERR_ARG, "rows_per_item must be 32, 64 or 128");  // hub: any value (0: every row shared)
     db->dev->tune_rows_per_item = t->rows_per_item;
     db->dev->tune_hub = t->hub;
+    if (t->round_region_mb) db->dev->round_region_bytes.store((uint64_t)t->round_region_mb << 20);
     return GVA_OK;
 }
 

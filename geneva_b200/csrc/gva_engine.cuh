@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <array>
+#include <atomic>
 #include <cstdint>
 #include <memory>
 #include <string>
@@ -43,6 +44,9 @@ struct DevDB {
     // frontier budget of batched runs given none: 3/4 of the device memory
     // free when the first such run started (querying it costs a driver call)
     uint64_t default_budget = 0;
+    // device-scheduled rounds (BatchSession::run_device): bytes of each of a
+    // run's two frontier regions; doubled after a run that overflowed them
+    std::atomic<uint64_t> round_region_bytes{0};
 };
 
 int upload_graph(HostGraph& g, int device, DevDB*& out);
@@ -93,7 +97,12 @@ struct BatchStats {
     double phase_ms[5] = {0, 0, 0, 0, 0};
     double session_ms = 0.0;  // session set-up, support read-back and tear-down
     uint64_t rounds = 0, splits = 0, launches = 0, nodes = 0;
+    uint64_t device_rounds = 0;
     KernelStat kstat[K_NUM];
+    // wall-clock marks of one run (ms from its start): plans ordered, then
+    // per half (two at most) session prepared, rounds done, results read
+    double timeline_ms[7] = {0, 0, 0, 0, 0, 0, 0};
+    double loop_end_ms = 0.0;  // finish_batch: rounds done, ms after its start
 };
 
 // Counts the embeddings of many plans in shared rounds.  counts[q] always;
@@ -105,7 +114,7 @@ size_t step_key_bytes(const Step& st, uint8_t* buf);
 
 int run_batch(DevDB& db, std::vector<std::vector<Step>> steps, cudaStream_t s, uint64_t budget,
               const uint32_t* vgraph, uint32_t G, uint64_t* counts, uint64_t* graph_counts_host,
-              uint32_t* support_host, bool profile, BatchStats* stats);
+              uint32_t* support_host, bool profile, BatchStats* stats, bool host_rounds = false);
 uint64_t batch_kernel_launches();
 
 // Pinned host staging, grown on demand.
@@ -166,6 +175,14 @@ public:
         return submit(std::move(copy), tags, ids, presorted);
     }
     int round();
+    // Runs every round of a single-wave session on the device: each round's
+    // planning kernel chooses the writing tasks, places their outputs and
+    // lists the next round's tasks, so the host launches all rounds at once
+    // and synchronises once.  Leaves the session idle with every plan's count
+    // set; or, when the session does not qualify (several waves, profiling,
+    // rounds already run, a budget below the frontier regions) or a round
+    // overflowed its region, leaves the initial tasks active for round().
+    int run_device();
     bool idle() const { return active.empty(); }
     std::vector<int> take_completed();
     const PlanRec& plan(int q) const { return plans[q]; }
@@ -192,6 +209,8 @@ public:
     } tune;
 
     uint64_t rounds = 0, splits = 0, launches = 0;
+    uint64_t device_rounds = 0;  // rounds scheduled on the device (run_device)
+    bool host_rounds = false;    // run_device declines: every round scheduled on the host
     double submit_ms = 0, round_host_ms = 0, wait_ms = 0;  // host time split
     // round_host_ms by part: task scan + uploads, count launches, totals and
     // budget choice, write launch, next tasks and completion
@@ -200,6 +219,8 @@ public:
 
 private:
     void add_task(int node, const uint32_t* in, uint64_t rows, std::shared_ptr<void> owner);
+    void start_seeds(int first_node);  // tasks of the seed nodes' children, from the seed vertex lists
+    int ship_nodes();                  // descriptors of nodes submitted since the last shipment
     void fill_node_desc(int id, void* out) const;
     void finish_task(int node);
     void try_close(int node);
@@ -212,6 +233,7 @@ private:
     bool profile;
     bool per_graph = false;
     uint32_t ctx_words = 0;
+    size_t acc_bytes = 0;  // per-graph counters and bitmaps (acc)
     int sms = 148;
     void* acc = nullptr;
     std::vector<int> free_slots;
@@ -251,8 +273,11 @@ struct PreparedBatch {
     bool per_graph = false, graph_counts = false;
     double prep_ms = 0.0;
 };
+// host_rounds: finish_batch schedules every round on the host (else on the
+// device when the session qualifies, BatchSession::run_device)
 int prepare_batch(DevDB& db, std::vector<std::vector<Step>>&& steps, cudaStream_t s, uint64_t budget,
-                  bool per_graph, bool graph_counts, bool profile, PreparedBatch& out, bool presorted = false);
+                  bool per_graph, bool graph_counts, bool profile, PreparedBatch& out, bool presorted = false,
+                  bool host_rounds = false);
 // order (optional): plan q's results go to index order[q] of the arrays
 int finish_batch(DevDB& db, PreparedBatch& pb, uint64_t* counts, uint64_t* graph_counts_host, uint32_t* support_host,
                  BatchStats* stats, const volatile int* cancel = nullptr, const uint32_t* order = nullptr);

@@ -180,6 +180,14 @@ typedef struct gva_batch_opts {
  * planner, one query per thread; queries of up to 16 vertices and 32 edge
  * lines, DV mode), the others on the host */
 #define GVA_BATCH_PLAN_ON_DEVICE 1
+/* schedule every round on the host: each round's task totals are read back
+ * and the host chooses the writing tasks, their output places (splitting
+ * tasks larger than the budget) and the next round's tasks.  By default a
+ * run of one batch schedules its rounds on the device (a planning kernel per
+ * round; the host launches every round at once) when the budget holds two
+ * frontier regions, and falls back to host scheduling when a round outgrows
+ * its region. */
+#define GVA_BATCH_HOST_ROUNDS 2
 
 typedef struct gva_batch_stats {
     double gpu_ms;
@@ -193,6 +201,15 @@ typedef struct gva_batch_stats {
     /* round_host_ms by part: task list and uploads, count launches, totals
      * and budget choice, write launch, next tasks and completion */
     double round_phase_ms[5];
+    /* wall-clock marks of the run (ms from the call's start of the batched
+     * run): plans ordered; then for each of up to two halves (a run of
+     * 12,288 plans or more runs as two, concurrently) the half's session
+     * prepared, its rounds done and its results read back (0 for an absent
+     * half) */
+    double timeline_ms[7];
+    /* rounds scheduled on the device: the run's rounds were launched at
+     * once, each round's planning kernel choosing the next round's tasks */
+    uint64_t device_rounds;
 } gva_batch_stats;
 
 /* Declares the database a union of graphs: graph g owns vertex ids
@@ -230,7 +247,10 @@ typedef struct gva_tuning {
     double ms;          /* gva_db_autotune: calibration time of the chosen shape */
     double default_ms;  /* gva_db_autotune: calibration time of the default shape */
     uint32_t tried;     /* gva_db_autotune: shapes timed */
-    uint32_t reserved;
+    /* MiB of each of the two frontier regions of device-scheduled rounds
+     * (0: unchanged by gva_db_set_tuning; default 2048); doubled after a run
+     * whose round outgrew it */
+    uint32_t round_region_mb;
 } gva_tuning;
 int gva_db_get_tuning(const gva_db* db, gva_tuning* out);
 int gva_db_set_tuning(gva_db* db, const gva_tuning* tuning);

@@ -199,3 +199,60 @@ def test_batch_count_texts_equals_planned_batch(small_db, oracle):
     want = [oracle.count(og, t) for t in pats[:10]]
     assert [int(c) for i, c in enumerate(counts) if i not in (5, 6, 7)] == want
     assert int(counts[5]) == int(counts[6]) == int(counts[7]) == 0
+
+
+def test_device_rounds_match_host_rounds(small_db, oracle):
+    """Rounds scheduled on the device (a planning kernel per round, every
+    round launched at once) give the counts, per-graph counts and supports of
+    rounds scheduled on the host, and the oracle's counts."""
+    db, gdb, og = small_db
+    pats = [p for p in _patterns(db, 160, 31) if oracle.count(og, p, cap_rows=1_000_000) is not None]
+    for mode in (gv.MODE_DV, gv.MODE_SV):
+        plans = [gv.Plan.from_text(p, mode) for p in pats]
+        dc, (dgc, dsup), ds = gv.batch_count(gdb, plans, graph_counts=True, support=True)
+        hc, (hgc, hsup), hs = gv.batch_count(gdb, plans, graph_counts=True, support=True, host_rounds=True)
+        assert ds["device_rounds"] == ds["rounds"] > 0
+        assert hs["device_rounds"] == 0 and hs["rounds"] > 0
+        assert np.array_equal(dc, hc) and np.array_equal(dgc, hgc) and np.array_equal(dsup, hsup)
+        for p, c in zip(pats, dc):
+            assert int(c) == oracle.count(og, p), p
+
+
+def test_device_rounds_overflow_falls_back_to_host(native, oracle):
+    """A round whose output outgrows its frontier region makes the run start
+    over with host-scheduled rounds (same results) and doubles the region for
+    later runs."""
+    rng = np.random.default_rng(5)
+    V = 3000
+    vl = np.zeros(V + 1, dtype=np.uint32)
+    vl[1:] = rng.integers(1, 3, size=V)
+    edges = set()
+    while len(edges) < 30000:
+        a, b = (int(x) for x in rng.integers(1, V + 1, size=2))
+        if a != b:
+            edges.add((min(a, b), max(a, b), 1))
+    e = np.array(sorted(edges), dtype=np.uint32)
+    gdb = gv.Database.from_edges(vl, e[:, 0], e[:, 1], e[:, 2])
+    og = oracle.from_edges(vl, e[:, 0], e[:, 1], e[:, 2])
+    pats = ["v 0 %d\nv 1 %d\nv 2 %d\ne 0 1 1\ne 1 2 1\n" % (a, b, c) for a in (1, 2) for b in (1, 2) for c in (1, 2)]
+    pats += ["v 0 1\nv 1 2\nv 2 1\nv 3 2\ne 0 1 1\ne 1 2 1\ne 2 3 1\ne 3 0 1\n",  # a 4-cycle
+             "v 0 1\nv 1 2\nv 2 1\nv 3 2\ne 0 1 1\ne 1 2 1\ne 2 3 1\n",  # a 3-edge path
+             "v 0 1\nv 1 2\nv 2 2\nv 3 1\ne 0 1 1\ne 0 2 1\ne 0 3 1\n"]  # a 3-edge star
+    plans = [gv.Plan.from_text(p) for p in pats]
+    want, _, hs = gv.batch_count(gdb, plans, host_rounds=True)
+    assert [int(c) for c in want] == [oracle.count(og, p) for p in pats]
+    t = gdb.tuning()
+    try:
+        gdb.set_tuning(t["rows_per_item"], t["hub"], round_region_mb=1)
+        got, _, s = gv.batch_count(gdb, plans)
+        assert s["device_rounds"] == 0 and s["rounds"] > 0
+        assert gdb.tuning()["round_region_mb"] == 2
+        assert np.array_equal(got, want)
+        gdb.set_tuning(t["rows_per_item"], t["hub"], round_region_mb=64)
+        got, _, s = gv.batch_count(gdb, plans)
+        assert s["device_rounds"] == s["rounds"] > 0
+        assert np.array_equal(got, want)
+    finally:
+        gdb.set_tuning(t["rows_per_item"], t["hub"], round_region_mb=t["round_region_mb"])
+    oracle.free(og)
+    gdb.close()
