@@ -948,7 +948,7 @@ def batch_bench(args, rank, world, local, dist, torch, gv, workloads):
                       **{k: tstats[k] for k in ("device_rounds", "gpu_ms", "lower_ms", "submit_ms", "round_host_ms",
                                                 "round_phase_ms", "wait_ms", "session_ms", "timeline_ms")},
                       timeline="ms from the start of the batched run: plans ordered; per half: session prepared, "
-                               "rounds done, results read",
+                               "rounds done, results read, session freed",
                       host_rounds={"ms_per_step": statistics.mean(host_ms),
                                    "embeddings_per_s": emb_local / args.steps / (statistics.mean(host_ms) / 1000.0),
                                    "agree": host_rounds_agree,

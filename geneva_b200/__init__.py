@@ -113,7 +113,7 @@ class _BatchStats(ctypes.Structure):
                 ("launches", ctypes.c_uint64), ("trie_nodes", ctypes.c_uint64), ("kernels", _KernelStat * 5),
                 ("lower_ms", ctypes.c_double), ("submit_ms", ctypes.c_double), ("round_host_ms", ctypes.c_double),
                 ("wait_ms", ctypes.c_double), ("session_ms", ctypes.c_double),
-                ("round_phase_ms", ctypes.c_double * 5), ("timeline_ms", ctypes.c_double * 7),
+                ("round_phase_ms", ctypes.c_double * 5), ("timeline_ms", ctypes.c_double * 9),
                 ("device_rounds", ctypes.c_uint64)]
 
 
@@ -260,9 +260,9 @@ class Database:
     def autotune(self, plans, stream: Optional[int] = None) -> dict:
         """Times a calibration batch under each candidate launch shape and keeps
         the fastest (gva_db_autotune)."""
-        arr = (ctypes.c_void_p * max(len(plans), 1))(*[p._h.value for p in plans])
+        arr = _plan_handles(plans)
         t = _Tuning()
-        _check(library().gva_db_autotune(self._h, arr, len(plans), stream or None, ctypes.byref(t)))
+        _check(library().gva_db_autotune(self._h, arr.ctypes.data, len(plans), stream or None, ctypes.byref(t)))
         return {"rows_per_item": int(t.rows_per_item), "hub": int(t.hub), "ms": float(t.ms),
                 "default_ms": float(t.default_ms), "shapes_tried": int(t.tried)}
 
@@ -295,11 +295,42 @@ def probe_graph(mygraph: str, metadata: str) -> dict:
     return d
 
 
+def _text_array(texts: Sequence[str]):
+    """The texts as one NUL-separated buffer and an array of pointers into
+    it (what a const char* const* parameter takes), built without a
+    per-text ctypes object.  Returns (keep-alive buffer, uint64 pointers)."""
+    n = len(texts)
+    if n == 0:
+        return b"\0", np.zeros(1, dtype=np.uint64)
+    buf = ("\0".join(texts) + "\0").encode()
+    lens = np.fromiter(map(len, texts), dtype=np.int64, count=n)
+    if len(buf) == int(lens.sum()) + n:  # one byte per character: offsets from the lengths
+        starts = np.cumsum(lens + 1) - (lens + 1)
+    else:
+        ends = np.flatnonzero(np.frombuffer(buf, dtype=np.uint8) == 0)
+        if len(ends) != n:
+            raise ValueError("query texts must not contain NUL characters")
+        starts = np.empty(n, dtype=np.int64)
+        starts[0] = 0
+        starts[1:] = ends[:-1] + 1
+    base = ctypes.cast(ctypes.c_char_p(buf), ctypes.c_void_p).value
+    return buf, starts.astype(np.uint64) + np.uint64(base)
+
+
+def _plan_handles(plans) -> np.ndarray:
+    """Plan handles as a uint64 array: kept by a PlanBatch, else gathered."""
+    h = getattr(plans, "_harr", None)
+    if h is not None:
+        return h
+    return np.array([p._h.value or 0 for p in plans] or [0], dtype=np.uint64)
+
+
 class Plan:
     """Match order + restrictions (gva_plan)."""
 
-    def __init__(self, handle):
+    def __init__(self, handle, batch=None):
         self._h = ctypes.c_void_p(handle)
+        self._batch = batch  # the PlanBatch owning the handle, if any
 
     @classmethod
     def from_text(cls, text: str, mode: int = MODE_DV) -> "Plan":
@@ -308,41 +339,29 @@ class Plan:
         return cls(h.value)
 
     @classmethod
-    def batch_from_texts(cls, texts: Sequence[str], mode: int = MODE_DV) -> List["Plan"]:
-        """Plans many queries in one call on the host's cores (gva_plan_batch)."""
+    def _batch(cls, call, texts: Sequence[str]) -> "PlanBatch":
         n = len(texts)
-        enc = (ctypes.c_char_p * max(n, 1))(*[t.encode() for t in texts])
-        out = (ctypes.c_void_p * max(n, 1))()
-        st = (ctypes.c_int * max(n, 1))()
-        rc = library().gva_plan_batch(ctypes.cast(enc, ctypes.c_void_p), n, mode, ctypes.cast(out, ctypes.c_void_p),
-                                      ctypes.cast(st, ctypes.c_void_p))
-        plans = [cls(out[i]) if out[i] else None for i in range(n)]
+        buf, ptrs = _text_array(texts)
+        out = np.zeros(max(n, 1), dtype=np.uint64)
+        st = np.zeros(max(n, 1), dtype=np.int32)
+        rc = call(ptrs.ctypes.data, n, out.ctypes.data, st.ctypes.data)
+        batch = PlanBatch(out[:n])
         if rc:
             msg = library().gva_last_error().decode()
-            for p in plans:
-                if p is not None:
-                    p.close()
+            batch.close()
             raise GenevaError(rc, msg)
-        return plans
+        return batch
 
     @classmethod
-    def batch_from_texts_device(cls, texts: Sequence[str], device: int = 0) -> List["Plan"]:
+    def batch_from_texts(cls, texts: Sequence[str], mode: int = MODE_DV) -> "PlanBatch":
+        """Plans many queries in one call on the host's cores (gva_plan_batch)."""
+        return cls._batch(lambda t, n, o, s: library().gva_plan_batch(t, n, mode, o, s), texts)
+
+    @classmethod
+    def batch_from_texts_device(cls, texts: Sequence[str], device: int = 0) -> "PlanBatch":
         """DV plans of many queries computed by the device planner
         (gva_plan_batch_device); the same plans as batch_from_texts."""
-        n = len(texts)
-        enc = (ctypes.c_char_p * max(n, 1))(*[t.encode() for t in texts])
-        out = (ctypes.c_void_p * max(n, 1))()
-        st = (ctypes.c_int * max(n, 1))()
-        rc = library().gva_plan_batch_device(device, ctypes.cast(enc, ctypes.c_void_p), n,
-                                             ctypes.cast(out, ctypes.c_void_p), ctypes.cast(st, ctypes.c_void_p))
-        plans = [cls(out[i]) if out[i] else None for i in range(n)]
-        if rc:
-            msg = library().gva_last_error().decode()
-            for p in plans:
-                if p is not None:
-                    p.close()
-            raise GenevaError(rc, msg)
-        return plans
+        return cls._batch(lambda t, n, o, s: library().gva_plan_batch_device(device, t, n, o, s), texts)
 
     @classmethod
     def from_file(cls, path: str, mode: int = MODE_DV) -> "Plan":
@@ -368,9 +387,43 @@ class Plan:
         return library().gva_plan_num_phases(self._h)
 
     def close(self):
-        if self._h:
+        # a plan of a PlanBatch only lets go of its handle: the batch frees it
+        if self._h and self._batch is None:
             library().gva_plan_free(self._h)
-            self._h = ctypes.c_void_p()
+        self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class PlanBatch(tuple):
+    """Plans made together (Plan.batch_from_texts): a tuple of Plan (None
+    where a text failed to plan) that owns their handles and keeps them as one
+    array, so batched calls take them without a per-plan conversion.  The
+    handles are freed when the batch and every plan taken from it are gone,
+    or by close()."""
+
+    def __new__(cls, handles: np.ndarray):
+        harr = np.array(handles, dtype=np.uint64)
+        self = super().__new__(cls, [Plan(int(h)) if h else None for h in harr.tolist()])
+        self._harr = harr
+        for q in tuple.__iter__(self):
+            if q is not None:
+                q._batch = self
+        return self
+
+    def close(self):
+        lib = library()
+        for q in tuple.__iter__(self):
+            if q is not None:
+                q._h = ctypes.c_void_p()
+        for h in self._harr.tolist():
+            if h:
+                lib.gva_plan_free(ctypes.c_void_p(h))
+        self._harr = np.zeros(len(self._harr), dtype=np.uint64)
 
     def __del__(self):
         try:
@@ -462,13 +515,13 @@ def batch_count(db: Database, plans: Sequence[Plan], stream: Optional[int] = Non
     uint32 supporting-graph counts when support, else None.  host_rounds:
     schedule every round on the host (GVA_BATCH_HOST_ROUNDS)."""
     n = len(plans)
-    arr = (ctypes.c_void_p * max(n, 1))(*[p._h.value for p in plans])
+    arr = _plan_handles(plans)
     counts = np.zeros(n, dtype=np.uint64)
     gc = np.zeros((n, db.num_graphs), dtype=np.uint64) if graph_counts else None
     sup = np.zeros(n, dtype=np.uint32) if support else None
     o = _BatchOpts(stream or None, budget_bytes, 1 if profile else 0, BATCH_HOST_ROUNDS if host_rounds else 0)
     st = _BatchStats()
-    _check(library().gva_batch_count(db._h, arr, n, ctypes.byref(o), counts.ctypes.data,
+    _check(library().gva_batch_count(db._h, arr.ctypes.data, n, ctypes.byref(o), counts.ctypes.data,
                                      gc.ctypes.data if gc is not None else None,
                                      sup.ctypes.data if sup is not None else None, ctypes.byref(st)))
     per_graph = gc if graph_counts else sup
@@ -498,15 +551,14 @@ def batch_count_texts(db: Database, texts: Sequence[str], mode: int = MODE_DV, s
     Returns (counts, per_graph, stats) as batch_count; a text that fails to
     plan raises GenevaError after the others were counted."""
     n = len(texts)
-    enc = [t.encode() for t in texts]
-    arr = (ctypes.c_char_p * max(n, 1))(*enc)
+    buf, arr = _text_array(texts)
     counts = np.zeros(n, dtype=np.uint64)
     gc = np.zeros((n, db.num_graphs), dtype=np.uint64) if graph_counts else None
     sup = np.zeros(n, dtype=np.uint32) if support else None
     status = np.zeros(max(n, 1), dtype=np.int32)
     o = _BatchOpts(stream or None, budget_bytes, 1 if profile else 0, BATCH_PLAN_ON_DEVICE if plan_on_device else 0)
     st = _BatchStats()
-    _check(library().gva_batch_count_texts(db._h, ctypes.cast(arr, ctypes.c_void_p), n, mode, ctypes.byref(o),
+    _check(library().gva_batch_count_texts(db._h, arr.ctypes.data, n, mode, ctypes.byref(o),
                                            counts.ctypes.data, gc.ctypes.data if gc is not None else None,
                                            sup.ctypes.data if sup is not None else None, status.ctypes.data,
                                            ctypes.byref(st)))
@@ -662,12 +714,11 @@ def mni_support(db: Database, patterns: Sequence[str], cap: int = 0, plain: bool
     graph, as min(MNI, cap) (cap 0 = exact) (gva_mni_support).  plain runs
     one pattern at a time.  Returns (supports uint32[n], stats)."""
     n = len(patterns)
-    enc = [p.encode() for p in patterns]
-    arr = (ctypes.c_char_p * max(n, 1))(*enc)
+    buf, arr = _text_array(patterns)
     sup = np.zeros(n, dtype=np.uint32)
     o = _MniOpts(stream or None, cap, 1 if plain else 0, 1 if profile else 0, 0)
     st = _MniStats()
-    _check(library().gva_mni_support(db._h, ctypes.cast(arr, ctypes.c_void_p), n, ctypes.byref(o), sup.ctypes.data,
+    _check(library().gva_mni_support(db._h, arr.ctypes.data, n, ctypes.byref(o), sup.ctypes.data,
                                      ctypes.byref(st)))
     stats = {f: getattr(st, f) for f, _ in _MniStats._fields_ if f != "kernel"}
     k = st.kernel

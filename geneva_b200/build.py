@@ -26,7 +26,8 @@ NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompil
 CXX_FLAGS = ["-O2", "-std=c++17", "-fPIC", "-Wall", "-Wno-sign-compare", f"-I{ROOT / 'include'}"]
 
 CU_SOURCES = ["gva_engine.cu", "gva_batch.cu", "gva_static.cu", "gva_mni.cu", "gva_dplan.cu"]
-CPP_SOURCES = ["gva_plan.cpp", "gva_graph.cpp", "gva_capi.cpp", "gva_mine.cpp", "gva_convert.cpp", "gva_text.cpp"]
+CPP_SOURCES = ["gva_plan.cpp", "gva_graph.cpp", "gva_capi.cpp", "gva_mine.cpp", "gva_convert.cpp", "gva_text.cpp",
+               "gva_pool.cpp"]
 
 
 def nvcc() -> str:

@@ -37,6 +37,7 @@
 #include "../../include/geneva.h"
 #include "gva_engine.cuh"
 #include "gva_kernels.cuh"
+#include "gva_pool.h"
 
 namespace gva {
 
@@ -1416,12 +1417,7 @@ int BatchSession::submit(std::vector<std::vector<Step>>&& wave, const std::vecto
                 L.nodes[cur].first_term = q;
             }
         };
-        {
-            std::vector<std::thread> pool;
-            for (unsigned t = 1; t < T; ++t) pool.emplace_back(build, t);
-            build(0);
-            for (auto& th : pool) th.join();
-        }
+        pool_run(T, build);
         std::vector<size_t> off(T + 1, (size_t)first_chunk_node);
         for (unsigned t = 0; t < T; ++t) off[t + 1] = off[t] + loc[t].nodes.size();
         nodes.resize(off[T]);
@@ -1439,12 +1435,7 @@ int BatchSession::submit(std::vector<std::vector<Step>>&& wave, const std::vecto
             }
             for (size_t qi = cut[t]; qi < cut[t + 1]; ++qi) plans[q0 + (int)qi].terminal = L.term[qi - cut[t]] + o;
         };
-        {
-            std::vector<std::thread> pool;
-            for (unsigned t = 1; t < T; ++t) pool.emplace_back(place, t);
-            place(0);
-            for (auto& th : pool) th.join();
-        }
+        pool_run(T, place);
         // children of seed nodes: each chunk's chain joins its seed node's list
         for (unsigned t = 0; t < T; ++t)
             for (const auto& rl : loc[t].root_list) {
@@ -1538,10 +1529,7 @@ int BatchSession::submit(std::vector<std::vector<Step>>&& wave, const std::vecto
             for (size_t id = (size_t)first_node + t; id < nn; id += T)
                 fill_node_desc((int)id, desc_host.data() + (id - shipped) * sizeof(TaskDesc));
         };
-        std::vector<std::thread> pool;
-        for (unsigned t = 1; t < T; ++t) pool.emplace_back(fill, t);
-        fill(0);
-        for (auto& th : pool) th.join();
+        pool_run(T, fill);
     }
     start_seeds(first_node);
     return GVA_OK;
@@ -2359,6 +2347,7 @@ int finish_batch(DevDB& db, PreparedBatch& pb, uint64_t* counts, uint64_t* graph
         }
     }
     if (stats) {
+        stats->read_end_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_fin0).count();
         stats->submit_ms = ses.submit_ms;
         stats->round_host_ms = ses.round_host_ms;
         stats->wait_ms = ses.wait_ms;
@@ -2413,28 +2402,13 @@ static void order_by_step_keys(const std::vector<std::vector<Step>>& steps, std:
     size_t w = 1;
     for (const auto& v : steps) w = std::max(w, v.size());
     std::vector<uint64_t> key(n * w, 0);  // 0 ends a plan's sequence
-    const unsigned nth = n < 2048 ? 1u : std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
-    auto run = [&](auto&& fn) {
-        if (nth == 1) {
-            fn(0u);
-            return;
-        }
-        std::vector<std::thread> pool;
-        for (unsigned t = 0; t < nth; ++t) pool.emplace_back(fn, t);
-        for (auto& th : pool) th.join();
-    };
-    run([&](unsigned t) {
-        uint8_t kb[512];
-        for (size_t i = t; i < n; i += nth)
-            for (size_t j = 0; j < steps[i].size(); ++j) {
-                const size_t len = step_key_bytes(steps[i][j], kb);
-                uint64_t h = 1469598103934665603ull;
-                for (size_t b = 0; b < len; ++b) h = (h ^ kb[b]) * 1099511628211ull;
-                key[i * w + j] = h | 1;
-            }
-    });
+    // chunks of the plans, each hashed and sorted by one job, then merged pairwise
+    size_t chunks = 1;
+    const size_t width = n < 2048 ? 1 : std::min<size_t>(32, pool_width());
+    while (chunks * 2 <= width) chunks *= 2;
+    std::vector<size_t> cut(chunks + 1);
+    for (size_t c = 0; c <= chunks; ++c) cut[c] = n * c / chunks;
     order.resize(n);
-    for (size_t i = 0; i < n; ++i) order[i] = (uint32_t)i;
     auto less = [&](uint32_t a, uint32_t b) {
         const uint64_t* ka = key.data() + (size_t)a * w;
         const uint64_t* kb = key.data() + (size_t)b * w;
@@ -2442,26 +2416,32 @@ static void order_by_step_keys(const std::vector<std::vector<Step>>& steps, std:
             if (ka[j] != kb[j]) return ka[j] < kb[j];
         return a < b;
     };
-    // sorted chunks, merged pairwise
-    size_t chunks = 1;
-    while (chunks * 2 <= nth && chunks < 32) chunks *= 2;
-    std::vector<size_t> cut(chunks + 1);
-    for (size_t c = 0; c <= chunks; ++c) cut[c] = n * c / chunks;
-    {
-        std::vector<std::thread> pool;
-        for (size_t c = 0; c < chunks; ++c)
-            pool.emplace_back([&, c]() { std::sort(order.begin() + cut[c], order.begin() + cut[c + 1], less); });
-        for (auto& th : pool) th.join();
-    }
-    for (size_t width = 1; width < chunks; width *= 2) {
-        std::vector<std::thread> pool;
-        for (size_t c = 0; c + width < chunks; c += 2 * width) {
-            const size_t lo = cut[c], mid = cut[c + width], hi = cut[std::min(chunks, c + 2 * width)];
-            pool.emplace_back([&, lo, mid, hi]() {
-                std::inplace_merge(order.begin() + lo, order.begin() + mid, order.begin() + hi, less);
-            });
+    pool_run((unsigned)chunks, [&](unsigned c) {
+        uint64_t kb[64];  // step key bytes, zero-padded to whole words
+        for (size_t i = cut[c]; i < cut[c + 1]; ++i) {
+            order[i] = (uint32_t)i;
+            for (size_t j = 0; j < steps[i].size(); ++j) {
+                const size_t len = step_key_bytes(steps[i][j], reinterpret_cast<uint8_t*>(kb));
+                const size_t words = (len + 7) / 8;
+                memset(reinterpret_cast<uint8_t*>(kb) + len, 0, words * 8 - len);
+                uint64_t h = 0x243f6a8885a308d3ull ^ len;
+                for (size_t q = 0; q < words; ++q) {
+                    h = (h ^ kb[q]) * 0x9e3779b97f4a7c15ull;
+                    h ^= h >> 29;
+                }
+                key[i * w + j] = h | 1;
+            }
         }
-        for (auto& th : pool) th.join();
+        std::sort(order.begin() + cut[c], order.begin() + cut[c + 1], less);
+    });
+    for (size_t span = 1; span < chunks; span *= 2) {
+        const unsigned jobs = (unsigned)((chunks + 2 * span - 1) / (2 * span));
+        pool_run(jobs, [&](unsigned m) {
+            const size_t c = (size_t)m * 2 * span;
+            if (c + span >= chunks) return;
+            const size_t lo = cut[c], mid = cut[c + span], hi = cut[std::min(chunks, c + 2 * span)];
+            std::inplace_merge(order.begin() + lo, order.begin() + mid, order.begin() + hi, less);
+        });
     }
 }
 
@@ -2505,9 +2485,10 @@ int run_batch(DevDB& db, std::vector<std::vector<Step>> steps, cudaStream_t s, u
         const double t_prep = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
         // results straight to the caller's arrays, at each plan's index before sorting
         if (!r) r = finish_batch(db, pb, counts, graph_counts_host, support_host, &bss[k], nullptr, order.data() + cut[k]);
-        bss[k].timeline_ms[1 + 3 * k] = t_prep;
-        bss[k].timeline_ms[2 + 3 * k] = t_prep + bss[k].loop_end_ms;
-        bss[k].timeline_ms[3 + 3 * k] =
+        bss[k].timeline_ms[1 + 4 * k] = t_prep;
+        bss[k].timeline_ms[2 + 4 * k] = t_prep + bss[k].loop_end_ms;
+        bss[k].timeline_ms[3 + 4 * k] = t_prep + bss[k].read_end_ms;
+        bss[k].timeline_ms[4 + 4 * k] =
             std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
         rcs[k] = r;
         if (r) errs[k] = last_error_cstr();
@@ -2534,7 +2515,7 @@ int run_batch(DevDB& db, std::vector<std::vector<Step>> steps, cudaStream_t s, u
         total.launches += bs.launches;
         total.nodes += bs.nodes;
         for (int i = 0; i < 5; ++i) total.phase_ms[i] += bs.phase_ms[i];
-        for (int i = 1; i < 7; ++i) total.timeline_ms[i] += bs.timeline_ms[i];
+        for (int i = 1; i < 9; ++i) total.timeline_ms[i] += bs.timeline_ms[i];
         for (int i = 0; i < K_NUM; ++i) {
             total.kstat[i].launches += bs.kstat[i].launches;
             total.kstat[i].ms += bs.kstat[i].ms;

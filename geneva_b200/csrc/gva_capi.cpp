@@ -17,6 +17,7 @@
 #include "gva_engine.cuh"
 #include "gva_dplan.h"
 #include "gva_internal.h"
+#include "gva_pool.h"
 
 namespace gva {
 const char* last_error_cstr();
@@ -34,7 +35,7 @@ namespace {
 // the calling thread.
 template <typename F>
 int parallel_for(int n, F fn) {
-    const unsigned nth = n < 256 ? 1u : std::max(1u, std::min(64u, std::thread::hardware_concurrency()));
+    const unsigned nth = n < 256 ? 1u : gva::pool_width();
     if (nth == 1) {
         for (int i = 0; i < n; ++i) {
             int st = fn(i);
@@ -44,19 +45,16 @@ int parallel_for(int n, F fn) {
     }
     std::vector<int> rc(nth, GVA_OK);
     std::vector<std::string> msg(nth);
-    std::vector<std::thread> pool;
-    for (unsigned t = 0; t < nth; ++t)
-        pool.emplace_back([&, t]() {
-            for (int i = (int)t; i < n; i += (int)nth) {
-                int st = fn(i);
-                if (st) {
-                    rc[t] = st;
-                    msg[t] = gva::last_error_cstr();
-                    return;
-                }
+    gva::pool_run(nth, [&](unsigned t) {
+        for (int i = (int)t; i < n; i += (int)nth) {
+            int st = fn(i);
+            if (st) {
+                rc[t] = st;
+                msg[t] = gva::last_error_cstr();
+                return;
             }
-        });
-    for (auto& th : pool) th.join();
+        }
+    });
     for (unsigned t = 0; t < nth; ++t)
         if (rc[t]) return gva::fail(rc[t], msg[t]);
     return GVA_OK;
@@ -454,7 +452,7 @@ void fill_batch_stats(const BatchStats& bs, double lower_ms, gva_batch_stats* st
     stats->wait_ms = bs.wait_ms;
     stats->session_ms = bs.session_ms;
     for (int i = 0; i < 5; ++i) stats->round_phase_ms[i] = bs.phase_ms[i];
-    for (int i = 0; i < 7; ++i) stats->timeline_ms[i] = bs.timeline_ms[i];
+    for (int i = 0; i < 9; ++i) stats->timeline_ms[i] = bs.timeline_ms[i];
     stats->device_rounds = bs.device_rounds;
     for (int i = 0; i < K_NUM && i < 5; ++i) {
         strncpy(stats->kernels[i].name, kKernelNames[i], sizeof stats->kernels[i].name - 1);

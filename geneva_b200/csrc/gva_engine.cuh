@@ -100,9 +100,11 @@ struct BatchStats {
     uint64_t device_rounds = 0;
     KernelStat kstat[K_NUM];
     // wall-clock marks of one run (ms from its start): plans ordered, then
-    // per half (two at most) session prepared, rounds done, results read
-    double timeline_ms[7] = {0, 0, 0, 0, 0, 0, 0};
+    // per half (two at most) session prepared, rounds done, results read,
+    // session freed
+    double timeline_ms[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
     double loop_end_ms = 0.0;  // finish_batch: rounds done, ms after its start
+    double read_end_ms = 0.0;  // finish_batch: results read, ms after its start
 };
 
 // Counts the embeddings of many plans in shared rounds.  counts[q] always;

@@ -204,9 +204,9 @@ typedef struct gva_batch_stats {
     /* wall-clock marks of the run (ms from the call's start of the batched
      * run): plans ordered; then for each of up to two halves (a run of
      * 12,288 plans or more runs as two, concurrently) the half's session
-     * prepared, its rounds done and its results read back (0 for an absent
-     * half) */
-    double timeline_ms[7];
+     * prepared, its rounds done, its results read back and its session freed
+     * (0 for an absent half) */
+    double timeline_ms[9];
     /* rounds scheduled on the device: the run's rounds were launched at
      * once, each round's planning kernel choosing the next round's tasks */
     uint64_t device_rounds;

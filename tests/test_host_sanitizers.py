@@ -1,6 +1,6 @@
 """Host code under AddressSanitizer and UndefinedBehaviorSanitizer (CPU only):
 the CPU test drivers for the miner's host loop, the heap-free planner, the
-planner's two entries and the database build are rebuilt with
+planner's two entries, the database build and the host worker pool are rebuilt with
 -fsanitize=address,undefined and run on small cases; any invalid access, leak
 or undefined operation fails the run.
 """
@@ -23,6 +23,7 @@ DRIVERS = {
     "mygraph_roundtrip_check": [TESTS / "mygraph_roundtrip_check.cpp", CSRC / "gva_convert.cpp", CSRC / "gva_graph.cpp",
                                 CSRC / "gva_plan.cpp"],
     "text_format_check": [TESTS / "text_format_check.cpp", CSRC / "gva_text.cpp"],
+    "pool_check": [TESTS / "pool_check.cpp", CSRC / "gva_pool.cpp"],
 }
 RUNS = [
     ("mine_grow_check", ["3", "2", "4", "7", "0.3", "4"]),
@@ -34,6 +35,7 @@ RUNS = [
     ("graph_build_check", ["1", "2", "70000"]),  # the threaded sort and fill
     ("mygraph_roundtrip_check", ["10", "3", None]),  # None: a scratch directory
     ("text_format_check", ["2", "8000"]),
+    ("pool_check", ["4", "200", "37"]),  # concurrent and nested jobs on the host worker pool
 ]
 
 

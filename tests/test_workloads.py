@@ -50,4 +50,4 @@ def test_mined_patterns_container():
 
 
 def test_batch_planning_of_nothing(native):
-    assert gv.Plan.batch_from_texts([]) == []
+    assert list(gv.Plan.batch_from_texts([])) == []
