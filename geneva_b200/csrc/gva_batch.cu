@@ -1060,6 +1060,10 @@ BatchSession::~BatchSession() {
     keep(nodes, t_spare.nodes);
     keep(node_steps, t_spare.node_steps);
     keep(plans, t_spare.plans);
+    if (!waves.empty()) {  // thousands of small step vectors: freed off this thread
+        auto w = std::make_shared<std::vector<std::vector<std::vector<Step>>>>(std::move(waves));
+        defer([w]() mutable { w.reset(); });
+    }
     if (desc_host.capacity() > t_spare.desc_host.capacity()) desc_host.swap(t_spare.desc_host);
     cudaSetDevice(db.device);
     active.clear();

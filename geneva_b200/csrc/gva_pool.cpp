@@ -5,6 +5,7 @@
 #include <algorithm>
 #include <atomic>
 #include <condition_variable>
+#include <deque>
 #include <mutex>
 #include <thread>
 #include <vector>
@@ -110,10 +111,56 @@ Pool& pool() {
     return p;
 }
 
+// One background thread running deferred work in order.
+class Deferred {
+public:
+    Deferred() : th_([this]() { work(); }) {}
+    ~Deferred() {
+        {
+            std::lock_guard<std::mutex> lk(mu_);
+            stop_ = true;
+        }
+        cv_.notify_all();
+        th_.join();
+    }
+    void post(std::function<void()> fn) {
+        {
+            std::lock_guard<std::mutex> lk(mu_);
+            q_.push_back(std::move(fn));
+        }
+        cv_.notify_one();
+    }
+
+private:
+    void work() {
+        std::unique_lock<std::mutex> lk(mu_);
+        for (;;) {
+            cv_.wait(lk, [&]() { return stop_ || !q_.empty(); });
+            if (q_.empty()) return;  // stopping with nothing left
+            std::function<void()> fn = std::move(q_.front());
+            q_.pop_front();
+            lk.unlock();
+            fn();
+            fn = nullptr;  // what it captured is released off the lock too
+            lk.lock();
+        }
+    }
+    std::mutex mu_;
+    std::condition_variable cv_;
+    std::deque<std::function<void()>> q_;
+    bool stop_ = false;
+    std::thread th_;
+};
+
 }  // namespace
 
 void pool_run(unsigned n, const std::function<void(unsigned)>& fn) { pool().run(n, fn); }
 
 unsigned pool_width() { return pool().width(); }
+
+void defer(std::function<void()> fn) {
+    static Deferred d;
+    d.post(std::move(fn));
+}
 
 }  // namespace gva

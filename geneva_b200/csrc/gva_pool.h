@@ -19,4 +19,10 @@ void pool_run(unsigned n, const std::function<void(unsigned)>& fn);
 // Threads a job can use at once: the workers plus the caller.
 unsigned pool_width();
 
+// Runs fn later on a background thread (in submission order); for work
+// whose result nobody waits for, such as freeing the many small heap blocks
+// of a finished batch's plans (milliseconds of free() calls that would
+// otherwise sit on the caller's path).
+void defer(std::function<void()> fn);
+
 }  // namespace gva
