@@ -286,6 +286,21 @@ __device__ __forceinline__ bool ext_injective(const ExtArgs& p, const uint32_t* 
     return true;
 }
 
+// The same test against the row's matched vertices held in registers
+// (extensions with at most 8 injectivity columns; unused entries never
+// equal a vertex id).
+__device__ __forceinline__ void load_eqv(const ExtArgs& p, const uint32_t* row, uint32_t (&eqv)[8]) {
+    const uint32_t n = p.n_eq;
+#pragma unroll
+    for (int e = 0; e < 8; ++e) eqv[e] = e < (int)n ? row[p.eq_cols[e]] : 0xffffffffu;
+}
+__device__ __forceinline__ bool injective8(const uint32_t (&eqv)[8], uint32_t c) {
+    bool coll = false;
+#pragma unroll
+    for (int e = 0; e < 8; ++e) coll |= c == eqv[e];
+    return !coll;
+}
+
 // Output staging of one warp: accepted (row, candidate) pairs are appended
 // in ballot order to a shared tile of kTileRows rows and flushed 32 rows at a
 // time with coalesced stores.
@@ -379,6 +394,9 @@ __device__ __forceinline__ uint64_t ext_item(const TaskDesc& d, const uint32_t* 
             const uint32_t mine = is_hub ? 0 : len;
             words += mine;
             const uint32_t* gadj = FUSED ? gen_s[lane].gadj : p.adj;
+            const bool eq8 = p.n_eq <= 8;  // matched vertices in registers
+            uint32_t eqv[8];
+            if (!FUSED && eq8) load_eqv(p, row, eqv);
             // own rows: lanes step through their lists together
             const uint32_t steps = __reduce_max_sync(0xffffffffu, mine);
             for (uint32_t s = 0; s < steps; ++s) {
@@ -386,7 +404,7 @@ __device__ __forceinline__ uint64_t ext_item(const TaskDesc& d, const uint32_t* 
                 uint32_t c = 0;
                 if (s < mine) {
                     c = __ldg(gadj + lo + s);
-                    ok = FUSED ? ext_accept(p, row, c, gen_s[lane]) : ext_injective(p, row, c);
+                    ok = FUSED ? ext_accept(p, row, c, gen_s[lane]) : (eq8 ? injective8(eqv, c) : ext_injective(p, row, c));
                 }
                 cnt += ok ? 1u : 0u;
                 if (WRITE) tile_append(*tl, ok, row, k, c, true);
@@ -406,6 +424,7 @@ __device__ __forceinline__ uint64_t ext_item(const TaskDesc& d, const uint32_t* 
                 const uint32_t hlo = __shfl_sync(0xffffffffu, lo, h), hhi = __shfl_sync(0xffffffffu, hi, h);
                 const uint32_t* hrow = rows_s + (base + h) * k;
                 const uint32_t* hadj = FUSED ? gen_s[h].gadj : p.adj;
+                if (!FUSED && eq8) load_eqv(p, hrow, eqv);
                 uint32_t hc = 0;
                 if (hhi - hlo >= 128) {
                     for (uint32_t j0 = hlo & ~3u; j0 < hhi; j0 += 128) {
@@ -418,7 +437,8 @@ __device__ __forceinline__ uint64_t ext_item(const TaskDesc& d, const uint32_t* 
                             const uint32_t c = vv[q];
                             bool ok = false;
                             if (j + q >= hlo && j + q < hhi)
-                                ok = FUSED ? ext_accept(p, hrow, c, gen_s[h]) : ext_injective(p, hrow, c);
+                                ok = FUSED ? ext_accept(p, hrow, c, gen_s[h])
+                                           : (eq8 ? injective8(eqv, c) : ext_injective(p, hrow, c));
                             hc += ok ? 1u : 0u;
                             if (WRITE) tile_append(*tl, ok, hrow, k, c, true);
                         }
@@ -430,7 +450,8 @@ __device__ __forceinline__ uint64_t ext_item(const TaskDesc& d, const uint32_t* 
                         uint32_t c = 0;
                         if (j < hhi) {
                             c = __ldg(hadj + j);
-                            ok = FUSED ? ext_accept(p, hrow, c, gen_s[h]) : ext_injective(p, hrow, c);
+                            ok = FUSED ? ext_accept(p, hrow, c, gen_s[h])
+                                       : (eq8 ? injective8(eqv, c) : ext_injective(p, hrow, c));
                         }
                         hc += ok ? 1u : 0u;
                         if (WRITE) tile_append(*tl, ok, hrow, k, c, true);
@@ -687,7 +708,7 @@ __global__ void __launch_bounds__(1024) scan_items_top_kernel(uint64_t* __restri
 // at the item's scanned offset, in the order the count pass counted them.
 // Items without output are skipped.
 template <bool FUSED>
-__global__ void __launch_bounds__(kRoundWarps * 32, FUSED ? 4 : 6)
+__global__ void __launch_bounds__(kRoundWarps * 32, FUSED ? 4 : 5)
 round_write_kernel(RoundArgs a) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const WarpSmem ws = warp_smem<true, FUSED>(smem_raw, a);

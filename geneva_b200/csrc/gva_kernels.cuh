@@ -206,30 +206,56 @@ __device__ __forceinline__ bool ext_accept(const ExtArgs& p, const uint32_t* row
     return true;
 }
 
+// Candidates of a short list [lo, hi) below bound b that equal none of the
+// row's NEQ matched vertices (columns eq_cols), in one pass over the list;
+// the list is ascending, so the walk stops at the bound (no search for it).
+// A vertex in two columns still excludes its candidate once.
+template <int NEQ>
+__device__ __forceinline__ uint32_t short_list_count(const uint32_t* __restrict__ adj, uint32_t lo, uint32_t hi,
+                                                     uint64_t b, const uint32_t* row, const uint8_t* eq_cols) {
+    uint32_t eqv[NEQ > 0 ? NEQ : 1];
+#pragma unroll
+    for (int e = 0; e < NEQ; ++e) eqv[e] = row[eq_cols[e]];
+    uint32_t m = 0;
+    for (uint32_t j = lo; j < hi; ++j) {
+        const uint32_t c = __ldg(adj + j);
+        if ((uint64_t)c >= b) break;
+        bool coll = false;
+#pragma unroll
+        for (int e = 0; e < NEQ; ++e) coll |= c == eqv[e];
+        m += coll ? 0u : 1u;
+    }
+    return m;
+}
+
 // Number of candidates of one row of a plain extension (no fused checks):
-// the segment minus the already-matched vertices in it.
+// the segment below the restriction bound minus the already-matched
+// vertices in it.
 __device__ __forceinline__ uint32_t ext_count_plain(const ExtArgs& p, const uint32_t* row) {
     uint32_t lo, hi;
-    ext_range(p, row, lo, hi);
+    seg_of(p.off, p.L, row[p.src_col], p.lab, lo, hi);
     if (lo >= hi) return 0;
-    uint32_t n = hi - lo;
-    if (n <= 8 && p.n_eq <= 8) {
-        // a short list: each candidate against the matched vertices, one
-        // pass over the list (a vertex in two columns still excludes its
-        // candidate once)
-        uint32_t eqv[8];
-#pragma unroll
-        for (int e = 0; e < 8; ++e) eqv[e] = e < (int)p.n_eq ? row[p.eq_cols[e]] : 0xffffffffu;
-        uint32_t m = 0;
-        for (uint32_t j = lo; j < hi; ++j) {
-            const uint32_t c = __ldg(p.adj + j);
-            bool coll = false;
-#pragma unroll
-            for (int e = 0; e < 8; ++e) coll |= c == eqv[e];
-            m += coll ? 0u : 1u;
+    const uint32_t n_eq = p.n_eq;
+    if (hi - lo <= 8 && n_eq <= 8) {
+        const uint64_t b = p.bound_col >= 0 ? (uint64_t)row[p.bound_col] + p.bound_incl : ~0ull;
+        switch (n_eq) {
+            case 0: return short_list_count<0>(p.adj, lo, hi, b, row, p.eq_cols);
+            case 1: return short_list_count<1>(p.adj, lo, hi, b, row, p.eq_cols);
+            case 2: return short_list_count<2>(p.adj, lo, hi, b, row, p.eq_cols);
+            case 3: return short_list_count<3>(p.adj, lo, hi, b, row, p.eq_cols);
+            case 4: return short_list_count<4>(p.adj, lo, hi, b, row, p.eq_cols);
+            case 5: return short_list_count<5>(p.adj, lo, hi, b, row, p.eq_cols);
+            case 6: return short_list_count<6>(p.adj, lo, hi, b, row, p.eq_cols);
+            case 7: return short_list_count<7>(p.adj, lo, hi, b, row, p.eq_cols);
+            default: return short_list_count<8>(p.adj, lo, hi, b, row, p.eq_cols);
         }
-        return m;
     }
+    if (p.bound_col >= 0) {
+        const uint64_t b = (uint64_t)row[p.bound_col] + p.bound_incl;
+        hi = lower_bound_u32(p.adj, lo, hi, b);
+        if (lo >= hi) return 0;
+    }
+    uint32_t n = hi - lo;
     for (uint32_t j = 0; j < p.n_eq; ++j) {
         const uint32_t w = row[p.eq_cols[j]];
         bool dup = false;  // the same vertex in two columns collides once
