@@ -828,6 +828,8 @@ struct PlanArgs {
     uint64_t items_cap;        // capacity of the per-item arrays
     uint32_t rows_next;        // rows per item of the next round
     uint32_t* overflow;        // set (never cleared) when a capacity is exceeded
+    uint64_t* bsum;            // [(nb + 1) * kPlanVals] per-block sums, then their exclusive scan and the totals
+    uint32_t nb;               // blocks of kPlanThreads tasks covering refs_cap
 };
 
 constexpr int kPlanThreads = 512;
@@ -895,35 +897,48 @@ __device__ __forceinline__ void plan_scan(const uint64_t v[kPlanVals], uint64_t 
     __syncthreads();  // sh read by every thread before the next scan rewrites it
 }
 
-// One block: records every task's output rows (node_total), places the
-// writing tasks' outputs in the round's region, lists them for the write
-// pass, and lists the next round's tasks (their children, light class
-// first) with their item prefix.  A region, task or item capacity exceeded
+// Planning of one round in three launches over blocks of kPlanThreads
+// tasks: the blocks' sums (plan_sum_kernel), their exclusive scan and the
+// round's totals (plan_top_kernel, one block), then every task's places
+// (plan_write_kernel): each task's output rows are recorded (node_total),
+// the writing tasks' outputs placed in the round's region and listed for the
+// write pass, and the next round's tasks (their children, light class first)
+// listed with their item prefix.  A region, task or item capacity exceeded
 // marks the run overflowed: no later launch of the run finds work, and the
 // host runs the session's rounds itself.
-__global__ void __launch_bounds__(kPlanThreads) round_plan_kernel(PlanArgs p) {
+__global__ void __launch_bounds__(kPlanThreads) plan_sum_kernel(PlanArgs p) {
     __shared__ uint64_t sh[kPlanThreads / 32][kPlanVals];
-    __shared__ uint64_t tot_s[kPlanVals];
-    __shared__ uint32_t bad_s;
-    RunState& st = *p.st;
-    RunState& nx = *p.nx;
+    const RunState& st = *p.st;
     const uint32_t nt = st.overflow ? 0u : st.nt;
-    const uint32_t ntl = st.nt_light;
-    uint64_t v[kPlanVals], ex[kPlanVals], sum[kPlanVals];
+    const uint32_t t = blockIdx.x * kPlanThreads + threadIdx.x;
+    uint64_t v[kPlanVals] = {}, ex[kPlanVals], sum[kPlanVals];
     uint32_t node;
     uint64_t tot, per;
-    // pass 1: the round's sums
-    uint64_t acc[kPlanVals] = {};
-    for (uint32_t t = threadIdx.x; t < nt; t += kPlanThreads) {
-        plan_values(p, ntl, t, v, node, tot, per);
+    if (t < nt) plan_values(p, st.nt_light, t, v, node, tot, per);
+    plan_scan(v, ex, sum, sh);
+    if (threadIdx.x < kPlanVals) p.bsum[(size_t)blockIdx.x * kPlanVals + threadIdx.x] = sum[threadIdx.x];
+}
+
+__global__ void __launch_bounds__(kPlanThreads) plan_top_kernel(PlanArgs p) {
+    __shared__ uint64_t sh[kPlanThreads / 32][kPlanVals];
+    RunState& st = *p.st;
+    RunState& nx = *p.nx;
+    uint64_t v[kPlanVals], ex[kPlanVals], sum[kPlanVals], carry[kPlanVals] = {};
+    for (uint32_t base = 0; base < p.nb; base += kPlanThreads) {
+        const uint32_t b = base + threadIdx.x;
 #pragma unroll
-        for (int k = 0; k < kPlanVals; ++k) acc[k] += v[k];
+        for (int k = 0; k < kPlanVals; ++k) v[k] = b < p.nb ? p.bsum[(size_t)b * kPlanVals + k] : 0;
+        plan_scan(v, ex, sum, sh);
+        if (b < p.nb)
+#pragma unroll
+            for (int k = 0; k < kPlanVals; ++k) p.bsum[(size_t)b * kPlanVals + k] = carry[k] + ex[k];
+#pragma unroll
+        for (int k = 0; k < kPlanVals; ++k) carry[k] += sum[k];
     }
-    plan_scan(acc, ex, sum, sh);
     if (threadIdx.x == 0) {
-        const bool bad = st.overflow || sum[0] > p.region_words || sum[4] + sum[5] > p.refs_cap ||
-                         sum[6] + sum[7] > p.items_cap;
-        bad_s = bad ? 1u : 0u;
+        const uint64_t* tot = carry;
+        const bool bad = st.overflow || tot[0] > p.region_words || tot[4] + tot[5] > p.refs_cap ||
+                         tot[6] + tot[7] > p.items_cap;
         if (bad) {
             st.overflow = 1;
             st.nw = 0;
@@ -933,57 +948,56 @@ __global__ void __launch_bounds__(kPlanThreads) round_plan_kernel(PlanArgs p) {
             nx.ni = nx.ni_light = 0;
             *p.overflow = 1;
         } else {
-            st.nw = (uint32_t)sum[1];
-            st.wi = sum[2];
-            st.wi_light = sum[3];
-            nx.nt = (uint32_t)(sum[4] + sum[5]);
-            nx.nt_light = (uint32_t)sum[4];
-            nx.ni = sum[6] + sum[7];
-            nx.ni_light = sum[6];
-            p.witem0[sum[1]] = sum[2];
-            p.next_item0[sum[4] + sum[5]] = sum[6] + sum[7];
+            st.nw = (uint32_t)tot[1];
+            st.wi = tot[2];
+            st.wi_light = tot[3];
+            nx.nt = (uint32_t)(tot[4] + tot[5]);
+            nx.nt_light = (uint32_t)tot[4];
+            nx.ni = tot[6] + tot[7];
+            nx.ni_light = tot[6];
+            p.witem0[tot[1]] = tot[2];
+            p.next_item0[tot[4] + tot[5]] = tot[6] + tot[7];
         }
 #pragma unroll
-        for (int k = 0; k < kPlanVals; ++k) tot_s[k] = sum[k];
+        for (int k = 0; k < kPlanVals; ++k) p.bsum[(size_t)p.nb * kPlanVals + k] = tot[k];
     }
-    __syncthreads();
-    if (bad_s) return;
-    const uint64_t light_tasks = tot_s[4], light_items = tot_s[6];
-    // pass 2: prefixes, outputs and the next round's tasks
-    uint64_t carry[kPlanVals] = {};
-    for (uint32_t base = 0; base < nt; base += kPlanThreads) {
-        const uint32_t t = base + threadIdx.x;
-#pragma unroll
-        for (int k = 0; k < kPlanVals; ++k) v[k] = 0;
-        tot = per = 0;
-        node = 0;
-        if (t < nt) plan_values(p, ntl, t, v, node, tot, per);
-        plan_scan(v, ex, sum, sh);
-        if (t < nt) {
-            p.node_total[node] = tot;
-            uint32_t* out = nullptr;
-            if (v[1]) {
-                out = p.region + carry[0] + ex[0];
-                const uint64_t slot = carry[1] + ex[1];
-                p.wtask[slot] = t;
-                p.witem0[slot] = carry[2] + ex[2];
-                const NodeRun nr = p.info[node];
-                const uint64_t j0 = carry[4] + ex[4], i0 = carry[6] + ex[6];
-                for (uint32_t i = 0; i < nr.n_light; ++i) {
-                    p.next_refs[j0 + i] = TaskRef{__ldg(p.children + nr.child0 + i), 0u, out, tot};
-                    p.next_item0[j0 + i] = i0 + (uint64_t)i * per;
-                }
-                const uint64_t j1 = light_tasks + carry[5] + ex[5], i1 = light_items + carry[7] + ex[7];
-                for (uint32_t i = 0; i < nr.n_fused; ++i) {
-                    p.next_refs[j1 + i] = TaskRef{__ldg(p.children + nr.child0 + nr.n_light + i), 0u, out, tot};
-                    p.next_item0[j1 + i] = i1 + (uint64_t)i * per;
-                }
-            }
-            p.outs[t] = out;
+}
+
+__global__ void __launch_bounds__(kPlanThreads) plan_write_kernel(PlanArgs p) {
+    __shared__ uint64_t sh[kPlanThreads / 32][kPlanVals];
+    const RunState& st = *p.st;
+    if (st.overflow) return;  // uniform: set before this launch
+    const uint32_t nt = st.nt;
+    const uint32_t t = blockIdx.x * kPlanThreads + threadIdx.x;
+    uint64_t v[kPlanVals] = {}, ex[kPlanVals], sum[kPlanVals];
+    uint32_t node = 0;
+    uint64_t tot = 0, per = 0;
+    if (t < nt) plan_values(p, st.nt_light, t, v, node, tot, per);
+    plan_scan(v, ex, sum, sh);
+    if (t >= nt) return;
+    const uint64_t* carry = p.bsum + (size_t)blockIdx.x * kPlanVals;
+    const uint64_t light_tasks = p.bsum[(size_t)p.nb * kPlanVals + 4];
+    const uint64_t light_items = p.bsum[(size_t)p.nb * kPlanVals + 6];
+    p.node_total[node] = tot;
+    uint32_t* out = nullptr;
+    if (v[1]) {
+        out = p.region + carry[0] + ex[0];
+        const uint64_t slot = carry[1] + ex[1];
+        p.wtask[slot] = t;
+        p.witem0[slot] = carry[2] + ex[2];
+        const NodeRun nr = p.info[node];
+        const uint64_t j0 = carry[4] + ex[4], i0 = carry[6] + ex[6];
+        for (uint32_t i = 0; i < nr.n_light; ++i) {
+            p.next_refs[j0 + i] = TaskRef{__ldg(p.children + nr.child0 + i), 0u, out, tot};
+            p.next_item0[j0 + i] = i0 + (uint64_t)i * per;
         }
-#pragma unroll
-        for (int k = 0; k < kPlanVals; ++k) carry[k] += sum[k];
+        const uint64_t j1 = light_tasks + carry[5] + ex[5], i1 = light_items + carry[7] + ex[7];
+        for (uint32_t i = 0; i < nr.n_fused; ++i) {
+            p.next_refs[j1 + i] = TaskRef{__ldg(p.children + nr.child0 + nr.n_light + i), 0u, out, tot};
+            p.next_item0[j1 + i] = i1 + (uint64_t)i * per;
+        }
     }
+    p.outs[t] = out;
 }
 
 std::atomic<uint64_t> g_batch_launches{0};
@@ -2024,8 +2038,10 @@ int BatchSession::run_device() {
     const size_t o_ntot = o_witem0 + al(((size_t)refs_cap + 1) * 8);
     const size_t o_info = o_ntot + al(nn * 8);
     const size_t o_kids = o_info + al(nn * sizeof(NodeRun));
+    const uint32_t nb = (refs_cap + kPlanThreads - 1) / kPlanThreads;
     const size_t o_flag = o_kids + al(std::max<size_t>(kids.size(), 1) * 4);
-    const size_t o_items = o_flag + 256;
+    const size_t o_bsum = o_flag + 256;
+    const size_t o_items = o_bsum + al(((size_t)nb + 1) * kPlanVals * 8);
     const size_t o_chunks = o_items + al(items_cap * 8);
     const size_t small_bytes = o_chunks + al((chunks_cap + 1) * 8);
     {
@@ -2131,8 +2147,12 @@ int BatchSession::run_device() {
         pa.items_cap = items_cap;
         pa.rows_next = R[d + 1];
         pa.overflow = d_flag;
-        round_plan_kernel<<<1, kPlanThreads, 0, s>>>(pa);
-        nl += 3;
+        pa.bsum = (uint64_t*)(blk + o_bsum);
+        pa.nb = nb;
+        plan_sum_kernel<<<nb, kPlanThreads, 0, s>>>(pa);
+        plan_top_kernel<<<1, kPlanThreads, 0, s>>>(pa);
+        plan_write_kernel<<<nb, kPlanThreads, 0, s>>>(pa);
+        nl += 5;
         if (d < D) {  // the deepest round's tasks have no children
             RoundArgs wa = ra;
             wa.wtask = wtask;
