@@ -206,13 +206,24 @@ __device__ __forceinline__ bool ext_accept(const ExtArgs& p, const uint32_t* row
     return true;
 }
 
+// A row of width k + 1 that exists only as a row of width k plus the
+// candidate c in column k: a step that follows another is evaluated on the
+// rows the first one would write without writing them.  The row helpers
+// below take either this or a plain pointer to k words.
+struct ExtRow {
+    const uint32_t* row;
+    uint32_t k;
+    uint32_t c;
+    __device__ __forceinline__ uint32_t operator[](uint32_t j) const { return j < k ? row[j] : c; }
+};
+
 // Candidates of a short list [lo, hi) below bound b that equal none of the
 // row's NEQ matched vertices (columns eq_cols), in one pass over the list;
 // the list is ascending, so the walk stops at the bound (no search for it).
 // A vertex in two columns still excludes its candidate once.
-template <int NEQ>
+template <int NEQ, class Row>
 __device__ __forceinline__ uint32_t short_list_count(const uint32_t* __restrict__ adj, uint32_t lo, uint32_t hi,
-                                                     uint64_t b, const uint32_t* row, const uint8_t* eq_cols) {
+                                                     uint64_t b, const Row& row, const uint8_t* eq_cols) {
     uint32_t eqv[NEQ > 0 ? NEQ : 1];
 #pragma unroll
     for (int e = 0; e < NEQ; ++e) eqv[e] = row[eq_cols[e]];
@@ -231,7 +242,8 @@ __device__ __forceinline__ uint32_t short_list_count(const uint32_t* __restrict_
 // Number of candidates of one row of a plain extension (no fused checks):
 // the segment below the restriction bound minus the already-matched
 // vertices in it.
-__device__ __forceinline__ uint32_t ext_count_plain(const ExtArgs& p, const uint32_t* row) {
+template <class Row>
+__device__ __forceinline__ uint32_t ext_count_plain(const ExtArgs& p, const Row& row) {
     uint32_t lo, hi;
     seg_of(p.off, p.L, row[p.src_col], p.lab, lo, hi);
     if (lo >= hi) return 0;
@@ -277,7 +289,8 @@ __device__ __forceinline__ uint32_t ext_count_row(const ExtArgs& p, const uint32
     return ext_count_plain(p, row);
 }
 
-__device__ __forceinline__ bool red_keep_row(const RedArgs& p, const uint32_t* row) {
+template <class Row>
+__device__ __forceinline__ bool red_keep_row(const RedArgs& p, const Row& row) {
     for (uint32_t j = 0; j < p.n_pairs; ++j) {
         const uint32_t s = row[p.rs[j]];
         const uint32_t e = row[p.re[j]];
