@@ -2156,18 +2156,22 @@ int BatchSession::run_device() {
     for (size_t id = 0; id < nn; ++id)
         for (int c = nodes[id].first_child; c >= 0; c = nodes[c].next_sibling)
             if (live(c)) leaf[id] = 0;
-    auto fuse = [&](int n, int c) { return pair_fusion && leaf[c] && !nodes[n].fused && !nodes[c].fused; };
+    auto fuse = [&](int n, int c) {
+        return pair_fusion && nodes[n].depth > 0 && leaf[c] && !nodes[n].fused && !nodes[c].fused;
+    };
+    std::vector<char> by_pair(nn, 0);  // leaves counted in their parent's pair tasks
+    for (size_t id = 0; id < nn; ++id)
+        for (int c = nodes[id].first_child; c >= 0; c = nodes[c].next_sibling)
+            if (live(c) && fuse((int)id, c)) {
+                by_pair[c] = 1;
+                n_pairs[id]++;
+            }
     for (size_t id = 0; id < nn; ++id) {
         const BNode& nd = nodes[id];
         bool o = nd.first_term >= 0;
         for (int c = nd.first_child; c >= 0; c = nodes[c].next_sibling)
-            if (live(c)) {
-                if (nd.depth > 0 && fuse((int)id, c))
-                    n_pairs[id]++;
-                else
-                    o = true;
-            }
-        own[id] = o ? 1 : 0;
+            if (live(c) && !by_pair[c]) o = true;
+        own[id] = o && !by_pair[id] ? 1 : 0;
     }
     // the templates of the tasks made from a node's output: per child n that
     // can match, (n, 0) when n has a task of its own and (n, 1 + leaf) per
@@ -2213,7 +2217,7 @@ int BatchSession::run_device() {
         size_t cnt[3] = {0, 0, 0};
         for (uint32_t cls : cls_order)
             for (int c = nd.first_child; c >= 0; c = nodes[c].next_sibling)
-                if (live(c))
+                if (live(c) && !by_pair[c])  // leaves counted in id's pair tasks are done
                     templates(c, cls, [&](uint2 tp) {
                         kids.push_back(tp);
                         cnt[cls]++;
