@@ -507,15 +507,22 @@ __device__ __forceinline__ uint64_t red_item(const TaskDesc& d, const uint32_t* 
     return warp_sum(total);
 }
 
-// A leaf step (plain extension or reduction, it only counts) on one row its
-// parent step would write.
+// A leaf step (it only counts: an extension, plain or with fused back-edge
+// checks, or a reduction) on one row its parent step would write.
 __device__ __forceinline__ uint32_t leaf_count(const TaskDesc& c, const ExtRow& r) {
-    return c.kind == STEP_EXT ? ext_count_plain(c.e, r) : (red_keep_row(c.r, r) ? 1u : 0u);
+    if (c.kind != STEP_EXT) return red_keep_row(c.r, r) ? 1u : 0u;
+    if (c.e.n_chk == 0) return ext_count_plain(c.e, r);
+    GenState g;
+    ext_generator(c.e, r, g);
+    uint32_t n = 0;
+    for (uint32_t j = g.lo; j < g.hi; ++j) n += ext_accept(c.e, r, __ldg(g.gadj + j), g) ? 1u : 0u;
+    return n;
 }
 
 // Pair task (device-scheduled rounds): the count of leaf step c over the
-// rows that step d (a plain extension or a reduction) makes from the item's
-// rows, without writing them: every candidate d accepts is tested by c on
+// rows that step d (a plain extension or a reduction; c any extension or
+// reduction) makes from the item's rows, without writing them: every
+// candidate d accepts is tested by c on
 // the spot.  The same candidates as d's write pass would append (lists
 // longer than `hub` shared by the warp), so the count equals c's count over
 // d's written output; per-graph accounting goes by each row's first vertex,
@@ -2139,10 +2146,10 @@ int BatchSession::run_device() {
     for (const BTask& tk : active)
         if (nodes[tk.node].depth != 1) return GVA_OK;
     // Leaf steps counted on their parent's rows: a leaf (no child that can
-    // match) of the light class under a light-class node n is counted by a
-    // pair task (n, leaf) in n's round, from n's input rows; n then writes
-    // only for its other children, and has a task of its own only when it
-    // ends a plan or has such children.
+    // match) under a light-class node n is counted by a pair task (n, leaf)
+    // in n's round, from n's input rows; n then writes only for its other
+    // children, and has a task of its own only when it ends a plan or has
+    // such children.
     auto t_lap = t_start;
     auto lap = [&](int k) {  // phase_ms: schedule tables, uploads, launches, -, results
         const auto now = std::chrono::steady_clock::now();
@@ -2156,9 +2163,7 @@ int BatchSession::run_device() {
     for (size_t id = 0; id < nn; ++id)
         for (int c = nodes[id].first_child; c >= 0; c = nodes[c].next_sibling)
             if (live(c)) leaf[id] = 0;
-    auto fuse = [&](int n, int c) {
-        return pair_fusion && nodes[n].depth > 0 && leaf[c] && !nodes[n].fused && !nodes[c].fused;
-    };
+    auto fuse = [&](int n, int c) { return pair_fusion && nodes[n].depth > 0 && leaf[c] && !nodes[n].fused; };
     std::vector<char> by_pair(nn, 0);  // leaves counted in their parent's pair tasks
     for (size_t id = 0; id < nn; ++id)
         for (int c = nodes[id].first_child; c >= 0; c = nodes[c].next_sibling)

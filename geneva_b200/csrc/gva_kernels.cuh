@@ -129,6 +129,17 @@ __device__ __forceinline__ uint32_t find_in(const uint32_t* __restrict__ adj, ui
     return (pos < hi && __ldg(adj + pos) == w) ? pos : 0xffffffffu;
 }
 
+// A row of width k + 1 that exists only as a row of width k plus the
+// candidate c in column k: a step that follows another is evaluated on the
+// rows the first one would write without writing them.  The row helpers
+// below take either this or a plain pointer to k words.
+struct ExtRow {
+    const uint32_t* row;
+    uint32_t k;
+    uint32_t c;
+    __device__ __forceinline__ uint32_t operator[](uint32_t j) const { return j < k ? row[j] : c; }
+};
+
 // Candidate source of a row with fused checks: the shortest of the source
 // segment and the dir-0 check segments, each cut below the restriction
 // bound.  The segments stay in the state, so that membership tests of the
@@ -142,7 +153,8 @@ struct GenState {
     uint32_t clo[kMaxChecks], chi[kMaxChecks];  // dir-0 check segments
 };
 
-__device__ __forceinline__ void ext_generator(const ExtArgs& p, const uint32_t* row, GenState& g) {
+template <class Row>
+__device__ __forceinline__ void ext_generator(const ExtArgs& p, const Row& row, GenState& g) {
     uint32_t slo, shi;
     seg_of(p.off, p.L, row[p.src_col], p.lab, slo, shi);
     g.gadj = p.adj;
@@ -193,7 +205,8 @@ __device__ __forceinline__ bool seg_has(const uint32_t* __restrict__ off, const 
 
 // Whether generated candidate c survives injectivity, the source edge (when
 // the generator is a check segment) and every other check.
-__device__ __forceinline__ bool ext_accept(const ExtArgs& p, const uint32_t* row, uint32_t c, const GenState& g) {
+template <class Row>
+__device__ __forceinline__ bool ext_accept(const ExtArgs& p, const Row& row, uint32_t c, const GenState& g) {
     for (uint32_t j = 0; j < p.n_eq; ++j)
         if (row[p.eq_cols[j]] == c) return false;
     if (g.which >= 0 && find_in(p.adj, g.slo, g.shi, c) == 0xffffffffu) return false;
@@ -205,17 +218,6 @@ __device__ __forceinline__ bool ext_accept(const ExtArgs& p, const uint32_t* row
     }
     return true;
 }
-
-// A row of width k + 1 that exists only as a row of width k plus the
-// candidate c in column k: a step that follows another is evaluated on the
-// rows the first one would write without writing them.  The row helpers
-// below take either this or a plain pointer to k words.
-struct ExtRow {
-    const uint32_t* row;
-    uint32_t k;
-    uint32_t c;
-    __device__ __forceinline__ uint32_t operator[](uint32_t j) const { return j < k ? row[j] : c; }
-};
 
 // Candidates of a short list [lo, hi) below bound b that equal none of the
 // row's NEQ matched vertices (columns eq_cols), in one pass over the list;
