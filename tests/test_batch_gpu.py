@@ -239,10 +239,10 @@ def test_device_rounds_overflow_falls_back_to_host(native, oracle):
              "v 0 1\nv 1 2\nv 2 1\nv 3 2\ne 0 1 1\ne 1 2 1\ne 2 3 1\n",  # a 3-edge path
              "v 0 1\nv 1 2\nv 2 2\nv 3 1\ne 0 1 1\ne 0 2 1\ne 0 3 1\n"]  # a 3-edge star
     checked = len(pats)
-    # a 4-edge path: its 2-edge prefixes (~150 K rows of 3 columns) are
-    # written, more than a 1 MiB region holds (the last two steps are counted
-    # from them without being written)
-    pats += ["v 0 1\nv 1 2\nv 2 1\nv 3 2\nv 4 1\ne 0 1 1\ne 1 2 1\ne 2 3 1\ne 3 4 1\n"]
+    # a 5-edge path: its 3-edge prefixes (several hundred thousand rows of 4
+    # columns) are written, more than a 1 MiB region holds (its last two steps
+    # are counted from them without being written)
+    pats += ["v 0 1\nv 1 2\nv 2 1\nv 3 2\nv 4 1\nv 5 2\ne 0 1 1\ne 1 2 1\ne 2 3 1\ne 3 4 1\ne 4 5 1\n"]
     plans = [gv.Plan.from_text(p) for p in pats]
     want, _, hs = gv.batch_count(gdb, plans, host_rounds=True)
     assert [int(c) for c in want[:checked]] == [oracle.count(og, p) for p in pats[:checked]]
