@@ -79,12 +79,9 @@ struct BatchCtx {
 // Per-round task reference: a node's descriptor and a frontier slice.  The
 // slice is cut into items of `rows_per_item` rows; task t owns the count
 // pass's items [item0[t], item0[t + 1]).
-// pair (device-scheduled rounds only): 0, or 1 + a leaf node whose step is
-// counted on the rows `node`'s step would write (the task's count is the
-// leaf's; nothing is written)
 struct TaskRef {
     uint32_t node;
-    uint32_t pair;
+    uint32_t pad;
     const uint32_t* in;
     uint64_t nrows;
 };
@@ -101,19 +98,14 @@ constexpr int kScanChunkLog2 = 12;
 // the write pass's (written by this round's planning kernel) and the four
 // work-queue heads (zero when the state is created).  A set `overflow` makes
 // every later launch of the run find no work.
-// Tasks come light class first, then pair tasks, then the fused class.
 struct RunState {
-    uint64_t ni, ni_light, ni_pair;  // count items: all, light class, pair tasks
-    uint64_t wi, wi_light;           // write items: all, light class (pair tasks never write)
-    uint32_t nt, nt_light, nt_pair;  // count tasks: all, light class, pair tasks
-    uint32_t nw;                     // writing tasks
-    uint32_t overflow;               // frontier region, task or item capacity exceeded
-    uint32_t pad;
-    unsigned long long heads[5];  // queue heads: count light, count fused, write light, write fused, pair count
+    uint64_t ni, ni_light;  // count items: all, light class (the light class's items come first)
+    uint64_t wi, wi_light;  // write items: all, light class
+    uint32_t nt, nt_light;  // count tasks: all, light class
+    uint32_t nw;            // writing tasks
+    uint32_t overflow;      // frontier region, task or item capacity exceeded
+    unsigned long long heads[4];  // queue heads: count light, count fused, write light, write fused
 };
-
-// launch classes of the round kernels
-enum LaunchClass : uint32_t { CLS_LIGHT = 0, CLS_FUSED = 1, CLS_PAIR = 2 };
 
 struct RoundArgs {
     const TaskDesc* nodes;
@@ -150,7 +142,7 @@ struct Span {
 };
 
 template <bool WRITE>
-__device__ __forceinline__ Span launch_span(const RoundArgs& a, uint32_t cls) {
+__device__ __forceinline__ Span launch_span(const RoundArgs& a, bool fused) {
     Span s;
     s.warps = gridDim.x * kRoundWarps;
     if (!a.dyn) {
@@ -163,19 +155,13 @@ __device__ __forceinline__ Span launch_span(const RoundArgs& a, uint32_t cls) {
         return s;
     }
     const RunState& st = *a.dyn;
-    if (WRITE) {
-        s.base = cls == CLS_FUSED ? st.wi_light : 0;
-        s.n = cls == CLS_FUSED ? st.wi - st.wi_light : st.wi_light;
-        s.nt = st.nw;
-    } else {
-        const uint64_t lp = st.ni_light + st.ni_pair;
-        s.base = cls == CLS_LIGHT ? 0 : cls == CLS_PAIR ? st.ni_light : lp;
-        s.n = cls == CLS_LIGHT ? st.ni_light : cls == CLS_PAIR ? st.ni_pair : st.ni - lp;
-        s.nt = st.nt;
-    }
+    const uint64_t all = WRITE ? st.wi : st.ni, light = WRITE ? st.wi_light : st.ni_light;
+    s.base = fused ? light : 0;
+    s.n = fused ? all - light : light;
+    s.nt = WRITE ? st.nw : st.nt;
     s.n_count_items = st.ni;
     s.n_chunks = (st.ni + kScanChunk - 1) / kScanChunk;
-    s.queue = a.dyn->heads + (cls == CLS_PAIR ? 4 : (WRITE ? 2 : 0) + (cls == CLS_FUSED ? 1 : 0));
+    s.queue = a.dyn->heads + (WRITE ? 2 : 0) + (fused ? 1 : 0);
     return s;
 }
 
@@ -507,86 +493,6 @@ __device__ __forceinline__ uint64_t red_item(const TaskDesc& d, const uint32_t* 
     return warp_sum(total);
 }
 
-// A leaf step (it only counts: an extension, plain or with fused back-edge
-// checks, or a reduction) on one row its parent step would write.
-__device__ __forceinline__ uint32_t leaf_count(const TaskDesc& c, const ExtRow& r) {
-    if (c.kind != STEP_EXT) return red_keep_row(c.r, r) ? 1u : 0u;
-    if (c.e.n_chk == 0) return ext_count_plain(c.e, r);
-    GenState g;
-    ext_generator(c.e, r, g);
-    uint32_t n = 0;
-    for (uint32_t j = g.lo; j < g.hi; ++j) n += ext_accept(c.e, r, __ldg(g.gadj + j), g) ? 1u : 0u;
-    return n;
-}
-
-// Pair task (device-scheduled rounds): the count of leaf step c over the
-// rows that step d (a plain extension or a reduction; c any extension or
-// reduction) makes from the item's rows, without writing them: every
-// candidate d accepts is tested by c on
-// the spot.  The same candidates as d's write pass would append (lists
-// longer than `hub` shared by the warp), so the count equals c's count over
-// d's written output; per-graph accounting goes by each row's first vertex,
-// which the rows d makes share with their source row.
-__device__ __forceinline__ uint64_t pair_item(const TaskDesc& d, const TaskDesc& c, const uint32_t* rows_s, uint32_t nr,
-                                           uint32_t hub, const BatchCtx& ctx) {
-    const int lane = threadIdx.x & 31;
-    const bool graphs = c.mode == MODE_COUNT_GRAPHS || c.mode == MODE_WRITE_AND_GRAPHS;
-    uint64_t total = 0;
-    if (d.kind != STEP_EXT) {  // a reduction keeps or drops each row
-        const RedArgs& p = d.r;
-        const uint32_t k = p.k;
-        for (uint32_t base = 0; base < nr; base += 32) {
-            const uint32_t r = base + lane;
-            const bool valid = r < nr;
-            const uint32_t* row = rows_s + (valid ? r : 0) * k;
-            uint32_t cnt = 0;
-            if (valid && red_keep_row(p, row)) cnt = leaf_count(c, ExtRow{row, k, 0u});
-            if (graphs) add_graph_count(ctx, c.query, row[0], cnt, valid);
-            total += cnt;
-        }
-        return warp_sum(total);
-    }
-    const ExtArgs& p = d.e;
-    const uint32_t k = p.k;
-    const bool eq8 = p.n_eq <= 8;
-    for (uint32_t base = 0; base < nr; base += 32) {
-        const uint32_t r = base + lane;
-        const bool valid = r < nr;
-        const uint32_t* row = rows_s + (valid ? r : 0) * k;
-        uint32_t lo = 0, hi = 0;
-        if (valid) ext_range(p, row, lo, hi);
-        const uint32_t len = hi > lo ? hi - lo : 0;
-        const bool is_hub = len > hub;
-        uint32_t eqv[8];
-        if (eq8) load_eqv(p, row, eqv);
-        uint32_t cnt = 0;
-        if (!is_hub)
-            for (uint32_t j = lo; j < hi; ++j) {
-                const uint32_t x = __ldg(p.adj + j);
-                if (eq8 ? injective8(eqv, x) : ext_injective(p, row, x)) cnt += leaf_count(c, ExtRow{row, k, x});
-            }
-        // hub rows: the whole warp, one candidate per lane
-        uint32_t hubs = __ballot_sync(0xffffffffu, is_hub);
-        while (hubs) {
-            const int h = __ffs(hubs) - 1;
-            hubs &= hubs - 1;
-            const uint32_t hlo = __shfl_sync(0xffffffffu, lo, h), hhi = __shfl_sync(0xffffffffu, hi, h);
-            const uint32_t* hrow = rows_s + (base + h) * k;
-            if (eq8) load_eqv(p, hrow, eqv);
-            uint32_t hc = 0;
-            for (uint32_t j = hlo + lane; j < hhi; j += 32) {
-                const uint32_t x = __ldg(p.adj + j);
-                if (eq8 ? injective8(eqv, x) : ext_injective(p, hrow, x)) hc += leaf_count(c, ExtRow{hrow, k, x});
-            }
-            hc = __reduce_add_sync(0xffffffffu, hc);
-            if (lane == h) cnt += hc;
-        }
-        if (graphs) add_graph_count(ctx, c.query, row[0], cnt, valid);
-        total += cnt;
-    }
-    return warp_sum(total);
-}
-
 // Class of a task: fused extensions apart from everything else.
 __host__ __device__ __forceinline__ bool fused_class(uint32_t kind, uint32_t n_chk) {
     return kind == STEP_EXT && n_chk > 0;
@@ -607,11 +513,6 @@ __host__ __device__ constexpr size_t round_warp_words(uint32_t rows_per_item, ui
 size_t round_smem_bytes(uint32_t rows_per_item, uint32_t kmax, bool write, bool fused) {
     return (size_t)kRoundWarps *
            (sizeof(TaskDesc) + (fused ? kGenBytes : 0) + 4 * round_warp_words(rows_per_item, kmax, write, fused));
-}
-// Pair tasks' count pass: two descriptors (the task's step and the leaf
-// step) and one buffer of item rows per warp.
-size_t pair_smem_bytes(uint32_t rows_per_item, uint32_t kmax) {
-    return (size_t)kRoundWarps * (2 * sizeof(TaskDesc) + 4 * (((size_t)rows_per_item * kmax + 3) & ~(size_t)3));
 }
 
 struct WarpSmem {
@@ -653,7 +554,7 @@ round_count_kernel(RoundArgs a) {
     uint64_t begin, end;
     uint32_t cur = 0;    // light class: buffer of the current item
     bool ready = false;  // light class: the current item's rows were issued with the previous item
-    const Span sp = launch_span<false>(a, FUSED ? CLS_FUSED : CLS_LIGHT);
+    const Span sp = launch_span<false>(a, FUSED);
     while (next_chunk(sp, begin, end)) {
         for (uint64_t item = sp.base + begin; item < sp.base + end; ++item) {
             if (item >= t_hi || item < t_lo) {
@@ -700,48 +601,6 @@ round_count_kernel(RoundArgs a) {
                 c = red_item<false>(d, rows, nr, a.ctx, nullptr);
             if (lane == 0) a.items[item] = c;
             __syncwarp();  // every lane done with these rows before the buffer is refilled
-        }
-    }
-}
-
-// Pair tasks' count pass (device-scheduled rounds): persistent like the
-// count pass, over the pair tasks' items; each item's rows are staged, the
-// task's step expands them and the leaf step counts what it makes
-// (pair_item).
-__global__ void __launch_bounds__(kRoundWarps * 32, 5) round_pair_kernel(RoundArgs a) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    TaskDesc& d = reinterpret_cast<TaskDesc*>(smem_raw)[warp];
-    TaskDesc& c = reinterpret_cast<TaskDesc*>(smem_raw)[kRoundWarps + warp];
-    uint32_t* rows = reinterpret_cast<uint32_t*>(smem_raw + 2 * kRoundWarps * sizeof(TaskDesc)) +
-                     (size_t)warp * (((size_t)a.rows_per_item * a.kmax + 3) & ~(size_t)3);
-    uint32_t t = 0xffffffffu;
-    uint64_t t_lo = 0, t_hi = 0;
-    const uint32_t* in = nullptr;
-    uint64_t nrows = 0;
-    uint64_t begin, end;
-    const Span sp = launch_span<false>(a, CLS_PAIR);
-    while (next_chunk(sp, begin, end)) {
-        for (uint64_t item = sp.base + begin; item < sp.base + end; ++item) {
-            if (item >= t_hi || item < t_lo) {
-                t = find_slot(a.item0, sp.nt + 1, item);
-                t_lo = __ldg(a.item0 + t);
-                t_hi = __ldg(a.item0 + t + 1);
-                const TaskRef& ref = a.refs[t];
-                in = ref.in;
-                nrows = ref.nrows;
-                __syncwarp();
-                load_desc(d, a.nodes + ref.node);
-                load_desc(c, a.nodes + (ref.pair - 1));
-            }
-            const uint64_t row0 = (item - t_lo) * a.rows_per_item;
-            const uint32_t nr = (uint32_t)umin64(a.rows_per_item, nrows - row0);
-            const uint32_t k = d.kind == STEP_EXT ? d.e.k : d.r.k;
-            __syncwarp();
-            stage_rows(rows, in, row0, nr, k);
-            const uint64_t n = pair_item(d, c, rows, nr, a.hub, a.ctx);
-            if (lane == 0) a.items[item] = n;
-            __syncwarp();  // every lane done with these rows before they are restaged
         }
     }
 }
@@ -863,7 +722,7 @@ round_write_kernel(RoundArgs a) {
     uint64_t begin, end;
     uint32_t cur = 0;    // light class: buffer of the current item
     bool ready = false;  // light class: the current item's rows were issued with the previous item
-    const Span sp = launch_span<true>(a, FUSED ? CLS_FUSED : CLS_LIGHT);
+    const Span sp = launch_span<true>(a, FUSED);
     while (next_chunk(sp, begin, end)) {
         for (uint64_t wi = sp.base + begin; wi < sp.base + end; ++wi) {
             if (wi >= w_hi || wi < w_lo) {
@@ -939,16 +798,14 @@ round_write_kernel(RoundArgs a) {
 // ------------------------------------------------- device-side planning ----
 // Rounds scheduled on the device (BatchSession::run_device).  Every task of
 // a round sits at the same trie depth (nothing is deferred or split), so a
-// round's tasks are made from the previous round's writing tasks.  Per node:
-// the tasks that read its output, as a range of task templates (node, pair;
-// light class first; the host makes them: each child that can match, unless
-// it only feeds leaves counted in pair tasks and ends no plan, and a pair
-// task per such leaf), and the words of one output row.
+// round's tasks are the children of the previous round's writing tasks.
+// Per node: the children that can match, light class first, as a range of
+// the children array, and the words of one output row.
 struct NodeRun {
     uint32_t child0;
-    uint16_t n_light, n_fused;  // templates: light class, then pair tasks, then fused class
-    uint32_t out_w;             // EXT: width + 1; REDUCE: width
-    uint16_t n_pair, pad;
+    uint16_t n_light, n_fused;
+    uint32_t out_w;  // EXT: width + 1; REDUCE: width
+    uint32_t pad;
 };
 
 struct PlanArgs {
@@ -958,8 +815,8 @@ struct PlanArgs {
     const uint64_t* item0;     // [nt + 1] this round's count-pass item prefix
     const uint64_t* totals;    // [nt] output rows per task
     const NodeRun* info;
-    const uint2* children;     // task templates (node, pair) of every node's range
-    uint64_t* node_total;      // output rows per node (zeroed before the run); a pair task's go to its leaf
+    const uint32_t* children;
+    uint64_t* node_total;      // output rows per node (zeroed before the run)
     uint32_t* region;          // this round's output frontier region
     uint64_t region_words;
     uint32_t** outs;           // [nt] output base per task (null: not written)
@@ -976,20 +833,18 @@ struct PlanArgs {
 };
 
 constexpr int kPlanThreads = 512;
-constexpr int kPlanVals = 10;
+constexpr int kPlanVals = 8;
 
 // Task t's contributions: 0 output words (rounded up to 16 bytes), 1 writes,
-// 2 write items, 3 write items of the light class, 4 / 5 / 8 light / fused /
-// pair tasks made from it, 6 / 7 / 9 their items.  A task writes when it has
-// output rows and tasks that read them.  node: the node whose output rows
-// the task counted (a pair task's leaf).
+// 2 write items, 3 write items of the light class, 4 / 5 light / fused child
+// tasks, 6 / 7 their items.  A task writes when it has output rows and a
+// child that can match.
 __device__ __forceinline__ void plan_values(const PlanArgs& p, uint32_t nt_light, uint32_t t, uint64_t v[kPlanVals],
                                             uint32_t& node, uint64_t& tot, uint64_t& per) {
-    const TaskRef ref = p.refs[t];
-    node = ref.pair ? ref.pair - 1 : ref.node;
+    node = p.refs[t].node;
     tot = p.totals[t];
     const NodeRun nr = p.info[node];
-    const bool w = tot > 0 && nr.n_light + nr.n_fused + nr.n_pair > 0;
+    const bool w = tot > 0 && nr.n_light + nr.n_fused > 0;
     per = w ? (tot + p.rows_next - 1) / p.rows_next : 0;
     const uint64_t items = p.item0[t + 1] - p.item0[t];
     v[0] = w ? ((tot * nr.out_w + 3) & ~3ull) : 0;
@@ -1000,8 +855,6 @@ __device__ __forceinline__ void plan_values(const PlanArgs& p, uint32_t nt_light
     v[5] = w ? nr.n_fused : 0;
     v[6] = per * nr.n_light;
     v[7] = per * nr.n_fused;
-    v[8] = w ? nr.n_pair : 0;
-    v[9] = per * nr.n_pair;
 }
 
 // Exclusive block scan of kPlanVals values per thread; sum receives the
@@ -1084,28 +937,26 @@ __global__ void __launch_bounds__(kPlanThreads) plan_top_kernel(PlanArgs p) {
     }
     if (threadIdx.x == 0) {
         const uint64_t* tot = carry;
-        const uint64_t tasks = tot[4] + tot[5] + tot[8], items = tot[6] + tot[7] + tot[9];
-        const bool bad = st.overflow || tot[0] > p.region_words || tasks > p.refs_cap || items > p.items_cap;
+        const bool bad = st.overflow || tot[0] > p.region_words || tot[4] + tot[5] > p.refs_cap ||
+                         tot[6] + tot[7] > p.items_cap;
         if (bad) {
             st.overflow = 1;
             st.nw = 0;
             st.wi = st.wi_light = 0;
             nx.overflow = 1;
-            nx.nt = nx.nt_light = nx.nt_pair = 0;
-            nx.ni = nx.ni_light = nx.ni_pair = 0;
+            nx.nt = nx.nt_light = 0;
+            nx.ni = nx.ni_light = 0;
             *p.overflow = 1;
         } else {
             st.nw = (uint32_t)tot[1];
             st.wi = tot[2];
             st.wi_light = tot[3];
-            nx.nt = (uint32_t)tasks;
+            nx.nt = (uint32_t)(tot[4] + tot[5]);
             nx.nt_light = (uint32_t)tot[4];
-            nx.nt_pair = (uint32_t)tot[8];
-            nx.ni = items;
+            nx.ni = tot[6] + tot[7];
             nx.ni_light = tot[6];
-            nx.ni_pair = tot[9];
             p.witem0[tot[1]] = tot[2];
-            p.next_item0[tasks] = items;
+            p.next_item0[tot[4] + tot[5]] = tot[6] + tot[7];
         }
 #pragma unroll
         for (int k = 0; k < kPlanVals; ++k) p.bsum[(size_t)p.nb * kPlanVals + k] = tot[k];
@@ -1125,9 +976,8 @@ __global__ void __launch_bounds__(kPlanThreads) plan_write_kernel(PlanArgs p) {
     plan_scan(v, ex, sum, sh);
     if (t >= nt) return;
     const uint64_t* carry = p.bsum + (size_t)blockIdx.x * kPlanVals;
-    const uint64_t* all = p.bsum + (size_t)p.nb * kPlanVals;  // the round's totals
-    const uint64_t light_tasks = all[4], light_items = all[6];
-    const uint64_t lp_tasks = all[4] + all[8], lp_items = all[6] + all[9];
+    const uint64_t light_tasks = p.bsum[(size_t)p.nb * kPlanVals + 4];
+    const uint64_t light_items = p.bsum[(size_t)p.nb * kPlanVals + 6];
     p.node_total[node] = tot;
     uint32_t* out = nullptr;
     if (v[1]) {
@@ -1138,20 +988,12 @@ __global__ void __launch_bounds__(kPlanThreads) plan_write_kernel(PlanArgs p) {
         const NodeRun nr = p.info[node];
         const uint64_t j0 = carry[4] + ex[4], i0 = carry[6] + ex[6];
         for (uint32_t i = 0; i < nr.n_light; ++i) {
-            const uint2 tp = p.children[nr.child0 + i];
-            p.next_refs[j0 + i] = TaskRef{tp.x, tp.y, out, tot};
+            p.next_refs[j0 + i] = TaskRef{__ldg(p.children + nr.child0 + i), 0u, out, tot};
             p.next_item0[j0 + i] = i0 + (uint64_t)i * per;
         }
-        const uint64_t j2 = light_tasks + carry[8] + ex[8], i2 = light_items + carry[9] + ex[9];
-        for (uint32_t i = 0; i < nr.n_pair; ++i) {
-            const uint2 tp = p.children[nr.child0 + nr.n_light + i];
-            p.next_refs[j2 + i] = TaskRef{tp.x, tp.y, out, tot};
-            p.next_item0[j2 + i] = i2 + (uint64_t)i * per;
-        }
-        const uint64_t j1 = lp_tasks + carry[5] + ex[5], i1 = lp_items + carry[7] + ex[7];
+        const uint64_t j1 = light_tasks + carry[5] + ex[5], i1 = light_items + carry[7] + ex[7];
         for (uint32_t i = 0; i < nr.n_fused; ++i) {
-            const uint2 tp = p.children[nr.child0 + nr.n_light + nr.n_pair + i];
-            p.next_refs[j1 + i] = TaskRef{tp.x, tp.y, out, tot};
+            p.next_refs[j1 + i] = TaskRef{__ldg(p.children + nr.child0 + nr.n_light + i), 0u, out, tot};
             p.next_item0[j1 + i] = i1 + (uint64_t)i * per;
         }
     }
@@ -1297,7 +1139,6 @@ int BatchSession::init() {
         GVA_CUDA_B(cudaFuncSetAttribute(round_count_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, most));
         GVA_CUDA_B(cudaFuncSetAttribute(round_write_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, most));
         GVA_CUDA_B(cudaFuncSetAttribute(round_write_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, most));
-        GVA_CUDA_B(cudaFuncSetAttribute(round_pair_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, most));
         smem_set[dev].store(true, std::memory_order_release);
     }
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
@@ -2142,114 +1983,82 @@ int BatchSession::run_device() {
                    (wait - wait0);
         }
     } timer{t_start, round_host_ms, wait_ms, wait_before};
-    const size_t nn = nodes.size();
-    for (const BTask& tk : active)
-        if (nodes[tk.node].depth != 1) return GVA_OK;
-    // Leaf steps counted on their parent's rows: a leaf (no child that can
-    // match) under a light-class node n is counted by a pair task (n, leaf)
-    // in n's round, from n's input rows; n then writes only for its other
-    // children, and has a task of its own only when it ends a plan or has
-    // such children.
     auto t_lap = t_start;
     auto lap = [&](int k) {  // phase_ms: schedule tables, uploads, launches, -, results
         const auto now = std::chrono::steady_clock::now();
         phase_ms[k] += std::chrono::duration<double, std::milli>(now - t_lap).count();
         t_lap = now;
     };
-    const bool pair_fusion = true;
-    auto live = [&](int c) { return !nodes[c].always_empty; };
-    std::vector<char> leaf(nn, 1), own(nn, 0);
-    std::vector<uint32_t> n_pairs(nn, 0);
-    for (size_t id = 0; id < nn; ++id)
-        for (int c = nodes[id].first_child; c >= 0; c = nodes[c].next_sibling)
-            if (live(c)) leaf[id] = 0;
-    auto fuse = [&](int n, int c) { return pair_fusion && nodes[n].depth > 0 && leaf[c] && !nodes[n].fused; };
-    std::vector<char> by_pair(nn, 0);  // leaves counted in their parent's pair tasks
-    for (size_t id = 0; id < nn; ++id)
-        for (int c = nodes[id].first_child; c >= 0; c = nodes[c].next_sibling)
-            if (live(c) && fuse((int)id, c)) {
-                by_pair[c] = 1;
-                n_pairs[id]++;
-            }
-    for (size_t id = 0; id < nn; ++id) {
-        const BNode& nd = nodes[id];
-        bool o = nd.first_term >= 0;
-        for (int c = nd.first_child; c >= 0; c = nodes[c].next_sibling)
-            if (live(c) && !by_pair[c]) o = true;
-        own[id] = o && !by_pair[id] ? 1 : 0;
-    }
-    // the templates of the tasks made from a node's output: per child n that
-    // can match, (n, 0) when n has a task of its own and (n, 1 + leaf) per
-    // leaf counted from n's input; cls: CLS_LIGHT / CLS_PAIR / CLS_FUSED
-    auto templates = [&](int n, uint32_t cls, auto&& emit) {
-        if (cls != CLS_PAIR) {
-            if (own[n] && nodes[n].fused == (cls == CLS_FUSED ? 1u : 0u)) emit(uint2{(uint32_t)n, 0u});
-            return;
-        }
-        if (n_pairs[n])
-            for (int c = nodes[n].first_child; c >= 0; c = nodes[c].next_sibling)
-                if (live(c) && fuse(n, c)) emit(uint2{(uint32_t)n, (uint32_t)c + 1u});
-    };
-    const uint32_t cls_order[3] = {CLS_LIGHT, CLS_PAIR, CLS_FUSED};
-    // rounds: through the deepest node with a task of its own or pair tasks
+    const size_t nn = nodes.size();
+    for (const BTask& tk : active)
+        if (nodes[tk.node].depth != 1) return GVA_OK;
     int D = 0;
-    for (size_t id = 0; id < nn; ++id)
-        if (nodes[id].depth > 0 && live((int)id) && (own[id] || n_pairs[id])) D = std::max(D, nodes[id].depth);
+    for (const BNode& nd : nodes) D = std::max(D, nd.depth);
     if (D < 1) return GVA_OK;
-    // per depth: widest input row, tasks of each class at most
-    std::vector<uint32_t> kmax(D + 2, 1), light_at(D + 2, 0), fused_at(D + 2, 0), pair_at(D + 2, 0);
-    for (size_t id = 0; id < nn; ++id) {
-        const BNode& nd = nodes[id];
-        if (nd.depth < 1 || nd.depth > D) continue;
+    // per depth: widest input row, nodes, nodes of each class
+    std::vector<uint32_t> kmax(D + 2, 1), at_depth(D + 2, 0), light_at(D + 2, 0), fused_at(D + 2, 0);
+    for (const BNode& nd : nodes) {
         kmax[nd.depth] = std::max(kmax[nd.depth], nd.width_in);
-        if (own[id]) (nd.fused ? fused_at : light_at)[nd.depth]++;
-        pair_at[nd.depth] += n_pairs[id];
+        at_depth[nd.depth]++;
+        (nd.fused ? fused_at : light_at)[nd.depth]++;
     }
     uint32_t refs_cap = 1;
-    for (int d = 1; d <= D; ++d) refs_cap = std::max(refs_cap, light_at[d] + fused_at[d] + pair_at[d]);
+    for (int d = 1; d <= D; ++d) refs_cap = std::max(refs_cap, at_depth[d]);
     std::vector<uint32_t> R(D + 2, 32);
     for (int d = 1; d <= D; ++d)
         R[d] = std::min<uint32_t>(tune.rows_per_item, std::max<uint32_t>(32, (768 / kmax[d]) & ~31u));
-    // per node: the templates of the tasks that read its output, light class first
+    // children that can match, light class first: counted per node, placed
+    // by a prefix over the nodes, then listed (both passes on the host's
+    // cores, by ranges of nodes)
     std::vector<NodeRun> info(nn);
-    std::vector<uint2> kids;
-    kids.reserve(2 * nn);
-    for (size_t id = 0; id < nn; ++id) {
-        const BNode& nd = nodes[id];
-        NodeRun r{};
-        r.child0 = (uint32_t)kids.size();
-        r.out_w = nd.kind == STEP_EXT ? nd.width_in + 1 : nd.width_in;
-        size_t cnt[3] = {0, 0, 0};
-        for (uint32_t cls : cls_order)
+    const unsigned T = nn >= 8192 ? std::min<unsigned>(pool_width(), 32) : 1u;
+    std::atomic<bool> too_many{false};
+    pool_run(T, [&](unsigned t) {
+        for (size_t id = nn * t / T; id < nn * (t + 1) / T; ++id) {
+            const BNode& nd = nodes[id];
+            NodeRun r{};
+            r.out_w = nd.kind == STEP_EXT ? nd.width_in + 1 : nd.width_in;
+            size_t cnt[2] = {0, 0};
             for (int c = nd.first_child; c >= 0; c = nodes[c].next_sibling)
-                if (live(c) && !by_pair[c])  // leaves counted in id's pair tasks are done
-                    templates(c, cls, [&](uint2 tp) {
-                        kids.push_back(tp);
-                        cnt[cls]++;
-                    });
-        if (cnt[0] > 0xffff || cnt[1] > 0xffff || cnt[2] > 0xffff) return GVA_OK;  // beyond the schedule's task counts
-        r.n_light = (uint16_t)cnt[CLS_LIGHT];
-        r.n_fused = (uint16_t)cnt[CLS_FUSED];
-        r.n_pair = (uint16_t)cnt[CLS_PAIR];
-        info[id] = r;
-    }
-    // the first round's tasks (depth 1, from the seed lists): light class,
-    // pair tasks, fused class
-    std::vector<TaskRef> r0;
-    r0.reserve(2 * active.size());
-    uint32_t n_cls0[3] = {0, 0, 0};
-    for (uint32_t cls : cls_order) {
-        const size_t before = r0.size();
-        for (const BTask& tk : active) {
-            if (!live(tk.node) || tk.rows == 0) continue;
-            templates(tk.node, cls, [&](uint2 tp) { r0.push_back(TaskRef{tp.x, tp.y, tk.in, tk.rows}); });
+                if (!nodes[c].always_empty) cnt[nodes[c].fused ? 1 : 0]++;
+            if (cnt[0] > 0xffff || cnt[1] > 0xffff) too_many = true;  // beyond the schedule's child counts
+            r.n_light = (uint16_t)cnt[0];
+            r.n_fused = (uint16_t)cnt[1];
+            info[id] = r;
         }
-        n_cls0[cls] = (uint32_t)(r0.size() - before);
+    });
+    if (too_many) return GVA_OK;
+    uint32_t nk = 0;
+    for (size_t id = 0; id < nn; ++id) {
+        info[id].child0 = nk;
+        nk += info[id].n_light + info[id].n_fused;
+    }
+    std::vector<uint32_t> kids(nk);
+    pool_run(T, [&](unsigned t) {
+        for (size_t id = nn * t / T; id < nn * (t + 1) / T; ++id) {
+            uint32_t at[2] = {info[id].child0, info[id].child0 + info[id].n_light};
+            for (int c = nodes[id].first_child; c >= 0; c = nodes[c].next_sibling)
+                if (!nodes[c].always_empty) kids[at[nodes[c].fused ? 1 : 0]++] = (uint32_t)c;
+        }
+    });
+    // the first round's tasks (depth 1, from the seed lists), light class first
+    std::vector<TaskRef> r0;
+    r0.reserve(active.size());
+    uint32_t nt_light0 = 0;
+    for (uint32_t f = 0; f < 2; ++f) {
+        for (const BTask& tk : active) {
+            const BNode& nd = nodes[tk.node];
+            if (nd.always_empty || nd.fused != f || tk.rows == 0) continue;
+            r0.push_back(TaskRef{(uint32_t)tk.node, 0u, tk.in, tk.rows});
+        }
+        if (f == 0) nt_light0 = (uint32_t)r0.size();
     }
     std::vector<uint64_t> i0(r0.size() + 1, 0);
-    for (size_t t = 0; t < r0.size(); ++t) i0[t + 1] = i0[t] + (r0[t].nrows + R[1] - 1) / R[1];
-    const uint64_t ni_light0 = i0[n_cls0[CLS_LIGHT]];
-    const uint64_t ni_pair0 = i0[n_cls0[CLS_LIGHT] + n_cls0[CLS_PAIR]] - ni_light0;
+    uint64_t ni_light0 = 0;
+    for (size_t t = 0; t < r0.size(); ++t) {
+        i0[t + 1] = i0[t] + (r0[t].nrows + R[1] - 1) / R[1];
+        if (t + 1 == nt_light0) ni_light0 = i0[t + 1];
+    }
     // two frontier regions (a round writes one while its tasks read the other)
     uint64_t region = db.round_region_bytes.load();
     if (region == 0) region = 2ull << 30;
@@ -2272,7 +2081,7 @@ int BatchSession::run_device() {
     const size_t o_info = o_ntot + al(nn * 8);
     const size_t o_kids = o_info + al(nn * sizeof(NodeRun));
     const uint32_t nb = (refs_cap + kPlanThreads - 1) / kPlanThreads;
-    const size_t o_flag = o_kids + al(std::max<size_t>(kids.size(), 1) * sizeof(uint2));
+    const size_t o_flag = o_kids + al(std::max<size_t>(kids.size(), 1) * 4);
     const size_t o_bsum = o_flag + 256;
     const size_t o_items = o_bsum + al(((size_t)nb + 1) * kPlanVals * 8);
     const size_t o_chunks = o_items + al(items_cap * 8);
@@ -2306,25 +2115,22 @@ int BatchSession::run_device() {
     uint64_t* witem0 = (uint64_t*)(blk + o_witem0);
     uint64_t* ntot = (uint64_t*)(blk + o_ntot);
     NodeRun* d_info = (NodeRun*)(blk + o_info);
-    uint2* d_kids = (uint2*)(blk + o_kids);
+    uint32_t* d_kids = (uint32_t*)(blk + o_kids);
     uint32_t* d_flag = (uint32_t*)(blk + o_flag);
     uint64_t* items = (uint64_t*)(blk + o_items);
     uint64_t* chunks = (uint64_t*)(blk + o_chunks);
     RunState s1{};
     s1.ni = i0.back();
     s1.ni_light = ni_light0;
-    s1.ni_pair = ni_pair0;
     s1.nt = (uint32_t)r0.size();
-    s1.nt_light = n_cls0[CLS_LIGHT];
-    s1.nt_pair = n_cls0[CLS_PAIR];
+    s1.nt_light = nt_light0;
     // pageable sources: each copy is complete when its call returns
     GVA_CUDA_B(cudaMemsetAsync(blk + o_state, 0, (D + 2) * sizeof(RunState), s));
     GVA_CUDA_B(cudaMemsetAsync(ntot, 0, nn * 8, s));
     GVA_CUDA_B(cudaMemsetAsync(d_flag, 0, 4, s));
     GVA_CUDA_B(cudaMemcpyAsync(states + 1, &s1, sizeof s1, cudaMemcpyHostToDevice, s));
     GVA_CUDA_B(cudaMemcpyAsync(d_info, info.data(), nn * sizeof(NodeRun), cudaMemcpyHostToDevice, s));
-    if (!kids.empty())
-        GVA_CUDA_B(cudaMemcpyAsync(d_kids, kids.data(), kids.size() * sizeof(uint2), cudaMemcpyHostToDevice, s));
+    if (!kids.empty()) GVA_CUDA_B(cudaMemcpyAsync(d_kids, kids.data(), kids.size() * 4, cudaMemcpyHostToDevice, s));
     if (!r0.empty()) GVA_CUDA_B(cudaMemcpyAsync(refs[1], r0.data(), r0.size() * sizeof(TaskRef), cudaMemcpyHostToDevice, s));
     GVA_CUDA_B(cudaMemcpyAsync(item0[1], i0.data(), i0.size() * 8, cudaMemcpyHostToDevice, s));
 
@@ -2357,11 +2163,6 @@ int BatchSession::run_device() {
         if (fused_at[d]) {
             const size_t smem = round_smem_bytes(R[d], kmax[d], false, true);
             round_count_kernel<true><<<grid((const void*)round_count_kernel<true>, smem), kRoundWarps * 32, smem, s>>>(ra);
-            ++nl;
-        }
-        if (pair_at[d]) {
-            const size_t smem = pair_smem_bytes(R[d], kmax[d]);
-            round_pair_kernel<<<grid((const void*)round_pair_kernel, smem), kRoundWarps * 32, smem, s>>>(ra);
             ++nl;
         }
         scan_items_local_kernel<<<2 * sms, 1024, 0, s>>>(items, 0, chunks, states + d);

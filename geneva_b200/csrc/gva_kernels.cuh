@@ -129,17 +129,6 @@ __device__ __forceinline__ uint32_t find_in(const uint32_t* __restrict__ adj, ui
     return (pos < hi && __ldg(adj + pos) == w) ? pos : 0xffffffffu;
 }
 
-// A row of width k + 1 that exists only as a row of width k plus the
-// candidate c in column k: a step that follows another is evaluated on the
-// rows the first one would write without writing them.  The row helpers
-// below take either this or a plain pointer to k words.
-struct ExtRow {
-    const uint32_t* row;
-    uint32_t k;
-    uint32_t c;
-    __device__ __forceinline__ uint32_t operator[](uint32_t j) const { return j < k ? row[j] : c; }
-};
-
 // Candidate source of a row with fused checks: the shortest of the source
 // segment and the dir-0 check segments, each cut below the restriction
 // bound.  The segments stay in the state, so that membership tests of the
@@ -153,8 +142,7 @@ struct GenState {
     uint32_t clo[kMaxChecks], chi[kMaxChecks];  // dir-0 check segments
 };
 
-template <class Row>
-__device__ __forceinline__ void ext_generator(const ExtArgs& p, const Row& row, GenState& g) {
+__device__ __forceinline__ void ext_generator(const ExtArgs& p, const uint32_t* row, GenState& g) {
     uint32_t slo, shi;
     seg_of(p.off, p.L, row[p.src_col], p.lab, slo, shi);
     g.gadj = p.adj;
@@ -205,8 +193,7 @@ __device__ __forceinline__ bool seg_has(const uint32_t* __restrict__ off, const 
 
 // Whether generated candidate c survives injectivity, the source edge (when
 // the generator is a check segment) and every other check.
-template <class Row>
-__device__ __forceinline__ bool ext_accept(const ExtArgs& p, const Row& row, uint32_t c, const GenState& g) {
+__device__ __forceinline__ bool ext_accept(const ExtArgs& p, const uint32_t* row, uint32_t c, const GenState& g) {
     for (uint32_t j = 0; j < p.n_eq; ++j)
         if (row[p.eq_cols[j]] == c) return false;
     if (g.which >= 0 && find_in(p.adj, g.slo, g.shi, c) == 0xffffffffu) return false;
@@ -223,9 +210,9 @@ __device__ __forceinline__ bool ext_accept(const ExtArgs& p, const Row& row, uin
 // row's NEQ matched vertices (columns eq_cols), in one pass over the list;
 // the list is ascending, so the walk stops at the bound (no search for it).
 // A vertex in two columns still excludes its candidate once.
-template <int NEQ, class Row>
+template <int NEQ>
 __device__ __forceinline__ uint32_t short_list_count(const uint32_t* __restrict__ adj, uint32_t lo, uint32_t hi,
-                                                     uint64_t b, const Row& row, const uint8_t* eq_cols) {
+                                                     uint64_t b, const uint32_t* row, const uint8_t* eq_cols) {
     uint32_t eqv[NEQ > 0 ? NEQ : 1];
 #pragma unroll
     for (int e = 0; e < NEQ; ++e) eqv[e] = row[eq_cols[e]];
@@ -244,8 +231,7 @@ __device__ __forceinline__ uint32_t short_list_count(const uint32_t* __restrict_
 // Number of candidates of one row of a plain extension (no fused checks):
 // the segment below the restriction bound minus the already-matched
 // vertices in it.
-template <class Row>
-__device__ __forceinline__ uint32_t ext_count_plain(const ExtArgs& p, const Row& row) {
+__device__ __forceinline__ uint32_t ext_count_plain(const ExtArgs& p, const uint32_t* row) {
     uint32_t lo, hi;
     seg_of(p.off, p.L, row[p.src_col], p.lab, lo, hi);
     if (lo >= hi) return 0;
@@ -291,8 +277,7 @@ __device__ __forceinline__ uint32_t ext_count_row(const ExtArgs& p, const uint32
     return ext_count_plain(p, row);
 }
 
-template <class Row>
-__device__ __forceinline__ bool red_keep_row(const RedArgs& p, const Row& row) {
+__device__ __forceinline__ bool red_keep_row(const RedArgs& p, const uint32_t* row) {
     for (uint32_t j = 0; j < p.n_pairs; ++j) {
         const uint32_t s = row[p.rs[j]];
         const uint32_t e = row[p.re[j]];
