@@ -1106,10 +1106,14 @@ BatchSession::~BatchSession() {
     for (void* p : {(void*)d_desc, (void*)d_items, (void*)d_small, (void*)d_chunks, (void*)d_read, acc, d_nodes})
         if (p) cudaFreeAsync(p, s);
     cudaStreamSynchronize(s);
+    pin_give(desc_pin, desc_pin_cap);  // the stream drained: no copy reads it any more
+    if (desc_ev) cudaEventDestroy(desc_ev);
 }
 
 int BatchSession::init() {
     GVA_CUDA_B(cudaSetDevice(db.device));
+    GVA_CUDA_B(cudaEventCreateWithFlags(&desc_ev, cudaEventDisableTiming));
+    inited = true;
     if (budget == 0) {
         if (db.default_budget == 0) {
             size_t fr = 0, tot = 0;
@@ -1555,18 +1559,39 @@ int BatchSession::submit(std::vector<std::vector<Step>>&& wave, const std::vecto
         nodes[cur].first_term = q;
     }
     }
-    // the new nodes' descriptors, on the host's cores, into pinned staging
-    // that the next round ships
+    // the new nodes' descriptors, on the host's cores, into the staging that
+    // the next round (or device-scheduled run) ships; only descriptors not
+    // yet shipped are kept.  An initialised session stages them in pinned
+    // memory (an asynchronous copy), one never initialised in host memory
+    // (tries built without a device make no device call).
     {
         const size_t nn = nodes.size();
-        // host memory only (no device call), so tries are built without a device;
-        // only descriptors not yet shipped are kept
-        if (desc_host.size() < (nn - shipped) * sizeof(TaskDesc)) desc_host.resize((nn - shipped) * sizeof(TaskDesc));
+        const size_t sz = sizeof(TaskDesc);
+        unsigned char* dst = nullptr;
+        if (inited) {
+            if (desc_pending) {  // the last shipment still reads the buffer
+                GVA_CUDA_B(cudaEventSynchronize(desc_ev));
+                desc_pending = false;
+            }
+            const size_t need = (nn - shipped) * sz;
+            if (need > desc_pin_cap) {
+                size_t cap = 0;
+                char* p = pin_take(std::max(need, 2 * desc_pin_cap), cap);
+                if (!p) return fail(GVA_ERR_NOMEM, "pinned staging allocation failed");
+                if (desc_pin && first_node > (int)shipped) memcpy(p, desc_pin, (first_node - shipped) * sz);
+                pin_give(desc_pin, desc_pin_cap);
+                desc_pin = p;
+                desc_pin_cap = cap;
+            }
+            dst = reinterpret_cast<unsigned char*>(desc_pin);
+        } else {
+            if (desc_host.size() < (nn - shipped) * sz) desc_host.resize((nn - shipped) * sz);
+            dst = desc_host.data();
+        }
         const size_t nnew = nn - (size_t)first_node;
         const unsigned T = nnew >= 8192 ? hw : 1u;
         auto fill = [&](unsigned t) {
-            for (size_t id = (size_t)first_node + t; id < nn; id += T)
-                fill_node_desc((int)id, desc_host.data() + (id - shipped) * sizeof(TaskDesc));
+            for (size_t id = (size_t)first_node + t; id < nn; id += T) fill_node_desc((int)id, dst + (id - shipped) * sz);
         };
         pool_run(T, fill);
     }
@@ -1937,10 +1962,15 @@ int BatchSession::ship_nodes() {
         node_cap = cap;
     }
     if (shipped < nodes.size()) {  // descriptors of the nodes submitted since the last shipment
-        // a pageable source: the copy is complete when the call returns, so
-        // the next wave may refill the buffer
-        GVA_CUDA_B(cudaMemcpyAsync((char*)d_nodes + shipped * sizeof(TaskDesc), desc_host.data(),
+        // from pinned staging: asynchronous, the next wave refills the buffer
+        // after desc_ev (from host memory: complete when the call returns)
+        GVA_CUDA_B(cudaMemcpyAsync((char*)d_nodes + shipped * sizeof(TaskDesc),
+                                   inited ? (const void*)desc_pin : (const void*)desc_host.data(),
                                    (nodes.size() - shipped) * sizeof(TaskDesc), cudaMemcpyHostToDevice, s));
+        if (inited) {
+            GVA_CUDA_B(cudaEventRecord(desc_ev, s));
+            desc_pending = true;
+        }
         shipped = nodes.size();
     }
     return GVA_OK;

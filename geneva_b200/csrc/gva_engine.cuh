@@ -251,6 +251,15 @@ private:
     size_t node_cap = 0;
     size_t shipped = 0;            // nodes whose descriptors are on the device
     std::vector<unsigned char> desc_host;  // descriptors filled at submit, shipped by the next round
+                                           // (sessions never initialised: no device)
+    // initialised sessions fill the descriptors into pinned memory instead,
+    // so that shipping them is an asynchronous copy; desc_ev marks the last
+    // copy out of it (the buffer is refilled only after that copy landed)
+    bool inited = false;
+    char* desc_pin = nullptr;
+    size_t desc_pin_cap = 0;
+    cudaEvent_t desc_ev = nullptr;
+    bool desc_pending = false;
     std::vector<int> scratch_order;
     std::vector<char> scratch_flag;
     std::vector<uint64_t> scratch_off;
