@@ -239,9 +239,8 @@ def test_device_rounds_overflow_falls_back_to_host(native, oracle):
              "v 0 1\nv 1 2\nv 2 1\nv 3 2\ne 0 1 1\ne 1 2 1\ne 2 3 1\n",  # a 3-edge path
              "v 0 1\nv 1 2\nv 2 2\nv 3 1\ne 0 1 1\ne 0 2 1\ne 0 3 1\n"]  # a 3-edge star
     checked = len(pats)
-    # a 5-edge path: its 3-edge prefixes (several hundred thousand rows of 4
-    # columns) are written, more than a 1 MiB region holds (its last two steps
-    # are counted from them without being written)
+    # a 5-edge path: its written prefixes (up to millions of rows of 5
+    # columns) outgrow a 1 MiB region, and fit two of 1 GiB
     pats += ["v 0 1\nv 1 2\nv 2 1\nv 3 2\nv 4 1\nv 5 2\ne 0 1 1\ne 1 2 1\ne 2 3 1\ne 3 4 1\ne 4 5 1\n"]
     plans = [gv.Plan.from_text(p) for p in pats]
     want, _, hs = gv.batch_count(gdb, plans, host_rounds=True)
@@ -253,7 +252,7 @@ def test_device_rounds_overflow_falls_back_to_host(native, oracle):
         assert s["device_rounds"] == 0 and s["rounds"] > 0
         assert gdb.tuning["round_region_mb"] == 2
         assert np.array_equal(got, want)
-        gdb.set_tuning(t["rows_per_item"], t["hub"], round_region_mb=64)
+        gdb.set_tuning(t["rows_per_item"], t["hub"], round_region_mb=1024)
         got, _, s = gv.batch_count(gdb, plans)
         assert s["device_rounds"] == s["rounds"] > 0
         assert np.array_equal(got, want)
