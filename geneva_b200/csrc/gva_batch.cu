@@ -1211,6 +1211,42 @@ size_t step_key_bytes(const Step& st, uint8_t* buf) {
     return n;
 }
 
+// A 64-bit hash of the same fields as step_key_bytes, taken from the step
+// directly (no serialisation): steps with equal key bytes hash equal.  Never 0.
+uint64_t step_key_hash(const Step& st) {
+    uint64_t h = 0x243f6a8885a308d3ull;
+    auto mix = [&](uint64_t w) {
+        h = (h ^ w) * 0x9e3779b97f4a7c15ull;
+        h ^= h >> 29;
+    };
+    // the first n of a byte array, 8 at a time, bytes past n masked off
+    auto bytes = [&](const uint8_t* a, uint32_t n) {
+        for (uint32_t j = 0; j < n; j += 8) {
+            uint64_t w = 0;
+            memcpy(&w, a + j, n - j < 8 ? n - j : 8);
+            mix(w);
+        }
+    };
+    mix((uint64_t)st.kind | (uint64_t)st.width_in << 32);
+    mix((uint64_t)st.part | (uint64_t)st.label << 32);
+    mix(st.always_empty);
+    if (st.kind == STEP_EXT) {
+        mix((uint64_t)(uint32_t)st.src_col | (uint64_t)(uint32_t)st.bound_col << 32);
+        mix((uint64_t)st.bound_inclusive | (uint64_t)st.n_eq << 32);
+        bytes(st.eq_cols, st.n_eq);
+        mix(st.n_chk);
+        for (uint32_t i = 0; i < st.n_chk; ++i) {
+            mix((uint64_t)st.chk_col[i] | (uint64_t)st.chk_dir[i] << 8);
+            mix((uint64_t)st.chk_part[i] | (uint64_t)st.chk_lab[i] << 32);
+        }
+    } else if (st.kind == STEP_REDUCE) {
+        mix(st.n_pairs);
+        for (uint32_t i = 0; i < st.n_pairs; ++i)
+            mix((uint64_t)st.rs_col[i] | (uint64_t)st.re_col[i] << 8 | (uint64_t)st.re_label[i] << 32);
+    }
+    return h | 1;
+}
+
 void BatchSession::fill_node_desc(int id, void* out) const {
     const BNode& nd = nodes[id];
     TaskDesc& d = *reinterpret_cast<TaskDesc*>(out);
@@ -2538,20 +2574,9 @@ static void order_by_step_keys(const std::vector<std::vector<Step>>& steps, std:
         return a < b;
     };
     pool_run((unsigned)chunks, [&](unsigned c) {
-        uint64_t kb[64];  // step key bytes, zero-padded to whole words
         for (size_t i = cut[c]; i < cut[c + 1]; ++i) {
             order[i] = (uint32_t)i;
-            for (size_t j = 0; j < steps[i].size(); ++j) {
-                const size_t len = step_key_bytes(steps[i][j], reinterpret_cast<uint8_t*>(kb));
-                const size_t words = (len + 7) / 8;
-                memset(reinterpret_cast<uint8_t*>(kb) + len, 0, words * 8 - len);
-                uint64_t h = 0x243f6a8885a308d3ull ^ len;
-                for (size_t q = 0; q < words; ++q) {
-                    h = (h ^ kb[q]) * 0x9e3779b97f4a7c15ull;
-                    h ^= h >> 29;
-                }
-                key[i * w + j] = h | 1;
-            }
+            for (size_t j = 0; j < steps[i].size(); ++j) key[i * w + j] = step_key_hash(steps[i][j]);
         }
         std::sort(order.begin() + cut[c], order.begin() + cut[c + 1], less);
     });

@@ -113,6 +113,8 @@ struct BatchStats {
 // its input); two steps are the same trie node when these bytes and their
 // parents agree.  buf must hold 512 bytes.
 size_t step_key_bytes(const Step& st, uint8_t* buf);
+// 64-bit hash of the same fields, never 0 (a sort key: equal keys hash equal)
+uint64_t step_key_hash(const Step& st);
 
 int run_batch(DevDB& db, std::vector<std::vector<Step>> steps, cudaStream_t s, uint64_t budget,
               const uint32_t* vgraph, uint32_t G, uint64_t* counts, uint64_t* graph_counts_host,

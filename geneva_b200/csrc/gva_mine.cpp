@@ -40,6 +40,7 @@
 #include "gva_internal.h"
 #include "gva_dplan.h"
 #include "gva_grow.h"
+#include "gva_pool.h"
 
 namespace gva {
 
@@ -77,9 +78,7 @@ int run_mine(DevDB& db, cudaStream_t s, uint64_t budget, uint32_t max_edges, uin
         const unsigned pt = std::max(1u, std::min<unsigned>(nthreads, (unsigned)((b1 - b0) / 64 + 1)));
         std::vector<int> rcs(pt, GVA_OK);
         std::vector<std::string> msgs(pt);
-        std::vector<std::thread> pool;
-        for (unsigned t = 0; t < pt; ++t)
-            pool.emplace_back([&, t]() {
+        pool_run(pt, [&](unsigned t) {
                 uint32_t sdl[3 * kMaxPatEdges];
                 std::unique_ptr<DPlanQuery> dq(new DPlanQuery());
                 std::unique_ptr<DPlan> dp(new DPlan());
@@ -111,7 +110,6 @@ int run_mine(DevDB& db, cudaStream_t s, uint64_t budget, uint32_t max_edges, uin
                     }
                 }
             });
-        for (auto& th : pool) th.join();
         st.plan_ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
         for (unsigned t = 0; t < pt; ++t)
             if (rcs[t]) {
@@ -189,17 +187,11 @@ int run_mine(DevDB& db, cudaStream_t s, uint64_t budget, uint32_t max_edges, uin
         std::vector<uint64_t> key(n * width_k, 0);
         {
             const unsigned kt = std::max(1u, std::min<unsigned>(nthreads, (unsigned)(n / 256 + 1)));
-            std::vector<std::thread> pool;
-            for (unsigned t = 0; t < kt; ++t)
-                pool.emplace_back([&, t]() {
-                    uint8_t kb[512];
-                    for (size_t i = t; i < n; i += kt)
-                        for (size_t j = 0; j < all[i].size(); ++j) {
-                            const size_t len = step_key_bytes(all[i][j], kb);
-                            key[i * width_k + j] = code_hash(kb, (uint32_t)len) | 1;  // 0 marks the end
-                        }
-                });
-            for (auto& th : pool) th.join();
+            pool_run(kt, [&](unsigned t) {
+                for (size_t i = t; i < n; i += kt)
+                    for (size_t j = 0; j < all[i].size(); ++j)
+                        key[i * width_k + j] = step_key_hash(all[i][j]);  // never 0: 0 marks the end
+            });
         }
         std::vector<uint32_t> order(n);
         for (size_t i = 0; i < n; ++i) order[i] = (uint32_t)i;
