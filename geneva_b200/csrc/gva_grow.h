@@ -17,6 +17,7 @@
 
 #include "../../include/geneva.h"
 #include "gva_internal.h"
+#include "gva_pool.h"
 
 namespace gva {
 namespace {
@@ -358,17 +359,15 @@ void parallel_sort(It first, It last, Less less, unsigned nthreads) {
     while (chunks * 2 <= nthreads && chunks < 64) chunks *= 2;
     std::vector<size_t> cut(chunks + 1);
     for (size_t c = 0; c <= chunks; ++c) cut[c] = n * c / chunks;
-    std::vector<std::thread> pool;
-    for (size_t c = 0; c < chunks; ++c)
-        pool.emplace_back([&, c]() { std::sort(first + cut[c], first + cut[c + 1], less); });
-    for (auto& t : pool) t.join();
+    pool_run((unsigned)chunks, [&](unsigned c) { std::sort(first + cut[c], first + cut[c + 1], less); });
     for (size_t width = 1; width < chunks; width *= 2) {
-        pool.clear();
-        for (size_t c = 0; c + width < chunks; c += 2 * width) {
+        const unsigned jobs = (unsigned)((chunks + 2 * width - 1) / (2 * width));
+        pool_run(jobs, [&](unsigned m) {
+            const size_t c = (size_t)m * 2 * width;
+            if (c + width >= chunks) return;
             const size_t lo = cut[c], mid = cut[c + width], hi = cut[std::min(chunks, c + 2 * width)];
-            pool.emplace_back([=]() { std::inplace_merge(first + lo, first + mid, first + hi, less); });
-        }
-        for (auto& t : pool) t.join();
+            std::inplace_merge(first + lo, first + mid, first + hi, less);
+        });
     }
 }
 
@@ -483,9 +482,7 @@ void grow_level(const std::vector<Pattern>& level, const CodeSet& level_codes, F
     std::vector<CodeSet> seen(nthreads);
     std::vector<uint64_t> dropped(nthreads, 0);  // extensions dropped before their codes
     std::vector<std::vector<std::vector<Ext>>> exts(nthreads, std::vector<std::vector<Ext>>(kBuckets));
-    std::vector<std::thread> pool;
-    for (unsigned t = 0; t < nthreads; ++t)
-        pool.emplace_back([&, t]() {
+    pool_run(nthreads, [&](unsigned t) {
             CodeBuf cb;
             // per parent edge e: what removing it leaves, so that the
             // connectivity of (parent + x) - e is known without building it:
@@ -632,7 +629,6 @@ void grow_level(const std::vector<Pattern>& level, const CodeSet& level_codes, F
                 }
             }
         });
-    for (auto& th : pool) th.join();
     // (2) each partition is deduplicated across threads (sorted by code, so
     // the level's order depends on the codes only), and each distinct
     // candidate is kept only if every connected k-edge sub-pattern other
@@ -642,9 +638,7 @@ void grow_level(const std::vector<Pattern>& level, const CodeSet& level_codes, F
     std::vector<std::vector<Pattern>> buckets(kBuckets);
     std::vector<uint64_t> pruned(kBuckets, 0);
     std::atomic<uint32_t> next_bucket{0};
-    pool.clear();
-    for (unsigned t = 0; t < nthreads; ++t)
-        pool.emplace_back([&]() {
+    pool_run(nthreads, [&](unsigned) {
             std::vector<const Ext*> all;
             CodeBuf sb;
             for (uint32_t b; (b = next_bucket.fetch_add(1)) < kBuckets;) {
@@ -679,7 +673,6 @@ void grow_level(const std::vector<Pattern>& level, const CodeSet& level_codes, F
                 }
             }
         });
-    for (auto& th : pool) th.join();
     for (unsigned t = 0; t < nthreads; ++t) gt.pruned += dropped[t];
     std::vector<size_t> at(kBuckets + 1, 0);
     for (uint32_t b = 0; b < kBuckets; ++b) {
@@ -688,15 +681,12 @@ void grow_level(const std::vector<Pattern>& level, const CodeSet& level_codes, F
     }
     next.clear();
     next.resize(at[kBuckets]);
-    pool.clear();
-    for (unsigned t = 0; t < nthreads; ++t)
-        pool.emplace_back([&, t]() {
-            for (uint32_t b = t; b < kBuckets; b += nthreads) {
-                std::copy(buckets[b].begin(), buckets[b].end(), next.begin() + at[b]);
-                std::vector<Pattern>().swap(buckets[b]);
-            }
-        });
-    for (auto& th : pool) th.join();
+    pool_run(nthreads, [&](unsigned t) {
+        for (uint32_t b = t; b < kBuckets; b += nthreads) {
+            std::copy(buckets[b].begin(), buckets[b].end(), next.begin() + at[b]);
+            std::vector<Pattern>().swap(buckets[b]);
+        }
+    });
     exts.clear();
     seen.clear();
     gt.merge_ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_merge).count();
@@ -784,20 +774,17 @@ int mine_levels(uint32_t L, uint32_t P, const std::vector<char>& has_part, const
         std::vector<std::vector<uint8_t>> code_arena(pt);
         std::vector<uint32_t> code_at(fi.size()), code_len(fi.size());
         std::vector<uint8_t> code_thread(fi.size());
-        std::vector<std::thread> pool;
-        for (unsigned t = 0; t < pt; ++t)
-            pool.emplace_back([&, t]() {
-                CodeBuf cb;
-                for (size_t j = t; j < fi.size(); j += pt) {
-                    canonical(next[fi[j]], width, cb);
-                    code_at[j] = (uint32_t)code_arena[t].size();
-                    code_len[j] = cb.len;
-                    code_thread[j] = (uint8_t)t;
-                    code_arena[t].insert(code_arena[t].end(), cb.b, cb.b + cb.len);
-                    texts[j] = query_text(next[fi[j]], labels);
-                }
-            });
-        for (auto& th : pool) th.join();
+        pool_run(pt, [&](unsigned t) {
+            CodeBuf cb;
+            for (size_t j = t; j < fi.size(); j += pt) {
+                canonical(next[fi[j]], width, cb);
+                code_at[j] = (uint32_t)code_arena[t].size();
+                code_len[j] = cb.len;
+                code_thread[j] = (uint8_t)t;
+                code_arena[t].insert(code_arena[t].end(), cb.b, cb.b + cb.len);
+                texts[j] = query_text(next[fi[j]], labels);
+            }
+        });
         level.clear();
         level_codes = CodeSet();
         for (size_t j = 0; j < fi.size(); ++j) {

@@ -16,7 +16,7 @@ from conftest import ROOT
 CSRC = ROOT / "geneva_b200" / "csrc"
 TESTS = ROOT / "tests"
 DRIVERS = {
-    "mine_grow_check": [TESTS / "mine_grow_check.cpp"],
+    "mine_grow_check": [TESTS / "mine_grow_check.cpp", CSRC / "gva_pool.cpp"],
     "dplan_check": [TESTS / "dplan_check.cpp", CSRC / "gva_plan.cpp", CSRC / "gva_graph.cpp"],
     "plan_query_check": [TESTS / "plan_query_check.cpp", CSRC / "gva_plan.cpp", CSRC / "gva_graph.cpp"],
     "graph_build_check": [TESTS / "graph_build_check.cpp", CSRC / "gva_graph.cpp", CSRC / "gva_plan.cpp"],

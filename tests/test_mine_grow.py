@@ -37,7 +37,8 @@ def checker(tmp_path_factory):
     if cxx is None:
         pytest.skip("g++ not available")
     exe = tmp_path_factory.mktemp("grow") / "mine_grow_check"
-    subprocess.run([cxx, "-O2", "-std=c++17", "-pthread", "-o", str(exe), str(ROOT / "tests" / "mine_grow_check.cpp")],
+    subprocess.run([cxx, "-O2", "-std=c++17", "-pthread", "-o", str(exe), str(ROOT / "tests" / "mine_grow_check.cpp"),
+                    str(ROOT / "geneva_b200" / "csrc" / "gva_pool.cpp")],
                    check=True, capture_output=True, text=True)
     return exe
 
