@@ -925,6 +925,18 @@ def batch_bench(args, rank, world, local, dist, torch, gv, workloads):
     torch.cuda.synchronize()
     e2e_t = red(time.perf_counter() - t1, dist.ReduceOp.MAX if dist else None)
     e2e_value = red(e2e_emb, dist.ReduceOp.SUM if dist else None) / e2e_t
+    # the same with the texts planned by the planning kernel on the device
+    c_dev, _, _ = gv.batch_count_texts(gdb, queries, stream=sp, support=True, plan_on_device=True)
+    torch.cuda.synchronize()
+    t1 = time.perf_counter()
+    for _ in range(e2e_steps):
+        c_dev, _, _ = gv.batch_count_texts(gdb, queries, stream=sp, support=True, plan_on_device=True)
+    torch.cuda.synchronize()
+    e2e_dev_t = red(time.perf_counter() - t1, dist.ReduceOp.MAX if dist else None)
+    e2e_dev = {"value": red(e2e_emb, dist.ReduceOp.SUM if dist else None) / e2e_dev_t,
+               "ms_per_step": 1000.0 * e2e_dev_t / e2e_steps, "agree": bool(np.array_equal(c_dev, c)),
+               "path": "gva_batch_count_texts with GVA_BATCH_PLAN_ON_DEVICE (texts read on the host, planned by "
+                       "the planning kernel, lowered on the host), one warm-up call"}
 
     peak, peak_kind = measured_peak_gbs()
     name, s = max(kstats.items(), key=lambda kv: kv[1]["ms"]) if kstats else ("none", {"launches": 0, "ms": 0, "bytes": 0})
@@ -968,7 +980,8 @@ def batch_bench(args, rank, world, local, dist, torch, gv, workloads):
                                            f"counted with supports, each launch shape twice (gva_db_autotune)"),
         "e2e": {"value": e2e_value, "unit": "embeddings/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "note": "pattern texts read, planned on the host's cores and matched in one call each step "
-                        "(gva_batch_count_texts), counts and supports copied to host memory; database resident"},
+                        "(gva_batch_count_texts), counts and supports copied to host memory; database resident",
+                "plan_on_device": e2e_dev},
         "gpu_launches": launches,
         "clocks": clk,
     }
