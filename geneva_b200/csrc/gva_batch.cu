@@ -2558,7 +2558,13 @@ static void order_by_step_keys(const std::vector<std::vector<Step>>& steps, std:
     const size_t n = steps.size();
     size_t w = 1;
     for (const auto& v : steps) w = std::max(w, v.size());
-    std::vector<uint64_t> key(n * w, 0);  // 0 ends a plan's sequence
+    // 0 ends a plan's sequence; the buffer is kept per thread (a fresh one
+    // of this size would be mapped and faulted in page by page every call)
+    // (a local reference: the jobs below run on other threads, where the
+    // thread-local name would mean their own buffer)
+    static thread_local std::vector<uint64_t> key_buf;
+    std::vector<uint64_t>& key = key_buf;
+    key.assign(n * w, 0);
     // chunks of the plans, each hashed and sorted by one job, then merged pairwise
     size_t chunks = 1;
     const size_t width = n < 2048 ? 1 : std::min<size_t>(32, pool_width());
