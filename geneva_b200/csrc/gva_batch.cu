@@ -301,45 +301,64 @@ __device__ __forceinline__ bool injective8(const uint32_t (&eqv)[8], uint32_t c)
     return !coll;
 }
 
-// Output staging of one warp: accepted (row, candidate) pairs are appended
-// in ballot order to a shared tile of kTileRows rows and flushed 32 rows at a
-// time with coalesced stores.
+// Output staging of one warp: every accepted (row, candidate) is appended
+// in ballot order to a shared tile as a pair (offset of the row among the
+// warp's staged rows, candidate), and the tile is flushed 32 rows at a time:
+// the lanes write the output words in order (coalesced stores), each read
+// from the staged row or from the pair.  Two words per output row in shared
+// memory instead of the whole row.
 struct Tile {
-    uint32_t* t;      // kTileRows * w words
-    uint32_t w;       // output row width
-    uint32_t n;       // rows held
-    uint32_t* out;    // next output row in global memory
-    uint64_t room;    // rows this item may still write (its count from the count pass)
+    uint32_t* t;           // kTileRows (row offset, candidate) pairs
+    const uint32_t* base;  // the staged rows the offsets point into
+    uint32_t k;            // input row width
+    uint32_t w;            // output row width: k + 1 (extension) or k (reduction)
+    uint32_t inv;          // ceil(2^20 / w): q / w = (q * inv) >> 20 for every q < kTileRows * w
+    uint32_t n;            // rows held
+    uint32_t* out;         // next output row in global memory
+    uint64_t room;         // rows this item may still write (its count from the count pass)
 };
+
+__device__ __forceinline__ void tile_init(Tile& tl, uint32_t* t, const uint32_t* base, uint32_t k, bool extend,
+                                          uint32_t* out, uint64_t room) {
+    tl.t = t;
+    tl.base = base;
+    tl.k = k;
+    tl.w = extend ? k + 1 : k;
+    tl.inv = ((1u << 20) + tl.w - 1) / tl.w;
+    tl.n = 0;
+    tl.out = out;
+    tl.room = room;
+}
 
 __device__ __forceinline__ void tile_flush(Tile& tl, uint32_t rows) {
     const int lane = threadIdx.x & 31;
-    const uint32_t nw = rows * tl.w;
     // never past the item's counted rows, whatever the data (e.g. repeated
     // neighbours, which the count and write tests would see differently)
     const uint32_t keep = (uint32_t)umin64(rows, tl.room);
     const uint32_t kw = keep * tl.w;
-    for (uint32_t w = lane; w < kw; w += 32) tl.out[w] = tl.t[w];
+    for (uint32_t q = lane; q < kw; q += 32) {
+        const uint32_t r = (q * tl.inv) >> 20;
+        const uint32_t col = q - r * tl.w;
+        tl.out[q] = col < tl.k ? tl.base[tl.t[2 * r] + col] : tl.t[2 * r + 1];
+    }
     tl.out += kw;
     tl.room -= keep;
     __syncwarp();
-    const uint32_t rest = (tl.n - rows) * tl.w;
-    for (uint32_t w = lane; w < rest; w += 32) tl.t[w] = tl.t[nw + w];
+    const uint32_t rest = 2 * (tl.n - rows);
+    for (uint32_t q = lane; q < rest; q += 32) tl.t[q] = tl.t[2 * rows + q];
     tl.n -= rows;
     __syncwarp();
 }
 
-// Appends, for every lane with `take`, its row (k words of `row`) followed by
-// `c` when `extend` (output width k + 1), else the row alone.
-__device__ __forceinline__ void tile_append(Tile& tl, bool take, const uint32_t* row, uint32_t k, uint32_t c,
-                                            bool extend) {
+// Appends, for every lane with `take`, its row (`row`, among the staged
+// rows) extended by `c` (an extension) or alone (a reduction).
+__device__ __forceinline__ void tile_append(Tile& tl, bool take, const uint32_t* row, uint32_t c) {
     const int lane = threadIdx.x & 31;
     const uint32_t m = __ballot_sync(0xffffffffu, take);
     if (take) {
         const uint32_t pos = tl.n + __popc(m & ((1u << lane) - 1u));
-        uint32_t* dst = tl.t + pos * tl.w;
-        for (uint32_t q = 0; q < k; ++q) dst[q] = row[q];
-        if (extend) dst[k] = c;
+        tl.t[2 * pos] = (uint32_t)(row - tl.base);
+        tl.t[2 * pos + 1] = c;
     }
     tl.n += __popc(m);
     __syncwarp();
@@ -407,7 +426,7 @@ __device__ __forceinline__ uint64_t ext_item(const TaskDesc& d, const uint32_t* 
                     ok = FUSED ? ext_accept(p, row, c, gen_s[lane]) : (eq8 ? injective8(eqv, c) : ext_injective(p, row, c));
                 }
                 cnt += ok ? 1u : 0u;
-                if (WRITE) tile_append(*tl, ok, row, k, c, true);
+                if (WRITE) tile_append(*tl, ok, row, c);
             }
             // hub rows: the whole warp.  Lists of 128 candidates or more are
             // read as 16-byte vectors (4 consecutive candidates per lane, 128
@@ -440,7 +459,7 @@ __device__ __forceinline__ uint64_t ext_item(const TaskDesc& d, const uint32_t* 
                                 ok = FUSED ? ext_accept(p, hrow, c, gen_s[h])
                                            : (eq8 ? injective8(eqv, c) : ext_injective(p, hrow, c));
                             hc += ok ? 1u : 0u;
-                            if (WRITE) tile_append(*tl, ok, hrow, k, c, true);
+                            if (WRITE) tile_append(*tl, ok, hrow, c);
                         }
                     }
                 } else {
@@ -454,7 +473,7 @@ __device__ __forceinline__ uint64_t ext_item(const TaskDesc& d, const uint32_t* 
                                        : (eq8 ? injective8(eqv, c) : ext_injective(p, hrow, c));
                         }
                         hc += ok ? 1u : 0u;
-                        if (WRITE) tile_append(*tl, ok, hrow, k, c, true);
+                        if (WRITE) tile_append(*tl, ok, hrow, c);
                     }
                 }
                 hc = __reduce_add_sync(0xffffffffu, hc);
@@ -486,7 +505,7 @@ __device__ __forceinline__ uint64_t red_item(const TaskDesc& d, const uint32_t* 
         const bool valid = r < nr;
         const uint32_t* row = rows_s + (valid ? r : 0) * k;
         const bool keep = valid && red_keep_row(p, row);
-        if (WRITE) tile_append(*tl, keep, row, k, 0, false);
+        if (WRITE) tile_append(*tl, keep, row, 0u);
         if (graphs) add_graph_count(ctx, d.query, row[0], keep ? 1u : 0u, valid);
         total += keep ? 1u : 0u;
     }
@@ -507,7 +526,7 @@ constexpr size_t kGenBytes = 32 * sizeof(GenState);  // per warp
 // generator states already take shared memory, stages one item at a time.
 __host__ __device__ constexpr uint32_t row_buffers(bool fused) { return fused ? 1u : 2u; }
 __host__ __device__ constexpr size_t round_warp_words(uint32_t rows_per_item, uint32_t kmax, bool write, bool fused) {
-    return (((size_t)row_buffers(fused) * rows_per_item * kmax + (write ? (size_t)kTileRows * (kmax + 1) : 0)) + 3) &
+    return (((size_t)row_buffers(fused) * rows_per_item * kmax + (write ? (size_t)kTileRows * 2 : 0)) + 3) &
            ~(size_t)3;
 }
 size_t round_smem_bytes(uint32_t rows_per_item, uint32_t kmax, bool write, bool fused) {
@@ -778,11 +797,7 @@ round_write_kernel(RoundArgs a) {
                 cur ^= 1;
             }
             Tile tl;
-            tl.t = ws.tile;
-            tl.w = ext ? k + 1 : k;
-            tl.n = 0;
-            tl.out = out + (off - t_off0) * tl.w;
-            tl.room = off_next - off;
+            tile_init(tl, ws.tile, rows, k, ext, out + (off - t_off0) * (ext ? k + 1 : k), off_next - off);
             if (FUSED)
                 ext_item<true, true>(d, rows, nr, a.hub, a.ctx, &tl, ws.gen, nullptr);
             else if (ext)
