@@ -790,8 +790,8 @@ def batch_bench(args, rank, world, local, dist, torch, gv, workloads):
     # list (untimed), kept for every step
     tuning = gdb.autotune(plans[:args.tune_patterns], stream=sp) if args.tune_patterns > 0 else gdb.tuning
 
-    def step(profile=False):
-        counts, sup, stats = gv.batch_count(gdb, plans, stream=sp, support=True, profile=profile)
+    def step(profile=False, **rounds):
+        counts, sup, stats = gv.batch_count(gdb, plans, stream=sp, support=True, profile=profile, **rounds)
         return counts, sup, stats
 
     for _ in range(max(args.warmup, 3)):
@@ -839,12 +839,14 @@ def batch_bench(args, rank, world, local, dist, torch, gv, workloads):
         flush.zero_()
     stream.synchronize()
     torch.cuda.nvtx.range_push("device_step")
-    step()
+    step(device_rounds=True)
     torch.cuda.nvtx.range_pop()
     stream.synchronize()
 
-    # ---- the same step with every round scheduled on the host (each round's
-    # totals read back before its write pass), for comparison
+    # ---- the same step with its rounds scheduled the other way (on the
+    # device when the timed steps were scheduled on the host, and the
+    # reverse), for comparison
+    other = "device" if tstats["device_rounds"] == 0 else "host"
     host_ms = []
     for i in range(3):
         with torch.cuda.stream(stream):
@@ -853,7 +855,7 @@ def batch_bench(args, rank, world, local, dist, torch, gv, workloads):
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record(stream)
-        c_h, s_h, _ = gv.batch_count(gdb, plans, stream=sp, support=True, host_rounds=True)
+        c_h, s_h, _ = gv.batch_count(gdb, plans, stream=sp, support=True, **{other + "_rounds": True})
         e1.record(stream)
         e1.synchronize()
         if i:
@@ -971,11 +973,12 @@ def batch_bench(args, rank, world, local, dist, torch, gv, workloads):
                                                 "round_phase_ms", "wait_ms", "session_ms", "timeline_ms")},
                       timeline="ms from the start of the batched run: plans ordered; per half: session prepared, "
                                "rounds done, results read, session freed",
-                      host_rounds={"ms_per_step": statistics.mean(host_ms),
-                                   "embeddings_per_s": emb_local / args.steps / (statistics.mean(host_ms) / 1000.0),
-                                   "agree": host_rounds_agree,
-                                   "path": "the same step with every round scheduled on the host "
-                                           "(GVA_BATCH_HOST_ROUNDS), mean of 2 after 1 warm-up"}),
+                      scheduling="device" if tstats["device_rounds"] else "host",
+                      other_scheduling={"scheduling": other, "ms_per_step": statistics.mean(host_ms),
+                                        "embeddings_per_s": emb_local / args.steps / (statistics.mean(host_ms) / 1000.0),
+                                        "agree": host_rounds_agree,
+                                        "path": f"the same step with every round scheduled on the {other} "
+                                                f"(GVA_BATCH_{other.upper()}_ROUNDS), mean of 2 after 1 warm-up"}),
         "tuning": dict(tuning, calibration=f"first {min(args.tune_patterns, len(plans))} patterns of the list, "
                                            f"counted with supports, each launch shape twice (gva_db_autotune)"),
         "e2e": {"value": e2e_value, "unit": "embeddings/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,

@@ -96,6 +96,7 @@ class _MniOpts(ctypes.Structure):
 
 BATCH_PLAN_ON_DEVICE = 1
 BATCH_HOST_ROUNDS = 2
+BATCH_DEVICE_ROUNDS = 4
 
 
 class _BatchOpts(ctypes.Structure):
@@ -507,19 +508,22 @@ def match(db: Database, plan: Plan, stream: Optional[int] = None, budget_bytes: 
 
 def batch_count(db: Database, plans: Sequence[Plan], stream: Optional[int] = None, budget_bytes: int = 0,
                 graph_counts: bool = False, support: bool = False, profile: bool = False,
-                host_rounds: bool = False):
+                host_rounds: bool = False, device_rounds: bool = False):
     """Counts embeddings of many plans in shared rounds (gva_batch_count).
 
     Returns (counts[n] uint64, per_graph, stats) where per_graph is the
     [n, num_graphs] uint64 count matrix when graph_counts, else the [n]
-    uint32 supporting-graph counts when support, else None.  host_rounds:
-    schedule every round on the host (GVA_BATCH_HOST_ROUNDS)."""
+    uint32 supporting-graph counts when support, else None.  host_rounds /
+    device_rounds: schedule every round on the host / on the device
+    (GVA_BATCH_HOST_ROUNDS / GVA_BATCH_DEVICE_ROUNDS; default: on the device
+    for a run in one piece, on the host for one split in halves)."""
     n = len(plans)
     arr = _plan_handles(plans)
     counts = np.zeros(n, dtype=np.uint64)
     gc = np.zeros((n, db.num_graphs), dtype=np.uint64) if graph_counts else None
     sup = np.zeros(n, dtype=np.uint32) if support else None
-    o = _BatchOpts(stream or None, budget_bytes, 1 if profile else 0, BATCH_HOST_ROUNDS if host_rounds else 0)
+    o = _BatchOpts(stream or None, budget_bytes, 1 if profile else 0,
+                   (BATCH_HOST_ROUNDS if host_rounds else 0) | (BATCH_DEVICE_ROUNDS if device_rounds else 0))
     st = _BatchStats()
     _check(library().gva_batch_count(db._h, arr.ctypes.data, n, ctypes.byref(o), counts.ctypes.data,
                                      gc.ctypes.data if gc is not None else None,

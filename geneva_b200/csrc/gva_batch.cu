@@ -2614,7 +2614,7 @@ static void order_by_step_keys(const std::vector<std::vector<Step>>& steps, std:
 
 int run_batch(DevDB& db, std::vector<std::vector<Step>> steps, cudaStream_t s, uint64_t budget,
               const uint32_t* vgraph, uint32_t G, uint64_t* counts, uint64_t* graph_counts_host,
-              uint32_t* support_host, bool profile, BatchStats* stats, bool host_rounds) {
+              uint32_t* support_host, bool profile, BatchStats* stats, int rounds) {
     (void)vgraph;
     (void)G;
     const auto t0 = std::chrono::steady_clock::now();
@@ -2632,6 +2632,9 @@ int run_batch(DevDB& db, std::vector<std::vector<Step>> steps, cudaStream_t s, u
     // (a profiled run keeps one stream: per-kernel event timings of two
     // overlapping streams would each include the other's kernels)
     const size_t K = n >= 12288 && !profile ? 2 : 1;
+    // two halves hide each other's host round trips: host scheduling there
+    // (measured faster), device scheduling for a run in one piece
+    const bool host_rounds = rounds == ROUNDS_HOST || (rounds == ROUNDS_AUTO && K == 2);
     std::vector<size_t> cut(K + 1);
     for (size_t k = 0; k <= K; ++k) cut[k] = n * k / K;
     const bool per_graph = graph_counts_host || support_host;

@@ -439,6 +439,12 @@ int gva_db_set_graphs(gva_db* db, const uint64_t* first, uint32_t num_graphs) {
 }
 
 namespace {
+int rounds_mode(int flags) {
+    if (flags & GVA_BATCH_HOST_ROUNDS) return ROUNDS_HOST;
+    if (flags & GVA_BATCH_DEVICE_ROUNDS) return ROUNDS_DEVICE;
+    return ROUNDS_AUTO;
+}
+
 void fill_batch_stats(const BatchStats& bs, double lower_ms, gva_batch_stats* stats) {
     memset(stats, 0, sizeof *stats);
     stats->gpu_ms = bs.gpu_ms;
@@ -469,6 +475,8 @@ int gva_batch_count(gva_db* db, const gva_plan* const* plans, int nplans, const 
     if (!db || (nplans > 0 && (!plans || !counts))) return fail(GVA_ERR_ARG, "null argument");
     gva_batch_opts o{};
     if (opts) o = *opts;
+    if ((o.flags & GVA_BATCH_HOST_ROUNDS) && (o.flags & GVA_BATCH_DEVICE_ROUNDS))
+        return fail(GVA_ERR_ARG, "GVA_BATCH_HOST_ROUNDS and GVA_BATCH_DEVICE_ROUNDS exclude each other");
     std::vector<std::vector<Step>> steps(nplans);
     for (int i = 0; i < nplans; ++i)
         if (!plans[i]) return fail(GVA_ERR_ARG, "null plan");
@@ -481,8 +489,7 @@ int gva_batch_count(gva_db* db, const gva_plan* const* plans, int nplans, const 
     BatchStats bs;
     int st = run_batch(*db->dev, std::move(steps), (cudaStream_t)o.stream, o.budget_bytes, db->dev->vgraph,
                        db->dev->num_graphs,
-                       counts, graph_counts, graph_support, o.profile != 0, &bs,
-                       (o.flags & GVA_BATCH_HOST_ROUNDS) != 0);
+                       counts, graph_counts, graph_support, o.profile != 0, &bs, rounds_mode(o.flags));
     if (stats) fill_batch_stats(bs, lower_ms, stats);
     return st;
 }
@@ -494,6 +501,8 @@ int gva_batch_count_texts(gva_db* db, const char* const* texts, int n, int mode,
     if (mode != GVA_MODE_DV && mode != GVA_MODE_SV) return fail(GVA_ERR_ARG, "mode must be GVA_MODE_DV or GVA_MODE_SV");
     gva_batch_opts o{};
     if (opts) o = *opts;
+    if ((o.flags & GVA_BATCH_HOST_ROUNDS) && (o.flags & GVA_BATCH_DEVICE_ROUNDS))
+        return fail(GVA_ERR_ARG, "GVA_BATCH_HOST_ROUNDS and GVA_BATCH_DEVICE_ROUNDS exclude each other");
     const auto t_lower = std::chrono::steady_clock::now();
     std::vector<std::vector<Step>> steps(n);
     std::vector<int> st(n, GVA_OK);
@@ -608,7 +617,7 @@ int gva_batch_count_texts(gva_db* db, const char* const* texts, int n, int mode,
     BatchStats bs;
     int rc = n ? run_batch(*db->dev, std::move(steps), (cudaStream_t)o.stream, o.budget_bytes, db->dev->vgraph,
                            db->dev->num_graphs, counts, graph_counts, graph_support, o.profile != 0, &bs,
-                           (o.flags & GVA_BATCH_HOST_ROUNDS) != 0)
+                           rounds_mode(o.flags))
                : GVA_OK;
     if (stats) fill_batch_stats(bs, lower_ms, stats);
     if (rc) return rc;

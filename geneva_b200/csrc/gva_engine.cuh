@@ -116,9 +116,12 @@ size_t step_key_bytes(const Step& st, uint8_t* buf);
 // 64-bit hash of the same fields, never 0 (a sort key: equal keys hash equal)
 uint64_t step_key_hash(const Step& st);
 
+// Round scheduling of run_batch: ROUNDS_AUTO = on the device when the run is
+// one piece, on the host when it runs as two halves
+enum RoundsMode { ROUNDS_AUTO = 0, ROUNDS_HOST = 1, ROUNDS_DEVICE = 2 };
 int run_batch(DevDB& db, std::vector<std::vector<Step>> steps, cudaStream_t s, uint64_t budget,
               const uint32_t* vgraph, uint32_t G, uint64_t* counts, uint64_t* graph_counts_host,
-              uint32_t* support_host, bool profile, BatchStats* stats, bool host_rounds = false);
+              uint32_t* support_host, bool profile, BatchStats* stats, int rounds = ROUNDS_AUTO);
 uint64_t batch_kernel_launches();
 
 // Pinned host staging, grown on demand.

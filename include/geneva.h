@@ -180,14 +180,19 @@ typedef struct gva_batch_opts {
  * planner, one query per thread; queries of up to 16 vertices and 32 edge
  * lines, DV mode), the others on the host */
 #define GVA_BATCH_PLAN_ON_DEVICE 1
-/* schedule every round on the host: each round's task totals are read back
- * and the host chooses the writing tasks, their output places (splitting
- * tasks larger than the budget) and the next round's tasks.  By default a
- * run of one batch schedules its rounds on the device (a planning kernel per
- * round; the host launches every round at once) when the budget holds two
- * frontier regions, and falls back to host scheduling when a round outgrows
- * its region. */
+/* Round scheduling.  On the device, a planning kernel per round chooses the
+ * writing tasks, places their outputs and lists the next round's tasks, so
+ * the host launches every round at once and synchronises once (when the
+ * budget holds two frontier regions; a round that outgrows its region makes
+ * the run start over on the host).  On the host, each round's task totals
+ * are read back and the host chooses the writes (splitting tasks larger than
+ * the budget) and the next round's tasks.  By default a run in one piece is
+ * scheduled on the device, and a run of 12,288 plans or more, which runs as
+ * two halves whose round trips hide behind each other's kernels, on the
+ * host (measured the faster of the two there).  The flags force one or the
+ * other; they exclude each other. */
 #define GVA_BATCH_HOST_ROUNDS 2
+#define GVA_BATCH_DEVICE_ROUNDS 4
 
 typedef struct gva_batch_stats {
     double gpu_ms;

@@ -260,3 +260,25 @@ def test_device_rounds_overflow_falls_back_to_host(native, oracle):
         gdb.set_tuning(t["rows_per_item"], t["hub"], round_region_mb=t["round_region_mb"])
     oracle.free(og)
     gdb.close()
+
+
+def test_split_runs_schedule_on_the_host_unless_asked(small_db, oracle):
+    """A run of 12,288 plans or more runs as two halves, scheduled on the host
+    by default; GVA_BATCH_DEVICE_ROUNDS schedules the same halves on the
+    device, with the same results; the two flags together are refused."""
+    import ctypes
+    db, gdb, og = small_db
+    pats = [p for p in _patterns(db, 120, 43) if oracle.count(og, p, cap_rows=1_000_000) is not None]
+    reps = 12288 // len(pats) + 1
+    plans = gv.Plan.batch_from_texts(pats * reps)
+    hc, hs, hst = gv.batch_count(gdb, plans, support=True)
+    dc, ds, dst = gv.batch_count(gdb, plans, support=True, device_rounds=True)
+    assert hst["device_rounds"] == 0 and dst["device_rounds"] > 0
+    assert np.array_equal(hc, dc) and np.array_equal(hs, ds)
+    assert [int(c) for c in hc[:len(pats)]] == [oracle.count(og, p) for p in pats]
+    o = gv._BatchOpts(None, 0, 0, gv.BATCH_HOST_ROUNDS | gv.BATCH_DEVICE_ROUNDS)
+    counts = np.zeros(len(plans), dtype=np.uint64)
+    arr = gv._plan_handles(plans)
+    rc = gv.library().gva_batch_count(gdb._h, arr.ctypes.data, len(plans), ctypes.byref(o), counts.ctypes.data,
+                                      None, None, None)
+    assert rc != 0 and b"exclude each other" in gv.library().gva_last_error()
