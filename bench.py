@@ -129,20 +129,28 @@ class ClockSampler:
         self.thread = None
 
     def start(self):
+        """Starts sampling every 50 ms and returns once the first sample has
+        arrived (nvidia-smi's start-up, a burst of host work, then lies before
+        the timed region instead of inside it), or after 5 s without one."""
+        self.t0 = time.perf_counter()
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+                 "-lms", "50"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
         except FileNotFoundError:
             return
         self.thread = threading.Thread(target=self._read, daemon=True)
         self.thread.start()
+        deadline = time.perf_counter() + 5.0
+        while not self.samples and time.perf_counter() < deadline:
+            time.sleep(0.005)
+        self.t0 = time.perf_counter()
 
     def _read(self):
         for line in self.proc.stdout:
             parts = [p.strip() for p in line.split(",")]
             if len(parts) >= 8:
-                self.samples.append(parts)
+                self.samples.append((time.perf_counter(), parts))
 
     def stop(self) -> dict:
         if self.proc:
@@ -151,6 +159,10 @@ class ClockSampler:
                 self.proc.wait(timeout=5)
             except subprocess.TimeoutExpired:
                 self.proc.kill()
+        # the samples taken in the timed region (after start() returned); the
+        # last one before it when the region was shorter than the interval
+        inside = [s for t, s in self.samples if t >= self.t0]
+        self.samples = inside or [s for _, s in self.samples[-1:]]
         if not self.samples:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
         sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]

@@ -2633,7 +2633,8 @@ int run_batch(DevDB& db, std::vector<std::vector<Step>> steps, cudaStream_t s, u
     // overlapping streams would each include the other's kernels)
     const size_t K = n >= 12288 && !profile ? 2 : 1;
     // two halves hide each other's host round trips: host scheduling there
-    // (measured faster), device scheduling for a run in one piece
+    // (no schedule tables or frontier regions per half; the two measure
+    // alike), device scheduling for a run in one piece
     const bool host_rounds = rounds == ROUNDS_HOST || (rounds == ROUNDS_AUTO && K == 2);
     std::vector<size_t> cut(K + 1);
     for (size_t k = 0; k <= K; ++k) cut[k] = n * k / K;

@@ -189,8 +189,8 @@ typedef struct gva_batch_opts {
  * the budget) and the next round's tasks.  By default a run in one piece is
  * scheduled on the device, and a run of 12,288 plans or more, which runs as
  * two halves whose round trips hide behind each other's kernels, on the
- * host (measured the faster of the two there).  The flags force one or the
- * other; they exclude each other. */
+ * host (no schedule tables or frontier regions per half; the two measured
+ * alike there).  The flags force one or the other; they exclude each other. */
 #define GVA_BATCH_HOST_ROUNDS 2
 #define GVA_BATCH_DEVICE_ROUNDS 4
 
