@@ -477,7 +477,7 @@ struct DPlanView {
 template <typename View>
 int lower_core(const View& plan, const HostGraph& g, std::vector<Step>& steps, bool fuse_reductions) {
     steps.clear();
-    steps.reserve(plan.nphase() + 2);
+    steps.reserve(2 * plan.nphase() + 1);  // a phase lowers to at most two steps, the first one plus a seed
     int newest = -1;  // query vertex added by the last extension step
     const uint32_t P = (uint32_t)g.parts.size();
     if (plan.vnum() > (uint32_t)kMaxCols) return fail(GVA_ERR_UNSUPPORTED, "query has more than 32 vertices");

@@ -764,14 +764,29 @@ int finish_plan(Planner& p, int mode, Plan& out) {
 
 int read_query_text(const std::string& text, std::vector<uint32_t>& labels_out, std::vector<uint32_t>& sdl) {
     Cursor c(text);
-    std::map<uint32_t, uint32_t> labels;  // vid -> label, first definition wins
+    // vid -> label, first definition wins, kept in vid order (insertion into
+    // a short sorted array; past GVA_MAX_QUERY_VERTICES distinct ids the
+    // query is refused anyway, so one more entry marks that)
+    constexpr uint32_t kCap = GVA_MAX_QUERY_VERTICES + 1;
+    uint32_t vids[kCap], labs[kCap];
+    uint32_t n = 0;
     char ch;
     bool in_edges = false;
     while (c.get(ch)) {
         if (ch == 'v') {
             uint32_t vid, lab;
             if (!c.read_uint(vid) || !c.read_uint(lab)) break;
-            labels.emplace(vid, lab);
+            uint32_t at = n;
+            while (at > 0 && vids[at - 1] > vid) --at;
+            if (at > 0 && vids[at - 1] == vid) continue;  // defined before: the first definition stands
+            if (n == kCap) continue;                      // too many already (refused below)
+            for (uint32_t j = n; j > at; --j) {
+                vids[j] = vids[j - 1];
+                labs[j] = labs[j - 1];
+            }
+            vids[at] = vid;
+            labs[at] = lab;
+            ++n;
         } else if (ch == 'e') {
             --c.i;
             in_edges = true;
@@ -780,14 +795,12 @@ int read_query_text(const std::string& text, std::vector<uint32_t>& labels_out, 
             c.skip_line();
         }
     }
-    const uint32_t n = (uint32_t)labels.size();
     if (n == 0) return fail(GVA_ERR_FORMAT, "query has no vertices");
     if (n > GVA_MAX_QUERY_VERTICES) return fail(GVA_ERR_UNSUPPORTED, "query has more than 32 vertices");
     labels_out.clear();
-    uint32_t expect = 0;
-    for (auto& kv : labels) {
-        if (kv.first != expect++) return fail(GVA_ERR_FORMAT, "query vertex ids must be 0..n-1");
-        labels_out.push_back(kv.second);
+    for (uint32_t i = 0; i < n; ++i) {
+        if (vids[i] != i) return fail(GVA_ERR_FORMAT, "query vertex ids must be 0..n-1");
+        labels_out.push_back(labs[i]);
     }
     if (!in_edges) return fail(GVA_ERR_FORMAT, "query has no edges");
     sdl.clear();

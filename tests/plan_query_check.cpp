@@ -2,7 +2,10 @@
 // (plan_from_query, used by the miner) against its entry from query text
 // (plan_from_text, the reference's input) on seeded random connected queries
 // with cycles, repeated labels and repeated edge lines: plans, output
-// columns and lowered steps must be identical.
+// columns and lowered steps must be identical.  The query reader of the
+// texts path (read_query_text) must give back the arrays each text was made
+// from, and its rules (first definition of a vertex wins, ids 0..n-1, at
+// most 32 vertices, comments skipped) hold on hand-made texts.
 //
 // usage: plan_query_check queries seed
 #include <cstdio>
@@ -59,6 +62,13 @@ int main(int argc, char** argv) {
             sdl.push_back(l);
             text += "e " + std::to_string(e.first) + " " + std::to_string(e.second) + " " + std::to_string(l) + "\n";
         }
+        {
+            std::vector<uint32_t> rl, rs;
+            if (read_query_text(text, rl, rs) || rl != labels || rs != sdl) {
+                printf("query %d: the query reader gives other arrays\n%s", q, text.c_str());
+                return 1;
+            }
+        }
         for (int mode : {GVA_MODE_DV, GVA_MODE_SV}) {
             Plan a, b;
             const int ra = plan_from_text(text, mode, a);
@@ -79,6 +89,32 @@ int main(int argc, char** argv) {
                 return 1;
             }
             ++planned;
+        }
+    }
+    // the reader's rules on hand-made texts
+    struct Case {
+        std::string text;
+        int status;
+        std::vector<uint32_t> labels;
+    };
+    std::string big;
+    for (int v = 0; v < 33; ++v) big += "v " + std::to_string(v) + " 1\n";
+    big += "e 0 1 1\n";
+    const Case cases[] = {
+        {"v 0 1\nv 0 2\nv 1 3\ne 0 1 1\n", GVA_OK, {1, 3}},        // first definition wins
+        {"v 1 3\nv 0 1\ne 0 1 1\n", GVA_OK, {1, 3}},                // ids in any order
+        {"# a comment\nv 0 1\n# another\nv 1 2\ne 0 1 1\n", GVA_OK, {1, 2}},
+        {"v 1 1\nv 2 1\ne 1 2 1\n", GVA_ERR_FORMAT, {}},            // ids not 0..n-1
+        {"v 0 1\nv 1 1\n", GVA_ERR_FORMAT, {}},                     // no edges
+        {"e 0 1 1\n", GVA_ERR_FORMAT, {}},                           // no vertices
+        {big, GVA_ERR_UNSUPPORTED, {}},                               // 33 vertices
+    };
+    for (const Case& c : cases) {
+        std::vector<uint32_t> rl, rs;
+        const int r = read_query_text(c.text, rl, rs);
+        if (r != c.status || (r == GVA_OK && rl != c.labels)) {
+            printf("query reader: status %d on\n%s", r, c.text.c_str());
+            return 1;
         }
     }
     printf("ok %d plans\n", planned);
