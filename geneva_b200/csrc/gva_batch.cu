@@ -2565,10 +2565,10 @@ static int second_stream(int device, cudaStream_t s, cudaStream_t& out) {
 }
 
 // Plans ordered by their sequences of step keys (64-bit hashes of the key
-// bytes), so that plans sharing a step prefix are adjacent and the trie is
-// built against the previous plan only (presorted submit), with the same
-// nodes as the indexed build.  Keys hashed and chunks sorted on the host's
-// cores.
+// fields), so that plans sharing a step prefix are adjacent and the trie is
+// built against the previous plan only (presorted submit), with the nodes of
+// the indexed build (but for seed nodes repeated across buckets, below).
+// Keys hashed, bucketed and sorted on the host's cores.
 static void order_by_step_keys(const std::vector<std::vector<Step>>& steps, std::vector<uint32_t>& order) {
     const size_t n = steps.size();
     size_t w = 1;
@@ -2580,13 +2580,49 @@ static void order_by_step_keys(const std::vector<std::vector<Step>>& steps, std:
     static thread_local std::vector<uint64_t> key_buf;
     std::vector<uint64_t>& key = key_buf;
     key.assign(n * w, 0);
-    // chunks of the plans, each hashed and sorted by one job, then merged pairwise
-    size_t chunks = 1;
-    const size_t width = n < 2048 ? 1 : std::min<size_t>(32, pool_width());
-    while (chunks * 2 <= width) chunks *= 2;
-    std::vector<size_t> cut(chunks + 1);
-    for (size_t c = 0; c <= chunks; ++c) cut[c] = n * c / chunks;
+    // Plans go to buckets by their first two steps (a plan's trie path is
+    // decided in its bucket: plans sharing two or more leading steps share a
+    // bucket), buckets are filled by ranges of plans and sorted one job each;
+    // no merge.  Equal first steps in two buckets only repeat a seed node
+    // (seed nodes launch nothing; their children differ).
+    const size_t T = n < 2048 ? 1 : std::min<size_t>(32, pool_width());
+    const uint32_t B = (uint32_t)std::min<size_t>(256, 4 * T);
+    std::vector<size_t> cut(T + 1);
+    for (size_t c = 0; c <= T; ++c) cut[c] = n * c / T;
+    static thread_local std::vector<uint16_t> bucket_buf;
+    std::vector<uint16_t>& bucket = bucket_buf;
+    bucket.resize(n);
+    std::vector<uint32_t> cnt((size_t)T * B, 0);  // [chunk][bucket], then where the chunk's entries of a bucket start
+    pool_run((unsigned)T, [&](unsigned c) {
+        uint32_t* my = cnt.data() + (size_t)c * B;
+        for (size_t i = cut[c]; i < cut[c + 1]; ++i) {
+            for (size_t j = 0; j < steps[i].size(); ++j) key[i * w + j] = step_key_hash(steps[i][j]);
+            uint64_t h = key[i * w] * 0x9e3779b97f4a7c15ull ^ (w > 1 ? key[i * w + 1] : 0);
+            h ^= h >> 31;
+            h *= 0xbf58476d1ce4e5b9ull;
+            h ^= h >> 29;
+            bucket[i] = (uint16_t)(h % B);
+            my[bucket[i]]++;
+        }
+    });
+    std::vector<size_t> bstart(B + 1, 0);
+    {
+        size_t at = 0;
+        for (uint32_t b = 0; b < B; ++b) {
+            bstart[b] = at;
+            for (size_t c = 0; c < T; ++c) {
+                const uint32_t k = cnt[c * B + b];
+                cnt[c * B + b] = (uint32_t)at;
+                at += k;
+            }
+        }
+        bstart[B] = at;
+    }
     order.resize(n);
+    pool_run((unsigned)T, [&](unsigned c) {
+        uint32_t* my = cnt.data() + (size_t)c * B;
+        for (size_t i = cut[c]; i < cut[c + 1]; ++i) order[my[bucket[i]]++] = (uint32_t)i;
+    });
     auto less = [&](uint32_t a, uint32_t b) {
         const uint64_t* ka = key.data() + (size_t)a * w;
         const uint64_t* kb = key.data() + (size_t)b * w;
@@ -2594,22 +2630,7 @@ static void order_by_step_keys(const std::vector<std::vector<Step>>& steps, std:
             if (ka[j] != kb[j]) return ka[j] < kb[j];
         return a < b;
     };
-    pool_run((unsigned)chunks, [&](unsigned c) {
-        for (size_t i = cut[c]; i < cut[c + 1]; ++i) {
-            order[i] = (uint32_t)i;
-            for (size_t j = 0; j < steps[i].size(); ++j) key[i * w + j] = step_key_hash(steps[i][j]);
-        }
-        std::sort(order.begin() + cut[c], order.begin() + cut[c + 1], less);
-    });
-    for (size_t span = 1; span < chunks; span *= 2) {
-        const unsigned jobs = (unsigned)((chunks + 2 * span - 1) / (2 * span));
-        pool_run(jobs, [&](unsigned m) {
-            const size_t c = (size_t)m * 2 * span;
-            if (c + span >= chunks) return;
-            const size_t lo = cut[c], mid = cut[c + span], hi = cut[std::min(chunks, c + 2 * span)];
-            std::inplace_merge(order.begin() + lo, order.begin() + mid, order.begin() + hi, less);
-        });
-    }
+    pool_run(B, [&](unsigned b) { std::sort(order.begin() + bstart[b], order.begin() + bstart[b + 1], less); });
 }
 
 int run_batch(DevDB& db, std::vector<std::vector<Step>> steps, cudaStream_t s, uint64_t budget,
@@ -2621,8 +2642,6 @@ int run_batch(DevDB& db, std::vector<std::vector<Step>> steps, cudaStream_t s, u
     const size_t n = steps.size();
     std::vector<uint32_t> order;
     order_by_step_keys(steps, order);
-    std::vector<std::vector<Step>> sorted(n);
-    for (size_t i = 0; i < n; ++i) sorted[i] = std::move(steps[order[i]]);
     const double order_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
     // a large batch runs as two contiguous halves of the sorted plans (plans
     // share prefixes within a half), each prepared and run by its own host
@@ -2649,8 +2668,9 @@ int run_batch(DevDB& db, std::vector<std::vector<Step>> steps, cudaStream_t s, u
     std::vector<std::string> errs(K);
     auto run_half = [&](size_t k) {
         PreparedBatch pb;
-        std::vector<std::vector<Step>> part(std::make_move_iterator(sorted.begin() + cut[k]),
-                                            std::make_move_iterator(sorted.begin() + cut[k + 1]));
+        // this half's plans in sorted order, moved out of the caller's list
+        std::vector<std::vector<Step>> part(cut[k + 1] - cut[k]);
+        for (size_t j = 0; j < part.size(); ++j) part[j] = std::move(steps[order[cut[k] + j]]);
         int r = prepare_batch(db, std::move(part), streams[k], budget, per_graph, graph_counts_host != nullptr,
                               profile, pb, true, host_rounds);
         const double t_prep = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
