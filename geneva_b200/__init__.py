@@ -304,13 +304,13 @@ def _text_array(texts: Sequence[str]):
     if n == 0:
         return b"\0", np.zeros(1, dtype=np.uint64)
     buf = ("\0".join(texts) + "\0").encode()
+    if buf.count(b"\0") != n:
+        raise ValueError("query texts must not contain NUL characters")
     lens = np.fromiter(map(len, texts), dtype=np.int64, count=n)
     if len(buf) == int(lens.sum()) + n:  # one byte per character: offsets from the lengths
         starts = np.cumsum(lens + 1) - (lens + 1)
     else:
         ends = np.flatnonzero(np.frombuffer(buf, dtype=np.uint8) == 0)
-        if len(ends) != n:
-            raise ValueError("query texts must not contain NUL characters")
         starts = np.empty(n, dtype=np.int64)
         starts[0] = 0
         starts[1:] = ends[:-1] + 1

@@ -4,6 +4,7 @@ import ctypes
 import re
 import subprocess
 
+import numpy as np
 import pytest
 
 import geneva_b200 as gv
@@ -69,3 +70,23 @@ def test_load_without_gpu_fails_cleanly(native, enron_dir):
     with pytest.raises(gv.GenevaError) as ei:
         gv.loadDataBase(enron_dir / "Enron.mygraph", enron_dir / "Enron.metadata")
     assert ei.value.status == 3
+
+
+def test_text_marshalling_and_plan_batches_host_only(native, golden_plans):
+    """Query texts go to the library as one buffer and an array of pointers
+    into it (one byte per character or not); a plan batch keeps its handles
+    in one array and plans like gva_plan_from_text."""
+    texts = ["v 0 1\nv 1 2\ne 0 1 1\n", "# Zürich\nv 0 3\nv 1 3\ne 0 1 2\n", ""]
+    buf, ptrs = gv._text_array(texts)
+    assert [ctypes.string_at(int(p)).decode() for p in ptrs] == texts
+    with pytest.raises(ValueError):
+        gv._text_array(["v 0 1\0v 1 1"])
+    qs = [g["q"] for g in golden_plans[:200]]
+    batch = gv.Plan.batch_from_texts(qs)
+    assert len(batch) == len(qs) and isinstance(batch, gv.PlanBatch)
+    assert [p.describe() for p in batch] == [gv.Plan.from_text(q).describe() for q in qs]
+    assert np.array_equal(gv._plan_handles(batch), np.array([p._h.value for p in batch], dtype=np.uint64))
+    sub = batch[:5]  # a plain tuple of the batch's plans: handles gathered one by one
+    assert list(gv._plan_handles(sub)) == [p._h.value for p in sub]
+    batch.close()
+    assert all(not p._h for p in batch)
